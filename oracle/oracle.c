@@ -1,0 +1,882 @@
+/* CPU restatement of the reference's GCMC energy hot path (FP64).
+ *
+ * TEST INFRASTRUCTURE: the oracle the GPU kernels are checked against; see
+ * oracle.h. Pinned against the reference itself through tests/golden/.
+ */
+#include "oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define SQR(x) ((x) * (x))
+
+/* NINT of src/utils.h:60 */
+static inline double nint(double x) { return (double)(int)(x >= 0.0 ? x + 0.5 : x - 0.5); }
+
+/* rectangular branch of ApplyBoundaryCondition, src/potentials.h:241-245 */
+static inline void min_image(const or_sys *s, double *d)
+{
+  for (int c = 0; c < 3; c++) d[c] -= s->box[c] * nint(d[c] * (1.0 / s->box[c]));
+}
+
+static inline double dist2(const or_sys *s, const double *a, const double *b, double *d)
+{
+  d[0] = a[0] - b[0];
+  d[1] = a[1] - b[1];
+  d[2] = a[2] - b[2];
+  min_image(s, d);
+  return SQR(d[0]) + SQR(d[1]) + SQR(d[2]);
+}
+
+/* PotentialValue, LENNARD_JONES case: src/potentials.c:5867-5877 */
+double or_lj(const or_sys *s, int ta, int tb, double r2)
+{
+  int ij = ta * s->ntypes + tb;
+  double r3 = s->sig2[ij] / r2;
+  r3 = r3 * r3 * r3;
+  return 4.0 * s->eps[ij] * (r3 * (r3 - 1.0)) - s->shift[ij];
+}
+
+/* PotentialValueCoulombic, EWALD case: src/potentials.c:12471-12472 */
+double or_real_ewald(const or_sys *s, double qa, double qb, double r)
+{
+  return s->coulomb * qa * qb * (erfc(s->alpha * r) / r);
+}
+
+/* ---------------------------------------------------------------------- */
+void or_point_energy(const or_sys *s, int type, double q, const double *p, int exclude,
+                     double *out)
+{
+  double d[3];
+  double uv = 0.0, uc = 0.0, av = 0.0, ac = 0.0;
+  /* framework VDW: src/framework_energy.c:151-170; charge: :258-279 */
+  for (int i = 0; i < s->nfw; i++) {
+    double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
+    if (r2 < s->rc2_vdw) uv += or_lj(s, type, s->fw_type[i], r2);
+    if (s->ewald && q != 0.0 && r2 < s->rc2_cc) uc += or_real_ewald(s, q, s->fw_q[i], sqrt(r2));
+  }
+  /* other adsorbates: src/inter_energy.c:365-388, :455-480 */
+  for (int m = 0; m < s->nmol; m++) {
+    if (m == exclude) continue;
+    for (int a = 0; a < s->natom; a++) {
+      const double *pb = s->ads_xyz + 3 * (m * s->natom + a);
+      double r2 = dist2(s, p, pb, d);
+      if (r2 < s->rc2_vdw) av += or_lj(s, type, s->mol_type[a], r2);
+      if (s->ewald && q != 0.0 && r2 < s->rc2_cc) ac += or_real_ewald(s, q, s->mol_q[a], sqrt(r2));
+    }
+  }
+  out[0] = uv; out[1] = uc; out[2] = av; out[3] = ac;
+}
+
+/* The four difference routines in the order of src/mc_moves.c:1601-1624:
+ * CalculateInterVDWEnergyDifferenceAdsorbate (src/inter_energy.c:3071),
+ * CalculateInterChargeChargeEnergyDifferenceAdsorbate (:3652),
+ * CalculateFrameworkAdsorbateVDWEnergyDifference (src/framework_energy.c:4870),
+ * CalculateFrameworkAdsorbateChargeChargeEnergyDifference (:5412).
+ * A new-position pair energy >= EnergyOverlapCriteria is an overlap. */
+int or_move_delta(const or_sys *s, int m, const double *new_xyz, double *out)
+{
+  double d[3];
+  const double *old_xyz = s->ads_xyz + 3 * m * s->natom;
+  double dav = 0.0, dac = 0.0, dhv = 0.0, dhc = 0.0;
+  out[0] = out[1] = out[2] = out[3] = 0.0;
+  /* adsorbate-adsorbate VDW */
+  for (int a = 0; a < s->natom; a++) {
+    int ta = s->mol_type[a];
+    for (int j = 0; j < s->nmol; j++) {
+      if (j == m) continue;
+      for (int b = 0; b < s->natom; b++) {
+        const double *pb = s->ads_xyz + 3 * (j * s->natom + b);
+        double r2 = dist2(s, new_xyz + 3 * a, pb, d);
+        if (r2 < s->rc2_vdw) {
+          double e = or_lj(s, ta, s->mol_type[b], r2);
+          if (e >= s->overlap) return 1;
+          dav += e;
+        }
+        r2 = dist2(s, old_xyz + 3 * a, pb, d);
+        if (r2 < s->rc2_vdw) dav -= or_lj(s, ta, s->mol_type[b], r2);
+      }
+    }
+  }
+  /* adsorbate-adsorbate charge-charge */
+  if (s->ewald) {
+    for (int a = 0; a < s->natom; a++) {
+      double qa = s->mol_q[a];
+      if (qa == 0.0) continue;
+      for (int j = 0; j < s->nmol; j++) {
+        if (j == m) continue;
+        for (int b = 0; b < s->natom; b++) {
+          double qb = s->mol_q[b];
+          const double *pb = s->ads_xyz + 3 * (j * s->natom + b);
+          double r2 = dist2(s, new_xyz + 3 * a, pb, d);
+          if (r2 < s->rc2_cc) {
+            double e = or_real_ewald(s, qa, qb, sqrt(r2));
+            if (e >= s->overlap) return 1;
+            dac += e;
+          }
+          r2 = dist2(s, old_xyz + 3 * a, pb, d);
+          if (r2 < s->rc2_cc) dac -= or_real_ewald(s, qa, qb, sqrt(r2));
+        }
+      }
+    }
+  }
+  /* framework VDW */
+  for (int a = 0; a < s->natom; a++) {
+    int ta = s->mol_type[a];
+    for (int i = 0; i < s->nfw; i++) {
+      double r2 = dist2(s, new_xyz + 3 * a, s->fw_xyz + 3 * i, d);
+      if (r2 < s->rc2_vdw) {
+        double e = or_lj(s, ta, s->fw_type[i], r2);
+        if (e >= s->overlap) return 1;
+        dhv += e;
+      }
+    }
+  }
+  for (int a = 0; a < s->natom; a++) {
+    int ta = s->mol_type[a];
+    for (int i = 0; i < s->nfw; i++) {
+      double r2 = dist2(s, old_xyz + 3 * a, s->fw_xyz + 3 * i, d);
+      if (r2 < s->rc2_vdw) dhv -= or_lj(s, ta, s->fw_type[i], r2);
+    }
+  }
+  /* framework charge-charge */
+  if (s->ewald) {
+    for (int a = 0; a < s->natom; a++) {
+      double qa = s->mol_q[a];
+      if (qa == 0.0) continue;
+      for (int i = 0; i < s->nfw; i++) {
+        double r2 = dist2(s, new_xyz + 3 * a, s->fw_xyz + 3 * i, d);
+        if (r2 < s->rc2_cc) {
+          double e = or_real_ewald(s, qa, s->fw_q[i], sqrt(r2));
+          if (e >= s->overlap) return 1;
+          dhc += e;
+        }
+      }
+    }
+    for (int a = 0; a < s->natom; a++) {
+      double qa = s->mol_q[a];
+      if (qa == 0.0) continue;
+      for (int i = 0; i < s->nfw; i++) {
+        double r2 = dist2(s, old_xyz + 3 * a, s->fw_xyz + 3 * i, d);
+        if (r2 < s->rc2_cc) dhc -= or_real_ewald(s, qa, s->fw_q[i], sqrt(r2));
+      }
+    }
+  }
+  out[0] = dhv; out[1] = dav; out[2] = dhc; out[3] = dac;
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Ewald Fourier part */
+
+static double recip_factor(const or_sys *s, const int *k)
+{
+  /* SetupKVectors, src/ewald.c:560-595 (orthorhombic: k = 2 pi n / L) */
+  double kx = 2.0 * M_PI * k[0] / s->box[0];
+  double ky = 2.0 * M_PI * k[1] / s->box[1];
+  double kz = 2.0 * M_PI * k[2] / s->box[2];
+  double k2 = kx * kx + ky * ky + kz * kz;
+  double vol = s->box[0] * s->box[1] * s->box[2];
+  double pre = (k[0] == 0 ? 2.0 : 4.0) * M_PI / vol;
+  return s->coulomb * pre * exp((-0.25 / SQR(s->alpha)) * k2) / k2;
+}
+
+/* exp(i k.r) per site for all wave vectors: phase per axis from the
+ * fractional coordinate times 2 pi (src/ewald.c:6941-7100) */
+static void site_phase(const or_sys *s, const double *p, const int *k, double *re, double *im)
+{
+  double a = 2.0 * M_PI * (k[0] * p[0] / s->box[0] + k[1] * p[1] / s->box[1] +
+                           k[2] * p[2] / s->box[2]);
+  *re = cos(a);
+  *im = sin(a);
+}
+
+void or_structure_factor(const or_sys *s, int n, const double *q, const double *xyz,
+                         double *sk)
+{
+  for (int kk = 0; kk < s->nk; kk++) {
+    const int *k = s->kidx + 3 * kk;
+    double sr = 0.0, si = 0.0;
+    for (int i = 0; i < n; i++) {
+      double re, im;
+      site_phase(s, xyz + 3 * i, k, &re, &im);
+      sr += q[i] * re;
+      si += q[i] * im;
+    }
+    sk[2 * kk] = sr;
+    sk[2 * kk + 1] = si;
+  }
+}
+
+void or_ewald_setup(or_sys *s)
+{
+  if (!s->ewald) return;
+  for (int kk = 0; kk < s->nk; kk++) s->kfactor[kk] = recip_factor(s, s->kidx + 3 * kk);
+  or_structure_factor(s, s->nfw, s->fw_q, s->fw_xyz, s->sk_fw);
+  /* EwaldEnergyIon, src/ewald.c:615-724: a unit charge at the origin */
+  double e = 0.0;
+  for (int kk = 0; kk < s->nk; kk++) e += s->kfactor[kk];
+  s->uion = -(e - s->coulomb * s->alpha / sqrt(M_PI));
+  double net = 0.0;
+  for (int i = 0; i < s->nfw; i++) net += s->fw_q[i];
+  s->net_fw = net;
+}
+
+void or_recompute_sk_ads(or_sys *s)
+{
+  if (!s->ewald) return;
+  int n = s->nmol * s->natom;
+  double *q = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double net = 0.0;
+  for (int m = 0; m < s->nmol; m++)
+    for (int a = 0; a < s->natom; a++) {
+      q[m * s->natom + a] = s->mol_q[a];
+      net += s->mol_q[a];
+    }
+  or_structure_factor(s, n, q, s->ads_xyz, s->sk_ads);
+  s->net_ads = net;
+  free(q);
+}
+
+/* intramolecular exclusion erf(alpha r)/r over all charged pairs of one
+ * molecule (src/ewald.c:7312-7330, exclusion list src/molecule.c:2838-2851) */
+static double exclusion_energy(const or_sys *s, const double *xyz)
+{
+  double e = 0.0;
+  for (int a = 0; a < s->natom - 1; a++)
+    for (int b = a + 1; b < s->natom; b++) {
+      if (s->mol_q[a] == 0.0 || s->mol_q[b] == 0.0) continue;
+      double dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1],
+             dz = xyz[3 * a + 2] - xyz[3 * b + 2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      e += s->coulomb * s->mol_q[a] * s->mol_q[b] * erf(s->alpha * r) / r;
+    }
+  return e;
+}
+
+static double self_energy(const or_sys *s)
+{
+  double e = 0.0;
+  for (int a = 0; a < s->natom; a++)
+    if (s->mol_q[a] != 0.0) e += s->coulomb * SQR(s->mol_q[a]) * s->alpha / sqrt(M_PI);
+  return e;
+}
+
+static double mol_charge(const or_sys *s)
+{
+  double q = 0.0;
+  for (int a = 0; a < s->natom; a++) q += s->mol_q[a];
+  return q;
+}
+
+/* CalculateEwaldFourierAdsorbate, src/ewald.c:6859-7567 (charges only) */
+void or_ewald_delta(const or_sys *s, int nold, const double *xold, int nnew,
+                    const double *xnew, double *out, double *sk_new)
+{
+  double e_ads = 0.0, e_host = 0.0;
+  for (int kk = 0; kk < s->nk; kk++) {
+    const int *k = s->kidx + 3 * kk;
+    double dr = 0.0, di = 0.0;
+    for (int o = 0; o < nold; o++)
+      for (int a = 0; a < s->natom; a++) {
+        if (s->mol_q[a] == 0.0) continue;
+        double re, im;
+        site_phase(s, xold + 3 * (o * s->natom + a), k, &re, &im);
+        dr -= s->mol_q[a] * re;
+        di -= s->mol_q[a] * im;
+      }
+    for (int o = 0; o < nnew; o++)
+      for (int a = 0; a < s->natom; a++) {
+        if (s->mol_q[a] == 0.0) continue;
+        double re, im;
+        site_phase(s, xnew + 3 * (o * s->natom + a), k, &re, &im);
+        dr += s->mol_q[a] * re;
+        di += s->mol_q[a] * im;
+      }
+    double sr = s->sk_ads[2 * kk], si = s->sk_ads[2 * kk + 1];
+    double nr = sr + dr, ni = si + di;
+    double f = s->kfactor[kk];
+    e_host += f * (s->sk_fw[2 * kk] * (nr - sr) + s->sk_fw[2 * kk + 1] * (ni - si));
+    e_ads += f * (SQR(nr) - SQR(sr) + SQR(ni) - SQR(si));
+    if (sk_new) { sk_new[2 * kk] = nr; sk_new[2 * kk + 1] = ni; }
+  }
+  double excl_new = 0.0, excl_old = 0.0;
+  for (int o = 0; o < nnew; o++) excl_new += exclusion_energy(s, xnew + 3 * o * s->natom);
+  for (int o = 0; o < nold; o++) excl_old += exclusion_energy(s, xold + 3 * o * s->natom);
+  double self = self_energy(s);
+  double dq = (nnew - nold) * mol_charge(s);
+  double dads = e_ads - (excl_new - excl_old) - (nnew - nold) * self;
+  dads += s->uion * SQR(s->net_ads + dq) - s->uion * SQR(s->net_ads);
+  double dhost = 2.0 * e_host;
+  dhost += 2.0 * s->uion * s->net_fw * (s->net_ads + dq) - 2.0 * s->uion * s->net_fw * s->net_ads;
+  out[0] = dads;
+  out[1] = dhost;
+  out[2] = dq;
+}
+
+void or_total_energy(const or_sys *s, double *out)
+{
+  double hv = 0.0, av = 0.0, hc = 0.0, ac = 0.0, hf = 0.0, af = 0.0;
+  double d[3];
+  for (int m = 0; m < s->nmol; m++)
+    for (int a = 0; a < s->natom; a++) {
+      const double *p = s->ads_xyz + 3 * (m * s->natom + a);
+      int ta = s->mol_type[a];
+      double qa = s->mol_q[a];
+      for (int i = 0; i < s->nfw; i++) {
+        double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
+        if (r2 < s->rc2_vdw) hv += or_lj(s, ta, s->fw_type[i], r2);
+        if (s->ewald && qa != 0.0 && r2 < s->rc2_cc) hc += or_real_ewald(s, qa, s->fw_q[i], sqrt(r2));
+      }
+      for (int j = m + 1; j < s->nmol; j++)
+        for (int b = 0; b < s->natom; b++) {
+          double r2 = dist2(s, p, s->ads_xyz + 3 * (j * s->natom + b), d);
+          if (r2 < s->rc2_vdw) av += or_lj(s, ta, s->mol_type[b], r2);
+          if (s->ewald && qa != 0.0 && s->mol_q[b] != 0.0 && r2 < s->rc2_cc)
+            ac += or_real_ewald(s, qa, s->mol_q[b], sqrt(r2));
+        }
+    }
+  if (s->ewald) {
+    for (int kk = 0; kk < s->nk; kk++) {
+      double f = s->kfactor[kk];
+      af += f * (SQR(s->sk_ads[2 * kk]) + SQR(s->sk_ads[2 * kk + 1]));
+      hf += f * (s->sk_fw[2 * kk] * s->sk_ads[2 * kk] + s->sk_fw[2 * kk + 1] * s->sk_ads[2 * kk + 1]);
+    }
+    double excl = 0.0;
+    for (int m = 0; m < s->nmol; m++) excl += exclusion_energy(s, s->ads_xyz + 3 * m * s->natom);
+    af -= excl + s->nmol * self_energy(s);
+    af += s->uion * SQR(s->net_ads);
+    hf = 2.0 * hf + 2.0 * s->uion * s->net_fw * s->net_ads;
+  }
+  out[0] = hv; out[1] = av; out[2] = hc; out[3] = ac; out[4] = hf; out[5] = af;
+}
+
+/* ---------------------------------------------------------------------- */
+/* MT19937-64 (Matsumoto & Nishimura 2004), as seeded and scaled by the
+ * reference: src/utils.c:324-378 */
+#define MT_NN 312
+#define MT_MM 156
+#define MT_MATRIX_A 0xB5026F5AA96619E9ULL
+#define MT_UM 0xFFFFFFFF80000000ULL
+#define MT_LM 0x7FFFFFFFULL
+
+void or_mt_seed(or_mt64 *g, uint64_t seed)
+{
+  g->mt[0] = seed;
+  for (g->mti = 1; g->mti < MT_NN; g->mti++)
+    g->mt[g->mti] = 6364136223846793005ULL * (g->mt[g->mti - 1] ^ (g->mt[g->mti - 1] >> 62)) +
+                    (uint64_t)g->mti;
+}
+
+static uint64_t mt_next(or_mt64 *g)
+{
+  static const uint64_t mag01[2] = {0ULL, MT_MATRIX_A};
+  uint64_t x;
+  if (g->mti >= MT_NN) {
+    int i;
+    for (i = 0; i < MT_NN - MT_MM; i++) {
+      x = (g->mt[i] & MT_UM) | (g->mt[i + 1] & MT_LM);
+      g->mt[i] = g->mt[i + MT_MM] ^ (x >> 1) ^ mag01[(int)(x & 1ULL)];
+    }
+    for (; i < MT_NN - 1; i++) {
+      x = (g->mt[i] & MT_UM) | (g->mt[i + 1] & MT_LM);
+      g->mt[i] = g->mt[i + (MT_MM - MT_NN)] ^ (x >> 1) ^ mag01[(int)(x & 1ULL)];
+    }
+    x = (g->mt[MT_NN - 1] & MT_UM) | (g->mt[0] & MT_LM);
+    g->mt[MT_NN - 1] = g->mt[MT_MM - 1] ^ (x >> 1) ^ mag01[(int)(x & 1ULL)];
+    g->mti = 0;
+  }
+  x = g->mt[g->mti++];
+  x ^= (x >> 29) & 0x5555555555555555ULL;
+  x ^= (x << 17) & 0x71D67FFFEDA60000ULL;
+  x ^= (x << 37) & 0xFFF7EEE000000000ULL;
+  x ^= (x >> 43);
+  return x;
+}
+
+double or_mt_uniform(or_mt64 *g) { return (double)(mt_next(g) >> 11) * (1.0 / 9007199254740991.0); }
+
+double or_rng_mt(void *ctx, int slot)
+{
+  (void)slot;
+  return or_mt_uniform((or_mt64 *)ctx);
+}
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) */
+void or_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; r++) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    uint32_t n1 = (uint32_t)p1;
+    uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    uint32_t n3 = (uint32_t)p0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* One uniform in [0,1) per (seed, system, step, slot): 53 bits from one half
+ * of a Philox block; the block counter is (step lo, step hi, slot/2, system). */
+double or_philox_uniform(uint64_t seed, uint32_t system, uint64_t step, uint32_t slot)
+{
+  uint32_t ctr[4] = {(uint32_t)step, (uint32_t)(step >> 32), slot >> 1, system};
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t o[4];
+  or_philox4x32(ctr, key, o);
+  uint32_t hi = (slot & 1) ? o[2] : o[0];
+  uint32_t lo = (slot & 1) ? o[3] : o[1];
+  uint64_t x = ((uint64_t)hi << 21) ^ (uint64_t)(lo >> 11);
+  return (double)x * (1.0 / 9007199254740992.0);
+}
+
+typedef struct { uint64_t seed; uint32_t system; uint64_t step; } philox_ctx;
+static double rng_philox(void *ctx, int slot)
+{
+  philox_ctx *c = (philox_ctx *)ctx;
+  return or_philox_uniform(c->seed, c->system, c->step, (uint32_t)slot);
+}
+
+/* ---------------------------------------------------------------------- */
+/* CBMC. Slot numbers name each random draw so that a counter-based stream
+ * can serve the same code; the sequential MT stream ignores them and is
+ * consumed in the reference's order. */
+enum {
+  SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
+  SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16,       /* 16 + 3*i + {z,y,x} */
+  SLOT_ORIENT_SELECT = 63, SLOT_ORIENT = 64,     /* 64 + 4*i + {X0,Y1,Y2} */
+  SLOT_SPHERE = 192                               /* discarded sphere vectors */
+};
+#define MAX_TRIALS 16
+#define MAX_ATOMS 8
+
+/* SelectTrialPosition, src/cbmc.c:563-599 */
+static int select_trial(const double *bf, const int *ov, int n, double u)
+{
+  double largest = -DBL_MAX, sum = 0.0, w[MAX_TRIALS];
+  for (int i = 0; i < n; i++)
+    if (!ov[i] && bf[i] > largest) largest = bf[i];
+  for (int i = 0; i < n; i++) {
+    w[i] = ov[i] ? 0.0 : exp(bf[i] - largest);
+    sum += w[i];
+  }
+  int sel = 0;
+  double cum = w[0], ws = u * sum;
+  while (cum < ws) cum += w[++sel];
+  return sel;
+}
+
+/* RandomNumberOnUnitSphere (src/utils.c:688); for rigid groups the vector is
+ * not used but the reference draws it, so the sequential stream must too */
+static void discard_sphere(or_rng_fn rng, void *ctx, int trial)
+{
+  double r1, r2, sq;
+  int a = 0;
+  do {
+    r1 = 2.0 * rng(ctx, SLOT_SPHERE + 2 * (trial * 4 + (a & 3))) - 1.0;
+    r2 = 2.0 * rng(ctx, SLOT_SPHERE + 2 * (trial * 4 + (a & 3)) + 1) - 1.0;
+    sq = r1 * r1 + r2 * r2;
+    a++;
+  } while (sq >= 1.0 && a < 64);
+}
+
+/* RandomArrayRotationMatrix (Shoemake), src/utils.c:835-874 */
+static void random_rotation(double x0, double y1, double y2, double R[3][3])
+{
+  y1 *= 2.0 * M_PI;
+  y2 *= 2.0 * M_PI;
+  double r1 = sqrt(1.0 - x0), r2 = sqrt(x0);
+  double u0 = cos(y2) * r2, u1 = sin(y1) * r1, u2 = cos(y1) * r1, u3 = sin(y2) * r2;
+  double ci = 2.0 * u0 * u0 - 1.0, ce = 2.0 * u0;
+  R[0][0] = ci + 2.0 * u1 * u1;
+  R[1][1] = ci + 2.0 * u2 * u2;
+  R[2][2] = ci + 2.0 * u3 * u3;
+  R[1][2] = 2.0 * u2 * u3 - ce * u1;
+  R[2][0] = 2.0 * u3 * u1 - ce * u2;
+  R[0][1] = 2.0 * u1 * u2 - ce * u3;
+  R[2][1] = 2.0 * u3 * u2 + ce * u1;
+  R[0][2] = 2.0 * u1 * u3 + ce * u2;
+  R[1][0] = 2.0 * u2 * u1 + ce * u3;
+}
+
+/* energies of one trial configuration of the beads in `beads` (all but the
+ * first bead), ComputeExternalEnergies src/cbmc.c:1179-1476: a host VDW
+ * energy >= EnergyOverlapCriteria for any bead marks the trial overlapping */
+static int trial_energies(const or_sys *s, const double *xyz, int exclude, double *e)
+{
+  e[0] = e[1] = e[2] = e[3] = 0.0;
+  for (int a = 0; a < s->natom; a++) {
+    if (a == s->start_bead) continue;
+    double pe[4];
+    or_point_energy(s, s->mol_type[a], s->mol_q[a], xyz + 3 * a, exclude, pe);
+    if (pe[0] >= s->overlap) return 1;
+    e[0] += pe[0]; e[1] += pe[1]; e[2] += pe[2]; e[3] += pe[3];
+  }
+  return 0;
+}
+
+/* shared body of GrowMolecule (src/cbmc.c:3056-3181) and RetraceMolecule
+ * (:2928-3054) for one rigid group grown from the starting bead */
+static void cbmc_common(const or_sys *s, int retrace, int m, int nf, int nt, or_rng_fn rng,
+                        void *ctx, double *out, double *new_xyz)
+{
+  const int sb = s->start_bead, type0 = s->mol_type[sb];
+  const double q0 = s->mol_q[sb];
+  const int exclude = retrace ? m : s->nmol;
+  const double *old = retrace ? s->ads_xyz + 3 * m * s->natom : NULL;
+  double bf[MAX_TRIALS], e1[MAX_TRIALS][4], pos1[MAX_TRIALS][3];
+  int ov[MAX_TRIALS];
+  int any = 0;
+  out[0] = 1.0;
+  for (int k = 1; k < 6; k++) out[k] = 0.0;
+  /* HandleFirstBead, src/cbmc.c:623-795 */
+  for (int i = 0; i < nf; i++) {
+    if (retrace && i == 0) {
+      pos1[0][0] = old[3 * sb]; pos1[0][1] = old[3 * sb + 1]; pos1[0][2] = old[3 * sb + 2];
+    } else {
+      double sz = rng(ctx, SLOT_FIRST + 3 * i + 0);
+      double sy = rng(ctx, SLOT_FIRST + 3 * i + 1);
+      double sx = rng(ctx, SLOT_FIRST + 3 * i + 2);
+      pos1[i][0] = s->box[0] * sx;
+      pos1[i][1] = s->box[1] * sy;
+      pos1[i][2] = s->box[2] * sz;
+    }
+    or_point_energy(s, type0, q0, pos1[i], exclude, e1[i]);
+    if (e1[i][0] >= s->overlap || e1[i][1] >= s->overlap || e1[i][2] >= s->overlap ||
+        e1[i][3] >= s->overlap) {
+      ov[i] = 1;
+    } else {
+      ov[i] = 0;
+      any = 1;
+      bf[i] = -s->beta * (e1[i][0] + e1[i][2]);      /* LJ_BIASING */
+    }
+  }
+  if (!any) return;
+  double w1 = 0.0;
+  for (int i = 0; i < nf; i++)
+    if (!ov[i]) w1 += exp(bf[i]);
+  int sel = 0;
+  if (!retrace) sel = select_trial(bf, ov, nf, rng(ctx, SLOT_FIRST_SELECT));
+  double rosen = w1 / (double)nf;
+  if (!retrace && rosen < 1e-150) return;   /* MinimumRosenbluthFactor */
+  double u[4] = {e1[sel][0], e1[sel][1], e1[sel][2], e1[sel][3]};
+  double grown[MAX_ATOMS * 3];
+  grown[3 * sb] = pos1[sel][0]; grown[3 * sb + 1] = pos1[sel][1]; grown[3 * sb + 2] = pos1[sel][2];
+
+  if (s->natom > 1) {
+    /* Rosen / RosenOld (src/cbmc.c:2762-2926) with the rigid-group branch of
+     * GenerateTrialOrientationsSimpleSphere (:1480-1578) */
+    double bft[MAX_TRIALS], et[MAX_TRIALS][4], tx[MAX_TRIALS][MAX_ATOMS * 3];
+    int ovt[MAX_TRIALS];
+    int anyt = 0;
+    for (int iu = 0; iu < nt; iu++) {
+      if (retrace && iu == 0) {
+        for (int a = 0; a < 3 * s->natom; a++) tx[0][a] = old[a];
+      } else {
+        discard_sphere(rng, ctx, iu);
+        double x0 = rng(ctx, SLOT_ORIENT + 4 * iu + 0);
+        double y1 = rng(ctx, SLOT_ORIENT + 4 * iu + 1);
+        double y2 = rng(ctx, SLOT_ORIENT + 4 * iu + 2);
+        double R[3][3];
+        random_rotation(x0, y1, y2, R);
+        for (int a = 0; a < s->natom; a++) {
+          double c[3];
+          for (int d = 0; d < 3; d++) c[d] = s->mol_ref[3 * a + d] - s->mol_ref[3 * sb + d];
+          for (int d = 0; d < 3; d++)
+            tx[iu][3 * a + d] = grown[3 * sb + d] + c[0] * R[d][0] + c[1] * R[d][1] + c[2] * R[d][2];
+        }
+      }
+      ovt[iu] = trial_energies(s, tx[iu], exclude, et[iu]);
+      if (!ovt[iu]) {
+        anyt = 1;
+        bft[iu] = -s->beta * (et[iu][0] + et[iu][2]);  /* LJ_BIASING */
+      } else {
+        bft[iu] = 0.0;
+      }
+    }
+    if (!anyt) return;
+    double w = 0.0;
+    for (int iu = 0; iu < nt; iu++)
+      if (!ovt[iu]) w += exp(bft[iu]);
+    w /= (double)nt;
+    int iw = 0;
+    if (!retrace) iw = select_trial(bft, ovt, nt, rng(ctx, SLOT_ORIENT_SELECT));
+    rosen *= w;
+    if (!retrace && rosen < 1e-150) return;
+    for (int k = 0; k < 4; k++) u[k] += et[iw][k];
+    for (int a = 0; a < s->natom; a++)
+      if (a != sb)
+        for (int d = 0; d < 3; d++) grown[3 * a + d] = tx[iw][3 * a + d];
+  }
+  /* LJ-biasing correction, src/cbmc.c:3171-3178 (and :3044-3051) */
+  rosen *= exp(-s->beta * (u[1] + u[3]));
+  out[0] = 0.0;
+  out[1] = rosen;
+  out[2] = u[0]; out[3] = u[2]; out[4] = u[1]; out[5] = u[3];
+  if (new_xyz && !retrace)
+    for (int a = 0; a < 3 * s->natom; a++) new_xyz[a] = grown[a];
+}
+
+void or_cbmc_grow(const or_sys *s, int nf, int nt, or_rng_fn rng, void *ctx, double *out,
+                  double *new_xyz)
+{
+  cbmc_common(s, 0, s->nmol, nf, nt, rng, ctx, out, new_xyz);
+}
+
+void or_cbmc_retrace(const or_sys *s, int m, int nf, int nt, or_rng_fn rng, void *ctx,
+                     double *out)
+{
+  cbmc_common(s, 1, m, nf, nt, rng, ctx, out, NULL);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Energy grids */
+
+/* CalculateDerivativesAtPositionVDW (src/framework_hessian.c:63-109) with the
+ * LJ branch of PotentialThirdDerivative (src/potentials.c:10959-10990).
+ * out = {U, dU/dx, dU/dy, dU/dz, d2U/dxdy, d2U/dxdz, d2U/dydz, d3U/dxdydz} */
+void or_grid_derivatives(const or_sys *s, int type, const double *p, double *o)
+{
+  double d[3];
+  for (int k = 0; k < 8; k++) o[k] = 0.0;
+  for (int i = 0; i < s->nfw; i++) {
+    double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
+    if (r2 >= s->rc2_vdw) continue;
+    int ij = type * s->ntypes + s->fw_type[i];
+    double e = s->eps[ij];
+    double r3 = s->sig2[ij] / r2;
+    r3 = r3 * r3 * r3;
+    double U = 4.0 * e * (r3 * (r3 - 1.0)) - s->shift[ij];
+    double DF = 24.0 * e * (r3 * (1.0 - 2.0 * r3)) / r2;
+    double DDF = 96.0 * e * (r3 * (7.0 * r3 - 2.0)) / SQR(r2);
+    double DDDF = 384.0 * e * (r3 * (5.0 - 28.0 * r3)) / SQR(SQR(r2));
+    o[0] += U;
+    o[1] += d[0] * DF;
+    o[2] += d[1] * DF;
+    o[3] += d[2] * DF;
+    o[4] += DDF * d[0] * d[1];
+    o[5] += DDF * d[0] * d[2];
+    o[6] += DDF * d[1] * d[2];
+    o[7] += DDDF * d[0] * d[1] * d[2];
+  }
+}
+
+/* MakeGrid, src/grids.c:512-585: point (i,j,k) at i*size/n + shift, values
+ * capped above EnergyOverlapCriteria and stored in "unit cube" scaling.
+ * Layout: grid[m][i][j][k] for m=0..7 (the file plane order of
+ * src/grids.c:734-738). */
+void or_grid_build(const or_sys *s, int type, const int npts[3], const double size[3],
+                   const double shift[3], float *grid)
+{
+  const int nx = npts[0] + 1, ny = npts[1] + 1, nz = npts[2] + 1;
+  const size_t plane = (size_t)nx * ny * nz;
+  double delta[3];
+  for (int c = 0; c < 3; c++) delta[c] = size[c] / (double)npts[c];
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        double p[3] = {i * size[0] / npts[0] + shift[0], j * size[1] / npts[1] + shift[1],
+                       k * size[2] / npts[2] + shift[2]};
+        double o[8];
+        or_grid_derivatives(s, type, p, o);
+        if (o[0] > s->overlap) {
+          o[0] = 2.0 * s->overlap;
+          for (int c = 1; c <= 3; c++) {
+            if (o[c] > s->overlap) o[c] = s->overlap;
+            if (o[c] < -s->overlap) o[c] = -s->overlap;
+          }
+          o[4] = o[5] = o[6] = o[7] = 0.0;
+        }
+        size_t idx = ((size_t)i * ny + j) * nz + k;
+        grid[0 * plane + idx] = (float)o[0];
+        grid[1 * plane + idx] = (float)o[1] * delta[0];
+        grid[2 * plane + idx] = (float)o[2] * delta[1];
+        grid[3 * plane + idx] = (float)o[3] * delta[2];
+        grid[4 * plane + idx] = (float)o[4] * (delta[0] * delta[1]);
+        grid[5 * plane + idx] = (float)o[5] * (delta[0] * delta[2]);
+        grid[6 * plane + idx] = (float)o[6] * (delta[1] * delta[2]);
+        grid[7 * plane + idx] = (float)o[7] * (delta[0] * delta[1] * delta[2]);
+      }
+}
+
+/* Cubic Hermite basis on [0,1]: value p0,p1 and slope d0,d1 */
+static inline void hermite(double t, double *h)
+{
+  double t2 = t * t, t3 = t2 * t;
+  h[0] = 1.0 - 3.0 * t2 + 2.0 * t3;   /* p0 */
+  h[1] = 3.0 * t2 - 2.0 * t3;         /* p1 */
+  h[2] = t - 2.0 * t2 + t3;           /* d0 */
+  h[3] = -t2 + t3;                    /* d1 */
+}
+
+/* InterpolateVDWGrid (src/grids.c:979-1077). The reference solves for the 64
+ * tricubic coefficients with the Lekien-Marsden matrix and evaluates the
+ * polynomial; the same interpolant is the tensor product of 1D cubic Hermite
+ * bases over the 8 stored derivatives (f, f_x, f_y, f_z, f_xy, f_xz, f_yz,
+ * f_xyz at the 8 corners), which is what is evaluated here. */
+double or_grid_interpolate(const float *grid, const int npts[3], const double size[3],
+                           const double shift[3], const double cell[3], const double *pin)
+{
+  double p[3];
+  for (int c = 0; c < 3; c++) {
+    p[c] = pin[c] - cell[c] * nint(pin[c] / cell[c]);
+    if (p[c] < 0.0) p[c] += cell[c];
+  }
+  const int nx = npts[0] + 1, ny = npts[1] + 1, nz = npts[2] + 1;
+  const size_t plane = (size_t)nx * ny * nz;
+  double sc[3], r[3];
+  int i0[3];
+  for (int c = 0; c < 3; c++) {
+    sc[c] = ((p[c] - shift[c]) / size[c]) * (double)npts[c];
+    i0[c] = (int)sc[c];
+    r[c] = sc[c] - i0[c];
+  }
+  /* cap, src/grids.c:1058-1060 */
+  for (int dx = 0; dx < 2; dx++)
+    for (int dy = 0; dy < 2; dy++)
+      for (int dz = 0; dz < 2; dz++) {
+        size_t idx = ((size_t)(i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz);
+        if (grid[idx] > 1e10f) return 1e8;
+      }
+  double hx[4], hy[4], hz[4];
+  hermite(r[0], hx);
+  hermite(r[1], hy);
+  hermite(r[2], hz);
+  /* derivative plane for (x order, y order, z order) in {0,1}^3 */
+  static const int plane_of[2][2][2] = {{{0, 3}, {2, 6}}, {{1, 5}, {4, 7}}};
+  double v = 0.0;
+  for (int dx = 0; dx < 2; dx++)
+    for (int dy = 0; dy < 2; dy++)
+      for (int dz = 0; dz < 2; dz++) {
+        size_t idx = ((size_t)(i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz);
+        for (int ox = 0; ox < 2; ox++)
+          for (int oy = 0; oy < 2; oy++)
+            for (int oz = 0; oz < 2; oz++) {
+              double f = grid[plane_of[ox][oy][oz] * plane + idx];
+              v += f * hx[2 * ox + dx] * hy[2 * oy + dy] * hz[2 * oz + dz];
+            }
+      }
+  return v;
+}
+
+/* ---------------------------------------------------------------------- */
+/* GCMC engine on the counter-based stream. Move semantics follow
+ * src/mc_moves.c: TranslationMoveAdsorbate (:1529-1762),
+ * RotationMoveAdsorbate (:2636), SwapAddAdsorbateMove (:6941-7140),
+ * SwapRemoveAdsorbateMove (:7150-7350). */
+
+static void rotate_axis(double *c, int axis, double th)
+{
+  /* RotationAround{X,Y,Z}Axis, src/utils.c:876-936 */
+  double cs = cos(th), sn = sin(th);
+  double x = c[0], y = c[1], z = c[2];
+  if (axis == 0) { c[1] = cs * y + sn * z; c[2] = -sn * y + cs * z; }
+  else if (axis == 1) { c[0] = cs * x - sn * z; c[2] = sn * x + cs * z; }
+  else { c[0] = cs * x + sn * y; c[1] = -sn * x + cs * y; }
+}
+
+void or_mc_run(or_sys *s, const or_mc_params *p, or_mc_state *st, uint64_t step0,
+               long long nsteps)
+{
+  const int na = s->natom;
+  double *nk = s->ewald ? (double *)malloc(sizeof(double) * 2 * s->nk) : NULL;
+  for (long long it = 0; it < nsteps; it++) {
+    philox_ctx ctx = {p->seed, p->system, step0 + (uint64_t)it};
+    double u0 = rng_philox(&ctx, SLOT_MOVE);
+    int mv = 0;
+    while (mv < 3 && u0 >= p->cum[mv]) mv++;
+    if (mv == 0 || mv == 1) {
+      if (s->nmol == 0 || (mv == 1 && na == 1)) continue;
+      st->moves++;
+      st->attempts[mv]++;
+      int m = (int)(rng_philox(&ctx, SLOT_MOLECULE) * s->nmol);
+      if (m >= s->nmol) m = s->nmol - 1;
+      double vnew = 2.0 * rng_philox(&ctx, SLOT_VNEW) - 1.0;
+      int axis = (int)(3.0 * rng_philox(&ctx, SLOT_AXIS));
+      if (axis > 2) axis = 2;
+      double nx[MAX_ATOMS * 3];
+      const double *ox = s->ads_xyz + 3 * m * na;
+      if (mv == 0) {
+        for (int a = 0; a < 3 * na; a++) nx[a] = ox[a];
+        for (int a = 0; a < na; a++) nx[3 * a + axis] += vnew * p->max_translation;
+      } else {
+        int sb = s->start_bead;
+        for (int a = 0; a < na; a++) {
+          double c[3] = {ox[3 * a] - ox[3 * sb], ox[3 * a + 1] - ox[3 * sb + 1],
+                         ox[3 * a + 2] - ox[3 * sb + 2]};
+          rotate_axis(c, axis, vnew * p->max_rotation);
+          for (int d = 0; d < 3; d++) nx[3 * a + d] = c[d] + ox[3 * sb + d];
+        }
+      }
+      double dl[4], de[3] = {0.0, 0.0, 0.0};
+      if (or_move_delta(s, m, nx, dl)) continue;
+      if (s->ewald) or_ewald_delta(s, 1, ox, 1, nx, de, nk);
+      double du = dl[0] + dl[1] + dl[2] + dl[3] + de[0] + de[1];
+      if (rng_philox(&ctx, SLOT_ACCEPT) < exp(-s->beta * du)) {
+        st->accepted[mv]++;
+        for (int a = 0; a < 3 * na; a++) s->ads_xyz[3 * m * na + a] = nx[a];
+        if (s->ewald) memcpy(s->sk_ads, nk, sizeof(double) * 2 * s->nk);
+        st->u[0] += dl[0]; st->u[1] += dl[1]; st->u[2] += dl[2]; st->u[3] += dl[3];
+        st->u[4] += de[1]; st->u[5] += de[0];
+      }
+    } else if (mv == 2) {
+      st->moves++;
+      st->attempts[2]++;
+      if (s->nmol >= s->maxmol) continue;
+      double o[6], nx[MAX_ATOMS * 3];
+      or_cbmc_grow(s, p->ntrial_first, p->ntrial, rng_philox, &ctx, o, nx);
+      if (o[0] != 0.0) continue;
+      double w = o[1], de[3] = {0.0, 0.0, 0.0};
+      if (s->ewald) {
+        or_ewald_delta(s, 0, NULL, 1, nx, de, nk);
+        w *= exp(-s->beta * (de[0] + de[1]));
+      }
+      if (rng_philox(&ctx, SLOT_ACCEPT) < w * p->fugacity_beta_v / (1.0 + s->nmol)) {
+        st->accepted[2]++;
+        for (int a = 0; a < 3 * na; a++) s->ads_xyz[3 * s->nmol * na + a] = nx[a];
+        s->nmol++;
+        if (s->ewald) {
+          memcpy(s->sk_ads, nk, sizeof(double) * 2 * s->nk);
+          s->net_ads += de[2];
+        }
+        st->u[0] += o[2]; st->u[1] += o[3]; st->u[2] += o[4]; st->u[3] += o[5];
+        st->u[4] += de[1]; st->u[5] += de[0];
+      }
+    } else {
+      st->moves++;
+      st->attempts[3]++;
+      if (s->nmol == 0) continue;
+      int m = (int)(rng_philox(&ctx, SLOT_MOLECULE) * s->nmol);
+      if (m >= s->nmol) m = s->nmol - 1;
+      double o[6], de[3] = {0.0, 0.0, 0.0};
+      or_cbmc_retrace(s, m, p->ntrial_first, p->ntrial, rng_philox, &ctx, o);
+      if (o[0] != 0.0) continue;
+      double w = o[1];
+      const double *ox = s->ads_xyz + 3 * m * na;
+      if (s->ewald) {
+        or_ewald_delta(s, 1, ox, 0, NULL, de, nk);
+        w *= exp(s->beta * (de[0] + de[1]));
+      }
+      if (rng_philox(&ctx, SLOT_ACCEPT) < (double)s->nmol / (w * p->fugacity_beta_v)) {
+        st->accepted[3]++;
+        int last = s->nmol - 1;
+        for (int a = 0; a < 3 * na; a++) s->ads_xyz[3 * m * na + a] = s->ads_xyz[3 * last * na + a];
+        s->nmol--;
+        if (s->ewald) {
+          memcpy(s->sk_ads, nk, sizeof(double) * 2 * s->nk);
+          s->net_ads += de[2];
+        }
+        st->u[0] -= o[2]; st->u[1] -= o[3]; st->u[2] -= o[4]; st->u[3] -= o[5];
+        st->u[4] += de[1]; st->u[5] += de[0];
+      }
+    }
+  }
+  free(nk);
+}

@@ -1,0 +1,312 @@
+"""Seeded synthetic adsorption systems for the GCMC energy hot path.
+
+A `System` holds everything the hot path needs: the rigid framework (positions,
+pseudo-atom types, per-atom charges), the pseudo-atom table with its
+Lennard-Jones parameters, the adsorbate molecule definitions, the cell, the
+cut-off and the Ewald parameters, the state point and the MC move mix. The
+same object is written out as RASPA input files (`raspa_io`) for the
+reference and handed to the GPU engine, so both see the same numbers.
+
+Frameworks are placed by seeded random sequential addition (Poisson-disk
+sampling) under periodic boundaries with a minimum separation, as the
+synthetic workloads prescribe; charges are drawn uniformly and shifted so
+the framework is neutral.
+
+Pseudo-atom names follow the RASPA force-field conventions
+(`CH4_sp3`, `C_co2`, `O_co2`, `CH3_sp3`, `CH2_sp3`); the framework types are
+named `Sifw` and `Ofw` so that no name is a prefix of another (the reference
+matches pseudo-atom names by exact string, src/molecule.c:125-135).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import units
+
+# Lennard-Jones parameters (epsilon/k_B in K, sigma in Angstrom) and the
+# default charge (e) of every pseudo-atom used by the synthetic workloads.
+PSEUDO_ATOMS = {
+    #  name       eps/K   sigma   charge  mass
+    "Ofw":      (50.0,   3.00,   0.0,    15.9994),
+    "Sifw":     (22.0,   2.30,   0.0,    28.0855),
+    "CH4_sp3":  (148.0,  3.73,   0.0,    16.04246),
+    "C_co2":    (27.0,   2.80,   0.70,   12.0),
+    "O_co2":    (79.0,   3.05,  -0.35,   15.9994),
+    "CH3_sp3":  (98.0,   3.75,   0.0,    15.03452),
+    "CH2_sp3":  (46.0,   3.95,   0.0,    14.02658),
+}
+TYPE_ORDER = list(PSEUDO_ATOMS.keys())
+
+
+@dataclasses.dataclass
+class Molecule:
+    """A rigid (or single-bead) adsorbate.
+
+    `positions` is the reference geometry in Angstrom; `starting_bead` is the
+    bead placed first by CBMC (src/cbmc.c:623 `HandleFirstBead`), the others
+    are grown as one rigid group (src/cbmc.c:1480-1578).
+    """
+    name: str
+    atom_types: List[str]
+    positions: np.ndarray
+    starting_bead: int = 0
+    rigid: bool = True
+    critical: tuple = (190.564, 4599200.0, 0.01142)
+
+    @property
+    def n_atoms(self) -> int:
+        return len(self.atom_types)
+
+    def charges(self) -> np.ndarray:
+        return np.array([PSEUDO_ATOMS[t][2] for t in self.atom_types], dtype=np.float64)
+
+
+METHANE = Molecule("methane", ["CH4_sp3"], np.zeros((1, 3)), 0, True,
+                   (190.564, 4599200.0, 0.01142))
+CO2 = Molecule("CO2", ["O_co2", "C_co2", "O_co2"],
+               np.array([[0.0, 0.0, 1.16], [0.0, 0.0, 0.0], [0.0, 0.0, -1.16]]),
+               1, True, (304.1282, 7377300.0, 0.22394))
+
+
+@dataclasses.dataclass
+class MoveMix:
+    """Relative move probabilities (normalised when used)."""
+    translation: float = 1.0
+    rotation: float = 0.0
+    swap_insert: float = 0.5   # a 'SwapProbability' p splits into p/2 insert + p/2 delete
+    swap_delete: float = 0.5
+
+    def cumulative(self) -> np.ndarray:
+        p = np.array([self.translation, self.rotation, self.swap_insert, self.swap_delete], float)
+        return np.cumsum(p / p.sum())
+
+
+@dataclasses.dataclass
+class System:
+    name: str
+    unit_cell: np.ndarray            # (3,) orthorhombic cell lengths, Angstrom
+    unit_cells: np.ndarray           # (3,) replication
+    frac: np.ndarray                 # (n_uc, 3) fractional positions in one unit cell
+    uc_types: List[str]              # per unit-cell atom
+    uc_charges: np.ndarray           # per unit-cell atom, e
+    molecule: Molecule
+    temperature: float
+    pressure: float                  # Pa (fugacity, coefficient 1)
+    cutoff: float = 12.0
+    ewald: bool = False
+    alpha: float = 0.265
+    kmax: tuple = (8, 8, 8)
+    trials: int = 10
+    trials_first_bead: int = 10
+    moves: MoveMix = dataclasses.field(default_factory=MoveMix)
+    seed: int = 0
+    max_translation: float = 1.0
+    max_rotation_deg: float = 30.0
+
+    # ----- derived quantities --------------------------------------------
+    @property
+    def box(self) -> np.ndarray:
+        return self.unit_cell * self.unit_cells
+
+    @property
+    def volume(self) -> float:
+        return float(np.prod(self.box))
+
+    def framework(self):
+        """Cartesian framework atoms of the full simulation box.
+
+        Returns (pos[N,3] float64, type[N] int32, charge[N] float64). Atoms are
+        ordered like the reference builds its replicated cell: unit cells in
+        x-major order, then the atoms of each cell in file order.
+        """
+        uc = self.unit_cell
+        cells = []
+        for i in range(int(self.unit_cells[0])):
+            for j in range(int(self.unit_cells[1])):
+                for k in range(int(self.unit_cells[2])):
+                    cells.append((i, j, k))
+        pos = []
+        for (i, j, k) in cells:
+            p = np.empty_like(self.frac)
+            p[:, 0] = uc[0] * self.frac[:, 0] + uc[0] * i
+            p[:, 1] = uc[1] * self.frac[:, 1] + uc[1] * j
+            p[:, 2] = uc[2] * self.frac[:, 2] + uc[2] * k
+            pos.append(p)
+        pos = np.concatenate(pos, axis=0) if pos else np.zeros((0, 3))
+        ncell = len(cells)
+        t = np.array([TYPE_ORDER.index(x) for x in self.uc_types] * ncell, dtype=np.int32)
+        q = np.tile(self.uc_charges, ncell).astype(np.float64)
+        return pos, t, q
+
+    def n_framework(self) -> int:
+        return len(self.uc_types) * int(np.prod(self.unit_cells))
+
+    def lj_tables(self):
+        """Lorentz-Berthelot mixed, truncated-and-shifted LJ table.
+
+        Returns (eps[T,T] internal units, sigma2[T,T] A^2, shift[T,T]) where
+        shift = U(rc) (src/potentials.c:5263-5287, 5867-5877).
+        """
+        n = len(TYPE_ORDER)
+        eps = np.zeros((n, n))
+        sig2 = np.zeros((n, n))
+        shift = np.zeros((n, n))
+        rc2 = self.cutoff ** 2
+        for a, na in enumerate(TYPE_ORDER):
+            for b, nb in enumerate(TYPE_ORDER):
+                ea, sa = PSEUDO_ATOMS[na][:2]
+                eb, sb = PSEUDO_ATOMS[nb][:2]
+                e = math.sqrt(ea * eb) * units.KELVIN_TO_ENERGY
+                s = 0.5 * (sa + sb)
+                eps[a, b] = e
+                sig2[a, b] = s * s
+                r3 = (s * s / rc2) ** 3
+                shift[a, b] = 4.0 * e * (r3 * (r3 - 1.0))
+        return eps, sig2, shift
+
+    def molecule_types(self) -> np.ndarray:
+        return np.array([TYPE_ORDER.index(t) for t in self.molecule.atom_types], dtype=np.int32)
+
+    def n_kvectors(self) -> int:
+        return len(kvector_indices(self.kmax))
+
+
+def kvector_indices(kmax: Sequence[int]) -> np.ndarray:
+    """Integer wave vectors in the reference's order (src/ewald.c:532-599).
+
+    kx runs 0..kmax_x (half space), ky and kz run -kmax..kmax; a vector is kept
+    when 0 < kx^2+ky^2+kz^2 < (1.05*max(kmax))^2 (src/ewald.c:224-259).
+    """
+    kx, ky, kz = (int(k) for k in kmax)
+    rc = (1.05 * max(kx, ky, kz)) ** 2
+    out = []
+    for i in range(0, kx + 1):
+        for j in range(-ky, ky + 1):
+            for k in range(-kz, kz + 1):
+                s = i * i + j * j + k * k
+                if s != 0 and s < rc:
+                    out.append((i, j, k))
+    return np.array(out, dtype=np.int32).reshape(-1, 3)
+
+
+def poisson_disk(rng: np.random.Generator, n: int, cell: np.ndarray, dmin: float,
+                 max_tries: int = 2_000_000) -> np.ndarray:
+    """Random sequential addition of `n` points in an orthorhombic periodic
+    cell with minimum image separation >= dmin. Returns fractional coords."""
+    cell = np.asarray(cell, float)
+    pts = np.empty((n, 3))
+    m = 0
+    tries = 0
+    d2 = dmin * dmin
+    while m < n:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError(f"poisson_disk: could not place {n} points (placed {m})")
+        c = rng.random(3)
+        if m:
+            d = pts[:m] - c
+            d -= np.rint(d)
+            d *= cell
+            if np.min(np.einsum("ij,ij->i", d, d)) < d2:
+                continue
+        pts[m] = c
+        m += 1
+    return pts
+
+
+def _quantise_frac(frac: np.ndarray) -> np.ndarray:
+    # fractional coordinates are written with 12 decimals; keep exactly those
+    return np.round(frac, 12)
+
+
+def _neutral_charges(rng: np.random.Generator, n: int, qmax: float) -> np.ndarray:
+    """Uniform charges in [-qmax, qmax], shifted to a neutral total.
+
+    Charges are kept on a 1e-8 e lattice (the precision written to the CIF)
+    and the lattice sum is made exactly zero, so the neutral framework the
+    reference reads is the one the GPU sees."""
+    q = rng.uniform(-qmax, qmax, n)
+    q -= q.mean()
+    iq = np.rint(q * 1e8).astype(np.int64)
+    iq[-1] -= iq.sum()
+    return iq.astype(np.float64) * 1e-8
+
+
+def _assign_types(n: int, rng: np.random.Generator) -> List[str]:
+    # one third Si, two thirds O, interleaved in a seeded random order
+    n_si = n // 3
+    labels = ["Sifw"] * n_si + ["Ofw"] * (n - n_si)
+    perm = rng.permutation(n)
+    return [labels[i] for i in perm]
+
+
+def methane_system(seed: int = 0, cycles_hint: int = 2000) -> System:
+    """Plain GCMC of single-site methane in a rigid neutral framework:
+    orthorhombic 20.0 x 19.9 x 13.4 A cell replicated 2x2x3, 288 atoms per
+    cell (96 Si, 192 O) at >= 1.6 A separation, 12 A truncated-shifted LJ,
+    T = 300 K, fugacity 1e5 Pa, translation/insertion/deletion in equal
+    proportion."""
+    rng = np.random.default_rng(seed)
+    cell = np.array([20.0, 19.9, 13.4])
+    frac = _quantise_frac(poisson_disk(rng, 288, cell, 1.6))
+    types = ["Sifw"] * 96 + ["Ofw"] * 192
+    return System(
+        name=f"methane_s{seed}", unit_cell=cell, unit_cells=np.array([2, 2, 3]),
+        frac=frac, uc_types=types, uc_charges=np.zeros(288), molecule=METHANE,
+        temperature=300.0, pressure=1e5, cutoff=12.0, ewald=False,
+        moves=MoveMix(translation=1.0, rotation=0.0, swap_insert=0.5, swap_delete=0.5),
+        seed=seed)
+
+
+def co2_system(seed: int = 1, n_atoms: int = 1536, cell: float = 25.8,
+               kmax: int = 8, temperature: float = 298.0, pressure: float = 1e5,
+               dmin: float = 1.5, name: Optional[str] = None) -> System:
+    """Rigid 3-site CO2 in a charged cubic framework: `n_atoms` atoms placed
+    at >= `dmin` separation, charges uniform in [-1.2, 1.2] e shifted to net
+    zero, Ewald alpha = 0.265/A with kmax per axis, 12 A cut-off, CBMC
+    insertion/deletion with 10 first-bead trials x 10 orientations,
+    translation and rotation. Cells narrower than 24 A are replicated 2x2x2,
+    as the reference requires a box of at least twice the cut-off."""
+    rng = np.random.default_rng(seed)
+    c = np.array([cell, cell, cell], float)
+    frac = _quantise_frac(poisson_disk(rng, n_atoms, c, dmin))
+    types = _assign_types(n_atoms, rng)
+    q = _neutral_charges(rng, n_atoms, 1.2)
+    reps = np.array([2, 2, 2]) if cell < 24.0 else np.array([1, 1, 1])
+    return System(
+        name=name or f"co2_s{seed}", unit_cell=c, unit_cells=reps, frac=frac,
+        uc_types=types, uc_charges=q, molecule=CO2, temperature=temperature,
+        pressure=pressure, cutoff=12.0, ewald=True, alpha=0.265,
+        kmax=(kmax, kmax, kmax), trials=10, trials_first_bead=10,
+        moves=MoveMix(translation=1.0, rotation=1.0, swap_insert=1.0, swap_delete=1.0),
+        seed=seed)
+
+
+def batched_co2_systems(n: int = 64, seed: int = 2) -> List[System]:
+    """Independent CO2 systems of uneven size: cubic cells 18-36 A with
+    512-4096 framework atoms (framework density held near the 1536-atom /
+    25.8 A reference), kmax 6-10 per axis, pressures log-spaced 1e3-1e7 Pa,
+    T in {273, 298, 323} K, each seeded on its own."""
+    rng = np.random.default_rng(seed)
+    out = []
+    pressures = np.logspace(3, 7, n)
+    temps = (273.0, 298.0, 323.0)
+    for i in range(n):
+        cell = float(rng.uniform(18.0, 36.0))
+        natoms = int(np.clip(round(1536 * (cell / 25.8) ** 3), 512, 4096))
+        kmax = int(rng.integers(6, 11))
+        out.append(co2_system(seed=seed * 1000 + i, n_atoms=natoms, cell=cell, kmax=kmax,
+                              temperature=temps[i % 3], pressure=float(pressures[i]),
+                              name=f"co2_b{i}"))
+    return out
+
+
+def tiny_co2_system(seed: int = 7, n_atoms: int = 96, cell: float = 24.5,
+                    kmax: int = 3) -> System:
+    """A small charged system for fast exact checks (a few hundred atoms)."""
+    return co2_system(seed=seed, n_atoms=n_atoms, cell=cell, kmax=kmax, dmin=1.5,
+                      name=f"co2tiny_s{seed}")
