@@ -1,0 +1,172 @@
+/* raspa_gpu.h — C ABI of the B200 GCMC energy path (libraspa_gpu.so).
+ *
+ * The reference (RASPA2) evaluates every Monte Carlo energy through a small
+ * set of C routines over process-global state; its host MC loop
+ * (src/mc_moves.c, src/cbmc.c) calls them once per trial position or move.
+ * This library exports the same operations over an explicit system handle,
+ * with plain pointers and sizes, so that a patched copy of those routines can
+ * forward to the GPU, plus batched entry points that
+ * evaluate a whole CBMC trial set per call and a persistent engine that runs
+ * many independent systems entirely on the device.
+ *
+ * Units: lengths in Angstrom, charges in e, energies in the reference's
+ * internal unit (amu A^2 / ps^2; src/constants.c:147). Positions are
+ * Cartesian, row-major [n][3] doubles. All calls are synchronous on the
+ * library's stream unless stated; none of them exits the process: every
+ * function returns 0 (RGPU_SUCCESS) or a negative error code
+ * (rgpu_error_string() describes it).
+ */
+#ifndef RASPA_GPU_H
+#define RASPA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RGPU_SUCCESS 0
+#define RGPU_E_INVALID -1      /* bad argument or size beyond a compiled limit */
+#define RGPU_E_CUDA -2         /* a CUDA runtime call failed (see rgpu_error_string) */
+#define RGPU_E_NODEVICE -3     /* no CUDA device */
+#define RGPU_E_CAPACITY -4     /* molecule capacity of the system exceeded */
+
+/* precision of a call */
+#define RGPU_FP64 0            /* FP64 throughout (the reference's REAL) */
+#define RGPU_MIXED 1           /* FP32 pair terms / FP64 sums and S(k) */
+
+typedef struct rgpu_system rgpu_system;
+typedef struct rgpu_engine rgpu_engine;
+
+/* Description of one simulation box (rigid framework + one rigid adsorbate
+ * component). Replaces what the reference reads into Framework[],
+ * Components[], PseudoAtoms and the Ewald globals (src/input.c ReadInputFile,
+ * src/ewald.c:200-261 InitializeEwald, :532-599 SetupKVectors). */
+typedef struct {
+  double box[3];              /* orthorhombic box lengths; each >= 2 * cutoff */
+  double cutoff;              /* VDW and real-space charge cut-off */
+  double beta;                /* 1 / (k_B T), inverse internal energy units */
+  double coulomb;             /* COULOMBIC_CONVERSION_FACTOR (src/constants.c:162) */
+  double overlap;             /* EnergyOverlapCriteria (src/input.c:367) */
+  int nfw;                    /* framework atoms */
+  const double *fw_xyz;       /* [nfw][3] */
+  const int *fw_type;         /* [nfw] pseudo-atom type (index into the LJ table) */
+  const double *fw_q;         /* [nfw] charge */
+  int ntypes;                 /* LJ table dimension */
+  const double *eps;          /* [ntypes*ntypes] epsilon (internal units), mixed */
+  const double *sig2;         /* [ntypes*ntypes] sigma^2 */
+  const double *shift;        /* [ntypes*ntypes] U(cutoff) (0 for truncated) */
+  int natom;                  /* atoms per adsorbate molecule (<= 8) */
+  const int *mol_type;        /* [natom] */
+  const double *mol_q;        /* [natom] */
+  const double *mol_ref;      /* [natom][3] rigid reference geometry */
+  int start_bead;             /* CBMC starting bead */
+  int ewald;                  /* 1: Ewald summation (charges), 0: no charges */
+  double alpha;               /* Ewald screening parameter */
+  int kmax[3];                /* wave vectors per axis */
+  int maxmol;                 /* molecule capacity */
+  /* MC move parameters (used by the engine) */
+  double move_cum[4];         /* cumulative probabilities: translate, rotate, insert, delete */
+  double max_translation;     /* Angstrom */
+  double max_rotation;        /* radian */
+  double fugacity_beta_v;     /* beta * fugacity * volume (ideal-gas Rosenbluth weight 1) */
+  int ntrial_first;           /* NumberOfTrialPositionsForTheFirstBead (<= 16) */
+  int ntrial;                 /* NumberOfTrialPositions (<= 16) */
+  uint64_t seed;              /* random stream seed */
+  uint32_t stream_id;         /* random stream id of this system */
+} rgpu_system_desc;
+
+const char *rgpu_error_string(int code);
+int rgpu_device_count(void);
+
+/* ---- system lifetime and adsorbate state -------------------------------- */
+int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *desc);
+int rgpu_system_destroy(rgpu_system *sys);
+/* Replaces the adsorbate configuration (nmol molecules, [nmol][natom][3]) and
+ * recomputes the stored structure factors; the state the reference builds
+ * with InsertAdsorbateMolecule (src/molecule.c:3075) and
+ * PrecomputeTotalEwaldContributions (src/ewald.c:1289). */
+int rgpu_set_adsorbates(rgpu_system *sys, int nmol, const double *xyz);
+int rgpu_get_adsorbates(rgpu_system *sys, int *nmol, double *xyz, int capacity);
+/* Moves molecule m to xyz ([natom][3]) after an accepted displacement
+ * (src/mc_moves.c:1743-1748); appends / removes a molecule (the last one
+ * takes the freed slot, src/molecule.c:3193 RemoveAdsorbateMolecule). These
+ * update positions only; S(k) follows through rgpu_ewald_accept. */
+int rgpu_update_molecule(rgpu_system *sys, int m, const double *xyz);
+int rgpu_insert_molecule(rgpu_system *sys, const double *xyz);
+int rgpu_remove_molecule(rgpu_system *sys, int m);
+
+/* ---- energies (the reference's per-call routines) ------------------------ */
+/* Energies of `n` bead positions in one call:
+ *   out[4*i+0] host VDW      CalculateFrameworkVDWEnergyAtPosition   src/framework_energy.c:60
+ *   out[4*i+1] host charge   CalculateFrameworkChargeEnergyAtPosition src/framework_energy.c:176
+ *   out[4*i+2] adsorbate VDW CalculateInterVDWEnergyAdsorbateAtPosition src/inter_energy.c:321
+ *   out[4*i+3] adsorbate q   CalculateInterChargeEnergyAdsorbateAtPosition src/inter_energy.c:393
+ * xyz[n][3]; atom[i] = index of the bead in the molecule (type and charge);
+ * exclude[i] = adsorbate molecule left out (-1 for none). Batched form of the
+ * trial loops of HandleFirstBead (src/cbmc.c:644-743) and
+ * ComputeExternalEnergies (src/cbmc.c:1179-1476). n <= 64 per call. */
+int rgpu_bead_energies(rgpu_system *sys, int precision, int n, const double *xyz, const int *atom,
+                       const int *exclude, double *out);
+
+/* Energy differences of molecule m moved to new_xyz ([natom][3]):
+ *   out = {dU host VDW, dU host charge, dU adsorbate VDW, dU adsorbate charge}
+ * CalculateFrameworkAdsorbateVDWEnergyDifference (src/framework_energy.c:4870),
+ * CalculateFrameworkAdsorbateChargeChargeEnergyDifference (:5412),
+ * CalculateInterVDWEnergyDifferenceAdsorbate (src/inter_energy.c:3071),
+ * CalculateInterChargeChargeEnergyDifferenceAdsorbate (:3652).
+ * *overlap = 1 when a new-position pair energy reaches the overlap criterion
+ * (the routines' `return OVERLAP=TRUE`). */
+int rgpu_move_energy_difference(rgpu_system *sys, int precision, int m, const double *new_xyz, double *out,
+                                int *overlap);
+
+/* Ewald Fourier difference, CalculateEwaldFourierAdsorbate(New, Old, mol,
+ * store) (src/ewald.c:6859): old_mol >= 0 removes that molecule's sites,
+ * new_xyz != NULL adds a molecule at new_xyz. out = {dU adsorbate-adsorbate
+ * Fourier, dU host-adsorbate Fourier, net charge change}. The candidate
+ * S(k) is kept on the device until rgpu_ewald_accept. */
+int rgpu_ewald_fourier_difference(rgpu_system *sys, int precision, int old_mol, const double *new_xyz,
+                                  double *out);
+/* AcceptEwaldAdsorbateMove (src/ewald.c:11732): the candidate becomes S(k). */
+int rgpu_ewald_accept(rgpu_system *sys);
+
+/* Total energies of the current configuration recomputed from scratch
+ * (CalculateEnergy, src/integration.c:250): out = {host VDW, adsorbate VDW,
+ * host real, adsorbate real, host Fourier, adsorbate Fourier}. FP64. */
+int rgpu_total_energy(rgpu_system *sys, double *out);
+
+/* ---- energy grids (src/grids.c) ----------------------------------------- */
+/* MakeGrid (src/grids.c:431-690) for pseudo-atom `type`: (n+1)^3 points
+ * i*size/n + shift per axis, 8 FP32 values per point (value, 3 first, 3 mixed
+ * second, 1 third derivative, scaled to the unit cell of the grid), layout
+ * grid[8][nx+1][ny+1][nz+1] (the plane order of the reference's grid file,
+ * src/grids.c:734-738). d_grid is device memory of that size. */
+int rgpu_grid_build(rgpu_system *sys, int type, const int npts[3], const double size[3],
+                    const double shift[3], float *d_grid);
+/* InterpolateVDWGrid (src/grids.c:979-1077) at n points (host arrays),
+ * reading the device grid; cell = the unit-cell lengths the grid spans. */
+int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3], const double shift[3],
+                          const double cell[3], int n, const double *xyz, double *out);
+
+/* ---- persistent batched engine ------------------------------------------ */
+/* Groups systems for one persistent launch; each system is advanced by one
+ * thread block. `threads` = block size (128..512, multiple of 32). */
+int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads);
+int rgpu_engine_destroy(rgpu_engine *eng);
+/* Advances every system by `nsteps` MC moves (asynchronous on `stream`, a
+ * cudaStream_t or NULL for the library stream). */
+int rgpu_engine_run(rgpu_engine *eng, long long nsteps, void *stream);
+int rgpu_engine_sync(rgpu_engine *eng);
+/* Running energies (8 doubles, first six as rgpu_total_energy), counters
+ * (12: attempts[4], accepted[4], moves, overlaps, 2 spare), molecule count,
+ * status word (0 = fine) and next step index of one system. */
+int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters12, int *nmol, int *status,
+                      unsigned long long *step);
+/* Resets the running energies to `energy8` (e.g. after rgpu_total_energy). */
+int rgpu_system_set_energy(rgpu_system *sys, const double *energy8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

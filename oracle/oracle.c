@@ -70,6 +70,30 @@ void or_point_energy(const or_sys *s, int type, double q, const double *p, int e
   out[0] = uv; out[1] = uc; out[2] = av; out[3] = ac;
 }
 
+/* Sums of |pair term| of or_point_energy: the scale against which the
+ * rounding error of a sum of cancelling pair terms is measured. */
+void or_point_energy_abs(const or_sys *s, int type, double q, const double *p, int exclude,
+                         double *out)
+{
+  double d[3];
+  double uv = 0.0, uc = 0.0, av = 0.0, ac = 0.0;
+  for (int i = 0; i < s->nfw; i++) {
+    double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
+    if (r2 < s->rc2_vdw) uv += fabs(or_lj(s, type, s->fw_type[i], r2));
+    if (s->ewald && q != 0.0 && r2 < s->rc2_cc) uc += fabs(or_real_ewald(s, q, s->fw_q[i], sqrt(r2)));
+  }
+  for (int m = 0; m < s->nmol; m++) {
+    if (m == exclude) continue;
+    for (int a = 0; a < s->natom; a++) {
+      const double *pb = s->ads_xyz + 3 * (m * s->natom + a);
+      double r2 = dist2(s, p, pb, d);
+      if (r2 < s->rc2_vdw) av += fabs(or_lj(s, type, s->mol_type[a], r2));
+      if (s->ewald && q != 0.0 && r2 < s->rc2_cc) ac += fabs(or_real_ewald(s, q, s->mol_q[a], sqrt(r2)));
+    }
+  }
+  out[0] = uv; out[1] = uc; out[2] = av; out[3] = ac;
+}
+
 /* The four difference routines in the order of src/mc_moves.c:1601-1624:
  * CalculateInterVDWEnergyDifferenceAdsorbate (src/inter_energy.c:3071),
  * CalculateInterChargeChargeEnergyDifferenceAdsorbate (:3652),
@@ -222,6 +246,38 @@ void or_ewald_setup(or_sys *s)
   double net = 0.0;
   for (int i = 0; i < s->nfw; i++) net += s->fw_q[i];
   s->net_fw = net;
+}
+
+/* scale of the Fourier difference: sum over k of the absolute values of the
+ * per-k terms of or_ewald_delta (out = {ads scale, host scale}) */
+void or_ewald_delta_abs(const or_sys *s, int nold, const double *xold, int nnew,
+                        const double *xnew, double *out)
+{
+  double sa = 0.0, sh = 0.0;
+  for (int kk = 0; kk < s->nk; kk++) {
+    const int *k = s->kidx + 3 * kk;
+    double dr = 0.0, di = 0.0, dm = 0.0;
+    for (int o = 0; o < nold + nnew; o++) {
+      const double *x = o < nold ? xold + 3 * o * s->natom : xnew + 3 * (o - nold) * s->natom;
+      for (int a = 0; a < s->natom; a++) {
+        if (s->mol_q[a] == 0.0) continue;
+        double re, im;
+        site_phase(s, x + 3 * a, k, &re, &im);
+        double q = o < nold ? -s->mol_q[a] : s->mol_q[a];
+        dr += q * re;
+        di += q * im;
+        dm += fabs(s->mol_q[a]);
+      }
+    }
+    double f = s->kfactor[kk];
+    double so = sqrt(SQR(s->sk_ads[2 * kk]) + SQR(s->sk_ads[2 * kk + 1]));
+    double sf = sqrt(SQR(s->sk_fw[2 * kk]) + SQR(s->sk_fw[2 * kk + 1]));
+    sa += f * (2.0 * so * dm + dm * dm);
+    sh += 2.0 * f * sf * dm;
+    (void)dr; (void)di;
+  }
+  out[0] = sa;
+  out[1] = sh;
 }
 
 void or_recompute_sk_ads(or_sys *s)

@@ -59,6 +59,10 @@ double or_real_ewald(const or_sys *s, double qa, double qb, double r);
 void or_point_energy(const or_sys *s, int type, double q, const double *p, int exclude,
                      double *out);
 
+/* sums of |pair term| of or_point_energy (the scale of its rounding error) */
+void or_point_energy_abs(const or_sys *s, int type, double q, const double *p, int exclude,
+                         double *out);
+
 /* translation/rotation energy differences for molecule m moved to new_xyz
  * (src/mc_moves.c:1601-1629 and the four *Difference routines). Returns 1 on
  * overlap; out = {dU host VDW, dU ads VDW, dU host cc, dU ads cc}. */
@@ -73,6 +77,9 @@ void or_structure_factor(const or_sys *s, int n, const double *q, const double *
 void or_ewald_delta(const or_sys *s, int nold, const double *xold, int nnew,
                     const double *xnew, double *out, double *sk_new);
 void or_recompute_sk_ads(or_sys *s);
+/* scale of or_ewald_delta's terms: out = {ads-ads, host-ads} */
+void or_ewald_delta_abs(const or_sys *s, int nold, const double *xold, int nnew,
+                        const double *xnew, double *out);
 /* totals {host VDW, ads VDW, host cc real, ads cc real, host Fourier, ads Fourier}
  * (src/integration.c:250 CalculateEnergy for this system class) */
 void or_total_energy(const or_sys *s, double *out);

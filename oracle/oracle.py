@@ -165,6 +165,22 @@ class Oracle:
                               C.c_int(exclude), _ptr(out))
         return out
 
+    def point_abs(self, type_, q, p, exclude=-1):
+        out = np.zeros(4)
+        p = np.ascontiguousarray(p, float)
+        lib().or_point_energy_abs(C.byref(self.s), C.c_int(type_), C.c_double(q), _ptr(p),
+                                  C.c_int(exclude), _ptr(out))
+        return out
+
+    def ewald_delta_abs(self, old=None, new=None):
+        out = np.zeros(2)
+        o = np.ascontiguousarray(old if old is not None else np.zeros((0, 3)), float).reshape(-1)
+        n = np.ascontiguousarray(new if new is not None else np.zeros((0, 3)), float).reshape(-1)
+        na = self.s.natom
+        lib().or_ewald_delta_abs(C.byref(self.s), C.c_int(len(o) // (3 * na)), _ptr(o),
+                                 C.c_int(len(n) // (3 * na)), _ptr(n), _ptr(out))
+        return out
+
     def move_delta(self, m, new_xyz):
         out = np.zeros(4)
         nx = np.ascontiguousarray(new_xyz, float)

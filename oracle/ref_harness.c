@@ -62,6 +62,7 @@
 #include "thermo_baro_stats.h"
 #include "equations_of_state.h"
 #include "statistics.h"
+#include "output.h"
 
 extern bool STREAM;
 extern char *INPUT_CRYSTAL;
@@ -368,7 +369,12 @@ int main(int argc, char **argv)
       double r = InterpolateVDWGrid((int)v[0], p);
       p1("interp", 1, &r);
     } else if (!strcmp(cmd, "makegrid")) {
+      /* the MAKE_GRID branch of run() (src/run.c:144-152) */
       fflush(out);
+      OpenOutputFile();
+      PrintPreSimulationStatus();
+      Framework[0].FrameworkModel = FULL;
+      CurrentSystem = 0;
       MakeGrid();
     } else {
       fprintf(stderr, "unknown command %s\n", cmd);

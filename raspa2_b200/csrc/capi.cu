@@ -1,0 +1,846 @@
+/* C ABI of libraspa_gpu (include/raspa_gpu.h).
+ *
+ * Host side of the drop-in boundary: builds the device image of a system
+ * (framework sorted by pseudo-atom type, force-field tables resolved for the
+ * adsorbate, k-vectors and Ewald prefactors), keeps the adsorbate state on the
+ * device, and forwards each reference-named operation to the kernels. No
+ * function exits the process; errors are returned as codes.
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/raspa_gpu.h"
+#include "rgpu_engine.h"
+#include "rgpu_types.h"
+
+static thread_local char g_err[512];
+
+static int fail(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(RGPU_E_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" const char *rgpu_error_string(int code)
+{
+  if (code == RGPU_SUCCESS) return "success";
+  return g_err[0] ? g_err : "unknown error";
+}
+
+extern "C" int rgpu_device_count(void)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+struct rgpu_system {
+  rgpu_system_desc d;         /* pointer members are not kept */
+  RgpuSys h;                  /* host image of the descriptor */
+  RgpuSys *d_sys;
+  cudaStream_t st;
+  int kw;
+  /* device buffers */
+  double4 *fw64;
+  int4 *fw32;
+  char4 *kvec;
+  double *kfactor;
+  double2 *sk_fw, *sk_ads, *ds;
+  double *ads_xyz;
+  int *nmol;
+  double *energy;
+  unsigned long long *step;
+  long long *counters;
+  int *status;
+  int4 *rec32;
+  void *rec64;
+  /* per-call scratch */
+  double *io_xyz, *io_out, *io_q;
+  int *io_atom, *io_excl, *io_ov;
+  /* host mirrors */
+  std::vector<double> h_xyz;  /* [nmol*natom*3] */
+  int h_nmol;
+  int records_stale;          /* device records must be rebuilt from ads_xyz */
+  double net_ads, pending_dq;
+  int grid_type_seg;
+  std::vector<int> fw_seg_type; /* framework pseudo-atom type of each segment */
+  std::vector<double> lj_eps, lj_sig2, lj_shift;
+  int ntypes;
+};
+
+struct rgpu_engine {
+  std::vector<rgpu_system *> sys;
+  RgpuSys *d_systems;
+  int mixed, threads, kw, max_ads, nfw_smem;
+  cudaStream_t st;
+};
+
+static void sys_free(rgpu_system *s)
+{
+  if (!s) return;
+  void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
+                  s->nmol, s->energy, s->step, s->counters, s->status, s->rec32, s->rec64, s->io_xyz,
+                  s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+extern "C" int rgpu_system_destroy(rgpu_system *sys)
+{
+  sys_free(sys);
+  return RGPU_SUCCESS;
+}
+
+/* k-vector list of src/ewald.c:224-259 and the prefactor of :584-591 */
+static void kvectors(const rgpu_system_desc *d, std::vector<char4> &kv, std::vector<double> &kf)
+{
+  const int kx = d->kmax[0], ky = d->kmax[1], kz = d->kmax[2];
+  const int km = std::max(kx, std::max(ky, kz));
+  const double rc = (1.05 * km) * (1.05 * km);
+  const double vol = d->box[0] * d->box[1] * d->box[2];
+  for (int i = 0; i <= kx; i++)
+    for (int j = -ky; j <= ky; j++)
+      for (int k = -kz; k <= kz; k++) {
+        int s = i * i + j * j + k * k;
+        if (s == 0 || !(s < rc)) continue;
+        kv.push_back(make_char4((signed char)i, (signed char)j, (signed char)k, 0));
+        double rx = 2.0 * M_PI * i / d->box[0], ry = 2.0 * M_PI * j / d->box[1], rz = 2.0 * M_PI * k / d->box[2];
+        double k2 = rx * rx + ry * ry + rz * rz;
+        double pre = (i == 0 ? 2.0 : 4.0) * M_PI / vol;
+        kf.push_back(d->coulomb * pre * exp((-0.25 / (d->alpha * d->alpha)) * k2) / k2);
+      }
+}
+
+static int upload_records(rgpu_system *s)
+{
+  const int nads = s->h_nmol * s->d.natom;
+  CK(rgpu_records_launch(s->d_sys, nads, s->rec32, s->rec64, s->st));
+  s->records_stale = 0;
+  return RGPU_SUCCESS;
+}
+
+/* pulls positions and molecule count back after the engine moved them */
+static int refresh_from_device(rgpu_system *s)
+{
+  if (!s->records_stale) return RGPU_SUCCESS;
+  int n = 0;
+  CK(cudaMemcpyAsync(&n, s->nmol, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  s->h_nmol = n;
+  s->h_xyz.assign((size_t)n * s->d.natom * 3, 0.0);
+  if (n)
+    CK(cudaMemcpyAsync(s->h_xyz.data(), s->ads_xyz, sizeof(double) * s->h_xyz.size(), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  s->net_ads = n * s->h.mol_charge;
+  return upload_records(s);
+}
+
+extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
+{
+  if (!out || !d) return fail(RGPU_E_INVALID, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RGPU_E_NODEVICE, "no CUDA device");
+  if (d->natom < 1 || d->natom > RGPU_MAX_ATOMS) return fail(RGPU_E_INVALID, "natom %d outside [1,%d]", d->natom, RGPU_MAX_ATOMS);
+  if (d->nfw < 1 || !d->fw_xyz || !d->fw_type || !d->fw_q) return fail(RGPU_E_INVALID, "framework missing");
+  if (d->ntypes < 1 || !d->eps || !d->sig2 || !d->shift) return fail(RGPU_E_INVALID, "LJ table missing");
+  if (!d->mol_type || !d->mol_q || !d->mol_ref) return fail(RGPU_E_INVALID, "molecule missing");
+  if (d->start_bead < 0 || d->start_bead >= d->natom) return fail(RGPU_E_INVALID, "start_bead");
+  if (d->maxmol < 1 || (long long)d->maxmol * d->natom > (1 << 20)) return fail(RGPU_E_INVALID, "maxmol");
+  if (d->ntrial_first < 1 || d->ntrial_first > RGPU_MAX_TRIALS || d->ntrial < 1 || d->ntrial > RGPU_MAX_TRIALS)
+    return fail(RGPU_E_INVALID, "trial counts must be in [1,%d]", RGPU_MAX_TRIALS);
+  if (d->ntrial * (d->natom - 1) > RGPU_MAX_POS) return fail(RGPU_E_INVALID, "ntrial*(natom-1) > %d", RGPU_MAX_POS);
+  for (int c = 0; c < 3; c++)
+    if (!(d->box[c] >= 2.0 * d->cutoff)) return fail(RGPU_E_INVALID, "box length %g < 2*cutoff", d->box[c]);
+  if (d->ewald && (d->kmax[0] < 1 || d->kmax[1] < 1 || d->kmax[2] < 1 ||
+                   std::max(d->kmax[0], std::max(d->kmax[1], d->kmax[2])) > 20))
+    return fail(RGPU_E_INVALID, "kmax must be in [1,20]");
+  for (int i = 0; i < d->nfw; i++)
+    if (d->fw_type[i] < 0 || d->fw_type[i] >= d->ntypes) return fail(RGPU_E_INVALID, "framework type %d", d->fw_type[i]);
+  for (int a = 0; a < d->natom; a++)
+    if (d->mol_type[a] < 0 || d->mol_type[a] >= d->ntypes) return fail(RGPU_E_INVALID, "molecule type");
+
+  rgpu_system *s = new rgpu_system();
+  memset(&s->h, 0, sizeof(RgpuSys));
+  s->d = *d;
+  s->h_nmol = 0;
+  s->records_stale = 0;
+  s->net_ads = 0.0;
+  s->pending_dq = 0.0;
+  s->ntypes = d->ntypes;
+  s->lj_eps.assign(d->eps, d->eps + d->ntypes * d->ntypes);
+  s->lj_sig2.assign(d->sig2, d->sig2 + d->ntypes * d->ntypes);
+  s->lj_shift.assign(d->shift, d->shift + d->ntypes * d->ntypes);
+  RgpuSys &h = s->h;
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+    sys_free(s);
+    return fail(RGPU_E_CUDA, "stream");
+  }
+  /* framework sorted by type into segments */
+  std::vector<int> order(d->nfw);
+  for (int i = 0; i < d->nfw; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d->fw_type[a] < d->fw_type[b]; });
+  std::vector<double4> fw64(d->nfw);
+  std::vector<int4> fw32(d->nfw);
+  int nseg = 0;
+  double netq = 0.0;
+  int charged = 0;
+  for (int idx = 0; idx < d->nfw; idx++) {
+    const int i = order[idx];
+    if (idx == 0 || d->fw_type[i] != d->fw_type[order[idx - 1]]) {
+      if (nseg == RGPU_MAX_FWTYPES) {
+        sys_free(s);
+        return fail(RGPU_E_INVALID, "more than %d framework types", RGPU_MAX_FWTYPES);
+      }
+      h.seg_start[nseg] = idx;
+      s->fw_seg_type.push_back(d->fw_type[i]);
+      nseg++;
+    }
+    const double x = d->fw_xyz[3 * i], y = d->fw_xyz[3 * i + 1], z = d->fw_xyz[3 * i + 2], q = d->fw_q[i];
+    fw64[idx] = make_double4(x, y, z, q);
+    float qf = (float)q;
+    int qb;
+    memcpy(&qb, &qf, 4);
+    fw32[idx] = make_int4(0, 0, 0, qb);
+    netq += q;
+    if (q != 0.0) charged = 1;
+  }
+  h.seg_start[nseg] = d->nfw;
+  h.nseg = nseg;
+  h.nfw = d->nfw;
+  h.fw_charged = charged && d->ewald;
+  for (int c = 0; c < 3; c++) {
+    h.box[c] = d->box[c];
+    h.inv_box[c] = 1.0 / d->box[c];
+    h.fix_scale[c] = (float)(d->box[c] / 4294967296.0);
+    h.kmax[c] = d->ewald ? d->kmax[c] : 0;
+  }
+  for (int idx = 0; idx < d->nfw; idx++) {
+    fw32[idx].x = 0;
+  }
+  for (int idx = 0; idx < d->nfw; idx++) {
+    /* fixed-point coordinates (see rgpu_types.h) */
+    double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
+    int v[3];
+    for (int c = 0; c < 3; c++) {
+      double f = p[c] * h.inv_box[c];
+      f -= floor(f);
+      long long q = llrint(f * 4294967296.0);
+      v[c] = (int)(unsigned)(q & 0xffffffffLL);
+    }
+    fw32[idx].x = v[0]; fw32[idx].y = v[1]; fw32[idx].z = v[2];
+  }
+  h.rc2 = d->cutoff * d->cutoff;
+  h.rc2f = (float)h.rc2;
+  h.overlap = d->overlap;
+  h.beta = d->beta;
+  h.coulomb = d->coulomb;
+  h.alpha = d->ewald ? d->alpha : 0.0;
+  h.coulombf = (float)d->coulomb;
+  h.alphaf = (float)h.alpha;
+  h.natom = d->natom;
+  h.start_bead = d->start_bead;
+  h.maxmol = d->maxmol;
+  int molq = 0;
+  double mq = 0.0, self = 0.0;
+  for (int a = 0; a < d->natom; a++) {
+    h.mol_q[a] = d->ewald ? d->mol_q[a] : 0.0;
+    h.mol_qf[a] = (float)h.mol_q[a];
+    if (h.mol_q[a] != 0.0) molq = 1;
+    mq += h.mol_q[a];
+    self += d->coulomb * h.mol_q[a] * h.mol_q[a] * h.alpha / sqrt(M_PI);
+    for (int c = 0; c < 3; c++) h.mol_ref[a][c] = d->mol_ref[3 * a + c];
+    const int ta = d->mol_type[a];
+    for (int sg = 0; sg < nseg; sg++) {
+      const int tb = s->fw_seg_type[sg], ij = ta * d->ntypes + tb;
+      h.lj_bf[a][sg].eps4 = 4.0 * d->eps[ij];
+      h.lj_bf[a][sg].sig2 = d->sig2[ij];
+      h.lj_bf[a][sg].shift = d->shift[ij];
+      h.ljf_bf[a][sg].eps4 = (float)(4.0 * d->eps[ij]);
+      h.ljf_bf[a][sg].sig2 = (float)d->sig2[ij];
+      h.ljf_bf[a][sg].shift = (float)d->shift[ij];
+    }
+    for (int b = 0; b < d->natom; b++) {
+      const int ij = ta * d->ntypes + d->mol_type[b];
+      h.lj_bb[a][b].eps4 = 4.0 * d->eps[ij];
+      h.lj_bb[a][b].sig2 = d->sig2[ij];
+      h.lj_bb[a][b].shift = d->shift[ij];
+      h.ljf_bb[a][b].eps4 = (float)(4.0 * d->eps[ij]);
+      h.ljf_bb[a][b].sig2 = (float)d->sig2[ij];
+      h.ljf_bb[a][b].shift = (float)d->shift[ij];
+    }
+  }
+  h.mol_charged = molq;
+  h.mol_charge = mq;
+  h.self_mol = self;
+  h.ewald = d->ewald;
+  for (int c = 0; c < 4; c++) h.cum[c] = d->move_cum[c];
+  h.max_translation = d->max_translation;
+  h.max_rotation = d->max_rotation;
+  h.fugacity_beta_v = d->fugacity_beta_v;
+  h.ntrial_first = d->ntrial_first;
+  h.ntrial = d->ntrial;
+  h.seed = d->seed;
+  h.sys_id = d->stream_id;
+  h.net_fw = netq;
+
+  std::vector<char4> kv;
+  std::vector<double> kf;
+  if (d->ewald) kvectors(d, kv, kf);
+  h.nk = (int)kv.size();
+  s->kw = 2 * std::max(h.kmax[0], std::max(h.kmax[1], h.kmax[2])) + 1;
+  double uion = 0.0;
+  for (double f : kf) uion += f;
+  /* EwaldEnergyIon, src/ewald.c:615-724 */
+  h.uion = d->ewald ? -(uion - d->coulomb * h.alpha / sqrt(M_PI)) : 0.0;
+
+  const size_t nads = (size_t)d->maxmol * d->natom;
+  const int nk1 = std::max(h.nk, 1);
+#define ALLOC(p, n) \
+  if (cudaMalloc((void **)&(p), (n)) != cudaSuccess) { sys_free(s); return fail(RGPU_E_CUDA, "cudaMalloc " #p); }
+  ALLOC(s->d_sys, sizeof(RgpuSys));
+  ALLOC(s->fw64, sizeof(double4) * d->nfw);
+  ALLOC(s->fw32, sizeof(int4) * d->nfw);
+  ALLOC(s->kvec, sizeof(char4) * nk1);
+  ALLOC(s->kfactor, sizeof(double) * nk1);
+  ALLOC(s->sk_fw, sizeof(double2) * nk1);
+  ALLOC(s->sk_ads, sizeof(double2) * nk1);
+  ALLOC(s->ds, sizeof(double2) * nk1);
+  ALLOC(s->ads_xyz, sizeof(double) * 3 * nads);
+  ALLOC(s->nmol, sizeof(int));
+  ALLOC(s->energy, sizeof(double) * RGPU_NE);
+  ALLOC(s->step, sizeof(unsigned long long));
+  ALLOC(s->counters, sizeof(long long) * RGPU_NCNT);
+  ALLOC(s->status, sizeof(int));
+  ALLOC(s->rec32, sizeof(int4) * nads);
+  ALLOC(s->rec64, 32 * nads);
+  const size_t io_n = std::max((size_t)RGPU_MAX_POS, std::max((size_t)d->nfw, nads));
+  ALLOC(s->io_xyz, sizeof(double) * 3 * io_n);
+  ALLOC(s->io_q, sizeof(double) * io_n);
+  ALLOC(s->io_out, sizeof(double) * 4 * RGPU_MAX_POS);
+  ALLOC(s->io_atom, sizeof(int) * RGPU_MAX_POS);
+  ALLOC(s->io_excl, sizeof(int) * RGPU_MAX_POS);
+  ALLOC(s->io_ov, sizeof(int) * RGPU_MAX_POS);
+#undef ALLOC
+  h.fw64 = s->fw64;
+  h.fw32 = s->fw32;
+  h.kvec = s->kvec;
+  h.kfactor = s->kfactor;
+  h.sk_fw = s->sk_fw;
+  h.sk_ads = s->sk_ads;
+  h.ads_xyz = s->ads_xyz;
+  h.nmol = s->nmol;
+  h.energy = s->energy;
+  h.step = s->step;
+  h.counters = s->counters;
+  h.status = s->status;
+  cudaStream_t st = s->st;
+  int rc = RGPU_SUCCESS;
+  do {
+    if (cudaMemcpyAsync(s->fw64, fw64.data(), sizeof(double4) * d->nfw, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(s->fw32, fw32.data(), sizeof(int4) * d->nfw, cudaMemcpyHostToDevice, st) ||
+        cudaMemsetAsync(s->nmol, 0, sizeof(int), st) || cudaMemsetAsync(s->energy, 0, sizeof(double) * RGPU_NE, st) ||
+        cudaMemsetAsync(s->step, 0, sizeof(unsigned long long), st) ||
+        cudaMemsetAsync(s->counters, 0, sizeof(long long) * RGPU_NCNT, st) ||
+        cudaMemsetAsync(s->status, 0, sizeof(int), st) || cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * nk1, st) ||
+        cudaMemsetAsync(s->sk_fw, 0, sizeof(double2) * nk1, st) ||
+        cudaMemcpyAsync(s->d_sys, &h, sizeof(RgpuSys), cudaMemcpyHostToDevice, st)) {
+      rc = fail(RGPU_E_CUDA, "upload");
+      break;
+    }
+    if (h.nk) {
+      if (cudaMemcpyAsync(s->kvec, kv.data(), sizeof(char4) * h.nk, cudaMemcpyHostToDevice, st) ||
+          cudaMemcpyAsync(s->kfactor, kf.data(), sizeof(double) * h.nk, cudaMemcpyHostToDevice, st)) {
+        rc = fail(RGPU_E_CUDA, "upload k");
+        break;
+      }
+      /* S_fw(k) (PrecomputeFixedEwaldContributions, src/ewald.c:744) from the
+       * framework in its original order */
+      std::vector<double> q(d->fw_q, d->fw_q + d->nfw);
+      if (cudaMemcpyAsync(s->io_xyz, d->fw_xyz, sizeof(double) * 3 * d->nfw, cudaMemcpyHostToDevice, st) ||
+          cudaMemcpyAsync(s->io_q, q.data(), sizeof(double) * d->nfw, cudaMemcpyHostToDevice, st) ||
+          rgpu_structure_factor_launch(s->d_sys, s->io_xyz, s->io_q, d->nfw, h.nk, s->sk_fw, st)) {
+        rc = fail(RGPU_E_CUDA, "S_fw");
+        break;
+      }
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(RGPU_E_CUDA, "%s", cudaGetErrorString(cudaGetLastError()));
+  } while (0);
+  if (rc) {
+    sys_free(s);
+    return rc;
+  }
+  *out = s;
+  return RGPU_SUCCESS;
+}
+
+static int recompute_sk_ads(rgpu_system *s)
+{
+  const int nads = s->h_nmol * s->d.natom;
+  if (!s->h.nk) return RGPU_SUCCESS;
+  if (nads == 0) {
+    CK(cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * s->h.nk, s->st));
+    return RGPU_SUCCESS;
+  }
+  std::vector<double> q(nads);
+  for (int i = 0; i < nads; i++) q[i] = s->h.mol_q[i % s->d.natom];
+  CK(cudaMemcpyAsync(s->io_xyz, s->h_xyz.data(), sizeof(double) * 3 * nads, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->io_q, q.data(), sizeof(double) * nads, cudaMemcpyHostToDevice, s->st));
+  CK(rgpu_structure_factor_launch(s->d_sys, s->io_xyz, s->io_q, nads, s->h.nk, s->sk_ads, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_set_adsorbates(rgpu_system *s, int nmol, const double *xyz)
+{
+  if (!s || nmol < 0 || (nmol > 0 && !xyz)) return fail(RGPU_E_INVALID, "bad argument");
+  if (nmol > s->d.maxmol) return fail(RGPU_E_CAPACITY, "nmol %d > maxmol %d", nmol, s->d.maxmol);
+  const size_t n = (size_t)nmol * s->d.natom * 3;
+  s->h_xyz.assign(xyz, xyz + n);
+  s->h_nmol = nmol;
+  if (n) CK(cudaMemcpyAsync(s->ads_xyz, s->h_xyz.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->nmol, &s->h_nmol, sizeof(int), cudaMemcpyHostToDevice, s->st));
+  s->net_ads = nmol * s->h.mol_charge;
+  s->pending_dq = 0.0;
+  int rc = upload_records(s);
+  if (rc) return rc;
+  rc = recompute_sk_ads(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_get_adsorbates(rgpu_system *s, int *nmol, double *xyz, int capacity)
+{
+  if (!s || !nmol) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  *nmol = s->h_nmol;
+  if (xyz) {
+    if (capacity < s->h_nmol) return fail(RGPU_E_CAPACITY, "capacity %d < nmol %d", capacity, s->h_nmol);
+    memcpy(xyz, s->h_xyz.data(), sizeof(double) * s->h_xyz.size());
+  }
+  return RGPU_SUCCESS;
+}
+
+static int write_molecule(rgpu_system *s, int m, const double *xyz)
+{
+  const int na = s->d.natom;
+  memcpy(&s->h_xyz[(size_t)m * na * 3], xyz, sizeof(double) * 3 * na);
+  CK(cudaMemcpyAsync(s->ads_xyz + (size_t)m * na * 3, &s->h_xyz[(size_t)m * na * 3], sizeof(double) * 3 * na,
+                     cudaMemcpyHostToDevice, s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_update_molecule(rgpu_system *s, int m, const double *xyz)
+{
+  if (!s || !xyz) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  if (m < 0 || m >= s->h_nmol) return fail(RGPU_E_INVALID, "molecule %d", m);
+  rc = write_molecule(s, m, xyz);
+  if (rc) return rc;
+  return upload_records(s);
+}
+
+extern "C" int rgpu_insert_molecule(rgpu_system *s, const double *xyz)
+{
+  if (!s || !xyz) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  if (s->h_nmol >= s->d.maxmol) return fail(RGPU_E_CAPACITY, "maxmol %d reached", s->d.maxmol);
+  s->h_xyz.resize((size_t)(s->h_nmol + 1) * s->d.natom * 3);
+  rc = write_molecule(s, s->h_nmol, xyz);
+  if (rc) return rc;
+  s->h_nmol++;
+  CK(cudaMemcpyAsync(s->nmol, &s->h_nmol, sizeof(int), cudaMemcpyHostToDevice, s->st));
+  rc = upload_records(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_remove_molecule(rgpu_system *s, int m)
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  if (m < 0 || m >= s->h_nmol) return fail(RGPU_E_INVALID, "molecule %d", m);
+  const int na = s->d.natom, last = s->h_nmol - 1;
+  if (m != last) {
+    std::vector<double> tmp(&s->h_xyz[(size_t)last * na * 3], &s->h_xyz[(size_t)last * na * 3] + 3 * na);
+    rc = write_molecule(s, m, tmp.data());
+    if (rc) return rc;
+  }
+  s->h_nmol--;
+  s->h_xyz.resize((size_t)s->h_nmol * na * 3);
+  CK(cudaMemcpyAsync(s->nmol, &s->h_nmol, sizeof(int), cudaMemcpyHostToDevice, s->st));
+  rc = upload_records(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+/* ---------------------------------------------------------------------- */
+static int bead_batch(rgpu_system *s, int precision, int n, const double *xyz, const int *atom, const int *excl,
+                      int pair_check, double *out, int *ov)
+{
+  CK(cudaMemcpyAsync(s->io_xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->io_atom, atom, sizeof(int) * n, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->io_excl, excl, sizeof(int) * n, cudaMemcpyHostToDevice, s->st));
+  const int mixed = precision == RGPU_MIXED;
+  const void *ads = mixed ? (const void *)s->rec32 : (const void *)s->rec64;
+  CK(rgpu_point_energies_launch(mixed, s->d_sys, ads, s->h_nmol * s->d.natom, s->io_xyz, s->io_atom, s->io_excl, n,
+                                pair_check, s->io_out, s->io_ov, s->st));
+  CK(cudaMemcpyAsync(out, s->io_out, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s->st));
+  if (ov) CK(cudaMemcpyAsync(ov, s->io_ov, sizeof(int) * n, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_bead_energies(rgpu_system *s, int precision, int n, const double *xyz, const int *atom,
+                                  const int *exclude, double *out)
+{
+  if (!s || n < 0 || (n && (!xyz || !atom || !exclude || !out))) return fail(RGPU_E_INVALID, "bad argument");
+  if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++)
+    if (atom[i] < 0 || atom[i] >= s->d.natom) return fail(RGPU_E_INVALID, "atom index %d", atom[i]);
+  for (int base = 0; base < n; base += RGPU_MAX_POS) {
+    int b = std::min(RGPU_MAX_POS, n - base);
+    rc = bead_batch(s, precision, b, xyz + 3 * base, atom + base, exclude + base, 0, out + 4 * base, nullptr);
+    if (rc) return rc;
+  }
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_move_energy_difference(rgpu_system *s, int precision, int m, const double *new_xyz, double *out,
+                                           int *overlap)
+{
+  if (!s || !new_xyz || !out) return fail(RGPU_E_INVALID, "bad argument");
+  if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  if (m < 0 || m >= s->h_nmol) return fail(RGPU_E_INVALID, "molecule %d", m);
+  const int na = s->d.natom;
+  double xyz[2 * RGPU_MAX_ATOMS * 3], res[2 * RGPU_MAX_ATOMS * 4];
+  int atom[2 * RGPU_MAX_ATOMS], excl[2 * RGPU_MAX_ATOMS], ov[2 * RGPU_MAX_ATOMS];
+  for (int a = 0; a < na; a++) {
+    for (int c = 0; c < 3; c++) {
+      xyz[3 * a + c] = new_xyz[3 * a + c];
+      xyz[3 * (na + a) + c] = s->h_xyz[((size_t)m * na + a) * 3 + c];
+    }
+    atom[a] = atom[na + a] = a;
+    excl[a] = excl[na + a] = m;
+  }
+  rc = bead_batch(s, precision, 2 * na, xyz, atom, excl, na, res, ov);
+  if (rc) return rc;
+  int o = 0;
+  for (int k = 0; k < 4; k++) out[k] = 0.0;
+  for (int a = 0; a < na; a++) {
+    o |= ov[a];
+    for (int k = 0; k < 4; k++) out[k] += res[4 * a + k] - res[4 * (na + a) + k];
+  }
+  if (overlap) *overlap = o;
+  return RGPU_SUCCESS;
+}
+
+static double exclusion_energy(const rgpu_system *s, const double *xyz)
+{
+  const RgpuSys &h = s->h;
+  double e = 0.0;
+  for (int a = 0; a < h.natom - 1; a++)
+    for (int b = a + 1; b < h.natom; b++) {
+      if (h.mol_q[a] == 0.0 || h.mol_q[b] == 0.0) continue;
+      double dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1], dz = xyz[3 * a + 2] - xyz[3 * b + 2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      e += h.coulomb * h.mol_q[a] * h.mol_q[b] * erf(h.alpha * r) / r;
+    }
+  return e;
+}
+
+extern "C" int rgpu_ewald_fourier_difference(rgpu_system *s, int precision, int old_mol, const double *new_xyz,
+                                             double *out)
+{
+  if (!s || !out) return fail(RGPU_E_INVALID, "bad argument");
+  if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  out[0] = out[1] = out[2] = 0.0;
+  s->pending_dq = 0.0;
+  if (!s->h.ewald || !s->h.nk) return RGPU_SUCCESS;
+  if (old_mol >= s->h_nmol) return fail(RGPU_E_INVALID, "molecule %d", old_mol);
+  const int na = s->d.natom;
+  double xyz[2 * RGPU_MAX_ATOMS * 3], q[2 * RGPU_MAX_ATOMS];
+  int ns = 0;
+  double ex_old = 0.0, ex_new = 0.0;
+  int dn = 0;
+  if (old_mol >= 0) {
+    const double *o = &s->h_xyz[(size_t)old_mol * na * 3];
+    for (int a = 0; a < na; a++) {
+      if (s->h.mol_q[a] == 0.0) continue;
+      for (int c = 0; c < 3; c++) xyz[3 * ns + c] = o[3 * a + c];
+      q[ns++] = -s->h.mol_q[a];
+    }
+    ex_old = exclusion_energy(s, o);
+    dn--;
+  }
+  if (new_xyz) {
+    for (int a = 0; a < na; a++) {
+      if (s->h.mol_q[a] == 0.0) continue;
+      for (int c = 0; c < 3; c++) xyz[3 * ns + c] = new_xyz[3 * a + c];
+      q[ns++] = s->h.mol_q[a];
+    }
+    ex_new = exclusion_energy(s, new_xyz);
+    dn++;
+  }
+  double e[2] = {0.0, 0.0};
+  if (ns) {
+    CK(cudaMemcpyAsync(s->io_xyz, xyz, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->io_q, q, sizeof(double) * ns, cudaMemcpyHostToDevice, s->st));
+    CK(rgpu_ewald_delta_launch(precision == RGPU_MIXED, s->d_sys, s->io_xyz, s->io_q, ns, s->ds, s->io_out, s->kw,
+                               s->st));
+    CK(cudaMemcpyAsync(e, s->io_out, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+  } else {
+    CK(cudaMemsetAsync(s->ds, 0, sizeof(double2) * s->h.nk, s->st));
+  }
+  const RgpuSys &h = s->h;
+  const double dq = dn * h.mol_charge;
+  double d_ads = e[0] - (ex_new - ex_old) - dn * h.self_mol;
+  d_ads += h.uion * (s->net_ads + dq) * (s->net_ads + dq) - h.uion * s->net_ads * s->net_ads;
+  double d_host = 2.0 * e[1] + 2.0 * h.uion * h.net_fw * dq;
+  out[0] = d_ads;
+  out[1] = d_host;
+  out[2] = dq;
+  s->pending_dq = dq;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_ewald_accept(rgpu_system *s)
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  if (!s->h.ewald || !s->h.nk) return RGPU_SUCCESS;
+  CK(rgpu_ewald_accept_launch(s->d_sys, s->ds, s->h.nk, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  s->net_ads += s->pending_dq;
+  s->pending_dq = 0.0;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_total_energy(rgpu_system *s, double *out)
+{
+  if (!s || !out) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  const int na = s->d.natom, nads = s->h_nmol * na;
+  double hv = 0, hc = 0, av = 0, ac = 0;
+  std::vector<int> atom(RGPU_MAX_POS), excl(RGPU_MAX_POS);
+  std::vector<double> res(4 * RGPU_MAX_POS);
+  for (int base = 0; base < nads; base += RGPU_MAX_POS) {
+    int b = std::min(RGPU_MAX_POS, nads - base);
+    for (int i = 0; i < b; i++) {
+      atom[i] = (base + i) % na;
+      excl[i] = (base + i) / na;
+    }
+    rc = bead_batch(s, RGPU_FP64, b, &s->h_xyz[(size_t)base * 3], atom.data(), excl.data(), 0, res.data(), nullptr);
+    if (rc) return rc;
+    for (int i = 0; i < b; i++) {
+      hv += res[4 * i];
+      hc += res[4 * i + 1];
+      av += res[4 * i + 2];
+      ac += res[4 * i + 3];
+    }
+  }
+  double hf = 0.0, af = 0.0;
+  const RgpuSys &h = s->h;
+  if (h.ewald && h.nk) {
+    rc = recompute_sk_ads(s);
+    if (rc) return rc;
+    std::vector<double2> sa(h.nk), sf(h.nk);
+    std::vector<double> kf(h.nk);
+    CK(cudaMemcpyAsync(sa.data(), s->sk_ads, sizeof(double2) * h.nk, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(sf.data(), s->sk_fw, sizeof(double2) * h.nk, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(kf.data(), s->kfactor, sizeof(double) * h.nk, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int k = 0; k < h.nk; k++) {
+      af += kf[k] * (sa[k].x * sa[k].x + sa[k].y * sa[k].y);
+      hf += kf[k] * (sf[k].x * sa[k].x + sf[k].y * sa[k].y);
+    }
+    double ex = 0.0;
+    for (int m = 0; m < s->h_nmol; m++) ex += exclusion_energy(s, &s->h_xyz[(size_t)m * na * 3]);
+    const double net = s->h_nmol * h.mol_charge;
+    af -= ex + s->h_nmol * h.self_mol;
+    af += h.uion * net * net;
+    hf = 2.0 * hf + 2.0 * h.uion * h.net_fw * net;
+    s->net_ads = net;
+  }
+  out[0] = hv;
+  out[1] = 0.5 * av;
+  out[2] = hc;
+  out[3] = 0.5 * ac;
+  out[4] = hf;
+  out[5] = af;
+  return RGPU_SUCCESS;
+}
+
+/* ---------------------------------------------------------------------- */
+extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], const double size[3], const double shift[3],
+                               float *d_grid)
+{
+  if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
+  if (type < 0 || type >= s->ntypes) return fail(RGPU_E_INVALID, "type %d", type);
+  for (int c = 0; c < 3; c++)
+    if (npts[c] < 1) return fail(RGPU_E_INVALID, "npts");
+  RgpuLJ lj[RGPU_MAX_FWTYPES];
+  memset(lj, 0, sizeof lj);
+  for (int sg = 0; sg < s->h.nseg; sg++) {
+    const int ij = type * s->ntypes + s->fw_seg_type[sg];
+    lj[sg].eps4 = 4.0 * s->lj_eps[ij];
+    lj[sg].sig2 = s->lj_sig2[ij];
+    lj[sg].shift = s->lj_shift[ij];
+  }
+  CK(rgpu_grid_build_launch_lj(s->d_sys, lj, npts, size, shift, d_grid, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3],
+                                     const double shift[3], const double cell[3], int n, const double *xyz,
+                                     double *out)
+{
+  if (!d_grid || !npts || !size || !shift || !cell || n < 0 || (n && (!xyz || !out)))
+    return fail(RGPU_E_INVALID, "bad argument");
+  if (n == 0) return RGPU_SUCCESS;
+  double *dx = nullptr, *dout = nullptr;
+  CK(cudaMalloc((void **)&dx, sizeof(double) * 3 * n));
+  if (cudaMalloc((void **)&dout, sizeof(double) * n) != cudaSuccess) {
+    cudaFree(dx);
+    return fail(RGPU_E_CUDA, "cudaMalloc");
+  }
+  int rc = RGPU_SUCCESS;
+  if (cudaMemcpy(dx, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice) ||
+      rgpu_grid_interp_launch(d_grid, npts, size, shift, cell, n, dx, dout, 0) ||
+      cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost))
+    rc = fail(RGPU_E_CUDA, "grid interpolation: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFree(dx);
+  cudaFree(dout);
+  return rc;
+}
+
+/* ---------------------------------------------------------------------- */
+extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads)
+{
+  if (!out || !systems || n < 1) return fail(RGPU_E_INVALID, "bad argument");
+  if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
+  if (threads < 64 || threads > 512 || threads % 32) return fail(RGPU_E_INVALID, "threads %d", threads);
+  *out = nullptr;
+  rgpu_engine *e = new rgpu_engine();
+  e->mixed = precision == RGPU_MIXED;
+  e->threads = threads;
+  e->kw = 1;
+  e->max_ads = 0;
+  int maxfw = 0;
+  for (int i = 0; i < n; i++) {
+    rgpu_system *s = systems[i];
+    if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
+    e->sys.push_back(s);
+    e->kw = std::max(e->kw, s->kw);
+    e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
+    maxfw = std::max(maxfw, s->d.nfw);
+  }
+  int dev = 0, smem_max = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  e->nfw_smem = maxfw;
+  if (rgpu_engine_smem_bytes(e->mixed, maxfw, e->max_ads, e->kw) > (size_t)smem_max) e->nfw_smem = 0;
+  if (rgpu_engine_smem_bytes(e->mixed, e->nfw_smem, e->max_ads, e->kw) > (size_t)smem_max) {
+    delete e;
+    return fail(RGPU_E_INVALID, "adsorbate capacity does not fit in shared memory");
+  }
+  std::vector<RgpuSys> hs(n);
+  for (int i = 0; i < n; i++) {
+    hs[i] = e->sys[i]->h;
+    hs[i].smem_fw = e->nfw_smem > 0;
+  }
+  if (cudaMalloc((void **)&e->d_systems, sizeof(RgpuSys) * n) != cudaSuccess) {
+    delete e;
+    return fail(RGPU_E_CUDA, "cudaMalloc engine");
+  }
+  e->st = e->sys[0]->st;
+  if (cudaMemcpy(e->d_systems, hs.data(), sizeof(RgpuSys) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(e->d_systems);
+    delete e;
+    return fail(RGPU_E_CUDA, "upload engine");
+  }
+  *out = e;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_destroy(rgpu_engine *e)
+{
+  if (!e) return RGPU_SUCCESS;
+  cudaFree(e->d_systems);
+  delete e;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
+{
+  if (!e || nsteps < 0) return fail(RGPU_E_INVALID, "bad argument");
+  cudaStream_t st = stream ? (cudaStream_t)stream : e->st;
+  /* every system's own stream work (uploads) must be visible to the launch */
+  for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
+  const int n = (int)e->sys.size();
+  CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->nfw_smem, e->threads, n, st));
+  for (rgpu_system *s : e->sys) s->records_stale = 1;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_sync(rgpu_engine *e)
+{
+  if (!e) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaStreamSynchronize(e->st));
+  CK(cudaDeviceSynchronize());
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *counters12, int *nmol, int *status,
+                                 unsigned long long *step)
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaDeviceSynchronize());
+  if (energy8) CK(cudaMemcpy(energy8, s->energy, sizeof(double) * RGPU_NE, cudaMemcpyDeviceToHost));
+  if (counters12) CK(cudaMemcpy(counters12, s->counters, sizeof(long long) * RGPU_NCNT, cudaMemcpyDeviceToHost));
+  if (nmol) CK(cudaMemcpy(nmol, s->nmol, sizeof(int), cudaMemcpyDeviceToHost));
+  if (status) CK(cudaMemcpy(status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (step) CK(cudaMemcpy(step, s->step, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_set_energy(rgpu_system *s, const double *energy8)
+{
+  if (!s || !energy8) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaMemcpy(s->energy, energy8, sizeof(double) * RGPU_NE, cudaMemcpyHostToDevice));
+  return RGPU_SUCCESS;
+}

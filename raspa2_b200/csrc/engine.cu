@@ -1,0 +1,741 @@
+/* Kernels of the B200 GCMC energy path.
+ *
+ *  - rgpu_engine_kernel: the persistent batched MC engine. One thread block
+ *    owns one simulation box for the whole launch: the framework and the
+ *    adsorbate records live in shared memory, the structure factors S(k) and
+ *    the authoritative FP64 positions in HBM/L2. Each block advances its box
+ *    by `nsteps` MC moves (translation, rotation, CBMC insertion, CBMC
+ *    deletion: src/mc_moves.c:1529, :2636, :6941, :7150) without returning
+ *    to the host, drawing every random number from the counter-based Philox
+ *    stream (so FP64 and mixed runs see identical streams).
+ *  - per-call kernels behind the reference-named C entry points: batched
+ *    bead energies, energy differences of a moved molecule, Ewald Fourier
+ *    difference and accept, full energy, structure factors.
+ */
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "rgpu_device.cuh"
+#include "rgpu_engine.h"
+
+#define RGPU_MAX_UNITS 512
+
+/* ------------------------------------------------------------------------ */
+/* shared-memory plan of the engine (offsets in bytes from the dynamic base) */
+struct EngineLayout {
+  size_t sys, fw, ads, xyz, pos, res, ovf, uv, uc, uo, sites, tab, red, ctl, total;
+};
+
+__host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+__host__ __device__ inline EngineLayout engine_layout(int mixed, int nfw_smem, int max_ads_atoms, int kw)
+{
+  EngineLayout L;
+  size_t o = 0;
+  L.sys = o; o = rgpu_align(o + sizeof(RgpuSys));
+  L.fw = o; o = rgpu_align(o + (size_t)nfw_smem * (mixed ? sizeof(int4) : sizeof(double4)));
+  L.ads = o; o = rgpu_align(o + (size_t)max_ads_atoms * (mixed ? sizeof(int4) : sizeof(AdsRec64)));
+  L.xyz = o; o = rgpu_align(o + (mixed ? (size_t)max_ads_atoms * 3 * sizeof(double) : 0));
+  L.pos = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(BeadPos));
+  L.res = o; o = rgpu_align(o + RGPU_MAX_POS * 4 * sizeof(double));
+  L.ovf = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(int));
+  L.uv = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
+  L.uc = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
+  L.uo = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(int));
+  L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
+  L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed ? sizeof(float2) : sizeof(double2)));
+  L.red = o; o = rgpu_align(o + 72 * sizeof(double));
+  L.ctl = o; o = rgpu_align(o + 64 * sizeof(double));
+  L.total = o;
+  return L;
+}
+
+size_t rgpu_engine_smem_bytes(int mixed, int nfw_smem, int max_ads_atoms, int kw)
+{
+  return engine_layout(mixed, nfw_smem, max_ads_atoms, kw).total;
+}
+
+/* broadcast/control block in shared memory */
+struct Ctl {
+  double u[4];        /* energies of the chosen configuration */
+  double rosen;
+  double e_ads, e_host;
+  double dl[4];
+  int nmol;
+  int fail;
+  int accept;
+  int sel;
+  int nads;           /* adsorbate atoms = nmol * natom */
+};
+
+template <bool MIXED>
+struct Eng {
+  RgpuSys *S;
+  const void *fw;
+  void *ads;                 /* int4[] or AdsRec64[] */
+  double (*xyz)[3];          /* FP64 positions (MIXED: separate array; FP64: inside ads records) */
+  BeadPos *pos;
+  double (*res)[4];
+  int *ovf;
+  EvalScratch sc;
+  EwSite *sites;
+  typename PhaseT<MIXED>::T *tab;
+  int kw;
+  double *red;
+  Ctl *ctl;
+};
+
+/* position of atom a of molecule m */
+template <bool MIXED>
+__device__ __forceinline__ void atom_xyz(const Eng<MIXED> &E, int m, int a, double *p)
+{
+  const int idx = m * E.S->natom + a;
+  if (MIXED) {
+    p[0] = E.xyz[idx][0]; p[1] = E.xyz[idx][1]; p[2] = E.xyz[idx][2];
+  } else {
+    const AdsRec64 &r = ((const AdsRec64 *)E.ads)[idx];
+    p[0] = r.x; p[1] = r.y; p[2] = r.z;
+  }
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void atom_store(const Eng<MIXED> &E, int m, int a, const double *p)
+{
+  const RgpuSys &S = *E.S;
+  const int idx = m * S.natom + a;
+  if (MIXED) {
+    E.xyz[idx][0] = p[0]; E.xyz[idx][1] = p[1]; E.xyz[idx][2] = p[2];
+    ((int4 *)E.ads)[idx] = make_int4(rgpu_to_fix(p[0], S.inv_box[0]), rgpu_to_fix(p[1], S.inv_box[1]),
+                                     rgpu_to_fix(p[2], S.inv_box[2]), m * 16 + a);
+  } else {
+    AdsRec64 r;
+    r.x = p[0]; r.y = p[1]; r.z = p[2]; r.tag = m * 16 + a;
+    ((AdsRec64 *)E.ads)[idx] = r;
+  }
+}
+
+/* RotationAround{X,Y,Z}Axis, src/utils.c:876-936 */
+__device__ __forceinline__ void rotate_axis(double *c, int axis, double th)
+{
+  double cs, sn;
+  sincos(th, &sn, &cs);
+  double x = c[0], y = c[1], z = c[2];
+  if (axis == 0) { c[1] = cs * y + sn * z; c[2] = -sn * y + cs * z; }
+  else if (axis == 1) { c[0] = cs * x - sn * z; c[2] = sn * x + cs * z; }
+  else { c[0] = cs * x + sn * y; c[1] = -sn * x + cs * y; }
+}
+
+/* RandomArrayRotationMatrix (Shoemake), src/utils.c:835-874 */
+__device__ __forceinline__ void random_rotation(double x0, double y1, double y2, double R[3][3])
+{
+  y1 *= 2.0 * M_PI;
+  y2 *= 2.0 * M_PI;
+  double r1 = sqrt(1.0 - x0), r2 = sqrt(x0);
+  double s1, c1, s2, c2;
+  sincos(y1, &s1, &c1);
+  sincos(y2, &s2, &c2);
+  double u0 = c2 * r2, u1 = s1 * r1, u2 = c1 * r1, u3 = s2 * r2;
+  double ci = 2.0 * u0 * u0 - 1.0, ce = 2.0 * u0;
+  R[0][0] = ci + 2.0 * u1 * u1;
+  R[1][1] = ci + 2.0 * u2 * u2;
+  R[2][2] = ci + 2.0 * u3 * u3;
+  R[1][2] = 2.0 * u2 * u3 - ce * u1;
+  R[2][0] = 2.0 * u3 * u1 - ce * u2;
+  R[0][1] = 2.0 * u1 * u2 - ce * u3;
+  R[2][1] = 2.0 * u3 * u2 + ce * u1;
+  R[0][2] = 2.0 * u1 * u3 + ce * u2;
+  R[1][0] = 2.0 * u2 * u1 + ce * u3;
+}
+
+/* SelectTrialPosition, src/cbmc.c:563-599 */
+__device__ inline int select_trial(const double *bf, const int *ov, int n, double u)
+{
+  double largest = -DBL_MAX, sum = 0.0, w[RGPU_MAX_TRIALS];
+  for (int i = 0; i < n; i++)
+    if (!ov[i] && bf[i] > largest) largest = bf[i];
+  for (int i = 0; i < n; i++) {
+    w[i] = ov[i] ? 0.0 : exp(bf[i] - largest);
+    sum += w[i];
+  }
+  int sel = 0;
+  double cum = w[0], ws = u * sum;
+  while (cum < ws && sel < n - 1) cum += w[++sel];
+  return sel;
+}
+
+/* Ewald difference for the sites in E.sites[0..ns); all threads call. */
+template <bool MIXED>
+__device__ void engine_ewald(const Eng<MIXED> &E, int ns, double &e_ads, double &e_host)
+{
+  ewald_phases<MIXED>(*E.S, E.sites, ns, E.tab, E.kw);
+  __syncthreads();
+  ewald_energy_sum<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, e_ads, e_host, E.red);
+}
+
+/* ------------------------------------------------------------------------ */
+/* translation (mv=0) and rotation (mv=1):
+ * TranslationMoveAdsorbate src/mc_moves.c:1529-1762, RotationMoveAdsorbate :2636 */
+template <bool MIXED>
+__device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, nmol = C.nmol;
+  int m = (int)(rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOLECULE) * nmol);
+  if (m >= nmol) m = nmol - 1;
+  const double vnew = 2.0 * rgpu_uniform(S.seed, S.sys_id, step, SLOT_VNEW) - 1.0;
+  int axis = (int)(3.0 * rgpu_uniform(S.seed, S.sys_id, step, SLOT_AXIS));
+  if (axis > 2) axis = 2;
+  if (threadIdx.x < na) {
+    const int a = threadIdx.x;
+    double o[3], n[3];
+    atom_xyz(E, m, a, o);
+    if (mv == 0) {
+      n[0] = o[0]; n[1] = o[1]; n[2] = o[2];
+      n[axis] += vnew * S.max_translation;
+    } else {
+      double sb[3];
+      atom_xyz(E, m, S.start_bead, sb);
+      double c[3] = {o[0] - sb[0], o[1] - sb[1], o[2] - sb[2]};
+      rotate_axis(c, axis, vnew * S.max_rotation);
+      n[0] = c[0] + sb[0]; n[1] = c[1] + sb[1]; n[2] = c[2] + sb[2];
+    }
+    bead_set(E.pos[a], S, n[0], n[1], n[2], a, m);
+    bead_set(E.pos[na + a], S, o[0], o[1], o[2], a, m);
+    E.sites[a].b = E.pos[a];
+    E.sites[a].q = S.mol_q[a];
+    E.sites[na + a].b = E.pos[na + a];
+    E.sites[na + a].q = -S.mol_q[a];
+  }
+  __syncthreads();
+  eval_positions<MIXED>(S, E.fw, E.ads, C.nads, E.pos, 2 * na, na, E.res, E.ovf, E.sc, RGPU_MAX_UNITS);
+  if (threadIdx.x == 0) {
+    int ov = 0;
+    double dl[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int a = 0; a < na; a++) {
+      ov |= E.ovf[a];
+      for (int k = 0; k < 4; k++) dl[k] += E.res[a][k] - E.res[na + a][k];
+    }
+    C.fail = ov;
+    for (int k = 0; k < 4; k++) C.dl[k] = dl[k];
+  }
+  __syncthreads();
+  if (C.fail) {
+    if (threadIdx.x == 0) S.counters[RGPU_CNT_OVERLAP]++;
+    return;
+  }
+  double ea = 0.0, eh = 0.0;
+  const bool ew = S.ewald && S.mol_charged;
+  if (ew) engine_ewald<MIXED>(E, 2 * na, ea, eh);
+  if (threadIdx.x == 0) {
+    double d_ads = 0.0, d_host = 0.0;
+    if (ew) {
+      /* exclusions cancel for a rigid displacement but are kept for parity */
+      double xn[RGPU_MAX_ATOMS][3], xo[RGPU_MAX_ATOMS][3];
+      for (int a = 0; a < na; a++) {
+        xn[a][0] = E.pos[a].x; xn[a][1] = E.pos[a].y; xn[a][2] = E.pos[a].z;
+        xo[a][0] = E.pos[na + a].x; xo[a][1] = E.pos[na + a].y; xo[a][2] = E.pos[na + a].z;
+      }
+      ewald_finish(S, ea, eh, ewald_exclusion(S, xn), ewald_exclusion(S, xo), 0, 0.0, d_ads, d_host);
+    }
+    double du = C.dl[0] + C.dl[1] + C.dl[2] + C.dl[3] + d_ads + d_host;
+    double u = rgpu_uniform(S.seed, S.sys_id, step, SLOT_ACCEPT);
+    double pacc = exp(-S.beta * du);
+    if (!isfinite(du)) *S.status |= RGPU_ERR_NONFINITE;
+    C.accept = u < pacc;
+    if (C.accept) {
+      S.counters[RGPU_CNT_ACCEPT + mv]++;
+      S.energy[RGPU_E_HOST_VDW] += C.dl[0];
+      S.energy[RGPU_E_HOST_REAL] += C.dl[1];
+      S.energy[RGPU_E_ADS_VDW] += C.dl[2];
+      S.energy[RGPU_E_ADS_REAL] += C.dl[3];
+      S.energy[RGPU_E_HOST_FOURIER] += d_host;
+      S.energy[RGPU_E_ADS_FOURIER] += d_ads;
+    }
+  }
+  __syncthreads();
+  if (C.accept) {
+    if (threadIdx.x < na) {
+      double p[3] = {E.pos[threadIdx.x].x, E.pos[threadIdx.x].y, E.pos[threadIdx.x].z};
+      atom_store(E, m, threadIdx.x, p);
+    }
+    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, 2 * na);
+  }
+  __syncthreads();
+}
+
+/* ------------------------------------------------------------------------ */
+/* CBMC insertion / deletion of a rigid molecule grown from the starting bead:
+ * GrowMolecule src/cbmc.c:3056-3181 and RetraceMolecule :2928-3054 with
+ * HandleFirstBead :623-795, Rosen/RosenOld :2762-2926, the rigid-group branch
+ * of GenerateTrialOrientationsSimpleSphere :1480-1578 and
+ * ComputeExternalEnergies :1154-1478, LJ biasing; acceptance of
+ * SwapAddAdsorbateMove src/mc_moves.c:7016 and SwapRemoveAdsorbateMove :7228. */
+template <bool MIXED>
+__device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, sb = S.start_bead, nmol = C.nmol;
+  const int nf = S.ntrial_first, nt = S.ntrial;
+  int m = nmol;
+  if (!insert) {
+    m = (int)(rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOLECULE) * nmol);
+    if (m >= nmol) m = nmol - 1;
+  }
+  const int exclude = insert ? -1 : m;
+  /* first-bead trials */
+  if (threadIdx.x < nf) {
+    const int i = threadIdx.x;
+    double p[3];
+    if (!insert && i == 0) {
+      atom_xyz(E, m, sb, p);
+    } else {
+      double sz = rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST + 3 * i + 0);
+      double sy = rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST + 3 * i + 1);
+      double sx = rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST + 3 * i + 2);
+      p[0] = S.box[0] * sx; p[1] = S.box[1] * sy; p[2] = S.box[2] * sz;
+    }
+    bead_set(E.pos[i], S, p[0], p[1], p[2], sb, exclude);
+  }
+  __syncthreads();
+  eval_positions<MIXED>(S, E.fw, E.ads, C.nads, E.pos, nf, 0, E.res, E.ovf, E.sc, RGPU_MAX_UNITS);
+  if (threadIdx.x == 0) {
+    double bf[RGPU_MAX_TRIALS];
+    int ov[RGPU_MAX_TRIALS], any = 0;
+    double w1 = 0.0;
+    for (int i = 0; i < nf; i++) {
+      ov[i] = (E.res[i][0] >= S.overlap || E.res[i][1] >= S.overlap || E.res[i][2] >= S.overlap ||
+               E.res[i][3] >= S.overlap);
+      bf[i] = ov[i] ? 0.0 : -S.beta * (E.res[i][0] + E.res[i][2]);
+      if (!ov[i]) { any = 1; w1 += exp(bf[i]); }
+    }
+    int sel = 0;
+    C.fail = !any;
+    if (any && insert) sel = select_trial(bf, ov, nf, rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST_SELECT));
+    C.rosen = w1 / (double)nf;
+    if (insert && C.rosen < 1e-150) C.fail = 1;
+    C.sel = sel;
+    for (int k = 0; k < 4; k++) C.u[k] = E.res[sel][k];
+  }
+  __syncthreads();
+  if (C.fail) {
+    if (threadIdx.x == 0) S.counters[RGPU_CNT_OVERLAP]++;
+    return;
+  }
+  const BeadPos first = E.pos[C.sel];
+  __syncthreads();
+  const int nb = na - 1;   /* beads grown per orientation trial */
+  if (na > 1) {
+    if (threadIdx.x < nt) {
+      const int t = threadIdx.x;
+      if (!insert && t == 0) {
+        int j = 0;
+        for (int a = 0; a < na; a++) {
+          if (a == sb) continue;
+          double p[3];
+          atom_xyz(E, m, a, p);
+          bead_set(E.pos[t * nb + j], S, p[0], p[1], p[2], a, exclude);
+          j++;
+        }
+      } else {
+        double R[3][3];
+        random_rotation(rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT + 4 * t + 0),
+                        rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT + 4 * t + 1),
+                        rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT + 4 * t + 2), R);
+        int j = 0;
+        for (int a = 0; a < na; a++) {
+          if (a == sb) continue;
+          double c[3] = {S.mol_ref[a][0] - S.mol_ref[sb][0], S.mol_ref[a][1] - S.mol_ref[sb][1],
+                         S.mol_ref[a][2] - S.mol_ref[sb][2]};
+          double p[3];
+          p[0] = first.x + c[0] * R[0][0] + c[1] * R[0][1] + c[2] * R[0][2];
+          p[1] = first.y + c[0] * R[1][0] + c[1] * R[1][1] + c[2] * R[1][2];
+          p[2] = first.z + c[0] * R[2][0] + c[1] * R[2][1] + c[2] * R[2][2];
+          bead_set(E.pos[t * nb + j], S, p[0], p[1], p[2], a, exclude);
+          j++;
+        }
+      }
+    }
+    __syncthreads();
+    eval_positions<MIXED>(S, E.fw, E.ads, C.nads, E.pos, nt * nb, 0, E.res, E.ovf, E.sc,
+                          RGPU_MAX_UNITS);
+    if (threadIdx.x == 0) {
+      double bf[RGPU_MAX_TRIALS], et[RGPU_MAX_TRIALS][4];
+      int ov[RGPU_MAX_TRIALS], any = 0;
+      double w = 0.0;
+      for (int t = 0; t < nt; t++) {
+        ov[t] = 0;
+        for (int k = 0; k < 4; k++) et[t][k] = 0.0;
+        for (int j = 0; j < nb; j++) {
+          const double *r = E.res[t * nb + j];
+          if (r[0] >= S.overlap) ov[t] = 1;
+          for (int k = 0; k < 4; k++) et[t][k] += r[k];
+        }
+        bf[t] = ov[t] ? 0.0 : -S.beta * (et[t][0] + et[t][2]);
+        if (!ov[t]) { any = 1; w += exp(bf[t]); }
+      }
+      int iw = 0;
+      if (!any) C.fail = 1;
+      else {
+        if (insert) iw = select_trial(bf, ov, nt, rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT_SELECT));
+        C.rosen *= w / (double)nt;
+        if (insert && C.rosen < 1e-150) C.fail = 1;
+        for (int k = 0; k < 4; k++) C.u[k] += et[iw][k];
+      }
+      C.sel = iw;
+    }
+    __syncthreads();
+    if (C.fail) {
+      if (threadIdx.x == 0) S.counters[RGPU_CNT_OVERLAP]++;
+      return;
+    }
+  }
+  /* sites of the chosen configuration: first bead + beads of trial C.sel */
+  if (threadIdx.x < na) {
+    const int a = threadIdx.x;
+    BeadPos b;
+    if (a == sb) b = first;
+    else {
+      int j = a < sb ? a : a - 1;
+      b = E.pos[C.sel * nb + j];
+    }
+    E.sites[a].b = b;
+    E.sites[a].q = insert ? S.mol_q[a] : -S.mol_q[a];
+  }
+  __syncthreads();
+  double ea = 0.0, eh = 0.0;
+  const bool ew = S.ewald && S.mol_charged;
+  if (ew) engine_ewald<MIXED>(E, na, ea, eh);
+  if (threadIdx.x == 0) {
+    /* LJ-biasing correction, src/cbmc.c:3171-3178 / :3044-3051 */
+    double rosen = C.rosen * exp(-S.beta * (C.u[1] + C.u[3]));
+    double d_ads = 0.0, d_host = 0.0;
+    if (ew) {
+      double x[RGPU_MAX_ATOMS][3];
+      for (int a = 0; a < na; a++) { x[a][0] = E.sites[a].b.x; x[a][1] = E.sites[a].b.y; x[a][2] = E.sites[a].b.z; }
+      double ex = ewald_exclusion(S, x);
+      double net = nmol * S.mol_charge;
+      if (insert) ewald_finish(S, ea, eh, ex, 0.0, 1, net, d_ads, d_host);
+      else ewald_finish(S, ea, eh, 0.0, ex, -1, net, d_ads, d_host);
+    }
+    double u = rgpu_uniform(S.seed, S.sys_id, step, SLOT_ACCEPT);
+    double pacc;
+    if (insert) pacc = rosen * exp(-S.beta * (d_ads + d_host)) * S.fugacity_beta_v / (1.0 + nmol);
+    else pacc = (double)nmol / (rosen * exp(S.beta * (d_ads + d_host)) * S.fugacity_beta_v);
+    if (!(pacc == pacc)) *S.status |= RGPU_ERR_NONFINITE;
+    C.accept = u < pacc;
+    const int mv = insert ? 2 : 3;
+    if (C.accept) {
+      S.counters[RGPU_CNT_ACCEPT + mv]++;
+      double sgn = insert ? 1.0 : -1.0;
+      S.energy[RGPU_E_HOST_VDW] += sgn * C.u[0];
+      S.energy[RGPU_E_HOST_REAL] += sgn * C.u[1];
+      S.energy[RGPU_E_ADS_VDW] += sgn * C.u[2];
+      S.energy[RGPU_E_ADS_REAL] += sgn * C.u[3];
+      S.energy[RGPU_E_HOST_FOURIER] += d_host;
+      S.energy[RGPU_E_ADS_FOURIER] += d_ads;
+    }
+  }
+  __syncthreads();
+  if (C.accept) {
+    if (insert) {
+      if (threadIdx.x < na) {
+        double p[3] = {E.sites[threadIdx.x].b.x, E.sites[threadIdx.x].b.y, E.sites[threadIdx.x].b.z};
+        atom_store(E, nmol, threadIdx.x, p);
+      }
+    } else {
+      /* RemoveAdsorbateMolecule (src/molecule.c:3193): the last molecule
+       * takes the freed slot */
+      const int last = nmol - 1;
+      if (threadIdx.x < na && m != last) {
+        double p[3];
+        atom_xyz(E, last, threadIdx.x, p);
+        atom_store(E, m, threadIdx.x, p);
+      }
+    }
+    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, na);
+    if (threadIdx.x == 0) {
+      C.nmol = insert ? nmol + 1 : nmol - 1;
+      C.nads = C.nmol * na;
+    }
+  }
+  __syncthreads();
+}
+
+/* ------------------------------------------------------------------------ */
+/* Loads a descriptor copy into shared memory. */
+__device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
+{
+  const uint32_t *s = (const uint32_t *)src;
+  uint32_t *d = (uint32_t *)dst;
+  for (int i = threadIdx.x; i < (int)(sizeof(RgpuSys) / 4); i += blockDim.x) d[i] = s[i];
+  __syncthreads();
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps, int kw,
+                                                          int max_ads_atoms, int nfw_smem)
+{
+  extern __shared__ __align__(256) unsigned char smem[];
+  const EngineLayout L = engine_layout(MIXED, nfw_smem, max_ads_atoms, kw);
+  for (int sysi = blockIdx.x; sysi < nsys; sysi += gridDim.x) {
+    Eng<MIXED> E;
+    E.S = (RgpuSys *)(smem + L.sys);
+    E.ads = smem + L.ads;
+    E.xyz = (double(*)[3])(smem + L.xyz);
+    E.pos = (BeadPos *)(smem + L.pos);
+    E.res = (double(*)[4])(smem + L.res);
+    E.ovf = (int *)(smem + L.ovf);
+    E.sc.uv = (double *)(smem + L.uv);
+    E.sc.uc = (double *)(smem + L.uc);
+    E.sc.uo = (int *)(smem + L.uo);
+    E.sites = (EwSite *)(smem + L.sites);
+    E.tab = (typename PhaseT<MIXED>::T *)(smem + L.tab);
+    E.kw = kw;
+    E.red = (double *)(smem + L.red);
+    E.ctl = (Ctl *)(smem + L.ctl);
+    /* load the descriptor */
+    load_sys(E.S, &systems[sysi]);
+    RgpuSys &S = *E.S;
+    /* framework to shared memory */
+    if (S.smem_fw) {
+      if (MIXED) {
+        int4 *d = (int4 *)(smem + L.fw);
+        for (int i = threadIdx.x; i < S.nfw; i += blockDim.x) d[i] = S.fw32[i];
+      } else {
+        double4 *d = (double4 *)(smem + L.fw);
+        for (int i = threadIdx.x; i < S.nfw; i += blockDim.x) d[i] = S.fw64[i];
+      }
+      E.fw = smem + L.fw;
+    } else {
+      E.fw = MIXED ? (const void *)S.fw32 : (const void *)S.fw64;
+    }
+    if (threadIdx.x == 0) {
+      E.ctl->nmol = *S.nmol;
+      E.ctl->nads = E.ctl->nmol * S.natom;
+    }
+    __syncthreads();
+    /* adsorbates to shared memory */
+    for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
+      const int mm = i / S.natom, a = i - mm * S.natom;
+      double p[3] = {S.ads_xyz[3 * i], S.ads_xyz[3 * i + 1], S.ads_xyz[3 * i + 2]};
+      atom_store(E, mm, a, p);
+    }
+    __syncthreads();
+    const uint64_t step0 = *S.step;
+    for (long long it = 0; it < nsteps; it++) {
+      const uint64_t step = step0 + (uint64_t)it;
+      const double u0 = rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOVE);
+      int mv = 0;
+      while (mv < 3 && u0 >= S.cum[mv]) mv++;
+      const int nmol = E.ctl->nmol;
+      if (mv <= 1) {
+        if (nmol == 0 || (mv == 1 && S.natom == 1)) continue;
+        if (threadIdx.x == 0) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + mv]++; }
+        step_displace<MIXED>(E, step, mv);
+      } else if (mv == 2) {
+        if (threadIdx.x == 0) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 2]++; }
+        if (nmol >= S.maxmol) {
+          if (threadIdx.x == 0) *S.status |= RGPU_ERR_MAXMOL;
+          continue;
+        }
+        step_swap<MIXED>(E, step, true);
+      } else {
+        if (threadIdx.x == 0) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 3]++; }
+        if (nmol == 0) continue;
+        step_swap<MIXED>(E, step, false);
+      }
+    }
+    __syncthreads();
+    /* write back positions and the molecule count */
+    for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
+      const int mm = i / S.natom, a = i - mm * S.natom;
+      double p[3];
+      atom_xyz(E, mm, a, p);
+      S.ads_xyz[3 * i] = p[0];
+      S.ads_xyz[3 * i + 1] = p[1];
+      S.ads_xyz[3 * i + 2] = p[2];
+    }
+    if (threadIdx.x == 0) {
+      *S.nmol = E.ctl->nmol;
+      *S.step = step0 + (uint64_t)nsteps;
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
+                               int max_ads_atoms, int nfw_smem, int threads, int blocks, cudaStream_t st)
+{
+  size_t smem = rgpu_engine_smem_bytes(mixed, nfw_smem, max_ads_atoms, kw);
+  cudaError_t e;
+  if (mixed) {
+    e = cudaFuncSetAttribute(rgpu_engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    rgpu_engine_kernel<true><<<blocks, threads, smem, st>>>(d_systems, nsys, nsteps, kw, max_ads_atoms, nfw_smem);
+  } else {
+    e = cudaFuncSetAttribute(rgpu_engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    rgpu_engine_kernel<false><<<blocks, threads, smem, st>>>(d_systems, nsys, nsteps, kw, max_ads_atoms, nfw_smem);
+  }
+  return cudaGetLastError();
+}
+
+/* ------------------------------------------------------------------------ */
+/* per-call kernels (one thread block per call; the plain path) */
+
+struct CallSmem {
+  double res[RGPU_MAX_POS][4];
+  int ovf[RGPU_MAX_POS];
+  double uv[RGPU_MAX_UNITS], uc[RGPU_MAX_UNITS];
+  int uo[RGPU_MAX_UNITS];
+  BeadPos pos[RGPU_MAX_POS];
+  double red[72];
+};
+
+
+/* Energies of P bead positions (P <= RGPU_MAX_POS), given as FP64 xyz with
+ * the molecule-atom index of each bead. out[p*4 + k], ov[p]. */
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, const void *ads, int nads,
+                                                        const double *xyz, const int *atom, const int *excl, int P,
+                                                        int pair_check, double *out, int *ov)
+{
+  __shared__ RgpuSys S;
+  __shared__ CallSmem sm;
+  load_sys(&S, sysp);
+  for (int p = threadIdx.x; p < P; p += blockDim.x) bead_set(sm.pos[p], S, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], atom[p], excl[p]);
+  __syncthreads();
+  EvalScratch sc = {sm.uv, sm.uc, sm.uo, nullptr};
+  eval_positions<MIXED>(S, MIXED ? (const void *)S.fw32 : (const void *)S.fw64, ads, nads, sm.pos, P,
+                        pair_check, sm.res, sm.ovf, sc, RGPU_MAX_UNITS);
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    for (int k = 0; k < 4; k++) out[4 * p + k] = sm.res[p][k];
+    if (ov) ov[p] = sm.ovf[p];
+  }
+}
+
+cudaError_t rgpu_point_energies_launch(int mixed, const RgpuSys *d_sys, const void *d_ads, int nads,
+                                       const double *d_xyz, const int *d_atom, const int *d_excl, int P,
+                                       int pair_check, double *d_out, int *d_ov, cudaStream_t st)
+{
+  if (P > RGPU_MAX_POS) return cudaErrorInvalidValue;
+  if (mixed)
+    k_point_energies<true><<<1, 256, 0, st>>>(d_sys, d_ads, nads, d_xyz, d_atom, d_excl, P, pair_check, d_out, d_ov);
+  else
+    k_point_energies<false><<<1, 256, 0, st>>>(d_sys, d_ads, nads, d_xyz, d_atom, d_excl, P, pair_check, d_out, d_ov);
+  return cudaGetLastError();
+}
+
+/* Ewald Fourier difference of ns signed sites (FP64 xyz + charges), writing
+ * dS(k) of the candidate into d_ds (for a later accept) and {e_ads, e_host}. */
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_ewald_delta(const RgpuSys *sysp, const double *xyz, const double *q, int ns,
+                                                     double2 *d_ds, double *out, int kw)
+{
+  __shared__ RgpuSys S;
+  __shared__ EwSite sites[2 * RGPU_MAX_ATOMS];
+  __shared__ typename PhaseT<MIXED>::T tab[2 * RGPU_MAX_ATOMS * 3 * 41];
+  __shared__ double red[72];
+  load_sys(&S, sysp);
+  for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+    bead_set(sites[s].b, S, xyz[3 * s], xyz[3 * s + 1], xyz[3 * s + 2], 0, -1);
+    sites[s].q = q[s];
+  }
+  __syncthreads();
+  ewald_phases<MIXED>(S, sites, ns, tab, kw);
+  __syncthreads();
+  double ea = 0.0, eh = 0.0;
+  for (int k = threadIdx.x; k < S.nk; k += blockDim.x) {
+    double2 d = ewald_dS<MIXED>(tab, kw, sites, ns, S.kvec[k]);
+    double2 so = S.sk_ads[k];
+    double2 sf = S.sk_fw[k];
+    double kf = S.kfactor[k];
+    ea += kf * (2.0 * (so.x * d.x + so.y * d.y) + d.x * d.x + d.y * d.y);
+    eh += kf * (sf.x * d.x + sf.y * d.y);
+    if (d_ds) d_ds[k] = d;
+  }
+  block_sum2(ea, eh, red);
+  if (threadIdx.x == 0) { out[0] = ea; out[1] = eh; }
+}
+
+__global__ void k_ewald_accept(const RgpuSys *sysp, const double2 *d_ds)
+{
+  const RgpuSys *S = sysp;
+  int nk = S->nk;
+  double2 *sk = S->sk_ads;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
+    double2 a = sk[k], d = d_ds[k];
+    sk[k] = make_double2(a.x + d.x, a.y + d.y);
+  }
+}
+
+cudaError_t rgpu_ewald_delta_launch(int mixed, const RgpuSys *d_sys, const double *d_xyz, const double *d_q, int ns,
+                                    double2 *d_ds, double *d_out, int kw, cudaStream_t st)
+{
+  if (ns > 2 * RGPU_MAX_ATOMS || kw > 41) return cudaErrorInvalidValue;
+  if (mixed) k_ewald_delta<true><<<1, 256, 0, st>>>(d_sys, d_xyz, d_q, ns, d_ds, d_out, kw);
+  else k_ewald_delta<false><<<1, 256, 0, st>>>(d_sys, d_xyz, d_q, ns, d_ds, d_out, kw);
+  return cudaGetLastError();
+}
+
+cudaError_t rgpu_ewald_accept_launch(const RgpuSys *d_sys, const double2 *d_ds, int nk, cudaStream_t st)
+{
+  int blocks = (nk + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  k_ewald_accept<<<blocks, 256, 0, st>>>(d_sys, d_ds);
+  return cudaGetLastError();
+}
+
+/* S(k) = sum_i q_i exp(i k.r_i) over n sites (FP64), one thread per k */
+__global__ void k_structure_factor(const RgpuSys *sysp, const double *xyz, const double *q, int n, double2 *sk)
+{
+  const RgpuSys *S = sysp;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= S->nk) return;
+  char4 kv = S->kvec[k];
+  double re = 0.0, im = 0.0;
+  for (int i = 0; i < n; i++) {
+    double a = 2.0 * (kv.x * xyz[3 * i] * S->inv_box[0] + kv.y * xyz[3 * i + 1] * S->inv_box[1] +
+                      kv.z * xyz[3 * i + 2] * S->inv_box[2]);
+    double sn, cs;
+    sincospi(a, &sn, &cs);
+    re += q[i] * cs;
+    im += q[i] * sn;
+  }
+  sk[k] = make_double2(re, im);
+}
+
+cudaError_t rgpu_structure_factor_launch(const RgpuSys *d_sys, const double *d_xyz, const double *d_q, int n,
+                                         int nk, double2 *d_sk, cudaStream_t st)
+{
+  int blocks = (nk + 127) / 128;
+  if (blocks < 1) blocks = 1;
+  k_structure_factor<<<blocks, 128, 0, st>>>(d_sys, d_xyz, d_q, n, d_sk);
+  return cudaGetLastError();
+}
+
+/* adsorbate records (fixed-point and FP64) from the authoritative positions */
+__global__ void k_build_records(const RgpuSys *sysp, int nads, int4 *rec32, AdsRec64 *rec64)
+{
+  const RgpuSys *S = sysp;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nads) return;
+  const int m = i / S->natom, a = i - m * S->natom;
+  const double x = S->ads_xyz[3 * i], y = S->ads_xyz[3 * i + 1], z = S->ads_xyz[3 * i + 2];
+  rec32[i] = make_int4(rgpu_to_fix(x, S->inv_box[0]), rgpu_to_fix(y, S->inv_box[1]), rgpu_to_fix(z, S->inv_box[2]),
+                       m * 16 + a);
+  AdsRec64 r;
+  r.x = x; r.y = y; r.z = z; r.tag = m * 16 + a;
+  rec64[i] = r;
+}
+
+cudaError_t rgpu_records_launch(const RgpuSys *d_sys, int nads, int4 *d_rec32, void *d_rec64, cudaStream_t st)
+{
+  if (nads <= 0) return cudaSuccess;
+  k_build_records<<<(nads + 127) / 128, 128, 0, st>>>(d_sys, nads, d_rec32, (AdsRec64 *)d_rec64);
+  return cudaGetLastError();
+}

@@ -1,0 +1,244 @@
+/* Energy-grid construction and tricubic lookup.
+ *
+ * Build: MakeGrid (src/grids.c:431-690) with the per-point derivatives of
+ * CalculateDerivativesAtPositionVDW (src/framework_hessian.c:63-109) and the
+ * LJ branch of PotentialThirdDerivative (src/potentials.c:10959-10990),
+ * computed in FP64 and stored as FP32 like the reference. One thread per grid
+ * point; a block covers a 4x8x8 tile and stages, chunk by chunk, only the
+ * framework atoms within cutoff + tile radius of the tile centre in shared
+ * memory, so each thread visits ~1/7 of the framework at 0.1 A spacing.
+ *
+ * Device layout is point-major: grid[((i*(ny+1) + j)*(nz+1) + k)*8 + m], so
+ * the 8 values of a corner are one 32-byte sector and a lookup gathers eight
+ * sectors (the reference's file is plane-major; the Python side converts).
+ *
+ * Lookup: InterpolateVDWGrid (src/grids.c:979-1077). The reference forms the
+ * 64 tricubic coefficients with the Lekien-Marsden matrix and evaluates the
+ * polynomial; the same interpolant is evaluated here as the tensor product of
+ * 1D cubic Hermite bases over the stored value and derivatives (FP64 math on
+ * the FP32 data, as in the reference).
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "rgpu_device.cuh"
+#include "rgpu_engine.h"
+
+#define GRID_TX 4
+#define GRID_TY 8
+#define GRID_TZ 8
+#define GRID_THREADS (GRID_TX * GRID_TY * GRID_TZ)
+
+struct GridParams {
+  int npts[3];
+  double size[3], shift[3], delta[3];
+  RgpuLJ lj[RGPU_MAX_FWTYPES];
+};
+
+__global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp, GridParams gp, float *grid)
+{
+  __shared__ double4 fwc[GRID_THREADS];
+  __shared__ int segc[GRID_THREADS];
+  __shared__ int wcount[GRID_THREADS / 32];
+  __shared__ int nsel;
+  const RgpuSys &S = *sysp;
+  const int nx = gp.npts[0] + 1, ny = gp.npts[1] + 1, nz = gp.npts[2] + 1;
+  const int tilesz = (nz + GRID_TZ - 1) / GRID_TZ, tilesy = (ny + GRID_TY - 1) / GRID_TY;
+  int b = blockIdx.x;
+  const int tk = b % tilesz; b /= tilesz;
+  const int tj = b % tilesy; b /= tilesy;
+  const int ti = b;
+  const int lk = threadIdx.x % GRID_TZ, lj = (threadIdx.x / GRID_TZ) % GRID_TY, li = threadIdx.x / (GRID_TZ * GRID_TY);
+  const int i = ti * GRID_TX + li, j = tj * GRID_TY + lj, k = tk * GRID_TZ + lk;
+  const bool valid = i < nx && j < ny && k < nz;
+  const double px = i * gp.size[0] / gp.npts[0] + gp.shift[0];
+  const double py = j * gp.size[1] / gp.npts[1] + gp.shift[1];
+  const double pz = k * gp.size[2] / gp.npts[2] + gp.shift[2];
+  /* tile centre and radius for culling */
+  const double cx = (ti * GRID_TX + 0.5 * (GRID_TX - 1)) * gp.size[0] / gp.npts[0] + gp.shift[0];
+  const double cy = (tj * GRID_TY + 0.5 * (GRID_TY - 1)) * gp.size[1] / gp.npts[1] + gp.shift[1];
+  const double cz = (tk * GRID_TZ + 0.5 * (GRID_TZ - 1)) * gp.size[2] / gp.npts[2] + gp.shift[2];
+  const double hx = 0.5 * (GRID_TX - 1) * gp.delta[0], hy = 0.5 * (GRID_TY - 1) * gp.delta[1],
+               hz = 0.5 * (GRID_TZ - 1) * gp.delta[2];
+  const double rcut = sqrt(S.rc2) + sqrt(hx * hx + hy * hy + hz * hz) + 1e-6;
+  const double rcut2 = rcut * rcut;
+  const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
+  const double ix = S.inv_box[0], iy = S.inv_box[1], iz = S.inv_box[2];
+  double o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int base = 0; base < S.nfw; base += GRID_THREADS) {
+    const int a = base + threadIdx.x;
+    int keep = 0;
+    double4 f = make_double4(0, 0, 0, 0);
+    int seg = 0;
+    if (a < S.nfw) {
+      f = S.fw64[a];
+      double dx = cx - f.x, dy = cy - f.y, dz = cz - f.z;
+      dx -= Lx * rgpu_nint(dx * ix);
+      dy -= Ly * rgpu_nint(dy * iy);
+      dz -= Lz * rgpu_nint(dz * iz);
+      keep = dx * dx + dy * dy + dz * dz < rcut2;
+      while (seg + 1 < S.nseg && a >= S.seg_start[seg + 1]) seg++;
+    }
+    unsigned m = __ballot_sync(RGPU_FULL, keep);
+    if (lane == 0) wcount[w] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = 0;
+      for (int q = 0; q < GRID_THREADS / 32; q++) { int c = wcount[q]; wcount[q] = s; s += c; }
+      nsel = s;
+    }
+    __syncthreads();
+    if (keep) {
+      int pos = wcount[w] + __popc(m & ((1u << lane) - 1u));
+      fwc[pos] = f;
+      segc[pos] = seg;
+    }
+    __syncthreads();
+    if (valid) {
+      for (int q = 0; q < nsel; q++) {
+        const double4 g = fwc[q];
+        double dx = px - g.x, dy = py - g.y, dz = pz - g.z;
+        dx -= Lx * rgpu_nint(dx * ix);
+        dy -= Ly * rgpu_nint(dy * iy);
+        dz -= Lz * rgpu_nint(dz * iz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < S.rc2) {
+          const RgpuLJ P = gp.lj[segc[q]];
+          const double eps = 0.25 * P.eps4;
+          double r3 = P.sig2 / r2;
+          r3 = r3 * r3 * r3;
+          const double U = 4.0 * eps * (r3 * (r3 - 1.0)) - P.shift;
+          const double DF = 24.0 * eps * (r3 * (1.0 - 2.0 * r3)) / r2;
+          const double DDF = 96.0 * eps * (r3 * (7.0 * r3 - 2.0)) / (r2 * r2);
+          const double DDDF = 384.0 * eps * (r3 * (5.0 - 28.0 * r3)) / (r2 * r2 * r2 * r2);
+          o[0] += U;
+          o[1] += dx * DF;
+          o[2] += dy * DF;
+          o[3] += dz * DF;
+          o[4] += DDF * dx * dy;
+          o[5] += DDF * dx * dz;
+          o[6] += DDF * dy * dz;
+          o[7] += DDDF * dx * dy * dz;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!valid) return;
+  /* cap, src/grids.c:546-563 */
+  if (o[0] > S.overlap) {
+    o[0] = 2.0 * S.overlap;
+    for (int c = 1; c <= 3; c++) {
+      if (o[c] > S.overlap) o[c] = S.overlap;
+      if (o[c] < -S.overlap) o[c] = -S.overlap;
+    }
+    o[4] = o[5] = o[6] = o[7] = 0.0;
+  }
+  const double dx = gp.delta[0], dy = gp.delta[1], dz = gp.delta[2];
+  float4 v0 = make_float4((float)o[0], (float)o[1] * (float)dx, (float)o[2] * (float)dy, (float)o[3] * (float)dz);
+  float4 v1 = make_float4((float)o[4] * (float)(dx * dy), (float)o[5] * (float)(dx * dz),
+                          (float)o[6] * (float)(dy * dz), (float)o[7] * (float)(dx * dy * dz));
+  float4 *dst = (float4 *)(grid + (((size_t)i * ny + j) * nz + k) * 8);
+  dst[0] = v0;
+  dst[1] = v1;
+}
+
+/* lj[s]: LJ parameters of the probe pseudo-atom with framework segment s */
+cudaError_t rgpu_grid_build_launch_lj(const RgpuSys *d_sys, const RgpuLJ *lj, const int npts[3], const double size[3],
+                                      const double shift[3], float *d_grid, cudaStream_t st)
+{
+  GridParams gp;
+  for (int c = 0; c < 3; c++) {
+    gp.npts[c] = npts[c];
+    gp.size[c] = size[c];
+    gp.shift[c] = shift[c];
+    gp.delta[c] = size[c] / (double)npts[c];
+  }
+  for (int s = 0; s < RGPU_MAX_FWTYPES; s++) gp.lj[s] = lj[s];
+  const int nx = npts[0] + 1, ny = npts[1] + 1, nz = npts[2] + 1;
+  const long long blocks = (long long)((nx + GRID_TX - 1) / GRID_TX) * ((ny + GRID_TY - 1) / GRID_TY) *
+                           ((nz + GRID_TZ - 1) / GRID_TZ);
+  if (blocks > 2147483647LL) return cudaErrorInvalidValue;
+  k_grid_build<<<(unsigned)blocks, GRID_THREADS, 0, st>>>(d_sys, gp, d_grid);
+  return cudaGetLastError();
+}
+
+/* Cubic Hermite basis on [0,1]: {p0, p1, slope0, slope1} */
+__device__ __forceinline__ void hermite(double t, double *h)
+{
+  const double t2 = t * t, t3 = t2 * t;
+  h[0] = 1.0 - 3.0 * t2 + 2.0 * t3;
+  h[1] = 3.0 * t2 - 2.0 * t3;
+  h[2] = t - 2.0 * t2 + t3;
+  h[3] = -t2 + t3;
+}
+
+struct InterpParams {
+  int npts[3];
+  double size[3], shift[3], cell[3];
+};
+
+__global__ void k_grid_interp(const float *grid, InterpParams ip, int n, const double *xyz, double *out)
+{
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int ny = ip.npts[1] + 1, nz = ip.npts[2] + 1;
+  double r[3];
+  int i0[3];
+  for (int c = 0; c < 3; c++) {
+    double p = xyz[3 * q + c];
+    p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
+    if (p < 0.0) p += ip.cell[c];
+    const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
+    i0[c] = (int)s;
+    r[c] = s - i0[c];
+  }
+  float v[8][8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+    const float4 *src = (const float4 *)(grid + (((size_t)(i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz)) * 8);
+    float4 a = __ldg(src), b = __ldg(src + 1);
+    v[c][0] = a.x; v[c][1] = a.y; v[c][2] = a.z; v[c][3] = a.w;
+    v[c][4] = b.x; v[c][5] = b.y; v[c][6] = b.z; v[c][7] = b.w;
+  }
+  /* cap, src/grids.c:1058-1060 */
+  for (int c = 0; c < 8; c++)
+    if (v[c][0] > 1e10f) { out[q] = 1e8; return; }
+  double hx[4], hy[4], hz[4];
+  hermite(r[0], hx);
+  hermite(r[1], hy);
+  hermite(r[2], hz);
+  /* stored value index for derivative order (ox, oy, oz) */
+  const int idx[2][2][2] = {{{0, 3}, {2, 6}}, {{1, 5}, {4, 7}}};
+  double val = 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+#pragma unroll
+    for (int ox = 0; ox < 2; ox++)
+#pragma unroll
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int oz = 0; oz < 2; oz++)
+          val += (double)v[c][idx[ox][oy][oz]] * hx[2 * ox + dx] * hy[2 * oy + dy] * hz[2 * oz + dz];
+  }
+  out[q] = val;
+}
+
+cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], const double size[3],
+                                    const double shift[3], const double cell[3], int n, const double *d_xyz,
+                                    double *d_out, cudaStream_t st)
+{
+  InterpParams ip;
+  for (int c = 0; c < 3; c++) {
+    ip.npts[c] = npts[c];
+    ip.size[c] = size[c];
+    ip.shift[c] = shift[c];
+    ip.cell[c] = cell[c];
+  }
+  if (n <= 0) return cudaSuccess;
+  k_grid_interp<<<(n + 255) / 256, 256, 0, st>>>(d_grid, ip, n, d_xyz, d_out);
+  return cudaGetLastError();
+}

@@ -1,0 +1,578 @@
+/* Device building blocks of the B200 GCMC energy path.
+ *
+ * Shared by the per-call entry points (capi.cu) and the persistent batched
+ * engine (engine.cu). Two precisions are instantiated from one template:
+ *   MIXED = false : FP64 everywhere (the plain path; parity 1e-9 relative);
+ *   MIXED = true  : FP32 pair terms and exp(ik.r) products on 32-bit
+ *                   fixed-point coordinates, FP32 per-warp sums, FP64 per-move
+ *                   sums, FP64 structure factors, totals and acceptance.
+ */
+#ifndef RGPU_DEVICE_CUH
+#define RGPU_DEVICE_CUH
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "erfc_fit.h"
+#include "rgpu_types.h"
+
+#define RGPU_FULL 0xffffffffu
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+ * easy as 1, 2, 3", SC'11). One uniform double in [0,1) per
+ * (seed, system, step, slot): the block counter is (step lo, step hi,
+ * slot/2, system), each half of the 128-bit output gives 53 bits. Every
+ * thread can draw any slot, so no random state is shared or carried. */
+__host__ __device__ inline void rgpu_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                            uint32_t k0, uint32_t k1, uint32_t out[4])
+{
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    uint32_t n1 = (uint32_t)p1;
+    uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    uint32_t n3 = (uint32_t)p0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__host__ __device__ inline double rgpu_uniform(uint64_t seed, uint32_t sys, uint64_t step, uint32_t slot)
+{
+  uint32_t o[4];
+  rgpu_philox((uint32_t)step, (uint32_t)(step >> 32), slot >> 1, sys, (uint32_t)seed,
+              (uint32_t)(seed >> 32), o);
+  uint32_t hi = (slot & 1) ? o[2] : o[0];
+  uint32_t lo = (slot & 1) ? o[3] : o[1];
+  uint64_t x = ((uint64_t)hi << 21) ^ (uint64_t)(lo >> 11);
+  return (double)x * (1.0 / 9007199254740992.0);
+}
+
+/* random-draw slots of one MC step (the oracle uses the same numbering) */
+enum {
+  SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
+  SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16, SLOT_ORIENT_SELECT = 63, SLOT_ORIENT = 64
+};
+
+/* ------------------------------------------------------------------------ */
+/* geometry */
+
+/* NINT of src/utils.h:60 */
+__device__ __forceinline__ double rgpu_nint(double x) { return (double)(int)(x >= 0.0 ? x + 0.5 : x - 0.5); }
+
+__host__ __device__ inline int rgpu_to_fix(double x, double inv_l)
+{
+  double f = x * inv_l;
+  f -= floor(f);
+  long long v = (long long)llrint(f * 4294967296.0);
+  return (int)(uint32_t)(v & 0xffffffffLL);
+}
+
+/* A bead position under evaluation. `atom` is the index of the bead in the
+ * adsorbate molecule (selects pseudo-atom type and charge). */
+struct BeadPos {
+  double x, y, z;
+  int xi, yi, zi;
+  int atom;
+  int excl;       /* adsorbate molecule left out of the sums (-1: none) */
+  int pad;
+};
+
+__device__ __forceinline__ void bead_set(BeadPos &b, const RgpuSys &S, double x, double y, double z, int atom,
+                                         int excl)
+{
+  b.x = x; b.y = y; b.z = z;
+  b.xi = rgpu_to_fix(x, S.inv_box[0]);
+  b.yi = rgpu_to_fix(y, S.inv_box[1]);
+  b.zi = rgpu_to_fix(z, S.inv_box[2]);
+  b.atom = atom;
+  b.excl = excl;
+}
+
+/* adsorbate atom record: position + tag = molecule*16 + atom index */
+struct AdsRec64 { double x, y, z; long long tag; };
+
+/* ------------------------------------------------------------------------ */
+/* pair terms */
+
+/* FP32 real-space Ewald kernel erfc(alpha r)/r * K qa qb with the fitted
+ * erfc of erfc_fit.h; rinv = 1/r */
+__device__ __forceinline__ float rgpu_erfc_f(float x)
+{
+  float t = __fdividef(1.0f, fmaf(RGPU_ERFC_P, x, 1.0f));
+  float p = RGPU_ERFC_C8;
+  p = fmaf(p, t, RGPU_ERFC_C7);
+  p = fmaf(p, t, RGPU_ERFC_C6);
+  p = fmaf(p, t, RGPU_ERFC_C5);
+  p = fmaf(p, t, RGPU_ERFC_C4);
+  p = fmaf(p, t, RGPU_ERFC_C3);
+  p = fmaf(p, t, RGPU_ERFC_C2);
+  p = fmaf(p, t, RGPU_ERFC_C1);
+  p = fmaf(p, t, RGPU_ERFC_C0);
+  /* exp(-x^2) = 2^(-x^2 log2 e) */
+  float e = exp2f(-x * x * 1.4426950408889634f);
+  return p * e;
+}
+
+/* ------------------------------------------------------------------------ */
+/* reductions */
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(RGPU_FULL, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(RGPU_FULL, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_or(int v)
+{
+  return __any_sync(RGPU_FULL, v) ? 1 : 0;
+}
+
+/* block-wide sum of two doubles; `red` holds >= 2*32 doubles; every thread
+ * returns the totals. Contains __syncthreads: call from all threads. */
+__device__ inline void block_sum2(double &a, double &b, double *red)
+{
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if (lane == 0) { red[2 * w] = a; red[2 * w + 1] = b; }
+  __syncthreads();
+  if (w == 0) {
+    a = lane < nw ? red[2 * lane] : 0.0;
+    b = lane < nw ? red[2 * lane + 1] : 0.0;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) { red[64] = a; red[65] = b; }
+  }
+  __syncthreads();
+  a = red[64];
+  b = red[65];
+  __syncthreads();
+}
+
+/* ------------------------------------------------------------------------ */
+/* Batched bead energies.
+ *
+ * For P bead positions, sums over the framework and over the adsorbate atoms
+ * not in the bead's own excluded molecule (BeadPos::excl):
+ *   res[p] = {host VDW, host real-space charge, adsorbate VDW, adsorbate real}
+ * (CalculateFrameworkVDWEnergyAtPosition src/framework_energy.c:60,
+ *  CalculateFrameworkChargeEnergyAtPosition :176,
+ *  CalculateInterVDWEnergyAdsorbateAtPosition src/inter_energy.c:321,
+ *  CalculateInterChargeEnergyAdsorbateAtPosition :393). For p < pair_check,
+ * ovf[p] = 1 when any single pair energy reaches EnergyOverlapCriteria (the
+ * early-out of the *EnergyDifference routines, e.g.
+ * src/framework_energy.c:4988-4990).
+ *
+ * Work split: the (position, atom-range) units are spread over the warps;
+ * lanes stride the atoms of a unit (consecutive records, conflict-free shared
+ * loads); a unit's lane sums are warp-reduced and parked in `unit_buf`; the
+ * per-position totals are then formed in FP64.
+ */
+struct EvalScratch {
+  double *uv;     /* [max units] */
+  double *uc;
+  int *uo;
+  int *upos;      /* position of the unit */
+};
+
+struct EvalPlan {
+  int cf, ca;     /* framework / adsorbate chunks per position */
+  int nunits;
+};
+
+__device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwarps, int max_units)
+{
+  EvalPlan pl;
+  int target = 4 * nwarps;
+  int cf = (target + P - 1) / P;
+  int maxcf = (nfw + 63) / 64;
+  if (cf > maxcf) cf = maxcf;
+  if (cf < 1) cf = 1;
+  int ca = 0;
+  if (nads > 0) {
+    ca = (int)((long long)cf * nads / (nfw > 0 ? nfw : 1));
+    int maxca = (nads + 63) / 64;
+    if (ca > maxca) ca = maxca;
+    if (ca < 1) ca = 1;
+  }
+  while (P * (cf + ca) > max_units && cf > 1) cf--;
+  while (P * (cf + ca) > max_units && ca > 1) ca--;
+  pl.cf = cf;
+  pl.ca = ca;
+  pl.nunits = P * (cf + ca);
+  return pl;
+}
+
+/* one unit of framework work, FP32 path */
+__device__ __forceinline__ void unit_fw_mixed(const RgpuSys &S, const int4 *fw, const BeadPos &b, int lo,
+                                              int hi, bool check, float &av, float &ac, int &ov)
+{
+  const int lane = threadIdx.x & 31;
+  const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
+  const float rc2 = S.rc2f;
+  const float thr = (float)S.overlap;
+  const float qa = S.mol_qf[b.atom] * S.coulombf;
+  const bool charged = S.fw_charged && qa != 0.0f;
+  const float alpha = S.alphaf;
+  for (int s = 0; s < S.nseg; s++) {
+    int a0 = max(lo, S.seg_start[s]), a1 = min(hi, S.seg_start[s + 1]);
+    if (a0 >= a1) continue;
+    const RgpuLJf P = S.ljf_bf[b.atom][s];
+    for (int j = a0 + lane; j < a1; j += 32) {
+      int4 f = fw[j];
+      float dx = __int2float_rn(f.x - b.xi) * sx;
+      float dy = __int2float_rn(f.y - b.yi) * sy;
+      float dz = __int2float_rn(f.z - b.zi) * sz;
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2 < rc2) {
+        float ri = rsqrtf(r2);
+        ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);      /* one Newton step */
+        float ir2 = ri * ri;
+        float s6 = P.sig2 * ir2;
+        s6 = s6 * s6 * s6;
+        float u = fmaf(P.eps4 * s6, s6 - 1.0f, -P.shift);
+        av += u;
+        if (check && u >= thr) ov = 1;
+        if (charged) {
+          float r = r2 * ri;
+          float uc = qa * __int_as_float(f.w) * rgpu_erfc_f(alpha * r) * ri;
+          ac += uc;
+          if (check && uc >= thr) ov = 1;
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw, const BeadPos &b, int lo,
+                                             int hi, bool check, double &av, double &ac, int &ov)
+{
+  const int lane = threadIdx.x & 31;
+  const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
+  const double ix = S.inv_box[0], iy = S.inv_box[1], iz = S.inv_box[2];
+  const double rc2 = S.rc2, thr = S.overlap;
+  const double qa = S.mol_q[b.atom] * S.coulomb;
+  const bool charged = S.fw_charged && qa != 0.0;
+  const double alpha = S.alpha;
+  for (int s = 0; s < S.nseg; s++) {
+    int a0 = max(lo, S.seg_start[s]), a1 = min(hi, S.seg_start[s + 1]);
+    if (a0 >= a1) continue;
+    const RgpuLJ P = S.lj_bf[b.atom][s];
+    for (int j = a0 + lane; j < a1; j += 32) {
+      double4 f = fw[j];
+      double dx = b.x - f.x, dy = b.y - f.y, dz = b.z - f.z;
+      dx -= Lx * rgpu_nint(dx * ix);
+      dy -= Ly * rgpu_nint(dy * iy);
+      dz -= Lz * rgpu_nint(dz * iz);
+      double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < rc2) {
+        double s6 = P.sig2 / r2;
+        s6 = s6 * s6 * s6;
+        double u = P.eps4 * (s6 * (s6 - 1.0)) - P.shift;
+        av += u;
+        if (check && u >= thr) ov = 1;
+        if (charged) {
+          double r = sqrt(r2);
+          double uc = qa * f.w * (erfc(alpha * r) / r);
+          ac += uc;
+          if (check && uc >= thr) ov = 1;
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo,
+                                               int hi, int exclude, bool check, float &av, float &ac, int &ov)
+{
+  const int lane = threadIdx.x & 31;
+  const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
+  const float rc2 = S.rc2f;
+  const float thr = (float)S.overlap;
+  const float qa = S.mol_qf[b.atom] * S.coulombf;
+  const bool charged = S.mol_charged && qa != 0.0f;
+  const float alpha = S.alphaf;
+  for (int j = lo + lane; j < hi; j += 32) {
+    int4 f = ads[j];
+    if ((f.w >> 4) == exclude) continue;
+    int at = f.w & 15;
+    float dx = __int2float_rn(f.x - b.xi) * sx;
+    float dy = __int2float_rn(f.y - b.yi) * sy;
+    float dz = __int2float_rn(f.z - b.zi) * sz;
+    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (r2 < rc2) {
+      const RgpuLJf P = S.ljf_bb[b.atom][at];
+      float ri = rsqrtf(r2);
+      ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);
+      float ir2 = ri * ri;
+      float s6 = P.sig2 * ir2;
+      s6 = s6 * s6 * s6;
+      float u = fmaf(P.eps4 * s6, s6 - 1.0f, -P.shift);
+      av += u;
+      if (check && u >= thr) ov = 1;
+      float qb = S.mol_qf[at];
+      if (charged && qb != 0.0f) {
+        float r = r2 * ri;
+        float uc = qa * qb * rgpu_erfc_f(alpha * r) * ri;
+        ac += uc;
+        if (check && uc >= thr) ov = 1;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *ads, const BeadPos &b, int lo,
+                                              int hi, int exclude, bool check, double &av, double &ac, int &ov)
+{
+  const int lane = threadIdx.x & 31;
+  const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
+  const double ix = S.inv_box[0], iy = S.inv_box[1], iz = S.inv_box[2];
+  const double rc2 = S.rc2, thr = S.overlap;
+  const double qa = S.mol_q[b.atom] * S.coulomb;
+  const bool charged = S.mol_charged && qa != 0.0;
+  const double alpha = S.alpha;
+  for (int j = lo + lane; j < hi; j += 32) {
+    AdsRec64 f = ads[j];
+    int tag = (int)f.tag;
+    if ((tag >> 4) == exclude) continue;
+    int at = tag & 15;
+    double dx = b.x - f.x, dy = b.y - f.y, dz = b.z - f.z;
+    dx -= Lx * rgpu_nint(dx * ix);
+    dy -= Ly * rgpu_nint(dy * iy);
+    dz -= Lz * rgpu_nint(dz * iz);
+    double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 < rc2) {
+      const RgpuLJ P = S.lj_bb[b.atom][at];
+      double s6 = P.sig2 / r2;
+      s6 = s6 * s6 * s6;
+      double u = P.eps4 * (s6 * (s6 - 1.0)) - P.shift;
+      av += u;
+      if (check && u >= thr) ov = 1;
+      double qb = S.mol_q[at];
+      if (charged && qb != 0.0) {
+        double r = sqrt(r2);
+        double uc = qa * qb * (erfc(alpha * r) / r);
+        ac += uc;
+        if (check && uc >= thr) ov = 1;
+      }
+    }
+  }
+}
+
+/* Evaluates P bead positions. All threads of the block must call it.
+ * fw: int4* (MIXED) or double4* (FP64); ads: int4* or AdsRec64*. */
+template <bool MIXED>
+__device__ void eval_positions(const RgpuSys &S, const void *fw, const void *ads, int nads, const BeadPos *pos,
+                               int P, int pair_check, double (*res)[4], int *ovf,
+                               EvalScratch sc, int max_units)
+{
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const EvalPlan pl = eval_plan(P, S.nfw, nads, nw, max_units);
+  const int per = pl.cf + pl.ca;
+  for (int u = w; u < pl.nunits; u += nw) {
+    const int p = u / per, c = u - p * per;
+    const BeadPos b = pos[p];
+    const bool check = p < pair_check;
+    int ov = 0;
+    double v, q;
+    if (MIXED) {
+      float av = 0.0f, ac = 0.0f;
+      if (c < pl.cf) {
+        int lo = (int)((long long)S.nfw * c / pl.cf), hi = (int)((long long)S.nfw * (c + 1) / pl.cf);
+        unit_fw_mixed(S, (const int4 *)fw, b, lo, hi, check, av, ac, ov);
+      } else {
+        int cc = c - pl.cf;
+        int lo = (int)((long long)nads * cc / pl.ca), hi = (int)((long long)nads * (cc + 1) / pl.ca);
+        unit_ads_mixed(S, (const int4 *)ads, b, lo, hi, b.excl, check, av, ac, ov);
+      }
+      v = (double)warp_sum(av);
+      q = (double)warp_sum(ac);
+    } else {
+      double av = 0.0, ac = 0.0;
+      if (c < pl.cf) {
+        int lo = (int)((long long)S.nfw * c / pl.cf), hi = (int)((long long)S.nfw * (c + 1) / pl.cf);
+        unit_fw_fp64(S, (const double4 *)fw, b, lo, hi, check, av, ac, ov);
+      } else {
+        int cc = c - pl.cf;
+        int lo = (int)((long long)nads * cc / pl.ca), hi = (int)((long long)nads * (cc + 1) / pl.ca);
+        unit_ads_fp64(S, (const AdsRec64 *)ads, b, lo, hi, b.excl, check, av, ac, ov);
+      }
+      v = warp_sum(av);
+      q = warp_sum(ac);
+    }
+    ov = warp_or(ov);
+    if (lane == 0) {
+      sc.uv[u] = v;
+      sc.uc[u] = q;
+      sc.uo[u] = ov;
+    }
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    double hv = 0.0, hc = 0.0, av = 0.0, ac = 0.0;
+    int ov = 0;
+    for (int c = 0; c < per; c++) {
+      int u = p * per + c;
+      if (c < pl.cf) { hv += sc.uv[u]; hc += sc.uc[u]; }
+      else { av += sc.uv[u]; ac += sc.uc[u]; }
+      ov |= sc.uo[u];
+    }
+    res[p][0] = hv; res[p][1] = hc; res[p][2] = av; res[p][3] = ac;
+    ovf[p] = ov;
+  }
+  __syncthreads();
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ewald Fourier difference (CalculateEwaldFourierAdsorbate,
+ * src/ewald.c:6859-7567, charge sites only).
+ *
+ * Sites carry a signed charge (+q for new, -q for old positions). Per site
+ * and axis, exp(i 2 pi k s) is tabulated for k in [-kmax, kmax]; on the mixed
+ * path the angle k*s is reduced exactly in 32-bit integer arithmetic on the
+ * fixed-point coordinate, so each phase has FP32 accuracy at every k. */
+struct EwSite { BeadPos b; double q; };
+
+template <bool MIXED>
+struct PhaseT { typedef double2 T; };
+template <>
+struct PhaseT<true> { typedef float2 T; };
+
+/* table layout: tab[(site*3 + axis)*KW + (k + kmax)], KW = 2*kmaxall+1 */
+template <bool MIXED>
+__device__ void ewald_phases(const RgpuSys &S, const EwSite *sites, int ns, typename PhaseT<MIXED>::T *tab, int kw)
+{
+  const int km = (kw - 1) / 2;
+  const int n = ns * 3 * kw;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int kk = i % kw - km;
+    int sa = i / kw;
+    int axis = sa % 3, s = sa / 3;
+    const BeadPos &b = sites[s].b;
+    if (MIXED) {
+      int xi = axis == 0 ? b.xi : (axis == 1 ? b.yi : b.zi);
+      int ang = (int)((unsigned)kk * (unsigned)xi);          /* k*s mod 1 turn, exact */
+      float turns = __int2float_rn(ang) * 2.3283064365386963e-10f;   /* 2^-32 */
+      float sn, cs;
+      sincospif(2.0f * turns, &sn, &cs);
+      ((float2 *)tab)[i] = make_float2(cs, sn);
+    } else {
+      double x = axis == 0 ? b.x : (axis == 1 ? b.y : b.z);
+      double f = x * S.inv_box[axis];
+      double sn, cs;
+      sincospi(2.0 * (double)kk * f, &sn, &cs);
+      ((double2 *)tab)[i] = make_double2(cs, sn);
+    }
+  }
+}
+
+/* delta S(k) for wave vector k from the tables */
+template <bool MIXED>
+__device__ __forceinline__ double2 ewald_dS(const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
+                                            int ns, char4 kv)
+{
+  const int km = (kw - 1) / 2;
+  if (MIXED) {
+    float re = 0.0f, im = 0.0f;
+    const float2 *t = (const float2 *)tab;
+    for (int s = 0; s < ns; s++) {
+      float2 a = t[(s * 3 + 0) * kw + kv.x + km];
+      float2 b = t[(s * 3 + 1) * kw + kv.y + km];
+      float2 c = t[(s * 3 + 2) * kw + kv.z + km];
+      float xr = a.x * b.x - a.y * b.y, xi = a.x * b.y + a.y * b.x;
+      float er = xr * c.x - xi * c.y, ei = xr * c.y + xi * c.x;
+      float q = (float)sites[s].q;
+      re = fmaf(q, er, re);
+      im = fmaf(q, ei, im);
+    }
+    return make_double2((double)re, (double)im);
+  } else {
+    double re = 0.0, im = 0.0;
+    const double2 *t = (const double2 *)tab;
+    for (int s = 0; s < ns; s++) {
+      double2 a = t[(s * 3 + 0) * kw + kv.x + km];
+      double2 b = t[(s * 3 + 1) * kw + kv.y + km];
+      double2 c = t[(s * 3 + 2) * kw + kv.z + km];
+      double xr = a.x * b.x - a.y * b.y, xi = a.x * b.y + a.y * b.x;
+      double er = xr * c.x - xi * c.y, ei = xr * c.y + xi * c.x;
+      re += sites[s].q * er;
+      im += sites[s].q * ei;
+    }
+    return make_double2(re, im);
+  }
+}
+
+/* Sum over k of the energy change; every thread returns {e_ads, e_host}:
+ * e_ads = sum kf (|S+dS|^2 - |S|^2), e_host = sum kf Re(S_fw^* dS). */
+template <bool MIXED>
+__device__ void ewald_energy_sum(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
+                                 const EwSite *sites, int ns, double &e_ads, double &e_host, double *red)
+{
+  double ea = 0.0, eh = 0.0;
+  for (int k = threadIdx.x; k < S.nk; k += blockDim.x) {
+    double2 d = ewald_dS<MIXED>(tab, kw, sites, ns, S.kvec[k]);
+    double2 so = S.sk_ads[k];
+    double2 sf = S.sk_fw[k];
+    double kf = S.kfactor[k];
+    ea += kf * (2.0 * (so.x * d.x + so.y * d.y) + d.x * d.x + d.y * d.y);
+    eh += kf * (sf.x * d.x + sf.y * d.y);
+  }
+  block_sum2(ea, eh, red);
+  e_ads = ea;
+  e_host = eh;
+}
+
+/* S_ads(k) += dS(k) (AcceptEwaldAdsorbateMove, src/ewald.c:11732). The same
+ * ewald_dS call as in the energy sum, so the stored sums are those the
+ * accepted energy was computed with. */
+template <bool MIXED>
+__device__ void ewald_apply(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
+                            int ns)
+{
+  for (int k = threadIdx.x; k < S.nk; k += blockDim.x) {
+    double2 d = ewald_dS<MIXED>(tab, kw, sites, ns, S.kvec[k]);
+    double2 so = S.sk_ads[k];
+    S.sk_ads[k] = make_double2(so.x + d.x, so.y + d.y);
+  }
+}
+
+/* intramolecular exclusion energy K qa qb erf(alpha r)/r over the charged
+ * pairs of one molecule (src/ewald.c:7312-7330), FP64 */
+__device__ inline double ewald_exclusion(const RgpuSys &S, const double (*xyz)[3])
+{
+  double e = 0.0;
+  for (int a = 0; a < S.natom - 1; a++)
+    for (int b = a + 1; b < S.natom; b++) {
+      if (S.mol_q[a] == 0.0 || S.mol_q[b] == 0.0) continue;
+      double dx = xyz[a][0] - xyz[b][0], dy = xyz[a][1] - xyz[b][1], dz = xyz[a][2] - xyz[b][2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      e += S.coulomb * S.mol_q[a] * S.mol_q[b] * erf(S.alpha * r) / r;
+    }
+  return e;
+}
+
+/* complete dU_ads / dU_host of src/ewald.c:7539-7565 for a change of
+ * (nnew - nold) molecules, given the k-sums and the exclusion energies */
+__device__ inline void ewald_finish(const RgpuSys &S, double e_ads, double e_host, double excl_new,
+                                    double excl_old, int dn, double net_ads, double &d_ads, double &d_host)
+{
+  double dq = dn * S.mol_charge;
+  d_ads = e_ads - (excl_new - excl_old) - dn * S.self_mol;
+  d_ads += S.uion * (net_ads + dq) * (net_ads + dq) - S.uion * net_ads * net_ads;
+  d_host = 2.0 * e_host + 2.0 * S.uion * S.net_fw * dq;
+}
+
+#endif

@@ -1,0 +1,30 @@
+/* Internal launch interface between capi.cu and the kernel files. */
+#ifndef RGPU_ENGINE_H
+#define RGPU_ENGINE_H
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "rgpu_types.h"
+
+size_t rgpu_engine_smem_bytes(int mixed, int nfw_smem, int max_ads_atoms, int kw);
+cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
+                               int max_ads_atoms, int nfw_smem, int threads, int blocks, cudaStream_t st);
+cudaError_t rgpu_point_energies_launch(int mixed, const RgpuSys *d_sys, const void *d_ads, int nads,
+                                       const double *d_xyz, const int *d_atom, const int *d_excl, int P,
+                                       int pair_check, double *d_out, int *d_ov, cudaStream_t st);
+cudaError_t rgpu_ewald_delta_launch(int mixed, const RgpuSys *d_sys, const double *d_xyz, const double *d_q, int ns,
+                                    double2 *d_ds, double *d_out, int kw, cudaStream_t st);
+cudaError_t rgpu_ewald_accept_launch(const RgpuSys *d_sys, const double2 *d_ds, int nk, cudaStream_t st);
+cudaError_t rgpu_structure_factor_launch(const RgpuSys *d_sys, const double *d_xyz, const double *d_q, int n,
+                                         int nk, double2 *d_sk, cudaStream_t st);
+cudaError_t rgpu_records_launch(const RgpuSys *d_sys, int nads, int4 *d_rec32, void *d_rec64, cudaStream_t st);
+
+/* grids (grid.cu) */
+cudaError_t rgpu_grid_build_launch_lj(const RgpuSys *d_sys, const RgpuLJ *lj, const int npts[3],
+                                      const double size[3], const double shift[3], float *d_grid, cudaStream_t st);
+cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], const double size[3],
+                                    const double shift[3], const double cell[3], int n, const double *d_xyz,
+                                    double *d_out, cudaStream_t st);
+
+#endif

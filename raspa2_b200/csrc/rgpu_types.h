@@ -1,0 +1,111 @@
+/* Host/device shared layouts of the B200 GCMC energy path.
+ *
+ * One `RgpuSys` describes one simulation box: geometry, force-field tables
+ * resolved for the adsorbate component, Ewald constants, MC move parameters
+ * and the device pointers of the box's state. It is built on the host
+ * (capi.cu) and copied to device memory; kernels copy it into shared memory.
+ *
+ * Positions on the mixed-precision path are 32-bit fixed-point fractional
+ * coordinates: x_fix = round(frac(x / L) * 2^32) as a signed int. The
+ * difference of two such ints, taken with wrap-around, is the minimum-image
+ * separation in units of L / 2^32, so the periodic boundary condition of
+ * ApplyBoundaryCondition (src/potentials.h:241-245) costs one integer
+ * subtraction and the separation keeps 24 significant bits relative to its
+ * own length rather than to the box length. (Valid for orthorhombic boxes at
+ * least twice the cut-off, which the reference also requires.)
+ */
+#ifndef RGPU_TYPES_H
+#define RGPU_TYPES_H
+
+#include <stdint.h>
+
+#define RGPU_MAX_ATOMS 8       /* atoms per adsorbate molecule */
+#define RGPU_MAX_FWTYPES 4     /* framework pseudo-atom types */
+#define RGPU_MAX_TRIALS 16     /* CBMC trial positions per step */
+#define RGPU_MAX_POS 64        /* bead positions evaluated in one batch */
+
+/* per-system counters */
+enum {
+  RGPU_CNT_ATTEMPT = 0,  /* [0..3]: translation, rotation, insertion, deletion */
+  RGPU_CNT_ACCEPT = 4,   /* [4..7] */
+  RGPU_CNT_MOVES = 8,    /* counted MC moves */
+  RGPU_CNT_OVERLAP = 9,  /* proposals rejected by overlap */
+  RGPU_NCNT = 12
+};
+
+/* per-system running energies (internal units, FP64) */
+enum {
+  RGPU_E_HOST_VDW = 0, RGPU_E_ADS_VDW = 1, RGPU_E_HOST_REAL = 2, RGPU_E_ADS_REAL = 3,
+  RGPU_E_HOST_FOURIER = 4, RGPU_E_ADS_FOURIER = 5, RGPU_NE = 8
+};
+
+/* status word bits */
+enum {
+  RGPU_OK = 0,
+  RGPU_ERR_MAXMOL = 1,      /* an insertion was refused for lack of molecule slots */
+  RGPU_ERR_NONFINITE = 2,   /* a non-finite energy reached an acceptance test */
+};
+
+typedef struct {
+  double eps4, sig2, shift;   /* 4*epsilon, sigma^2, U(rc) */
+} RgpuLJ;
+
+typedef struct {
+  float eps4, sig2, shift, pad;
+} RgpuLJf;
+
+typedef struct RgpuSys {
+  /* geometry */
+  double box[3], inv_box[3];
+  float fix_scale[3];         /* L / 2^32 per axis */
+  float rc2f;
+  double rc2;                 /* VDW and real-space cut-off squared (equal) */
+  double overlap;             /* EnergyOverlapCriteria */
+  double beta;
+  double coulomb, alpha;
+  float coulombf, alphaf;
+  /* framework, sorted by pseudo-atom type into segments */
+  int nfw;
+  int nseg;
+  int seg_start[RGPU_MAX_FWTYPES + 1];
+  int fw_charged;             /* any framework charge != 0 */
+  /* adsorbate component */
+  int natom, start_bead, maxmol;
+  int mol_charged;
+  double mol_q[RGPU_MAX_ATOMS];
+  float mol_qf[RGPU_MAX_ATOMS];
+  double mol_ref[RGPU_MAX_ATOMS][3];
+  RgpuLJ lj_bf[RGPU_MAX_ATOMS][RGPU_MAX_FWTYPES];   /* bead atom x framework segment */
+  RgpuLJ lj_bb[RGPU_MAX_ATOMS][RGPU_MAX_ATOMS];     /* bead atom x bead atom */
+  RgpuLJf ljf_bf[RGPU_MAX_ATOMS][RGPU_MAX_FWTYPES];
+  RgpuLJf ljf_bb[RGPU_MAX_ATOMS][RGPU_MAX_ATOMS];
+  /* Ewald (charges only) */
+  int ewald, nk;
+  int kmax[3];
+  double self_mol;            /* sum over the molecule's sites of K q^2 alpha / sqrt(pi) */
+  double excl_pref;           /* unused padding for alignment */
+  double uion, net_fw, mol_charge;
+  /* MC */
+  double cum[4];
+  double max_translation, max_rotation;
+  double fugacity_beta_v;     /* beta * f * V, ideal-gas Rosenbluth weight 1 */
+  int ntrial_first, ntrial;
+  uint64_t seed;
+  uint32_t sys_id;
+  int smem_fw;                /* framework staged in shared memory by the engine */
+  /* device pointers */
+  const double4 *fw64;        /* [nfw] x, y, z, q */
+  const int4 *fw32;           /* [nfw] fixed-point x, y, z, float bits of q */
+  const char4 *kvec;          /* [nk] */
+  const double *kfactor;      /* [nk] */
+  const double2 *sk_fw;       /* [nk] */
+  double2 *sk_ads;            /* [nk] */
+  double *ads_xyz;            /* [maxmol*natom*3] authoritative positions */
+  int *nmol;                  /* [1] */
+  double *energy;             /* [RGPU_NE] running totals */
+  unsigned long long *step;   /* [1] next step index */
+  long long *counters;        /* [RGPU_NCNT] */
+  int *status;                /* [1] */
+} RgpuSys;
+
+#endif

@@ -1,0 +1,277 @@
+"""ctypes binding of libraspa_gpu.so (include/raspa_gpu.h).
+
+The library is the product: there is no CPU fallback. Loading fails loudly
+when the shared object is missing or cannot be loaded, and creating a system
+fails when no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+from . import units
+from .systems import System, kvector_indices
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+RGPU_FP64 = 0
+RGPU_MIXED = 1
+
+EXPORTS = [
+    "rgpu_error_string", "rgpu_device_count", "rgpu_system_create", "rgpu_system_destroy",
+    "rgpu_set_adsorbates", "rgpu_get_adsorbates", "rgpu_update_molecule", "rgpu_insert_molecule",
+    "rgpu_remove_molecule", "rgpu_bead_energies", "rgpu_move_energy_difference",
+    "rgpu_ewald_fourier_difference", "rgpu_ewald_accept", "rgpu_total_energy", "rgpu_grid_build",
+    "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
+    "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy",
+]
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("box", C.c_double * 3), ("cutoff", C.c_double), ("beta", C.c_double),
+        ("coulomb", C.c_double), ("overlap", C.c_double),
+        ("nfw", C.c_int), ("fw_xyz", _dp), ("fw_type", _ip), ("fw_q", _dp),
+        ("ntypes", C.c_int), ("eps", _dp), ("sig2", _dp), ("shift", _dp),
+        ("natom", C.c_int), ("mol_type", _ip), ("mol_q", _dp), ("mol_ref", _dp),
+        ("start_bead", C.c_int), ("ewald", C.c_int), ("alpha", C.c_double),
+        ("kmax", C.c_int * 3), ("maxmol", C.c_int),
+        ("move_cum", C.c_double * 4), ("max_translation", C.c_double),
+        ("max_rotation", C.c_double), ("fugacity_beta_v", C.c_double),
+        ("ntrial_first", C.c_int), ("ntrial", C.c_int),
+        ("seed", C.c_uint64), ("stream_id", C.c_uint32),
+    ]
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_stale: bool = True):
+    """Loads libraspa_gpu.so (building it in-tree first if it is stale and
+    nvcc is available)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if build_if_stale and _build.stale():
+        try:
+            _build.build()
+        except Exception as e:  # no toolchain: only a prebuilt library can be used
+            if not os.path.exists(path):
+                raise NativeError(f"libraspa_gpu.so is missing and could not be built: {e}")
+    if not os.path.exists(path):
+        raise NativeError(f"libraspa_gpu.so not found at {path}")
+    L = C.CDLL(path)
+    L.rgpu_error_string.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = load().rgpu_error_string(rc)
+        raise NativeError(f"libraspa_gpu error {rc}: {msg.decode() if msg else ''}")
+
+
+def device_count() -> int:
+    return int(load().rgpu_device_count())
+
+
+def _arr(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class GpuSystem:
+    """One simulation box on the GPU (handle of rgpu_system)."""
+
+    def __init__(self, sysm: System, maxmol: int = 512, seed: int = 12345, stream_id: int = 0,
+                 max_translation: Optional[float] = None, max_rotation: Optional[float] = None):
+        L = load()
+        self.sysm = sysm
+        eps, sig2, shift = sysm.lj_tables()
+        pos, t, q = sysm.framework()
+        keep = []
+
+        def k(a, dt):
+            a = _arr(a, dt)
+            keep.append(a)
+            return a
+
+        d = SystemDesc()
+        d.box[:] = [float(x) for x in sysm.box]
+        d.cutoff = sysm.cutoff
+        d.beta = units.beta(sysm.temperature)
+        d.coulomb = units.COULOMBIC_CONVERSION_FACTOR
+        d.overlap = units.ENERGY_OVERLAP_CRITERIA
+        fwx = k(pos, np.float64); fwt = k(t, np.int32); fwq = k(q, np.float64)
+        d.nfw = len(fwt)
+        d.fw_xyz = fwx.ctypes.data_as(_dp); d.fw_type = fwt.ctypes.data_as(_ip); d.fw_q = fwq.ctypes.data_as(_dp)
+        e = k(eps, np.float64); s2 = k(sig2, np.float64); sh = k(shift, np.float64)
+        d.ntypes = e.shape[0]
+        d.eps = e.ctypes.data_as(_dp); d.sig2 = s2.ctypes.data_as(_dp); d.shift = sh.ctypes.data_as(_dp)
+        mt = k(sysm.molecule_types(), np.int32); mq = k(sysm.molecule.charges(), np.float64)
+        mr = k(sysm.molecule.positions, np.float64)
+        d.natom = len(mt)
+        d.mol_type = mt.ctypes.data_as(_ip); d.mol_q = mq.ctypes.data_as(_dp); d.mol_ref = mr.ctypes.data_as(_dp)
+        d.start_bead = sysm.molecule.starting_bead
+        d.ewald = 1 if sysm.ewald else 0
+        d.alpha = sysm.alpha
+        d.kmax[:] = list(sysm.kmax)
+        d.maxmol = maxmol
+        d.move_cum[:] = list(sysm.moves.cumulative())
+        d.max_translation = sysm.max_translation if max_translation is None else max_translation
+        d.max_rotation = (np.deg2rad(sysm.max_rotation_deg) if max_rotation is None else max_rotation)
+        d.fugacity_beta_v = (units.beta(sysm.temperature) * units.pressure_to_internal(sysm.pressure)
+                             * sysm.volume)
+        d.ntrial_first = sysm.trials_first_bead
+        d.ntrial = sysm.trials
+        d.seed = seed
+        d.stream_id = stream_id
+        self.natom = d.natom
+        self.maxmol = maxmol
+        h = C.c_void_p()
+        _check(L.rgpu_system_create(C.byref(h), C.byref(d)))
+        self.h = h
+        self.nk = len(kvector_indices(sysm.kmax)) if sysm.ewald else 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rgpu_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state ------------------------------------------------------------
+    def set_adsorbates(self, xyz):
+        xyz = _arr(np.asarray(xyz, float).reshape(-1, self.natom, 3), np.float64)
+        _check(load().rgpu_set_adsorbates(self.h, len(xyz), xyz.ctypes.data_as(_dp)))
+
+    def adsorbates(self) -> np.ndarray:
+        n = C.c_int()
+        _check(load().rgpu_get_adsorbates(self.h, C.byref(n), None, 0))
+        out = np.zeros((max(n.value, 1), self.natom, 3))
+        _check(load().rgpu_get_adsorbates(self.h, C.byref(n), out.ctypes.data_as(_dp), out.shape[0]))
+        return out[: n.value]
+
+    def update_molecule(self, m, xyz):
+        x = _arr(xyz, np.float64)
+        _check(load().rgpu_update_molecule(self.h, C.c_int(m), x.ctypes.data_as(_dp)))
+
+    def insert_molecule(self, xyz):
+        x = _arr(xyz, np.float64)
+        _check(load().rgpu_insert_molecule(self.h, x.ctypes.data_as(_dp)))
+
+    def remove_molecule(self, m):
+        _check(load().rgpu_remove_molecule(self.h, C.c_int(m)))
+
+    # ---- energies -----------------------------------------------------------
+    def bead_energies(self, xyz, atom, exclude, precision=RGPU_FP64) -> np.ndarray:
+        x = _arr(np.asarray(xyz, float).reshape(-1, 3), np.float64)
+        n = len(x)
+        a = _arr(np.broadcast_to(atom, (n,)), np.int32)
+        e = _arr(np.broadcast_to(exclude, (n,)), np.int32)
+        out = np.zeros((n, 4))
+        _check(load().rgpu_bead_energies(self.h, C.c_int(precision), C.c_int(n), x.ctypes.data_as(_dp),
+                                         a.ctypes.data_as(_ip), e.ctypes.data_as(_ip), out.ctypes.data_as(_dp)))
+        return out
+
+    def move_difference(self, m, new_xyz, precision=RGPU_FP64):
+        x = _arr(new_xyz, np.float64)
+        out = np.zeros(4)
+        ov = C.c_int()
+        _check(load().rgpu_move_energy_difference(self.h, C.c_int(precision), C.c_int(m), x.ctypes.data_as(_dp),
+                                                  out.ctypes.data_as(_dp), C.byref(ov)))
+        return bool(ov.value), out
+
+    def ewald_difference(self, old_mol=-1, new_xyz=None, precision=RGPU_FP64):
+        out = np.zeros(3)
+        x = None if new_xyz is None else _arr(new_xyz, np.float64)
+        _check(load().rgpu_ewald_fourier_difference(self.h, C.c_int(precision), C.c_int(old_mol),
+                                                    None if x is None else x.ctypes.data_as(_dp),
+                                                    out.ctypes.data_as(_dp)))
+        return out
+
+    def ewald_accept(self):
+        _check(load().rgpu_ewald_accept(self.h))
+
+    def total_energy(self) -> np.ndarray:
+        out = np.zeros(6)
+        _check(load().rgpu_total_energy(self.h, out.ctypes.data_as(_dp)))
+        return out
+
+    def state(self):
+        e = np.zeros(8)
+        c = np.zeros(12, np.int64)
+        n = C.c_int()
+        st = C.c_int()
+        step = C.c_ulonglong()
+        _check(load().rgpu_system_state(self.h, e.ctypes.data_as(_dp), c.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                        C.byref(n), C.byref(st), C.byref(step)))
+        return {"energy": e, "counters": c, "nmol": n.value, "status": st.value, "step": step.value}
+
+    def set_energy(self, e8):
+        e = _arr(np.resize(np.asarray(e8, float), 8), np.float64)
+        _check(load().rgpu_system_set_energy(self.h, e.ctypes.data_as(_dp)))
+
+    # ---- grids --------------------------------------------------------------
+    def grid_build(self, type_: int, npts, size, shift, d_grid_ptr: int):
+        n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64)
+        _check(load().rgpu_grid_build(self.h, C.c_int(type_), n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),
+                                      sh.ctypes.data_as(_dp), C.c_void_p(d_grid_ptr)))
+
+
+def grid_interpolate(d_grid_ptr: int, npts, size, shift, cell, xyz) -> np.ndarray:
+    n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64)
+    ce = _arr(cell, np.float64)
+    x = _arr(np.asarray(xyz, float).reshape(-1, 3), np.float64)
+    out = np.zeros(len(x))
+    _check(load().rgpu_grid_interpolate(C.c_void_p(d_grid_ptr), n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),
+                                        sh.ctypes.data_as(_dp), ce.ctypes.data_as(_dp), C.c_int(len(x)),
+                                        x.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
+    return out
+
+
+class Engine:
+    """Persistent batched engine over several GpuSystems (rgpu_engine)."""
+
+    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=256):
+        L = load()
+        arr = (C.c_void_p * len(systems))(*[s.h for s in systems])
+        h = C.c_void_p()
+        _check(L.rgpu_engine_create(C.byref(h), arr, C.c_int(len(systems)), C.c_int(precision), C.c_int(threads)))
+        self.h = h
+        self.systems = list(systems)
+
+    def run(self, nsteps: int, stream: Optional[int] = None):
+        _check(load().rgpu_engine_run(self.h, C.c_longlong(nsteps), C.c_void_p(stream or 0)))
+
+    def sync(self):
+        _check(load().rgpu_engine_sync(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rgpu_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,111 @@
+"""The persistent batched engine against the oracle's GCMC on the same
+counter-based random stream, plus energy-drift and batching checks."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from raspa2_b200 import native, systems, units
+
+from golden_cases import load, system_of
+
+pytestmark = pytest.mark.gpu
+
+
+def engine_run(sysm, mols, nsteps, precision, seed=777, stream_id=3, threads=256, maxmol=64):
+    g = native.GpuSystem(sysm, maxmol=maxmol, seed=seed, stream_id=stream_id)
+    g.set_adsorbates(mols)
+    e = native.Engine([g], precision=precision, threads=threads)
+    e.run(nsteps)
+    e.sync()
+    return g, g.state()
+
+
+def oracle_run(sysm, mols, nsteps, seed=777, stream_id=3, maxmol=64):
+    o = O.Oracle.from_system(sysm, maxmol=maxmol)
+    o.set_molecules(mols)
+    p = O.mc_params(sysm, seed, stream_id)
+    st = O.MCState()
+    o.mc_run(p, st, 0, nsteps)
+    return o, st
+
+
+@pytest.mark.parametrize("name", ["co2_tiny", "methane_config0"])
+def test_fp64_engine_reproduces_oracle_trajectory(cuda, name):
+    c = load(name)
+    s = system_of(c)
+    mols = np.array(c["molecules"])
+    n = 300
+    g, st = engine_run(s, mols, n, native.RGPU_FP64)
+    o, ost = oracle_run(s, mols, n)
+    assert st["status"] == 0
+    assert st["step"] == n
+    np.testing.assert_array_equal(st["counters"][0:4], np.array(ost.attempts))
+    np.testing.assert_array_equal(st["counters"][4:8], np.array(ost.accepted))
+    assert st["counters"][8] == ost.moves
+    assert st["nmol"] == o.nmol
+    np.testing.assert_allclose(g.adsorbates(), o.molecules(), rtol=0, atol=1e-10)
+    # running energy changes (engine order: hv, av, hc, ac, hF, aF)
+    np.testing.assert_allclose(st["energy"][:6], np.array(ost.u), rtol=1e-9, atol=1e-6)
+
+
+@pytest.mark.parametrize("precision,tol", [(native.RGPU_FP64, 1e-10), (native.RGPU_MIXED, 1e-6)])
+def test_energy_drift(cuda, precision, tol):
+    """Running totals after many accepted moves equal a full recomputation
+    (the reference's energy-drift check, src/output.c:7032)."""
+    c = load("co2_config1")
+    s = system_of(c)
+    g = native.GpuSystem(s, maxmol=128, seed=99, stream_id=1)
+    g.set_adsorbates(np.array(c["molecules"])[:4])
+    e0 = g.total_energy()
+    g.set_energy(np.concatenate([e0, [0, 0]]))
+    eng = native.Engine([g], precision=precision)
+    eng.run(2000)
+    eng.sync()
+    st = g.state()
+    assert st["status"] == 0
+    acc = st["counters"][4:8].sum()
+    assert acc > 20
+    e1 = g.total_energy()
+    kT = units.K_B * s.temperature
+    drift = np.abs(st["energy"][:6] - e1)
+    scale = np.maximum(np.abs(e1), kT)
+    assert np.all(drift <= tol * scale * max(1.0, acc / 100.0)), (st["energy"][:6], e1, drift / scale)
+
+
+def test_batched_systems_match_single_runs(cuda):
+    """Each system's result is the same alone and in a batch of uneven
+    systems (independent streams, one thread block each)."""
+    specs = [systems.tiny_co2_system(seed=7), systems.co2_system(seed=21, n_atoms=512, cell=20.0, kmax=5),
+             systems.methane_system(seed=3)]
+    n = 200
+    alone = []
+    for i, s in enumerate(specs):
+        g, st = engine_run(s, np.zeros((0, s.molecule.n_atoms, 3)), n, native.RGPU_MIXED, seed=5, stream_id=i)
+        alone.append((st, g.adsorbates()))
+    gs = []
+    for i, s in enumerate(specs):
+        g = native.GpuSystem(s, maxmol=64, seed=5, stream_id=i)
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+        gs.append(g)
+    e = native.Engine(gs, precision=native.RGPU_MIXED)
+    e.run(n)
+    e.sync()
+    for g, (st, xyz) in zip(gs, alone):
+        st2 = g.state()
+        np.testing.assert_array_equal(st2["counters"], st["counters"])
+        assert st2["nmol"] == st["nmol"]
+        np.testing.assert_array_equal(st2["energy"], st["energy"])
+        np.testing.assert_array_equal(g.adsorbates(), xyz)
+
+
+def test_mixed_engine_tracks_fp64(cuda):
+    """Same random stream: the mixed engine takes the same decisions as the
+    FP64 engine over a short run (decisions are FP64 on FP32-accurate sums)."""
+    c = load("co2_tiny")
+    s = system_of(c)
+    mols = np.array(c["molecules"])
+    _, a = engine_run(s, mols, 150, native.RGPU_FP64)
+    _, b = engine_run(s, mols, 150, native.RGPU_MIXED)
+    np.testing.assert_array_equal(a["counters"][:9], b["counters"][:9])
+    kT = units.K_B * s.temperature
+    np.testing.assert_allclose(b["energy"][:6], a["energy"][:6], rtol=1e-5, atol=1e-3 * kT)
