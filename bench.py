@@ -1,0 +1,402 @@
+"""Benchmark: batched mixed-precision GCMC MC moves/s on one node.
+
+Workload (default): 64 independent CO2 GCMC systems of uneven size advanced
+by one persistent launch of the batched engine per step: cubic cells 18-36 A
+with 512-4096 framework atoms per cell (2x2x2 replication below 24 A),
+charges uniform in [-1.2, 1.2] e made neutral, Ewald alpha 0.265/A with kmax
+6-10, pressures log-spaced 1e3-1e7 Pa, T in {273, 298, 323} K, rigid 3-site
+CO2 with CBMC insertion/deletion (10 first-bead x 10 orientation trials),
+translation and rotation; FP32 pair terms with FP64 S(k), totals and
+acceptance. Synthetic frameworks, seeded per system.
+
+One step = `--moves-per-step` MC moves attempted by every system (counted as
+the reference counts attempted moves). Timing: CUDA events on the engine's
+stream around each step, the L2 cache flushed between steps (outside the
+events), warm-up steps first; max over ranks; value = moves of all ranks /
+that time. With torchrun each rank runs its own 64 systems (weak scaling, no
+collective on the data path).
+
+`--impl reference` times the reference's own CPU implementation
+(oracle/_ref/simulate, built from the reference sources) on the same systems
+on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from raspa2_b200 import raspa_io, systems, units  # noqa: E402
+
+METRIC = "MC moves/sec, batched mixed-prec vs plain GPU at 1e-6 rel err; p50/p99 job ms"
+REF_SIMULATE = os.path.join(ROOT, "oracle", "_ref", "simulate")
+
+# algorithmic FLOP per unit of work (counting FMA = 2, MUFU = 1)
+FLOP_PAIR_LJ = 25.0        # in-cutoff pair, LJ only
+FLOP_PAIR_LJ_EWALD = 49.0  # in-cutoff pair, LJ + real-space Ewald
+FLOP_KSITE = 10.0          # dS(k) per (wave vector, moved site)
+FLOP_KVEC = 12.0           # FP64 energy terms per wave vector
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nsys", type=int, default=64)
+    p.add_argument("--moves-per-step", type=int, default=2000)
+    p.add_argument("--threads", type=int, default=256)
+    p.add_argument("--maxmol", type=int, default=384)
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--ref-cycles", type=int, default=10)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    return p.parse_args()
+
+
+# --------------------------------------------------------------------------
+# reference CPU implementation
+def reference_sample(systems_list, cycles, seed0, workdir, cores):
+    """Runs the reference `simulate` on every system (one process each, `cores`
+    at a time) for `cycles` production cycles from an empty framework and
+    parses the attempted moves and the MC-move CPU seconds of each run."""
+    dirs = []
+    for i, s in enumerate(systems_list):
+        d = os.path.join(workdir, f"s{i}")
+        raspa_io.write_inputs(s, d, cycles=cycles, init_cycles=0, print_every=10 ** 9, seed=seed0 + i)
+        dirs.append(d)
+
+    def run(d):
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_SIMULATE, "-i", "simulation.input"], cwd=d, capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"reference simulate failed in {d}: {r.stderr[-500:]}")
+        out = os.path.join(d, "Output", "System_0")
+        f = os.path.join(out, os.listdir(out)[0])
+        return parse_reference_output(f) + (wall,)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        res = list(ex.map(run, dirs))
+    pool_wall = time.perf_counter() - t0
+    moves = sum(r[0] for r in res)
+    cpu = sum(r[1] for r in res)
+    return moves, cpu, pool_wall, res
+
+
+def parse_reference_output(path):
+    txt = open(path).read()
+    moves = 0.0
+    for name in ("translation", "rotation"):
+        m = re.search(r"Performance of the %s move:\n=+\nComponent 0 \[[^\]]*\]\n\s*total\s+([\d.eE+-]+)\s+([\d.eE+-]+)\s+([\d.eE+-]+)" % name, txt)
+        if m:
+            moves += sum(float(x) for x in m.groups())
+    for name in ("swap addition", "swap deletion"):
+        m = re.search(r"Performance of the %s move:\n=+\nComponent \[[^\]]*\] total tried: ([\d.eE+-]+)" % name, txt)
+        if m:
+            moves += float(m.group(1))
+    blk = txt.split("Production run CPU timings of the MC moves:")[1].split("Total all components:")[0]
+    cpu = 0.0
+    for key in ("translation", "rotation", "swap (insertion)", "swap (deletion)"):
+        m = re.search(r"\n\s*%s:\s+([\d.eE+-]+) \[s\]" % re.escape(key), blk)
+        if m:
+            cpu += float(m.group(1))
+    return moves, cpu
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, sys_list):
+    if not os.path.exists(REF_SIMULATE):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/simulate was not built "
+                                                              "(needs the reference sources: make -C oracle ref)"}))
+        return
+    cores = min(cpu_cores(), len(sys_list))
+    tmp = tempfile.mkdtemp(prefix="raspa_ref_")
+    try:
+        for w in range(args.warmup):
+            reference_sample(sys_list, 1, 100 + w, os.path.join(tmp, f"w{w}"), cores)
+        total_moves, total_cpu, total_wall = 0.0, 0.0, 0.0
+        for k in range(args.steps):
+            mv, cpu, wall, _ = reference_sample(sys_list, args.ref_cycles, 1000 + 97 * k, os.path.join(tmp, f"k{k}"),
+                                                cores)
+            total_moves += mv
+            total_cpu += cpu
+            total_wall += wall
+        per_core = total_moves / total_cpu
+        value = per_core * cores
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "MC moves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * total_wall / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"co2_gcmc_batched_{len(sys_list)}", "systems": len(sys_list),
+                       "cycles_per_step": args.ref_cycles},
+            "cpu_baseline": {"value": value, "unit": "MC moves/s", "cores": cores, "kind": "reference",
+                             "sample": f"{len(sys_list)} systems x {args.ref_cycles} cycles per step, "
+                                       f"one process per system, {cores} at a time",
+                             "single_core": per_core, "wall_clock_aggregate": total_moves / total_wall},
+            "e2e": {"value": value, "unit": "MC moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap,utilization.gpu")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                s, m, util = float(p[0]), float(p[1]), float(p[6])
+            except ValueError:
+                continue
+            mx = m
+            if util > 0:
+                sm.append(s)
+            for n, v in zip(names, p[2:6]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(self.lines)}
+
+
+def make_systems(n, rank):
+    return systems.batched_co2_systems(n, seed=2 + 7919 * rank)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from raspa2_b200 import native
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    prec = native.RGPU_MIXED if args.precision == "mixed" else native.RGPU_FP64
+
+    sys_list = make_systems(args.nsys, rank)
+    gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240 + rank, stream_id=i) for i, s in enumerate(sys_list)]
+    for g, s in zip(gs, sys_list):
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+    eng = native.Engine(gs, precision=prec, threads=args.threads)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    def counters():
+        return np.array([g.state()["counters"] for g in gs])
+
+    # warm-up (equilibrates the loadings)
+    for _ in range(args.warmup):
+        eng.run(args.moves_per_step, stream.cuda_stream)
+    torch.cuda.synchronize()
+    c0 = counters()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        t_wall0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                evs[k][0].record(stream)
+                eng.run(args.moves_per_step, stream.cuda_stream)
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    t_dev = sum(ms) / 1000.0
+    c1 = counters()
+    d = (c1 - c0).sum(axis=0)
+    moves = float(d[8])
+    status = [g.state()["status"] for g in gs]
+    if world > 1:
+        t = torch.tensor([t_dev, moves], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+        t_dev_max, moves_all = float(tmax[0]), float(t[1])
+    else:
+        t_dev_max, moves_all = t_dev, moves
+    value = moves_all / t_dev_max
+
+    # roofline of the engine kernel (one launch per step)
+    n_charged = float(d[12])
+    n_lj = float(d[11]) - n_charged
+    flop = FLOP_PAIR_LJ * n_lj + FLOP_PAIR_LJ_EWALD * n_charged + FLOP_KSITE * float(d[13]) + FLOP_KVEC * float(d[14])
+    achieved = flop / t_dev / 1e12
+    peak = native.fp32_peak_tflops()
+
+    # end to end through the public API with host buffers: every step uploads
+    # every system's configuration, runs, and reads back positions, energies
+    # and counters
+    e2e = None
+    if args.e2e_steps > 0:
+        h2d = d2h = 0
+        torch.cuda.synchronize()
+        moves_e = 0.0
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            for g in gs:
+                x = g.host_xyz if hasattr(g, "host_xyz") else g.adsorbates()
+                g.set_adsorbates(x)
+                h2d += x.nbytes + 4
+            before = sum(g.state()["counters"][8] for g in gs)
+            eng.run(args.moves_per_step, stream.cuda_stream)
+            eng.sync()
+            for g in gs:
+                st = g.state()
+                g.host_xyz = g.adsorbates()
+                d2h += g.host_xyz.nbytes + 8 * 8 + 16 * 8 + 4 + 4 + 8
+                moves_e += st["counters"][8]
+            moves_e -= before
+        t_e = time.perf_counter() - t0
+        e2e = {"value": moves_e / t_e * (world if world > 1 else 1), "unit": "MC moves/s",
+               "h2d_bytes_per_step": int(h2d / args.e2e_steps), "d2h_bytes_per_step": int(d2h / args.e2e_steps),
+               "path": "rgpu_set_adsorbates + rgpu_engine_run + rgpu_system_state/rgpu_get_adsorbates per step"}
+
+    loads = [g.state()["nmol"] for g in gs]
+    line = {
+        "metric": METRIC, "value": value, "unit": "MC moves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == native.RGPU_MIXED else "f64",
+        "data": "synthetic (seeded frameworks, random-init adsorbate state)",
+        "config": {"workload": f"co2_gcmc_batched_{args.nsys}", "systems_per_gpu": args.nsys,
+                   "moves_per_step_per_system": args.moves_per_step, "threads_per_block": args.threads,
+                   "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
+                   "framework_atoms": [int(s.n_framework()) for s in sys_list[:8]] + ["..."],
+                   "mean_loading": float(np.mean(loads))},
+        "wall_s": t_wall, "gpu_launches": args.steps,
+        "status_nonzero_systems": int(sum(1 for s in status if s)),
+        "acceptance": {k: (float(d[4 + i]) / max(float(d[i]), 1.0)) for i, k in
+                       enumerate(["translation", "rotation", "insertion", "deletion"])},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured FP32 FMA probe (rgpu_fp32_peak_probe) on this GPU",
+                     "work": {"pairs_in_cutoff_lj": n_lj, "pairs_in_cutoff_lj_ewald": n_charged,
+                              "pairs_visited": float(d[10]), "k_site_products": float(d[13]),
+                              "k_energy_terms": float(d[14])}},
+        "clocks": clk.summary(),
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_plain:
+        line["plain_gpu"] = plain_gpu_rate(native, stream)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_SIMULATE):
+        cores = min(cpu_cores(), len(sys_list))
+        tmp = tempfile.mkdtemp(prefix="raspa_ref_")
+        try:
+            mv, cpu, wall, _ = reference_sample(sys_list, args.ref_cycles, 4242, tmp, cores)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        per_core = mv / cpu
+        line["cpu_baseline"] = {"value": per_core * cores, "unit": "MC moves/s", "cores": cores,
+                                "kind": "reference",
+                                "sample": f"{len(sys_list)} systems x {args.ref_cycles} cycles from empty, "
+                                          "reference simulate (oracle/_ref), one process per system",
+                                "single_core": per_core}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def plain_gpu_rate(native, stream, nsteps=2000):
+    """The plain comparator: one system (the 1536-atom CO2 system) at a time,
+    FP64, through the same engine with a single thread block."""
+    s = systems.co2_system(seed=1)
+    g = native.GpuSystem(s, maxmol=256, seed=5, stream_id=0)
+    g.set_adsorbates(np.zeros((0, 3, 3)))
+    e = native.Engine([g], precision=native.RGPU_FP64, threads=256)
+    e.run(nsteps, stream.cuda_stream)
+    e.sync()
+    c0 = g.state()["counters"][8]
+    t0 = time.perf_counter()
+    e.run(nsteps, stream.cuda_stream)
+    e.sync()
+    t = time.perf_counter() - t0
+    return {"engine_fp64_single_system_moves_per_s": (g.state()["counters"][8] - c0) / t,
+            "system": "co2 1536 atoms, kmax 8"}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        run_reference_arm(args, make_systems(args.nsys, 0))
+        return
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

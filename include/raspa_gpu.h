@@ -159,12 +159,18 @@ int rgpu_engine_destroy(rgpu_engine *eng);
 int rgpu_engine_run(rgpu_engine *eng, long long nsteps, void *stream);
 int rgpu_engine_sync(rgpu_engine *eng);
 /* Running energies (8 doubles, first six as rgpu_total_energy), counters
- * (12: attempts[4], accepted[4], moves, overlaps, 2 spare), molecule count,
- * status word (0 = fine) and next step index of one system. */
-int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters12, int *nmol, int *status,
+ * (16: attempts[4], accepted[4], counted moves, overlaps, pairs visited,
+ * pairs in cut-off, charged pairs in cut-off, k x site products, k sums,
+ * spare), molecule count, status word (0 = fine) and next step index. */
+int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters16, int *nmol, int *status,
                       unsigned long long *step);
 /* Resets the running energies to `energy8` (e.g. after rgpu_total_energy). */
 int rgpu_system_set_energy(rgpu_system *sys, const double *energy8);
+
+/* ---- measurement -------------------------------------------------------- */
+/* FP32 FMA throughput of the current device in TFLOP/s (FMA = 2 FLOP), the
+ * roofline denominator of the pair kernels. No counterpart in the reference. */
+int rgpu_fp32_peak_probe(double *tflops, double *seconds);
 
 #ifdef __cplusplus
 }

@@ -825,13 +825,13 @@ extern "C" int rgpu_engine_sync(rgpu_engine *e)
   return RGPU_SUCCESS;
 }
 
-extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *counters12, int *nmol, int *status,
+extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *counters16, int *nmol, int *status,
                                  unsigned long long *step)
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
   CK(cudaDeviceSynchronize());
   if (energy8) CK(cudaMemcpy(energy8, s->energy, sizeof(double) * RGPU_NE, cudaMemcpyDeviceToHost));
-  if (counters12) CK(cudaMemcpy(counters12, s->counters, sizeof(long long) * RGPU_NCNT, cudaMemcpyDeviceToHost));
+  if (counters16) CK(cudaMemcpy(counters16, s->counters, sizeof(long long) * RGPU_NCNT, cudaMemcpyDeviceToHost));
   if (nmol) CK(cudaMemcpy(nmol, s->nmol, sizeof(int), cudaMemcpyDeviceToHost));
   if (status) CK(cudaMemcpy(status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
   if (step) CK(cudaMemcpy(step, s->step, sizeof(unsigned long long), cudaMemcpyDeviceToHost));

@@ -68,6 +68,8 @@ struct Ctl {
   int accept;
   int sel;
   int nads;           /* adsorbate atoms = nmol * natom */
+  /* work done: pairs visited, in cut-off, charged in cut-off, k x site, k */
+  unsigned long long cnt[5];
 };
 
 template <bool MIXED>
@@ -170,6 +172,10 @@ template <bool MIXED>
 __device__ void engine_ewald(const Eng<MIXED> &E, int ns, double &e_ads, double &e_host)
 {
   ewald_phases<MIXED>(*E.S, E.sites, ns, E.tab, E.kw);
+  if (threadIdx.x == 0) {
+    E.ctl->cnt[3] += (unsigned long long)E.S->nk * ns;
+    E.ctl->cnt[4] += (unsigned long long)E.S->nk;
+  }
   __syncthreads();
   ewald_energy_sum<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, e_ads, e_host, E.red);
 }
@@ -497,6 +503,9 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     E.kw = kw;
     E.red = (double *)(smem + L.red);
     E.ctl = (Ctl *)(smem + L.ctl);
+    E.sc.cnt = E.ctl->cnt;
+    E.sc.upos = nullptr;
+    if (threadIdx.x < 5) E.ctl->cnt[threadIdx.x] = 0ULL;
     /* load the descriptor */
     load_sys(E.S, &systems[sysi]);
     RgpuSys &S = *E.S;
@@ -562,6 +571,7 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     if (threadIdx.x == 0) {
       *S.nmol = E.ctl->nmol;
       *S.step = step0 + (uint64_t)nsteps;
+      for (int c = 0; c < 5; c++) S.counters[RGPU_CNT_PAIRS + c] += (long long)E.ctl->cnt[c];
     }
     __syncthreads();
   }

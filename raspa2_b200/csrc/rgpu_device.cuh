@@ -186,6 +186,7 @@ struct EvalScratch {
   double *uc;
   int *uo;
   int *upos;      /* position of the unit */
+  unsigned long long *cnt;   /* optional {pairs visited, in cut-off, charged in cut-off} */
 };
 
 struct EvalPlan {
@@ -218,7 +219,7 @@ __device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwar
 
 /* one unit of framework work, FP32 path */
 __device__ __forceinline__ void unit_fw_mixed(const RgpuSys &S, const int4 *fw, const BeadPos &b, int lo,
-                                              int hi, bool check, float &av, float &ac, int &ov)
+                                              int hi, bool check, float &av, float &ac, int &ov, int &nin, int &nch)
 {
   const int lane = threadIdx.x & 31;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
@@ -238,6 +239,8 @@ __device__ __forceinline__ void unit_fw_mixed(const RgpuSys &S, const int4 *fw, 
       float dz = __int2float_rn(f.z - b.zi) * sz;
       float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       if (r2 < rc2) {
+      nin++;
+        nin++;
         float ri = rsqrtf(r2);
         ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);      /* one Newton step */
         float ir2 = ri * ri;
@@ -247,6 +250,7 @@ __device__ __forceinline__ void unit_fw_mixed(const RgpuSys &S, const int4 *fw, 
         av += u;
         if (check && u >= thr) ov = 1;
         if (charged) {
+          nch++;
           float r = r2 * ri;
           float uc = qa * __int_as_float(f.w) * rgpu_erfc_f(alpha * r) * ri;
           ac += uc;
@@ -258,7 +262,7 @@ __device__ __forceinline__ void unit_fw_mixed(const RgpuSys &S, const int4 *fw, 
 }
 
 __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw, const BeadPos &b, int lo,
-                                             int hi, bool check, double &av, double &ac, int &ov)
+                                             int hi, bool check, double &av, double &ac, int &ov, int &nin, int &nch)
 {
   const int lane = threadIdx.x & 31;
   const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
@@ -279,12 +283,15 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
       dz -= Lz * rgpu_nint(dz * iz);
       double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 < rc2) {
+      nin++;
+        nin++;
         double s6 = P.sig2 / r2;
         s6 = s6 * s6 * s6;
         double u = P.eps4 * (s6 * (s6 - 1.0)) - P.shift;
         av += u;
         if (check && u >= thr) ov = 1;
         if (charged) {
+          nch++;
           double r = sqrt(r2);
           double uc = qa * f.w * (erfc(alpha * r) / r);
           ac += uc;
@@ -296,7 +303,7 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
 }
 
 __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo,
-                                               int hi, int exclude, bool check, float &av, float &ac, int &ov)
+                                               int hi, int exclude, bool check, float &av, float &ac, int &ov, int &nin, int &nch)
 {
   const int lane = threadIdx.x & 31;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
@@ -314,6 +321,7 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
     float dz = __int2float_rn(f.z - b.zi) * sz;
     float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     if (r2 < rc2) {
+      nin++;
       const RgpuLJf P = S.ljf_bb[b.atom][at];
       float ri = rsqrtf(r2);
       ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);
@@ -325,6 +333,7 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
       if (check && u >= thr) ov = 1;
       float qb = S.mol_qf[at];
       if (charged && qb != 0.0f) {
+        nch++;
         float r = r2 * ri;
         float uc = qa * qb * rgpu_erfc_f(alpha * r) * ri;
         ac += uc;
@@ -335,7 +344,7 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
 }
 
 __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *ads, const BeadPos &b, int lo,
-                                              int hi, int exclude, bool check, double &av, double &ac, int &ov)
+                                              int hi, int exclude, bool check, double &av, double &ac, int &ov, int &nin, int &nch)
 {
   const int lane = threadIdx.x & 31;
   const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
@@ -355,6 +364,7 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
     dz -= Lz * rgpu_nint(dz * iz);
     double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 < rc2) {
+      nin++;
       const RgpuLJ P = S.lj_bb[b.atom][at];
       double s6 = P.sig2 / r2;
       s6 = s6 * s6 * s6;
@@ -363,6 +373,7 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
       if (check && u >= thr) ov = 1;
       double qb = S.mol_q[at];
       if (charged && qb != 0.0) {
+        nch++;
         double r = sqrt(r2);
         double uc = qa * qb * (erfc(alpha * r) / r);
         ac += uc;
@@ -386,17 +397,17 @@ __device__ void eval_positions(const RgpuSys &S, const void *fw, const void *ads
     const int p = u / per, c = u - p * per;
     const BeadPos b = pos[p];
     const bool check = p < pair_check;
-    int ov = 0;
+    int ov = 0, nin = 0, nch = 0;
     double v, q;
     if (MIXED) {
       float av = 0.0f, ac = 0.0f;
       if (c < pl.cf) {
         int lo = (int)((long long)S.nfw * c / pl.cf), hi = (int)((long long)S.nfw * (c + 1) / pl.cf);
-        unit_fw_mixed(S, (const int4 *)fw, b, lo, hi, check, av, ac, ov);
+        unit_fw_mixed(S, (const int4 *)fw, b, lo, hi, check, av, ac, ov, nin, nch);
       } else {
         int cc = c - pl.cf;
         int lo = (int)((long long)nads * cc / pl.ca), hi = (int)((long long)nads * (cc + 1) / pl.ca);
-        unit_ads_mixed(S, (const int4 *)ads, b, lo, hi, b.excl, check, av, ac, ov);
+        unit_ads_mixed(S, (const int4 *)ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch);
       }
       v = (double)warp_sum(av);
       q = (double)warp_sum(ac);
@@ -404,16 +415,28 @@ __device__ void eval_positions(const RgpuSys &S, const void *fw, const void *ads
       double av = 0.0, ac = 0.0;
       if (c < pl.cf) {
         int lo = (int)((long long)S.nfw * c / pl.cf), hi = (int)((long long)S.nfw * (c + 1) / pl.cf);
-        unit_fw_fp64(S, (const double4 *)fw, b, lo, hi, check, av, ac, ov);
+        unit_fw_fp64(S, (const double4 *)fw, b, lo, hi, check, av, ac, ov, nin, nch);
       } else {
         int cc = c - pl.cf;
         int lo = (int)((long long)nads * cc / pl.ca), hi = (int)((long long)nads * (cc + 1) / pl.ca);
-        unit_ads_fp64(S, (const AdsRec64 *)ads, b, lo, hi, b.excl, check, av, ac, ov);
+        unit_ads_fp64(S, (const AdsRec64 *)ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch);
       }
       v = warp_sum(av);
       q = warp_sum(ac);
     }
     ov = warp_or(ov);
+    if (sc.cnt) {
+      nin = __reduce_add_sync(RGPU_FULL, (unsigned)nin);
+      nch = __reduce_add_sync(RGPU_FULL, (unsigned)nch);
+      if (lane == 0) {
+        int lo, hi;
+        if (c < pl.cf) { lo = (int)((long long)S.nfw * c / pl.cf); hi = (int)((long long)S.nfw * (c + 1) / pl.cf); }
+        else { int cc = c - pl.cf; lo = (int)((long long)nads * cc / pl.ca); hi = (int)((long long)nads * (cc + 1) / pl.ca); }
+        atomicAdd(&sc.cnt[0], (unsigned long long)(hi - lo));
+        atomicAdd(&sc.cnt[1], (unsigned long long)nin);
+        atomicAdd(&sc.cnt[2], (unsigned long long)nch);
+      }
+    }
     if (lane == 0) {
       sc.uv[u] = v;
       sc.uc[u] = q;

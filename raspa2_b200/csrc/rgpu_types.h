@@ -30,7 +30,12 @@ enum {
   RGPU_CNT_ACCEPT = 4,   /* [4..7] */
   RGPU_CNT_MOVES = 8,    /* counted MC moves */
   RGPU_CNT_OVERLAP = 9,  /* proposals rejected by overlap */
-  RGPU_NCNT = 12
+  RGPU_CNT_PAIRS = 10,   /* bead-atom pairs visited */
+  RGPU_CNT_INCUT = 11,   /* pairs inside the cut-off (LJ evaluated) */
+  RGPU_CNT_CHARGED = 12, /* of those, pairs with a real-space charge term */
+  RGPU_CNT_KSITES = 13,  /* wave vector x site products of dS(k) */
+  RGPU_CNT_KVEC = 14,    /* wave vectors summed (energy terms) */
+  RGPU_NCNT = 16
 };
 
 /* per-system running energies (internal units, FP64) */

@@ -28,7 +28,7 @@ EXPORTS = [
     "rgpu_remove_molecule", "rgpu_bead_energies", "rgpu_move_energy_difference",
     "rgpu_ewald_fourier_difference", "rgpu_ewald_accept", "rgpu_total_energy", "rgpu_grid_build",
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
-    "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy",
+    "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
 ]
 
 
@@ -88,6 +88,14 @@ def _check(rc: int):
 
 def device_count() -> int:
     return int(load().rgpu_device_count())
+
+
+def fp32_peak_tflops() -> float:
+    """Measured FP32 FMA throughput of the current device (TFLOP/s)."""
+    t = C.c_double()
+    s = C.c_double()
+    _check(load().rgpu_fp32_peak_probe(C.byref(t), C.byref(s)))
+    return t.value
 
 
 def _arr(a, dt):
@@ -218,7 +226,7 @@ class GpuSystem:
 
     def state(self):
         e = np.zeros(8)
-        c = np.zeros(12, np.int64)
+        c = np.zeros(16, np.int64)
         n = C.c_int()
         st = C.c_int()
         step = C.c_ulonglong()
