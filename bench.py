@@ -324,6 +324,13 @@ def run_ours(args):
                "path": "rgpu_set_adsorbates + rgpu_engine_run + rgpu_system_state/rgpu_get_adsorbates per step"}
 
     loads = [g.state()["nmol"] for g in gs]
+    cyc = (c1 - c0)[:, 15].astype(float)
+    imbalance = {"max_over_mean_system_cycles": float(cyc.max() / max(cyc.mean(), 1.0)),
+                 "slowest_system": int(np.argmax(cyc)), "slowest_atoms": int(sys_list[int(np.argmax(cyc))].n_framework()),
+                 "slowest_loading": int(loads[int(np.argmax(cyc))]),
+                 "us_per_move_mean": float(np.mean(cyc / np.maximum((c1 - c0)[:, 8], 1)) / 1965.0),
+                 "share_eval": float((c1 - c0)[:, 16].sum() / max(cyc.sum(), 1.0)),
+                 "share_ewald": float((c1 - c0)[:, 17].sum() / max(cyc.sum(), 1.0))}
     line = {
         "metric": METRIC, "value": value, "unit": "MC moves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev_max / args.steps, "higher_is_better": True,
@@ -336,6 +343,7 @@ def run_ours(args):
                    "mean_loading": float(np.mean(loads))},
         "wall_s": t_wall, "gpu_launches": args.steps,
         "status_nonzero_systems": int(sum(1 for s in status if s)),
+        "load_balance": imbalance, "cluster": eng.cluster,
         "acceptance": {k: (float(d[4 + i]) / max(float(d[i]), 1.0)) for i, k in
                        enumerate(["translation", "rotation", "insertion", "deletion"])},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

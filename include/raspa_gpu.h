@@ -151,18 +151,24 @@ int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double s
 
 /* ---- persistent batched engine ------------------------------------------ */
 /* Groups systems for one persistent launch; each system is advanced by one
- * thread block. `threads` = block size (128..512, multiple of 32). */
-int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads);
+ * thread-block cluster of `cluster` CTAs (1, 2, 4 or 8; 0 chooses from the
+ * number of systems and SMs) that split its framework between them.
+ * `threads` = CTA size (64..512, multiple of 32). */
+int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
+                       int cluster);
+/* CTAs per system of an engine. */
+int rgpu_engine_cluster(rgpu_engine *eng);
 int rgpu_engine_destroy(rgpu_engine *eng);
 /* Advances every system by `nsteps` MC moves (asynchronous on `stream`, a
  * cudaStream_t or NULL for the library stream). */
 int rgpu_engine_run(rgpu_engine *eng, long long nsteps, void *stream);
 int rgpu_engine_sync(rgpu_engine *eng);
 /* Running energies (8 doubles, first six as rgpu_total_energy), counters
- * (16: attempts[4], accepted[4], counted moves, overlaps, pairs visited,
+ * (20: attempts[4], accepted[4], counted moves, overlaps, pairs visited,
  * pairs in cut-off, charged pairs in cut-off, k x site products, k sums,
+ * engine clock cycles, of which in pair evaluations, in Ewald sums, 2
  * spare), molecule count, status word (0 = fine) and next step index. */
-int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters16, int *nmol, int *status,
+int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters20, int *nmol, int *status,
                       unsigned long long *step);
 /* Resets the running energies to `energy8` (e.g. after rgpu_total_energy). */
 int rgpu_system_set_energy(rgpu_system *sys, const double *energy8);

@@ -60,6 +60,7 @@ struct rgpu_system {
   /* device buffers */
   double4 *fw64;
   int4 *fw32;
+  TileRec *tiles_d;
   char4 *kvec;
   double *kfactor;
   double2 *sk_fw, *sk_ads, *ds;
@@ -88,14 +89,14 @@ struct rgpu_system {
 struct rgpu_engine {
   std::vector<rgpu_system *> sys;
   RgpuSys *d_systems;
-  int mixed, threads, kw, max_ads, nfw_smem;
+  int mixed, threads, kw, max_ads, cluster, fw_items, tile_items;
   cudaStream_t st;
 };
 
 static void sys_free(rgpu_system *s)
 {
   if (!s) return;
-  void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
+  void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->tiles_d, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
                   s->nmol, s->energy, s->step, s->counters, s->status, s->rec32, s->rec64, s->io_xyz,
                   s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov};
   for (void *p : ptrs)
@@ -234,20 +235,89 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     h.fix_scale[c] = (float)(d->box[c] / 4294967296.0);
     h.kmax[c] = d->ewald ? d->kmax[c] : 0;
   }
-  for (int idx = 0; idx < d->nfw; idx++) {
-    fw32[idx].x = 0;
-  }
-  for (int idx = 0; idx < d->nfw; idx++) {
-    /* fixed-point coordinates (see rgpu_types.h) */
-    double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
-    int v[3];
-    for (int c = 0; c < 3; c++) {
-      double f = p[c] * h.inv_box[c];
-      f -= floor(f);
-      long long q = llrint(f * 4294967296.0);
-      v[c] = (int)(unsigned)(q & 0xffffffffLL);
+  /* Mixed-precision layout: fixed-point coordinates (see rgpu_types.h), the
+   * framework sorted along a Morton curve of ~4 A cells and cut into tiles of
+   * 32 spatially close atoms with a bounding box each; the two low bits of
+   * the z coordinate carry the atom's segment (pseudo-atom type), an offset
+   * of at most 3 * L / 2^32 (< 1e-8 A). */
+  std::vector<TileRec> tiles;
+  {
+    int g[3];
+    for (int c = 0; c < 3; c++) g[c] = std::max(1, std::min(1023, (int)(d->box[c] / 4.0)));
+    std::vector<unsigned long long> key(d->nfw);
+    std::vector<int> seg_of(d->nfw);
+    for (int idx = 0; idx < d->nfw; idx++) {
+      int sgi = 0;
+      while (sgi + 1 < nseg && idx >= h.seg_start[sgi + 1]) sgi++;
+      seg_of[idx] = sgi;
+      unsigned cell[3];
+      const double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
+      for (int c = 0; c < 3; c++) {
+        double f = p[c] * h.inv_box[c];
+        f -= floor(f);
+        int ci = (int)(f * g[c]);
+        cell[c] = (unsigned)std::min(std::max(ci, 0), g[c] - 1);
+      }
+      unsigned long long k = 0;
+      for (int bit = 0; bit < 10; bit++)
+        for (int c = 0; c < 3; c++) k |= (unsigned long long)((cell[c] >> bit) & 1u) << (3 * bit + c);
+      key[idx] = (k << 20) | (unsigned long long)idx;
     }
-    fw32[idx].x = v[0]; fw32[idx].y = v[1]; fw32[idx].z = v[2];
+    std::vector<int> sp(d->nfw);
+    for (int i = 0; i < d->nfw; i++) sp[i] = i;
+    std::sort(sp.begin(), sp.end(), [&](int a, int b) { return key[a] < key[b]; });
+    const int ntile = (d->nfw + 31) / 32;
+    fw32.assign((size_t)ntile * 32, make_int4(0, 0, 0, 0));
+    tiles.resize(ntile);
+    for (int t = 0; t < ntile; t++) {
+      const int n = std::min(32, d->nfw - 32 * t);
+      const double4 r0 = fw64[sp[32 * t]];
+      double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+      for (int j = 0; j < n; j++) {
+        const int idx = sp[32 * t + j];
+        const double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
+        const double p0[3] = {r0.x, r0.y, r0.z};
+        int v[3];
+        for (int c = 0; c < 3; c++) {
+          double f = p[c] * h.inv_box[c];
+          f -= floor(f);
+          long long q = llrint(f * 4294967296.0);
+          v[c] = (int)(unsigned)(q & 0xffffffffLL);
+          /* offset from the tile's first atom, minimum image */
+          double dd = p[c] - p0[c];
+          dd -= d->box[c] * floor(dd * h.inv_box[c] + 0.5);
+          lo[c] = std::min(lo[c], dd);
+          hi[c] = std::max(hi[c], dd);
+        }
+        v[2] = (v[2] & ~3) | seg_of[idx];
+        float qf = (float)fw64[idx].w;
+        int qb;
+        memcpy(&qb, &qf, 4);
+        fw32[(size_t)32 * t + j] = make_int4(v[0], v[1], v[2], qb);
+      }
+      TileRec tr;
+      double cen[3];
+      const double p0[3] = {r0.x, r0.y, r0.z};
+      float hh[3];
+      for (int c = 0; c < 3; c++) {
+        cen[c] = p0[c] + 0.5 * (lo[c] + hi[c]);
+        double half = 0.5 * (hi[c] - lo[c]);
+        /* margin for the fixed-point rounding of centre and atoms */
+        hh[c] = (float)(half * (1.0 + 1e-6) + 1e-5);
+        if (half >= 0.25 * d->box[c]) hh[c] = (float)(0.5 * d->box[c]);   /* no culling along this axis */
+      }
+      int cv[3];
+      for (int c = 0; c < 3; c++) {
+        double f = cen[c] * h.inv_box[c];
+        f -= floor(f);
+        long long q = llrint(f * 4294967296.0);
+        cv[c] = (int)(unsigned)(q & 0xffffffffLL);
+      }
+      tr.c = make_int4(cv[0], cv[1], cv[2], n);
+      tr.h = make_float4(hh[0], hh[1], hh[2], 0.0f);
+      tiles[t] = tr;
+    }
+    h.ntile = ntile;
   }
   h.rc2 = d->cutoff * d->cutoff;
   h.rc2f = (float)h.rc2;
@@ -319,7 +389,8 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   if (cudaMalloc((void **)&(p), (n)) != cudaSuccess) { sys_free(s); return fail(RGPU_E_CUDA, "cudaMalloc " #p); }
   ALLOC(s->d_sys, sizeof(RgpuSys));
   ALLOC(s->fw64, sizeof(double4) * d->nfw);
-  ALLOC(s->fw32, sizeof(int4) * d->nfw);
+  ALLOC(s->fw32, sizeof(int4) * 32 * (size_t)h.ntile);
+  ALLOC(s->tiles_d, sizeof(TileRec) * (size_t)h.ntile);
   ALLOC(s->kvec, sizeof(char4) * nk1);
   ALLOC(s->kfactor, sizeof(double) * nk1);
   ALLOC(s->sk_fw, sizeof(double2) * nk1);
@@ -343,6 +414,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
 #undef ALLOC
   h.fw64 = s->fw64;
   h.fw32 = s->fw32;
+  h.tiles = s->tiles_d;
   h.kvec = s->kvec;
   h.kfactor = s->kfactor;
   h.sk_fw = s->sk_fw;
@@ -357,7 +429,8 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   int rc = RGPU_SUCCESS;
   do {
     if (cudaMemcpyAsync(s->fw64, fw64.data(), sizeof(double4) * d->nfw, cudaMemcpyHostToDevice, st) ||
-        cudaMemcpyAsync(s->fw32, fw32.data(), sizeof(int4) * d->nfw, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(s->fw32, fw32.data(), sizeof(int4) * 32 * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(s->tiles_d, tiles.data(), sizeof(TileRec) * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
         cudaMemsetAsync(s->nmol, 0, sizeof(int), st) || cudaMemsetAsync(s->energy, 0, sizeof(double) * RGPU_NE, st) ||
         cudaMemsetAsync(s->step, 0, sizeof(unsigned long long), st) ||
         cudaMemsetAsync(s->counters, 0, sizeof(long long) * RGPU_NCNT, st) ||
@@ -749,39 +822,65 @@ extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], con
 }
 
 /* ---------------------------------------------------------------------- */
-extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads)
+/* Cluster size of an engine launch: the CTAs of one system. More CTAs per
+ * system when there are few systems (up to 8, the portable cluster size),
+ * one when the systems alone fill the GPU. */
+static int auto_cluster(int nsys)
+{
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int c = 1;
+  while (c < 8 && (long long)nsys * c * 2 <= sms) c *= 2;
+  return c;
+}
+
+extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
+                                  int cluster)
 {
   if (!out || !systems || n < 1) return fail(RGPU_E_INVALID, "bad argument");
   if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
   if (threads < 64 || threads > 512 || threads % 32) return fail(RGPU_E_INVALID, "threads %d", threads);
+  if (cluster < 0 || cluster > 8 || (cluster & (cluster - 1))) return fail(RGPU_E_INVALID, "cluster %d", cluster);
   *out = nullptr;
   rgpu_engine *e = new rgpu_engine();
   e->mixed = precision == RGPU_MIXED;
   e->threads = threads;
+  e->cluster = cluster ? cluster : auto_cluster(n);
   e->kw = 1;
   e->max_ads = 0;
-  int maxfw = 0;
+  int maxfw = 0, maxtile = 0;
   for (int i = 0; i < n; i++) {
     rgpu_system *s = systems[i];
     if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
     e->sys.push_back(s);
     e->kw = std::max(e->kw, s->kw);
     e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
-    maxfw = std::max(maxfw, s->d.nfw);
+    maxfw = std::max(maxfw, (s->d.nfw + e->cluster - 1) / e->cluster);
+    maxtile = std::max(maxtile, (s->h.ntile + e->cluster - 1) / e->cluster);
   }
   int dev = 0, smem_max = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  e->nfw_smem = maxfw;
-  if (rgpu_engine_smem_bytes(e->mixed, maxfw, e->max_ads, e->kw) > (size_t)smem_max) e->nfw_smem = 0;
-  if (rgpu_engine_smem_bytes(e->mixed, e->nfw_smem, e->max_ads, e->kw) > (size_t)smem_max) {
+  if (e->mixed) {
+    e->tile_items = maxtile;
+    e->fw_items = maxtile * 32;
+  } else {
+    e->tile_items = 0;
+    e->fw_items = maxfw;
+  }
+  if (rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw) > (size_t)smem_max) {
+    e->fw_items = 0;
+    e->tile_items = 0;
+  }
+  if (rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw) > (size_t)smem_max) {
     delete e;
     return fail(RGPU_E_INVALID, "adsorbate capacity does not fit in shared memory");
   }
   std::vector<RgpuSys> hs(n);
   for (int i = 0; i < n; i++) {
     hs[i] = e->sys[i]->h;
-    hs[i].smem_fw = e->nfw_smem > 0;
+    hs[i].smem_fw = e->fw_items > 0;
   }
   if (cudaMalloc((void **)&e->d_systems, sizeof(RgpuSys) * n) != cudaSuccess) {
     delete e;
@@ -812,9 +911,15 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   const int n = (int)e->sys.size();
-  CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->nfw_smem, e->threads, n, st));
+  CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items, e->cluster,
+                        e->threads, st));
   for (rgpu_system *s : e->sys) s->records_stale = 1;
   return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_cluster(rgpu_engine *e)
+{
+  return e ? e->cluster : 0;
 }
 
 extern "C" int rgpu_engine_sync(rgpu_engine *e)
@@ -825,13 +930,13 @@ extern "C" int rgpu_engine_sync(rgpu_engine *e)
   return RGPU_SUCCESS;
 }
 
-extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *counters16, int *nmol, int *status,
+extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *counters20, int *nmol, int *status,
                                  unsigned long long *step)
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
   CK(cudaDeviceSynchronize());
   if (energy8) CK(cudaMemcpy(energy8, s->energy, sizeof(double) * RGPU_NE, cudaMemcpyDeviceToHost));
-  if (counters16) CK(cudaMemcpy(counters16, s->counters, sizeof(long long) * RGPU_NCNT, cudaMemcpyDeviceToHost));
+  if (counters20) CK(cudaMemcpy(counters20, s->counters, sizeof(long long) * RGPU_NCNT, cudaMemcpyDeviceToHost));
   if (nmol) CK(cudaMemcpy(nmol, s->nmol, sizeof(int), cudaMemcpyDeviceToHost));
   if (status) CK(cudaMemcpy(status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
   if (step) CK(cudaMemcpy(step, s->step, sizeof(unsigned long long), cudaMemcpyDeviceToHost));

@@ -1,17 +1,20 @@
 /* Kernels of the B200 GCMC energy path.
  *
- *  - rgpu_engine_kernel: the persistent batched MC engine. One thread block
- *    owns one simulation box for the whole launch: the framework and the
- *    adsorbate records live in shared memory, the structure factors S(k) and
- *    the authoritative FP64 positions in HBM/L2. Each block advances its box
- *    by `nsteps` MC moves (translation, rotation, CBMC insertion, CBMC
- *    deletion: src/mc_moves.c:1529, :2636, :6941, :7150) without returning
- *    to the host, drawing every random number from the counter-based Philox
- *    stream (so FP64 and mixed runs see identical streams).
+ *  - rgpu_engine_kernel: the persistent batched MC engine. One thread-block
+ *    cluster owns one simulation box for the whole launch. The framework is
+ *    split between the CTAs of the cluster (each stages its share in shared
+ *    memory); every CTA keeps a full copy of the adsorbate records, draws the
+ *    same counter-based random numbers and takes the same decisions. Partial
+ *    sums of each energy evaluation and of each Ewald sum are combined across
+ *    the cluster through distributed shared memory in a fixed rank order, so
+ *    all CTAs see bitwise identical totals. Each cluster advances its box by
+ *    `nsteps` MC moves (translation, rotation, CBMC insertion, CBMC deletion:
+ *    src/mc_moves.c:1529, :2636, :6941, :7150) without returning to the host;
+ *    FP64 and mixed runs see identical random streams.
  *  - per-call kernels behind the reference-named C entry points: batched
- *    bead energies, energy differences of a moved molecule, Ewald Fourier
- *    difference and accept, full energy, structure factors.
+ *    bead energies, Ewald Fourier difference and accept, structure factors.
  */
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>
@@ -20,73 +23,89 @@
 #include "rgpu_device.cuh"
 #include "rgpu_engine.h"
 
+namespace cg = cooperative_groups;
+
 #define RGPU_MAX_UNITS 512
+#define RGPU_MAX_WARPS 32
 
 /* ------------------------------------------------------------------------ */
-/* shared-memory plan of the engine (offsets in bytes from the dynamic base) */
+/* shared-memory plan of the engine (offsets in bytes from the dynamic base).
+ * fw_items: framework records of this CTA's share (atoms; tiles*32 on the
+ * mixed path), tiles: tile records of the share (mixed only). */
 struct EngineLayout {
-  size_t sys, fw, ads, xyz, pos, res, ovf, uv, uc, uo, sites, tab, red, ctl, total;
+  size_t sys, fw, tiles, ads, xyz, pos, res, part, ovf, opart, uv, uc, uo, q, sites, tab, red, ctl, total;
 };
 
 __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
-__host__ __device__ inline EngineLayout engine_layout(int mixed, int nfw_smem, int max_ads_atoms, int kw)
+__host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw)
 {
   EngineLayout L;
   size_t o = 0;
   L.sys = o; o = rgpu_align(o + sizeof(RgpuSys));
-  L.fw = o; o = rgpu_align(o + (size_t)nfw_smem * (mixed ? sizeof(int4) : sizeof(double4)));
+  L.fw = o; o = rgpu_align(o + (size_t)fw_items * (mixed ? sizeof(int4) : sizeof(double4)));
+  L.tiles = o; o = rgpu_align(o + (size_t)tiles * sizeof(TileRec));
   L.ads = o; o = rgpu_align(o + (size_t)max_ads_atoms * (mixed ? sizeof(int4) : sizeof(AdsRec64)));
   L.xyz = o; o = rgpu_align(o + (mixed ? (size_t)max_ads_atoms * 3 * sizeof(double) : 0));
   L.pos = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(BeadPos));
   L.res = o; o = rgpu_align(o + RGPU_MAX_POS * 4 * sizeof(double));
+  L.part = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * 4 * sizeof(double));   /* double-buffered partials */
   L.ovf = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(int));
+  L.opart = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * sizeof(int));
   L.uv = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
   L.uc = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
   L.uo = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(int));
+  L.q = o; o = rgpu_align(o + (mixed ? (size_t)RGPU_MAX_WARPS * 64 * 12 : 0));
   L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
   L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed ? sizeof(float2) : sizeof(double2)));
   L.red = o; o = rgpu_align(o + 72 * sizeof(double));
-  L.ctl = o; o = rgpu_align(o + 64 * sizeof(double));
+  L.ctl = o; o = rgpu_align(o + 128 * sizeof(double));
   L.total = o;
   return L;
 }
 
-size_t rgpu_engine_smem_bytes(int mixed, int nfw_smem, int max_ads_atoms, int kw)
+size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw)
 {
-  return engine_layout(mixed, nfw_smem, max_ads_atoms, kw).total;
+  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw).total;
 }
 
 /* broadcast/control block in shared memory */
 struct Ctl {
   double u[4];        /* energies of the chosen configuration */
   double rosen;
-  double e_ads, e_host;
   double dl[4];
+  double ewp[2][2];   /* double-buffered Ewald partials {e_ads, e_host} */
+  double e_ads, e_host;
   int nmol;
   int fail;
   int accept;
   int sel;
   int nads;           /* adsorbate atoms = nmol * natom */
+  int xbuf;           /* exchange buffer index */
   /* work done: pairs visited, in cut-off, charged in cut-off, k x site, k */
   unsigned long long cnt[5];
+  long long cyc[2];   /* clock cycles in evaluations and Ewald sums */
 };
 
 template <bool MIXED>
 struct Eng {
   RgpuSys *S;
-  const void *fw;
-  void *ads;                 /* int4[] or AdsRec64[] */
+  EvalSlice sl;
+  void *ads;                 /* int4[] or AdsRec64[] (full copy) */
   double (*xyz)[3];          /* FP64 positions (MIXED: separate array; FP64: inside ads records) */
   BeadPos *pos;
-  double (*res)[4];
+  double (*res)[4];          /* combined results */
+  double (*part)[RGPU_MAX_POS][4];
   int *ovf;
+  int (*opart)[RGPU_MAX_POS];
   EvalScratch sc;
   EwSite *sites;
   typename PhaseT<MIXED>::T *tab;
   int kw;
+  int k0, k1;                /* this CTA's wave vectors */
   double *red;
   Ctl *ctl;
+  int rank, csize;
 };
 
 /* position of atom a of molecule m */
@@ -167,17 +186,78 @@ __device__ inline int select_trial(const double *bf, const int *ov, int n, doubl
   return sel;
 }
 
-/* Ewald difference for the sites in E.sites[0..ns); all threads call. */
+/* Evaluates P positions on this CTA's share and combines the partials of all
+ * CTAs of the cluster (rank order) into E.res / E.ovf. All threads call. */
+template <bool MIXED>
+__device__ void engine_eval(const Eng<MIXED> &E, int P, int pair_check)
+{
+  Ctl &C = *E.ctl;
+  const int b = C.xbuf;
+  const long long t0 = clock64();
+  eval_positions<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.part[b], E.opart[b], E.sc, RGPU_MAX_UNITS);
+  if (E.csize > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+      double s[4] = {0.0, 0.0, 0.0, 0.0};
+      int o = 0;
+      for (int r = 0; r < E.csize; r++) {
+        const double (*pr)[4] = (const double (*)[4])cl.map_shared_rank((double *)E.part[b], r);
+        const int *orr = cl.map_shared_rank((int *)E.opart[b], r);
+        for (int k = 0; k < 4; k++) s[k] += pr[p][k];
+        o |= orr[p];
+      }
+      for (int k = 0; k < 4; k++) E.res[p][k] = s[k];
+      E.ovf[p] = o;
+    }
+  } else {
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+      for (int k = 0; k < 4; k++) E.res[p][k] = E.part[b][p][k];
+      E.ovf[p] = E.opart[b][p];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    C.xbuf ^= 1;
+    C.cyc[0] += clock64() - t0;
+  }
+  __syncthreads();
+}
+
+/* Ewald difference for the sites in E.sites[0..ns): this CTA's wave vectors,
+ * then the cluster sum. All threads call. */
 template <bool MIXED>
 __device__ void engine_ewald(const Eng<MIXED> &E, int ns, double &e_ads, double &e_host)
 {
+  Ctl &C = *E.ctl;
+  const long long t0 = clock64();
   ewald_phases<MIXED>(*E.S, E.sites, ns, E.tab, E.kw);
   if (threadIdx.x == 0) {
-    E.ctl->cnt[3] += (unsigned long long)E.S->nk * ns;
-    E.ctl->cnt[4] += (unsigned long long)E.S->nk;
+    C.cnt[3] += (unsigned long long)(E.k1 - E.k0) * ns;
+    C.cnt[4] += (unsigned long long)(E.k1 - E.k0);
   }
   __syncthreads();
-  ewald_energy_sum<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, e_ads, e_host, E.red);
+  double ea, eh;
+  ewald_energy_sum<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, E.k0, E.k1, ea, eh, E.red);
+  if (E.csize > 1) {
+    const int b = C.xbuf;
+    if (threadIdx.x == 0) { C.ewp[b][0] = ea; C.ewp[b][1] = eh; }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    ea = 0.0;
+    eh = 0.0;
+    for (int r = 0; r < E.csize; r++) {
+      const Ctl *cr = cl.map_shared_rank(E.ctl, r);
+      ea += cr->ewp[b][0];
+      eh += cr->ewp[b][1];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) C.xbuf ^= 1;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) C.cyc[1] += clock64() - t0;
+  e_ads = ea;
+  e_host = eh;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -189,6 +269,7 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
   const int na = S.natom, nmol = C.nmol;
+  const bool lead = E.rank == 0 && threadIdx.x == 0;
   int m = (int)(rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOLECULE) * nmol);
   if (m >= nmol) m = nmol - 1;
   const double vnew = 2.0 * rgpu_uniform(S.seed, S.sys_id, step, SLOT_VNEW) - 1.0;
@@ -216,7 +297,7 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
     E.sites[na + a].q = -S.mol_q[a];
   }
   __syncthreads();
-  eval_positions<MIXED>(S, E.fw, E.ads, C.nads, E.pos, 2 * na, na, E.res, E.ovf, E.sc, RGPU_MAX_UNITS);
+  engine_eval<MIXED>(E, 2 * na, na);
   if (threadIdx.x == 0) {
     int ov = 0;
     double dl[4] = {0.0, 0.0, 0.0, 0.0};
@@ -229,7 +310,7 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
   }
   __syncthreads();
   if (C.fail) {
-    if (threadIdx.x == 0) S.counters[RGPU_CNT_OVERLAP]++;
+    if (lead) S.counters[RGPU_CNT_OVERLAP]++;
     return;
   }
   double ea = 0.0, eh = 0.0;
@@ -249,9 +330,9 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
     double du = C.dl[0] + C.dl[1] + C.dl[2] + C.dl[3] + d_ads + d_host;
     double u = rgpu_uniform(S.seed, S.sys_id, step, SLOT_ACCEPT);
     double pacc = exp(-S.beta * du);
-    if (!isfinite(du)) *S.status |= RGPU_ERR_NONFINITE;
+    if (E.rank == 0 && !isfinite(du)) *S.status |= RGPU_ERR_NONFINITE;
     C.accept = u < pacc;
-    if (C.accept) {
+    if (C.accept && E.rank == 0) {
       S.counters[RGPU_CNT_ACCEPT + mv]++;
       S.energy[RGPU_E_HOST_VDW] += C.dl[0];
       S.energy[RGPU_E_HOST_REAL] += C.dl[1];
@@ -267,7 +348,7 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
       double p[3] = {E.pos[threadIdx.x].x, E.pos[threadIdx.x].y, E.pos[threadIdx.x].z};
       atom_store(E, m, threadIdx.x, p);
     }
-    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, 2 * na);
+    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, 2 * na, E.k0, E.k1);
   }
   __syncthreads();
 }
@@ -286,6 +367,7 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
   Ctl &C = *E.ctl;
   const int na = S.natom, sb = S.start_bead, nmol = C.nmol;
   const int nf = S.ntrial_first, nt = S.ntrial;
+  const bool lead = E.rank == 0 && threadIdx.x == 0;
   int m = nmol;
   if (!insert) {
     m = (int)(rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOLECULE) * nmol);
@@ -307,7 +389,7 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
     bead_set(E.pos[i], S, p[0], p[1], p[2], sb, exclude);
   }
   __syncthreads();
-  eval_positions<MIXED>(S, E.fw, E.ads, C.nads, E.pos, nf, 0, E.res, E.ovf, E.sc, RGPU_MAX_UNITS);
+  engine_eval<MIXED>(E, nf, 0);
   if (threadIdx.x == 0) {
     double bf[RGPU_MAX_TRIALS];
     int ov[RGPU_MAX_TRIALS], any = 0;
@@ -328,7 +410,7 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
   }
   __syncthreads();
   if (C.fail) {
-    if (threadIdx.x == 0) S.counters[RGPU_CNT_OVERLAP]++;
+    if (lead) S.counters[RGPU_CNT_OVERLAP]++;
     return;
   }
   const BeadPos first = E.pos[C.sel];
@@ -366,8 +448,7 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
       }
     }
     __syncthreads();
-    eval_positions<MIXED>(S, E.fw, E.ads, C.nads, E.pos, nt * nb, 0, E.res, E.ovf, E.sc,
-                          RGPU_MAX_UNITS);
+    engine_eval<MIXED>(E, nt * nb, 0);
     if (threadIdx.x == 0) {
       double bf[RGPU_MAX_TRIALS], et[RGPU_MAX_TRIALS][4];
       int ov[RGPU_MAX_TRIALS], any = 0;
@@ -395,20 +476,20 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
     }
     __syncthreads();
     if (C.fail) {
-      if (threadIdx.x == 0) S.counters[RGPU_CNT_OVERLAP]++;
+      if (lead) S.counters[RGPU_CNT_OVERLAP]++;
       return;
     }
   }
   /* sites of the chosen configuration: first bead + beads of trial C.sel */
   if (threadIdx.x < na) {
     const int a = threadIdx.x;
-    BeadPos b;
-    if (a == sb) b = first;
+    BeadPos bp;
+    if (a == sb) bp = first;
     else {
       int j = a < sb ? a : a - 1;
-      b = E.pos[C.sel * nb + j];
+      bp = E.pos[C.sel * nb + j];
     }
-    E.sites[a].b = b;
+    E.sites[a].b = bp;
     E.sites[a].q = insert ? S.mol_q[a] : -S.mol_q[a];
   }
   __syncthreads();
@@ -431,10 +512,10 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
     double pacc;
     if (insert) pacc = rosen * exp(-S.beta * (d_ads + d_host)) * S.fugacity_beta_v / (1.0 + nmol);
     else pacc = (double)nmol / (rosen * exp(S.beta * (d_ads + d_host)) * S.fugacity_beta_v);
-    if (!(pacc == pacc)) *S.status |= RGPU_ERR_NONFINITE;
+    if (E.rank == 0 && !(pacc == pacc)) *S.status |= RGPU_ERR_NONFINITE;
     C.accept = u < pacc;
     const int mv = insert ? 2 : 3;
-    if (C.accept) {
+    if (C.accept && E.rank == 0) {
       S.counters[RGPU_CNT_ACCEPT + mv]++;
       double sgn = insert ? 1.0 : -1.0;
       S.energy[RGPU_E_HOST_VDW] += sgn * C.u[0];
@@ -462,7 +543,7 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
         atom_store(E, m, threadIdx.x, p);
       }
     }
-    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, na);
+    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, na, E.k0, E.k1);
     if (threadIdx.x == 0) {
       C.nmol = insert ? nmol + 1 : nmol - 1;
       C.nads = C.nmol * na;
@@ -481,53 +562,95 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
   __syncthreads();
 }
 
+/* share [lo, hi) of n items for rank r of c */
+__device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
+{
+  lo = (int)((long long)n * r / c);
+  hi = (int)((long long)n * (r + 1) / c);
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps, int kw,
-                                                          int max_ads_atoms, int nfw_smem)
+                                                          int max_ads_atoms, int fw_items, int tile_items)
 {
   extern __shared__ __align__(256) unsigned char smem[];
-  const EngineLayout L = engine_layout(MIXED, nfw_smem, max_ads_atoms, kw);
-  for (int sysi = blockIdx.x; sysi < nsys; sysi += gridDim.x) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int csize = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
+  const int sysi = blockIdx.x / csize;
+  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw);
+  if (sysi < nsys) {
     Eng<MIXED> E;
+    E.rank = rank;
+    E.csize = csize;
     E.S = (RgpuSys *)(smem + L.sys);
     E.ads = smem + L.ads;
     E.xyz = (double(*)[3])(smem + L.xyz);
     E.pos = (BeadPos *)(smem + L.pos);
     E.res = (double(*)[4])(smem + L.res);
+    E.part = (double(*)[RGPU_MAX_POS][4])(smem + L.part);
     E.ovf = (int *)(smem + L.ovf);
+    E.opart = (int(*)[RGPU_MAX_POS])(smem + L.opart);
     E.sc.uv = (double *)(smem + L.uv);
     E.sc.uc = (double *)(smem + L.uc);
     E.sc.uo = (int *)(smem + L.uo);
+    E.sc.upos = nullptr;
+    E.sc.qr2 = (float *)(smem + L.q);
+    E.sc.qq = E.sc.qr2 + RGPU_MAX_WARPS * 64;
+    E.sc.qt = (int *)(E.sc.qq + RGPU_MAX_WARPS * 64);
     E.sites = (EwSite *)(smem + L.sites);
     E.tab = (typename PhaseT<MIXED>::T *)(smem + L.tab);
     E.kw = kw;
     E.red = (double *)(smem + L.red);
     E.ctl = (Ctl *)(smem + L.ctl);
     E.sc.cnt = E.ctl->cnt;
-    E.sc.upos = nullptr;
     if (threadIdx.x < 5) E.ctl->cnt[threadIdx.x] = 0ULL;
-    /* load the descriptor */
+    if (threadIdx.x == 0) {
+      E.ctl->xbuf = 0;
+      E.ctl->cyc[0] = E.ctl->cyc[1] = 0;
+    }
     load_sys(E.S, &systems[sysi]);
     RgpuSys &S = *E.S;
-    /* framework to shared memory */
-    if (S.smem_fw) {
-      if (MIXED) {
-        int4 *d = (int4 *)(smem + L.fw);
-        for (int i = threadIdx.x; i < S.nfw; i += blockDim.x) d[i] = S.fw32[i];
+    /* this CTA's framework share, staged in shared memory when it fits */
+    if (MIXED) {
+      int t0, t1;
+      share(S.ntile, rank, csize, t0, t1);
+      E.sl.fw_lo = t0;
+      E.sl.fw_hi = t1;
+      if (S.smem_fw) {
+        int4 *dfw = (int4 *)(smem + L.fw);
+        TileRec *dt = (TileRec *)(smem + L.tiles);
+        for (int i = threadIdx.x; i < (t1 - t0) * 32; i += blockDim.x) dfw[i] = S.fw32[t0 * 32 + i];
+        for (int i = threadIdx.x; i < t1 - t0; i += blockDim.x) dt[i] = S.tiles[t0 + i];
+        E.sl.fw = dfw - (size_t)t0 * 32;
+        E.sl.tiles = dt - t0;
       } else {
-        double4 *d = (double4 *)(smem + L.fw);
-        for (int i = threadIdx.x; i < S.nfw; i += blockDim.x) d[i] = S.fw64[i];
+        E.sl.fw = S.fw32;
+        E.sl.tiles = S.tiles;
       }
-      E.fw = smem + L.fw;
     } else {
-      E.fw = MIXED ? (const void *)S.fw32 : (const void *)S.fw64;
+      int a0, a1;
+      share(S.nfw, rank, csize, a0, a1);
+      E.sl.fw_lo = a0;
+      E.sl.fw_hi = a1;
+      E.sl.tiles = nullptr;
+      if (S.smem_fw) {
+        double4 *d = (double4 *)(smem + L.fw);
+        for (int i = threadIdx.x; i < a1 - a0; i += blockDim.x) d[i] = S.fw64[a0 + i];
+        E.sl.fw = d - a0;
+      } else {
+        E.sl.fw = S.fw64;
+      }
     }
+    E.sl.ads = E.ads;
+    if (S.ewald) share(S.nk, rank, csize, E.k0, E.k1);
+    else { E.k0 = 0; E.k1 = 0; }
     if (threadIdx.x == 0) {
       E.ctl->nmol = *S.nmol;
       E.ctl->nads = E.ctl->nmol * S.natom;
     }
     __syncthreads();
-    /* adsorbates to shared memory */
+    /* adsorbates to shared memory (full copy in every CTA) */
     for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
       const int mm = i / S.natom, a = i - mm * S.natom;
       double p[3] = {S.ads_xyz[3 * i], S.ads_xyz[3 * i + 1], S.ads_xyz[3 * i + 2]};
@@ -535,67 +658,91 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     }
     __syncthreads();
     const uint64_t step0 = *S.step;
+    const long long t_start = clock64();
     for (long long it = 0; it < nsteps; it++) {
       const uint64_t step = step0 + (uint64_t)it;
       const double u0 = rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOVE);
       int mv = 0;
       while (mv < 3 && u0 >= S.cum[mv]) mv++;
       const int nmol = E.ctl->nmol;
+      share(E.ctl->nads, rank, csize, E.sl.ads_lo, E.sl.ads_hi);
+      const bool lead = rank == 0 && threadIdx.x == 0;
       if (mv <= 1) {
         if (nmol == 0 || (mv == 1 && S.natom == 1)) continue;
-        if (threadIdx.x == 0) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + mv]++; }
+        if (lead) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + mv]++; }
         step_displace<MIXED>(E, step, mv);
       } else if (mv == 2) {
-        if (threadIdx.x == 0) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 2]++; }
+        if (lead) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 2]++; }
         if (nmol >= S.maxmol) {
-          if (threadIdx.x == 0) *S.status |= RGPU_ERR_MAXMOL;
+          if (lead) *S.status |= RGPU_ERR_MAXMOL;
           continue;
         }
         step_swap<MIXED>(E, step, true);
       } else {
-        if (threadIdx.x == 0) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 3]++; }
+        if (lead) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 3]++; }
         if (nmol == 0) continue;
         step_swap<MIXED>(E, step, false);
       }
     }
     __syncthreads();
-    /* write back positions and the molecule count */
-    for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
-      const int mm = i / S.natom, a = i - mm * S.natom;
-      double p[3];
-      atom_xyz(E, mm, a, p);
-      S.ads_xyz[3 * i] = p[0];
-      S.ads_xyz[3 * i + 1] = p[1];
-      S.ads_xyz[3 * i + 2] = p[2];
-    }
-    if (threadIdx.x == 0) {
-      *S.nmol = E.ctl->nmol;
-      *S.step = step0 + (uint64_t)nsteps;
-      for (int c = 0; c < 5; c++) S.counters[RGPU_CNT_PAIRS + c] += (long long)E.ctl->cnt[c];
+    /* write back positions, the molecule count and the work counters */
+    if (rank == 0) {
+      for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
+        const int mm = i / S.natom, a = i - mm * S.natom;
+        double p[3];
+        atom_xyz(E, mm, a, p);
+        S.ads_xyz[3 * i] = p[0];
+        S.ads_xyz[3 * i + 1] = p[1];
+        S.ads_xyz[3 * i + 2] = p[2];
+      }
+      if (threadIdx.x == 0) {
+        *S.nmol = E.ctl->nmol;
+        *S.step = step0 + (uint64_t)nsteps;
+        S.counters[RGPU_CNT_CYCLES] += clock64() - t_start;
+        S.counters[RGPU_CNT_CYC_EVAL] += E.ctl->cyc[0];
+        S.counters[RGPU_CNT_CYC_EWALD] += E.ctl->cyc[1];
+      }
     }
     __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 0; c < 5; c++) atomicAdd((unsigned long long *)&S.counters[RGPU_CNT_PAIRS + c], E.ctl->cnt[c]);
   }
+  /* no CTA may leave while a peer can still read its shared memory */
+  cl.sync();
 }
 
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
-                               int max_ads_atoms, int nfw_smem, int threads, int blocks, cudaStream_t st)
+                               int max_ads_atoms, int fw_items, int tile_items, int cluster, int threads,
+                               cudaStream_t st)
 {
-  size_t smem = rgpu_engine_smem_bytes(mixed, nfw_smem, max_ads_atoms, kw);
+  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nsys * cluster), 1, 1);
+  cfg.blockDim = dim3((unsigned)threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   cudaError_t e;
   if (mixed) {
     e = cudaFuncSetAttribute(rgpu_engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    rgpu_engine_kernel<true><<<blocks, threads, smem, st>>>(d_systems, nsys, nsteps, kw, max_ads_atoms, nfw_smem);
+    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
+                           tile_items);
   } else {
     e = cudaFuncSetAttribute(rgpu_engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    rgpu_engine_kernel<false><<<blocks, threads, smem, st>>>(d_systems, nsys, nsteps, kw, max_ads_atoms, nfw_smem);
+    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<false>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
+                           tile_items);
   }
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
-
-/* ------------------------------------------------------------------------ */
-/* per-call kernels (one thread block per call; the plain path) */
 
 struct CallSmem {
   double res[RGPU_MAX_POS][4];
@@ -603,6 +750,8 @@ struct CallSmem {
   double uv[RGPU_MAX_UNITS], uc[RGPU_MAX_UNITS];
   int uo[RGPU_MAX_UNITS];
   BeadPos pos[RGPU_MAX_POS];
+  float qr2[8 * 64], qq[8 * 64];
+  int qt[8 * 64];
   double red[72];
 };
 
@@ -619,9 +768,16 @@ __global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, con
   load_sys(&S, sysp);
   for (int p = threadIdx.x; p < P; p += blockDim.x) bead_set(sm.pos[p], S, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], atom[p], excl[p]);
   __syncthreads();
-  EvalScratch sc = {sm.uv, sm.uc, sm.uo, nullptr};
-  eval_positions<MIXED>(S, MIXED ? (const void *)S.fw32 : (const void *)S.fw64, ads, nads, sm.pos, P,
-                        pair_check, sm.res, sm.ovf, sc, RGPU_MAX_UNITS);
+  EvalScratch sc = {sm.uv, sm.uc, sm.uo, nullptr, nullptr, sm.qr2, sm.qq, sm.qt};
+  EvalSlice sl;
+  sl.fw = MIXED ? (const void *)S.fw32 : (const void *)S.fw64;
+  sl.tiles = S.tiles;
+  sl.fw_lo = 0;
+  sl.fw_hi = MIXED ? S.ntile : S.nfw;
+  sl.ads = ads;
+  sl.ads_lo = 0;
+  sl.ads_hi = nads;
+  eval_positions<MIXED>(S, sl, sm.pos, P, pair_check, sm.res, sm.ovf, sc, RGPU_MAX_UNITS);
   for (int p = threadIdx.x; p < P; p += blockDim.x) {
     for (int k = 0; k < 4; k++) out[4 * p + k] = sm.res[p][k];
     if (ov) ov[p] = sm.ovf[p];

@@ -54,6 +54,15 @@ __host__ __device__ inline double rgpu_uniform(uint64_t seed, uint32_t sys, uint
   return (double)x * (1.0 / 9007199254740992.0);
 }
 
+/* both uniforms of one Philox block: slots 2*blk and 2*blk+1 */
+__device__ inline void rgpu_uniform_pair(uint64_t seed, uint32_t sys, uint64_t step, uint32_t blk, double *u)
+{
+  uint32_t o[4];
+  rgpu_philox((uint32_t)step, (uint32_t)(step >> 32), blk, sys, (uint32_t)seed, (uint32_t)(seed >> 32), o);
+  u[0] = (double)(((uint64_t)o[0] << 21) ^ (uint64_t)(o[1] >> 11)) * (1.0 / 9007199254740992.0);
+  u[1] = (double)(((uint64_t)o[2] << 21) ^ (uint64_t)(o[3] >> 11)) * (1.0 / 9007199254740992.0);
+}
+
 /* random-draw slots of one MC step (the oracle uses the same numbering) */
 enum {
   SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
@@ -165,7 +174,7 @@ __device__ inline void block_sum2(double &a, double &b, double *red)
 /* ------------------------------------------------------------------------ */
 /* Batched bead energies.
  *
- * For P bead positions, sums over the framework and over the adsorbate atoms
+ * For P bead positions, sums over framework atoms and over the adsorbate atoms
  * not in the bead's own excluded molecule (BeadPos::excl):
  *   res[p] = {host VDW, host real-space charge, adsorbate VDW, adsorbate real}
  * (CalculateFrameworkVDWEnergyAtPosition src/framework_energy.c:60,
@@ -176,17 +185,28 @@ __device__ inline void block_sum2(double &a, double &b, double *red)
  * early-out of the *EnergyDifference routines, e.g.
  * src/framework_energy.c:4988-4990).
  *
- * Work split: the (position, atom-range) units are spread over the warps;
- * lanes stride the atoms of a unit (consecutive records, conflict-free shared
- * loads); a unit's lane sums are warp-reduced and parked in `unit_buf`; the
- * per-position totals are then formed in FP64.
+ * A call covers a slice of the framework ([fw_lo, fw_hi): tiles on the mixed
+ * path, atoms on the FP64 path) and a slice of the adsorbate atoms, so that
+ * the CTAs of a cluster can share one system. Work is split into
+ * (position, slice chunk) units spread over the warps; a unit's lane sums are
+ * warp-reduced and the per-position sums formed in FP64.
+ *
+ * Mixed path: the framework is stored as spatially sorted tiles of 32 atoms
+ * with a bounding box each. Lanes first test 32 tile boxes against the cut-off
+ * sphere at once (a lower bound of the minimum-image distance), then visit
+ * only the surviving tiles; pairs inside the cut-off are appended to a
+ * per-warp queue and evaluated 32 at a time, so the LJ + erfc arithmetic runs
+ * with all lanes busy instead of under a divergent branch.
  */
 struct EvalScratch {
   double *uv;     /* [max units] */
   double *uc;
   int *uo;
-  int *upos;      /* position of the unit */
+  int *upos;      /* unused */
   unsigned long long *cnt;   /* optional {pairs visited, in cut-off, charged in cut-off} */
+  float *qr2;     /* per-warp queue of in-cut-off pairs (mixed path): [nwarps][64] */
+  float *qq;
+  int *qt;
 };
 
 struct EvalPlan {
@@ -194,21 +214,23 @@ struct EvalPlan {
   int nunits;
 };
 
-__device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwarps, int max_units)
+/* nfw: framework items of the slice (tiles or atoms), nads: adsorbate atoms of
+ * the slice, minitems: smallest worthwhile chunk of framework items */
+__device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwarps, int max_units, int minitems)
 {
   EvalPlan pl;
-  int target = 4 * nwarps;
+  int target = 3 * nwarps;
   int cf = (target + P - 1) / P;
-  int maxcf = (nfw + 63) / 64;
+  int maxcf = (nfw + minitems - 1) / minitems;
   if (cf > maxcf) cf = maxcf;
   if (cf < 1) cf = 1;
   int ca = 0;
   if (nads > 0) {
-    ca = (int)((long long)cf * nads / (nfw > 0 ? nfw : 1));
-    int maxca = (nads + 63) / 64;
-    if (ca > maxca) ca = maxca;
+    ca = (nads + 255) / 256;
+    if (ca > cf) ca = cf;
     if (ca < 1) ca = 1;
   }
+  if (nfw == 0) cf = 0;
   while (P * (cf + ca) > max_units && cf > 1) cf--;
   while (P * (cf + ca) > max_units && ca > 1) ca--;
   pl.cf = cf;
@@ -217,52 +239,108 @@ __device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwar
   return pl;
 }
 
-/* one unit of framework work, FP32 path */
-__device__ __forceinline__ void unit_fw_mixed(const RgpuSys &S, const int4 *fw, const BeadPos &b, int lo,
-                                              int hi, bool check, float &av, float &ac, int &ov, int &nin, int &nch)
+/* The LJ + real-space term of one queued pair; lane `lane` takes entry
+ * `lane` of the warp queue. */
+__device__ __forceinline__ void pair_mixed_queued(const RgpuLJf *P, float r2, float qj, bool charged, float qa,
+                                                  float alpha, bool check, float thr, float &av, float &ac, int &ov,
+                                                  int &nch, int type)
+{
+  const RgpuLJf L = P[type];
+  float ri = rsqrtf(r2);
+  ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);      /* one Newton step */
+  const float ir2 = ri * ri;
+  float s6 = L.sig2 * ir2;
+  s6 = s6 * s6 * s6;
+  const float u = fmaf(L.eps4 * s6, s6 - 1.0f, -L.shift);
+  av += u;
+  if (check && u >= thr) ov = 1;
+  if (charged) {
+    nch++;
+    const float r = r2 * ri;
+    const float uc = qa * qj * rgpu_erfc_f(alpha * r) * ri;
+    ac += uc;
+    if (check && uc >= thr) ov = 1;
+  }
+}
+
+/* framework tiles [t0, t1) for bead b, FP32 path (warp-wide) */
+__device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *fw, const TileRec *tiles, int t0, int t1,
+                                                 const BeadPos &b, bool check, float &av, float &ac, int &ov,
+                                                 int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
 {
   const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
   const float rc2 = S.rc2f;
   const float thr = (float)S.overlap;
   const float qa = S.mol_qf[b.atom] * S.coulombf;
   const bool charged = S.fw_charged && qa != 0.0f;
   const float alpha = S.alphaf;
-  for (int s = 0; s < S.nseg; s++) {
-    int a0 = max(lo, S.seg_start[s]), a1 = min(hi, S.seg_start[s + 1]);
-    if (a0 >= a1) continue;
-    const RgpuLJf P = S.ljf_bf[b.atom][s];
-    for (int j = a0 + lane; j < a1; j += 32) {
-      int4 f = fw[j];
-      float dx = __int2float_rn(f.x - b.xi) * sx;
-      float dy = __int2float_rn(f.y - b.yi) * sy;
-      float dz = __int2float_rn(f.z - b.zi) * sz;
-      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      if (r2 < rc2) {
-      nin++;
+  const RgpuLJf *P = S.ljf_bf[b.atom];
+  int qn = 0;
+  for (int tb = t0; tb < t1; tb += 32) {
+    const int t = tb + lane;
+    bool vis = false;
+    if (t < t1) {
+      const TileRec tr = tiles[t];
+      float dx = fmaxf(fabsf(__int2float_rn(tr.c.x - b.xi) * sx) - tr.h.x, 0.0f);
+      float dy = fmaxf(fabsf(__int2float_rn(tr.c.y - b.yi) * sy) - tr.h.y, 0.0f);
+      float dz = fmaxf(fabsf(__int2float_rn(tr.c.z - b.zi) * sz) - tr.h.z, 0.0f);
+      vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
+    }
+    unsigned m = __ballot_sync(RGPU_FULL, vis);
+    while (m) {
+      const int tt = tb + __ffs(m) - 1;
+      m &= m - 1;
+      const int n = tiles[tt].c.w;
+      nvis += n;
+      bool in = false;
+      float r2 = 0.0f;
+      int4 f = make_int4(0, 0, 0, 0);
+      if (lane < n) {
+        f = fw[tt * 32 + lane];
+        const float dx = __int2float_rn(f.x - b.xi) * sx;
+        const float dy = __int2float_rn(f.y - b.yi) * sy;
+        const float dz = __int2float_rn(f.z - b.zi) * sz;
+        r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        in = r2 < rc2;
+      }
+      const unsigned bal = __ballot_sync(RGPU_FULL, in);
+      if (in) {
+        const int p = qn + __popc(bal & lt);
+        qr2[p] = r2;
+        qq[p] = __int_as_float(f.w);
+        qt[p] = f.z & 3;
+      }
+      qn += __popc(bal);
+      if (qn >= 32) {
+        __syncwarp();
+        const float e_r2 = qr2[lane], e_q = qq[lane];
+        const int e_t = qt[lane];
+        float t_r2 = 0.0f, t_q = 0.0f;
+        int t_t = 0;
+        if (lane < qn - 32) { t_r2 = qr2[32 + lane]; t_q = qq[32 + lane]; t_t = qt[32 + lane]; }
+        __syncwarp();
+        if (lane < qn - 32) { qr2[lane] = t_r2; qq[lane] = t_q; qt[lane] = t_t; }
         nin++;
-        float ri = rsqrtf(r2);
-        ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);      /* one Newton step */
-        float ir2 = ri * ri;
-        float s6 = P.sig2 * ir2;
-        s6 = s6 * s6 * s6;
-        float u = fmaf(P.eps4 * s6, s6 - 1.0f, -P.shift);
-        av += u;
-        if (check && u >= thr) ov = 1;
-        if (charged) {
-          nch++;
-          float r = r2 * ri;
-          float uc = qa * __int_as_float(f.w) * rgpu_erfc_f(alpha * r) * ri;
-          ac += uc;
-          if (check && uc >= thr) ov = 1;
-        }
+        pair_mixed_queued(P, e_r2, e_q, charged, qa, alpha, check, thr, av, ac, ov, nch, e_t);
+        qn -= 32;
+        __syncwarp();
       }
     }
   }
+  __syncwarp();
+  if (lane < qn) {
+    nin++;
+    pair_mixed_queued(P, qr2[lane], qq[lane], charged, qa, alpha, check, thr, av, ac, ov, nch, qt[lane]);
+  }
+  __syncwarp();
 }
 
+/* framework atoms [lo, hi) of the type-sorted FP64 layout */
 __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw, const BeadPos &b, int lo,
-                                             int hi, bool check, double &av, double &ac, int &ov, int &nin, int &nch)
+                                             int hi, bool check, double &av, double &ac, int &ov, int &nin, int &nch,
+                                             int &nvis)
 {
   const int lane = threadIdx.x & 31;
   const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
@@ -271,6 +349,7 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
   const double qa = S.mol_q[b.atom] * S.coulomb;
   const bool charged = S.fw_charged && qa != 0.0;
   const double alpha = S.alpha;
+  nvis += hi - lo;
   for (int s = 0; s < S.nseg; s++) {
     int a0 = max(lo, S.seg_start[s]), a1 = min(hi, S.seg_start[s + 1]);
     if (a0 >= a1) continue;
@@ -283,7 +362,6 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
       dz -= Lz * rgpu_nint(dz * iz);
       double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 < rc2) {
-      nin++;
         nin++;
         double s6 = P.sig2 / r2;
         s6 = s6 * s6 * s6;
@@ -303,7 +381,8 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
 }
 
 __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo,
-                                               int hi, int exclude, bool check, float &av, float &ac, int &ov, int &nin, int &nch)
+                                               int hi, int exclude, bool check, float &av, float &ac, int &ov,
+                                               int &nin, int &nch, int &nvis)
 {
   const int lane = threadIdx.x & 31;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
@@ -312,6 +391,7 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
   const float qa = S.mol_qf[b.atom] * S.coulombf;
   const bool charged = S.mol_charged && qa != 0.0f;
   const float alpha = S.alphaf;
+  nvis += hi - lo;
   for (int j = lo + lane; j < hi; j += 32) {
     int4 f = ads[j];
     if ((f.w >> 4) == exclude) continue;
@@ -344,7 +424,8 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
 }
 
 __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *ads, const BeadPos &b, int lo,
-                                              int hi, int exclude, bool check, double &av, double &ac, int &ov, int &nin, int &nch)
+                                              int hi, int exclude, bool check, double &av, double &ac, int &ov,
+                                              int &nin, int &nch, int &nvis)
 {
   const int lane = threadIdx.x & 31;
   const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
@@ -353,6 +434,7 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
   const double qa = S.mol_q[b.atom] * S.coulomb;
   const bool charged = S.mol_charged && qa != 0.0;
   const double alpha = S.alpha;
+  nvis += hi - lo;
   for (int j = lo + lane; j < hi; j += 32) {
     AdsRec64 f = ads[j];
     int tag = (int)f.tag;
@@ -383,44 +465,56 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
   }
 }
 
-/* Evaluates P bead positions. All threads of the block must call it.
- * fw: int4* (MIXED) or double4* (FP64); ads: int4* or AdsRec64*. */
+/* Framework and adsorbate slices of one evaluation */
+struct EvalSlice {
+  const void *fw;          /* int4 atoms (mixed, tiled) or double4 atoms (FP64, type-sorted) */
+  const TileRec *tiles;    /* mixed only */
+  int fw_lo, fw_hi;        /* tiles (mixed) or atoms (FP64) */
+  const void *ads;         /* int4 or AdsRec64 records */
+  int ads_lo, ads_hi;
+};
+
+/* The (position, chunk) units of P positions over the slice: unit u covers
+ * position u / (cf + ca) and writes its FP64 sums and overlap flag to
+ * sc.uv/uc/uo[u]. No block barrier; returns the plan used. */
 template <bool MIXED>
-__device__ void eval_positions(const RgpuSys &S, const void *fw, const void *ads, int nads, const BeadPos *pos,
-                               int P, int pair_check, double (*res)[4], int *ovf,
+__device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
                                EvalScratch sc, int max_units)
 {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const EvalPlan pl = eval_plan(P, S.nfw, nads, nw, max_units);
+  const int nfw = sl.fw_hi - sl.fw_lo, nads = sl.ads_hi - sl.ads_lo;
+  const EvalPlan pl = eval_plan(P, nfw, nads, nw, max_units, MIXED ? 2 : 64);
   const int per = pl.cf + pl.ca;
   for (int u = w; u < pl.nunits; u += nw) {
     const int p = u / per, c = u - p * per;
     const BeadPos b = pos[p];
     const bool check = p < pair_check;
-    int ov = 0, nin = 0, nch = 0;
+    int ov = 0, nin = 0, nch = 0, nvis = 0;
     double v, q;
+    int lo, hi;
+    if (c < pl.cf) {
+      lo = sl.fw_lo + (int)((long long)nfw * c / pl.cf);
+      hi = sl.fw_lo + (int)((long long)nfw * (c + 1) / pl.cf);
+    } else {
+      const int cc = c - pl.cf;
+      lo = sl.ads_lo + (int)((long long)nads * cc / pl.ca);
+      hi = sl.ads_lo + (int)((long long)nads * (cc + 1) / pl.ca);
+    }
     if (MIXED) {
       float av = 0.0f, ac = 0.0f;
-      if (c < pl.cf) {
-        int lo = (int)((long long)S.nfw * c / pl.cf), hi = (int)((long long)S.nfw * (c + 1) / pl.cf);
-        unit_fw_mixed(S, (const int4 *)fw, b, lo, hi, check, av, ac, ov, nin, nch);
-      } else {
-        int cc = c - pl.cf;
-        int lo = (int)((long long)nads * cc / pl.ca), hi = (int)((long long)nads * (cc + 1) / pl.ca);
-        unit_ads_mixed(S, (const int4 *)ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch);
-      }
+      if (c < pl.cf)
+        unit_tiles_mixed(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
+                         sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
+      else
+        unit_ads_mixed(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
       v = (double)warp_sum(av);
       q = (double)warp_sum(ac);
     } else {
       double av = 0.0, ac = 0.0;
-      if (c < pl.cf) {
-        int lo = (int)((long long)S.nfw * c / pl.cf), hi = (int)((long long)S.nfw * (c + 1) / pl.cf);
-        unit_fw_fp64(S, (const double4 *)fw, b, lo, hi, check, av, ac, ov, nin, nch);
-      } else {
-        int cc = c - pl.cf;
-        int lo = (int)((long long)nads * cc / pl.ca), hi = (int)((long long)nads * (cc + 1) / pl.ca);
-        unit_ads_fp64(S, (const AdsRec64 *)ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch);
-      }
+      if (c < pl.cf)
+        unit_fw_fp64(S, (const double4 *)sl.fw, b, lo, hi, check, av, ac, ov, nin, nch, nvis);
+      else
+        unit_ads_fp64(S, (const AdsRec64 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
       v = warp_sum(av);
       q = warp_sum(ac);
     }
@@ -429,10 +523,7 @@ __device__ void eval_positions(const RgpuSys &S, const void *fw, const void *ads
       nin = __reduce_add_sync(RGPU_FULL, (unsigned)nin);
       nch = __reduce_add_sync(RGPU_FULL, (unsigned)nch);
       if (lane == 0) {
-        int lo, hi;
-        if (c < pl.cf) { lo = (int)((long long)S.nfw * c / pl.cf); hi = (int)((long long)S.nfw * (c + 1) / pl.cf); }
-        else { int cc = c - pl.cf; lo = (int)((long long)nads * cc / pl.ca); hi = (int)((long long)nads * (cc + 1) / pl.ca); }
-        atomicAdd(&sc.cnt[0], (unsigned long long)(hi - lo));
+        atomicAdd(&sc.cnt[0], (unsigned long long)nvis);
         atomicAdd(&sc.cnt[1], (unsigned long long)nin);
         atomicAdd(&sc.cnt[2], (unsigned long long)nch);
       }
@@ -443,6 +534,17 @@ __device__ void eval_positions(const RgpuSys &S, const void *fw, const void *ads
       sc.uo[u] = ov;
     }
   }
+  return pl;
+}
+
+/* Evaluates P bead positions over the slice; all threads of the block must
+ * call it. Writes this slice's partial results to res/ovf. */
+template <bool MIXED>
+__device__ void eval_positions(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
+                               double (*res)[4], int *ovf, EvalScratch sc, int max_units)
+{
+  const EvalPlan pl = eval_units<MIXED>(S, sl, pos, P, pair_check, sc, max_units);
+  const int per = pl.cf + pl.ca;
   __syncthreads();
   for (int p = threadIdx.x; p < P; p += blockDim.x) {
     double hv = 0.0, hc = 0.0, av = 0.0, ac = 0.0;
@@ -538,14 +640,16 @@ __device__ __forceinline__ double2 ewald_dS(const typename PhaseT<MIXED>::T *tab
   }
 }
 
-/* Sum over k of the energy change; every thread returns {e_ads, e_host}:
+/* Sum over wave vectors [k0, k1) of the energy change; every thread returns
+ * {e_ads, e_host}:
  * e_ads = sum kf (|S+dS|^2 - |S|^2), e_host = sum kf Re(S_fw^* dS). */
 template <bool MIXED>
 __device__ void ewald_energy_sum(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
-                                 const EwSite *sites, int ns, double &e_ads, double &e_host, double *red)
+                                 const EwSite *sites, int ns, int k0, int k1, double &e_ads, double &e_host,
+                                 double *red)
 {
   double ea = 0.0, eh = 0.0;
-  for (int k = threadIdx.x; k < S.nk; k += blockDim.x) {
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     double2 d = ewald_dS<MIXED>(tab, kw, sites, ns, S.kvec[k]);
     double2 so = S.sk_ads[k];
     double2 sf = S.sk_fw[k];
@@ -558,14 +662,37 @@ __device__ void ewald_energy_sum(const RgpuSys &S, const typename PhaseT<MIXED>:
   e_host = eh;
 }
 
+/* As ewald_energy_sum, without block reduction: warp w leaves its partial
+ * {e_ads, e_host} in red[2w], red[2w+1]. No block barrier. */
+template <bool MIXED>
+__device__ void ewald_energy_warps(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
+                                   const EwSite *sites, int ns, int k0, int k1, double *red)
+{
+  double ea = 0.0, eh = 0.0;
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    double2 d = ewald_dS<MIXED>(tab, kw, sites, ns, S.kvec[k]);
+    double2 so = S.sk_ads[k];
+    double2 sf = S.sk_fw[k];
+    double kf = S.kfactor[k];
+    ea += kf * (2.0 * (so.x * d.x + so.y * d.y) + d.x * d.x + d.y * d.y);
+    eh += kf * (sf.x * d.x + sf.y * d.y);
+  }
+  ea = warp_sum(ea);
+  eh = warp_sum(eh);
+  if ((threadIdx.x & 31) == 0) {
+    red[2 * (threadIdx.x >> 5)] = ea;
+    red[2 * (threadIdx.x >> 5) + 1] = eh;
+  }
+}
+
 /* S_ads(k) += dS(k) (AcceptEwaldAdsorbateMove, src/ewald.c:11732). The same
  * ewald_dS call as in the energy sum, so the stored sums are those the
  * accepted energy was computed with. */
 template <bool MIXED>
 __device__ void ewald_apply(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
-                            int ns)
+                            int ns, int k0, int k1)
 {
-  for (int k = threadIdx.x; k < S.nk; k += blockDim.x) {
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     double2 d = ewald_dS<MIXED>(tab, kw, sites, ns, S.kvec[k]);
     double2 so = S.sk_ads[k];
     S.sk_ads[k] = make_double2(so.x + d.x, so.y + d.y);

@@ -35,7 +35,10 @@ enum {
   RGPU_CNT_CHARGED = 12, /* of those, pairs with a real-space charge term */
   RGPU_CNT_KSITES = 13,  /* wave vector x site products of dS(k) */
   RGPU_CNT_KVEC = 14,    /* wave vectors summed (energy terms) */
-  RGPU_NCNT = 16
+  RGPU_CNT_CYCLES = 15,  /* SM clock cycles the system spent in the engine */
+  RGPU_CNT_CYC_EVAL = 16, /* of those, in pair-energy evaluations (rank 0) */
+  RGPU_CNT_CYC_EWALD = 17, /* of those, in Ewald sums (rank 0) */
+  RGPU_NCNT = 20
 };
 
 /* per-system running energies (internal units, FP64) */
@@ -58,6 +61,14 @@ typedef struct {
 typedef struct {
   float eps4, sig2, shift, pad;
 } RgpuLJf;
+
+/* Tile of the mixed-precision framework layout: 32 spatially close atoms.
+ * c = centre in fixed point with the atom count in .w; h = half extents (A)
+ * such that every atom of the tile lies within +-h of c (minimum image). */
+typedef struct {
+  int4 c;
+  float4 h;
+} TileRec;
 
 typedef struct RgpuSys {
   /* geometry */
@@ -99,8 +110,11 @@ typedef struct RgpuSys {
   uint32_t sys_id;
   int smem_fw;                /* framework staged in shared memory by the engine */
   /* device pointers */
-  const double4 *fw64;        /* [nfw] x, y, z, q */
-  const int4 *fw32;           /* [nfw] fixed-point x, y, z, float bits of q */
+  const double4 *fw64;        /* [nfw] x, y, z, q (sorted by type) */
+  const int4 *fw32;           /* [ntile*32] tiled: fixed-point x, y, z (low 2 bits of z = segment), float bits of q */
+  const TileRec *tiles;       /* [ntile] */
+  int ntile;
+  int pad_tile;
   const char4 *kvec;          /* [nk] */
   const double *kfactor;      /* [nk] */
   const double2 *sk_fw;       /* [nk] */

@@ -29,6 +29,7 @@ EXPORTS = [
     "rgpu_ewald_fourier_difference", "rgpu_ewald_accept", "rgpu_total_energy", "rgpu_grid_build",
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
+    "rgpu_engine_cluster",
 ]
 
 
@@ -226,7 +227,7 @@ class GpuSystem:
 
     def state(self):
         e = np.zeros(8)
-        c = np.zeros(16, np.int64)
+        c = np.zeros(20, np.int64)
         n = C.c_int()
         st = C.c_int()
         step = C.c_ulonglong()
@@ -259,11 +260,13 @@ def grid_interpolate(d_grid_ptr: int, npts, size, shift, cell, xyz) -> np.ndarra
 class Engine:
     """Persistent batched engine over several GpuSystems (rgpu_engine)."""
 
-    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=256):
+    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=256, cluster=0):
         L = load()
         arr = (C.c_void_p * len(systems))(*[s.h for s in systems])
         h = C.c_void_p()
-        _check(L.rgpu_engine_create(C.byref(h), arr, C.c_int(len(systems)), C.c_int(precision), C.c_int(threads)))
+        _check(L.rgpu_engine_create(C.byref(h), arr, C.c_int(len(systems)), C.c_int(precision), C.c_int(threads),
+                                    C.c_int(cluster)))
+        self.cluster = int(L.rgpu_engine_cluster(h))
         self.h = h
         self.systems = list(systems)
 

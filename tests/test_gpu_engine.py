@@ -11,10 +11,10 @@ from golden_cases import load, system_of
 pytestmark = pytest.mark.gpu
 
 
-def engine_run(sysm, mols, nsteps, precision, seed=777, stream_id=3, threads=256, maxmol=64):
+def engine_run(sysm, mols, nsteps, precision, seed=777, stream_id=3, threads=256, maxmol=64, cluster=0):
     g = native.GpuSystem(sysm, maxmol=maxmol, seed=seed, stream_id=stream_id)
     g.set_adsorbates(mols)
-    e = native.Engine([g], precision=precision, threads=threads)
+    e = native.Engine([g], precision=precision, threads=threads, cluster=cluster)
     e.run(nsteps)
     e.sync()
     return g, g.state()
@@ -29,13 +29,16 @@ def oracle_run(sysm, mols, nsteps, seed=777, stream_id=3, maxmol=64):
     return o, st
 
 
-@pytest.mark.parametrize("name", ["co2_tiny", "methane_config0"])
-def test_fp64_engine_reproduces_oracle_trajectory(cuda, name):
+@pytest.mark.parametrize("name,cluster", [("co2_tiny", 1), ("co2_tiny", 2), ("co2_config1", 8),
+                                          ("methane_config0", 2)])
+def test_fp64_engine_reproduces_oracle_trajectory(cuda, name, cluster):
+    """Same counter-based stream, same decisions: the FP64 engine (framework
+    split over `cluster` CTAs) follows the oracle's GCMC trajectory."""
     c = load(name)
     s = system_of(c)
     mols = np.array(c["molecules"])
     n = 300
-    g, st = engine_run(s, mols, n, native.RGPU_FP64)
+    g, st = engine_run(s, mols, n, native.RGPU_FP64, cluster=cluster)
     o, ost = oracle_run(s, mols, n)
     assert st["status"] == 0
     assert st["step"] == n
@@ -48,8 +51,9 @@ def test_fp64_engine_reproduces_oracle_trajectory(cuda, name):
     np.testing.assert_allclose(st["energy"][:6], np.array(ost.u), rtol=1e-9, atol=1e-6)
 
 
-@pytest.mark.parametrize("precision,tol", [(native.RGPU_FP64, 1e-10), (native.RGPU_MIXED, 1e-6)])
-def test_energy_drift(cuda, precision, tol):
+@pytest.mark.parametrize("precision,tol,cluster", [(native.RGPU_FP64, 1e-10, 2), (native.RGPU_MIXED, 1e-6, 2),
+                                                   (native.RGPU_MIXED, 1e-6, 1)])
+def test_energy_drift(cuda, precision, tol, cluster):
     """Running totals after many accepted moves equal a full recomputation
     (the reference's energy-drift check, src/output.c:7032)."""
     c = load("co2_config1")
@@ -58,7 +62,7 @@ def test_energy_drift(cuda, precision, tol):
     g.set_adsorbates(np.array(c["molecules"])[:4])
     e0 = g.total_energy()
     g.set_energy(np.concatenate([e0, [0, 0]]))
-    eng = native.Engine([g], precision=precision)
+    eng = native.Engine([g], precision=precision, cluster=cluster)
     eng.run(2000)
     eng.sync()
     st = g.state()
@@ -104,8 +108,8 @@ def test_mixed_engine_tracks_fp64(cuda):
     c = load("co2_tiny")
     s = system_of(c)
     mols = np.array(c["molecules"])
-    _, a = engine_run(s, mols, 150, native.RGPU_FP64)
-    _, b = engine_run(s, mols, 150, native.RGPU_MIXED)
+    _, a = engine_run(s, mols, 150, native.RGPU_FP64, cluster=2)
+    _, b = engine_run(s, mols, 150, native.RGPU_MIXED, cluster=2)
     np.testing.assert_array_equal(a["counters"][:9], b["counters"][:9])
     kT = units.K_B * s.temperature
     np.testing.assert_allclose(b["energy"][:6], a["energy"][:6], rtol=1e-5, atol=1e-3 * kT)

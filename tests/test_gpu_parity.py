@@ -37,7 +37,7 @@ def mixed_close(a, b, scale, kT):
     a, b, scale = (np.asarray(x, float) for x in (a, b, scale))
     err = np.abs(a - b)
     assert np.all(err <= MIXED_RTOL * (np.abs(b) + scale) + 1e-6 * kT), (a, b, err / (np.abs(b) + scale))
-    assert np.all(err <= 1e-4 * kT), (a, b, err / kT)
+    assert np.all(err <= 1e-4 * kT + 1e-6 * np.abs(b)), (a, b, err / kT)
 
 
 @pytest.fixture(scope="module", params=ENERGY_CASES)
