@@ -507,7 +507,7 @@ static double rng_philox(void *ctx, int slot)
 enum {
   SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
   SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16,       /* 16 + 3*i + {z,y,x} */
-  SLOT_ORIENT_SELECT = 63, SLOT_ORIENT = 64,     /* 64 + 4*i + {X0,Y1,Y2} */
+  SLOT_ORIENT_SELECT = 5, SLOT_ORIENT = 64,      /* 64 + 4*i + {X0,Y1,Y2} */
   SLOT_SPHERE = 192                               /* discarded sphere vectors */
 };
 #define MAX_TRIALS 16

@@ -89,7 +89,7 @@ struct rgpu_system {
 struct rgpu_engine {
   std::vector<rgpu_system *> sys;
   RgpuSys *d_systems;
-  int mixed, threads, kw, max_ads, cluster, fw_items, tile_items;
+  int mixed, threads, kw, max_ads, cluster, fw_items, tile_items, k_items;
   cudaStream_t st;
 };
 
@@ -798,12 +798,24 @@ extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], cons
   return RGPU_SUCCESS;
 }
 
+/* the lookup wraps points into [0, cell) per axis; the grid must span that
+ * range (the grid spans the unit-cell box, src/grids.c:337-359) */
+static bool grid_covers_cell(const int npts[3], const double size[3], const double shift[3], const double cell[3])
+{
+  for (int c = 0; c < 3; c++) {
+    if (npts[c] < 1 || !(size[c] > 0.0) || !(cell[c] > 0.0)) return false;
+    if (shift[c] > 1e-9 * cell[c] || shift[c] + size[c] < cell[c] * (1.0 - 1e-9)) return false;
+  }
+  return true;
+}
+
 extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3],
                                      const double shift[3], const double cell[3], int n, const double *xyz,
                                      double *out)
 {
   if (!d_grid || !npts || !size || !shift || !cell || n < 0 || (n && (!xyz || !out)))
     return fail(RGPU_E_INVALID, "bad argument");
+  if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
   if (n == 0) return RGPU_SUCCESS;
   double *dx = nullptr, *dout = nullptr;
   CK(cudaMalloc((void **)&dx, sizeof(double) * 3 * n));
@@ -849,7 +861,7 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
   e->cluster = cluster ? cluster : auto_cluster(n);
   e->kw = 1;
   e->max_ads = 0;
-  int maxfw = 0, maxtile = 0;
+  int maxfw = 0, maxtile = 0, maxk = 0;
   for (int i = 0; i < n; i++) {
     rgpu_system *s = systems[i];
     if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
@@ -858,6 +870,7 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
     e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
     maxfw = std::max(maxfw, (s->d.nfw + e->cluster - 1) / e->cluster);
     maxtile = std::max(maxtile, (s->h.ntile + e->cluster - 1) / e->cluster);
+    if (s->h.ewald) maxk = std::max(maxk, (s->h.nk + e->cluster - 1) / e->cluster);
   }
   int dev = 0, smem_max = 0;
   cudaGetDevice(&dev);
@@ -869,14 +882,21 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
     e->tile_items = 0;
     e->fw_items = maxfw;
   }
-  if (rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw) > (size_t)smem_max) {
-    e->fw_items = 0;
-    e->tile_items = 0;
-  }
-  if (rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw) > (size_t)smem_max) {
+  /* shared-memory staging, in order of preference: framework share and wave
+   * vectors, framework only, wave vectors only, neither */
+  const int fw_try[4] = {e->fw_items, e->fw_items, 0, 0}, tile_try[4] = {e->tile_items, e->tile_items, 0, 0};
+  const int k_try[4] = {maxk, 0, maxk, 0};
+  int pick = -1;
+  for (int t = 0; t < 4 && pick < 0; t++)
+    if (rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t]) <= (size_t)smem_max)
+      pick = t;
+  if (pick < 0) {
     delete e;
     return fail(RGPU_E_INVALID, "adsorbate capacity does not fit in shared memory");
   }
+  e->fw_items = fw_try[pick];
+  e->tile_items = tile_try[pick];
+  e->k_items = k_try[pick];
   std::vector<RgpuSys> hs(n);
   for (int i = 0; i < n; i++) {
     hs[i] = e->sys[i]->h;
@@ -911,8 +931,8 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   const int n = (int)e->sys.size();
-  CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items, e->cluster,
-                        e->threads, st));
+  CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
+                        e->k_items, e->cluster, e->threads, st));
   for (rgpu_system *s : e->sys) s->records_stale = 1;
   return RGPU_SUCCESS;
 }

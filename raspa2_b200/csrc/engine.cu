@@ -1,16 +1,18 @@
 /* Kernels of the B200 GCMC energy path.
  *
  *  - rgpu_engine_kernel: the persistent batched MC engine. One thread-block
- *    cluster owns one simulation box for the whole launch. The framework is
- *    split between the CTAs of the cluster (each stages its share in shared
- *    memory); every CTA keeps a full copy of the adsorbate records, draws the
- *    same counter-based random numbers and takes the same decisions. Partial
- *    sums of each energy evaluation and of each Ewald sum are combined across
- *    the cluster through distributed shared memory in a fixed rank order, so
- *    all CTAs see bitwise identical totals. Each cluster advances its box by
- *    `nsteps` MC moves (translation, rotation, CBMC insertion, CBMC deletion:
- *    src/mc_moves.c:1529, :2636, :6941, :7150) without returning to the host;
- *    FP64 and mixed runs see identical random streams.
+ *    cluster owns one simulation box for the whole launch. The framework and
+ *    the wave vectors are split between the CTAs of the cluster (each stages
+ *    its share, with its share of S(k), in shared memory); every CTA keeps a
+ *    full copy of the adsorbate records, draws the same counter-based random
+ *    numbers and takes the same decisions. Each energy evaluation leaves
+ *    per-unit partial sums in shared memory; after one cluster barrier the
+ *    lanes that need a total read the partials of every CTA through
+ *    distributed shared memory in a fixed order, so all CTAs see bitwise
+ *    identical totals. Each cluster advances its box by `nsteps` MC moves
+ *    (translation, rotation, CBMC insertion, CBMC deletion: src/mc_moves.c:1529,
+ *    :2636, :6941, :7150) without returning to the host; FP64 and mixed runs
+ *    see identical random streams.
  *  - per-call kernels behind the reference-named C entry points: batched
  *    bead energies, Ewald Fourier difference and accept, structure factors.
  */
@@ -27,18 +29,21 @@ namespace cg = cooperative_groups;
 
 #define RGPU_MAX_UNITS 512
 #define RGPU_MAX_WARPS 32
+#define RGPU_RND 128          /* random slots drawn per MC step */
 
 /* ------------------------------------------------------------------------ */
 /* shared-memory plan of the engine (offsets in bytes from the dynamic base).
  * fw_items: framework records of this CTA's share (atoms; tiles*32 on the
- * mixed path), tiles: tile records of the share (mixed only). */
+ * mixed path), tiles: tile records of the share (mixed only), k_items: wave
+ * vectors of the share staged with their S(k) (0: read from global memory). */
 struct EngineLayout {
-  size_t sys, fw, tiles, ads, xyz, pos, res, part, ovf, opart, uv, uc, uo, q, sites, tab, red, ctl, total;
+  size_t sys, fw, tiles, ads, xyz, pos, uv, uc, uo, q, sites, tab, red, kvec, kf, skfw, skads, ctl, total;
 };
 
 __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
-__host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw)
+__host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw,
+                                                      int k_items)
 {
   EngineLayout L;
   size_t o = 0;
@@ -48,44 +53,47 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.ads = o; o = rgpu_align(o + (size_t)max_ads_atoms * (mixed ? sizeof(int4) : sizeof(AdsRec64)));
   L.xyz = o; o = rgpu_align(o + (mixed ? (size_t)max_ads_atoms * 3 * sizeof(double) : 0));
   L.pos = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(BeadPos));
-  L.res = o; o = rgpu_align(o + RGPU_MAX_POS * 4 * sizeof(double));
-  L.part = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * 4 * sizeof(double));   /* double-buffered partials */
-  L.ovf = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(int));
-  L.opart = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * sizeof(int));
-  L.uv = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
-  L.uc = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
-  L.uo = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(int));
+  L.uv = o; o = rgpu_align(o + 2 * RGPU_MAX_UNITS * sizeof(double));    /* double-buffered unit partials */
+  L.uc = o; o = rgpu_align(o + 2 * RGPU_MAX_UNITS * sizeof(double));
+  L.uo = o; o = rgpu_align(o + 2 * RGPU_MAX_UNITS * sizeof(int));
   L.q = o; o = rgpu_align(o + (mixed ? (size_t)RGPU_MAX_WARPS * 64 * 12 : 0));
   L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
   L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed ? sizeof(float2) : sizeof(double2)));
-  L.red = o; o = rgpu_align(o + 72 * sizeof(double));
-  L.ctl = o; o = rgpu_align(o + 128 * sizeof(double));
+  L.red = o; o = rgpu_align(o + 2 * 2 * RGPU_MAX_WARPS * sizeof(double));
+  L.kvec = o; o = rgpu_align(o + (size_t)k_items * sizeof(char4));
+  L.kf = o; o = rgpu_align(o + (size_t)k_items * sizeof(double));
+  L.skfw = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
+  L.skads = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
+  L.ctl = o; o = rgpu_align(o + 4096);
   L.total = o;
   return L;
 }
 
-size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw)
+size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw, int k_items)
 {
-  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw).total;
+  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw, k_items).total;
 }
 
 /* broadcast/control block in shared memory */
 struct Ctl {
-  double u[4];        /* energies of the chosen configuration */
+  double rnd[2][RGPU_RND];    /* uniforms by slot, double-buffered by step parity */
+  double energy[RGPU_NE];     /* running energies (written back by rank 0) */
+  long long cnt[RGPU_CNT_PAIRS];  /* move counters (rank 0's written back) */
+  BeadPos first;              /* chosen first bead */
+  double u[4];                /* energies of the chosen configuration */
   double rosen;
   double dl[4];
-  double ewp[2][2];   /* double-buffered Ewald partials {e_ads, e_host} */
-  double e_ads, e_host;
   int nmol;
   int fail;
   int accept;
   int sel;
-  int nads;           /* adsorbate atoms = nmol * natom */
-  int xbuf;           /* exchange buffer index */
+  int nads;                   /* adsorbate atoms = nmol * natom */
+  int status;                 /* RGPU_ERR_* bits */
   /* work done: pairs visited, in cut-off, charged in cut-off, k x site, k */
-  unsigned long long cnt[5];
-  long long cyc[2];   /* clock cycles in evaluations and Ewald sums */
+  unsigned long long work[5];
+  long long cyc[2];           /* clock cycles in evaluations and Ewald sums */
 };
+static_assert(sizeof(Ctl) <= 4096, "control block exceeds its shared-memory slot");
 
 template <bool MIXED>
 struct Eng {
@@ -94,18 +102,19 @@ struct Eng {
   void *ads;                 /* int4[] or AdsRec64[] (full copy) */
   double (*xyz)[3];          /* FP64 positions (MIXED: separate array; FP64: inside ads records) */
   BeadPos *pos;
-  double (*res)[4];          /* combined results */
-  double (*part)[RGPU_MAX_POS][4];
-  int *ovf;
-  int (*opart)[RGPU_MAX_POS];
+  double *uv, *uc;           /* [2][RGPU_MAX_UNITS] */
+  int *uo;
   EvalScratch sc;
   EwSite *sites;
   typename PhaseT<MIXED>::T *tab;
   int kw;
   int k0, k1;                /* this CTA's wave vectors */
-  double *red;
+  double *red;               /* [2][2*RGPU_MAX_WARPS] */
   Ctl *ctl;
+  const double *rnd;         /* this step's uniforms */
   int rank, csize;
+  int xb;                    /* exchange buffer (same sequence in every thread and CTA) */
+  int nfw_items;             /* framework items (tiles or atoms) split over the cluster */
 };
 
 /* position of atom a of molecule m */
@@ -170,110 +179,166 @@ __device__ __forceinline__ void random_rotation(double x0, double y1, double y2,
   R[1][0] = 2.0 * u2 * u1 + ce * u3;
 }
 
-/* SelectTrialPosition, src/cbmc.c:563-599 */
-__device__ inline int select_trial(const double *bf, const int *ov, int n, double u)
+/* share [lo, hi) of n items for rank r of c */
+__device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 {
-  double largest = -DBL_MAX, sum = 0.0, w[RGPU_MAX_TRIALS];
-  for (int i = 0; i < n; i++)
-    if (!ov[i] && bf[i] > largest) largest = bf[i];
-  for (int i = 0; i < n; i++) {
-    w[i] = ov[i] ? 0.0 : exp(bf[i] - largest);
-    sum += w[i];
-  }
-  int sel = 0;
-  double cum = w[0], ws = u * sum;
-  while (cum < ws && sel < n - 1) cum += w[++sel];
-  return sel;
+  lo = (int)((long long)n * r / c);
+  hi = (int)((long long)n * (r + 1) / c);
 }
 
-/* Evaluates P positions on this CTA's share and combines the partials of all
- * CTAs of the cluster (rank order) into E.res / E.ovf. All threads call. */
+/* Pair evaluation of P positions on this CTA's share, then one cluster
+ * barrier; the totals are read with gather(). All threads call. */
 template <bool MIXED>
-__device__ void engine_eval(const Eng<MIXED> &E, int P, int pair_check)
+__device__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
 {
   Ctl &C = *E.ctl;
-  const int b = C.xbuf;
   const long long t0 = clock64();
-  eval_positions<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.part[b], E.opart[b], E.sc, RGPU_MAX_UNITS);
-  if (E.csize > 1) {
-    cg::cluster_group cl = cg::this_cluster();
-    cl.sync();
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-      double s[4] = {0.0, 0.0, 0.0, 0.0};
-      int o = 0;
-      for (int r = 0; r < E.csize; r++) {
-        const double (*pr)[4] = (const double (*)[4])cl.map_shared_rank((double *)E.part[b], r);
-        const int *orr = cl.map_shared_rank((int *)E.opart[b], r);
-        for (int k = 0; k < 4; k++) s[k] += pr[p][k];
-        o |= orr[p];
-      }
-      for (int k = 0; k < 4; k++) E.res[p][k] = s[k];
-      E.ovf[p] = o;
-    }
-  } else {
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-      for (int k = 0; k < 4; k++) E.res[p][k] = E.part[b][p][k];
-      E.ovf[p] = E.opart[b][p];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    C.xbuf ^= 1;
-    C.cyc[0] += clock64() - t0;
-  }
-  __syncthreads();
+  EvalScratch sc = E.sc;
+  sc.uv = E.uv + E.xb * RGPU_MAX_UNITS;
+  sc.uc = E.uc + E.xb * RGPU_MAX_UNITS;
+  sc.uo = E.uo + E.xb * RGPU_MAX_UNITS;
+  eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, sc, RGPU_MAX_UNITS);
+  cg::this_cluster().sync();
+  if (threadIdx.x == 0) C.cyc[0] += clock64() - t0;
 }
 
-/* Ewald difference for the sites in E.sites[0..ns): this CTA's wave vectors,
- * then the cluster sum. All threads call. */
+/* the unit plan CTA q used for P positions (eval_units with q's slice) */
 template <bool MIXED>
-__device__ void engine_ewald(const Eng<MIXED> &E, int ns, double &e_ads, double &e_host)
+__device__ __forceinline__ EvalPlan rank_plan(const Eng<MIXED> &E, int q, int P)
+{
+  int f0, f1, a0, a1;
+  share(E.nfw_items, q, E.csize, f0, f1);
+  share(E.ctl->nads, q, E.csize, a0, a1);
+  return eval_plan(P, f1 - f0, a1 - a0, blockDim.x >> 5, RGPU_MAX_UNITS, MIXED ? 2 : 64);
+}
+
+/* Totals of position p of the last evaluation of P positions (buffer b),
+ * summed over the cluster's CTAs in rank order and over their units in
+ * order. */
+template <bool MIXED>
+__device__ __forceinline__ void gather(const Eng<MIXED> &E, int b, int P, int p, double *r, int &ov)
+{
+  cg::cluster_group cl = cg::this_cluster();
+  r[0] = r[1] = r[2] = r[3] = 0.0;
+  ov = 0;
+  for (int q = 0; q < E.csize; q++) {
+    const double *uv = E.csize > 1 ? cl.map_shared_rank(E.uv, q) : E.uv;
+    const double *uc = E.csize > 1 ? cl.map_shared_rank(E.uc, q) : E.uc;
+    const int *uo = E.csize > 1 ? cl.map_shared_rank(E.uo, q) : E.uo;
+    const EvalPlan pl = rank_plan(E, q, P);
+    const int cf = pl.cf, per = pl.cf + pl.ca;
+    for (int c = 0; c < per; c++) {
+      const int u = b * RGPU_MAX_UNITS + p * per + c;
+      if (c < cf) { r[0] += uv[u]; r[1] += uc[u]; }
+      else { r[2] += uv[u]; r[3] += uc[u]; }
+      ov |= uo[u];
+    }
+  }
+}
+
+/* Ewald sum over this CTA's wave vectors for the sites in E.sites[0..ns),
+ * warp partials left in E.red[b]; one cluster barrier. All threads call. */
+template <bool MIXED>
+__device__ void engine_ewald(Eng<MIXED> &E, int ns)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
   ewald_phases<MIXED>(*E.S, E.sites, ns, E.tab, E.kw);
   if (threadIdx.x == 0) {
-    C.cnt[3] += (unsigned long long)(E.k1 - E.k0) * ns;
-    C.cnt[4] += (unsigned long long)(E.k1 - E.k0);
+    C.work[3] += (unsigned long long)(E.k1 - E.k0) * ns;
+    C.work[4] += (unsigned long long)(E.k1 - E.k0);
   }
   __syncthreads();
-  double ea, eh;
-  ewald_energy_sum<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, E.k0, E.k1, ea, eh, E.red);
-  if (E.csize > 1) {
-    const int b = C.xbuf;
-    if (threadIdx.x == 0) { C.ewp[b][0] = ea; C.ewp[b][1] = eh; }
-    cg::cluster_group cl = cg::this_cluster();
-    cl.sync();
-    ea = 0.0;
-    eh = 0.0;
-    for (int r = 0; r < E.csize; r++) {
-      const Ctl *cr = cl.map_shared_rank(E.ctl, r);
-      ea += cr->ewp[b][0];
-      eh += cr->ewp[b][1];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) C.xbuf ^= 1;
-    __syncthreads();
-  }
+  ewald_energy_warps<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, E.k0, E.k1, E.red + E.xb * 2 * RGPU_MAX_WARPS);
+  cg::this_cluster().sync();
   if (threadIdx.x == 0) C.cyc[1] += clock64() - t0;
-  e_ads = ea;
-  e_host = eh;
+}
+
+/* cluster total of the last Ewald sum (buffer b) */
+template <bool MIXED>
+__device__ __forceinline__ void gather_ewald(const Eng<MIXED> &E, int b, double &ea, double &eh)
+{
+  cg::cluster_group cl = cg::this_cluster();
+  ea = eh = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int q = 0; q < E.csize; q++) {
+    const double *red = E.csize > 1 ? cl.map_shared_rank(E.red, q) : E.red;
+    for (int w = 0; w < nw; w++) {
+      ea += red[b * 2 * RGPU_MAX_WARPS + 2 * w];
+      eh += red[b * 2 * RGPU_MAX_WARPS + 2 * w + 1];
+    }
+  }
+}
+
+/* Warp 0: Rosenbluth bookkeeping of n trials (lane t = trial t, nb beads each
+ * at positions t*nb + j of buffer b). First bead (nb = 1, first = true):
+ * overlap when any energy reaches the criterion (src/cbmc.c:699-701);
+ * orientations: when a bead's host VDW energy does (src/cbmc.c:1210-1215).
+ * LJ biasing (src/cbmc.c:734-735, :1432-1436). Selection as
+ * SelectTrialPosition (src/cbmc.c:563-599). Lane 0 leaves the weight sum
+ * (w_sum = sum exp(bf)), the selected trial and its energies in Ctl. */
+template <bool MIXED>
+__device__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool first, bool select, double usel,
+                            double &w_sum, int &sel, double *usum, int &any)
+{
+  const int lane = threadIdx.x & 31;
+  const RgpuSys &S = *E.S;
+  double e[4] = {0.0, 0.0, 0.0, 0.0};
+  int ov = 0;
+  double bf = 0.0;
+  if (lane < n) {
+    for (int j = 0; j < nb; j++) {
+      double r[4];
+      int o;
+      gather(E, b, n * nb, lane * nb + j, r, o);
+      if (first) ov |= (r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap);
+      else ov |= (r[0] >= S.overlap);
+      for (int k = 0; k < 4; k++) e[k] += r[k];
+    }
+    bf = -S.beta * (e[0] + e[2]);
+  }
+  const bool valid = lane < n && !ov;
+  const double w = valid ? exp(bf) : 0.0;
+  double largest = valid ? bf : -DBL_MAX;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) largest = fmax(largest, __shfl_xor_sync(RGPU_FULL, largest, o));
+  const double ws = valid ? exp(bf - largest) : 0.0;
+  const unsigned okmask = __ballot_sync(RGPU_FULL, valid);
+  any = okmask != 0u;
+  /* the sums run in trial order, as the reference's loops do */
+  double wsum = 0.0, shsum = 0.0;
+  for (int t = 0; t < n; t++) {
+    wsum += __shfl_sync(RGPU_FULL, w, t);
+    shsum += __shfl_sync(RGPU_FULL, ws, t);
+  }
+  int s = 0;
+  if (select && any) {
+    const double target = usel * shsum;
+    double cum = __shfl_sync(RGPU_FULL, ws, 0);
+    while (cum < target && s < n - 1) {
+      s++;
+      cum += __shfl_sync(RGPU_FULL, ws, s);
+    }
+  }
+  w_sum = wsum;
+  sel = s;
+  for (int k = 0; k < 4; k++) usum[k] = __shfl_sync(RGPU_FULL, e[k], s);
 }
 
 /* ------------------------------------------------------------------------ */
 /* translation (mv=0) and rotation (mv=1):
  * TranslationMoveAdsorbate src/mc_moves.c:1529-1762, RotationMoveAdsorbate :2636 */
 template <bool MIXED>
-__device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
+__device__ void step_displace(Eng<MIXED> &E, int mv)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
+  const double *R = E.rnd;
   const int na = S.natom, nmol = C.nmol;
-  const bool lead = E.rank == 0 && threadIdx.x == 0;
-  int m = (int)(rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOLECULE) * nmol);
+  int m = (int)(R[SLOT_MOLECULE] * nmol);
   if (m >= nmol) m = nmol - 1;
-  const double vnew = 2.0 * rgpu_uniform(S.seed, S.sys_id, step, SLOT_VNEW) - 1.0;
-  int axis = (int)(3.0 * rgpu_uniform(S.seed, S.sys_id, step, SLOT_AXIS));
+  const double vnew = 2.0 * R[SLOT_VNEW] - 1.0;
+  int axis = (int)(3.0 * R[SLOT_AXIS]);
   if (axis > 2) axis = 2;
   if (threadIdx.x < na) {
     const int a = threadIdx.x;
@@ -298,27 +363,42 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
   }
   __syncthreads();
   engine_eval<MIXED>(E, 2 * na, na);
-  if (threadIdx.x == 0) {
-    int ov = 0;
-    double dl[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int a = 0; a < na; a++) {
-      ov |= E.ovf[a];
-      for (int k = 0; k < 4; k++) dl[k] += E.res[a][k] - E.res[na + a][k];
+  const int be = E.xb;
+  E.xb ^= 1;
+  if (threadIdx.x < 32) {
+    /* lane a: totals of new position a and old position a (a < na <= 8) */
+    const int a = threadIdx.x;
+    double rn[4] = {0.0, 0.0, 0.0, 0.0}, ro[4] = {0.0, 0.0, 0.0, 0.0};
+    int o1 = 0, o2 = 0;
+    if (a < na) {
+      gather(E, be, 2 * na, a, rn, o1);
+      gather(E, be, 2 * na, na + a, ro, o2);
     }
-    C.fail = ov;
-    for (int k = 0; k < 4; k++) C.dl[k] = dl[k];
+    const int ov = __any_sync(RGPU_FULL, o1);
+    double dl[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j = 0; j < na; j++)
+      for (int k = 0; k < 4; k++)
+        dl[k] += __shfl_sync(RGPU_FULL, rn[k], j) - __shfl_sync(RGPU_FULL, ro[k], j);
+    if (a == 0) {
+      C.fail = ov;
+      for (int k = 0; k < 4; k++) C.dl[k] = dl[k];
+      if (ov) C.cnt[RGPU_CNT_OVERLAP]++;
+    }
   }
   __syncthreads();
-  if (C.fail) {
-    if (lead) S.counters[RGPU_CNT_OVERLAP]++;
-    return;
-  }
-  double ea = 0.0, eh = 0.0;
+  if (C.fail) return;
   const bool ew = S.ewald && S.mol_charged;
-  if (ew) engine_ewald<MIXED>(E, 2 * na, ea, eh);
+  int bw = 0;
+  if (ew) {
+    engine_ewald<MIXED>(E, 2 * na);
+    bw = E.xb;
+    E.xb ^= 1;
+  }
   if (threadIdx.x == 0) {
     double d_ads = 0.0, d_host = 0.0;
     if (ew) {
+      double ea, eh;
+      gather_ewald(E, bw, ea, eh);
       /* exclusions cancel for a rigid displacement but are kept for parity */
       double xn[RGPU_MAX_ATOMS][3], xo[RGPU_MAX_ATOMS][3];
       for (int a = 0; a < na; a++) {
@@ -328,18 +408,17 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
       ewald_finish(S, ea, eh, ewald_exclusion(S, xn), ewald_exclusion(S, xo), 0, 0.0, d_ads, d_host);
     }
     double du = C.dl[0] + C.dl[1] + C.dl[2] + C.dl[3] + d_ads + d_host;
-    double u = rgpu_uniform(S.seed, S.sys_id, step, SLOT_ACCEPT);
     double pacc = exp(-S.beta * du);
-    if (E.rank == 0 && !isfinite(du)) *S.status |= RGPU_ERR_NONFINITE;
-    C.accept = u < pacc;
-    if (C.accept && E.rank == 0) {
-      S.counters[RGPU_CNT_ACCEPT + mv]++;
-      S.energy[RGPU_E_HOST_VDW] += C.dl[0];
-      S.energy[RGPU_E_HOST_REAL] += C.dl[1];
-      S.energy[RGPU_E_ADS_VDW] += C.dl[2];
-      S.energy[RGPU_E_ADS_REAL] += C.dl[3];
-      S.energy[RGPU_E_HOST_FOURIER] += d_host;
-      S.energy[RGPU_E_ADS_FOURIER] += d_ads;
+    if (!isfinite(du)) C.status |= RGPU_ERR_NONFINITE;
+    C.accept = R[SLOT_ACCEPT] < pacc;
+    if (C.accept) {
+      C.cnt[RGPU_CNT_ACCEPT + mv]++;
+      C.energy[RGPU_E_HOST_VDW] += C.dl[0];
+      C.energy[RGPU_E_HOST_REAL] += C.dl[1];
+      C.energy[RGPU_E_ADS_VDW] += C.dl[2];
+      C.energy[RGPU_E_ADS_REAL] += C.dl[3];
+      C.energy[RGPU_E_HOST_FOURIER] += d_host;
+      C.energy[RGPU_E_ADS_FOURIER] += d_ads;
     }
   }
   __syncthreads();
@@ -349,8 +428,8 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
       atom_store(E, m, threadIdx.x, p);
     }
     if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, 2 * na, E.k0, E.k1);
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 /* ------------------------------------------------------------------------ */
@@ -361,16 +440,15 @@ __device__ void step_displace(const Eng<MIXED> &E, uint64_t step, int mv)
  * ComputeExternalEnergies :1154-1478, LJ biasing; acceptance of
  * SwapAddAdsorbateMove src/mc_moves.c:7016 and SwapRemoveAdsorbateMove :7228. */
 template <bool MIXED>
-__device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
+__device__ void step_swap(Eng<MIXED> &E, bool insert)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
   const int na = S.natom, sb = S.start_bead, nmol = C.nmol;
   const int nf = S.ntrial_first, nt = S.ntrial;
-  const bool lead = E.rank == 0 && threadIdx.x == 0;
   int m = nmol;
   if (!insert) {
-    m = (int)(rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOLECULE) * nmol);
+    m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
     if (m >= nmol) m = nmol - 1;
   }
   const int exclude = insert ? -1 : m;
@@ -381,42 +459,34 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
     if (!insert && i == 0) {
       atom_xyz(E, m, sb, p);
     } else {
-      double sz = rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST + 3 * i + 0);
-      double sy = rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST + 3 * i + 1);
-      double sx = rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST + 3 * i + 2);
-      p[0] = S.box[0] * sx; p[1] = S.box[1] * sy; p[2] = S.box[2] * sz;
+      p[0] = S.box[0] * E.rnd[SLOT_FIRST + 3 * i + 2];
+      p[1] = S.box[1] * E.rnd[SLOT_FIRST + 3 * i + 1];
+      p[2] = S.box[2] * E.rnd[SLOT_FIRST + 3 * i + 0];
     }
     bead_set(E.pos[i], S, p[0], p[1], p[2], sb, exclude);
   }
   __syncthreads();
   engine_eval<MIXED>(E, nf, 0);
-  if (threadIdx.x == 0) {
-    double bf[RGPU_MAX_TRIALS];
-    int ov[RGPU_MAX_TRIALS], any = 0;
-    double w1 = 0.0;
-    for (int i = 0; i < nf; i++) {
-      ov[i] = (E.res[i][0] >= S.overlap || E.res[i][1] >= S.overlap || E.res[i][2] >= S.overlap ||
-               E.res[i][3] >= S.overlap);
-      bf[i] = ov[i] ? 0.0 : -S.beta * (E.res[i][0] + E.res[i][2]);
-      if (!ov[i]) { any = 1; w1 += exp(bf[i]); }
+  int b1 = E.xb;
+  E.xb ^= 1;
+  if (threadIdx.x < 32) {
+    double wsum, u[4];
+    int sel, any;
+    cbmc_trials(E, b1, nf, 1, true, insert, E.rnd[SLOT_FIRST_SELECT], wsum, sel, u, any);
+    if (threadIdx.x == 0) {
+      C.rosen = wsum / (double)nf;
+      C.fail = !any || (insert && C.rosen < 1e-150);
+      C.sel = sel;
+      for (int k = 0; k < 4; k++) C.u[k] = u[k];
+      C.first = E.pos[sel];
+      if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
     }
-    int sel = 0;
-    C.fail = !any;
-    if (any && insert) sel = select_trial(bf, ov, nf, rgpu_uniform(S.seed, S.sys_id, step, SLOT_FIRST_SELECT));
-    C.rosen = w1 / (double)nf;
-    if (insert && C.rosen < 1e-150) C.fail = 1;
-    C.sel = sel;
-    for (int k = 0; k < 4; k++) C.u[k] = E.res[sel][k];
   }
   __syncthreads();
-  if (C.fail) {
-    if (lead) S.counters[RGPU_CNT_OVERLAP]++;
-    return;
-  }
-  const BeadPos first = E.pos[C.sel];
-  __syncthreads();
+  if (C.fail) return;
   const int nb = na - 1;   /* beads grown per orientation trial */
   if (na > 1) {
+    const BeadPos first = C.first;
     if (threadIdx.x < nt) {
       const int t = threadIdx.x;
       if (!insert && t == 0) {
@@ -430,9 +500,8 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
         }
       } else {
         double R[3][3];
-        random_rotation(rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT + 4 * t + 0),
-                        rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT + 4 * t + 1),
-                        rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT + 4 * t + 2), R);
+        random_rotation(E.rnd[SLOT_ORIENT + 4 * t + 0], E.rnd[SLOT_ORIENT + 4 * t + 1],
+                        E.rnd[SLOT_ORIENT + 4 * t + 2], R);
         int j = 0;
         for (int a = 0; a < na; a++) {
           if (a == sb) continue;
@@ -449,42 +518,31 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
     }
     __syncthreads();
     engine_eval<MIXED>(E, nt * nb, 0);
-    if (threadIdx.x == 0) {
-      double bf[RGPU_MAX_TRIALS], et[RGPU_MAX_TRIALS][4];
-      int ov[RGPU_MAX_TRIALS], any = 0;
-      double w = 0.0;
-      for (int t = 0; t < nt; t++) {
-        ov[t] = 0;
-        for (int k = 0; k < 4; k++) et[t][k] = 0.0;
-        for (int j = 0; j < nb; j++) {
-          const double *r = E.res[t * nb + j];
-          if (r[0] >= S.overlap) ov[t] = 1;
-          for (int k = 0; k < 4; k++) et[t][k] += r[k];
+    const int b2 = E.xb;
+    E.xb ^= 1;
+    if (threadIdx.x < 32) {
+      double wsum, u[4];
+      int sel, any;
+      cbmc_trials(E, b2, nt, nb, false, insert, E.rnd[SLOT_ORIENT_SELECT], wsum, sel, u, any);
+      if (threadIdx.x == 0) {
+        if (!any) C.fail = 1;
+        else {
+          C.rosen *= wsum / (double)nt;
+          if (insert && C.rosen < 1e-150) C.fail = 1;
+          for (int k = 0; k < 4; k++) C.u[k] += u[k];
         }
-        bf[t] = ov[t] ? 0.0 : -S.beta * (et[t][0] + et[t][2]);
-        if (!ov[t]) { any = 1; w += exp(bf[t]); }
+        C.sel = sel;
+        if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
       }
-      int iw = 0;
-      if (!any) C.fail = 1;
-      else {
-        if (insert) iw = select_trial(bf, ov, nt, rgpu_uniform(S.seed, S.sys_id, step, SLOT_ORIENT_SELECT));
-        C.rosen *= w / (double)nt;
-        if (insert && C.rosen < 1e-150) C.fail = 1;
-        for (int k = 0; k < 4; k++) C.u[k] += et[iw][k];
-      }
-      C.sel = iw;
     }
     __syncthreads();
-    if (C.fail) {
-      if (lead) S.counters[RGPU_CNT_OVERLAP]++;
-      return;
-    }
+    if (C.fail) return;
   }
   /* sites of the chosen configuration: first bead + beads of trial C.sel */
   if (threadIdx.x < na) {
     const int a = threadIdx.x;
     BeadPos bp;
-    if (a == sb) bp = first;
+    if (a == sb) bp = C.first;
     else {
       int j = a < sb ? a : a - 1;
       bp = E.pos[C.sel * nb + j];
@@ -493,14 +551,20 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
     E.sites[a].q = insert ? S.mol_q[a] : -S.mol_q[a];
   }
   __syncthreads();
-  double ea = 0.0, eh = 0.0;
   const bool ew = S.ewald && S.mol_charged;
-  if (ew) engine_ewald<MIXED>(E, na, ea, eh);
+  int bw = 0;
+  if (ew) {
+    engine_ewald<MIXED>(E, na);
+    bw = E.xb;
+    E.xb ^= 1;
+  }
   if (threadIdx.x == 0) {
     /* LJ-biasing correction, src/cbmc.c:3171-3178 / :3044-3051 */
     double rosen = C.rosen * exp(-S.beta * (C.u[1] + C.u[3]));
     double d_ads = 0.0, d_host = 0.0;
     if (ew) {
+      double ea, eh;
+      gather_ewald(E, bw, ea, eh);
       double x[RGPU_MAX_ATOMS][3];
       for (int a = 0; a < na; a++) { x[a][0] = E.sites[a].b.x; x[a][1] = E.sites[a].b.y; x[a][2] = E.sites[a].b.z; }
       double ex = ewald_exclusion(S, x);
@@ -508,22 +572,21 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
       if (insert) ewald_finish(S, ea, eh, ex, 0.0, 1, net, d_ads, d_host);
       else ewald_finish(S, ea, eh, 0.0, ex, -1, net, d_ads, d_host);
     }
-    double u = rgpu_uniform(S.seed, S.sys_id, step, SLOT_ACCEPT);
     double pacc;
     if (insert) pacc = rosen * exp(-S.beta * (d_ads + d_host)) * S.fugacity_beta_v / (1.0 + nmol);
     else pacc = (double)nmol / (rosen * exp(S.beta * (d_ads + d_host)) * S.fugacity_beta_v);
-    if (E.rank == 0 && !(pacc == pacc)) *S.status |= RGPU_ERR_NONFINITE;
-    C.accept = u < pacc;
+    if (!(pacc == pacc)) C.status |= RGPU_ERR_NONFINITE;
+    C.accept = E.rnd[SLOT_ACCEPT] < pacc;
     const int mv = insert ? 2 : 3;
-    if (C.accept && E.rank == 0) {
-      S.counters[RGPU_CNT_ACCEPT + mv]++;
+    if (C.accept) {
+      C.cnt[RGPU_CNT_ACCEPT + mv]++;
       double sgn = insert ? 1.0 : -1.0;
-      S.energy[RGPU_E_HOST_VDW] += sgn * C.u[0];
-      S.energy[RGPU_E_HOST_REAL] += sgn * C.u[1];
-      S.energy[RGPU_E_ADS_VDW] += sgn * C.u[2];
-      S.energy[RGPU_E_ADS_REAL] += sgn * C.u[3];
-      S.energy[RGPU_E_HOST_FOURIER] += d_host;
-      S.energy[RGPU_E_ADS_FOURIER] += d_ads;
+      C.energy[RGPU_E_HOST_VDW] += sgn * C.u[0];
+      C.energy[RGPU_E_HOST_REAL] += sgn * C.u[1];
+      C.energy[RGPU_E_ADS_VDW] += sgn * C.u[2];
+      C.energy[RGPU_E_ADS_REAL] += sgn * C.u[3];
+      C.energy[RGPU_E_HOST_FOURIER] += d_host;
+      C.energy[RGPU_E_ADS_FOURIER] += d_ads;
     }
   }
   __syncthreads();
@@ -548,8 +611,8 @@ __device__ void step_swap(const Eng<MIXED> &E, uint64_t step, bool insert)
       C.nmol = insert ? nmol + 1 : nmol - 1;
       C.nads = C.nmol * na;
     }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 /* ------------------------------------------------------------------------ */
@@ -562,38 +625,29 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
   __syncthreads();
 }
 
-/* share [lo, hi) of n items for rank r of c */
-__device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
-{
-  lo = (int)((long long)n * r / c);
-  hi = (int)((long long)n * (r + 1) / c);
-}
-
 template <bool MIXED>
 __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps, int kw,
-                                                          int max_ads_atoms, int fw_items, int tile_items)
+                                                          int max_ads_atoms, int fw_items, int tile_items,
+                                                          int k_items)
 {
   extern __shared__ __align__(256) unsigned char smem[];
   cg::cluster_group cl = cg::this_cluster();
   const int csize = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
   const int sysi = blockIdx.x / csize;
-  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw);
+  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw, k_items);
   if (sysi < nsys) {
     Eng<MIXED> E;
     E.rank = rank;
     E.csize = csize;
+    E.xb = 0;
     E.S = (RgpuSys *)(smem + L.sys);
     E.ads = smem + L.ads;
     E.xyz = (double(*)[3])(smem + L.xyz);
     E.pos = (BeadPos *)(smem + L.pos);
-    E.res = (double(*)[4])(smem + L.res);
-    E.part = (double(*)[RGPU_MAX_POS][4])(smem + L.part);
-    E.ovf = (int *)(smem + L.ovf);
-    E.opart = (int(*)[RGPU_MAX_POS])(smem + L.opart);
-    E.sc.uv = (double *)(smem + L.uv);
-    E.sc.uc = (double *)(smem + L.uc);
-    E.sc.uo = (int *)(smem + L.uo);
+    E.uv = (double *)(smem + L.uv);
+    E.uc = (double *)(smem + L.uc);
+    E.uo = (int *)(smem + L.uo);
     E.sc.upos = nullptr;
     E.sc.qr2 = (float *)(smem + L.q);
     E.sc.qq = E.sc.qr2 + RGPU_MAX_WARPS * 64;
@@ -603,14 +657,20 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     E.kw = kw;
     E.red = (double *)(smem + L.red);
     E.ctl = (Ctl *)(smem + L.ctl);
-    E.sc.cnt = E.ctl->cnt;
-    if (threadIdx.x < 5) E.ctl->cnt[threadIdx.x] = 0ULL;
-    if (threadIdx.x == 0) {
-      E.ctl->xbuf = 0;
-      E.ctl->cyc[0] = E.ctl->cyc[1] = 0;
-    }
+    Ctl &C = *E.ctl;
+    E.sc.cnt = C.work;
     load_sys(E.S, &systems[sysi]);
     RgpuSys &S = *E.S;
+    double2 *sk_global = S.sk_ads;
+    if (threadIdx.x < 5) C.work[threadIdx.x] = 0ULL;
+    if (threadIdx.x < RGPU_CNT_PAIRS) C.cnt[threadIdx.x] = 0;
+    if (threadIdx.x < RGPU_NE) C.energy[threadIdx.x] = S.energy[threadIdx.x];
+    if (threadIdx.x == 0) {
+      C.cyc[0] = C.cyc[1] = 0;
+      C.status = 0;
+      C.nmol = *S.nmol;
+      C.nads = C.nmol * S.natom;
+    }
     /* this CTA's framework share, staged in shared memory when it fits */
     if (MIXED) {
       int t0, t1;
@@ -643,15 +703,33 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
       }
     }
     E.sl.ads = E.ads;
+    E.nfw_items = MIXED ? S.ntile : S.nfw;
+    /* this CTA's wave vectors with their prefactors and S(k) */
     if (S.ewald) share(S.nk, rank, csize, E.k0, E.k1);
     else { E.k0 = 0; E.k1 = 0; }
-    if (threadIdx.x == 0) {
-      E.ctl->nmol = *S.nmol;
-      E.ctl->nads = E.ctl->nmol * S.natom;
-    }
+    const bool k_smem = k_items >= E.k1 - E.k0;
     __syncthreads();
+    if (k_smem && E.k1 > E.k0) {
+      char4 *kv = (char4 *)(smem + L.kvec);
+      double *kf = (double *)(smem + L.kf);
+      double2 *sf = (double2 *)(smem + L.skfw);
+      double2 *sa = (double2 *)(smem + L.skads);
+      for (int i = threadIdx.x; i < E.k1 - E.k0; i += blockDim.x) {
+        kv[i] = S.kvec[E.k0 + i];
+        kf[i] = S.kfactor[E.k0 + i];
+        sf[i] = S.sk_fw[E.k0 + i];
+        sa[i] = S.sk_ads[E.k0 + i];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        S.kvec = kv - E.k0;
+        S.kfactor = kf - E.k0;
+        S.sk_fw = sf - E.k0;
+        S.sk_ads = sa - E.k0;
+      }
+    }
     /* adsorbates to shared memory (full copy in every CTA) */
-    for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
+    for (int i = threadIdx.x; i < C.nads; i += blockDim.x) {
       const int mm = i / S.natom, a = i - mm * S.natom;
       double p[3] = {S.ads_xyz[3 * i], S.ads_xyz[3 * i + 1], S.ads_xyz[3 * i + 2]};
       atom_store(E, mm, a, p);
@@ -661,33 +739,40 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     const long long t_start = clock64();
     for (long long it = 0; it < nsteps; it++) {
       const uint64_t step = step0 + (uint64_t)it;
-      const double u0 = rgpu_uniform(S.seed, S.sys_id, step, SLOT_MOVE);
+      /* this step's random numbers, one Philox block per thread */
+      double *rb = C.rnd[it & 1];
+      if (threadIdx.x < RGPU_RND / 2) rgpu_uniform_pair(S.seed, S.sys_id, step, threadIdx.x, &rb[2 * threadIdx.x]);
+      __syncthreads();
+      E.rnd = rb;
+      const double u0 = rb[SLOT_MOVE];
       int mv = 0;
       while (mv < 3 && u0 >= S.cum[mv]) mv++;
-      const int nmol = E.ctl->nmol;
-      share(E.ctl->nads, rank, csize, E.sl.ads_lo, E.sl.ads_hi);
-      const bool lead = rank == 0 && threadIdx.x == 0;
+      const int nmol = C.nmol;
+      share(C.nads, rank, csize, E.sl.ads_lo, E.sl.ads_hi);
       if (mv <= 1) {
         if (nmol == 0 || (mv == 1 && S.natom == 1)) continue;
-        if (lead) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + mv]++; }
-        step_displace<MIXED>(E, step, mv);
+        if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + mv]++; }
+        step_displace<MIXED>(E, mv);
       } else if (mv == 2) {
-        if (lead) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 2]++; }
+        if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 2]++; }
         if (nmol >= S.maxmol) {
-          if (lead) *S.status |= RGPU_ERR_MAXMOL;
+          if (threadIdx.x == 0) C.status |= RGPU_ERR_MAXMOL;
           continue;
         }
-        step_swap<MIXED>(E, step, true);
+        step_swap<MIXED>(E, true);
       } else {
-        if (lead) { S.counters[RGPU_CNT_MOVES]++; S.counters[RGPU_CNT_ATTEMPT + 3]++; }
+        if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 3]++; }
         if (nmol == 0) continue;
-        step_swap<MIXED>(E, step, false);
+        step_swap<MIXED>(E, false);
       }
     }
     __syncthreads();
-    /* write back positions, the molecule count and the work counters */
+    /* write back: positions, molecule count, energies, counters (rank 0);
+     * this CTA's share of S(k) and its work counters (every CTA) */
+    if (k_smem)
+      for (int k = E.k0 + threadIdx.x; k < E.k1; k += blockDim.x) sk_global[k] = S.sk_ads[k];
     if (rank == 0) {
-      for (int i = threadIdx.x; i < E.ctl->nads; i += blockDim.x) {
+      for (int i = threadIdx.x; i < C.nads; i += blockDim.x) {
         const int mm = i / S.natom, a = i - mm * S.natom;
         double p[3];
         atom_xyz(E, mm, a, p);
@@ -695,27 +780,29 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
         S.ads_xyz[3 * i + 1] = p[1];
         S.ads_xyz[3 * i + 2] = p[2];
       }
+      if (threadIdx.x < RGPU_NE) S.energy[threadIdx.x] = C.energy[threadIdx.x];
       if (threadIdx.x == 0) {
-        *S.nmol = E.ctl->nmol;
+        *S.nmol = C.nmol;
         *S.step = step0 + (uint64_t)nsteps;
+        for (int c = 0; c < RGPU_CNT_PAIRS; c++) S.counters[c] += C.cnt[c];
+        *S.status |= C.status;
         S.counters[RGPU_CNT_CYCLES] += clock64() - t_start;
-        S.counters[RGPU_CNT_CYC_EVAL] += E.ctl->cyc[0];
-        S.counters[RGPU_CNT_CYC_EWALD] += E.ctl->cyc[1];
+        S.counters[RGPU_CNT_CYC_EVAL] += C.cyc[0];
+        S.counters[RGPU_CNT_CYC_EWALD] += C.cyc[1];
       }
     }
-    __syncthreads();
     if (threadIdx.x == 0)
-      for (int c = 0; c < 5; c++) atomicAdd((unsigned long long *)&S.counters[RGPU_CNT_PAIRS + c], E.ctl->cnt[c]);
+      for (int c = 0; c < 5; c++) atomicAdd((unsigned long long *)&S.counters[RGPU_CNT_PAIRS + c], C.work[c]);
   }
   /* no CTA may leave while a peer can still read its shared memory */
   cl.sync();
 }
 
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
-                               int max_ads_atoms, int fw_items, int tile_items, int cluster, int threads,
-                               cudaStream_t st)
+                               int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
+                               int threads, cudaStream_t st)
 {
-  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw);
+  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nsys * cluster), 1, 1);
   cfg.blockDim = dim3((unsigned)threads, 1, 1);
@@ -733,12 +820,12 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
     e = cudaFuncSetAttribute(rgpu_engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
-                           tile_items);
+                           tile_items, k_items);
   } else {
     e = cudaFuncSetAttribute(rgpu_engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<false>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
-                           tile_items);
+                           tile_items, k_items);
   }
   if (e != cudaSuccess) return e;
   return cudaGetLastError();

@@ -191,7 +191,9 @@ __global__ void k_grid_interp(const float *grid, InterpParams ip, int n, const d
     p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
     if (p < 0.0) p += ip.cell[c];
     const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
-    i0[c] = (int)s;
+    /* a point on the upper cell face (p == cell after wrapping) uses the last
+     * grid cell at r = 1, so the 2x2x2 corner block stays inside the grid */
+    i0[c] = min(max((int)s, 0), ip.npts[c] - 1);
     r[c] = s - i0[c];
   }
   float v[8][8];

@@ -66,7 +66,7 @@ __device__ inline void rgpu_uniform_pair(uint64_t seed, uint32_t sys, uint64_t s
 /* random-draw slots of one MC step (the oracle uses the same numbering) */
 enum {
   SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
-  SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16, SLOT_ORIENT_SELECT = 63, SLOT_ORIENT = 64
+  SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16, SLOT_ORIENT_SELECT = 5, SLOT_ORIENT = 64
 };
 
 /* ------------------------------------------------------------------------ */

@@ -96,7 +96,8 @@ def test_batched_systems_match_single_runs(cuda):
     e.sync()
     for g, (st, xyz) in zip(gs, alone):
         st2 = g.state()
-        np.testing.assert_array_equal(st2["counters"], st["counters"])
+        # counters 15.. are SM clock cycles (timing, not results)
+        np.testing.assert_array_equal(st2["counters"][:15], st["counters"][:15])
         assert st2["nmol"] == st["nmol"]
         np.testing.assert_array_equal(st2["energy"], st["energy"])
         np.testing.assert_array_equal(g.adsorbates(), xyz)
