@@ -163,6 +163,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RGPU_E_NODEVICE, "no CUDA device");
   if (d->natom < 1 || d->natom > RGPU_MAX_ATOMS) return fail(RGPU_E_INVALID, "natom %d outside [1,%d]", d->natom, RGPU_MAX_ATOMS);
   if (d->nfw < 1 || !d->fw_xyz || !d->fw_type || !d->fw_q) return fail(RGPU_E_INVALID, "framework missing");
+  if (d->nfw > (1 << 24)) return fail(RGPU_E_INVALID, "nfw %d above 2^24", d->nfw);
   if (d->ntypes < 1 || !d->eps || !d->sig2 || !d->shift) return fail(RGPU_E_INVALID, "LJ table missing");
   if (!d->mol_type || !d->mol_q || !d->mol_ref) return fail(RGPU_E_INVALID, "molecule missing");
   if (d->start_bead < 0 || d->start_bead >= d->natom) return fail(RGPU_E_INVALID, "start_bead");
@@ -782,6 +783,7 @@ extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], cons
                                float *d_grid)
 {
   if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
+  if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
   if (type < 0 || type >= s->ntypes) return fail(RGPU_E_INVALID, "type %d", type);
   for (int c = 0; c < 3; c++)
     if (npts[c] < 1) return fail(RGPU_E_INVALID, "npts");
@@ -815,6 +817,7 @@ extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], con
 {
   if (!d_grid || !npts || !size || !shift || !cell || n < 0 || (n && (!xyz || !out)))
     return fail(RGPU_E_INVALID, "bad argument");
+  if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
   if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
   if (n == 0) return RGPU_SUCCESS;
   double *dx = nullptr, *dout = nullptr;

@@ -6,9 +6,9 @@
  *    its share, with its share of S(k), in shared memory); every CTA keeps a
  *    full copy of the adsorbate records, draws the same counter-based random
  *    numbers and takes the same decisions. Each energy evaluation leaves
- *    per-unit partial sums in shared memory; after one cluster barrier the
- *    lanes that need a total read the partials of every CTA through
- *    distributed shared memory in a fixed order, so all CTAs see bitwise
+ *    this CTA's per-position sums in shared memory; after one cluster barrier
+ *    the lanes that need a total read the sums of every CTA through
+ *    distributed shared memory in rank order, so all CTAs see bitwise
  *    identical totals. Each cluster advances its box by `nsteps` MC moves
  *    (translation, rotation, CBMC insertion, CBMC deletion: src/mc_moves.c:1529,
  *    :2636, :6941, :7150) without returning to the host; FP64 and mixed runs
@@ -37,8 +37,17 @@ namespace cg = cooperative_groups;
  * mixed path), tiles: tile records of the share (mixed only), k_items: wave
  * vectors of the share staged with their S(k) (0: read from global memory). */
 struct EngineLayout {
-  size_t sys, fw, tiles, ads, xyz, pos, uv, uc, uo, q, sites, tab, red, kvec, kf, skfw, skads, ctl, total;
+  size_t sys, fw, tiles, ads, xyz, pos, uv, uc, uo, part, q, sites, tab, red, kvec, kf, skfw, skads, ctl, total;
 };
+
+/* this CTA's sums for one position of an evaluation: host VDW, host real,
+ * adsorbate VDW, adsorbate real, overlap flag. 16-byte aligned (48 bytes) so
+ * that v[0..1] and v[2..3] are read as double2. */
+struct __align__(16) PosSum {
+  double v[4];
+  int ov, pad;
+};
+static_assert(sizeof(PosSum) % 16 == 0, "PosSum must keep 16-byte alignment in arrays");
 
 __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -53,9 +62,10 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.ads = o; o = rgpu_align(o + (size_t)max_ads_atoms * (mixed ? sizeof(int4) : sizeof(AdsRec64)));
   L.xyz = o; o = rgpu_align(o + (mixed ? (size_t)max_ads_atoms * 3 * sizeof(double) : 0));
   L.pos = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(BeadPos));
-  L.uv = o; o = rgpu_align(o + 2 * RGPU_MAX_UNITS * sizeof(double));    /* double-buffered unit partials */
-  L.uc = o; o = rgpu_align(o + 2 * RGPU_MAX_UNITS * sizeof(double));
-  L.uo = o; o = rgpu_align(o + 2 * RGPU_MAX_UNITS * sizeof(int));
+  L.uv = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
+  L.uc = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
+  L.uo = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(int));
+  L.part = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * sizeof(PosSum));   /* double-buffered */
   L.q = o; o = rgpu_align(o + (mixed ? (size_t)RGPU_MAX_WARPS * 64 * 12 : 0));
   L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
   L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed ? sizeof(float2) : sizeof(double2)));
@@ -102,8 +112,9 @@ struct Eng {
   void *ads;                 /* int4[] or AdsRec64[] (full copy) */
   double (*xyz)[3];          /* FP64 positions (MIXED: separate array; FP64: inside ads records) */
   BeadPos *pos;
-  double *uv, *uc;           /* [2][RGPU_MAX_UNITS] */
+  double *uv, *uc;           /* [RGPU_MAX_UNITS] unit partials */
   int *uo;
+  PosSum *part;              /* [2][RGPU_MAX_POS] position sums of this CTA */
   EvalScratch sc;
   EwSite *sites;
   typename PhaseT<MIXED>::T *tab;
@@ -114,7 +125,6 @@ struct Eng {
   const double *rnd;         /* this step's uniforms */
   int rank, csize;
   int xb;                    /* exchange buffer (same sequence in every thread and CTA) */
-  int nfw_items;             /* framework items (tiles or atoms) split over the cluster */
 };
 
 /* position of atom a of molecule m */
@@ -179,11 +189,13 @@ __device__ __forceinline__ void random_rotation(double x0, double y1, double y2,
   R[1][0] = 2.0 * u2 * u1 + ce * u3;
 }
 
-/* share [lo, hi) of n items for rank r of c */
+/* share [lo, hi) of n items for rank r of c (c a power of two <= 8; n far
+ * below 2^28, so n * c fits in 32 bits) */
 __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 {
-  lo = (int)((long long)n * r / c);
-  hi = (int)((long long)n * (r + 1) / c);
+  const int sh = __ffs(c) - 1;
+  lo = (n * r) >> sh;
+  hi = (n * (r + 1)) >> sh;
 }
 
 /* Pair evaluation of P positions on this CTA's share, then one cluster
@@ -193,46 +205,41 @@ __device__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
-  EvalScratch sc = E.sc;
-  sc.uv = E.uv + E.xb * RGPU_MAX_UNITS;
-  sc.uc = E.uc + E.xb * RGPU_MAX_UNITS;
-  sc.uo = E.uo + E.xb * RGPU_MAX_UNITS;
-  eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, sc, RGPU_MAX_UNITS);
+  const EvalPlan pl = eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.sc, RGPU_MAX_UNITS);
+  const int per = pl.cf + pl.ca;
+  __syncthreads();
+  /* this CTA's sum per position, units in order */
+  PosSum *ps = E.part + E.xb * RGPU_MAX_POS;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    double hv = 0.0, hc = 0.0, av = 0.0, ac = 0.0;
+    int ov = 0;
+    for (int c = 0; c < per; c++) {
+      const int u = p * per + c;
+      if (c < pl.cf) { hv += E.uv[u]; hc += E.uc[u]; }
+      else { av += E.uv[u]; ac += E.uc[u]; }
+      ov |= E.uo[u];
+    }
+    ps[p].v[0] = hv; ps[p].v[1] = hc; ps[p].v[2] = av; ps[p].v[3] = ac;
+    ps[p].ov = ov;
+  }
   cg::this_cluster().sync();
   if (threadIdx.x == 0) C.cyc[0] += clock64() - t0;
 }
 
-/* the unit plan CTA q used for P positions (eval_units with q's slice) */
+/* Totals of position p of the last evaluation (buffer b): the CTAs' sums
+ * added in rank order. */
 template <bool MIXED>
-__device__ __forceinline__ EvalPlan rank_plan(const Eng<MIXED> &E, int q, int P)
-{
-  int f0, f1, a0, a1;
-  share(E.nfw_items, q, E.csize, f0, f1);
-  share(E.ctl->nads, q, E.csize, a0, a1);
-  return eval_plan(P, f1 - f0, a1 - a0, blockDim.x >> 5, RGPU_MAX_UNITS, MIXED ? 2 : 64);
-}
-
-/* Totals of position p of the last evaluation of P positions (buffer b),
- * summed over the cluster's CTAs in rank order and over their units in
- * order. */
-template <bool MIXED>
-__device__ __forceinline__ void gather(const Eng<MIXED> &E, int b, int P, int p, double *r, int &ov)
+__device__ __forceinline__ void gather(const Eng<MIXED> &E, int b, int p, double *r, int &ov)
 {
   cg::cluster_group cl = cg::this_cluster();
+  const PosSum *own = E.part + b * RGPU_MAX_POS + p;
   r[0] = r[1] = r[2] = r[3] = 0.0;
   ov = 0;
   for (int q = 0; q < E.csize; q++) {
-    const double *uv = E.csize > 1 ? cl.map_shared_rank(E.uv, q) : E.uv;
-    const double *uc = E.csize > 1 ? cl.map_shared_rank(E.uc, q) : E.uc;
-    const int *uo = E.csize > 1 ? cl.map_shared_rank(E.uo, q) : E.uo;
-    const EvalPlan pl = rank_plan(E, q, P);
-    const int cf = pl.cf, per = pl.cf + pl.ca;
-    for (int c = 0; c < per; c++) {
-      const int u = b * RGPU_MAX_UNITS + p * per + c;
-      if (c < cf) { r[0] += uv[u]; r[1] += uc[u]; }
-      else { r[2] += uv[u]; r[3] += uc[u]; }
-      ov |= uo[u];
-    }
+    const PosSum *ps = E.csize > 1 ? cl.map_shared_rank(own, q) : own;
+    const double2 a = *(const double2 *)&ps->v[0], c = *(const double2 *)&ps->v[2];
+    r[0] += a.x; r[1] += a.y; r[2] += c.x; r[3] += c.y;
+    ov |= ps->ov;
   }
 }
 
@@ -290,7 +297,7 @@ __device__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool firs
     for (int j = 0; j < nb; j++) {
       double r[4];
       int o;
-      gather(E, b, n * nb, lane * nb + j, r, o);
+      gather(E, b, lane * nb + j, r, o);
       if (first) ov |= (r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap);
       else ov |= (r[0] >= S.overlap);
       for (int k = 0; k < 4; k++) e[k] += r[k];
@@ -371,8 +378,8 @@ __device__ void step_displace(Eng<MIXED> &E, int mv)
     double rn[4] = {0.0, 0.0, 0.0, 0.0}, ro[4] = {0.0, 0.0, 0.0, 0.0};
     int o1 = 0, o2 = 0;
     if (a < na) {
-      gather(E, be, 2 * na, a, rn, o1);
-      gather(E, be, 2 * na, na + a, ro, o2);
+      gather(E, be, a, rn, o1);
+      gather(E, be, na + a, ro, o2);
     }
     const int ov = __any_sync(RGPU_FULL, o1);
     double dl[4] = {0.0, 0.0, 0.0, 0.0};
@@ -648,6 +655,10 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     E.uv = (double *)(smem + L.uv);
     E.uc = (double *)(smem + L.uc);
     E.uo = (int *)(smem + L.uo);
+    E.part = (PosSum *)(smem + L.part);
+    E.sc.uv = E.uv;
+    E.sc.uc = E.uc;
+    E.sc.uo = E.uo;
     E.sc.upos = nullptr;
     E.sc.qr2 = (float *)(smem + L.q);
     E.sc.qq = E.sc.qr2 + RGPU_MAX_WARPS * 64;
@@ -703,7 +714,6 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
       }
     }
     E.sl.ads = E.ads;
-    E.nfw_items = MIXED ? S.ntile : S.nfw;
     /* this CTA's wave vectors with their prefactors and S(k) */
     if (S.ewald) share(S.nk, rank, csize, E.k0, E.k1);
     else { E.k0 = 0; E.k1 = 0; }

@@ -254,7 +254,7 @@ __device__ __forceinline__ void pair_mixed_queued(const RgpuLJf *P, float r2, fl
   const float u = fmaf(L.eps4 * s6, s6 - 1.0f, -L.shift);
   av += u;
   if (check && u >= thr) ov = 1;
-  if (charged) {
+  if (charged && qj != 0.0f) {
     nch++;
     const float r = r2 * ri;
     const float uc = qa * qj * rgpu_erfc_f(alpha * r) * ri;
@@ -263,21 +263,77 @@ __device__ __forceinline__ void pair_mixed_queued(const RgpuLJf *P, float r2, fl
   }
 }
 
+/* Per-warp queue of pairs inside the cut-off (squared distance, partner
+ * charge, LJ table index). Lanes append their pair when `in`; whenever 32 or
+ * more pairs are queued, all lanes evaluate 32 of them at once, so the pair
+ * arithmetic runs with every lane busy instead of under a divergent branch. */
+struct PairQueue {
+  float *r2, *q;
+  int *t;
+  int n;
+  const RgpuLJf *P;
+  bool charged, check;
+  float qa, alpha, thr;
+};
+
+__device__ __forceinline__ void queue_add(PairQueue &Q, bool in, float r2, float q, int t, float &av, float &ac,
+                                          int &ov, int &nin, int &nch)
+{
+  const int lane = threadIdx.x & 31;
+  const unsigned bal = __ballot_sync(RGPU_FULL, in);
+  if (in) {
+    const int p = Q.n + __popc(bal & ((1u << lane) - 1u));
+    Q.r2[p] = r2;
+    Q.q[p] = q;
+    Q.t[p] = t;
+  }
+  Q.n += __popc(bal);
+  if (Q.n >= 32) {
+    __syncwarp();
+    const float e_r2 = Q.r2[lane], e_q = Q.q[lane];
+    const int e_t = Q.t[lane];
+    float t_r2 = 0.0f, t_q = 0.0f;
+    int t_t = 0;
+    if (lane < Q.n - 32) { t_r2 = Q.r2[32 + lane]; t_q = Q.q[32 + lane]; t_t = Q.t[32 + lane]; }
+    __syncwarp();
+    if (lane < Q.n - 32) { Q.r2[lane] = t_r2; Q.q[lane] = t_q; Q.t[lane] = t_t; }
+    nin++;
+    pair_mixed_queued(Q.P, e_r2, e_q, Q.charged, Q.qa, Q.alpha, Q.check, Q.thr, av, ac, ov, nch, e_t);
+    Q.n -= 32;
+    __syncwarp();
+  }
+}
+
+/* evaluates what is left in the queue */
+__device__ __forceinline__ void queue_drain(PairQueue &Q, float &av, float &ac, int &ov, int &nin, int &nch)
+{
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  if (lane < Q.n) {
+    nin++;
+    pair_mixed_queued(Q.P, Q.r2[lane], Q.q[lane], Q.charged, Q.qa, Q.alpha, Q.check, Q.thr, av, ac, ov, nch,
+                      Q.t[lane]);
+  }
+  Q.n = 0;
+  __syncwarp();
+}
+
 /* framework tiles [t0, t1) for bead b, FP32 path (warp-wide) */
 __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *fw, const TileRec *tiles, int t0, int t1,
                                                  const BeadPos &b, bool check, float &av, float &ac, int &ov,
                                                  int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
 {
   const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
   const float rc2 = S.rc2f;
-  const float thr = (float)S.overlap;
-  const float qa = S.mol_qf[b.atom] * S.coulombf;
-  const bool charged = S.fw_charged && qa != 0.0f;
-  const float alpha = S.alphaf;
-  const RgpuLJf *P = S.ljf_bf[b.atom];
-  int qn = 0;
+  PairQueue Q;
+  Q.r2 = qr2; Q.q = qq; Q.t = qt; Q.n = 0;
+  Q.P = S.ljf_bf[b.atom];
+  Q.qa = S.mol_qf[b.atom] * S.coulombf;
+  Q.charged = S.fw_charged && Q.qa != 0.0f;
+  Q.check = check;
+  Q.alpha = S.alphaf;
+  Q.thr = (float)S.overlap;
   for (int tb = t0; tb < t1; tb += 32) {
     const int t = tb + lane;
     bool vis = false;
@@ -305,36 +361,10 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
         r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         in = r2 < rc2;
       }
-      const unsigned bal = __ballot_sync(RGPU_FULL, in);
-      if (in) {
-        const int p = qn + __popc(bal & lt);
-        qr2[p] = r2;
-        qq[p] = __int_as_float(f.w);
-        qt[p] = f.z & 3;
-      }
-      qn += __popc(bal);
-      if (qn >= 32) {
-        __syncwarp();
-        const float e_r2 = qr2[lane], e_q = qq[lane];
-        const int e_t = qt[lane];
-        float t_r2 = 0.0f, t_q = 0.0f;
-        int t_t = 0;
-        if (lane < qn - 32) { t_r2 = qr2[32 + lane]; t_q = qq[32 + lane]; t_t = qt[32 + lane]; }
-        __syncwarp();
-        if (lane < qn - 32) { qr2[lane] = t_r2; qq[lane] = t_q; qt[lane] = t_t; }
-        nin++;
-        pair_mixed_queued(P, e_r2, e_q, charged, qa, alpha, check, thr, av, ac, ov, nch, e_t);
-        qn -= 32;
-        __syncwarp();
-      }
+      queue_add(Q, in, r2, __int_as_float(f.w), f.z & 3, av, ac, ov, nin, nch);
     }
   }
-  __syncwarp();
-  if (lane < qn) {
-    nin++;
-    pair_mixed_queued(P, qr2[lane], qq[lane], charged, qa, alpha, check, thr, av, ac, ov, nch, qt[lane]);
-  }
-  __syncwarp();
+  queue_drain(Q, av, ac, ov, nin, nch);
 }
 
 /* framework atoms [lo, hi) of the type-sorted FP64 layout */
@@ -382,45 +412,40 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
 
 __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo,
                                                int hi, int exclude, bool check, float &av, float &ac, int &ov,
-                                               int &nin, int &nch, int &nvis)
+                                               int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
 {
   const int lane = threadIdx.x & 31;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
   const float rc2 = S.rc2f;
-  const float thr = (float)S.overlap;
-  const float qa = S.mol_qf[b.atom] * S.coulombf;
-  const bool charged = S.mol_charged && qa != 0.0f;
-  const float alpha = S.alphaf;
+  PairQueue Q;
+  Q.r2 = qr2; Q.q = qq; Q.t = qt; Q.n = 0;
+  Q.P = S.ljf_bb[b.atom];
+  Q.qa = S.mol_qf[b.atom] * S.coulombf;
+  Q.charged = S.mol_charged && Q.qa != 0.0f;
+  Q.check = check;
+  Q.alpha = S.alphaf;
+  Q.thr = (float)S.overlap;
   nvis += hi - lo;
-  for (int j = lo + lane; j < hi; j += 32) {
-    int4 f = ads[j];
-    if ((f.w >> 4) == exclude) continue;
-    int at = f.w & 15;
-    float dx = __int2float_rn(f.x - b.xi) * sx;
-    float dy = __int2float_rn(f.y - b.yi) * sy;
-    float dz = __int2float_rn(f.z - b.zi) * sz;
-    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    if (r2 < rc2) {
-      nin++;
-      const RgpuLJf P = S.ljf_bb[b.atom][at];
-      float ri = rsqrtf(r2);
-      ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);
-      float ir2 = ri * ri;
-      float s6 = P.sig2 * ir2;
-      s6 = s6 * s6 * s6;
-      float u = fmaf(P.eps4 * s6, s6 - 1.0f, -P.shift);
-      av += u;
-      if (check && u >= thr) ov = 1;
-      float qb = S.mol_qf[at];
-      if (charged && qb != 0.0f) {
-        nch++;
-        float r = r2 * ri;
-        float uc = qa * qb * rgpu_erfc_f(alpha * r) * ri;
-        ac += uc;
-        if (check && uc >= thr) ov = 1;
+  for (int jb = lo; jb < hi; jb += 32) {
+    const int j = jb + lane;
+    bool in = false;
+    float r2 = 0.0f, q = 0.0f;
+    int at = 0;
+    if (j < hi) {
+      const int4 f = ads[j];
+      if ((f.w >> 4) != exclude) {
+        at = f.w & 15;
+        const float dx = __int2float_rn(f.x - b.xi) * sx;
+        const float dy = __int2float_rn(f.y - b.yi) * sy;
+        const float dz = __int2float_rn(f.z - b.zi) * sz;
+        r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        in = r2 < rc2;
+        q = S.mol_qf[at];
       }
     }
+    queue_add(Q, in, r2, q, at, av, ac, ov, nin, nch);
   }
+  queue_drain(Q, av, ac, ov, nin, nch);
 }
 
 __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *ads, const BeadPos &b, int lo,
@@ -485,20 +510,23 @@ __device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const Bead
   const int nfw = sl.fw_hi - sl.fw_lo, nads = sl.ads_hi - sl.ads_lo;
   const EvalPlan pl = eval_plan(P, nfw, nads, nw, max_units, MIXED ? 2 : 64);
   const int per = pl.cf + pl.ca;
+  /* work counts of this lane, summed over its units (statistics only) */
+  int nin = 0, nch = 0, nvis = 0;
   for (int u = w; u < pl.nunits; u += nw) {
     const int p = u / per, c = u - p * per;
     const BeadPos b = pos[p];
     const bool check = p < pair_check;
-    int ov = 0, nin = 0, nch = 0, nvis = 0;
+    int ov = 0;
     double v, q;
     int lo, hi;
+    /* chunk bounds; item counts stay far below 2^31 / RGPU_MAX_UNITS */
     if (c < pl.cf) {
-      lo = sl.fw_lo + (int)((long long)nfw * c / pl.cf);
-      hi = sl.fw_lo + (int)((long long)nfw * (c + 1) / pl.cf);
+      lo = sl.fw_lo + (int)((unsigned)(nfw * c) / (unsigned)pl.cf);
+      hi = sl.fw_lo + (int)((unsigned)(nfw * (c + 1)) / (unsigned)pl.cf);
     } else {
       const int cc = c - pl.cf;
-      lo = sl.ads_lo + (int)((long long)nads * cc / pl.ca);
-      hi = sl.ads_lo + (int)((long long)nads * (cc + 1) / pl.ca);
+      lo = sl.ads_lo + (int)((unsigned)(nads * cc) / (unsigned)pl.ca);
+      hi = sl.ads_lo + (int)((unsigned)(nads * (cc + 1)) / (unsigned)pl.ca);
     }
     if (MIXED) {
       float av = 0.0f, ac = 0.0f;
@@ -506,7 +534,8 @@ __device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const Bead
         unit_tiles_mixed(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
                          sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
       else
-        unit_ads_mixed(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
+        unit_ads_mixed(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
+                       sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
       v = (double)warp_sum(av);
       q = (double)warp_sum(ac);
     } else {
@@ -519,19 +548,19 @@ __device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const Bead
       q = warp_sum(ac);
     }
     ov = warp_or(ov);
-    if (sc.cnt) {
-      nin = __reduce_add_sync(RGPU_FULL, (unsigned)nin);
-      nch = __reduce_add_sync(RGPU_FULL, (unsigned)nch);
-      if (lane == 0) {
-        atomicAdd(&sc.cnt[0], (unsigned long long)nvis);
-        atomicAdd(&sc.cnt[1], (unsigned long long)nin);
-        atomicAdd(&sc.cnt[2], (unsigned long long)nch);
-      }
-    }
     if (lane == 0) {
       sc.uv[u] = v;
       sc.uc[u] = q;
       sc.uo[u] = ov;
+    }
+  }
+  if (sc.cnt && w < pl.nunits) {
+    nin = __reduce_add_sync(RGPU_FULL, (unsigned)nin);
+    nch = __reduce_add_sync(RGPU_FULL, (unsigned)nch);
+    if (lane == 0) {
+      atomicAdd(&sc.cnt[0], (unsigned long long)nvis);
+      atomicAdd(&sc.cnt[1], (unsigned long long)nin);
+      atomicAdd(&sc.cnt[2], (unsigned long long)nch);
     }
   }
   return pl;
