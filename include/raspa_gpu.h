@@ -149,6 +149,22 @@ int rgpu_grid_build(rgpu_system *sys, int type, const int npts[3], const double 
 int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3], const double shift[3],
                           const double cell[3], int n, const double *xyz, double *out);
 
+/* ---- grid lookup without device allocation ------------------------------ */
+/* No counterpart in the reference. Same result as rgpu_grid_interpolate for
+ * n <= RGPU_NOALLOC_MAX_POINTS points, but the call makes no device
+ * allocation: positions and results pass through a file-scope device array of
+ * 256 KB (one per device) instead of buffers allocated per call. The first
+ * call on each device looks up that array's address (cudaGetSymbolAddress)
+ * with the device current and keeps it, so make the first call before any
+ * stream capture. n above RGPU_NOALLOC_MAX_POINTS returns RGPU_E_INVALID.
+ * Calls that overlap on one device (several host threads) share the array
+ * and race: serialise them. Runs on the legacy default stream and returns
+ * when the results are in `out`. */
+#define RGPU_NOALLOC_MAX_POINTS 8192
+int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const double size[3],
+                                  const double shift[3], const double cell[3], int n, const double *xyz,
+                                  double *out);
+
 /* ---- persistent batched engine ------------------------------------------ */
 /* Groups systems for one persistent launch; each system is advanced by one
  * thread-block cluster of `cluster` CTAs (1, 2, 4 or 8; 0 chooses from the

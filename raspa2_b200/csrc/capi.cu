@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "../../include/raspa_gpu.h"
@@ -834,6 +835,61 @@ extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], con
   cudaFree(dx);
   cudaFree(dout);
   return rc;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Grid lookup without device allocation. The positions and results of one
+ * call live in a file-scope device array (one per device, 256 KB); the
+ * first call on a device looks up its address with cudaGetSymbolAddress
+ * and keeps it. Calls that overlap on one device share the array and race. */
+struct NoAllocInterp {
+  double xyz[RGPU_NOALLOC_MAX_POINTS * 3];
+  double out[RGPU_NOALLOC_MAX_POINTS];
+};
+static __device__ __align__(256) NoAllocInterp g_noalloc_interp;
+
+#define RGPU_NOALLOC_MAX_DEVICES 64
+static std::mutex g_noalloc_mu;
+static NoAllocInterp *g_noalloc_ptr[RGPU_NOALLOC_MAX_DEVICES];
+
+static int noalloc_scratch(NoAllocInterp **out)
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= RGPU_NOALLOC_MAX_DEVICES) return fail(RGPU_E_INVALID, "device %d", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_interp);
+    if (e != cudaSuccess) return fail(RGPU_E_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (NoAllocInterp *)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const double size[3],
+                                             const double shift[3], const double cell[3], int n,
+                                             const double *xyz, double *out)
+{
+  if (!d_grid || !npts || !size || !shift || !cell || n < 0 || (n && (!xyz || !out)))
+    return fail(RGPU_E_INVALID, "bad argument");
+  if (n > RGPU_NOALLOC_MAX_POINTS)
+    return fail(RGPU_E_INVALID, "n = %d points exceeds RGPU_NOALLOC_MAX_POINTS (%d)", n, RGPU_NOALLOC_MAX_POINTS);
+  if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
+  if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
+  NoAllocInterp *scr = nullptr;
+  int rc = noalloc_scratch(&scr);
+  if (rc != RGPU_SUCCESS) return rc;
+  if (n == 0) return RGPU_SUCCESS;
+  /* results start at zero, so a point the kernel did not write could never
+   * return a previous call's value */
+  CK(cudaMemsetAsync(scr->out, 0, sizeof(double) * n, 0));
+  CK(cudaMemcpyAsync(scr->xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0));
+  CK(rgpu_grid_interp_launch(d_grid, npts, size, shift, cell, n, scr->xyz, scr->out, 0));
+  CK(cudaMemcpyAsync(out, scr->out, sizeof(double) * n, cudaMemcpyDeviceToHost, 0));
+  CK(cudaStreamSynchronize(0));
+  return RGPU_SUCCESS;
 }
 
 /* ---------------------------------------------------------------------- */

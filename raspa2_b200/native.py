@@ -29,8 +29,10 @@ EXPORTS = [
     "rgpu_ewald_fourier_difference", "rgpu_ewald_accept", "rgpu_total_energy", "rgpu_grid_build",
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
-    "rgpu_engine_cluster",
+    "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc",
 ]
+
+RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
 
 
 class SystemDesc(C.Structure):
@@ -254,6 +256,21 @@ def grid_interpolate(d_grid_ptr: int, npts, size, shift, cell, xyz) -> np.ndarra
     _check(load().rgpu_grid_interpolate(C.c_void_p(d_grid_ptr), n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),
                                         sh.ctypes.data_as(_dp), ce.ctypes.data_as(_dp), C.c_int(len(x)),
                                         x.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
+    return out
+
+
+def grid_interpolate_noalloc(d_grid_ptr: int, npts, size, shift, cell, xyz) -> np.ndarray:
+    """rgpu_grid_interpolate_noalloc: as grid_interpolate, through the
+    library's static device scratch (at most RGPU_NOALLOC_MAX_POINTS points,
+    no device allocation; overlapping calls on one device race)."""
+    n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64)
+    ce = _arr(cell, np.float64)
+    x = _arr(np.asarray(xyz, float).reshape(-1, 3), np.float64)
+    out = np.zeros(len(x))
+    _check(load().rgpu_grid_interpolate_noalloc(C.c_void_p(d_grid_ptr), n.ctypes.data_as(_ip),
+                                                s.ctypes.data_as(_dp), sh.ctypes.data_as(_dp),
+                                                ce.ctypes.data_as(_dp), C.c_int(len(x)), x.ctypes.data_as(_dp),
+                                                out.ctypes.data_as(_dp)))
     return out
 
 
