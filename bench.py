@@ -60,8 +60,9 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--nsys", type=int, default=64)
     p.add_argument("--moves-per-step", type=int, default=2000)
-    p.add_argument("--threads", type=int, default=256)
-    p.add_argument("--maxmol", type=int, default=384)
+    p.add_argument("--threads", type=int, default=0, help="CTA size; 0 = autotuned")
+    p.add_argument("--cluster", type=int, default=0, help="CTAs per system; 0 = autotuned")
+    p.add_argument("--maxmol", type=int, default=768)
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--ref-cycles", type=int, default=10)
@@ -243,7 +244,7 @@ def run_ours(args):
     gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240 + rank, stream_id=i) for i, s in enumerate(sys_list)]
     for g, s in zip(gs, sys_list):
         g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
-    eng = native.Engine(gs, precision=prec, threads=args.threads)
+    eng = native.Engine(gs, precision=prec, threads=args.threads or 512, cluster=args.cluster)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
 
@@ -254,6 +255,17 @@ def run_ours(args):
     for _ in range(args.warmup):
         eng.run(args.moves_per_step, stream.cuda_stream)
     torch.cuda.synchronize()
+    # launch shape: autotuned on copies of the equilibrated systems unless
+    # both are given; the engine is rebuilt with the chosen shape and warmed
+    shape = {"cluster": eng.cluster, "threads": eng.threads, "tuned": False}
+    if not (args.threads and args.cluster):
+        from raspa2_b200 import autotune
+        tuned = autotune.tune(gs, precision=prec)
+        shape = {"cluster": tuned.cluster, "threads": tuned.threads, "tuned": True, "table": tuned.table}
+        eng.close()
+        eng = native.Engine(gs, precision=prec, threads=tuned.threads, cluster=tuned.cluster)
+        eng.run(args.moves_per_step, stream.cuda_stream)
+        torch.cuda.synchronize()
     c0 = counters()
     if world > 1:
         dist.barrier()
@@ -337,7 +349,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == native.RGPU_MIXED else "f64",
         "data": "synthetic (seeded frameworks, random-init adsorbate state)",
         "config": {"workload": f"co2_gcmc_batched_{args.nsys}", "systems_per_gpu": args.nsys,
-                   "moves_per_step_per_system": args.moves_per_step, "threads_per_block": args.threads,
+                   "moves_per_step_per_system": args.moves_per_step, "launch_shape": shape,
                    "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
                    "framework_atoms": [int(s.n_framework()) for s in sys_list[:8]] + ["..."],
                    "mean_loading": float(np.mean(loads))},
@@ -379,20 +391,31 @@ def run_ours(args):
 
 def plain_gpu_rate(native, stream, nsteps=2000):
     """The plain comparator: one system (the 1536-atom CO2 system) at a time,
-    FP64, through the same engine with a single thread block."""
+    FP64, through the same engine at its own best launch shape (autotuned
+    for the single system after equilibration). Device-timed."""
+    import torch
+    from raspa2_b200 import autotune
     s = systems.co2_system(seed=1)
     g = native.GpuSystem(s, maxmol=256, seed=5, stream_id=0)
     g.set_adsorbates(np.zeros((0, 3, 3)))
     e = native.Engine([g], precision=native.RGPU_FP64, threads=256)
     e.run(nsteps, stream.cuda_stream)
     e.sync()
-    c0 = g.state()["counters"][8]
-    t0 = time.perf_counter()
-    e.run(nsteps, stream.cuda_stream)
+    tuned = autotune.tune([g], precision=native.RGPU_FP64, moves=200, warm=50)
+    e.close()
+    e = native.Engine([g], precision=native.RGPU_FP64, threads=tuned.threads, cluster=tuned.cluster)
+    e.run(200, stream.cuda_stream)
     e.sync()
-    t = time.perf_counter() - t0
+    c0 = g.state()["counters"][8]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    e.run(nsteps, stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3
     return {"engine_fp64_single_system_moves_per_s": (g.state()["counters"][8] - c0) / t,
-            "system": "co2 1536 atoms, kmax 8"}
+            "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads},
+            "system": "co2 1536 atoms, kmax 8", "loading": int(g.state()["nmol"])}
 
 
 def main():

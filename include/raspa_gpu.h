@@ -169,7 +169,8 @@ int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const 
 /* Groups systems for one persistent launch; each system is advanced by one
  * thread-block cluster of `cluster` CTAs (1, 2, 4 or 8; 0 chooses from the
  * number of systems and SMs) that split its framework between them.
- * `threads` = CTA size (64..512, multiple of 32). */
+ * `threads` = CTA size, a multiple of 32 in 64..1024 (RGPU_MIXED) or
+ * 64..512 (RGPU_FP64). */
 int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
                        int cluster);
 /* CTAs per system of an engine. */

@@ -911,7 +911,11 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
 {
   if (!out || !systems || n < 1) return fail(RGPU_E_INVALID, "bad argument");
   if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
-  if (threads < 64 || threads > 512 || threads % 32) return fail(RGPU_E_INVALID, "threads %d", threads);
+  /* the mixed kernel is compiled for up to 1024 threads (64 registers), the
+   * FP64 one for up to 512 */
+  const int max_threads = precision == RGPU_MIXED ? 1024 : 512;
+  if (threads < 64 || threads > max_threads || threads % 32)
+    return fail(RGPU_E_INVALID, "threads %d outside [64,%d] or not a multiple of 32", threads, max_threads);
   if (cluster < 0 || cluster > 8 || (cluster & (cluster - 1))) return fail(RGPU_E_INVALID, "cluster %d", cluster);
   *out = nullptr;
   rgpu_engine *e = new rgpu_engine();
@@ -947,7 +951,8 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
   const int k_try[4] = {maxk, 0, maxk, 0};
   int pick = -1;
   for (int t = 0; t < 4 && pick < 0; t++)
-    if (rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t]) <= (size_t)smem_max)
+    if (rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t], threads) <=
+        (size_t)smem_max)
       pick = t;
   if (pick < 0) {
     delete e;

@@ -37,7 +37,7 @@ namespace cg = cooperative_groups;
  * mixed path), tiles: tile records of the share (mixed only), k_items: wave
  * vectors of the share staged with their S(k) (0: read from global memory). */
 struct EngineLayout {
-  size_t sys, fw, tiles, ads, xyz, pos, uv, uc, uo, part, q, sites, tab, red, kvec, kf, skfw, skads, ctl, total;
+  size_t sys, fw, tiles, ads, pos, uv, uc, uo, part, q, sites, tab, red, kvec, kf, skfw, skads, ctl, total;
 };
 
 /* this CTA's sums for one position of an evaluation: host VDW, host real,
@@ -52,7 +52,7 @@ static_assert(sizeof(PosSum) % 16 == 0, "PosSum must keep 16-byte alignment in a
 __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
 __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw,
-                                                      int k_items)
+                                                      int k_items, int nwarps)
 {
   EngineLayout L;
   size_t o = 0;
@@ -60,13 +60,12 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.fw = o; o = rgpu_align(o + (size_t)fw_items * (mixed ? sizeof(int4) : sizeof(double4)));
   L.tiles = o; o = rgpu_align(o + (size_t)tiles * sizeof(TileRec));
   L.ads = o; o = rgpu_align(o + (size_t)max_ads_atoms * (mixed ? sizeof(int4) : sizeof(AdsRec64)));
-  L.xyz = o; o = rgpu_align(o + (mixed ? (size_t)max_ads_atoms * 3 * sizeof(double) : 0));
   L.pos = o; o = rgpu_align(o + RGPU_MAX_POS * sizeof(BeadPos));
   L.uv = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
   L.uc = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
   L.uo = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(int));
   L.part = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * sizeof(PosSum));   /* double-buffered */
-  L.q = o; o = rgpu_align(o + (mixed ? (size_t)RGPU_MAX_WARPS * 64 * 12 : 0));
+  L.q = o; o = rgpu_align(o + (mixed ? (size_t)nwarps * 64 * 12 : 0));     /* per-warp pair queues */
   L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
   L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed ? sizeof(float2) : sizeof(double2)));
   L.red = o; o = rgpu_align(o + 2 * 2 * RGPU_MAX_WARPS * sizeof(double));
@@ -79,9 +78,10 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   return L;
 }
 
-size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw, int k_items)
+size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw, int k_items,
+                              int threads)
 {
-  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw, k_items).total;
+  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw, k_items, threads / 32).total;
 }
 
 /* broadcast/control block in shared memory */
@@ -110,7 +110,6 @@ struct Eng {
   RgpuSys *S;
   EvalSlice sl;
   void *ads;                 /* int4[] or AdsRec64[] (full copy) */
-  double (*xyz)[3];          /* FP64 positions (MIXED: separate array; FP64: inside ads records) */
   BeadPos *pos;
   double *uv, *uc;           /* [RGPU_MAX_UNITS] unit partials */
   int *uo;
@@ -127,13 +126,16 @@ struct Eng {
   int xb;                    /* exchange buffer (same sequence in every thread and CTA) */
 };
 
-/* position of atom a of molecule m */
+/* Position of atom a of molecule m. FP64 records carry the position; on the
+ * mixed path the FP64 positions stay in global memory (ads_xyz), which every
+ * CTA of the cluster writes with the same values on each accepted move. */
 template <bool MIXED>
 __device__ __forceinline__ void atom_xyz(const Eng<MIXED> &E, int m, int a, double *p)
 {
   const int idx = m * E.S->natom + a;
   if (MIXED) {
-    p[0] = E.xyz[idx][0]; p[1] = E.xyz[idx][1]; p[2] = E.xyz[idx][2];
+    const double *x = E.S->ads_xyz + 3 * idx;
+    p[0] = x[0]; p[1] = x[1]; p[2] = x[2];
   } else {
     const AdsRec64 &r = ((const AdsRec64 *)E.ads)[idx];
     p[0] = r.x; p[1] = r.y; p[2] = r.z;
@@ -146,7 +148,8 @@ __device__ __forceinline__ void atom_store(const Eng<MIXED> &E, int m, int a, co
   const RgpuSys &S = *E.S;
   const int idx = m * S.natom + a;
   if (MIXED) {
-    E.xyz[idx][0] = p[0]; E.xyz[idx][1] = p[1]; E.xyz[idx][2] = p[2];
+    double *x = E.S->ads_xyz + 3 * idx;
+    x[0] = p[0]; x[1] = p[1]; x[2] = p[2];
     ((int4 *)E.ads)[idx] = make_int4(rgpu_to_fix(p[0], S.inv_box[0]), rgpu_to_fix(p[1], S.inv_box[1]),
                                      rgpu_to_fix(p[2], S.inv_box[2]), m * 16 + a);
   } else {
@@ -633,7 +636,7 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps, int kw,
+__global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps, int kw,
                                                           int max_ads_atoms, int fw_items, int tile_items,
                                                           int k_items)
 {
@@ -642,7 +645,8 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
   const int csize = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
   const int sysi = blockIdx.x / csize;
-  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw, k_items);
+  const int nwarps = blockDim.x >> 5;
+  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw, k_items, nwarps);
   if (sysi < nsys) {
     Eng<MIXED> E;
     E.rank = rank;
@@ -650,7 +654,6 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     E.xb = 0;
     E.S = (RgpuSys *)(smem + L.sys);
     E.ads = smem + L.ads;
-    E.xyz = (double(*)[3])(smem + L.xyz);
     E.pos = (BeadPos *)(smem + L.pos);
     E.uv = (double *)(smem + L.uv);
     E.uc = (double *)(smem + L.uc);
@@ -661,8 +664,8 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     E.sc.uo = E.uo;
     E.sc.upos = nullptr;
     E.sc.qr2 = (float *)(smem + L.q);
-    E.sc.qq = E.sc.qr2 + RGPU_MAX_WARPS * 64;
-    E.sc.qt = (int *)(E.sc.qq + RGPU_MAX_WARPS * 64);
+    E.sc.qq = E.sc.qr2 + nwarps * 64;
+    E.sc.qt = (int *)(E.sc.qq + nwarps * 64);
     E.sites = (EwSite *)(smem + L.sites);
     E.tab = (typename PhaseT<MIXED>::T *)(smem + L.tab);
     E.kw = kw;
@@ -738,11 +741,15 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
         S.sk_ads = sa - E.k0;
       }
     }
-    /* adsorbates to shared memory (full copy in every CTA) */
+    /* adsorbate records to shared memory (full copy in every CTA) */
     for (int i = threadIdx.x; i < C.nads; i += blockDim.x) {
       const int mm = i / S.natom, a = i - mm * S.natom;
-      double p[3] = {S.ads_xyz[3 * i], S.ads_xyz[3 * i + 1], S.ads_xyz[3 * i + 2]};
-      atom_store(E, mm, a, p);
+      const double *x = S.ads_xyz + 3 * i;
+      if (MIXED)
+        ((int4 *)E.ads)[i] = make_int4(rgpu_to_fix(x[0], S.inv_box[0]), rgpu_to_fix(x[1], S.inv_box[1]),
+                                       rgpu_to_fix(x[2], S.inv_box[2]), mm * 16 + a);
+      else
+        atom_store(E, mm, a, x);
     }
     __syncthreads();
     const uint64_t step0 = *S.step;
@@ -782,7 +789,8 @@ __global__ void __launch_bounds__(512) rgpu_engine_kernel(RgpuSys *systems, int 
     if (k_smem)
       for (int k = E.k0 + threadIdx.x; k < E.k1; k += blockDim.x) sk_global[k] = S.sk_ads[k];
     if (rank == 0) {
-      for (int i = threadIdx.x; i < C.nads; i += blockDim.x) {
+      /* FP64 positions (the mixed path keeps them in global memory already) */
+      for (int i = threadIdx.x; !MIXED && i < C.nads; i += blockDim.x) {
         const int mm = i / S.natom, a = i - mm * S.natom;
         double p[3];
         atom_xyz(E, mm, a, p);
@@ -812,7 +820,7 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
                                int threads, cudaStream_t st)
 {
-  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items);
+  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items, threads);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nsys * cluster), 1, 1);
   cfg.blockDim = dim3((unsigned)threads, 1, 1);

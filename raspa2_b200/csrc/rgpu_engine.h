@@ -10,7 +10,8 @@
 /* fw_items / tile_items: framework records / tiles one CTA stages (0: the
  * framework is read from global memory); k_items: wave vectors one CTA
  * stages with their S(k) (0: read from global memory) */
-size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tile_items, int max_ads_atoms, int kw, int k_items);
+size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tile_items, int max_ads_atoms, int kw, int k_items,
+                              int threads);
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
                                int threads, cudaStream_t st);

@@ -112,6 +112,8 @@ class GpuSystem:
                  max_translation: Optional[float] = None, max_rotation: Optional[float] = None):
         L = load()
         self.sysm = sysm
+        self.init_args = dict(maxmol=maxmol, seed=seed, stream_id=stream_id, max_translation=max_translation,
+                              max_rotation=max_rotation)
         eps, sig2, shift = sysm.lj_tables()
         pos, t, q = sysm.framework()
         keep = []
@@ -277,13 +279,15 @@ def grid_interpolate_noalloc(d_grid_ptr: int, npts, size, shift, cell, xyz) -> n
 class Engine:
     """Persistent batched engine over several GpuSystems (rgpu_engine)."""
 
-    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=256, cluster=0):
+    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=512, cluster=0):
         L = load()
         arr = (C.c_void_p * len(systems))(*[s.h for s in systems])
         h = C.c_void_p()
         _check(L.rgpu_engine_create(C.byref(h), arr, C.c_int(len(systems)), C.c_int(precision), C.c_int(threads),
                                     C.c_int(cluster)))
         self.cluster = int(L.rgpu_engine_cluster(h))
+        self.threads = threads
+        self.precision = precision
         self.h = h
         self.systems = list(systems)
 

@@ -77,8 +77,9 @@ def test_energy_drift(cuda, precision, tol, cluster):
 
 
 def test_batched_systems_match_single_runs(cuda):
-    """Each system's result is the same alone and in a batch of uneven
-    systems (independent streams, one thread block each)."""
+    """Each system's result is bitwise the same alone and in a batch of
+    uneven systems at the same launch shape (independent random streams, one
+    cluster per system)."""
     specs = [systems.tiny_co2_system(seed=7), systems.co2_system(seed=21, n_atoms=512, cell=20.0, kmax=5),
              systems.methane_system(seed=3)]
     n = 200
@@ -91,7 +92,9 @@ def test_batched_systems_match_single_runs(cuda):
         g = native.GpuSystem(s, maxmol=64, seed=5, stream_id=i)
         g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
         gs.append(g)
-    e = native.Engine(gs, precision=native.RGPU_MIXED)
+    # same launch shape as engine_run (the unit split, hence the FP32
+    # summation order, follows the CTA size)
+    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=256)
     e.run(n)
     e.sync()
     for g, (st, xyz) in zip(gs, alone):
@@ -114,3 +117,28 @@ def test_mixed_engine_tracks_fp64(cuda):
     np.testing.assert_array_equal(a["counters"][:9], b["counters"][:9])
     kT = units.K_B * s.temperature
     np.testing.assert_allclose(b["energy"][:6], a["energy"][:6], rtol=1e-5, atol=1e-3 * kT)
+
+
+def test_autotune_leaves_systems_untouched(cuda):
+    """The tuner times shapes on copies: the caller's systems keep their
+    configuration, counters and random-stream position."""
+    from raspa2_b200 import autotune
+    specs = [systems.tiny_co2_system(seed=7), systems.tiny_co2_system(seed=8)]
+    gs = []
+    for i, s in enumerate(specs):
+        g = native.GpuSystem(s, maxmol=64, seed=5, stream_id=i)
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+        gs.append(g)
+    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=256, cluster=1)
+    e.run(200)
+    e.sync()
+    before = [(g.adsorbates().copy(), g.state()) for g in gs]
+    shape = autotune.tune(gs, precision=native.RGPU_MIXED, moves=50, warm=10, shapes=[(1, 256), (2, 256)],
+                          use_cache=False)
+    assert (shape.cluster, shape.threads) in [(1, 256), (2, 256)]
+    assert all("moves_per_s" in row for row in shape.table)
+    for g, (xyz, st) in zip(gs, before):
+        np.testing.assert_array_equal(g.adsorbates(), xyz)
+        st2 = g.state()
+        np.testing.assert_array_equal(st2["counters"][:15], st["counters"][:15])
+        assert st2["step"] == st["step"]
