@@ -68,6 +68,8 @@ def parse_args():
     p.add_argument("--ref-cycles", type=int, default=10)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--serve-jobs", type=int, default=300, help="jobs of the served Poisson stream (0 = skip)")
+    p.add_argument("--serve-rate", type=float, default=200.0, help="mean arrivals per second")
     return p.parse_args()
 
 
@@ -370,6 +372,8 @@ def run_ours(args):
         line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_gpu"] = plain_gpu_rate(native, stream)
+    if rank == 0 and world == 1 and args.serve_jobs > 0:
+        line["serving"] = serving_run(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_SIMULATE):
         cores = min(cpu_cores(), len(sys_list))
         tmp = tempfile.mkdtemp(prefix="raspa_ref_")
@@ -387,6 +391,22 @@ def run_ours(args):
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def serving_run(args):
+    """The served workload: a Poisson stream of methane / CO2 isotherm-point
+    jobs (frameworks of 288-4096 atoms per unit cell, 500-3000 cycles of 20
+    MC steps, pressures 1e3-1e7 Pa) through the continuous-batching server.
+    Latency = finish - arrival, wall clock, including queueing."""
+    from raspa2_b200 import serve
+    jobs = serve.served_jobs(args.serve_jobs, rate=args.serve_rate, seed=3)
+    srv = serve.Server()
+    st = srv.run(jobs, realtime=True)
+    st.update({"workload": "served isotherm points (methane/CO2)", "arrival_rate_jobs_per_s": args.serve_rate,
+               "launch_shape": {"cluster": srv.cluster, "threads": srv.threads}, "chunk_steps": srv.chunk,
+               "slots": srv.max_slots, "mem_budget_gb": srv.mem_budget / 1e9,
+               "status_nonzero_jobs": int(sum(1 for j in jobs if j.result["status"]))})
+    return st
 
 
 def plain_gpu_rate(native, stream, nsteps=2000):

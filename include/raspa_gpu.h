@@ -189,6 +189,19 @@ int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters20, 
                       unsigned long long *step);
 /* Resets the running energies to `energy8` (e.g. after rgpu_total_energy). */
 int rgpu_system_set_energy(rgpu_system *sys, const double *energy8);
+/* Step window of a system in the engine: rgpu_engine_run stops advancing it
+ * at step `end_step` (exclusive; 0 = no limit), and steps from `avg_start`
+ * on enter the ensemble sums. The reference samples its averages once per
+ * cycle (src/monte_carlo.c:580, src/statistics.c:1112); the engine samples
+ * once per MC step. */
+int rgpu_system_set_limits(rgpu_system *sys, unsigned long long end_step, unsigned long long avg_start);
+/* Ensemble sums: {steps sampled, sum N, sum N^2, sum U, sum U*N, sum U^2,
+ * 0, 0}, U = the six running energy terms added, N = molecules. Loading
+ * <N>, energy <U> and the enthalpy of adsorption
+ * (<UN> - <U><N>) / (<N^2> - <N>^2) - k_B T (src/statistics.c:4077-4079)
+ * follow from them. */
+int rgpu_system_averages(rgpu_system *sys, double *sums8);
+int rgpu_system_reset_averages(rgpu_system *sys);
 
 /* ---- measurement -------------------------------------------------------- */
 /* FP32 FMA throughput of the current device in TFLOP/s (FMA = 2 FLOP), the

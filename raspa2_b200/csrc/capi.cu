@@ -66,10 +66,12 @@ struct rgpu_system {
   double *kfactor;
   double2 *sk_fw, *sk_ads, *ds;
   double *ads_xyz;
+  RgpuState *state;           /* one block; the pointers below point into it */
   int *nmol;
   double *energy;
   unsigned long long *step;
   long long *counters;
+  double *sums;
   int *status;
   int4 *rec32;
   void *rec64;
@@ -77,6 +79,7 @@ struct rgpu_system {
   double *io_xyz, *io_out, *io_q;
   int *io_atom, *io_excl, *io_ov;
   /* host mirrors */
+  RgpuState h_state;          /* initial state at creation; last state read */
   std::vector<double> h_xyz;  /* [nmol*natom*3] */
   int h_nmol;
   int records_stale;          /* device records must be rebuilt from ads_xyz */
@@ -98,7 +101,7 @@ static void sys_free(rgpu_system *s)
 {
   if (!s) return;
   void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->tiles_d, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
-                  s->nmol, s->energy, s->step, s->counters, s->status, s->rec32, s->rec64, s->io_xyz,
+                  s->state, s->rec32, s->rec64, s->io_xyz,
                   s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -184,6 +187,8 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
 
   rgpu_system *s = new rgpu_system();
   memset(&s->h, 0, sizeof(RgpuSys));
+  memset(&s->h_state, 0, sizeof(RgpuState));
+  s->h_state.step[1] = ~0ULL;   /* no step limit */
   s->d = *d;
   s->h_nmol = 0;
   s->records_stale = 0;
@@ -399,11 +404,13 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   ALLOC(s->sk_ads, sizeof(double2) * nk1);
   ALLOC(s->ds, sizeof(double2) * nk1);
   ALLOC(s->ads_xyz, sizeof(double) * 3 * nads);
-  ALLOC(s->nmol, sizeof(int));
-  ALLOC(s->energy, sizeof(double) * RGPU_NE);
-  ALLOC(s->step, sizeof(unsigned long long));
-  ALLOC(s->counters, sizeof(long long) * RGPU_NCNT);
-  ALLOC(s->status, sizeof(int));
+  ALLOC(s->state, sizeof(RgpuState));
+  s->nmol = &s->state->nmol;
+  s->energy = s->state->energy;
+  s->step = s->state->step;
+  s->counters = s->state->counters;
+  s->sums = s->state->sums;
+  s->status = &s->state->status;
   ALLOC(s->rec32, sizeof(int4) * nads);
   ALLOC(s->rec64, 32 * nads);
   const size_t io_n = std::max((size_t)RGPU_MAX_POS, std::max((size_t)d->nfw, nads));
@@ -426,6 +433,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   h.energy = s->energy;
   h.step = s->step;
   h.counters = s->counters;
+  h.sums = s->sums;
   h.status = s->status;
   cudaStream_t st = s->st;
   int rc = RGPU_SUCCESS;
@@ -433,10 +441,8 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     if (cudaMemcpyAsync(s->fw64, fw64.data(), sizeof(double4) * d->nfw, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(s->fw32, fw32.data(), sizeof(int4) * 32 * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(s->tiles_d, tiles.data(), sizeof(TileRec) * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
-        cudaMemsetAsync(s->nmol, 0, sizeof(int), st) || cudaMemsetAsync(s->energy, 0, sizeof(double) * RGPU_NE, st) ||
-        cudaMemsetAsync(s->step, 0, sizeof(unsigned long long), st) ||
-        cudaMemsetAsync(s->counters, 0, sizeof(long long) * RGPU_NCNT, st) ||
-        cudaMemsetAsync(s->status, 0, sizeof(int), st) || cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * nk1, st) ||
+        cudaMemcpyAsync(s->state, &s->h_state, sizeof(RgpuState), cudaMemcpyHostToDevice, st) ||
+        cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * nk1, st) ||
         cudaMemsetAsync(s->sk_fw, 0, sizeof(double2) * nk1, st) ||
         cudaMemcpyAsync(s->d_sys, &h, sizeof(RgpuSys), cudaMemcpyHostToDevice, st)) {
       rc = fail(RGPU_E_CUDA, "upload");
@@ -1019,11 +1025,37 @@ extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *cou
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
   CK(cudaDeviceSynchronize());
-  if (energy8) CK(cudaMemcpy(energy8, s->energy, sizeof(double) * RGPU_NE, cudaMemcpyDeviceToHost));
-  if (counters20) CK(cudaMemcpy(counters20, s->counters, sizeof(long long) * RGPU_NCNT, cudaMemcpyDeviceToHost));
-  if (nmol) CK(cudaMemcpy(nmol, s->nmol, sizeof(int), cudaMemcpyDeviceToHost));
-  if (status) CK(cudaMemcpy(status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (step) CK(cudaMemcpy(step, s->step, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&s->h_state, s->state, sizeof(RgpuState), cudaMemcpyDeviceToHost));
+  if (energy8) memcpy(energy8, s->h_state.energy, sizeof(double) * RGPU_NE);
+  if (counters20) memcpy(counters20, s->h_state.counters, sizeof(long long) * RGPU_NCNT);
+  if (nmol) *nmol = s->h_state.nmol;
+  if (status) *status = s->h_state.status;
+  if (step) *step = s->h_state.step[0];
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_set_limits(rgpu_system *s, unsigned long long end_step, unsigned long long avg_start)
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  unsigned long long v[2] = {end_step ? end_step : ~0ULL, avg_start};
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(s->step + 1, v, sizeof v, cudaMemcpyHostToDevice));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_averages(rgpu_system *s, double *sums8)
+{
+  if (!s || !sums8) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(sums8, s->sums, sizeof(double) * RGPU_NSUM, cudaMemcpyDeviceToHost));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_reset_averages(rgpu_system *s)
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemset(s->sums, 0, sizeof(double) * RGPU_NSUM));
   return RGPU_SUCCESS;
 }
 

@@ -102,6 +102,7 @@ struct Ctl {
   /* work done: pairs visited, in cut-off, charged in cut-off, k x site, k */
   unsigned long long work[5];
   long long cyc[2];           /* clock cycles in evaluations and Ewald sums */
+  double sums[RGPU_NSUM];     /* ensemble sums of this launch */
 };
 static_assert(sizeof(Ctl) <= 4096, "control block exceeds its shared-memory slot");
 
@@ -682,6 +683,7 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
     if (threadIdx.x == 0) {
       C.cyc[0] = C.cyc[1] = 0;
       C.status = 0;
+      for (int k = 0; k < RGPU_NSUM; k++) C.sums[k] = 0.0;
       C.nmol = *S.nmol;
       C.nads = C.nmol * S.natom;
     }
@@ -752,9 +754,10 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
         atom_store(E, mm, a, x);
     }
     __syncthreads();
-    const uint64_t step0 = *S.step;
+    const uint64_t step0 = S.step[0], step_end = S.step[1], avg0 = S.step[2];
     const long long t_start = clock64();
-    for (long long it = 0; it < nsteps; it++) {
+    long long it = 0;
+    for (; it < nsteps && step0 + (uint64_t)it < step_end; it++) {
       const uint64_t step = step0 + (uint64_t)it;
       /* this step's random numbers, one Philox block per thread */
       double *rb = C.rnd[it & 1];
@@ -767,20 +770,31 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
       const int nmol = C.nmol;
       share(C.nads, rank, csize, E.sl.ads_lo, E.sl.ads_hi);
       if (mv <= 1) {
-        if (nmol == 0 || (mv == 1 && S.natom == 1)) continue;
-        if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + mv]++; }
-        step_displace<MIXED>(E, mv);
+        if (!(nmol == 0 || (mv == 1 && S.natom == 1))) {
+          if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + mv]++; }
+          step_displace<MIXED>(E, mv);
+        }
       } else if (mv == 2) {
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 2]++; }
         if (nmol >= S.maxmol) {
           if (threadIdx.x == 0) C.status |= RGPU_ERR_MAXMOL;
-          continue;
+        } else {
+          step_swap<MIXED>(E, true);
         }
-        step_swap<MIXED>(E, true);
       } else {
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 3]++; }
-        if (nmol == 0) continue;
-        step_swap<MIXED>(E, false);
+        if (nmol != 0) step_swap<MIXED>(E, false);
+      }
+      /* ensemble sums after the step (thread 0 owns the running values) */
+      if (threadIdx.x == 0 && step >= avg0) {
+        const double n = (double)C.nmol;
+        const double u = C.energy[0] + C.energy[1] + C.energy[2] + C.energy[3] + C.energy[4] + C.energy[5];
+        C.sums[RGPU_SUM_SAMPLES] += 1.0;
+        C.sums[RGPU_SUM_N] += n;
+        C.sums[RGPU_SUM_N2] += n * n;
+        C.sums[RGPU_SUM_U] += u;
+        C.sums[RGPU_SUM_UN] += u * n;
+        C.sums[RGPU_SUM_U2] += u * u;
       }
     }
     __syncthreads();
@@ -801,7 +815,8 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
       if (threadIdx.x < RGPU_NE) S.energy[threadIdx.x] = C.energy[threadIdx.x];
       if (threadIdx.x == 0) {
         *S.nmol = C.nmol;
-        *S.step = step0 + (uint64_t)nsteps;
+        S.step[0] = step0 + (uint64_t)it;
+        for (int k = 0; k < RGPU_NSUM; k++) S.sums[k] += C.sums[k];
         for (int c = 0; c < RGPU_CNT_PAIRS; c++) S.counters[c] += C.cnt[c];
         *S.status |= C.status;
         S.counters[RGPU_CNT_CYCLES] += clock64() - t_start;

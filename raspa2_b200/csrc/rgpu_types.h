@@ -54,6 +54,32 @@ enum {
   RGPU_ERR_NONFINITE = 2,   /* a non-finite energy reached an acceptance test */
 };
 
+/* per-system sums for ensemble averages, over the steps at or after
+ * RgpuState.step[2] */
+enum {
+  RGPU_SUM_SAMPLES = 0,  /* steps sampled */
+  RGPU_SUM_N = 1,        /* molecules */
+  RGPU_SUM_N2 = 2,
+  RGPU_SUM_U = 3,        /* total energy (the six running terms) */
+  RGPU_SUM_UN = 4,
+  RGPU_SUM_U2 = 5,
+  RGPU_NSUM = 8
+};
+
+/* The mutable state of one system in device memory, one block so that the
+ * host reads it with one copy. */
+typedef struct {
+  double energy[RGPU_NE];            /* running energies */
+  long long counters[RGPU_NCNT];
+  double sums[RGPU_NSUM];
+  /* [0] next step index, [1] step at which the engine stops advancing this
+   * system (exclusive), [2] first step entering the sums, [3] unused */
+  unsigned long long step[4];
+  int nmol;
+  int status;
+  int pad[2];
+} RgpuState;
+
 typedef struct {
   double eps4, sig2, shift;   /* 4*epsilon, sigma^2, U(rc) */
 } RgpuLJ;
@@ -121,9 +147,10 @@ typedef struct RgpuSys {
   double2 *sk_ads;            /* [nk] */
   double *ads_xyz;            /* [maxmol*natom*3] authoritative positions */
   int *nmol;                  /* [1] */
-  double *energy;             /* [RGPU_NE] running totals */
-  unsigned long long *step;   /* [1] next step index */
+  double *energy;             /* [RGPU_NE] running totals (inside the RgpuState block) */
+  unsigned long long *step;   /* [4], see RgpuState.step */
   long long *counters;        /* [RGPU_NCNT] */
+  double *sums;               /* [RGPU_NSUM] */
   int *status;                /* [1] */
 } RgpuSys;
 

@@ -29,7 +29,8 @@ EXPORTS = [
     "rgpu_ewald_fourier_difference", "rgpu_ewald_accept", "rgpu_total_energy", "rgpu_grid_build",
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
-    "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc",
+    "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
+    "rgpu_system_reset_averages",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -238,6 +239,27 @@ class GpuSystem:
         _check(load().rgpu_system_state(self.h, e.ctypes.data_as(_dp), c.ctypes.data_as(C.POINTER(C.c_longlong)),
                                         C.byref(n), C.byref(st), C.byref(step)))
         return {"energy": e, "counters": c, "nmol": n.value, "status": st.value, "step": step.value}
+
+    def set_limits(self, end_step: int = 0, avg_start: int = 0):
+        """The engine stops advancing this system at step `end_step`
+        (exclusive, 0 = never) and samples averages from `avg_start` on."""
+        _check(load().rgpu_system_set_limits(self.h, C.c_ulonglong(end_step), C.c_ulonglong(avg_start)))
+
+    def averages(self) -> dict:
+        """Ensemble averages over the sampled steps: loading <N>, energy <U>
+        (internal units), enthalpy of adsorption (internal units, from the
+        N-U fluctuation formula) and the raw sums."""
+        sm = np.zeros(8)
+        _check(load().rgpu_system_averages(self.h, sm.ctypes.data_as(_dp)))
+        n = max(sm[0], 1.0)
+        N, N2, U, UN = sm[1] / n, sm[2] / n, sm[3] / n, sm[4] / n
+        var = N2 - N * N
+        kT = units.K_B * self.sysm.temperature
+        dh = (UN - U * N) / var - kT if var > 0 else float("nan")
+        return {"samples": int(sm[0]), "loading": N, "energy": U, "enthalpy": dh, "sums": sm}
+
+    def reset_averages(self):
+        _check(load().rgpu_system_reset_averages(self.h))
 
     def set_energy(self, e8):
         e = _arr(np.resize(np.asarray(e8, float), 8), np.float64)

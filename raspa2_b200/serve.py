@@ -1,0 +1,233 @@
+"""Continuous-batching server of isotherm-point GCMC jobs on one GPU.
+
+A job is one adsorption state point: a framework, an adsorbate, a temperature
+and a pressure, run for a number of MC steps. The first `equil` steps
+equilibrate the loading; the steps after them are sampled.
+
+The server keeps every admitted job's state on the device until the job
+ends: positions, S(k) and the running energies. It advances all admitted
+jobs together, one engine launch of `chunk` MC steps at a time, so
+`chunk` is the granularity at which jobs are admitted and retired. Between
+launches:
+
+- jobs whose step count is reached are retired, and their averages are read
+  back;
+- jobs that have arrived are admitted, as long as both hold:
+  - an engine slot is free (one cluster per job; slots = SMs / cluster
+    size);
+  - the job's estimated device-memory footprint fits the budget.
+
+A newly admitted job's device set-up (framework upload, structure factors)
+is issued on its own stream while the current launch runs, so admission
+overlaps the other jobs' work on the GPU.
+
+The engine stops each job exactly at its step count (rgpu_system_set_limits).
+Each job has its own random stream, and the launch shape is fixed for the
+server's lifetime. A job's result is therefore bitwise the same whether it
+runs alone or in a mix, whatever else is admitted beside it.
+
+This is the host-side request loop; all MC work runs in the engine kernel.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import native, systems, units
+
+# a reference cycle is max(MinimumInnerCycles = 20, N) MC steps
+# (src/monte_carlo.c:367, src/input.c:346)
+RASPA_MIN_STEPS_PER_CYCLE = 20
+
+
+@dataclasses.dataclass
+class Job:
+    id: int
+    system: systems.System
+    steps: int                  # MC steps to run
+    equil: int = 0              # steps before sampling starts
+    seed: int = 1
+    arrival: float = 0.0        # seconds after the stream starts
+    maxmol: int = 512
+    # filled in by the server
+    admitted: Optional[float] = None
+    finished: Optional[float] = None
+    result: Optional[dict] = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def footprint_bytes(job: Job) -> int:
+    """Device memory of one job as rgpu_system_create allocates it, plus the
+    engine's per-system descriptor."""
+    s = job.system
+    nfw = s.n_framework()
+    ntile = (nfw + 31) // 32 + 8
+    nk = len(systems.kvector_indices(s.kmax)) if s.ewald else 1
+    nads = job.maxmol * s.molecule.n_atoms
+    io_n = max(64, nfw, nads)
+    b = nfw * 32 + ntile * (32 * 16 + 32)          # fw64, fw32, tiles
+    b += nk * (4 + 8 + 16 * 3)                     # kvec, kfactor, S_fw, S_ads, dS
+    b += nads * (24 + 16 + 32)                     # positions, records
+    b += io_n * 32 + 64 * (32 + 12) + 4096         # per-call scratch, descriptor, state
+    return int(b)
+
+
+class Server:
+    """Admits, advances and retires jobs; see the module docstring."""
+
+    def __init__(self, precision: int = native.RGPU_MIXED, threads: int = 1024, cluster: int = 1,
+                 chunk: int = 400, max_slots: Optional[int] = None, mem_budget: float = 150e9):
+        import torch
+
+        self.precision = precision
+        self.threads = threads
+        self.cluster = cluster
+        self.chunk = chunk
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        self.max_slots = max_slots or max(1, sms // cluster)
+        self.mem_budget = mem_budget
+        self.stream = torch.cuda.Stream()
+        self.launches = 0
+
+    def _admit(self, job: Job, now: float) -> "native.GpuSystem":
+        g = native.GpuSystem(job.system, maxmol=job.maxmol, seed=job.seed, stream_id=job.id)
+        g.set_adsorbates(np.zeros((0, job.system.molecule.n_atoms, 3)))
+        g.set_limits(job.steps, job.equil)
+        job.admitted = now
+        return g
+
+    @staticmethod
+    def _result(job: Job, g: "native.GpuSystem") -> dict:
+        st = g.state()
+        av = g.averages()
+        kT = units.K_B * job.system.temperature
+        return {"loading": av["loading"], "energy_K": av["energy"] / units.K_B,
+                "enthalpy_K": av["enthalpy"] / units.K_B if np.isfinite(av["enthalpy"]) else None,
+                "samples": av["samples"], "final_nmol": st["nmol"], "steps": int(st["step"]),
+                "status": st["status"], "energy_terms": st["energy"][:6].tolist(),
+                "counters": st["counters"][:10].tolist(), "kT": kT}
+
+    def run(self, jobs: Sequence[Job], realtime: bool = True) -> dict:
+        """Serves `jobs` (arrival times relative to the call) to completion.
+        With realtime=False every job is available at once. Returns the
+        latency and throughput figures; per-job results are on the jobs."""
+        import torch
+
+        pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
+        waiting: collections.deque = collections.deque()
+        active: List[list] = []          # [job, GpuSystem, steps done, footprint]
+        mem_used = 0
+        eng = None
+        dirty = True
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0  # noqa: E731
+        total_steps = 0
+        busy = 0.0
+        max_active = 0
+
+        def admit_ready():
+            nonlocal mem_used, dirty
+            t = now()
+            while pending and (pending[0].arrival <= t or not realtime):
+                waiting.append(pending.popleft())
+            while waiting and len(active) < self.max_slots:
+                fp = footprint_bytes(waiting[0])
+                if mem_used + fp > self.mem_budget and active:
+                    break
+                job = waiting.popleft()
+                active.append([job, self._admit(job, now()), 0, fp])
+                mem_used += fp
+                dirty = True
+
+        while pending or waiting or active:
+            admit_ready()
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
+                continue
+            if dirty:
+                if eng is not None:
+                    eng.close()
+                eng = native.Engine([a[1] for a in active], precision=self.precision, threads=self.threads,
+                                    cluster=self.cluster)
+                dirty = False
+            running = list(active)                            # the jobs in this launch
+            max_active = max(max_active, len(running))
+            tl = now()
+            eng.run(self.chunk, self.stream.cuda_stream)      # asynchronous
+            self.launches += 1
+            admit_ready()                                     # overlaps the launch
+            eng.sync()
+            busy += now() - tl
+            retired = set()
+            for a in running:
+                job, g, done, fp = a
+                adv = min(self.chunk, job.steps - done)       # the engine stops each job at its limit
+                total_steps += adv
+                a[2] = done + adv
+                if a[2] >= job.steps:
+                    job.result = self._result(job, g)
+                    job.finished = now()
+                    g.close()
+                    mem_used -= fp
+                    retired.add(job.id)
+                    dirty = True
+            active = [a for a in active if a[0].id not in retired]
+        if eng is not None:
+            eng.close()
+        torch.cuda.synchronize()
+        makespan = now()
+        lat = np.array([j.latency for j in jobs]) * 1e3
+        wait = np.array([j.admitted - j.arrival for j in jobs]) * 1e3
+        return {"jobs": len(jobs), "makespan_s": makespan, "launches": self.launches,
+                "p50_job_ms": float(np.percentile(lat, 50)), "p99_job_ms": float(np.percentile(lat, 99)),
+                "p50_wait_ms": float(np.percentile(wait, 50)), "p99_wait_ms": float(np.percentile(wait, 99)),
+                "mc_steps": int(total_steps), "mc_steps_per_s": total_steps / makespan, "max_active": max_active,
+                "p50_service_ms": float(np.percentile([(j.finished - j.admitted) * 1e3 for j in jobs], 50)),
+                "gpu_busy_frac": busy / makespan}
+
+
+# --------------------------------------------------------------------------
+# served workload: Poisson stream of methane / CO2 isotherm points
+
+def _framework_templates(n_each: int, seed: int) -> List[systems.System]:
+    """Distinct frameworks the jobs draw from: methane-type (neutral, the
+    config-0 density) and CO2-type (charged, the config-1 density), sizes
+    log-spaced over 288-4096 atoms."""
+    rng = np.random.default_rng(seed)
+    out = []
+    sizes = np.unique(np.round(np.geomspace(288, 4096, n_each)).astype(int))
+    for i, n in enumerate(sizes):
+        out.append(systems.methane_like_system(seed=seed * 100 + i, n_atoms=int(n)))
+        cell = 25.8 * (n / 1536.0) ** (1.0 / 3.0)
+        out.append(systems.co2_system(seed=seed * 100 + 50 + i, n_atoms=int(n), cell=float(cell),
+                                      kmax=int(rng.integers(6, 11)), name=f"co2_served{i}"))
+    return out
+
+
+def served_jobs(n: int, rate: float = 200.0, seed: int = 3, cycles=(500, 3000),
+                templates: Optional[List[systems.System]] = None) -> List[Job]:
+    """`n` jobs arriving as a Poisson stream of `rate` jobs/s. Each job is a
+    state point (pressure log-uniform 1e3-1e7 Pa, T in {273, 298, 323} K) of
+    one of the framework templates, run for a uniform number of cycles in
+    `cycles`; a cycle is 20 MC steps (the reference's minimum per cycle);
+    the first third is equilibration."""
+    rng = np.random.default_rng(seed)
+    templates = templates or _framework_templates(8, seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    jobs = []
+    for i in range(n):
+        base = templates[int(rng.integers(len(templates)))]
+        p = float(10.0 ** rng.uniform(3.0, 7.0))
+        T = float((273.0, 298.0, 323.0)[int(rng.integers(3))])
+        s = dataclasses.replace(base, pressure=p, temperature=T, name=f"{base.name}_j{i}")
+        steps = int(rng.integers(cycles[0], cycles[1] + 1)) * RASPA_MIN_STEPS_PER_CYCLE
+        jobs.append(Job(id=i, system=s, steps=steps, equil=steps // 3, seed=1000 + i, arrival=float(t[i])))
+    return jobs

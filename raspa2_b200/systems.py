@@ -293,6 +293,29 @@ def methane_system(seed: int = 0, cycles_hint: int = 2000, layout: str = "porous
         seed=seed)
 
 
+def methane_like_system(seed: int = 0, n_atoms: int = 288, temperature: float = 300.0,
+                        pressure: float = 1e5) -> System:
+    """Methane in a neutral Si/O framework of `n_atoms` atoms at the
+    density of the 288-atom x 2x2x3 methane system (3456 atoms in
+    40.0 x 39.8 x 40.2 A), in a cubic cell; cells narrower than 24 A are
+    replicated 2x2x2."""
+    rng = np.random.default_rng(seed)
+    density = 3456.0 / (40.0 * 39.8 * 40.2)
+    L = (n_atoms / density) ** (1.0 / 3.0)
+    cell = np.array([L, L, L])
+    pore = pore_radius(cell, VOID_FRACTION, rng)
+    frac = _quantise_frac(poisson_disk(rng, n_atoms, cell, 1.6, pore=pore))
+    n_si = n_atoms // 3
+    types = ["Sifw"] * n_si + ["Ofw"] * (n_atoms - n_si)
+    reps = np.array([2, 2, 2]) if L < 24.0 else np.array([1, 1, 1])
+    return System(
+        name=f"methane_n{n_atoms}_s{seed}", unit_cell=cell, unit_cells=reps,
+        frac=frac, uc_types=types, uc_charges=np.zeros(n_atoms), molecule=METHANE,
+        temperature=temperature, pressure=pressure, cutoff=12.0, ewald=False,
+        moves=MoveMix(translation=1.0, rotation=0.0, swap_insert=0.5, swap_delete=0.5),
+        seed=seed)
+
+
 def co2_system(seed: int = 1, n_atoms: int = 1536, cell: float = 25.8,
                kmax: int = 8, temperature: float = 298.0, pressure: float = 1e5,
                dmin: float = 1.5, name: Optional[str] = None, layout: str = "porous") -> System:
