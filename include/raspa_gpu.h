@@ -180,6 +180,10 @@ int rgpu_engine_destroy(rgpu_engine *eng);
  * cudaStream_t or NULL for the library stream). */
 int rgpu_engine_run(rgpu_engine *eng, long long nsteps, void *stream);
 int rgpu_engine_sync(rgpu_engine *eng);
+/* With `on` != 0, rgpu_engine_run replays a CUDA graph of the launch
+ * (captured on the first run, and again whenever nsteps changes) instead
+ * of launching the kernel directly. */
+int rgpu_engine_use_graph(rgpu_engine *eng, int on);
 /* Running energies (8 doubles, first six as rgpu_total_energy), counters
  * (20: attempts[4], accepted[4], counted moves, overlaps, pairs visited,
  * pairs in cut-off, charged pairs in cut-off, k x site products, k sums,

@@ -94,7 +94,12 @@ struct rgpu_engine {
   std::vector<rgpu_system *> sys;
   RgpuSys *d_systems;
   int mixed, threads, kw, max_ads, cluster, fw_items, tile_items, k_items;
+  size_t smem;
   cudaStream_t st;
+  /* CUDA graph of one launch, replayed by rgpu_engine_run when enabled */
+  int use_graph;
+  cudaGraphExec_t gexec;
+  long long g_nsteps;
 };
 
 static void sys_free(rgpu_system *s)
@@ -967,6 +972,10 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
   e->fw_items = fw_try[pick];
   e->tile_items = tile_try[pick];
   e->k_items = k_try[pick];
+  e->smem = rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw, e->k_items, threads);
+  e->use_graph = 0;
+  e->gexec = nullptr;
+  e->g_nsteps = -1;
   std::vector<RgpuSys> hs(n);
   for (int i = 0; i < n; i++) {
     hs[i] = e->sys[i]->h;
@@ -989,6 +998,7 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
 extern "C" int rgpu_engine_destroy(rgpu_engine *e)
 {
   if (!e) return RGPU_SUCCESS;
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
   cudaFree(e->d_systems);
   delete e;
   return RGPU_SUCCESS;
@@ -1001,9 +1011,40 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   const int n = (int)e->sys.size();
-  CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
-                        e->k_items, e->cluster, e->threads, st));
+  CK(rgpu_engine_prepare(e->mixed, e->smem));
+  if (!e->use_graph) {
+    CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
+                          e->k_items, e->cluster, e->threads, st));
+  } else {
+    if (!e->gexec || e->g_nsteps != nsteps) {
+      if (e->gexec) {
+        CK(cudaGraphExecDestroy(e->gexec));
+        e->gexec = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      cudaError_t le = rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items,
+                                          e->tile_items, e->k_items, e->cluster, e->threads, st);
+      cudaError_t ce = cudaStreamEndCapture(st, &g);
+      if (le != cudaSuccess || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(RGPU_E_CUDA, "engine capture: %s", cudaGetErrorString(le != cudaSuccess ? le : ce));
+      }
+      cudaError_t ie = cudaGraphInstantiate(&e->gexec, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) return fail(RGPU_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+      e->g_nsteps = nsteps;
+    }
+    CK(cudaGraphLaunch(e->gexec, st));
+  }
   for (rgpu_system *s : e->sys) s->records_stale = 1;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_use_graph(rgpu_engine *e, int on)
+{
+  if (!e) return fail(RGPU_E_INVALID, "bad argument");
+  e->use_graph = on != 0;
   return RGPU_SUCCESS;
 }
 

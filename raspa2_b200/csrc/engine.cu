@@ -831,6 +831,12 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
   cl.sync();
 }
 
+cudaError_t rgpu_engine_prepare(int mixed, size_t smem)
+{
+  if (mixed) return cudaFuncSetAttribute(rgpu_engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaFuncSetAttribute(rgpu_engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
                                int threads, cudaStream_t st)
@@ -849,19 +855,15 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e;
-  if (mixed) {
-    e = cudaFuncSetAttribute(rgpu_engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+  /* the dynamic shared-memory limit is raised by rgpu_engine_prepare, outside
+   * any stream capture */
+  if (mixed)
     e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
                            tile_items, k_items);
-  } else {
-    e = cudaFuncSetAttribute(rgpu_engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+  else
     e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<false>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
                            tile_items, k_items);
-  }
-  if (e != cudaSuccess) return e;
-  return cudaGetLastError();
+  return e;
 }
 
 struct CallSmem {

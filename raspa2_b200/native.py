@@ -30,7 +30,7 @@ EXPORTS = [
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
-    "rgpu_system_reset_averages",
+    "rgpu_system_reset_averages", "rgpu_engine_use_graph",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -318,6 +318,10 @@ class Engine:
 
     def sync(self):
         _check(load().rgpu_engine_sync(self.h))
+
+    def use_graph(self, on: bool = True):
+        """Replay a CUDA graph of the launch in run() (rgpu_engine_use_graph)."""
+        _check(load().rgpu_engine_use_graph(self.h, C.c_int(1 if on else 0)))
 
     def close(self):
         if getattr(self, "h", None):

@@ -1,0 +1,112 @@
+"""Generates tests/golden/stat_*.json: ensemble averages of whole GCMC runs of
+the reference program, the statistical pin of the engine.
+
+Runs in the build container only (it needs oracle/_ref/simulate, built from
+the reference's sources by `make -C oracle ref`). Each case runs the
+reference on one of the synthetic systems from an empty framework with
+`seeds` independent random seeds (one process per seed), then parses each
+run's output:
+
+- average absolute loading [molecules/unit cell] and its block error;
+- enthalpy of adsorption [K] and its block error.
+
+The JSON keeps every seed's values and their mean and standard error across
+seeds. tests/test_gpu_stats.py compares the engine's averages against it.
+
+    python tests/golden/make_stat_golden.py [--workdir DIR] [case ...]
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from raspa2_b200 import raspa_io, systems  # noqa: E402
+
+SIMULATE = os.path.join(ROOT, "oracle", "_ref", "simulate")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# name -> (builder, state point, initialisation cycles, production cycles)
+CASES = {
+    "methane_config0_1e5": (lambda: systems.methane_system(seed=0), dict(pressure=1e5, temperature=300.0), 1000, 8000),
+    "methane_config0_1e7": (lambda: systems.methane_system(seed=0), dict(pressure=1e7, temperature=300.0), 1000, 3000),
+    "co2_config1_1e5": (lambda: systems.co2_system(seed=1), dict(pressure=1e5, temperature=298.0), 1500, 2500),
+}
+SEEDS = 8
+
+
+def parse(path):
+    txt = open(path).read()
+    m = re.search(r"Average loading absolute \[molecules/unit cell\]\s+([-\d.eE+]+) \+/-\s+([-\d.eE+]+)", txt)
+    loading, loading_err = float(m.group(1)), float(m.group(2))
+    blk = txt.split("Enthalpy of adsorption:")[1]
+    m = re.search(r"Average\s+([-\d.eE+]+) \+/-\s+([-\d.eE+]+) \[K\]", blk)
+    h, h_err = float(m.group(1)), float(m.group(2))
+    return {"loading": loading, "loading_err": loading_err, "enthalpy_K": h, "enthalpy_err_K": h_err}
+
+
+def run_case(name, workdir):
+    build, state, init, prod = CASES[name]
+    s = dataclasses.replace(build(), **state)
+    dirs = []
+    for k in range(SEEDS):
+        d = os.path.join(workdir, f"{name}_{k}")
+        raspa_io.write_inputs(s, d, cycles=prod, init_cycles=init, print_every=10 ** 9, seed=9001 + 17 * k)
+        dirs.append(d)
+
+    def one(d):
+        r = subprocess.run([SIMULATE, "-i", "simulation.input"], cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"simulate failed in {d}: {r.stderr[-500:]}")
+        out = os.path.join(d, "Output", "System_0")
+        return parse(os.path.join(out, os.listdir(out)[0]))
+
+    return s, dirs, one
+
+
+def main(argv):
+    work = None
+    if argv[:1] == ["--workdir"]:
+        work, argv = argv[1], argv[2:]
+        os.makedirs(work, exist_ok=True)
+    names = argv or list(CASES)
+    work = work or tempfile.mkdtemp(prefix="raspa_stat_")
+    jobs = []
+    meta = {}
+    for name in names:
+        s, dirs, one = run_case(name, work)
+        meta[name] = s
+        jobs += [(name, d, one) for d in dirs]
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        res = list(ex.map(lambda j: (j[0], j[2](j[1])), jobs))
+    for name in names:
+        s = meta[name]
+        build, state, init, prod = CASES[name]
+        runs = [r for n, r in res if n == name]
+        L = np.array([r["loading"] for r in runs])
+        H = np.array([r["enthalpy_K"] for r in runs])
+        doc = {
+            "case": name, "system": s.name, "pressure_Pa": s.pressure, "temperature_K": s.temperature,
+            "unit_cells": [int(x) for x in s.unit_cells], "init_cycles": init, "production_cycles": prod,
+            "seeds": SEEDS, "runs": runs,
+            "loading_mean": float(L.mean()), "loading_se": float(L.std(ddof=1) / np.sqrt(len(L))),
+            "enthalpy_mean_K": float(H.mean()), "enthalpy_se_K": float(H.std(ddof=1) / np.sqrt(len(H))),
+            "source": "reference simulate (oracle/_ref) built from the reference sources",
+        }
+        with open(os.path.join(OUT, f"stat_{name}.json"), "w") as fh:
+            json.dump(doc, fh, indent=1)
+        print(name, doc["loading_mean"], "+-", doc["loading_se"], doc["enthalpy_mean_K"], "+-", doc["enthalpy_se_K"])
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

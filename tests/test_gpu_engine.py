@@ -142,3 +142,25 @@ def test_autotune_leaves_systems_untouched(cuda):
         st2 = g.state()
         np.testing.assert_array_equal(st2["counters"][:15], st["counters"][:15])
         assert st2["step"] == st["step"]
+
+
+def test_graph_replay_matches_direct_launches(cuda):
+    """rgpu_engine_use_graph: replaying the captured launch advances the
+    systems exactly as direct launches do."""
+    s = systems.tiny_co2_system(seed=7)
+    out = []
+    for graph in (False, True):
+        g = native.GpuSystem(s, maxmol=64, seed=9, stream_id=2)
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+        e = native.Engine([g], precision=native.RGPU_MIXED, threads=256, cluster=2)
+        e.use_graph(graph)
+        for _ in range(3):
+            e.run(150)
+        e.run(40)          # a different step count is captured anew
+        e.sync()
+        out.append((g.state(), g.adsorbates()))
+    (a, xa), (b, xb) = out
+    assert a["step"] == b["step"] == 490
+    np.testing.assert_array_equal(a["counters"][:15], b["counters"][:15])
+    np.testing.assert_array_equal(a["energy"], b["energy"])
+    np.testing.assert_array_equal(xa, xb)
