@@ -248,40 +248,73 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     h.kmax[c] = d->ewald ? d->kmax[c] : 0;
   }
   /* Mixed-precision layout: fixed-point coordinates (see rgpu_types.h), the
-   * framework sorted along a Morton curve of ~4 A cells and cut into tiles of
-   * 32 spatially close atoms with a bounding box each; the two low bits of
-   * the z coordinate carry the atom's segment (pseudo-atom type), an offset
-   * of at most 3 * L / 2^32 (< 1e-8 A). */
+   * framework cut into tiles of 32 spatially close atoms with a bounding box
+   * each, by recursive bisection: the atoms of a group are split at the
+   * median of their longest extent (in the unwrapped cell [0, L)) into two
+   * groups holding whole tiles, until a group is one tile. Compact tiles
+   * make the box test reject most of the atoms outside the cut-off sphere.
+   * The two low bits of the z coordinate carry the atom's segment
+   * (pseudo-atom type), an offset of at most 3 * L / 2^32 (< 1e-8 A). */
   std::vector<TileRec> tiles;
   {
-    int g[3];
-    for (int c = 0; c < 3; c++) g[c] = std::max(1, std::min(1023, (int)(d->box[c] / 4.0)));
-    std::vector<unsigned long long> key(d->nfw);
     std::vector<int> seg_of(d->nfw);
+    std::vector<double> fr((size_t)d->nfw * 3);
     for (int idx = 0; idx < d->nfw; idx++) {
       int sgi = 0;
       while (sgi + 1 < nseg && idx >= h.seg_start[sgi + 1]) sgi++;
       seg_of[idx] = sgi;
-      unsigned cell[3];
       const double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
       for (int c = 0; c < 3; c++) {
         double f = p[c] * h.inv_box[c];
-        f -= floor(f);
-        int ci = (int)(f * g[c]);
-        cell[c] = (unsigned)std::min(std::max(ci, 0), g[c] - 1);
+        fr[3 * (size_t)idx + c] = (f - floor(f)) * d->box[c];
       }
-      unsigned long long k = 0;
-      for (int bit = 0; bit < 10; bit++)
-        for (int c = 0; c < 3; c++) k |= (unsigned long long)((cell[c] >> bit) & 1u) << (3 * bit + c);
-      key[idx] = (k << 20) | (unsigned long long)idx;
     }
     std::vector<int> sp(d->nfw);
     for (int i = 0; i < d->nfw; i++) sp[i] = i;
-    std::sort(sp.begin(), sp.end(), [&](int a, int b) { return key[a] < key[b]; });
+    /* iterative bisection over ranges [b, e) of sp */
+    std::vector<std::pair<int, int>> todo{{0, d->nfw}};
+    while (!todo.empty()) {
+      const int b = todo.back().first, e = todo.back().second;
+      todo.pop_back();
+      const int n = e - b;
+      if (n <= 32) continue;
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int i = b; i < e; i++)
+        for (int c = 0; c < 3; c++) {
+          lo[c] = std::min(lo[c], fr[3 * (size_t)sp[i] + c]);
+          hi[c] = std::max(hi[c], fr[3 * (size_t)sp[i] + c]);
+        }
+      int ax = 0;
+      for (int c = 1; c < 3; c++)
+        if (hi[c] - lo[c] > hi[ax] - lo[ax]) ax = c;
+      const int nt = (n + 31) / 32;
+      const int m = b + 32 * (nt / 2);      /* the left group holds whole tiles */
+      std::nth_element(sp.begin() + b, sp.begin() + m, sp.begin() + e, [&](int x, int y) {
+        const double fx = fr[3 * (size_t)x + ax], fy = fr[3 * (size_t)y + ax];
+        return fx < fy || (fx == fy && x < y);
+      });
+      todo.push_back({b, m});
+      todo.push_back({m, e});
+    }
     const int ntile = (d->nfw + 31) / 32;
+    /* Tiles are stored in bit-reversed order of their place in the
+     * bisection, so that every contiguous range of 1/2^k of them (one CTA's
+     * share of a cluster, one warp's chunk) samples the whole framework
+     * evenly and carries about the same work for any bead position. */
+    std::vector<int> order;
+    {
+      int bits = 0;
+      while ((1 << bits) < ntile) bits++;
+      for (int i = 0; i < (1 << bits); i++) {
+        int r = 0;
+        for (int k = 0; k < bits; k++) r |= ((i >> k) & 1) << (bits - 1 - k);
+        if (r < ntile) order.push_back(r);
+      }
+    }
     fw32.assign((size_t)ntile * 32, make_int4(0, 0, 0, 0));
     tiles.resize(ntile);
-    for (int t = 0; t < ntile; t++) {
+    for (int o = 0; o < ntile; o++) {
+      const int t = order[o];
       const int n = std::min(32, d->nfw - 32 * t);
       const double4 r0 = fw64[sp[32 * t]];
       double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -305,7 +338,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
         float qf = (float)fw64[idx].w;
         int qb;
         memcpy(&qb, &qf, 4);
-        fw32[(size_t)32 * t + j] = make_int4(v[0], v[1], v[2], qb);
+        fw32[(size_t)32 * o + j] = make_int4(v[0], v[1], v[2], qb);
       }
       TileRec tr;
       double cen[3];
@@ -327,7 +360,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       }
       tr.c = make_int4(cv[0], cv[1], cv[2], n);
       tr.h = make_float4(hh[0], hh[1], hh[2], 0.0f);
-      tiles[t] = tr;
+      tiles[o] = tr;
     }
     h.ntile = ntile;
   }
