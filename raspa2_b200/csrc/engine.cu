@@ -103,6 +103,7 @@ struct Ctl {
   unsigned long long work[5];
   long long cyc[2];           /* clock cycles in evaluations and Ewald sums */
   double sums[RGPU_NSUM];     /* ensemble sums of this launch */
+  int next;                   /* unit counter of eval_units */
 };
 static_assert(sizeof(Ctl) <= 4096, "control block exceeds its shared-memory slot");
 
@@ -212,6 +213,7 @@ __device__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
   const EvalPlan pl = eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.sc, RGPU_MAX_UNITS);
   const int per = pl.cf + pl.ca;
   __syncthreads();
+  if (threadIdx.x == 0) C.next = 0;      /* unit counter of the next evaluation */
   /* this CTA's sum per position, units in order */
   PosSum *ps = E.part + E.xb * RGPU_MAX_POS;
   for (int p = threadIdx.x; p < P; p += blockDim.x) {
@@ -663,7 +665,6 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
     E.sc.uv = E.uv;
     E.sc.uc = E.uc;
     E.sc.uo = E.uo;
-    E.sc.upos = nullptr;
     E.sc.qr2 = (float *)(smem + L.q);
     E.sc.qq = E.sc.qr2 + nwarps * 64;
     E.sc.qt = (int *)(E.sc.qq + nwarps * 64);
@@ -674,6 +675,7 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
     E.ctl = (Ctl *)(smem + L.ctl);
     Ctl &C = *E.ctl;
     E.sc.cnt = C.work;
+    E.sc.next = &C.next;
     load_sys(E.S, &systems[sysi]);
     RgpuSys &S = *E.S;
     double2 *sk_global = S.sk_ads;
@@ -683,6 +685,7 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
     if (threadIdx.x == 0) {
       C.cyc[0] = C.cyc[1] = 0;
       C.status = 0;
+      C.next = 0;
       for (int k = 0; k < RGPU_NSUM; k++) C.sums[k] = 0.0;
       C.nmol = *S.nmol;
       C.nads = C.nmol * S.natom;
@@ -875,6 +878,7 @@ struct CallSmem {
   float qr2[8 * 64], qq[8 * 64];
   int qt[8 * 64];
   double red[72];
+  int next;
 };
 
 
@@ -889,8 +893,9 @@ __global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, con
   __shared__ CallSmem sm;
   load_sys(&S, sysp);
   for (int p = threadIdx.x; p < P; p += blockDim.x) bead_set(sm.pos[p], S, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], atom[p], excl[p]);
+  if (threadIdx.x == 0) sm.next = 0;
   __syncthreads();
-  EvalScratch sc = {sm.uv, sm.uc, sm.uo, nullptr, nullptr, sm.qr2, sm.qq, sm.qt};
+  EvalScratch sc = {sm.uv, sm.uc, sm.uo, &sm.next, nullptr, sm.qr2, sm.qq, sm.qt};
   EvalSlice sl;
   sl.fw = MIXED ? (const void *)S.fw32 : (const void *)S.fw64;
   sl.tiles = S.tiles;

@@ -202,7 +202,7 @@ struct EvalScratch {
   double *uv;     /* [max units] */
   double *uc;
   int *uo;
-  int *upos;      /* unused */
+  int *next;      /* unit counter of the dynamic schedule; 0 when an evaluation starts */
   unsigned long long *cnt;   /* optional {pairs visited, in cut-off, charged in cut-off} */
   float *qr2;     /* per-warp queue of in-cut-off pairs (mixed path): [nwarps][64] */
   float *qq;
@@ -499,9 +499,14 @@ struct EvalSlice {
   int ads_lo, ads_hi;
 };
 
-/* The (position, chunk) units of P positions over the slice: unit u covers
- * position u / (cf + ca) and writes its FP64 sums and overlap flag to
- * sc.uv/uc/uo[u]. No block barrier; returns the plan used. */
+/* The (position, chunk) units of P positions over the slice: the unit of
+ * position p and chunk c writes its FP64 sums and overlap flag to
+ * sc.uv/uc/uo[p * (cf + ca) + c]. Warps take units dynamically from
+ * *sc.next (framework chunks of every position first, then adsorbate
+ * chunks), fetching the next index while they work on the current one, so
+ * the warps of the block finish together. The stored sums do not depend on
+ * which warp evaluated a unit. No block barrier; *sc.next is left past the
+ * last unit (the caller resets it after its barrier). Returns the plan. */
 template <bool MIXED>
 __device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
                                EvalScratch sc, int max_units)
@@ -510,14 +515,30 @@ __device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const Bead
   const int nfw = sl.fw_hi - sl.fw_lo, nads = sl.ads_hi - sl.ads_lo;
   const EvalPlan pl = eval_plan(P, nfw, nads, nw, max_units, MIXED ? 2 : 64);
   const int per = pl.cf + pl.ca;
+  const int nfu = P * pl.cf;     /* framework units */
   /* work counts of this lane, summed over its units (statistics only) */
   int nin = 0, nch = 0, nvis = 0;
-  for (int u = w; u < pl.nunits; u += nw) {
-    const int p = u / per, c = u - p * per;
+  int v = 0;
+  if (lane == 0) v = atomicAdd(sc.next, 1);
+  v = __shfl_sync(RGPU_FULL, v, 0);
+  while (v < pl.nunits) {
+    int vn = 0;
+    if (lane == 0) vn = atomicAdd(sc.next, 1);
+    int p, c;
+    if (v < nfu) {
+      c = v / P;
+      p = v - c * P;
+    } else {
+      const int v2 = v - nfu;
+      const int ca = v2 / P;
+      p = v2 - ca * P;
+      c = pl.cf + ca;
+    }
+    const int u = p * per + c;
     const BeadPos b = pos[p];
     const bool check = p < pair_check;
     int ov = 0;
-    double v, q;
+    double e_v, e_q;
     int lo, hi;
     /* chunk bounds; item counts stay far below 2^31 / RGPU_MAX_UNITS */
     if (c < pl.cf) {
@@ -536,25 +557,26 @@ __device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const Bead
       else
         unit_ads_mixed(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
                        sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
-      v = (double)warp_sum(av);
-      q = (double)warp_sum(ac);
+      e_v = (double)warp_sum(av);
+      e_q = (double)warp_sum(ac);
     } else {
       double av = 0.0, ac = 0.0;
       if (c < pl.cf)
         unit_fw_fp64(S, (const double4 *)sl.fw, b, lo, hi, check, av, ac, ov, nin, nch, nvis);
       else
         unit_ads_fp64(S, (const AdsRec64 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
-      v = warp_sum(av);
-      q = warp_sum(ac);
+      e_v = warp_sum(av);
+      e_q = warp_sum(ac);
     }
     ov = warp_or(ov);
     if (lane == 0) {
-      sc.uv[u] = v;
-      sc.uc[u] = q;
+      sc.uv[u] = e_v;
+      sc.uc[u] = e_q;
       sc.uo[u] = ov;
     }
+    v = __shfl_sync(RGPU_FULL, vn, 0);
   }
-  if (sc.cnt && w < pl.nunits) {
+  if (sc.cnt) {
     nin = __reduce_add_sync(RGPU_FULL, (unsigned)nin);
     nch = __reduce_add_sync(RGPU_FULL, (unsigned)nch);
     if (lane == 0) {
@@ -575,6 +597,7 @@ __device__ void eval_positions(const RgpuSys &S, const EvalSlice &sl, const Bead
   const EvalPlan pl = eval_units<MIXED>(S, sl, pos, P, pair_check, sc, max_units);
   const int per = pl.cf + pl.ca;
   __syncthreads();
+  if (threadIdx.x == 0) *sc.next = 0;
   for (int p = threadIdx.x; p < P; p += blockDim.x) {
     double hv = 0.0, hc = 0.0, av = 0.0, ac = 0.0;
     int ov = 0;
