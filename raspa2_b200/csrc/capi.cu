@@ -407,6 +407,18 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   h.mol_charged = molq;
   h.mol_charge = mq;
   h.self_mol = self;
+  /* the exclusion sum K qa qb erf(alpha r)/r over the molecule's charged
+   * pairs (src/ewald.c:7312-7330) is a constant of a rigid molecule */
+  h.excl_mol = 0.0;
+  if (d->ewald)
+    for (int a = 0; a < d->natom - 1; a++)
+      for (int b = a + 1; b < d->natom; b++) {
+        if (d->mol_q[a] == 0.0 || d->mol_q[b] == 0.0) continue;
+        const double *ra = d->mol_ref + 3 * a, *rb = d->mol_ref + 3 * b;
+        const double r = sqrt((ra[0] - rb[0]) * (ra[0] - rb[0]) + (ra[1] - rb[1]) * (ra[1] - rb[1]) +
+                              (ra[2] - rb[2]) * (ra[2] - rb[2]));
+        h.excl_mol += d->coulomb * d->mol_q[a] * d->mol_q[b] * erf(d->alpha * r) / r;
+      }
   h.ewald = d->ewald;
   for (int c = 0; c < 4; c++) h.cum[c] = d->move_cum[c];
   h.max_translation = d->max_translation;

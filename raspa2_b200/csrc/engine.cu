@@ -104,6 +104,7 @@ struct Ctl {
   long long cyc[2];           /* clock cycles in evaluations and Ewald sums */
   double sums[RGPU_NSUM];     /* ensemble sums of this launch */
   int next;                   /* unit counter of eval_units */
+  double ewt[2][2];           /* this CTA's Ewald sums {e_ads, e_host}, by buffer */
 };
 static_assert(sizeof(Ctl) <= 4096, "control block exceeds its shared-memory slot");
 
@@ -262,7 +263,24 @@ __device__ void engine_ewald(Eng<MIXED> &E, int ns)
     C.work[4] += (unsigned long long)(E.k1 - E.k0);
   }
   __syncthreads();
-  ewald_energy_warps<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, E.k0, E.k1, E.red + E.xb * 2 * RGPU_MAX_WARPS);
+  double *red = E.red + E.xb * 2 * RGPU_MAX_WARPS;
+  ewald_energy_warps<MIXED>(*E.S, E.tab, E.kw, E.sites, ns, E.k0, E.k1, red);
+  __syncthreads();
+  /* this CTA's total (warp 0, fixed reduction order) */
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    double a = 0.0, h = 0.0;
+    if (threadIdx.x < nw) {
+      a = red[2 * threadIdx.x];
+      h = red[2 * threadIdx.x + 1];
+    }
+    a = warp_sum(a);
+    h = warp_sum(h);
+    if (threadIdx.x == 0) {
+      C.ewt[E.xb][0] = a;
+      C.ewt[E.xb][1] = h;
+    }
+  }
   cg::this_cluster().sync();
   if (threadIdx.x == 0) C.cyc[1] += clock64() - t0;
 }
@@ -273,13 +291,11 @@ __device__ __forceinline__ void gather_ewald(const Eng<MIXED> &E, int b, double 
 {
   cg::cluster_group cl = cg::this_cluster();
   ea = eh = 0.0;
-  const int nw = blockDim.x >> 5;
+  const double *own = &E.ctl->ewt[b][0];
   for (int q = 0; q < E.csize; q++) {
-    const double *red = E.csize > 1 ? cl.map_shared_rank(E.red, q) : E.red;
-    for (int w = 0; w < nw; w++) {
-      ea += red[b * 2 * RGPU_MAX_WARPS + 2 * w];
-      eh += red[b * 2 * RGPU_MAX_WARPS + 2 * w + 1];
-    }
+    const double *t = E.csize > 1 ? cl.map_shared_rank(own, q) : own;
+    ea += t[0];
+    eh += t[1];
   }
 }
 
@@ -412,13 +428,10 @@ __device__ void step_displace(Eng<MIXED> &E, int mv)
     if (ew) {
       double ea, eh;
       gather_ewald(E, bw, ea, eh);
-      /* exclusions cancel for a rigid displacement but are kept for parity */
-      double xn[RGPU_MAX_ATOMS][3], xo[RGPU_MAX_ATOMS][3];
-      for (int a = 0; a < na; a++) {
-        xn[a][0] = E.pos[a].x; xn[a][1] = E.pos[a].y; xn[a][2] = E.pos[a].z;
-        xo[a][0] = E.pos[na + a].x; xo[a][1] = E.pos[na + a].y; xo[a][2] = E.pos[na + a].z;
-      }
-      ewald_finish(S, ea, eh, ewald_exclusion(S, xn), ewald_exclusion(S, xo), 0, 0.0, d_ads, d_host);
+      /* the exclusion energy of a rigid molecule is the same before and
+       * after the displacement (the reference's difference of the two is
+       * zero up to rounding) */
+      ewald_finish(S, ea, eh, S.excl_mol, S.excl_mol, 0, 0.0, d_ads, d_host);
     }
     double du = C.dl[0] + C.dl[1] + C.dl[2] + C.dl[3] + d_ads + d_host;
     double pacc = exp(-S.beta * du);
@@ -578,9 +591,7 @@ __device__ void step_swap(Eng<MIXED> &E, bool insert)
     if (ew) {
       double ea, eh;
       gather_ewald(E, bw, ea, eh);
-      double x[RGPU_MAX_ATOMS][3];
-      for (int a = 0; a < na; a++) { x[a][0] = E.sites[a].b.x; x[a][1] = E.sites[a].b.y; x[a][2] = E.sites[a].b.z; }
-      double ex = ewald_exclusion(S, x);
+      const double ex = S.excl_mol;      /* rigid molecule */
       double net = nmol * S.mol_charge;
       if (insert) ewald_finish(S, ea, eh, ex, 0.0, 1, net, d_ads, d_host);
       else ewald_finish(S, ea, eh, 0.0, ex, -1, net, d_ads, d_host);

@@ -751,21 +751,6 @@ __device__ void ewald_apply(const RgpuSys &S, const typename PhaseT<MIXED>::T *t
   }
 }
 
-/* intramolecular exclusion energy K qa qb erf(alpha r)/r over the charged
- * pairs of one molecule (src/ewald.c:7312-7330), FP64 */
-__device__ inline double ewald_exclusion(const RgpuSys &S, const double (*xyz)[3])
-{
-  double e = 0.0;
-  for (int a = 0; a < S.natom - 1; a++)
-    for (int b = a + 1; b < S.natom; b++) {
-      if (S.mol_q[a] == 0.0 || S.mol_q[b] == 0.0) continue;
-      double dx = xyz[a][0] - xyz[b][0], dy = xyz[a][1] - xyz[b][1], dz = xyz[a][2] - xyz[b][2];
-      double r = sqrt(dx * dx + dy * dy + dz * dz);
-      e += S.coulomb * S.mol_q[a] * S.mol_q[b] * erf(S.alpha * r) / r;
-    }
-  return e;
-}
-
 /* complete dU_ads / dU_host of src/ewald.c:7539-7565 for a change of
  * (nnew - nold) molecules, given the k-sums and the exclusion energies */
 __device__ inline void ewald_finish(const RgpuSys &S, double e_ads, double e_host, double excl_new,

@@ -125,7 +125,7 @@ typedef struct RgpuSys {
   int ewald, nk;
   int kmax[3];
   double self_mol;            /* sum over the molecule's sites of K q^2 alpha / sqrt(pi) */
-  double excl_pref;           /* unused padding for alignment */
+  double excl_mol;            /* intramolecular exclusion energy of the rigid molecule (reference geometry) */
   double uion, net_fw, mol_charge;
   /* MC */
   double cum[4];
