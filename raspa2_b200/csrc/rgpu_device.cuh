@@ -337,31 +337,36 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
   for (int tb = t0; tb < t1; tb += 32) {
     const int t = tb + lane;
     bool vis = false;
+    int tn = 0;                  /* atoms of this lane's tile */
     if (t < t1) {
       const TileRec tr = tiles[t];
+      tn = tr.c.w;
       float dx = fmaxf(fabsf(__int2float_rn(tr.c.x - b.xi) * sx) - tr.h.x, 0.0f);
       float dy = fmaxf(fabsf(__int2float_rn(tr.c.y - b.yi) * sy) - tr.h.y, 0.0f);
       float dz = fmaxf(fabsf(__int2float_rn(tr.c.z - b.zi) * sz) - tr.h.z, 0.0f);
       vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
     }
     unsigned m = __ballot_sync(RGPU_FULL, vis);
+    /* two visible tiles per pass: their loads and distances are independent */
     while (m) {
-      const int tt = tb + __ffs(m) - 1;
+      const int i1 = __ffs(m) - 1;
       m &= m - 1;
-      const int n = tiles[tt].c.w;
-      nvis += n;
-      bool in = false;
-      float r2 = 0.0f;
-      int4 f = make_int4(0, 0, 0, 0);
-      if (lane < n) {
-        f = fw[tt * 32 + lane];
-        const float dx = __int2float_rn(f.x - b.xi) * sx;
-        const float dy = __int2float_rn(f.y - b.yi) * sy;
-        const float dz = __int2float_rn(f.z - b.zi) * sz;
-        r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        in = r2 < rc2;
-      }
-      queue_add(Q, in, r2, __int_as_float(f.w), f.z & 3, av, ac, ov, nin, nch);
+      const int i2 = m ? __ffs(m) - 1 : -1;
+      m &= m - 1;
+      const int n1 = __shfl_sync(RGPU_FULL, tn, i1);
+      const int n2s = __shfl_sync(RGPU_FULL, tn, i2 >= 0 ? i2 : 0);
+      const int n2 = i2 >= 0 ? n2s : 0;
+      nvis += n1 + n2;
+      int4 f1 = make_int4(0, 0, 0, 0), f2 = make_int4(0, 0, 0, 0);
+      if (lane < n1) f1 = fw[(tb + i1) * 32 + lane];
+      if (lane < n2) f2 = fw[(tb + i2) * 32 + lane];
+      const float dx1 = __int2float_rn(f1.x - b.xi) * sx, dx2 = __int2float_rn(f2.x - b.xi) * sx;
+      const float dy1 = __int2float_rn(f1.y - b.yi) * sy, dy2 = __int2float_rn(f2.y - b.yi) * sy;
+      const float dz1 = __int2float_rn(f1.z - b.zi) * sz, dz2 = __int2float_rn(f2.z - b.zi) * sz;
+      const float r21 = fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1));
+      const float r22 = fmaf(dx2, dx2, fmaf(dy2, dy2, dz2 * dz2));
+      queue_add(Q, lane < n1 && r21 < rc2, r21, __int_as_float(f1.w), f1.z & 3, av, ac, ov, nin, nch);
+      if (i2 >= 0) queue_add(Q, lane < n2 && r22 < rc2, r22, __int_as_float(f2.w), f2.z & 3, av, ac, ov, nin, nch);
     }
   }
   queue_drain(Q, av, ac, ov, nin, nch);
