@@ -248,7 +248,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     h.kmax[c] = d->ewald ? d->kmax[c] : 0;
   }
   /* Mixed-precision layout: fixed-point coordinates (see rgpu_types.h), the
-   * framework cut into tiles of 32 spatially close atoms with a bounding box
+   * framework cut into tiles of RGPU_TILE spatially close atoms with a bounding box
    * each, by recursive bisection: the atoms of a group are split at the
    * median of their longest extent (in the unwrapped cell [0, L)) into two
    * groups holding whole tiles, until a group is one tile. Compact tiles
@@ -277,7 +277,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       const int b = todo.back().first, e = todo.back().second;
       todo.pop_back();
       const int n = e - b;
-      if (n <= 32) continue;
+      if (n <= RGPU_TILE) continue;
       double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
       for (int i = b; i < e; i++)
         for (int c = 0; c < 3; c++) {
@@ -287,8 +287,8 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       int ax = 0;
       for (int c = 1; c < 3; c++)
         if (hi[c] - lo[c] > hi[ax] - lo[ax]) ax = c;
-      const int nt = (n + 31) / 32;
-      const int m = b + 32 * (nt / 2);      /* the left group holds whole tiles */
+      const int nt = (n + RGPU_TILE - 1) / RGPU_TILE;
+      const int m = b + RGPU_TILE * (nt / 2);      /* the left group holds whole tiles */
       std::nth_element(sp.begin() + b, sp.begin() + m, sp.begin() + e, [&](int x, int y) {
         const double fx = fr[3 * (size_t)x + ax], fy = fr[3 * (size_t)y + ax];
         return fx < fy || (fx == fy && x < y);
@@ -296,7 +296,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       todo.push_back({b, m});
       todo.push_back({m, e});
     }
-    const int ntile = (d->nfw + 31) / 32;
+    const int ntile = (d->nfw + RGPU_TILE - 1) / RGPU_TILE;
     /* Tiles are stored in bit-reversed order of their place in the
      * bisection, so that every contiguous range of 1/2^k of them (one CTA's
      * share of a cluster, one warp's chunk) samples the whole framework
@@ -311,15 +311,15 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
         if (r < ntile) order.push_back(r);
       }
     }
-    fw32.assign((size_t)ntile * 32, make_int4(0, 0, 0, 0));
+    fw32.assign((size_t)ntile * RGPU_TILE, make_int4(0, 0, 0, 0));
     tiles.resize(ntile);
     for (int o = 0; o < ntile; o++) {
       const int t = order[o];
-      const int n = std::min(32, d->nfw - 32 * t);
-      const double4 r0 = fw64[sp[32 * t]];
+      const int n = std::min(RGPU_TILE, d->nfw - RGPU_TILE * t);
+      const double4 r0 = fw64[sp[RGPU_TILE * t]];
       double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
       for (int j = 0; j < n; j++) {
-        const int idx = sp[32 * t + j];
+        const int idx = sp[RGPU_TILE * t + j];
         const double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
         const double p0[3] = {r0.x, r0.y, r0.z};
         int v[3];
@@ -338,7 +338,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
         float qf = (float)fw64[idx].w;
         int qb;
         memcpy(&qb, &qf, 4);
-        fw32[(size_t)32 * o + j] = make_int4(v[0], v[1], v[2], qb);
+        fw32[(size_t)RGPU_TILE * o + j] = make_int4(v[0], v[1], v[2], qb);
       }
       TileRec tr;
       double cen[3];
@@ -446,7 +446,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   if (cudaMalloc((void **)&(p), (n)) != cudaSuccess) { sys_free(s); return fail(RGPU_E_CUDA, "cudaMalloc " #p); }
   ALLOC(s->d_sys, sizeof(RgpuSys));
   ALLOC(s->fw64, sizeof(double4) * d->nfw);
-  ALLOC(s->fw32, sizeof(int4) * 32 * (size_t)h.ntile);
+  ALLOC(s->fw32, sizeof(int4) * RGPU_TILE * (size_t)h.ntile);
   ALLOC(s->tiles_d, sizeof(TileRec) * (size_t)h.ntile);
   ALLOC(s->kvec, sizeof(char4) * nk1);
   ALLOC(s->kfactor, sizeof(double) * nk1);
@@ -489,7 +489,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   int rc = RGPU_SUCCESS;
   do {
     if (cudaMemcpyAsync(s->fw64, fw64.data(), sizeof(double4) * d->nfw, cudaMemcpyHostToDevice, st) ||
-        cudaMemcpyAsync(s->fw32, fw32.data(), sizeof(int4) * 32 * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(s->fw32, fw32.data(), sizeof(int4) * RGPU_TILE * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(s->tiles_d, tiles.data(), sizeof(TileRec) * (size_t)h.ntile, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(s->state, &s->h_state, sizeof(RgpuState), cudaMemcpyHostToDevice, st) ||
         cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * nk1, st) ||
@@ -996,7 +996,7 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e->mixed) {
     e->tile_items = maxtile;
-    e->fw_items = maxtile * 32;
+    e->fw_items = maxtile * RGPU_TILE;
   } else {
     e->tile_items = 0;
     e->fw_items = maxfw;

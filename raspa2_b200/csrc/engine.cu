@@ -33,7 +33,7 @@ namespace cg = cooperative_groups;
 
 /* ------------------------------------------------------------------------ */
 /* shared-memory plan of the engine (offsets in bytes from the dynamic base).
- * fw_items: framework records of this CTA's share (atoms; tiles*32 on the
+ * fw_items: framework records of this CTA's share (atoms; tiles*RGPU_TILE on the
  * mixed path), tiles: tile records of the share (mixed only), k_items: wave
  * vectors of the share staged with their S(k) (0: read from global memory). */
 struct EngineLayout {
@@ -710,9 +710,9 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
       if (S.smem_fw) {
         int4 *dfw = (int4 *)(smem + L.fw);
         TileRec *dt = (TileRec *)(smem + L.tiles);
-        for (int i = threadIdx.x; i < (t1 - t0) * 32; i += blockDim.x) dfw[i] = S.fw32[t0 * 32 + i];
+        for (int i = threadIdx.x; i < (t1 - t0) * RGPU_TILE; i += blockDim.x) dfw[i] = S.fw32[t0 * RGPU_TILE + i];
         for (int i = threadIdx.x; i < t1 - t0; i += blockDim.x) dt[i] = S.tiles[t0 + i];
-        E.sl.fw = dfw - (size_t)t0 * 32;
+        E.sl.fw = dfw - (size_t)t0 * RGPU_TILE;
         E.sl.tiles = dt - t0;
       } else {
         E.sl.fw = S.fw32;

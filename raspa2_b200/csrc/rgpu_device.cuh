@@ -191,10 +191,11 @@ __device__ inline void block_sum2(double &a, double &b, double *red)
  * (position, slice chunk) units spread over the warps; a unit's lane sums are
  * warp-reduced and the per-position sums formed in FP64.
  *
- * Mixed path: the framework is stored as spatially sorted tiles of 32 atoms
- * with a bounding box each. Lanes first test 32 tile boxes against the cut-off
- * sphere at once (a lower bound of the minimum-image distance), then visit
- * only the surviving tiles; pairs inside the cut-off are appended to a
+ * Mixed path: the framework is stored as compact tiles of RGPU_TILE = 16
+ * atoms with a bounding box each. Lanes first test 32 tile boxes against the
+ * cut-off sphere at once (a lower bound of the minimum-image distance), then
+ * visit the surviving tiles two at a time (half a warp each); pairs inside
+ * the cut-off are appended to a
  * per-warp queue and evaluated 32 at a time, so the LJ + erfc arithmetic runs
  * with all lanes busy instead of under a divergent branch.
  */
@@ -219,7 +220,7 @@ struct EvalPlan {
 __device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwarps, int max_units, int minitems)
 {
   EvalPlan pl;
-  int target = 3 * nwarps;
+  int target = nwarps;
   int cf = (target + P - 1) / P;
   int maxcf = (nfw + minitems - 1) / minitems;
   if (cf > maxcf) cf = maxcf;
@@ -318,6 +319,8 @@ __device__ __forceinline__ void queue_drain(PairQueue &Q, float &av, float &ac, 
   __syncwarp();
 }
 
+static_assert(RGPU_TILE == 16, "unit_tiles_mixed visits two tiles per warp pass, one per half warp");
+
 /* framework tiles [t0, t1) for bead b, FP32 path (warp-wide) */
 __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *fw, const TileRec *tiles, int t0, int t1,
                                                  const BeadPos &b, bool check, float &av, float &ac, int &ov,
@@ -347,7 +350,9 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
       vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
     }
     unsigned m = __ballot_sync(RGPU_FULL, vis);
-    /* two visible tiles per pass: their loads and distances are independent */
+    /* two visible tiles per pass of the warp: lanes 0-15 take the atoms of
+     * the first, lanes 16-31 those of the second */
+    const int half = lane >> 4, hl = lane & 15;
     while (m) {
       const int i1 = __ffs(m) - 1;
       m &= m - 1;
@@ -357,16 +362,14 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
       const int n2s = __shfl_sync(RGPU_FULL, tn, i2 >= 0 ? i2 : 0);
       const int n2 = i2 >= 0 ? n2s : 0;
       nvis += n1 + n2;
-      int4 f1 = make_int4(0, 0, 0, 0), f2 = make_int4(0, 0, 0, 0);
-      if (lane < n1) f1 = fw[(tb + i1) * 32 + lane];
-      if (lane < n2) f2 = fw[(tb + i2) * 32 + lane];
-      const float dx1 = __int2float_rn(f1.x - b.xi) * sx, dx2 = __int2float_rn(f2.x - b.xi) * sx;
-      const float dy1 = __int2float_rn(f1.y - b.yi) * sy, dy2 = __int2float_rn(f2.y - b.yi) * sy;
-      const float dz1 = __int2float_rn(f1.z - b.zi) * sz, dz2 = __int2float_rn(f2.z - b.zi) * sz;
-      const float r21 = fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1));
-      const float r22 = fmaf(dx2, dx2, fmaf(dy2, dy2, dz2 * dz2));
-      queue_add(Q, lane < n1 && r21 < rc2, r21, __int_as_float(f1.w), f1.z & 3, av, ac, ov, nin, nch);
-      if (i2 >= 0) queue_add(Q, lane < n2 && r22 < rc2, r22, __int_as_float(f2.w), f2.z & 3, av, ac, ov, nin, nch);
+      const int mine = half ? i2 : i1, nmine = half ? n2 : n1;
+      int4 f = make_int4(0, 0, 0, 0);
+      if (hl < nmine) f = fw[(tb + mine) * RGPU_TILE + hl];
+      const float dx = __int2float_rn(f.x - b.xi) * sx;
+      const float dy = __int2float_rn(f.y - b.yi) * sy;
+      const float dz = __int2float_rn(f.z - b.zi) * sz;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      queue_add(Q, hl < nmine && r2 < rc2, r2, __int_as_float(f.w), f.z & 3, av, ac, ov, nin, nch);
     }
   }
   queue_drain(Q, av, ac, ov, nin, nch);

@@ -23,6 +23,7 @@
 #define RGPU_MAX_FWTYPES 4     /* framework pseudo-atom types */
 #define RGPU_MAX_TRIALS 16     /* CBMC trial positions per step */
 #define RGPU_MAX_POS 64        /* bead positions evaluated in one batch */
+#define RGPU_TILE 16           /* framework atoms per tile (mixed-precision layout) */
 
 /* per-system counters */
 enum {
@@ -88,7 +89,7 @@ typedef struct {
   float eps4, sig2, shift, pad;
 } RgpuLJf;
 
-/* Tile of the mixed-precision framework layout: 32 spatially close atoms.
+/* Tile of the mixed-precision framework layout: RGPU_TILE spatially close atoms.
  * c = centre in fixed point with the atom count in .w; h = half extents (A)
  * such that every atom of the tile lies within +-h of c (minimum image). */
 typedef struct {
@@ -137,7 +138,7 @@ typedef struct RgpuSys {
   int smem_fw;                /* framework staged in shared memory by the engine */
   /* device pointers */
   const double4 *fw64;        /* [nfw] x, y, z, q (sorted by type) */
-  const int4 *fw32;           /* [ntile*32] tiled: fixed-point x, y, z (low 2 bits of z = segment), float bits of q */
+  const int4 *fw32;           /* [ntile*RGPU_TILE] tiled: fixed-point x, y, z (low 2 bits of z = segment), float bits of q */
   const TileRec *tiles;       /* [ntile] */
   int ntile;
   int pad_tile;
