@@ -40,7 +40,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from raspa2_b200 import raspa_io, systems, units  # noqa: E402
+from raspa2_b200 import ranks, raspa_io, systems, units  # noqa: E402
 
 METRIC = "MC moves/sec, batched mixed-prec vs plain GPU at 1e-6 rel err; p50/p99 job ms"
 REF_SIMULATE = os.path.join(ROOT, "oracle", "_ref", "simulate")
@@ -224,7 +224,7 @@ class ClockSampler:
 
 
 def make_systems(n, rank):
-    return systems.batched_co2_systems(n, seed=2 + 7919 * rank)
+    return systems.batched_co2_systems(n, seed=ranks.batch_seed(2, rank))
 
 
 def run_ours(args):
@@ -232,9 +232,7 @@ def run_ours(args):
     import torch.distributed as dist
     from raspa2_b200 import native
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = ranks.rank_env()
     if world > 1:
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", init_method="env://",
@@ -292,14 +290,7 @@ def run_ours(args):
     d = (c1 - c0).sum(axis=0)
     moves = float(d[8])
     status = [g.state()["status"] for g in gs]
-    if world > 1:
-        t = torch.tensor([t_dev, moves], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-        t_dev_max, moves_all = float(tmax[0]), float(t[1])
-    else:
-        t_dev_max, moves_all = t_dev, moves
+    t_dev_max, moves_all = ranks.reduce_time_and_count(t_dev, moves, dev)
     value = moves_all / t_dev_max
 
     # roofline of the engine kernel (one launch per step)
@@ -333,7 +324,8 @@ def run_ours(args):
                 moves_e += st["counters"][8]
             moves_e -= before
         t_e = time.perf_counter() - t0
-        e2e = {"value": moves_e / t_e * (world if world > 1 else 1), "unit": "MC moves/s",
+        t_e, moves_e = ranks.reduce_time_and_count(t_e, moves_e, dev)
+        e2e = {"value": moves_e / t_e, "unit": "MC moves/s",
                "h2d_bytes_per_step": int(h2d / args.e2e_steps), "d2h_bytes_per_step": int(d2h / args.e2e_steps),
                "path": "rgpu_set_adsorbates + rgpu_engine_run + rgpu_system_state/rgpu_get_adsorbates per step"}
 
