@@ -67,7 +67,8 @@ typedef struct {
   int kmax[3];                /* wave vectors per axis */
   int maxmol;                 /* molecule capacity */
   /* MC move parameters (used by the engine) */
-  double move_cum[4];         /* cumulative probabilities: translate, rotate, insert, delete */
+  double move_cum[6];         /* cumulative probabilities: translate, rotate, insert, delete,
+                                 reinsert, Widom test insertion */
   double max_translation;     /* Angstrom */
   double max_rotation;        /* radian */
   double fugacity_beta_v;     /* beta * fugacity * volume (ideal-gas Rosenbluth weight 1) */

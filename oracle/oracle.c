@@ -508,6 +508,7 @@ enum {
   SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
   SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16,       /* 16 + 3*i + {z,y,x} */
   SLOT_ORIENT_SELECT = 5, SLOT_ORIENT = 64,      /* 64 + 4*i + {X0,Y1,Y2} */
+  SLOT_ORIENT_OLD = 128,                          /* retrace of a reinsertion: 128 + 4*i */
   SLOT_SPHERE = 192                               /* discarded sphere vectors */
 };
 #define MAX_TRIALS 16
@@ -579,13 +580,19 @@ static int trial_energies(const or_sys *s, const double *xyz, int exclude, doubl
 }
 
 /* shared body of GrowMolecule (src/cbmc.c:3056-3181) and RetraceMolecule
- * (:2928-3054) for one rigid group grown from the starting bead */
-static void cbmc_common(const or_sys *s, int retrace, int m, int nf, int nt, or_rng_fn rng,
-                        void *ctx, double *out, double *new_xyz)
+ * (:2928-3054) for one rigid group grown from the starting bead.
+ * reins: the growth and the retrace of a reinsertion (src/mc_moves.c:4415):
+ * molecule m stays excluded while the new configuration is grown; the
+ * growth leaves r = w_1(n) - exp(-beta u_1(selected)) in *stored_r, and the
+ * retrace evaluates the old first bead alone with w_1(o) = exp(-beta u_1(o))
+ * + r (CBMC_RETRACE_REINSERTION, src/cbmc.c:640-641, :750-762). */
+static void cbmc_common(const or_sys *s, int retrace, int reins, int m, int nf, int nt, or_rng_fn rng,
+                        void *ctx, double *out, double *new_xyz, double *stored_r)
 {
   const int sb = s->start_bead, type0 = s->mol_type[sb];
   const double q0 = s->mol_q[sb];
-  const int exclude = retrace ? m : s->nmol;
+  const int exclude = (retrace || reins) ? m : s->nmol;
+  const int nfirst = (retrace && reins) ? 1 : nf;   /* positions evaluated for the first bead */
   const double *old = retrace ? s->ads_xyz + 3 * m * s->natom : NULL;
   double bf[MAX_TRIALS], e1[MAX_TRIALS][4], pos1[MAX_TRIALS][3];
   int ov[MAX_TRIALS];
@@ -593,7 +600,7 @@ static void cbmc_common(const or_sys *s, int retrace, int m, int nf, int nt, or_
   out[0] = 1.0;
   for (int k = 1; k < 6; k++) out[k] = 0.0;
   /* HandleFirstBead, src/cbmc.c:623-795 */
-  for (int i = 0; i < nf; i++) {
+  for (int i = 0; i < nfirst; i++) {
     if (retrace && i == 0) {
       pos1[0][0] = old[3 * sb]; pos1[0][1] = old[3 * sb + 1]; pos1[0][2] = old[3 * sb + 2];
     } else {
@@ -616,10 +623,12 @@ static void cbmc_common(const or_sys *s, int retrace, int m, int nf, int nt, or_
   }
   if (!any) return;
   double w1 = 0.0;
-  for (int i = 0; i < nf; i++)
+  for (int i = 0; i < nfirst; i++)
     if (!ov[i]) w1 += exp(bf[i]);
   int sel = 0;
   if (!retrace) sel = select_trial(bf, ov, nf, rng(ctx, SLOT_FIRST_SELECT));
+  if (reins && !retrace) *stored_r = w1 - exp(bf[sel]);
+  if (reins && retrace) w1 += *stored_r;
   double rosen = w1 / (double)nf;
   if (!retrace && rosen < 1e-150) return;   /* MinimumRosenbluthFactor */
   double u[4] = {e1[sel][0], e1[sel][1], e1[sel][2], e1[sel][3]};
@@ -637,9 +646,10 @@ static void cbmc_common(const or_sys *s, int retrace, int m, int nf, int nt, or_
         for (int a = 0; a < 3 * s->natom; a++) tx[0][a] = old[a];
       } else {
         discard_sphere(rng, ctx, iu);
-        double x0 = rng(ctx, SLOT_ORIENT + 4 * iu + 0);
-        double y1 = rng(ctx, SLOT_ORIENT + 4 * iu + 1);
-        double y2 = rng(ctx, SLOT_ORIENT + 4 * iu + 2);
+        const int ob = (retrace && reins) ? SLOT_ORIENT_OLD : SLOT_ORIENT;
+        double x0 = rng(ctx, ob + 4 * iu + 0);
+        double y1 = rng(ctx, ob + 4 * iu + 1);
+        double y2 = rng(ctx, ob + 4 * iu + 2);
         double R[3][3];
         random_rotation(x0, y1, y2, R);
         for (int a = 0; a < s->natom; a++) {
@@ -683,13 +693,13 @@ static void cbmc_common(const or_sys *s, int retrace, int m, int nf, int nt, or_
 void or_cbmc_grow(const or_sys *s, int nf, int nt, or_rng_fn rng, void *ctx, double *out,
                   double *new_xyz)
 {
-  cbmc_common(s, 0, s->nmol, nf, nt, rng, ctx, out, new_xyz);
+  cbmc_common(s, 0, 0, s->nmol, nf, nt, rng, ctx, out, new_xyz, NULL);
 }
 
 void or_cbmc_retrace(const or_sys *s, int m, int nf, int nt, or_rng_fn rng, void *ctx,
                      double *out)
 {
-  cbmc_common(s, 1, m, nf, nt, rng, ctx, out, NULL);
+  cbmc_common(s, 1, 0, m, nf, nt, rng, ctx, out, NULL, NULL);
 }
 
 /* ---------------------------------------------------------------------- */
@@ -847,7 +857,7 @@ void or_mc_run(or_sys *s, const or_mc_params *p, or_mc_state *st, uint64_t step0
     philox_ctx ctx = {p->seed, p->system, step0 + (uint64_t)it};
     double u0 = rng_philox(&ctx, SLOT_MOVE);
     int mv = 0;
-    while (mv < 3 && u0 >= p->cum[mv]) mv++;
+    while (mv < 5 && u0 >= p->cum[mv]) mv++;
     if (mv == 0 || mv == 1) {
       if (s->nmol == 0 || (mv == 1 && na == 1)) continue;
       st->moves++;
@@ -905,6 +915,46 @@ void or_mc_run(or_sys *s, const or_mc_params *p, or_mc_state *st, uint64_t step0
         st->u[0] += o[2]; st->u[1] += o[3]; st->u[2] += o[4]; st->u[3] += o[5];
         st->u[4] += de[1]; st->u[5] += de[0];
       }
+    } else if (mv == 4) {
+      /* ReinsertionAdsorbateMove, src/mc_moves.c:4415-4600 */
+      if (s->nmol == 0) continue;
+      st->moves++;
+      st->attempts[4]++;
+      int m = (int)(rng_philox(&ctx, SLOT_MOLECULE) * s->nmol);
+      if (m >= s->nmol) m = s->nmol - 1;
+      double on[6], oo[6], nx[MAX_ATOMS * 3], r = 0.0, de[3] = {0.0, 0.0, 0.0};
+      cbmc_common(s, 0, 1, m, p->ntrial_first, p->ntrial, rng_philox, &ctx, on, nx, &r);
+      if (on[0] != 0.0) continue;
+      cbmc_common(s, 1, 1, m, p->ntrial_first, p->ntrial, rng_philox, &ctx, oo, NULL, &r);
+      if (oo[0] != 0.0) continue;
+      const double *ox = s->ads_xyz + 3 * m * na;
+      double pre = 1.0;
+      if (s->ewald) {
+        or_ewald_delta(s, 1, ox, 1, nx, de, nk);
+        pre = exp(-s->beta * (de[0] + de[1]));
+      }
+      if (rng_philox(&ctx, SLOT_ACCEPT) < pre * on[1] / oo[1]) {
+        st->accepted[4]++;
+        for (int a = 0; a < 3 * na; a++) s->ads_xyz[3 * m * na + a] = nx[a];
+        if (s->ewald) memcpy(s->sk_ads, nk, sizeof(double) * 2 * s->nk);
+        for (int k = 0; k < 4; k++) st->u[k] += on[2 + k] - oo[2 + k];
+        st->u[4] += de[1]; st->u[5] += de[0];
+      }
+    } else if (mv == 5) {
+      /* WidomAdsorbateMove, src/mc_moves.c:7844-8030: Rosenbluth weight of a
+       * test insertion, no change of state */
+      st->moves++;
+      st->attempts[5]++;
+      st->widom_n += 1.0;
+      double o[6], nx[MAX_ATOMS * 3], de[3] = {0.0, 0.0, 0.0};
+      or_cbmc_grow(s, p->ntrial_first, p->ntrial, rng_philox, &ctx, o, nx);
+      if (o[0] != 0.0) continue;
+      double w = o[1];
+      if (s->ewald) {
+        or_ewald_delta(s, 0, NULL, 1, nx, de, nk);
+        w *= exp(-s->beta * (de[0] + de[1]));
+      }
+      st->widom_sum += w;
     } else {
       st->moves++;
       st->attempts[3]++;

@@ -114,7 +114,8 @@ double or_grid_interpolate(const float *grid, const int npts[3], const double si
 /* Complete GCMC engine driven by the counter-based stream that the GPU engine
  * uses. See or_mc_params. */
 typedef struct {
-  double cum[4];           /* cumulative move probabilities: translate, rotate, insert, delete */
+  double cum[6];           /* cumulative move probabilities: translate, rotate, insert, delete,
+                              reinsert, Widom */
   double max_translation;  /* A */
   double max_rotation;     /* rad */
   double fugacity_beta_v;  /* beta * f * V (ideal-gas Rosenbluth weight 1) */
@@ -125,8 +126,9 @@ typedef struct {
 
 typedef struct {
   double u[6];             /* running totals as or_total_energy */
-  long long attempts[4], accepted[4];
+  long long attempts[6], accepted[6];   /* by move type as in cum */
   long long moves;         /* counted MC moves (see or_mc_run) */
+  double widom_sum, widom_n;            /* Widom Rosenbluth weights and samples */
 } or_mc_state;
 
 /* Runs `nsteps` MC steps starting at step index `step0`. */

@@ -33,15 +33,16 @@ class OrSys(C.Structure):
 
 
 class MCParams(C.Structure):
-    _fields_ = [("cum", C.c_double * 4), ("max_translation", C.c_double),
+    _fields_ = [("cum", C.c_double * 6), ("max_translation", C.c_double),
                 ("max_rotation", C.c_double), ("fugacity_beta_v", C.c_double),
                 ("ntrial_first", C.c_int), ("ntrial", C.c_int),
                 ("seed", C.c_uint64), ("system", C.c_uint32)]
 
 
 class MCState(C.Structure):
-    _fields_ = [("u", C.c_double * 6), ("attempts", C.c_longlong * 4),
-                ("accepted", C.c_longlong * 4), ("moves", C.c_longlong)]
+    _fields_ = [("u", C.c_double * 6), ("attempts", C.c_longlong * 6),
+                ("accepted", C.c_longlong * 6), ("moves", C.c_longlong),
+                ("widom_sum", C.c_double), ("widom_n", C.c_double)]
 
 
 _RNG_FN = C.CFUNCTYPE(C.c_double, C.c_void_p, C.c_int)

@@ -420,7 +420,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
         h.excl_mol += d->coulomb * d->mol_q[a] * d->mol_q[b] * erf(d->alpha * r) / r;
       }
   h.ewald = d->ewald;
-  for (int c = 0; c < 4; c++) h.cum[c] = d->move_cum[c];
+  for (int c = 0; c < 6; c++) h.cum[c] = d->move_cum[c];
   h.max_translation = d->max_translation;
   h.max_rotation = d->max_rotation;
   h.fugacity_beta_v = d->fugacity_beta_v;
@@ -1056,7 +1056,7 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   const int n = (int)e->sys.size();
-  CK(rgpu_engine_prepare(e->mixed, e->smem));
+  CK(rgpu_engine_prepare(e->mixed, e->threads, e->smem));
   if (!e->use_graph) {
     CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
                           e->k_items, e->cluster, e->threads, st));

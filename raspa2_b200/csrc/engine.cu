@@ -29,7 +29,7 @@ namespace cg = cooperative_groups;
 
 #define RGPU_MAX_UNITS 512
 #define RGPU_MAX_WARPS 32
-#define RGPU_RND 128          /* random slots drawn per MC step */
+#define RGPU_RND 192          /* random slots drawn per MC step */
 
 /* ------------------------------------------------------------------------ */
 /* shared-memory plan of the engine (offsets in bytes from the dynamic base).
@@ -88,10 +88,12 @@ size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_at
 struct Ctl {
   double rnd[2][RGPU_RND];    /* uniforms by slot, double-buffered by step parity */
   double energy[RGPU_NE];     /* running energies (written back by rank 0) */
-  long long cnt[RGPU_CNT_PAIRS];  /* move counters (rank 0's written back) */
+  long long cnt[RGPU_NCNT];   /* move counters [0, RGPU_CNT_PAIRS) and reinsertion counters (rank 0's written back) */
   BeadPos first;              /* chosen first bead */
   double u[4];                /* energies of the chosen configuration */
+  double uo[4];               /* energies of the retraced old configuration (reinsertion) */
   double rosen;
+  double rosen_old;
   double dl[4];
   int nmol;
   int fail;
@@ -207,7 +209,7 @@ __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 /* Pair evaluation of P positions on this CTA's share, then one cluster
  * barrier; the totals are read with gather(). All threads call. */
 template <bool MIXED>
-__device__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
+__device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
@@ -253,7 +255,7 @@ __device__ __forceinline__ void gather(const Eng<MIXED> &E, int b, int p, double
 /* Ewald sum over this CTA's wave vectors for the sites in E.sites[0..ns),
  * warp partials left in E.red[b]; one cluster barrier. All threads call. */
 template <bool MIXED>
-__device__ void engine_ewald(Eng<MIXED> &E, int ns)
+__device__ __forceinline__ void engine_ewald(Eng<MIXED> &E, int ns)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
@@ -307,8 +309,8 @@ __device__ __forceinline__ void gather_ewald(const Eng<MIXED> &E, int b, double 
  * SelectTrialPosition (src/cbmc.c:563-599). Lane 0 leaves the weight sum
  * (w_sum = sum exp(bf)), the selected trial and its energies in Ctl. */
 template <bool MIXED>
-__device__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool first, bool select, double usel,
-                            double &w_sum, int &sel, double *usum, int &any)
+__device__ __forceinline__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool first, bool select, double usel,
+                            double &w_sum, int &sel, double *usum, int &any, int off = 0, double *w_sel = nullptr)
 {
   const int lane = threadIdx.x & 31;
   const RgpuSys &S = *E.S;
@@ -319,7 +321,7 @@ __device__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool firs
     for (int j = 0; j < nb; j++) {
       double r[4];
       int o;
-      gather(E, b, lane * nb + j, r, o);
+      gather(E, b, off + lane * nb + j, r, o);
       if (first) ov |= (r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap);
       else ov |= (r[0] >= S.overlap);
       for (int k = 0; k < 4; k++) e[k] += r[k];
@@ -352,13 +354,15 @@ __device__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool firs
   w_sum = wsum;
   sel = s;
   for (int k = 0; k < 4; k++) usum[k] = __shfl_sync(RGPU_FULL, e[k], s);
+  const double ws_sel = __shfl_sync(RGPU_FULL, w, s);
+  if (w_sel) *w_sel = ws_sel;
 }
 
 /* ------------------------------------------------------------------------ */
 /* translation (mv=0) and rotation (mv=1):
  * TranslationMoveAdsorbate src/mc_moves.c:1529-1762, RotationMoveAdsorbate :2636 */
 template <bool MIXED>
-__device__ void step_displace(Eng<MIXED> &E, int mv)
+__device__ __forceinline__ void step_displace(Eng<MIXED> &E, int mv)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -459,17 +463,20 @@ __device__ void step_displace(Eng<MIXED> &E, int mv)
 }
 
 /* ------------------------------------------------------------------------ */
-/* CBMC insertion / deletion of a rigid molecule grown from the starting bead:
+/* CBMC insertion / deletion of a rigid molecule grown from the starting bead
+ * (widom: a test insertion that only samples its Rosenbluth weight,
+ * WidomAdsorbateMove src/mc_moves.c:7844-8030):
  * GrowMolecule src/cbmc.c:3056-3181 and RetraceMolecule :2928-3054 with
  * HandleFirstBead :623-795, Rosen/RosenOld :2762-2926, the rigid-group branch
  * of GenerateTrialOrientationsSimpleSphere :1480-1578 and
  * ComputeExternalEnergies :1154-1478, LJ biasing; acceptance of
  * SwapAddAdsorbateMove src/mc_moves.c:7016 and SwapRemoveAdsorbateMove :7228. */
 template <bool MIXED>
-__device__ void step_swap(Eng<MIXED> &E, bool insert)
+__device__ __forceinline__ void step_swap(Eng<MIXED> &E, bool insert, bool widom = false)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
+  if (widom && threadIdx.x == 0) C.sums[RGPU_SUM_WIDOM_N] += 1.0;   /* overlap samples count with weight 0 */
   const int na = S.natom, sb = S.start_bead, nmol = C.nmol;
   const int nf = S.ntrial_first, nt = S.ntrial;
   int m = nmol;
@@ -600,7 +607,8 @@ __device__ void step_swap(Eng<MIXED> &E, bool insert)
     if (insert) pacc = rosen * exp(-S.beta * (d_ads + d_host)) * S.fugacity_beta_v / (1.0 + nmol);
     else pacc = (double)nmol / (rosen * exp(S.beta * (d_ads + d_host)) * S.fugacity_beta_v);
     if (!(pacc == pacc)) C.status |= RGPU_ERR_NONFINITE;
-    C.accept = E.rnd[SLOT_ACCEPT] < pacc;
+    C.accept = !widom && E.rnd[SLOT_ACCEPT] < pacc;
+    if (widom) C.sums[RGPU_SUM_WIDOM_W] += rosen * exp(-S.beta * (d_ads + d_host));
     const int mv = insert ? 2 : 3;
     if (C.accept) {
       C.cnt[RGPU_CNT_ACCEPT + mv]++;
@@ -640,6 +648,198 @@ __device__ void step_swap(Eng<MIXED> &E, bool insert)
 }
 
 /* ------------------------------------------------------------------------ */
+/* CBMC reinsertion of molecule m, ReinsertionAdsorbateMove src/mc_moves.c:4415-4600:
+ * a new configuration is grown with m excluded (GrowMolecule, CBMC_INSERTION)
+ * and the old one retraced (RetraceMolecule, CBMC_RETRACE_REINSERTION): the
+ * old first bead alone, its weight completed with the new growth's other
+ * first-bead trials (src/cbmc.c:750-762), and the old orientation among
+ * nt - 1 fresh ones. Accepted with probability
+ * exp(-beta dU_Fourier) W(new) / W(old).
+ * Evaluation 1 holds the nf new first-bead trials, the old first bead and
+ * the retrace orientations (all known up front); evaluation 2 the new
+ * orientations around the chosen first bead. */
+template <bool MIXED>
+__device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, sb = S.start_bead, nmol = C.nmol;
+  const int nf = S.ntrial_first, nt = S.ntrial, nb = na - 1;
+  int m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
+  if (m >= nmol) m = nmol - 1;
+  const int old_first = nf;              /* position of the old first bead */
+  const int old_orient = nf + 1;         /* first position of the retrace orientations */
+  if (threadIdx.x < nf) {
+    const int i = threadIdx.x;
+    bead_set(E.pos[i], S, S.box[0] * E.rnd[SLOT_FIRST + 3 * i + 2], S.box[1] * E.rnd[SLOT_FIRST + 3 * i + 1],
+             S.box[2] * E.rnd[SLOT_FIRST + 3 * i + 0], sb, m);
+  } else if (threadIdx.x == nf) {
+    double p[3];
+    atom_xyz(E, m, sb, p);
+    bead_set(E.pos[old_first], S, p[0], p[1], p[2], sb, m);
+  }
+  if (na > 1 && threadIdx.x >= 32 && threadIdx.x < 32 + nt) {
+    const int t = threadIdx.x - 32;
+    double o[3];
+    atom_xyz(E, m, sb, o);
+    double R[3][3];
+    if (t > 0)
+      random_rotation(E.rnd[SLOT_ORIENT_OLD + 4 * t + 0], E.rnd[SLOT_ORIENT_OLD + 4 * t + 1],
+                      E.rnd[SLOT_ORIENT_OLD + 4 * t + 2], R);
+    int j = 0;
+    for (int a = 0; a < na; a++) {
+      if (a == sb) continue;
+      double p[3];
+      if (t == 0) {
+        atom_xyz(E, m, a, p);
+      } else {
+        const double c[3] = {S.mol_ref[a][0] - S.mol_ref[sb][0], S.mol_ref[a][1] - S.mol_ref[sb][1],
+                             S.mol_ref[a][2] - S.mol_ref[sb][2]};
+        for (int d = 0; d < 3; d++) p[d] = o[d] + c[0] * R[d][0] + c[1] * R[d][1] + c[2] * R[d][2];
+      }
+      bead_set(E.pos[old_orient + t * nb + j], S, p[0], p[1], p[2], a, m);
+      j++;
+    }
+  }
+  __syncthreads();
+  engine_eval<MIXED>(E, nf + 1 + (na > 1 ? nt * nb : 0), 0);
+  const int b1 = E.xb;
+  E.xb ^= 1;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double wsum, u[4], wsel;
+    int sel, any;
+    cbmc_trials(E, b1, nf, 1, true, true, E.rnd[SLOT_FIRST_SELECT], wsum, sel, u, any, 0, &wsel);
+    /* the old first bead */
+    double r[4];
+    int o;
+    gather(E, b1, old_first, r, o);
+    const bool ovo = r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap;
+    const double w_old1 = ovo ? 0.0 : exp(-S.beta * (r[0] + r[2]));
+    /* the retrace orientations (trial 0 = the old one) */
+    double wo = 0.0, uo[4] = {r[0], r[1], r[2], r[3]};
+    int anyo = 1;
+    if (na > 1) {
+      double uot[4];
+      int selo;
+      cbmc_trials(E, b1, nt, nb, false, false, 0.0, wo, selo, uot, anyo, old_orient);
+      for (int k = 0; k < 4; k++) uo[k] += uot[k];
+    }
+    if (lane == 0) {
+      C.rosen = wsum / (double)nf;
+      double rosen_old = (w_old1 + (wsum - wsel)) / (double)nf;
+      if (na > 1) rosen_old *= wo / (double)nt;
+      C.fail = !any || C.rosen < 1e-150 || ovo || !anyo;
+      C.rosen_old = rosen_old;
+      C.sel = sel;
+      for (int k = 0; k < 4; k++) {
+        C.u[k] = u[k];
+        C.uo[k] = uo[k];
+      }
+      C.first = E.pos[sel];
+      if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
+    }
+  }
+  __syncthreads();
+  if (C.fail) return;
+  if (na > 1) {
+    const BeadPos first = C.first;
+    if (threadIdx.x < nt) {
+      const int t = threadIdx.x;
+      double R[3][3];
+      random_rotation(E.rnd[SLOT_ORIENT + 4 * t + 0], E.rnd[SLOT_ORIENT + 4 * t + 1],
+                      E.rnd[SLOT_ORIENT + 4 * t + 2], R);
+      int j = 0;
+      for (int a = 0; a < na; a++) {
+        if (a == sb) continue;
+        const double c[3] = {S.mol_ref[a][0] - S.mol_ref[sb][0], S.mol_ref[a][1] - S.mol_ref[sb][1],
+                             S.mol_ref[a][2] - S.mol_ref[sb][2]};
+        double p[3];
+        p[0] = first.x + c[0] * R[0][0] + c[1] * R[0][1] + c[2] * R[0][2];
+        p[1] = first.y + c[0] * R[1][0] + c[1] * R[1][1] + c[2] * R[1][2];
+        p[2] = first.z + c[0] * R[2][0] + c[1] * R[2][1] + c[2] * R[2][2];
+        bead_set(E.pos[t * nb + j], S, p[0], p[1], p[2], a, m);
+        j++;
+      }
+    }
+    __syncthreads();
+    engine_eval<MIXED>(E, nt * nb, 0);
+    const int b2 = E.xb;
+    E.xb ^= 1;
+    if (threadIdx.x < 32) {
+      double wsum, u[4];
+      int sel, any;
+      cbmc_trials(E, b2, nt, nb, false, true, E.rnd[SLOT_ORIENT_SELECT], wsum, sel, u, any);
+      if (threadIdx.x == 0) {
+        if (!any) C.fail = 1;
+        else {
+          C.rosen *= wsum / (double)nt;
+          if (C.rosen < 1e-150) C.fail = 1;
+          for (int k = 0; k < 4; k++) C.u[k] += u[k];
+        }
+        C.sel = sel;
+        if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
+      }
+    }
+    __syncthreads();
+    if (C.fail) return;
+  }
+  /* Ewald sites: the new configuration (+q) and the old one (-q) */
+  if (threadIdx.x < na) {
+    const int a = threadIdx.x;
+    BeadPos bp;
+    if (a == sb) bp = C.first;
+    else bp = E.pos[C.sel * nb + (a < sb ? a : a - 1)];
+    E.sites[a].b = bp;
+    E.sites[a].q = S.mol_q[a];
+    double p[3];
+    atom_xyz(E, m, a, p);
+    bead_set(E.sites[na + a].b, S, p[0], p[1], p[2], a, m);
+    E.sites[na + a].q = -S.mol_q[a];
+  }
+  __syncthreads();
+  const bool ew = S.ewald && S.mol_charged;
+  int bw = 0;
+  if (ew) {
+    engine_ewald<MIXED>(E, 2 * na);
+    bw = E.xb;
+    E.xb ^= 1;
+  }
+  if (threadIdx.x == 0) {
+    /* LJ-biasing corrections of both Rosenbluth weights, src/cbmc.c:3171-3178, :3044-3051 */
+    const double rosen_new = C.rosen * exp(-S.beta * (C.u[1] + C.u[3]));
+    const double rosen_old = C.rosen_old * exp(-S.beta * (C.uo[1] + C.uo[3]));
+    double d_ads = 0.0, d_host = 0.0;
+    if (ew) {
+      double ea, eh;
+      gather_ewald(E, bw, ea, eh);
+      ewald_finish(S, ea, eh, S.excl_mol, S.excl_mol, 0, 0.0, d_ads, d_host);
+    }
+    const double pacc = exp(-S.beta * (d_ads + d_host)) * rosen_new / rosen_old;
+    if (!(pacc == pacc)) C.status |= RGPU_ERR_NONFINITE;
+    C.accept = E.rnd[SLOT_ACCEPT] < pacc;
+    if (C.accept) {
+      C.cnt[RGPU_CNT_REINS_ACCEPT]++;
+      C.energy[RGPU_E_HOST_VDW] += C.u[0] - C.uo[0];
+      C.energy[RGPU_E_HOST_REAL] += C.u[1] - C.uo[1];
+      C.energy[RGPU_E_ADS_VDW] += C.u[2] - C.uo[2];
+      C.energy[RGPU_E_ADS_REAL] += C.u[3] - C.uo[3];
+      C.energy[RGPU_E_HOST_FOURIER] += d_host;
+      C.energy[RGPU_E_ADS_FOURIER] += d_ads;
+    }
+  }
+  __syncthreads();
+  if (C.accept) {
+    if (threadIdx.x < na) {
+      double p[3] = {E.sites[threadIdx.x].b.x, E.sites[threadIdx.x].b.y, E.sites[threadIdx.x].b.z};
+      atom_store(E, m, threadIdx.x, p);
+    }
+    if (ew) ewald_apply<MIXED>(S, E.tab, E.kw, E.sites, 2 * na, E.k0, E.k1);
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Loads a descriptor copy into shared memory. */
 __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
 {
@@ -649,10 +849,13 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
   __syncthreads();
 }
 
-template <bool MIXED>
-__global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps, int kw,
-                                                          int max_ads_atoms, int fw_items, int tile_items,
-                                                          int k_items)
+/* WIDE: compiled for CTAs of up to 1024 threads (64 registers per thread);
+ * otherwise up to 512 threads with 128 registers. The launch picks the
+ * instantiation from the CTA size. */
+template <bool MIXED, bool WIDE>
+__global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps,
+                                                                       int kw, int max_ads_atoms, int fw_items,
+                                                                       int tile_items, int k_items)
 {
   extern __shared__ __align__(256) unsigned char smem[];
   cg::cluster_group cl = cg::this_cluster();
@@ -691,7 +894,7 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
     RgpuSys &S = *E.S;
     double2 *sk_global = S.sk_ads;
     if (threadIdx.x < 5) C.work[threadIdx.x] = 0ULL;
-    if (threadIdx.x < RGPU_CNT_PAIRS) C.cnt[threadIdx.x] = 0;
+    if (threadIdx.x < RGPU_NCNT) C.cnt[threadIdx.x] = 0;
     if (threadIdx.x < RGPU_NE) C.energy[threadIdx.x] = S.energy[threadIdx.x];
     if (threadIdx.x == 0) {
       C.cyc[0] = C.cyc[1] = 0;
@@ -775,12 +978,12 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
       const uint64_t step = step0 + (uint64_t)it;
       /* this step's random numbers, one Philox block per thread */
       double *rb = C.rnd[it & 1];
-      if (threadIdx.x < RGPU_RND / 2) rgpu_uniform_pair(S.seed, S.sys_id, step, threadIdx.x, &rb[2 * threadIdx.x]);
+      for (int i = threadIdx.x; i < RGPU_RND / 2; i += blockDim.x) rgpu_uniform_pair(S.seed, S.sys_id, step, i, &rb[2 * i]);
       __syncthreads();
       E.rnd = rb;
       const double u0 = rb[SLOT_MOVE];
       int mv = 0;
-      while (mv < 3 && u0 >= S.cum[mv]) mv++;
+      while (mv < 5 && u0 >= S.cum[mv]) mv++;
       const int nmol = C.nmol;
       share(C.nads, rank, csize, E.sl.ads_lo, E.sl.ads_hi);
       if (mv <= 1) {
@@ -795,9 +998,18 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
         } else {
           step_swap<MIXED>(E, true);
         }
-      } else {
+      } else if (mv == 3) {
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 3]++; }
         if (nmol != 0) step_swap<MIXED>(E, false);
+      } else if (mv == 4) {
+        /* the reference returns before counting when there is no molecule */
+        if (nmol != 0) {
+          if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_REINS_ATTEMPT]++; }
+          step_reinsert<MIXED>(E);
+        }
+      } else {
+        if (threadIdx.x == 0) C.cnt[RGPU_CNT_MOVES]++;
+        step_swap<MIXED>(E, true, true);
       }
       /* ensemble sums after the step (thread 0 owns the running values) */
       if (threadIdx.x == 0 && step >= avg0) {
@@ -832,6 +1044,8 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
         S.step[0] = step0 + (uint64_t)it;
         for (int k = 0; k < RGPU_NSUM; k++) S.sums[k] += C.sums[k];
         for (int c = 0; c < RGPU_CNT_PAIRS; c++) S.counters[c] += C.cnt[c];
+        S.counters[RGPU_CNT_REINS_ATTEMPT] += C.cnt[RGPU_CNT_REINS_ATTEMPT];
+        S.counters[RGPU_CNT_REINS_ACCEPT] += C.cnt[RGPU_CNT_REINS_ACCEPT];
         *S.status |= C.status;
         S.counters[RGPU_CNT_CYCLES] += clock64() - t_start;
         S.counters[RGPU_CNT_CYC_EVAL] += C.cyc[0];
@@ -845,10 +1059,12 @@ __global__ void __launch_bounds__(MIXED ? 1024 : 512) rgpu_engine_kernel(RgpuSys
   cl.sync();
 }
 
-cudaError_t rgpu_engine_prepare(int mixed, size_t smem)
+cudaError_t rgpu_engine_prepare(int mixed, int threads, size_t smem)
 {
-  if (mixed) return cudaFuncSetAttribute(rgpu_engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return cudaFuncSetAttribute(rgpu_engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (mixed && threads > 512) return cudaFuncSetAttribute(rgpu_engine_kernel<true, true>, a, (int)smem);
+  if (mixed) return cudaFuncSetAttribute(rgpu_engine_kernel<true, false>, a, (int)smem);
+  return cudaFuncSetAttribute(rgpu_engine_kernel<false, false>, a, (int)smem);
 }
 
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
@@ -871,12 +1087,15 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
   cudaError_t e;
   /* the dynamic shared-memory limit is raised by rgpu_engine_prepare, outside
    * any stream capture */
-  if (mixed)
-    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
-                           tile_items, k_items);
+  if (mixed && threads > 512)
+    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true, true>, d_systems, nsys, nsteps, kw, max_ads_atoms,
+                           fw_items, tile_items, k_items);
+  else if (mixed)
+    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true, false>, d_systems, nsys, nsteps, kw, max_ads_atoms,
+                           fw_items, tile_items, k_items);
   else
-    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<false>, d_systems, nsys, nsteps, kw, max_ads_atoms, fw_items,
-                           tile_items, k_items);
+    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<false, false>, d_systems, nsys, nsteps, kw, max_ads_atoms,
+                           fw_items, tile_items, k_items);
   return e;
 }
 

@@ -66,7 +66,8 @@ __device__ inline void rgpu_uniform_pair(uint64_t seed, uint32_t sys, uint64_t s
 /* random-draw slots of one MC step (the oracle uses the same numbering) */
 enum {
   SLOT_MOVE = 0, SLOT_MOLECULE = 1, SLOT_VNEW = 2, SLOT_AXIS = 3, SLOT_ACCEPT = 4,
-  SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16, SLOT_ORIENT_SELECT = 5, SLOT_ORIENT = 64
+  SLOT_FIRST_SELECT = 15, SLOT_FIRST = 16, SLOT_ORIENT_SELECT = 5, SLOT_ORIENT = 64,
+  SLOT_ORIENT_OLD = 128  /* retrace orientations of a reinsertion: 128 + 4 * trial */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -516,7 +517,7 @@ struct EvalSlice {
  * which warp evaluated a unit. No block barrier; *sc.next is left past the
  * last unit (the caller resets it after its barrier). Returns the plan. */
 template <bool MIXED>
-__device__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
+__device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
                                EvalScratch sc, int max_units)
 {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -638,7 +639,7 @@ struct PhaseT<true> { typedef float2 T; };
 
 /* table layout: tab[(site*3 + axis)*KW + (k + kmax)], KW = 2*kmaxall+1 */
 template <bool MIXED>
-__device__ void ewald_phases(const RgpuSys &S, const EwSite *sites, int ns, typename PhaseT<MIXED>::T *tab, int kw)
+__device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sites, int ns, typename PhaseT<MIXED>::T *tab, int kw)
 {
   const int km = (kw - 1) / 2;
   const int n = ns * 3 * kw;
@@ -725,7 +726,7 @@ __device__ void ewald_energy_sum(const RgpuSys &S, const typename PhaseT<MIXED>:
 /* As ewald_energy_sum, without block reduction: warp w leaves its partial
  * {e_ads, e_host} in red[2w], red[2w+1]. No block barrier. */
 template <bool MIXED>
-__device__ void ewald_energy_warps(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
+__device__ __forceinline__ void ewald_energy_warps(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
                                    const EwSite *sites, int ns, int k0, int k1, double *red)
 {
   double ea = 0.0, eh = 0.0;
@@ -749,7 +750,7 @@ __device__ void ewald_energy_warps(const RgpuSys &S, const typename PhaseT<MIXED
  * ewald_dS call as in the energy sum, so the stored sums are those the
  * accepted energy was computed with. */
 template <bool MIXED>
-__device__ void ewald_apply(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
+__device__ __forceinline__ void ewald_apply(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
                             int ns, int k0, int k1)
 {
   for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {

@@ -39,6 +39,8 @@ enum {
   RGPU_CNT_CYCLES = 15,  /* SM clock cycles the system spent in the engine */
   RGPU_CNT_CYC_EVAL = 16, /* of those, in pair-energy evaluations (rank 0) */
   RGPU_CNT_CYC_EWALD = 17, /* of those, in Ewald sums (rank 0) */
+  RGPU_CNT_REINS_ATTEMPT = 18, /* CBMC reinsertions attempted */
+  RGPU_CNT_REINS_ACCEPT = 19,  /* and accepted */
   RGPU_NCNT = 20
 };
 
@@ -64,6 +66,8 @@ enum {
   RGPU_SUM_U = 3,        /* total energy (the six running terms) */
   RGPU_SUM_UN = 4,
   RGPU_SUM_U2 = 5,
+  RGPU_SUM_WIDOM_W = 6,  /* Widom test insertions: sum of Rosenbluth weights */
+  RGPU_SUM_WIDOM_N = 7,  /* and their number */
   RGPU_NSUM = 8
 };
 
@@ -129,7 +133,7 @@ typedef struct RgpuSys {
   double excl_mol;            /* intramolecular exclusion energy of the rigid molecule (reference geometry) */
   double uion, net_fw, mol_charge;
   /* MC */
-  double cum[4];
+  double cum[6];              /* cumulative move probabilities (order of rgpu_system_desc.move_cum) */
   double max_translation, max_rotation;
   double fugacity_beta_v;     /* beta * f * V, ideal-gas Rosenbluth weight 1 */
   int ntrial_first, ntrial;

@@ -45,7 +45,7 @@ class SystemDesc(C.Structure):
         ("natom", C.c_int), ("mol_type", _ip), ("mol_q", _dp), ("mol_ref", _dp),
         ("start_bead", C.c_int), ("ewald", C.c_int), ("alpha", C.c_double),
         ("kmax", C.c_int * 3), ("maxmol", C.c_int),
-        ("move_cum", C.c_double * 4), ("max_translation", C.c_double),
+        ("move_cum", C.c_double * 6), ("max_translation", C.c_double),
         ("max_rotation", C.c_double), ("fugacity_beta_v", C.c_double),
         ("ntrial_first", C.c_int), ("ntrial", C.c_int),
         ("seed", C.c_uint64), ("stream_id", C.c_uint32),

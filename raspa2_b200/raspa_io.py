@@ -152,6 +152,10 @@ def simulation_input(sys: System, cycles: int = 0, init_cycles: int = 0,
     if mv.rotation > 0 and sys.molecule.n_atoms > 1:
         comp.append(f"            RotationProbability      {mv.rotation}")
     comp.append(f"            SwapProbability          {mv.swap_insert + mv.swap_delete}")
+    if mv.reinsertion > 0:
+        comp.append(f"            ReinsertionProbability   {mv.reinsertion}")
+    if mv.widom > 0:
+        comp.append(f"            WidomProbability         {mv.widom}")
     comp.append("            CreateNumberOfMolecules  0")
     return "\n".join(lines + comp) + "\n" + extra
 

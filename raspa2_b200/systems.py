@@ -74,14 +74,19 @@ CO2 = Molecule("CO2", ["O_co2", "C_co2", "O_co2"],
 
 @dataclasses.dataclass
 class MoveMix:
-    """Relative move probabilities (normalised when used)."""
+    """Relative move probabilities (normalised when used), in the engine's
+    order: translation, rotation, CBMC insertion, CBMC deletion, CBMC
+    reinsertion, Widom test insertion."""
     translation: float = 1.0
     rotation: float = 0.0
     swap_insert: float = 0.5   # a 'SwapProbability' p splits into p/2 insert + p/2 delete
     swap_delete: float = 0.5
+    reinsertion: float = 0.0
+    widom: float = 0.0
 
     def cumulative(self) -> np.ndarray:
-        p = np.array([self.translation, self.rotation, self.swap_insert, self.swap_delete], float)
+        p = np.array([self.translation, self.rotation, self.swap_insert, self.swap_delete,
+                      self.reinsertion, self.widom], float)
         return np.cumsum(p / p.sum())
 
 

@@ -40,7 +40,7 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 CASES = {
     "methane_config0_1e5": (lambda: systems.methane_system(seed=0), dict(pressure=1e5, temperature=300.0), 1000, 8000),
     "methane_config0_1e7": (lambda: systems.methane_system(seed=0), dict(pressure=1e7, temperature=300.0), 1000, 3000),
-    "co2_config1_1e5": (lambda: systems.co2_system(seed=1), dict(pressure=1e5, temperature=298.0), 1500, 2500),
+    "co2_config1_1e5": (lambda: systems.co2_system(seed=1), dict(pressure=1e5, temperature=298.0), 4000, 4000),
 }
 SEEDS = 8
 
