@@ -186,10 +186,11 @@ int rgpu_engine_sync(rgpu_engine *eng);
  * of launching the kernel directly. */
 int rgpu_engine_use_graph(rgpu_engine *eng, int on);
 /* Running energies (8 doubles, first six as rgpu_total_energy), counters
- * (20: attempts[4], accepted[4], counted moves, overlaps, pairs visited,
- * pairs in cut-off, charged pairs in cut-off, k x site products, k sums,
- * engine clock cycles, of which in pair evaluations, in Ewald sums, 2
- * spare), molecule count, status word (0 = fine) and next step index. */
+ * (20: attempts[4] and accepted[4] of translation, rotation, insertion,
+ * deletion; counted moves, overlaps, pairs visited, pairs in cut-off,
+ * charged pairs in cut-off, k x site products, k sums, engine clock cycles,
+ * of which in pair evaluations, in Ewald sums; reinsertions attempted,
+ * accepted), molecule count, status word (0 = fine) and next step index. */
 int rgpu_system_state(rgpu_system *sys, double *energy8, long long *counters20, int *nmol, int *status,
                       unsigned long long *step);
 /* Resets the running energies to `energy8` (e.g. after rgpu_total_energy). */
@@ -201,10 +202,14 @@ int rgpu_system_set_energy(rgpu_system *sys, const double *energy8);
  * once per MC step. */
 int rgpu_system_set_limits(rgpu_system *sys, unsigned long long end_step, unsigned long long avg_start);
 /* Ensemble sums: {steps sampled, sum N, sum N^2, sum U, sum U*N, sum U^2,
- * 0, 0}, U = the six running energy terms added, N = molecules. Loading
- * <N>, energy <U> and the enthalpy of adsorption
- * (<UN> - <U><N>) / (<N^2> - <N>^2) - k_B T (src/statistics.c:4077-4079)
- * follow from them. */
+ * sum of Widom Rosenbluth weights, Widom samples}, U = the six running
+ * energy terms added, N = molecules. Loading <N>, energy <U> and the
+ * enthalpy of adsorption (<UN> - <U><N>) / (<N^2> - <N>^2) - k_B T
+ * (src/statistics.c:4077-4079) follow from the first six; the average Widom
+ * weight <W> (src/mc_moves.c:7844-8030; an overlapping test insertion counts
+ * with W = 0) gives the excess chemical potential -k_B T ln <W> and the
+ * Henry coefficient beta <W> per unit volume. Widom samples are taken at
+ * every Widom step, whatever the step window. */
 int rgpu_system_averages(rgpu_system *sys, double *sums8);
 int rgpu_system_reset_averages(rgpu_system *sys);
 

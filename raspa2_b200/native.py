@@ -256,7 +256,9 @@ class GpuSystem:
         var = N2 - N * N
         kT = units.K_B * self.sysm.temperature
         dh = (UN - U * N) / var - kT if var > 0 else float("nan")
-        return {"samples": int(sm[0]), "loading": N, "energy": U, "enthalpy": dh, "sums": sm}
+        widom = sm[6] / sm[7] if sm[7] > 0 else float("nan")
+        return {"samples": int(sm[0]), "loading": N, "energy": U, "enthalpy": dh, "widom_weight": widom,
+                "sums": sm}
 
     def reset_averages(self):
         _check(load().rgpu_system_reset_averages(self.h))
