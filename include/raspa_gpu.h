@@ -174,6 +174,13 @@ int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const 
  * 64..512 (RGPU_FP64). */
 int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
                        int cluster);
+/* As rgpu_engine_create, with the shared memory and registers of each CTA
+ * sized so that `ctas_per_sm` CTAs (1..4) can share one SM: CTAs of
+ * different systems then interleave on an SM and fill each other's barrier
+ * waits. Framework and wave vectors that no longer fit are read from global
+ * memory (L2). No counterpart in the reference. */
+int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
+                          int cluster, int ctas_per_sm);
 /* CTAs per system of an engine. */
 int rgpu_engine_cluster(rgpu_engine *eng);
 int rgpu_engine_destroy(rgpu_engine *eng);

@@ -94,6 +94,7 @@ struct rgpu_engine {
   std::vector<rgpu_system *> sys;
   RgpuSys *d_systems;
   int mixed, threads, kw, max_ads, cluster, fw_items, tile_items, k_items;
+  bool wide;                  /* 64-register build of the mixed kernel */
   size_t smem;
   cudaStream_t st;
   /* CUDA graph of one launch, replayed by rgpu_engine_run when enabled */
@@ -965,7 +966,14 @@ static int auto_cluster(int nsys)
 extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
                                   int cluster)
 {
+  return rgpu_engine_create_ex(out, systems, n, precision, threads, cluster, 1);
+}
+
+extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *systems, int n, int precision,
+                                     int threads, int cluster, int ctas_per_sm)
+{
   if (!out || !systems || n < 1) return fail(RGPU_E_INVALID, "bad argument");
+  if (ctas_per_sm < 1 || ctas_per_sm > 4) return fail(RGPU_E_INVALID, "ctas_per_sm %d outside [1,4]", ctas_per_sm);
   if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
   /* the mixed kernel is compiled for up to 1024 threads (64 registers), the
    * FP64 one for up to 512 */
@@ -973,10 +981,18 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
   if (threads < 64 || threads > max_threads || threads % 32)
     return fail(RGPU_E_INVALID, "threads %d outside [64,%d] or not a multiple of 32", threads, max_threads);
   if (cluster < 0 || cluster > 8 || (cluster & (cluster - 1))) return fail(RGPU_E_INVALID, "cluster %d", cluster);
+  /* registers: 128 per thread (the narrow build) unless the CTAs of an SM
+   * need more than 65536 together; then the mixed kernel's 64-register build */
+  const bool wide = threads > 512 || (long long)threads * 128 * ctas_per_sm > 65536;
+  if (wide && precision != RGPU_MIXED)
+    return fail(RGPU_E_INVALID, "FP64 engine: %d CTAs of %d threads do not fit one SM", ctas_per_sm, threads);
+  if ((long long)threads * 64 * ctas_per_sm > 65536)
+    return fail(RGPU_E_INVALID, "%d CTAs of %d threads do not fit one SM", ctas_per_sm, threads);
   *out = nullptr;
   rgpu_engine *e = new rgpu_engine();
   e->mixed = precision == RGPU_MIXED;
   e->threads = threads;
+  e->wide = wide;
   e->cluster = cluster ? cluster : auto_cluster(n);
   e->kw = 1;
   e->max_ads = 0;
@@ -994,6 +1010,13 @@ extern "C" int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems
   int dev = 0, smem_max = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (ctas_per_sm > 1) {
+    /* room for ctas_per_sm CTAs per SM, each with its 1 KB of reserved
+     * shared memory */
+    int per_sm = 0;
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    smem_max = std::min(smem_max, per_sm / ctas_per_sm - 1024);
+  }
   if (e->mixed) {
     e->tile_items = maxtile;
     e->fw_items = maxtile * RGPU_TILE;
@@ -1056,10 +1079,10 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   const int n = (int)e->sys.size();
-  CK(rgpu_engine_prepare(e->mixed, e->threads, e->smem));
+  CK(rgpu_engine_prepare(e->mixed, e->wide, e->smem));
   if (!e->use_graph) {
     CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
-                          e->k_items, e->cluster, e->threads, st));
+                          e->k_items, e->cluster, e->threads, e->wide, st));
   } else {
     if (!e->gexec || e->g_nsteps != nsteps) {
       if (e->gexec) {
@@ -1069,7 +1092,7 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       cudaError_t le = rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items,
-                                          e->tile_items, e->k_items, e->cluster, e->threads, st);
+                                          e->tile_items, e->k_items, e->cluster, e->threads, e->wide, st);
       cudaError_t ce = cudaStreamEndCapture(st, &g);
       if (le != cudaSuccess || ce != cudaSuccess) {
         if (g) cudaGraphDestroy(g);

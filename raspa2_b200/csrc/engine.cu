@@ -850,8 +850,8 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
 }
 
 /* WIDE: compiled for CTAs of up to 1024 threads (64 registers per thread);
- * otherwise up to 512 threads with 128 registers. The launch picks the
- * instantiation from the CTA size. */
+ * otherwise up to 512 threads with 128 registers. The engine picks WIDE for
+ * CTAs above 512 threads and when several CTAs must share an SM. */
 template <bool MIXED, bool WIDE>
 __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps,
                                                                        int kw, int max_ads_atoms, int fw_items,
@@ -1059,17 +1059,17 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
   cl.sync();
 }
 
-cudaError_t rgpu_engine_prepare(int mixed, int threads, size_t smem)
+cudaError_t rgpu_engine_prepare(int mixed, bool wide, size_t smem)
 {
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (mixed && threads > 512) return cudaFuncSetAttribute(rgpu_engine_kernel<true, true>, a, (int)smem);
+  if (mixed && wide) return cudaFuncSetAttribute(rgpu_engine_kernel<true, true>, a, (int)smem);
   if (mixed) return cudaFuncSetAttribute(rgpu_engine_kernel<true, false>, a, (int)smem);
   return cudaFuncSetAttribute(rgpu_engine_kernel<false, false>, a, (int)smem);
 }
 
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
-                               int threads, cudaStream_t st)
+                               int threads, bool wide, cudaStream_t st)
 {
   size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items, threads);
   cudaLaunchConfig_t cfg = {};
@@ -1087,7 +1087,7 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
   cudaError_t e;
   /* the dynamic shared-memory limit is raised by rgpu_engine_prepare, outside
    * any stream capture */
-  if (mixed && threads > 512)
+  if (mixed && wide)
     e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true, true>, d_systems, nsys, nsteps, kw, max_ads_atoms,
                            fw_items, tile_items, k_items);
   else if (mixed)

@@ -30,7 +30,7 @@ EXPORTS = [
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
-    "rgpu_system_reset_averages", "rgpu_engine_use_graph",
+    "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -303,12 +303,13 @@ def grid_interpolate_noalloc(d_grid_ptr: int, npts, size, shift, cell, xyz) -> n
 class Engine:
     """Persistent batched engine over several GpuSystems (rgpu_engine)."""
 
-    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=512, cluster=0):
+    def __init__(self, systems: Sequence[GpuSystem], precision=RGPU_MIXED, threads=512, cluster=0, ctas_per_sm=1):
         L = load()
         arr = (C.c_void_p * len(systems))(*[s.h for s in systems])
         h = C.c_void_p()
-        _check(L.rgpu_engine_create(C.byref(h), arr, C.c_int(len(systems)), C.c_int(precision), C.c_int(threads),
-                                    C.c_int(cluster)))
+        _check(L.rgpu_engine_create_ex(C.byref(h), arr, C.c_int(len(systems)), C.c_int(precision), C.c_int(threads),
+                                       C.c_int(cluster), C.c_int(ctas_per_sm)))
+        self.ctas_per_sm = ctas_per_sm
         self.cluster = int(L.rgpu_engine_cluster(h))
         self.threads = threads
         self.precision = precision

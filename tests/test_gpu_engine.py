@@ -11,10 +11,11 @@ from golden_cases import load, system_of
 pytestmark = pytest.mark.gpu
 
 
-def engine_run(sysm, mols, nsteps, precision, seed=777, stream_id=3, threads=256, maxmol=64, cluster=0):
+def engine_run(sysm, mols, nsteps, precision, seed=777, stream_id=3, threads=256, maxmol=64, cluster=0,
+               ctas_per_sm=1):
     g = native.GpuSystem(sysm, maxmol=maxmol, seed=seed, stream_id=stream_id)
     g.set_adsorbates(mols)
-    e = native.Engine([g], precision=precision, threads=threads, cluster=cluster)
+    e = native.Engine([g], precision=precision, threads=threads, cluster=cluster, ctas_per_sm=ctas_per_sm)
     e.run(nsteps)
     e.sync()
     return g, g.state()
@@ -29,16 +30,17 @@ def oracle_run(sysm, mols, nsteps, seed=777, stream_id=3, maxmol=64):
     return o, st
 
 
-@pytest.mark.parametrize("name,cluster", [("co2_tiny", 1), ("co2_tiny", 2), ("co2_config1", 8),
-                                          ("methane_config0", 2)])
-def test_fp64_engine_reproduces_oracle_trajectory(cuda, name, cluster):
+@pytest.mark.parametrize("name,cluster,occ", [("co2_tiny", 1, 1), ("co2_tiny", 2, 1), ("co2_config1", 8, 1),
+                                              ("methane_config0", 2, 1), ("co2_config1", 2, 2)])
+def test_fp64_engine_reproduces_oracle_trajectory(cuda, name, cluster, occ):
     """Same counter-based stream, same decisions: the FP64 engine (framework
-    split over `cluster` CTAs) follows the oracle's GCMC trajectory."""
+    split over `cluster` CTAs; with occ = 2 sized for two CTAs per SM, so
+    with less staged in shared memory) follows the oracle's GCMC trajectory."""
     c = load(name)
     s = system_of(c)
     mols = np.array(c["molecules"])
     n = 300
-    g, st = engine_run(s, mols, n, native.RGPU_FP64, cluster=cluster)
+    g, st = engine_run(s, mols, n, native.RGPU_FP64, cluster=cluster, ctas_per_sm=occ)
     o, ost = oracle_run(s, mols, n)
     assert st["status"] == 0
     assert st["step"] == n
