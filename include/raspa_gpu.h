@@ -76,6 +76,18 @@ typedef struct {
   int ntrial;                 /* NumberOfTrialPositions (<= 16) */
   uint64_t seed;              /* random stream seed */
   uint32_t stream_id;         /* random stream id of this system */
+  /* Flexible linear chain (e.g. united-atom alkanes): atoms 0..natom-1 in
+   * chain order, grown from atom 0 (start_bead must be 0), uncharged. Fixed
+   * bond length, one harmonic bend 0.5 bend_k (theta - bend_theta0)^2 per
+   * atom triple, one TraPPE torsion t0 + t1 (1 + cos phi) + t2 (1 - cos 2 phi)
+   * + t3 (1 + cos 3 phi) per quadruple (src/internal_energy.c TRAPPE_DIHEDRAL,
+   * HARMONIC_BEND), LJ between atoms four or more bonds apart. Energies in
+   * internal units, angles in radians. flexible = 0: rigid molecule
+   * (mol_ref is its geometry). */
+  int flexible;
+  double bond;
+  double bend_k, bend_theta0;
+  double torsion[4];
 } rgpu_system_desc;
 
 const char *rgpu_error_string(int code);
@@ -136,6 +148,12 @@ int rgpu_ewald_accept(rgpu_system *sys);
  * (CalculateEnergy, src/integration.c:250): out = {host VDW, adsorbate VDW,
  * host real, adsorbate real, host Fourier, adsorbate Fourier}. FP64. */
 int rgpu_total_energy(rgpu_system *sys, double *out);
+
+/* Intramolecular energy (bends, torsions, LJ of atoms four or more bonds
+ * apart) of all molecules of a flexible-chain system, recomputed from the
+ * current positions; 0 for rigid molecules. The engine's running value is
+ * energy8[6] of rgpu_system_state. */
+int rgpu_intra_energy(rgpu_system *sys, double *out);
 
 /* ---- energy grids (src/grids.c) ----------------------------------------- */
 /* MakeGrid (src/grids.c:431-690) for pseudo-atom `type`: (n+1)^3 points

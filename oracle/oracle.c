@@ -703,6 +703,223 @@ void or_cbmc_retrace(const or_sys *s, int m, int nf, int nt, or_rng_fn rng, void
 }
 
 /* ---------------------------------------------------------------------- */
+/* Flexible linear chains. CBMC growth bead by bead from atom 0
+ * (GrowMolecule / RetraceMolecule, src/cbmc.c:2928-3181, for a linear
+ * chain; bonded terms sampled as in GenerateTrialOrientationsMCScheme,
+ * src/cbmc.c:1580-2480): bead i >= 1 at the fixed bond length from bead i-1,
+ * its bend angle drawn from sin(theta) exp(-beta U_bend) (Gaussian proposal
+ * accepted with probability sin(theta)), its dihedral from exp(-beta
+ * U_torsion) (uniform proposal accepted with exp(-beta (U - min U))). The
+ * draws are keyed (stage, bead, trial, draw) in the counter-based stream;
+ * the GPU engine uses the same keys. Bend HARMONIC_BEND and torsion
+ * TRAPPE_DIHEDRAL as src/internal_energy.c:205, :2324. */
+#define CHAIN_SLOT_SEL (1u << 15)
+#define CHAIN_SLOT (1u << 16)
+#define CHAIN_TRIES 64
+
+static uint32_t chain_slot(int stage, int bead, int trial, int k)
+{
+  return CHAIN_SLOT + ((((uint32_t)stage * 8u + (uint32_t)bead) * 16u + (uint32_t)trial) << 9) + (uint32_t)k;
+}
+
+static double bend_energy(const or_sys *s, double th)
+{
+  double d = th - s->bend_theta0;
+  return 0.5 * s->bend_k * d * d;
+}
+
+static double torsion_energy(const or_sys *s, double c)
+{
+  double c2 = 2.0 * c * c - 1.0, c3 = c * (4.0 * c * c - 3.0);
+  return s->torsion[0] + s->torsion[1] * (1.0 + c) + s->torsion[2] * (1.0 - c2) + s->torsion[3] * (1.0 + c3);
+}
+
+static double angle3(const double *a, const double *b, const double *c)
+{
+  double u[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]}, v[3] = {c[0] - b[0], c[1] - b[1], c[2] - b[2]};
+  double cs = (u[0] * v[0] + u[1] * v[1] + u[2] * v[2]) /
+              sqrt((u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+  if (cs > 1.0) cs = 1.0;
+  if (cs < -1.0) cs = -1.0;
+  return acos(cs);
+}
+
+static void cross3(const double *a, const double *b, double *o)
+{
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static double cos_dihedral(const double *a, const double *b, const double *c, const double *d)
+{
+  double b1[3], b2[3], b3[3], n1[3], n2[3];
+  for (int k = 0; k < 3; k++) { b1[k] = b[k] - a[k]; b2[k] = c[k] - b[k]; b3[k] = d[k] - c[k]; }
+  cross3(b1, b2, n1);
+  cross3(b2, b3, n2);
+  double cs = (n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2]) /
+              sqrt((n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2]) * (n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]));
+  if (cs > 1.0) cs = 1.0;
+  if (cs < -1.0) cs = -1.0;
+  return cs;
+}
+
+/* bead at distance L from c with angle theta (b-c-new) and dihedral phi
+ * (a-b-c-new); without a, phi is the azimuth about b-c from the coordinate
+ * axis least aligned with it */
+static void place(const double *a, const double *b, const double *c, double L, double theta, double phi,
+                  double *out)
+{
+  double bc[3] = {c[0] - b[0], c[1] - b[1], c[2] - b[2]};
+  double nb = sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]);
+  for (int k = 0; k < 3; k++) bc[k] /= nb;
+  double ref[3] = {0.0, 0.0, 0.0};
+  if (a) {
+    for (int k = 0; k < 3; k++) ref[k] = b[k] - a[k];
+  } else {
+    double ax = fabs(bc[0]), ay = fabs(bc[1]), az = fabs(bc[2]);
+    if (ax <= ay && ax <= az) ref[0] = 1.0;
+    else if (ay <= az) ref[1] = 1.0;
+    else ref[2] = 1.0;
+  }
+  double n[3], m[3];
+  cross3(ref, bc, n);
+  double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  for (int k = 0; k < 3; k++) n[k] /= nn;
+  cross3(n, bc, m);
+  double dx = -L * cos(theta), dy = L * sin(theta) * cos(phi), dz = L * sin(theta) * sin(phi);
+  for (int k = 0; k < 3; k++) out[k] = c[k] + dx * bc[k] + dy * m[k] + dz * n[k];
+}
+
+static double bonded_energy(const or_sys *s, const double (*x)[3], int i, const double *p)
+{
+  double e = 0.0;
+  if (i >= 2) e += bend_energy(s, angle3(x[i - 2], x[i - 1], p));
+  if (i >= 3) e += torsion_energy(s, cos_dihedral(x[i - 3], x[i - 2], x[i - 1], p));
+  return e;
+}
+
+static double intra_lj(const or_sys *s, const double (*x)[3], int i, const double *p)
+{
+  double e = 0.0;
+  for (int j = 0; j + 4 <= i; j++) {
+    double d[3] = {p[0] - x[j][0], p[1] - x[j][1], p[2] - x[j][2]};
+    double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    if (r2 < s->rc2_vdw) e += or_lj(s, s->mol_type[i], s->mol_type[j], r2);
+  }
+  return e;
+}
+
+double or_intra_energy(const or_sys *s)
+{
+  double e = 0.0;
+  if (!s->flexible) return 0.0;
+  for (int m = 0; m < s->nmol; m++) {
+    const double(*x)[3] = (const double(*)[3])(s->ads_xyz + 3 * m * s->natom);
+    for (int i = 1; i < s->natom; i++) e += bonded_energy(s, x, i, x[i]) + intra_lj(s, x, i, x[i]);
+  }
+  return e;
+}
+
+static double chain_u(const philox_ctx *c, int stage, int i, int t, int k)
+{
+  return or_philox_uniform(c->seed, c->system, c->step, chain_slot(stage, i, t, k));
+}
+
+/* trial position of bead i >= 1 after beads x[0..i-1]; returns its bonded energy */
+static double chain_trial(const or_sys *s, const double (*x)[3], int i, const philox_ctx *c, int stage, int t,
+                          double *p)
+{
+  int k = 0;
+  if (i == 1) {
+    double z = 2.0 * chain_u(c, stage, i, t, 0) - 1.0;
+    double psi = 2.0 * M_PI * chain_u(c, stage, i, t, 1);
+    double r = sqrt(fmax(0.0, 1.0 - z * z));
+    p[0] = x[0][0] + s->bond * r * cos(psi);
+    p[1] = x[0][1] + s->bond * r * sin(psi);
+    p[2] = x[0][2] + s->bond * z;
+    return 0.0;
+  }
+  double theta = s->bend_theta0;
+  for (int a = 0; a < CHAIN_TRIES; a++, k += 3) {
+    double u1 = chain_u(c, stage, i, t, k), u2 = chain_u(c, stage, i, t, k + 1), u3 = chain_u(c, stage, i, t, k + 2);
+    double th = s->bend_theta0 + s->bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
+    if (th > 0.0 && th < M_PI && u3 < sin(th)) {
+      theta = th;
+      break;
+    }
+  }
+  k = 3 * CHAIN_TRIES;
+  double phi;
+  if (i == 2) {
+    phi = 2.0 * M_PI * chain_u(c, stage, i, t, k) - M_PI;
+  } else {
+    phi = M_PI;
+    for (int a = 0; a < CHAIN_TRIES; a++, k += 2) {
+      double f = 2.0 * M_PI * chain_u(c, stage, i, t, k) - M_PI;
+      if (chain_u(c, stage, i, t, k + 1) < exp(-s->beta * (torsion_energy(s, cos(f)) - s->torsion_min))) {
+        phi = f;
+        break;
+      }
+    }
+  }
+  place(i >= 3 ? x[i - 3] : NULL, x[i - 2], x[i - 1], s->bond, theta, phi, p);
+  return bonded_energy(s, x, i, p);
+}
+
+/* CBMC growth (retrace = 0) or retrace of a chain; exclude = molecule left
+ * out of the adsorbate sums, m = molecule retraced. out = {fail, W, host VDW,
+ * adsorbate VDW, intramolecular}; x receives the chosen beads. */
+static void chain_grow(const or_sys *s, int retrace, int stage, int m, int exclude, int nf, int nt,
+                       const philox_ctx *c, double *out, double (*x)[3])
+{
+  const int na = s->natom;
+  double rosen = 1.0, hv = 0.0, av = 0.0, intra = 0.0;
+  out[0] = 1.0;
+  for (int i = 0; i < na; i++) {
+    const int k = i == 0 ? nf : nt;
+    double w[MAX_TRIALS], pe[MAX_TRIALS][4], lj[MAX_TRIALS], ub[MAX_TRIALS], pos[MAX_TRIALS][3];
+    int any = 0;
+    for (int t = 0; t < k; t++) {
+      ub[t] = 0.0;
+      if (retrace && t == 0) {
+        for (int d = 0; d < 3; d++) pos[0][d] = s->ads_xyz[3 * (m * na + i) + d];
+        ub[0] = bonded_energy(s, (const double(*)[3])x, i, pos[0]);
+      } else if (i == 0) {
+        for (int d = 0; d < 3; d++) pos[t][d] = s->box[d] * chain_u(c, stage, 0, t, d);
+      } else {
+        ub[t] = chain_trial(s, (const double(*)[3])x, i, c, stage, t, pos[t]);
+      }
+      or_point_energy(s, s->mol_type[i], s->mol_q[i], pos[t], exclude, pe[t]);
+      lj[t] = intra_lj(s, (const double(*)[3])x, i, pos[t]);
+      int ov = pe[t][0] >= s->overlap || pe[t][1] >= s->overlap || pe[t][2] >= s->overlap ||
+               pe[t][3] >= s->overlap || lj[t] >= s->overlap;
+      w[t] = ov ? 0.0 : exp(-s->beta * (pe[t][0] + pe[t][2] + lj[t]));
+      if (!ov) any = 1;
+    }
+    double wsum = 0.0;
+    for (int t = 0; t < k; t++) wsum += w[t];
+    int sel = 0;
+    if (!retrace && any) {
+      double target = or_philox_uniform(c->seed, c->system, c->step, CHAIN_SLOT_SEL + stage * 8 + i) * wsum;
+      double cum = w[0];
+      while (cum < target && sel < k - 1) cum += w[++sel];
+    }
+    rosen *= wsum / (double)k;
+    if (!any || (!retrace && rosen < 1e-150)) return;
+    hv += pe[sel][0];
+    av += pe[sel][2];
+    intra += lj[sel] + ub[sel];
+    for (int d = 0; d < 3; d++) x[i][d] = pos[sel][d];
+  }
+  out[0] = 0.0;
+  out[1] = rosen;
+  out[2] = hv;
+  out[3] = av;
+  out[4] = intra;
+}
+
+/* ---------------------------------------------------------------------- */
 /* Energy grids */
 
 /* CalculateDerivativesAtPositionVDW (src/framework_hessian.c:63-109) with the
@@ -891,6 +1108,57 @@ void or_mc_run(or_sys *s, const or_mc_params *p, or_mc_state *st, uint64_t step0
         if (s->ewald) memcpy(s->sk_ads, nk, sizeof(double) * 2 * s->nk);
         st->u[0] += dl[0]; st->u[1] += dl[1]; st->u[2] += dl[2]; st->u[3] += dl[3];
         st->u[4] += de[1]; st->u[5] += de[0];
+      }
+    } else if (s->flexible && mv >= 2) {
+      /* flexible chains: CBMC insertion, deletion, reinsertion, Widom */
+      if (mv == 4 && s->nmol == 0) continue;
+      st->moves++;
+      st->attempts[mv]++;
+      if (mv == 5) st->widom_n += 1.0;
+      if (mv == 2 && s->nmol >= s->maxmol) continue;
+      if (mv == 3 && s->nmol == 0) continue;
+      int m = s->nmol;
+      if (mv == 3 || mv == 4) {
+        m = (int)(rng_philox(&ctx, SLOT_MOLECULE) * s->nmol);
+        if (m >= s->nmol) m = s->nmol - 1;
+      }
+      double o[5], x[MAX_ATOMS][3];
+      if (mv == 2 || mv == 5) {
+        chain_grow(s, 0, 0, s->nmol, s->nmol, p->ntrial_first, p->ntrial, &ctx, o, x);
+        if (o[0] != 0.0) continue;
+        if (mv == 5) {
+          st->widom_sum += o[1];
+          continue;
+        }
+        if (rng_philox(&ctx, SLOT_ACCEPT) < o[1] * p->fugacity_beta_v / (1.0 + s->nmol)) {
+          st->accepted[2]++;
+          for (int a = 0; a < na; a++)
+            for (int d = 0; d < 3; d++) s->ads_xyz[3 * (s->nmol * na + a) + d] = x[a][d];
+          s->nmol++;
+          st->u[0] += o[2]; st->u[1] += o[3]; st->u_intra += o[4];
+        }
+      } else if (mv == 3) {
+        chain_grow(s, 1, 1, m, m, p->ntrial_first, p->ntrial, &ctx, o, x);
+        if (o[0] != 0.0) continue;
+        if (rng_philox(&ctx, SLOT_ACCEPT) < (double)s->nmol / (o[1] * p->fugacity_beta_v)) {
+          st->accepted[3]++;
+          int last = s->nmol - 1;
+          for (int a = 0; a < 3 * na; a++) s->ads_xyz[3 * m * na + a] = s->ads_xyz[3 * last * na + a];
+          s->nmol--;
+          st->u[0] -= o[2]; st->u[1] -= o[3]; st->u_intra -= o[4];
+        }
+      } else {
+        double on[5], xn[MAX_ATOMS][3];
+        chain_grow(s, 0, 0, m, m, p->ntrial_first, p->ntrial, &ctx, on, xn);
+        if (on[0] != 0.0) continue;
+        chain_grow(s, 1, 1, m, m, p->ntrial_first, p->ntrial, &ctx, o, x);
+        if (o[0] != 0.0) continue;
+        if (rng_philox(&ctx, SLOT_ACCEPT) < on[1] / o[1]) {
+          st->accepted[4]++;
+          for (int a = 0; a < na; a++)
+            for (int d = 0; d < 3; d++) s->ads_xyz[3 * (m * na + a) + d] = xn[a][d];
+          st->u[0] += on[2] - o[2]; st->u[1] += on[3] - o[3]; st->u_intra += on[4] - o[4];
+        }
       }
     } else if (mv == 2) {
       st->moves++;

@@ -47,6 +47,12 @@ typedef struct {
   double *kfactor;                      /* [nk] */
   double *sk_fw, *sk_ads;               /* [nk*2] (re, im) */
   double uion, net_fw, net_ads;
+  /* flexible linear chain grown from atom 0 (flexible = 1): fixed bond
+   * length, harmonic bends, TraPPE torsions, LJ between atoms four or more
+   * bonds apart; energies in internal units, angles in radians */
+  int flexible;
+  double bond, bend_k, bend_theta0, bend_sigma;
+  double torsion[4], torsion_min;
 } or_sys;
 
 /* pair terms */
@@ -129,7 +135,12 @@ typedef struct {
   long long attempts[6], accepted[6];   /* by move type as in cum */
   long long moves;         /* counted MC moves (see or_mc_run) */
   double widom_sum, widom_n;            /* Widom Rosenbluth weights and samples */
+  double u_intra;                       /* intramolecular energy of flexible chains */
 } or_mc_state;
+
+/* intramolecular energy (bends, torsions, LJ of atoms >= 4 bonds apart) of
+ * all molecules of a flexible-chain system */
+double or_intra_energy(const or_sys *s);
 
 /* Runs `nsteps` MC steps starting at step index `step0`. */
 void or_mc_run(or_sys *s, const or_mc_params *p, or_mc_state *st, uint64_t step0,

@@ -29,6 +29,8 @@ class OrSys(C.Structure):
         ("ewald", C.c_int), ("alpha", C.c_double), ("nk", C.c_int), ("kidx", _ip),
         ("kfactor", _dp), ("sk_fw", _dp), ("sk_ads", _dp),
         ("uion", C.c_double), ("net_fw", C.c_double), ("net_ads", C.c_double),
+        ("flexible", C.c_int), ("bond", C.c_double), ("bend_k", C.c_double), ("bend_theta0", C.c_double),
+        ("bend_sigma", C.c_double), ("torsion", C.c_double * 4), ("torsion_min", C.c_double),
     ]
 
 
@@ -42,7 +44,7 @@ class MCParams(C.Structure):
 class MCState(C.Structure):
     _fields_ = [("u", C.c_double * 6), ("attempts", C.c_longlong * 6),
                 ("accepted", C.c_longlong * 6), ("moves", C.c_longlong),
-                ("widom_sum", C.c_double), ("widom_n", C.c_double)]
+                ("widom_sum", C.c_double), ("widom_n", C.c_double), ("u_intra", C.c_double)]
 
 
 _RNG_FN = C.CFUNCTYPE(C.c_double, C.c_void_p, C.c_int)
@@ -70,6 +72,7 @@ def lib():
         L.or_philox_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32]
         L.or_grid_interpolate.restype = C.c_double
         L.or_rng_mt.restype = C.c_double
+        L.or_intra_energy.restype = C.c_double
         _lib = L
     return _lib
 
@@ -139,10 +142,28 @@ class Oracle:
         eps, sig2, shift = sysm.lj_tables()
         pos, t, q = sysm.framework()
         kidx = systems.kvector_indices(sysm.kmax) if sysm.ewald else None
-        return cls(sysm.box, sysm.cutoff, units.beta(sysm.temperature), eps, sig2, shift,
-                   pos, t, q, sysm.molecule_types(), sysm.molecule.charges(),
-                   sysm.molecule.positions, sysm.molecule.starting_bead,
-                   ewald=sysm.ewald, alpha=sysm.alpha, kidx=kidx, maxmol=maxmol)
+        o = cls(sysm.box, sysm.cutoff, units.beta(sysm.temperature), eps, sig2, shift,
+                pos, t, q, sysm.molecule_types(), sysm.molecule.charges(),
+                sysm.molecule.positions, sysm.molecule.starting_bead,
+                ewald=sysm.ewald, alpha=sysm.alpha, kidx=kidx, maxmol=maxmol)
+        mol = sysm.molecule
+        if not mol.rigid:
+            s = o.s
+            s.flexible = 1
+            s.bond = mol.bond
+            s.bend_k = mol.bend_k * units.K_B
+            s.bend_theta0 = np.deg2rad(mol.bend_theta0)
+            s.bend_sigma = 1.0 / np.sqrt(s.beta * s.bend_k)
+            s.torsion[:] = [x * units.K_B for x in mol.torsion]
+            phi = np.linspace(-np.pi, np.pi, 20001)
+            c = np.cos(phi)
+            e = (s.torsion[0] + s.torsion[1] * (1 + c) + s.torsion[2] * (1 - (2 * c * c - 1))
+                 + s.torsion[3] * (1 + c * (4 * c * c - 3)))
+            s.torsion_min = e.min() - 1e-6 * (e.max() - e.min()) - 1e-12
+        return o
+
+    def intra_energy(self):
+        return lib().or_intra_energy(C.byref(self.s))
 
     # ---- state -------------------------------------------------------------
     @property

@@ -19,6 +19,7 @@
 
 #include "../../include/raspa_gpu.h"
 #include "rgpu_engine.h"
+#include "rgpu_chain.h"
 #include "rgpu_types.h"
 
 static thread_local char g_err[512];
@@ -177,10 +178,18 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   if (d->ntypes < 1 || !d->eps || !d->sig2 || !d->shift) return fail(RGPU_E_INVALID, "LJ table missing");
   if (!d->mol_type || !d->mol_q || !d->mol_ref) return fail(RGPU_E_INVALID, "molecule missing");
   if (d->start_bead < 0 || d->start_bead >= d->natom) return fail(RGPU_E_INVALID, "start_bead");
+  if (d->flexible) {
+    if (d->start_bead != 0) return fail(RGPU_E_INVALID, "a flexible chain is grown from atom 0 (start_bead 0)");
+    if (!(d->bond > 0.0)) return fail(RGPU_E_INVALID, "flexible chain: bond length must be positive");
+    if (d->natom > 1 && !(d->bend_k > 0.0)) return fail(RGPU_E_INVALID, "flexible chain: bend_k must be positive");
+    for (int a = 0; a < d->natom; a++)
+      if (d->mol_q[a] != 0.0) return fail(RGPU_E_INVALID, "flexible chains must be uncharged");
+  }
   if (d->maxmol < 1 || (long long)d->maxmol * d->natom > (1 << 20)) return fail(RGPU_E_INVALID, "maxmol");
   if (d->ntrial_first < 1 || d->ntrial_first > RGPU_MAX_TRIALS || d->ntrial < 1 || d->ntrial > RGPU_MAX_TRIALS)
     return fail(RGPU_E_INVALID, "trial counts must be in [1,%d]", RGPU_MAX_TRIALS);
-  if (d->ntrial * (d->natom - 1) > RGPU_MAX_POS) return fail(RGPU_E_INVALID, "ntrial*(natom-1) > %d", RGPU_MAX_POS);
+  if (!d->flexible && d->ntrial * (d->natom - 1) > RGPU_MAX_POS)
+    return fail(RGPU_E_INVALID, "ntrial*(natom-1) > %d", RGPU_MAX_POS);
   for (int c = 0; c < 3; c++)
     if (!(d->box[c] >= 2.0 * d->cutoff)) return fail(RGPU_E_INVALID, "box length %g < 2*cutoff", d->box[c]);
   if (d->ewald && (d->kmax[0] < 1 || d->kmax[1] < 1 || d->kmax[2] < 1 ||
@@ -408,6 +417,23 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   h.mol_charged = molq;
   h.mol_charge = mq;
   h.self_mol = self;
+  h.flexible = d->flexible;
+  if (d->flexible) {
+    h.bond = d->bond;
+    h.bend_k = d->bend_k;
+    h.bend_theta0 = d->bend_theta0;
+    h.bend_sigma = d->bend_k > 0.0 ? 1.0 / sqrt(d->beta * d->bend_k) : 0.0;
+    for (int c = 0; c < 4; c++) h.torsion[c] = d->torsion[c];
+    /* minimum of the torsion energy (scale of the rejection in chain_trial),
+     * on a fine grid less a margin so that exp(-beta (U - min)) <= 1 */
+    double tmin = 1e300, tmax = -1e300;
+    for (int g = 0; g <= 20000; g++) {
+      const double e = chain_torsion_energy(h, cos(-M_PI + 2.0 * M_PI * g / 20000.0));
+      tmin = std::min(tmin, e);
+      tmax = std::max(tmax, e);
+    }
+    h.torsion_min = tmin - 1e-6 * (tmax - tmin) - 1e-12;
+  }
   /* the exclusion sum K qa qb erf(alpha r)/r over the molecule's charged
    * pairs (src/ewald.c:7312-7330) is a constant of a rigid molecule */
   h.excl_mol = 0.0;
@@ -777,6 +803,20 @@ extern "C" int rgpu_ewald_accept(rgpu_system *s)
   CK(cudaStreamSynchronize(s->st));
   s->net_ads += s->pending_dq;
   s->pending_dq = 0.0;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_intra_energy(rgpu_system *s, double *out)
+{
+  if (!s || !out) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  const int na = s->d.natom;
+  double e = 0.0;
+  if (s->h.flexible)
+    for (int m = 0; m < s->h_nmol; m++)
+      e += chain_intra_energy(s->h, (const double(*)[3]) & s->h_xyz[(size_t)m * na * 3], na);
+  *out = e;
   return RGPU_SUCCESS;
 }
 

@@ -22,6 +22,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "rgpu_chain.h"
 #include "rgpu_device.cuh"
 #include "rgpu_engine.h"
 
@@ -30,6 +31,7 @@ namespace cg = cooperative_groups;
 #define RGPU_MAX_UNITS 512
 #define RGPU_MAX_WARPS 32
 #define RGPU_RND 192          /* random slots drawn per MC step */
+#define RGPU_CTL_BYTES 6144   /* shared-memory slot of the control block */
 
 /* ------------------------------------------------------------------------ */
 /* shared-memory plan of the engine (offsets in bytes from the dynamic base).
@@ -73,7 +75,7 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.kf = o; o = rgpu_align(o + (size_t)k_items * sizeof(double));
   L.skfw = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
   L.skads = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
-  L.ctl = o; o = rgpu_align(o + 4096);
+  L.ctl = o; o = rgpu_align(o + RGPU_CTL_BYTES);
   L.total = o;
   return L;
 }
@@ -94,6 +96,13 @@ struct Ctl {
   double uo[4];               /* energies of the retraced old configuration (reinsertion) */
   double rosen;
   double rosen_old;
+  /* flexible chains: chosen bead positions of the configuration being grown
+   * or retraced (cp) and of a reinsertion's new one (cpn), bonded energies
+   * of the current trials, intramolecular energies of the configurations */
+  double cp[RGPU_MAX_ATOMS][3];
+  double cpn[RGPU_MAX_ATOMS][3];
+  double ub[RGPU_MAX_TRIALS];
+  double uintra, uintra_old;
   double dl[4];
   int nmol;
   int fail;
@@ -108,7 +117,7 @@ struct Ctl {
   int next;                   /* unit counter of eval_units */
   double ewt[2][2];           /* this CTA's Ewald sums {e_ads, e_host}, by buffer */
 };
-static_assert(sizeof(Ctl) <= 4096, "control block exceeds its shared-memory slot");
+static_assert(sizeof(Ctl) <= RGPU_CTL_BYTES, "control block exceeds its shared-memory slot");
 
 template <bool MIXED>
 struct Eng {
@@ -127,6 +136,7 @@ struct Eng {
   double *red;               /* [2][2*RGPU_MAX_WARPS] */
   Ctl *ctl;
   const double *rnd;         /* this step's uniforms */
+  uint64_t step;             /* index of the current MC step */
   int rank, csize;
   int xb;                    /* exchange buffer (same sequence in every thread and CTA) */
 };
@@ -840,6 +850,194 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
 }
 
 /* ------------------------------------------------------------------------ */
+/* CBMC growth (retrace = false) or retrace (retrace = true) of a flexible
+ * chain, bead by bead from atom 0 (GrowMolecule / RetraceMolecule,
+ * src/cbmc.c:2928-3181, for a linear chain): the first bead from nf trials
+ * (random in the box; for a retrace trial 0 is the old bead), every other
+ * bead from nt trials drawn by chain_trial (bonded Boltzmann factor built
+ * in). The weight of a trial is exp(-beta (host VDW + adsorbate VDW + LJ
+ * with the chain's beads four or more bonds back)); a trial overlaps when
+ * one of them reaches the criterion. Leaves in Ctl the Rosenbluth weight
+ * (product over beads of sum w / trials), the chosen beads (cp), their
+ * host and adsorbate VDW (u[0], u[2]) and the intramolecular energy
+ * (uintra: bonded + LJ), or fail. Molecule m is the one retraced; `exclude`
+ * leaves a molecule out of the adsorbate sums. All threads call. */
+template <bool MIXED>
+__device__ __forceinline__ void grow_chain(Eng<MIXED> &E, bool retrace, int stage, int m, int exclude)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, nf = S.ntrial_first, nt = S.ntrial;
+  if (threadIdx.x == 0) {
+    C.rosen = 1.0;
+    C.u[0] = C.u[1] = C.u[2] = C.u[3] = 0.0;
+    C.uintra = 0.0;
+    C.fail = 0;
+  }
+  for (int i = 0; i < na; i++) {
+    const int k = i == 0 ? nf : nt;
+    if (threadIdx.x < k) {
+      const int t = threadIdx.x;
+      double p[3], ub = 0.0;
+      if (retrace && t == 0) {
+        atom_xyz(E, m, i, p);
+        ub = chain_bonded_energy(S, C.cp, i, p);
+      } else if (i == 0) {
+        for (int d = 0; d < 3; d++)
+          p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
+      } else {
+        const uint64_t step = E.step;
+        ub = chain_trial(S, C.cp, i,
+                         [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); }, p);
+      }
+      bead_set(E.pos[t], S, p[0], p[1], p[2], i, exclude);
+      C.ub[t] = ub;
+    }
+    __syncthreads();
+    engine_eval<MIXED>(E, k, 0);
+    const int b = E.xb;
+    E.xb ^= 1;
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double r[4] = {0.0, 0.0, 0.0, 0.0}, lj = 0.0, bf = 0.0;
+      int o = 0, ov = 0;
+      if (lane < k) {
+        gather(E, b, lane, r, o);
+        const double p[3] = {E.pos[lane].x, E.pos[lane].y, E.pos[lane].z};
+        lj = chain_intra_lj(S, C.cp, i, p);
+        ov = r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap || lj >= S.overlap;
+        bf = -S.beta * (r[0] + r[2] + lj);
+      }
+      const bool valid = lane < k && !ov;
+      const double w = valid ? exp(bf) : 0.0;
+      const bool any = __ballot_sync(RGPU_FULL, valid) != 0u;
+      double wsum = 0.0;
+      for (int t = 0; t < k; t++) wsum += __shfl_sync(RGPU_FULL, w, t);
+      int sel = 0;
+      if (!retrace && any) {
+        /* SelectTrialPosition (src/cbmc.c:563-599) on the weights themselves */
+        const double target = rgpu_uniform(S.seed, S.sys_id, E.step, RGPU_SLOT_CHAIN_SEL + stage * 8 + i) * wsum;
+        double cum = __shfl_sync(RGPU_FULL, w, 0);
+        while (cum < target && sel < k - 1) {
+          sel++;
+          cum += __shfl_sync(RGPU_FULL, w, sel);
+        }
+      }
+      const double hv = __shfl_sync(RGPU_FULL, r[0], sel), av = __shfl_sync(RGPU_FULL, r[2], sel);
+      const double ljs = __shfl_sync(RGPU_FULL, lj, sel);
+      if (lane == 0) {
+        C.rosen *= wsum / (double)k;
+        if (!any || (!retrace && C.rosen < 1e-150)) C.fail = 1;
+        C.u[0] += hv;
+        C.u[2] += av;
+        C.uintra += ljs + C.ub[sel];
+        C.cp[i][0] = E.pos[sel].x;
+        C.cp[i][1] = E.pos[sel].y;
+        C.cp[i][2] = E.pos[sel].z;
+        if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
+      }
+    }
+    __syncthreads();
+    if (C.fail) return;
+  }
+}
+
+/* CBMC insertion, deletion and Widom test insertion of a flexible chain
+ * (SwapAddAdsorbateMove src/mc_moves.c:7016, SwapRemoveAdsorbateMove :7228,
+ * WidomAdsorbateMove :7844; uncharged chains, no Fourier part). */
+template <bool MIXED>
+__device__ __forceinline__ void step_swap_chain(Eng<MIXED> &E, bool insert, bool widom)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, nmol = C.nmol;
+  if (widom && threadIdx.x == 0) C.sums[RGPU_SUM_WIDOM_N] += 1.0;
+  int m = nmol;
+  if (!insert) {
+    m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
+    if (m >= nmol) m = nmol - 1;
+  }
+  grow_chain<MIXED>(E, !insert, insert ? 0 : 1, m, insert ? -1 : m);
+  if (C.fail) return;
+  if (threadIdx.x == 0) {
+    double pacc;
+    if (insert) pacc = C.rosen * S.fugacity_beta_v / (1.0 + nmol);
+    else pacc = (double)nmol / (C.rosen * S.fugacity_beta_v);
+    if (!(pacc == pacc)) C.status |= RGPU_ERR_NONFINITE;
+    C.accept = !widom && E.rnd[SLOT_ACCEPT] < pacc;
+    if (widom) C.sums[RGPU_SUM_WIDOM_W] += C.rosen;
+    if (C.accept) {
+      C.cnt[RGPU_CNT_ACCEPT + (insert ? 2 : 3)]++;
+      const double sgn = insert ? 1.0 : -1.0;
+      C.energy[RGPU_E_HOST_VDW] += sgn * C.u[0];
+      C.energy[RGPU_E_ADS_VDW] += sgn * C.u[2];
+      C.energy[RGPU_E_INTRA] += sgn * C.uintra;
+    }
+  }
+  __syncthreads();
+  if (C.accept) {
+    if (insert) {
+      if (threadIdx.x < na) atom_store(E, nmol, threadIdx.x, C.cp[threadIdx.x]);
+    } else {
+      const int last = nmol - 1;
+      if (threadIdx.x < na && m != last) {
+        double p[3];
+        atom_xyz(E, last, threadIdx.x, p);
+        atom_store(E, m, threadIdx.x, p);
+      }
+    }
+    if (threadIdx.x == 0) {
+      C.nmol = insert ? nmol + 1 : nmol - 1;
+      C.nads = C.nmol * na;
+    }
+    __syncthreads();
+  }
+}
+
+/* CBMC reinsertion of a flexible chain (ReinsertionAdsorbateMove,
+ * src/mc_moves.c:4415): a new configuration grown with molecule m left out,
+ * the old one retraced; accepted with W(new) / W(old). */
+template <bool MIXED>
+__device__ __forceinline__ void step_reinsert_chain(Eng<MIXED> &E)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, nmol = C.nmol;
+  int m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
+  if (m >= nmol) m = nmol - 1;
+  grow_chain<MIXED>(E, false, 0, m, m);
+  if (C.fail) return;
+  if (threadIdx.x == 0) {
+    C.rosen_old = C.rosen;     /* the new configuration's weight, kept while the old one is retraced */
+    C.dl[0] = C.u[0];
+    C.dl[2] = C.u[2];
+    C.uintra_old = C.uintra;
+    for (int a = 0; a < na; a++)
+      for (int d = 0; d < 3; d++) C.cpn[a][d] = C.cp[a][d];
+  }
+  __syncthreads();
+  grow_chain<MIXED>(E, true, 1, m, m);
+  if (C.fail) return;
+  if (threadIdx.x == 0) {
+    const double w_new = C.rosen_old, w_old = C.rosen;
+    const double pacc = w_new / w_old;
+    if (!(pacc == pacc)) C.status |= RGPU_ERR_NONFINITE;
+    C.accept = E.rnd[SLOT_ACCEPT] < pacc;
+    if (C.accept) {
+      C.cnt[RGPU_CNT_REINS_ACCEPT]++;
+      C.energy[RGPU_E_HOST_VDW] += C.dl[0] - C.u[0];
+      C.energy[RGPU_E_ADS_VDW] += C.dl[2] - C.u[2];
+      C.energy[RGPU_E_INTRA] += C.uintra_old - C.uintra;
+    }
+  }
+  __syncthreads();
+  if (C.accept) {
+    if (threadIdx.x < na) atom_store(E, m, threadIdx.x, C.cpn[threadIdx.x]);
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Loads a descriptor copy into shared memory. */
 __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
 {
@@ -981,6 +1179,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
       for (int i = threadIdx.x; i < RGPU_RND / 2; i += blockDim.x) rgpu_uniform_pair(S.seed, S.sys_id, step, i, &rb[2 * i]);
       __syncthreads();
       E.rnd = rb;
+      E.step = step;
       const double u0 = rb[SLOT_MOVE];
       int mv = 0;
       while (mv < 5 && u0 >= S.cum[mv]) mv++;
@@ -995,26 +1194,34 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 2]++; }
         if (nmol >= S.maxmol) {
           if (threadIdx.x == 0) C.status |= RGPU_ERR_MAXMOL;
+        } else if (S.flexible) {
+          step_swap_chain<MIXED>(E, true, false);
         } else {
           step_swap<MIXED>(E, true);
         }
       } else if (mv == 3) {
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 3]++; }
-        if (nmol != 0) step_swap<MIXED>(E, false);
+        if (nmol != 0) {
+          if (S.flexible) step_swap_chain<MIXED>(E, false, false);
+          else step_swap<MIXED>(E, false);
+        }
       } else if (mv == 4) {
         /* the reference returns before counting when there is no molecule */
         if (nmol != 0) {
           if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_REINS_ATTEMPT]++; }
-          step_reinsert<MIXED>(E);
+          if (S.flexible) step_reinsert_chain<MIXED>(E);
+          else step_reinsert<MIXED>(E);
         }
       } else {
         if (threadIdx.x == 0) C.cnt[RGPU_CNT_MOVES]++;
-        step_swap<MIXED>(E, true, true);
+        if (S.flexible) step_swap_chain<MIXED>(E, true, true);
+        else step_swap<MIXED>(E, true, true);
       }
       /* ensemble sums after the step (thread 0 owns the running values) */
       if (threadIdx.x == 0 && step >= avg0) {
         const double n = (double)C.nmol;
-        const double u = C.energy[0] + C.energy[1] + C.energy[2] + C.energy[3] + C.energy[4] + C.energy[5];
+        const double u = C.energy[0] + C.energy[1] + C.energy[2] + C.energy[3] + C.energy[4] + C.energy[5] +
+                         C.energy[RGPU_E_INTRA];
         C.sums[RGPU_SUM_SAMPLES] += 1.0;
         C.sums[RGPU_SUM_N] += n;
         C.sums[RGPU_SUM_N2] += n * n;

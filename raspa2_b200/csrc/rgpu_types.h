@@ -47,7 +47,9 @@ enum {
 /* per-system running energies (internal units, FP64) */
 enum {
   RGPU_E_HOST_VDW = 0, RGPU_E_ADS_VDW = 1, RGPU_E_HOST_REAL = 2, RGPU_E_ADS_REAL = 3,
-  RGPU_E_HOST_FOURIER = 4, RGPU_E_ADS_FOURIER = 5, RGPU_NE = 8
+  RGPU_E_HOST_FOURIER = 4, RGPU_E_ADS_FOURIER = 5,
+  RGPU_E_INTRA = 6,      /* bend + torsion + intramolecular LJ of flexible molecules */
+  RGPU_NE = 8
 };
 
 /* status word bits */
@@ -140,6 +142,11 @@ typedef struct RgpuSys {
   uint64_t seed;
   uint32_t sys_id;
   int smem_fw;                /* framework staged in shared memory by the engine */
+  /* flexible linear chain (rgpu_system_desc), grown from atom 0 */
+  int flexible;
+  int pad_flex;
+  double bond, bend_k, bend_theta0, bend_sigma;   /* bend_sigma = 1 / sqrt(beta bend_k) */
+  double torsion[4], torsion_min;                 /* torsion_min: minimum of the torsion energy over phi */
   /* device pointers */
   const double4 *fw64;        /* [nfw] x, y, z, q (sorted by type) */
   const int4 *fw32;           /* [ntile*RGPU_TILE] tiled: fixed-point x, y, z (low 2 bits of z = segment), float bits of q */

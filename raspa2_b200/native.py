@@ -30,7 +30,7 @@ EXPORTS = [
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
-    "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex",
+    "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_intra_energy",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -49,6 +49,8 @@ class SystemDesc(C.Structure):
         ("max_rotation", C.c_double), ("fugacity_beta_v", C.c_double),
         ("ntrial_first", C.c_int), ("ntrial", C.c_int),
         ("seed", C.c_uint64), ("stream_id", C.c_uint32),
+        ("flexible", C.c_int), ("bond", C.c_double), ("bend_k", C.c_double), ("bend_theta0", C.c_double),
+        ("torsion", C.c_double * 4),
     ]
 
 
@@ -154,6 +156,13 @@ class GpuSystem:
         d.ntrial = sysm.trials
         d.seed = seed
         d.stream_id = stream_id
+        mol = sysm.molecule
+        if not mol.rigid:
+            d.flexible = 1
+            d.bond = mol.bond
+            d.bend_k = mol.bend_k * units.K_B
+            d.bend_theta0 = np.deg2rad(mol.bend_theta0)
+            d.torsion[:] = [t * units.K_B for t in mol.torsion]
         self.natom = d.natom
         self.maxmol = maxmol
         h = C.c_void_p()
@@ -229,6 +238,12 @@ class GpuSystem:
         out = np.zeros(6)
         _check(load().rgpu_total_energy(self.h, out.ctypes.data_as(_dp)))
         return out
+
+    def intra_energy(self) -> float:
+        """Intramolecular energy of flexible chains (rgpu_intra_energy)."""
+        out = C.c_double()
+        _check(load().rgpu_intra_energy(self.h, C.byref(out)))
+        return out.value
 
     def state(self):
         e = np.zeros(8)

@@ -44,11 +44,17 @@ TYPE_ORDER = list(PSEUDO_ATOMS.keys())
 
 @dataclasses.dataclass
 class Molecule:
-    """A rigid (or single-bead) adsorbate.
+    """An adsorbate: rigid (or single-bead), or a flexible linear chain.
 
-    `positions` is the reference geometry in Angstrom; `starting_bead` is the
-    bead placed first by CBMC (src/cbmc.c:623 `HandleFirstBead`), the others
-    are grown as one rigid group (src/cbmc.c:1480-1578).
+    Rigid: `positions` is the reference geometry in Angstrom; `starting_bead`
+    is the bead placed first by CBMC (src/cbmc.c:623 `HandleFirstBead`), the
+    others are grown as one rigid group (src/cbmc.c:1480-1578).
+
+    Flexible chain (rigid = False): atoms in chain order, grown from atom 0,
+    fixed bond length `bond`, harmonic bends 0.5 k (theta - theta0)^2
+    (`bend_k` in K/rad^2, `bend_theta0` in degrees) and TraPPE torsions
+    (`torsion`, four coefficients in K), LJ between atoms four or more bonds
+    apart; `positions` is then only a sample conformation.
     """
     name: str
     atom_types: List[str]
@@ -56,6 +62,10 @@ class Molecule:
     starting_bead: int = 0
     rigid: bool = True
     critical: tuple = (190.564, 4599200.0, 0.01142)
+    bond: float = 0.0
+    bend_k: float = 0.0
+    bend_theta0: float = 0.0
+    torsion: tuple = (0.0, 0.0, 0.0, 0.0)
 
     @property
     def n_atoms(self) -> int:
@@ -70,6 +80,19 @@ METHANE = Molecule("methane", ["CH4_sp3"], np.zeros((1, 3)), 0, True,
 CO2 = Molecule("CO2", ["O_co2", "C_co2", "O_co2"],
                np.array([[0.0, 0.0, 1.16], [0.0, 0.0, 0.0], [0.0, 0.0, -1.16]]),
                1, True, (304.1282, 7377300.0, 0.22394))
+
+
+def _zigzag(n: int, bond: float, theta_deg: float) -> np.ndarray:
+    """all-trans conformation of an n-bead chain"""
+    th = np.deg2rad(theta_deg)
+    dx, dy = bond * np.sin(th / 2.0), bond * np.cos(th / 2.0)
+    return np.array([[i * dx, (i % 2) * dy, 0.0] for i in range(n)])
+
+
+# united-atom n-hexane with TraPPE bends and torsions and 1.54 A bonds
+HEXANE = Molecule("hexane", ["CH3_sp3"] + ["CH2_sp3"] * 4 + ["CH3_sp3"], _zigzag(6, 1.54, 114.0), 0, False,
+                  (507.82, 3034000.0, 0.299), bond=1.54, bend_k=62500.0, bend_theta0=114.0,
+                  torsion=(0.0, 355.03, -68.19, 791.32))
 
 
 @dataclasses.dataclass
@@ -318,6 +341,27 @@ def methane_like_system(seed: int = 0, n_atoms: int = 288, temperature: float = 
         frac=frac, uc_types=types, uc_charges=np.zeros(n_atoms), molecule=METHANE,
         temperature=temperature, pressure=pressure, cutoff=12.0, ewald=False,
         moves=MoveMix(translation=1.0, rotation=0.0, swap_insert=0.5, swap_delete=0.5),
+        seed=seed)
+
+
+def hexane_system(seed: int = 4, n_atoms: int = 4096, cell: float = 40.0, temperature: float = 433.0,
+                  pressure: float = 1e5, name: Optional[str] = None) -> System:
+    """United-atom n-hexane (flexible chain, TraPPE bends and torsions, 1.54 A
+    bonds) in a neutral Si/O framework of `n_atoms` atoms in a cubic cell,
+    grown by CBMC with 8 first-bead trials and 16 trials per further bead;
+    translation, rotation, reinsertion and swap moves."""
+    rng = np.random.default_rng(seed)
+    c = np.array([cell, cell, cell], float)
+    pore = pore_radius(c, VOID_FRACTION, rng)
+    frac = _quantise_frac(poisson_disk(rng, n_atoms, c, 1.6, pore=pore))
+    n_si = n_atoms // 3
+    types = ["Sifw"] * n_si + ["Ofw"] * (n_atoms - n_si)
+    reps = np.array([2, 2, 2]) if cell < 24.0 else np.array([1, 1, 1])
+    return System(
+        name=name or f"hexane_s{seed}", unit_cell=c, unit_cells=reps, frac=frac, uc_types=types,
+        uc_charges=np.zeros(n_atoms), molecule=HEXANE, temperature=temperature, pressure=pressure,
+        cutoff=12.0, ewald=False, trials=16, trials_first_bead=8,
+        moves=MoveMix(translation=1.0, rotation=1.0, swap_insert=1.0, swap_delete=1.0, reinsertion=1.0),
         seed=seed)
 
 

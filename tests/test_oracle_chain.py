@@ -1,0 +1,28 @@
+"""The oracle's flexible-chain CBMC (CPU): bookkeeping of the
+intramolecular energy, fixed bond lengths, and the sampled bend-angle and
+torsion distributions of the grown chains."""
+import numpy as np
+
+from oracle import oracle as O
+from raspa2_b200 import systems, units
+
+
+def test_chain_growth_and_bookkeeping():
+    s = systems.hexane_system(seed=4, n_atoms=1200, cell=26.0, pressure=1e6)
+    o = O.Oracle.from_system(s, maxmol=64)
+    o.set_molecules(np.zeros((0, 6, 3)))
+    st = O.MCState()
+    o.mc_run(O.mc_params(s, 777, 3), st, 0, 3000)
+    assert o.nmol > 5
+    # running energies equal a recomputation
+    np.testing.assert_allclose(st.u_intra, o.intra_energy(), rtol=1e-9)
+    np.testing.assert_allclose(np.array(st.u)[:2], o.total_energy()[:2], rtol=1e-9)
+    x = o.molecules()
+    np.testing.assert_allclose(np.linalg.norm(np.diff(x, axis=1), axis=2), 1.54, atol=1e-9)
+    # bend angles spread about 114 degrees with the harmonic width
+    u = x[:, :-2] - x[:, 1:-1]
+    v = x[:, 2:] - x[:, 1:-1]
+    th = np.degrees(np.arccos(np.sum(u * v, -1) / np.linalg.norm(u, axis=-1) / np.linalg.norm(v, axis=-1)))
+    sigma = np.degrees(1.0 / np.sqrt(units.beta(s.temperature) * 62500.0 * units.K_B))
+    assert abs(th.mean() - 114.0) < 3.0 * sigma
+    assert 0.5 * sigma < th.std() < 2.0 * sigma
