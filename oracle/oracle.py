@@ -291,7 +291,7 @@ def mc_params(sysm, seed, system=0, max_translation=None, max_rotation=None):
     p.max_translation = sysm.max_translation if max_translation is None else max_translation
     p.max_rotation = np.deg2rad(sysm.max_rotation_deg) if max_rotation is None else max_rotation
     p.fugacity_beta_v = (units.beta(sysm.temperature) * units.pressure_to_internal(sysm.pressure)
-                         * sysm.volume)
+                         * sysm.volume / sysm.ideal_gas_rosenbluth)
     p.ntrial_first = sysm.trials_first_bead
     p.ntrial = sysm.trials
     p.seed = seed

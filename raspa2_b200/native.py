@@ -151,7 +151,7 @@ class GpuSystem:
         d.max_translation = sysm.max_translation if max_translation is None else max_translation
         d.max_rotation = (np.deg2rad(sysm.max_rotation_deg) if max_rotation is None else max_rotation)
         d.fugacity_beta_v = (units.beta(sysm.temperature) * units.pressure_to_internal(sysm.pressure)
-                             * sysm.volume)
+                             * sysm.volume / sysm.ideal_gas_rosenbluth)
         d.ntrial_first = sysm.trials_first_bead
         d.ntrial = sysm.trials
         d.seed = seed

@@ -80,10 +80,15 @@ def write_molecule(sys: System, path: str) -> None:
              "rigid" if (m.rigid or m.n_atoms == 1) else "flexible",
              "# number of atoms", f"{m.n_atoms}", "# atomic positions"]
     for i, (t, p) in enumerate(zip(m.atom_types, m.positions)):
-        if m.n_atoms == 1:
+        if m.n_atoms == 1 or not m.rigid:
             lines.append(f"{i} {t}")
         else:
             lines.append(f"{i} {t} {p[0]:.10f} {p[1]:.10f} {p[2]:.10f}")
+    if not m.rigid:
+        _flexible_chain_terms(m, lines)
+        with open(path, "w") as fh:
+            fh.write("\n".join(lines) + "\n")
+        return
     nbond = m.n_atoms - 1 if m.n_atoms > 1 else 0
     lines.append("# Chiral centers Bond  BondDipoles Bend  UrayBradley InvBend  Torsion Imp. "
                  "Torsion Bond/Bond Stretch/Bend Bend/Bend Stretch/Torsion Bend/Torsion "
@@ -99,6 +104,34 @@ def write_molecule(sys: System, path: str) -> None:
     lines += ["# Number of config moves", "0"]
     with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
+
+
+def _flexible_chain_terms(m, lines) -> None:
+    """Bonded terms of a linear chain: fixed bonds, harmonic bends, TraPPE
+    torsions, intramolecular LJ between atoms four or more bonds apart."""
+    n = m.n_atoms
+    bends = [(i, i + 1, i + 2) for i in range(n - 2)]
+    tors = [(i, i + 1, i + 2, i + 3) for i in range(n - 3)]
+    intra = [(i, j) for i in range(n) for j in range(i + 4, n)]
+    lines.append("# Chiral centers Bond  BondDipoles Bend  UrayBradley InvBend  Torsion Imp. "
+                 "Torsion Bond/Bond Stretch/Bend Bend/Bend Stretch/Torsion Bend/Torsion "
+                 "IntraVDW IntraCoulomb")
+    lines.append(f"               0    {n - 1}            0    {len(bends)}            0       0        {len(tors)}"
+                 "            0         0            0         0               0            0"
+                 f"        {len(intra)}            0")
+    lines.append("# Bond stretch: atom n1-n2, type, parameters")
+    for i in range(n - 1):
+        lines.append(f"{i} {i + 1} FIXED_BOND {m.bond}")
+    lines.append("# Bond bending: atom n1-n2-n3, type, parameters")
+    for a, b, c in bends:
+        lines.append(f"{a} {b} {c} HARMONIC_BEND {m.bend_k} {m.bend_theta0}")
+    lines.append("# Torsion n1-n2-n3-n4 type")
+    for a, b, c, d in tors:
+        lines.append(f"{a} {b} {c} {d} TRAPPE_DIHEDRAL " + " ".join(f"{x}" for x in m.torsion))
+    lines.append("# Intra VDW: atom n1-n2")
+    for i, j in intra:
+        lines.append(f"{i} {j}")
+    lines += ["# Number of config moves", "0"]
 
 
 def simulation_input(sys: System, cycles: int = 0, init_cycles: int = 0,
@@ -145,7 +178,7 @@ def simulation_input(sys: System, cycles: int = 0, init_cycles: int = 0,
         f"Component 0 MoleculeName             {sys.molecule.name}",
         "            MoleculeDefinition       Local",
         f"            StartingBead             {sys.molecule.starting_bead}",
-        "            IdealGasRosenbluthWeight 1.0",
+        f"            IdealGasRosenbluthWeight {sys.ideal_gas_rosenbluth}",
         "            FugacityCoefficient      1.0",
         f"            TranslationProbability   {mv.translation}",
     ]

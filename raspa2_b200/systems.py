@@ -38,6 +38,8 @@ PSEUDO_ATOMS = {
     "O_co2":    (79.0,   3.05,  -0.35,   15.9994),
     "CH3_sp3":  (98.0,   3.75,   0.0,    15.03452),
     "CH2_sp3":  (46.0,   3.95,   0.0,    14.02658),
+    # no interaction: the single atom of an otherwise empty box
+    "Dummy":    (0.0,    1.00,   0.0,    1.0),
 }
 TYPE_ORDER = list(PSEUDO_ATOMS.keys())
 
@@ -134,6 +136,10 @@ class System:
     seed: int = 0
     max_translation: float = 1.0
     max_rotation_deg: float = 30.0
+    # Rosenbluth weight of the molecule alone in an empty box (the
+    # reference's IdealGasRosenbluthWeight); insertion and deletion
+    # acceptance use W / ideal_gas_rosenbluth. 1 for rigid molecules.
+    ideal_gas_rosenbluth: float = 1.0
 
     # ----- derived quantities --------------------------------------------
     @property
@@ -363,6 +369,19 @@ def hexane_system(seed: int = 4, n_atoms: int = 4096, cell: float = 40.0, temper
         cutoff=12.0, ewald=False, trials=16, trials_first_bead=8,
         moves=MoveMix(translation=1.0, rotation=1.0, swap_insert=1.0, swap_delete=1.0, reinsertion=1.0),
         seed=seed)
+
+
+def empty_box_system(molecule: Molecule, temperature: float, cell: float = 30.0, trials: int = 16,
+                     trials_first_bead: int = 8) -> System:
+    """`molecule` alone in an empty cubic box (one non-interacting framework
+    atom), with Widom test insertions only: its average Rosenbluth weight is
+    the ideal-gas Rosenbluth weight of the molecule for this CBMC scheme."""
+    return System(
+        name=f"empty_{molecule.name}", unit_cell=np.array([cell, cell, cell]), unit_cells=np.array([1, 1, 1]),
+        frac=np.array([[0.5, 0.5, 0.5]]), uc_types=["Dummy"], uc_charges=np.zeros(1), molecule=molecule,
+        temperature=temperature, pressure=1e5, cutoff=12.0, ewald=False, trials=trials,
+        trials_first_bead=trials_first_bead,
+        moves=MoveMix(translation=0.0, rotation=0.0, swap_insert=0.0, swap_delete=0.0, widom=1.0), seed=0)
 
 
 def co2_system(seed: int = 1, n_atoms: int = 1536, cell: float = 25.8,

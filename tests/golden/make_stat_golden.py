@@ -41,8 +41,14 @@ CASES = {
     "methane_config0_1e5": (lambda: systems.methane_system(seed=0), dict(pressure=1e5, temperature=300.0), 1000, 8000),
     "methane_config0_1e7": (lambda: systems.methane_system(seed=0), dict(pressure=1e7, temperature=300.0), 1000, 3000),
     "co2_config1_1e5": (lambda: systems.co2_system(seed=1), dict(pressure=1e5, temperature=298.0), 4000, 4000),
+    # flexible chains: the reference runs with its own ideal-gas Rosenbluth
+    # weight, measured first by Widom insertions into an empty box
+    "hexane_small_3e4": (lambda: systems.hexane_system(seed=4, n_atoms=1200, cell=26.0),
+                         dict(pressure=3e4, temperature=433.0), 2000, 6000),
 }
+WIDOM_CYCLES = 20000
 SEEDS = 8
+IDEAL = {}
 
 
 def parse(path):
@@ -55,9 +61,28 @@ def parse(path):
     return {"loading": loading, "loading_err": loading_err, "enthalpy_K": h, "enthalpy_err_K": h_err}
 
 
+def reference_ideal_gas_rosenbluth(molecule, temperature, workdir):
+    """Average Widom Rosenbluth weight of the reference program for the
+    molecule alone in an empty box (its IdealGasRosenbluthWeight)."""
+    s = systems.empty_box_system(molecule, temperature)
+    d = os.path.join(workdir, f"widom_{molecule.name}_{temperature:g}")
+    raspa_io.write_inputs(s, d, cycles=WIDOM_CYCLES, init_cycles=0, print_every=10 ** 9, seed=4242)
+    r = subprocess.run([SIMULATE, "-i", "simulation.input"], cwd=d, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"simulate failed in {d}: {r.stderr[-500:]}")
+    out = os.path.join(d, "Output", "System_0")
+    txt = open(os.path.join(out, os.listdir(out)[0])).read()
+    m = re.search(r"Average Widom Rosenbluth-weight:\s+([-\d.eE+]+) \+/-\s+([-\d.eE+]+)", txt)
+    return float(m.group(1)), float(m.group(2))
+
+
 def run_case(name, workdir):
     build, state, init, prod = CASES[name]
     s = dataclasses.replace(build(), **state)
+    if not s.molecule.rigid:
+        w, w_err = reference_ideal_gas_rosenbluth(s.molecule, s.temperature, workdir)
+        s = dataclasses.replace(s, ideal_gas_rosenbluth=w)
+        IDEAL[name] = (w, w_err)
     dirs = []
     for k in range(SEEDS):
         d = os.path.join(workdir, f"{name}_{k}")
@@ -103,6 +128,8 @@ def main(argv):
             "enthalpy_mean_K": float(H.mean()), "enthalpy_se_K": float(H.std(ddof=1) / np.sqrt(len(H))),
             "source": "reference simulate (oracle/_ref) built from the reference sources",
         }
+        if name in IDEAL:
+            doc["ideal_gas_rosenbluth_reference"], doc["ideal_gas_rosenbluth_reference_err"] = IDEAL[name]
         with open(os.path.join(OUT, f"stat_{name}.json"), "w") as fh:
             json.dump(doc, fh, indent=1)
         print(name, doc["loading_mean"], "+-", doc["loading_se"], doc["enthalpy_mean_K"], "+-", doc["enthalpy_se_K"])

@@ -31,6 +31,7 @@ NSIGMA = 4.0
 CASES = {
     "methane_config0_1e5": (lambda: systems.methane_system(seed=0), 64, 20000, 80000, 128),
     "methane_config0_1e7": (lambda: systems.methane_system(seed=0), 64, 100000, 120000, 512),
+    "co2_config1_1e5": (lambda: systems.co2_system(seed=1), 64, 400000, 400000, 384),
 }
 
 
