@@ -23,6 +23,7 @@ on all host cores.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import re
@@ -68,6 +69,10 @@ def parse_args():
     p.add_argument("--ref-cycles", type=int, default=10)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--hexane-systems", type=int, default=64,
+                   help="systems of the grid-accelerated hexane workload (0 = skip)")
+    p.add_argument("--hexane-moves", type=int, default=1000, help="moves per system per timed hexane step")
+    p.add_argument("--hexane-spacing", type=float, default=0.1, help="energy-grid spacing of the hexane workload [A]")
     p.add_argument("--serve-jobs", type=int, default=300, help="jobs of the served Poisson stream (0 = skip)")
     p.add_argument("--serve-rate", type=float, default=200.0, help="mean arrivals per second")
     return p.parse_args()
@@ -366,6 +371,8 @@ def run_ours(args):
         line["plain_gpu"] = plain_gpu_rate(native, stream)
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         line["serving"] = serving_run(args)
+    if rank == 0 and world == 1 and args.hexane_systems > 0:
+        line["hexane_grid"] = hexane_grid_run(args, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_SIMULATE):
         cores = min(cpu_cores(), len(sys_list))
         tmp = tempfile.mkdtemp(prefix="raspa_ref_")
@@ -399,6 +406,88 @@ def serving_run(args):
                "slots": srv.max_slots, "mem_budget_gb": srv.mem_budget / 1e9,
                "status_nonzero_jobs": int(sum(1 for j in jobs if j.result["status"]))})
     return st
+
+
+def hexane_grid_run(args, stream, steps=3, warmup=3):
+    """Grid-accelerated CBMC of united-atom n-hexane: one 4096-atom neutral
+    framework in a cubic 40 A cell at 64 pressures (1e2-1e6 Pa, T = 433 K),
+    one system per pressure, all sharing the two bead-type energy grids
+    (0.1 A: 401^3 points x 8 FP32 values = 2.06 GB each), mixed precision,
+    8 first-bead x 16 trials. Device-timed moves/s, then the running host VDW
+    energy of every system against direct FP64 pair sums of its final
+    configuration."""
+    import torch
+    from raspa2_b200 import native
+    base = systems.hexane_system(seed=4, n_atoms=4096, cell=40.0, temperature=433.0)
+    pressures = np.logspace(2, 6, args.hexane_systems)
+    sl = [dataclasses.replace(base, pressure=float(p)) for p in pressures]
+    gs = [native.GpuSystem(s, maxmol=256, seed=9000, stream_id=i) for i, s in enumerate(sl)]
+    t0 = time.perf_counter()
+    geom = gs[0].use_energy_grids(args.hexane_spacing)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    for g in gs[1:]:
+        g.use_energy_grids(args.hexane_spacing, like=gs[0])
+    for g in gs:
+        g.set_adsorbates(np.zeros((0, 6, 3)))
+    from raspa2_b200 import autotune
+    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=512, cluster=1)
+    for _ in range(warmup):
+        e.run(args.hexane_moves, stream.cuda_stream)
+    e.sync()
+    tuned = autotune.tune(gs, precision=native.RGPU_MIXED)
+    e.close()
+    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=tuned.threads, cluster=tuned.cluster)
+    e.run(args.hexane_moves, stream.cuda_stream)
+    e.sync()
+    c0 = np.array([g.state()["counters"] for g in gs])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=stream.device)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            e.run(args.hexane_moves, stream.cuda_stream)
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in evs) / 1e3
+    d = (np.array([g.state()["counters"] for g in gs]) - c0).sum(axis=0)
+    moves = float(d[8])
+    # bead positions looked up per move type: translation/rotation 6 new + 6
+    # old, insertion/deletion 8 first-bead + 5 x 16 trials, reinsertion both
+    lookups = 12.0 * (d[0] + d[1]) + 88.0 * (d[2] + d[3]) + 176.0 * d[18]
+    # direct FP64 pair sums of every final configuration against the running
+    # host VDW energy (grids switched off for the recomputation)
+    kT = 433.0 * units.K_B
+    errs, rel = [], []
+    for g in gs:
+        st = g.state()
+        g.set_grids(None, None, None, None, None)
+        direct = g.total_energy()[0]
+        g.use_energy_grids(args.hexane_spacing, like=gs[0])
+        if st["nmol"] == 0:
+            continue
+        errs.append(abs(st["energy"][0] - direct) / st["nmol"] / kT)
+        rel.append(abs(st["energy"][0] - direct) / abs(direct))
+    loads = [g.state()["nmol"] for g in gs]
+    e.close()
+    out = {"workload": "hexane_grid_cbmc_64 (4096-atom 40 A framework, 64 pressures 1e2-1e6 Pa, 433 K)",
+           "systems": len(gs), "moves_per_step_per_system": args.hexane_moves, "steps": steps,
+           "moves_per_s": moves / t, "ms_per_step": 1000.0 * t / steps,
+           "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads},
+           "grid": {"spacing_A": args.hexane_spacing, "points_per_axis": [int(x) + 1 for x in geom[0]],
+                    "bytes_per_grid": int(np.prod(geom[0].astype(np.int64) + 1) * 32), "types": 2,
+                    "build_s": t_build},
+           "grid_lookups_per_s_est": lookups / t,
+           "grid_bytes_per_s_est": 256.0 * lookups / t,
+           "loading_molecules": {"min": int(min(loads)), "max": int(max(loads)), "mean": float(np.mean(loads))},
+           "host_vdw_vs_direct_fp64": {"systems_compared": len(errs), "max_abs_per_molecule_kT": float(max(errs)),
+                                       "median_rel": float(np.median(rel)), "max_rel": float(max(rel))},
+           "acceptance": {k: (float(d[4 + i]) / max(float(d[i]), 1.0)) for i, k in
+                          enumerate(["translation", "rotation", "insertion", "deletion"])},
+           "reinsertion_acceptance": float(d[19]) / max(float(d[18]), 1.0)}
+    del flush
+    return out
 
 
 def plain_gpu_rate(native, stream, nsteps=2000):

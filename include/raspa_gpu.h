@@ -158,9 +158,12 @@ int rgpu_intra_energy(rgpu_system *sys, double *out);
 /* ---- energy grids (src/grids.c) ----------------------------------------- */
 /* MakeGrid (src/grids.c:431-690) for pseudo-atom `type`: (n+1)^3 points
  * i*size/n + shift per axis, 8 FP32 values per point (value, 3 first, 3 mixed
- * second, 1 third derivative, scaled to the unit cell of the grid), layout
- * grid[8][nx+1][ny+1][nz+1] (the plane order of the reference's grid file,
- * src/grids.c:734-738). d_grid is device memory of that size. */
+ * second, 1 third derivative, scaled to the unit cell of the grid), stored
+ * point-major: grid[((i*(ny+1) + j)*(nz+1) + k)*8 + m], so that a lookup
+ * reads each corner's 8 values as two 16-byte loads. The reference's grid
+ * file holds the same values plane by plane (src/grids.c:734-738): plane m
+ * is grid[...*8 + m]. d_grid is 16-byte aligned device memory of
+ * (nx+1)(ny+1)(nz+1)*8 floats. */
 int rgpu_grid_build(rgpu_system *sys, int type, const int npts[3], const double size[3],
                     const double shift[3], float *d_grid);
 /* InterpolateVDWGrid (src/grids.c:979-1077) at n points (host arrays),
@@ -183,6 +186,18 @@ int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double s
 int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const double size[3],
                                   const double shift[3], const double cell[3], int n, const double *xyz,
                                   double *out);
+
+/* Uses energy grids in the engine: the host VDW energy of molecule atom a
+ * becomes the tricubic lookup in d_grids[a] (a grid of rgpu_grid_build for
+ * that atom's pseudo-atom type; atoms of one type can share a grid) instead
+ * of the pair sum over the framework, as the reference does with
+ * UseTabularGrid (src/grids.c:979, called from src/framework_energy.c).
+ * npts/size/shift/cell as rgpu_grid_interpolate; the molecule must be
+ * uncharged. d_grids = NULL switches the grids off. Takes effect for
+ * engines created afterwards; rgpu_bead_energies and rgpu_total_energy
+ * keep the direct pair sums. */
+int rgpu_system_set_grids(rgpu_system *sys, const float *const *d_grids, const int npts[3], const double size[3],
+                          const double shift[3], const double cell[3]);
 
 /* ---- persistent batched engine ------------------------------------------ */
 /* Groups systems for one persistent launch; each system is advanced by one
@@ -237,6 +252,25 @@ int rgpu_system_set_limits(rgpu_system *sys, unsigned long long end_step, unsign
  * every Widom step, whatever the step window. */
 int rgpu_system_averages(rgpu_system *sys, double *sums8);
 int rgpu_system_reset_averages(rgpu_system *sys);
+
+/* ---- checkpoints (binary crash files) ------------------------------------ */
+/* The counterpart of the binary crash file that ContinueAfterCrash writes
+ * and reads (WriteBinaryRestartFiles, src/output.c:7903;
+ * ReadBinaryRestartFiles, src/input.c:9378): a system's whole mutable state
+ * as one host buffer. It holds the molecule positions (FP64), the stored
+ * adsorbate structure factor S_ads(k) as updated move by move (FP64), the
+ * running energies, counters, ensemble sums, step window and status word.
+ * The random stream is keyed by step, and the step is saved, so a system
+ * created from the same descriptor (same seed and stream id) and restored
+ * from a checkpoint continues the saved trajectory move for move. Restoring
+ * into a system of another temperature, pressure, move mix or stream is
+ * allowed; another box, framework, force field, molecule or Ewald set-up is
+ * refused (RGPU_E_INVALID). Energy grids are part of the descriptor, not of
+ * the state: set them on the restoring system. The buffer is host memory of
+ * rgpu_system_checkpoint_size bytes (it grows with the molecule count). */
+int rgpu_system_checkpoint_size(rgpu_system *sys, size_t *bytes);
+int rgpu_system_checkpoint(rgpu_system *sys, void *buf, size_t bytes);
+int rgpu_system_restore(rgpu_system *sys, const void *buf, size_t bytes);
 
 /* ---- measurement -------------------------------------------------------- */
 /* FP32 FMA throughput of the current device in TFLOP/s (FMA = 2 FLOP), the

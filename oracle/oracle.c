@@ -45,16 +45,26 @@ double or_real_ewald(const or_sys *s, double qa, double qb, double r)
   return s->coulomb * qa * qb * (erfc(s->alpha * r) / r);
 }
 
+/* the framework VDW energy of a type-`type` bead at p from its energy grid;
+ * returns 0 (and leaves *e) when that type has none */
+static int grid_vdw(const or_sys *s, int type, const double *p, double *e)
+{
+  if (!s->grid || !s->grid[type]) return 0;
+  *e = or_grid_interpolate(s->grid[type], s->grid_npts, s->grid_size, s->grid_shift, s->grid_cell, p);
+  return 1;
+}
+
 /* ---------------------------------------------------------------------- */
 void or_point_energy(const or_sys *s, int type, double q, const double *p, int exclude,
                      double *out)
 {
   double d[3];
   double uv = 0.0, uc = 0.0, av = 0.0, ac = 0.0;
-  /* framework VDW: src/framework_energy.c:151-170; charge: :258-279 */
+  /* framework VDW: src/framework_energy.c:151-170 (grid: :60-75); charge: :258-279 */
+  const int gv = grid_vdw(s, type, p, &uv);
   for (int i = 0; i < s->nfw; i++) {
     double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
-    if (r2 < s->rc2_vdw) uv += or_lj(s, type, s->fw_type[i], r2);
+    if (!gv && r2 < s->rc2_vdw) uv += or_lj(s, type, s->fw_type[i], r2);
     if (s->ewald && q != 0.0 && r2 < s->rc2_cc) uc += or_real_ewald(s, q, s->fw_q[i], sqrt(r2));
   }
   /* other adsorbates: src/inter_energy.c:365-388, :455-480 */
@@ -149,6 +159,12 @@ int or_move_delta(const or_sys *s, int m, const double *new_xyz, double *out)
   /* framework VDW */
   for (int a = 0; a < s->natom; a++) {
     int ta = s->mol_type[a];
+    double e;
+    if (grid_vdw(s, ta, new_xyz + 3 * a, &e)) {
+      if (e >= s->overlap) return 1;
+      dhv += e;
+      continue;
+    }
     for (int i = 0; i < s->nfw; i++) {
       double r2 = dist2(s, new_xyz + 3 * a, s->fw_xyz + 3 * i, d);
       if (r2 < s->rc2_vdw) {
@@ -160,6 +176,11 @@ int or_move_delta(const or_sys *s, int m, const double *new_xyz, double *out)
   }
   for (int a = 0; a < s->natom; a++) {
     int ta = s->mol_type[a];
+    double e;
+    if (grid_vdw(s, ta, old_xyz + 3 * a, &e)) {
+      dhv -= e;
+      continue;
+    }
     for (int i = 0; i < s->nfw; i++) {
       double r2 = dist2(s, old_xyz + 3 * a, s->fw_xyz + 3 * i, d);
       if (r2 < s->rc2_vdw) dhv -= or_lj(s, ta, s->fw_type[i], r2);
@@ -381,9 +402,12 @@ void or_total_energy(const or_sys *s, double *out)
       const double *p = s->ads_xyz + 3 * (m * s->natom + a);
       int ta = s->mol_type[a];
       double qa = s->mol_q[a];
+      double g;
+      const int gv = grid_vdw(s, ta, p, &g);
+      if (gv) hv += g;
       for (int i = 0; i < s->nfw; i++) {
         double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
-        if (r2 < s->rc2_vdw) hv += or_lj(s, ta, s->fw_type[i], r2);
+        if (!gv && r2 < s->rc2_vdw) hv += or_lj(s, ta, s->fw_type[i], r2);
         if (s->ewald && qa != 0.0 && r2 < s->rc2_cc) hc += or_real_ewald(s, qa, s->fw_q[i], sqrt(r2));
       }
       for (int j = m + 1; j < s->nmol; j++)
@@ -1018,7 +1042,10 @@ double or_grid_interpolate(const float *grid, const int npts[3], const double si
   int i0[3];
   for (int c = 0; c < 3; c++) {
     sc[c] = ((p[c] - shift[c]) / size[c]) * (double)npts[c];
+    /* a point on the upper face (p == cell) uses the last cell at r = 1 */
     i0[c] = (int)sc[c];
+    if (i0[c] > npts[c] - 1) i0[c] = npts[c] - 1;
+    if (i0[c] < 0) i0[c] = 0;
     r[c] = sc[c] - i0[c];
   }
   /* cap, src/grids.c:1058-1060 */

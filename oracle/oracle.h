@@ -53,6 +53,12 @@ typedef struct {
   int flexible;
   double bond, bend_k, bend_theta0, bend_sigma;
   double torsion[4], torsion_min;
+  /* energy grids (UseTabularGrid, src/framework_energy.c): grid[t] != NULL
+   * replaces the framework VDW pair sum of pseudo-atom type t by the lookup
+   * or_grid_interpolate in that grid (plane-major, as or_grid_build writes) */
+  const float *const *grid;             /* [ntypes] or NULL */
+  int grid_npts[3];
+  double grid_size[3], grid_shift[3], grid_cell[3];
 } or_sys;
 
 /* pair terms */

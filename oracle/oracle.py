@@ -31,6 +31,8 @@ class OrSys(C.Structure):
         ("uion", C.c_double), ("net_fw", C.c_double), ("net_ads", C.c_double),
         ("flexible", C.c_int), ("bond", C.c_double), ("bend_k", C.c_double), ("bend_theta0", C.c_double),
         ("bend_sigma", C.c_double), ("torsion", C.c_double * 4), ("torsion_min", C.c_double),
+        ("grid", C.POINTER(C.POINTER(C.c_float))), ("grid_npts", C.c_int * 3), ("grid_size", C.c_double * 3),
+        ("grid_shift", C.c_double * 3), ("grid_cell", C.c_double * 3),
     ]
 
 
@@ -164,6 +166,25 @@ class Oracle:
 
     def intra_energy(self):
         return lib().or_intra_energy(C.byref(self.s))
+
+    def set_grids(self, grids, npts, size, shift, cell):
+        """grids: {pseudo-atom type: plane-major grid (8, nx+1, ny+1, nz+1)}
+        whose lookups replace that type's framework VDW pair sums; None
+        switches them off."""
+        if grids is None:
+            self.s.grid = None
+            self._grids = None
+            return
+        keepg = {t: np.ascontiguousarray(g, np.float32) for t, g in grids.items()}
+        tab = (C.POINTER(C.c_float) * self.s.ntypes)()
+        for t, g in keepg.items():
+            tab[t] = g.ctypes.data_as(C.POINTER(C.c_float))
+        self._grids = (keepg, tab)
+        self.s.grid = C.cast(tab, C.POINTER(C.POINTER(C.c_float)))
+        self.s.grid_npts[:] = [int(x) for x in npts]
+        self.s.grid_size[:] = [float(x) for x in size]
+        self.s.grid_shift[:] = [float(x) for x in shift]
+        self.s.grid_cell[:] = [float(x) for x in cell]
 
     # ---- state -------------------------------------------------------------
     @property

@@ -41,7 +41,7 @@ def _signature(systems: Sequence["native.GpuSystem"], precision: int) -> tuple:
     sig = []
     for g in systems:
         fw = g.sysm.framework()[0]
-        sig.append((len(fw), g.natom, tuple(g.sysm.kmax), g.maxmol))
+        sig.append((len(fw), g.natom, tuple(g.sysm.kmax), g.maxmol, bool(getattr(g, "grids_active", False))))
     return (precision, tuple(sorted(sig)))
 
 
@@ -61,6 +61,8 @@ def candidates(nsys: int, precision: int, sms: int) -> List[Tuple[int, int]]:
 
 def _clone(g: "native.GpuSystem", xyz: np.ndarray) -> "native.GpuSystem":
     c = native.GpuSystem(g.sysm, **g.init_args)
+    if getattr(g, "grids_active", False):
+        c.share_grids_of(g)
     c.set_adsorbates(xyz)
     return c
 

@@ -86,6 +86,7 @@ struct rgpu_system {
   int records_stale;          /* device records must be rebuilt from ads_xyz */
   double net_ads, pending_dq;
   int grid_type_seg;
+  uint64_t fingerprint;       /* of the model a checkpoint must match (checkpoint_fingerprint) */
   std::vector<int> fw_seg_type; /* framework pseudo-atom type of each segment */
   std::vector<double> lj_eps, lj_sig2, lj_shift;
   int ntypes;
@@ -166,6 +167,52 @@ static int refresh_from_device(rgpu_system *s)
   return upload_records(s);
 }
 
+/* FNV-1a over the parts of a descriptor that a saved state depends on: the
+ * box, the framework, the force field, the molecule and the Ewald set-up.
+ * Temperature, pressure, move mix and random stream may differ between the
+ * system that saved a checkpoint and the one restoring it. */
+static uint64_t fnv1a(uint64_t h, const void *p, size_t n)
+{
+  const unsigned char *b = (const unsigned char *)p;
+  for (size_t i = 0; i < n; i++) {
+    h ^= b[i];
+    h *= 1099511628211ULL;
+  }
+  return h;
+}
+
+static uint64_t checkpoint_fingerprint(const rgpu_system_desc *d)
+{
+  uint64_t h = 1469598103934665603ULL;
+  h = fnv1a(h, d->box, sizeof d->box);
+  h = fnv1a(h, &d->cutoff, sizeof d->cutoff);
+  h = fnv1a(h, &d->nfw, sizeof d->nfw);
+  h = fnv1a(h, d->fw_xyz, sizeof(double) * 3 * d->nfw);
+  h = fnv1a(h, d->fw_type, sizeof(int) * d->nfw);
+  h = fnv1a(h, d->fw_q, sizeof(double) * d->nfw);
+  h = fnv1a(h, &d->ntypes, sizeof d->ntypes);
+  h = fnv1a(h, d->eps, sizeof(double) * d->ntypes * d->ntypes);
+  h = fnv1a(h, d->sig2, sizeof(double) * d->ntypes * d->ntypes);
+  h = fnv1a(h, d->shift, sizeof(double) * d->ntypes * d->ntypes);
+  h = fnv1a(h, &d->natom, sizeof d->natom);
+  h = fnv1a(h, d->mol_type, sizeof(int) * d->natom);
+  h = fnv1a(h, d->mol_q, sizeof(double) * d->natom);
+  h = fnv1a(h, d->mol_ref, sizeof(double) * 3 * d->natom);
+  h = fnv1a(h, &d->ewald, sizeof d->ewald);
+  if (d->ewald) {
+    h = fnv1a(h, &d->alpha, sizeof d->alpha);
+    h = fnv1a(h, d->kmax, sizeof d->kmax);
+  }
+  h = fnv1a(h, &d->flexible, sizeof d->flexible);
+  if (d->flexible) {
+    h = fnv1a(h, &d->bond, sizeof d->bond);
+    h = fnv1a(h, &d->bend_k, sizeof d->bend_k);
+    h = fnv1a(h, &d->bend_theta0, sizeof d->bend_theta0);
+    h = fnv1a(h, d->torsion, sizeof d->torsion);
+  }
+  return h;
+}
+
 extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
 {
   if (!out || !d) return fail(RGPU_E_INVALID, "null argument");
@@ -201,6 +248,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     if (d->mol_type[a] < 0 || d->mol_type[a] >= d->ntypes) return fail(RGPU_E_INVALID, "molecule type");
 
   rgpu_system *s = new rgpu_system();
+  s->fingerprint = checkpoint_fingerprint(d);
   memset(&s->h, 0, sizeof(RgpuSys));
   memset(&s->h_state, 0, sizeof(RgpuState));
   s->h_state.step[1] = ~0ULL;   /* no step limit */
@@ -806,6 +854,39 @@ extern "C" int rgpu_ewald_accept(rgpu_system *s)
   return RGPU_SUCCESS;
 }
 
+static bool grid_covers_cell(const int npts[3], const double size[3], const double shift[3], const double cell[3]);
+
+extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids, const int npts[3],
+                                     const double size[3], const double shift[3], const double cell[3])
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  RgpuSys &h = s->h;
+  if (!d_grids) {
+    h.use_grid = 0;
+    for (int a = 0; a < RGPU_MAX_ATOMS; a++) h.grid[a] = nullptr;
+  } else {
+    if (!npts || !size || !shift || !cell) return fail(RGPU_E_INVALID, "bad argument");
+    if (h.mol_charged)
+      return fail(RGPU_E_INVALID, "grids replace the host VDW pair sums only: the molecule must be uncharged");
+    if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
+    for (int a = 0; a < h.natom; a++) {
+      if (!d_grids[a]) return fail(RGPU_E_INVALID, "no grid for molecule atom %d", a);
+      if ((uintptr_t)d_grids[a] % 16) return fail(RGPU_E_INVALID, "grids must be 16-byte aligned");
+      h.grid[a] = d_grids[a];
+    }
+    for (int c = 0; c < 3; c++) {
+      h.grid_geom.npts[c] = npts[c];
+      h.grid_geom.size[c] = size[c];
+      h.grid_geom.shift[c] = shift[c];
+      h.grid_geom.cell[c] = cell[c];
+    }
+    h.use_grid = 1;
+  }
+  CK(cudaMemcpyAsync(s->d_sys, &h, sizeof(RgpuSys), cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
 extern "C" int rgpu_intra_energy(rgpu_system *s, double *out)
 {
   if (!s || !out) return fail(RGPU_E_INVALID, "bad argument");
@@ -1037,10 +1118,12 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->kw = 1;
   e->max_ads = 0;
   int maxfw = 0, maxtile = 0, maxk = 0;
+  bool all_grids = true;
   for (int i = 0; i < n; i++) {
     rgpu_system *s = systems[i];
     if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
     e->sys.push_back(s);
+    all_grids = all_grids && s->h.use_grid;
     e->kw = std::max(e->kw, s->kw);
     e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
     maxfw = std::max(maxfw, (s->d.nfw + e->cluster - 1) / e->cluster);
@@ -1063,6 +1146,11 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   } else {
     e->tile_items = 0;
     e->fw_items = maxfw;
+  }
+  if (all_grids) {
+    /* no framework pairs are evaluated: nothing of the framework to stage */
+    e->tile_items = 0;
+    e->fw_items = 0;
   }
   /* shared-memory staging, in order of preference: framework share and wave
    * vectors, framework only, wave vectors only, neither */
@@ -1180,6 +1268,98 @@ extern "C" int rgpu_system_state(rgpu_system *s, double *energy8, long long *cou
   if (nmol) *nmol = s->h_state.nmol;
   if (status) *status = s->h_state.status;
   if (step) *step = s->h_state.step[0];
+  return RGPU_SUCCESS;
+}
+
+/* ---- checkpoints ---------------------------------------------------------- */
+namespace {
+struct CheckpointHeader {
+  char magic[8];              /* "RGPUCKP1" */
+  uint64_t fingerprint;
+  int32_t natom, nk, nmol, pad;
+  double net_ads, pending_dq;
+};
+const char CKPT_MAGIC[8] = {'R', 'G', 'P', 'U', 'C', 'K', 'P', '1'};
+}
+
+static size_t checkpoint_bytes(const rgpu_system *s, int nmol)
+{
+  return sizeof(CheckpointHeader) + sizeof(RgpuState) + sizeof(double) * 3 * (size_t)nmol * s->d.natom +
+         sizeof(double2) * (size_t)s->h.nk;
+}
+
+extern "C" int rgpu_system_checkpoint_size(rgpu_system *s, size_t *bytes)
+{
+  if (!s || !bytes) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaDeviceSynchronize());
+  int n = 0;
+  CK(cudaMemcpy(&n, s->nmol, sizeof(int), cudaMemcpyDeviceToHost));
+  *bytes = checkpoint_bytes(s, n);
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_checkpoint(rgpu_system *s, void *buf, size_t bytes)
+{
+  if (!s || !buf) return fail(RGPU_E_INVALID, "bad argument");
+  CK(cudaDeviceSynchronize());
+  RgpuState st;
+  CK(cudaMemcpy(&st, s->state, sizeof(RgpuState), cudaMemcpyDeviceToHost));
+  const size_t need = checkpoint_bytes(s, st.nmol);
+  if (bytes < need) return fail(RGPU_E_CAPACITY, "checkpoint needs %zu bytes, %zu given", need, bytes);
+  int rc = refresh_from_device(s);
+  if (rc) return rc;
+  char *p = (char *)buf;
+  CheckpointHeader hd;
+  memset(&hd, 0, sizeof hd);
+  memcpy(hd.magic, CKPT_MAGIC, 8);
+  hd.fingerprint = s->fingerprint;
+  hd.natom = s->d.natom;
+  hd.nk = s->h.nk;
+  hd.nmol = st.nmol;
+  hd.net_ads = s->net_ads;
+  hd.pending_dq = s->pending_dq;
+  memcpy(p, &hd, sizeof hd);
+  p += sizeof hd;
+  memcpy(p, &st, sizeof st);
+  p += sizeof st;
+  const size_t nx = (size_t)st.nmol * s->d.natom * 3;
+  if (nx) CK(cudaMemcpy(p, s->ads_xyz, sizeof(double) * nx, cudaMemcpyDeviceToHost));
+  p += sizeof(double) * nx;
+  if (s->h.nk) CK(cudaMemcpy(p, s->sk_ads, sizeof(double2) * s->h.nk, cudaMemcpyDeviceToHost));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_restore(rgpu_system *s, const void *buf, size_t bytes)
+{
+  if (!s || !buf || bytes < sizeof(CheckpointHeader) + sizeof(RgpuState)) return fail(RGPU_E_INVALID, "bad argument");
+  const char *p = (const char *)buf;
+  CheckpointHeader hd;
+  memcpy(&hd, p, sizeof hd);
+  p += sizeof hd;
+  if (memcmp(hd.magic, CKPT_MAGIC, 8)) return fail(RGPU_E_INVALID, "not a checkpoint");
+  if (hd.fingerprint != s->fingerprint || hd.natom != s->d.natom || hd.nk != s->h.nk)
+    return fail(RGPU_E_INVALID, "checkpoint of another framework, molecule or force field");
+  if (hd.nmol < 0 || hd.nmol > s->d.maxmol) return fail(RGPU_E_CAPACITY, "checkpoint holds %d molecules, maxmol %d",
+                                                        hd.nmol, s->d.maxmol);
+  if (bytes != checkpoint_bytes(s, hd.nmol)) return fail(RGPU_E_INVALID, "checkpoint size %zu", bytes);
+  RgpuState st;
+  memcpy(&st, p, sizeof st);
+  p += sizeof st;
+  if (st.nmol != hd.nmol) return fail(RGPU_E_INVALID, "checkpoint inconsistent");
+  CK(cudaDeviceSynchronize());
+  const size_t nx = (size_t)hd.nmol * s->d.natom * 3;
+  s->h_xyz.assign((const double *)p, (const double *)p + nx);
+  p += sizeof(double) * nx;
+  s->h_nmol = hd.nmol;
+  s->net_ads = hd.net_ads;
+  s->pending_dq = hd.pending_dq;
+  s->h_state = st;
+  if (nx) CK(cudaMemcpy(s->ads_xyz, s->h_xyz.data(), sizeof(double) * nx, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->state, &st, sizeof st, cudaMemcpyHostToDevice));
+  if (s->h.nk) CK(cudaMemcpy(s->sk_ads, p, sizeof(double2) * s->h.nk, cudaMemcpyHostToDevice));
+  int rc = upload_records(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->st));
   return RGPU_SUCCESS;
 }
 

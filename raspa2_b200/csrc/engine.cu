@@ -25,6 +25,7 @@
 #include "rgpu_chain.h"
 #include "rgpu_device.cuh"
 #include "rgpu_engine.h"
+#include "rgpu_grid.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -218,6 +219,14 @@ __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 
 /* Pair evaluation of P positions on this CTA's share, then one cluster
  * barrier; the totals are read with gather(). All threads call. */
+/* Host VDW of one bead from its type's energy grid, out of line so that the
+ * lookup's registers stay out of the evaluation loop's allocation. */
+__device__ __noinline__ double engine_grid_value(const RgpuSys *S, int atom, double x, double y, double z)
+{
+  const double p[3] = {x, y, z};
+  return rgpu_grid_value(S->grid[atom], S->grid_geom, p);
+}
+
 template <bool MIXED>
 __device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
 {
@@ -237,6 +246,12 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check
       if (c < pl.cf) { hv += E.uv[u]; hc += E.uc[u]; }
       else { av += E.uv[u]; ac += E.uc[u]; }
       ov |= E.uo[u];
+    }
+    if (E.S->use_grid && E.rank == 0) {
+      /* host VDW from the bead type's energy grid (one CTA of the cluster) */
+      const double g = engine_grid_value(E.S, E.pos[p].atom, E.pos[p].x, E.pos[p].y, E.pos[p].z);
+      hv += g;
+      ov |= g >= E.S->overlap;
     }
     ps[p].v[0] = hv; ps[p].v[1] = hc; ps[p].v[2] = av; ps[p].v[3] = ac;
     ps[p].ov = ov;
@@ -1134,6 +1149,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
       }
     }
     E.sl.ads = E.ads;
+    if (S.use_grid) E.sl.fw_hi = E.sl.fw_lo;   /* host VDW from the grids: no framework pairs */
     /* this CTA's wave vectors with their prefactors and S(k) */
     if (S.ewald) share(S.nk, rank, csize, E.k0, E.k1);
     else { E.k0 = 0; E.k1 = 0; }

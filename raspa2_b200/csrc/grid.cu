@@ -23,6 +23,7 @@
 
 #include "rgpu_device.cuh"
 #include "rgpu_engine.h"
+#include "rgpu_grid.cuh"
 
 #define GRID_TX 4
 #define GRID_TY 8
@@ -164,76 +165,19 @@ cudaError_t rgpu_grid_build_launch_lj(const RgpuSys *d_sys, const RgpuLJ *lj, co
   return cudaGetLastError();
 }
 
-/* Cubic Hermite basis on [0,1]: {p0, p1, slope0, slope1} */
-__device__ __forceinline__ void hermite(double t, double *h)
-{
-  const double t2 = t * t, t3 = t2 * t;
-  h[0] = 1.0 - 3.0 * t2 + 2.0 * t3;
-  h[1] = 3.0 * t2 - 2.0 * t3;
-  h[2] = t - 2.0 * t2 + t3;
-  h[3] = -t2 + t3;
-}
-
-struct InterpParams {
-  int npts[3];
-  double size[3], shift[3], cell[3];
-};
-
-__global__ void k_grid_interp(const float *grid, InterpParams ip, int n, const double *xyz, double *out)
+__global__ void k_grid_interp(const float *grid, RgpuGridGeom ip, int n, const double *xyz, double *out)
 {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
-  const int ny = ip.npts[1] + 1, nz = ip.npts[2] + 1;
-  double r[3];
-  int i0[3];
-  for (int c = 0; c < 3; c++) {
-    double p = xyz[3 * q + c];
-    p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
-    if (p < 0.0) p += ip.cell[c];
-    const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
-    /* a point on the upper cell face (p == cell after wrapping) uses the last
-     * grid cell at r = 1, so the 2x2x2 corner block stays inside the grid */
-    i0[c] = min(max((int)s, 0), ip.npts[c] - 1);
-    r[c] = s - i0[c];
-  }
-  float v[8][8];
-#pragma unroll
-  for (int c = 0; c < 8; c++) {
-    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
-    const float4 *src = (const float4 *)(grid + (((size_t)(i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz)) * 8);
-    float4 a = __ldg(src), b = __ldg(src + 1);
-    v[c][0] = a.x; v[c][1] = a.y; v[c][2] = a.z; v[c][3] = a.w;
-    v[c][4] = b.x; v[c][5] = b.y; v[c][6] = b.z; v[c][7] = b.w;
-  }
-  /* cap, src/grids.c:1058-1060 */
-  for (int c = 0; c < 8; c++)
-    if (v[c][0] > 1e10f) { out[q] = 1e8; return; }
-  double hx[4], hy[4], hz[4];
-  hermite(r[0], hx);
-  hermite(r[1], hy);
-  hermite(r[2], hz);
-  /* stored value index for derivative order (ox, oy, oz) */
-  const int idx[2][2][2] = {{{0, 3}, {2, 6}}, {{1, 5}, {4, 7}}};
-  double val = 0.0;
-#pragma unroll
-  for (int c = 0; c < 8; c++) {
-    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
-#pragma unroll
-    for (int ox = 0; ox < 2; ox++)
-#pragma unroll
-      for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-        for (int oz = 0; oz < 2; oz++)
-          val += (double)v[c][idx[ox][oy][oz]] * hx[2 * ox + dx] * hy[2 * oy + dy] * hz[2 * oz + dz];
-  }
-  out[q] = val;
+  const double p[3] = {xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]};
+  out[q] = rgpu_grid_value(grid, ip, p);
 }
 
 cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], const double size[3],
                                     const double shift[3], const double cell[3], int n, const double *d_xyz,
                                     double *d_out, cudaStream_t st)
 {
-  InterpParams ip;
+  RgpuGridGeom ip;
   for (int c = 0; c < 3; c++) {
     ip.npts[c] = npts[c];
     ip.size[c] = size[c];

@@ -1,0 +1,74 @@
+/* Tricubic lookup in an energy grid (InterpolateVDWGrid, src/grids.c:979-1077).
+ *
+ * The grid is the layout written by k_grid_build: (nx+1)(ny+1)(nz+1) points,
+ * point-major, 8 floats per point (value, three first, three mixed second
+ * and the third mixed derivative, scaled to the grid cell). The interpolant
+ * is the Hermite tensor product of those values at the 8 corners of the
+ * cell holding the point, the same polynomial as the reference's 64 x 64
+ * coefficient product. Points are wrapped into the unit cell the grid spans.
+ */
+#ifndef RGPU_GRID_CUH
+#define RGPU_GRID_CUH
+
+#include "rgpu_types.h"
+
+/* Cubic Hermite basis on [0,1]: {p0, p1, slope0, slope1} */
+__device__ __forceinline__ void rgpu_hermite(double t, double *h)
+{
+  const double t2 = t * t, t3 = t2 * t;
+  h[0] = 1.0 - 3.0 * t2 + 2.0 * t3;
+  h[1] = 3.0 * t2 - 2.0 * t3;
+  h[2] = t - 2.0 * t2 + t3;
+  h[3] = -t2 + t3;
+}
+
+/* energy at p (FP64); a corner value above 1e10 (an atom core) gives 1e8,
+ * as the reference's cap (src/grids.c:1058-1060) */
+__device__ __forceinline__ double rgpu_grid_value(const float *grid, const RgpuGridGeom &ip, const double *xyz)
+{
+  const int ny = ip.npts[1] + 1, nz = ip.npts[2] + 1;
+  double r[3];
+  int i0[3];
+  for (int c = 0; c < 3; c++) {
+    double p = xyz[c];
+    p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
+    if (p < 0.0) p += ip.cell[c];
+    const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
+    /* a point on the upper cell face (p == cell after wrapping) uses the last
+     * grid cell at r = 1, so the 2x2x2 corner block stays inside the grid */
+    i0[c] = min(max((int)s, 0), ip.npts[c] - 1);
+    r[c] = s - i0[c];
+  }
+  float v[8][8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+    const float4 *src = (const float4 *)(grid + (((size_t)(i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz)) * 8);
+    float4 a = __ldg(src), b = __ldg(src + 1);
+    v[c][0] = a.x; v[c][1] = a.y; v[c][2] = a.z; v[c][3] = a.w;
+    v[c][4] = b.x; v[c][5] = b.y; v[c][6] = b.z; v[c][7] = b.w;
+  }
+  for (int c = 0; c < 8; c++)
+    if (v[c][0] > 1e10f) return 1e8;
+  double hx[4], hy[4], hz[4];
+  rgpu_hermite(r[0], hx);
+  rgpu_hermite(r[1], hy);
+  rgpu_hermite(r[2], hz);
+  /* stored value index for derivative order (ox, oy, oz) */
+  const int idx[2][2][2] = {{{0, 3}, {2, 6}}, {{1, 5}, {4, 7}}};
+  double val = 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+#pragma unroll
+    for (int ox = 0; ox < 2; ox++)
+#pragma unroll
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int oz = 0; oz < 2; oz++)
+          val += (double)v[c][idx[ox][oy][oz]] * hx[2 * ox + dx] * hy[2 * oy + dy] * hz[2 * oz + dz];
+  }
+  return val;
+}
+
+#endif

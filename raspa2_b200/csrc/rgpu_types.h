@@ -103,6 +103,14 @@ typedef struct {
   float4 h;
 } TileRec;
 
+/* geometry of an energy grid: npts cells per axis over `size` from `shift`,
+ * spanning a unit cell of lengths `cell` */
+typedef struct {
+  int npts[3];
+  int pad;
+  double size[3], shift[3], cell[3];
+} RgpuGridGeom;
+
 typedef struct RgpuSys {
   /* geometry */
   double box[3], inv_box[3];
@@ -147,6 +155,12 @@ typedef struct RgpuSys {
   int pad_flex;
   double bond, bend_k, bend_theta0, bend_sigma;   /* bend_sigma = 1 / sqrt(beta bend_k) */
   double torsion[4], torsion_min;                 /* torsion_min: minimum of the torsion energy over phi */
+  /* energy grids (rgpu_system_set_grids): the engine takes the host VDW
+   * energy of molecule atom a from grid[a] instead of the pair sums */
+  int use_grid;
+  int pad_grid;
+  RgpuGridGeom grid_geom;
+  const float *grid[RGPU_MAX_ATOMS];
   /* device pointers */
   const double4 *fw64;        /* [nfw] x, y, z, q (sorted by type) */
   const int4 *fw32;           /* [ntile*RGPU_TILE] tiled: fixed-point x, y, z (low 2 bits of z = segment), float bits of q */

@@ -31,6 +31,7 @@ EXPORTS = [
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
     "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_intra_energy",
+    "rgpu_system_set_grids", "rgpu_system_checkpoint_size", "rgpu_system_checkpoint", "rgpu_system_restore",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -239,6 +240,62 @@ class GpuSystem:
         _check(load().rgpu_total_energy(self.h, out.ctypes.data_as(_dp)))
         return out
 
+    def set_grids(self, grid_ptrs, npts, size, shift, cell):
+        """Host VDW energies of the engine from energy grids: grid_ptrs[a] is
+        the device pointer of the grid of molecule atom a (rgpu_system_set_grids);
+        None switches them off."""
+        L = load()
+        self.grids_active = grid_ptrs is not None
+        if grid_ptrs is None:
+            _check(L.rgpu_system_set_grids(self.h, None, None, None, None, None))
+            return
+        arr = (C.c_void_p * len(grid_ptrs))(*grid_ptrs)
+        n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64); ce = _arr(cell, np.float64)
+        _check(L.rgpu_system_set_grids(self.h, arr, n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),
+                                       sh.ctypes.data_as(_dp), ce.ctypes.data_as(_dp)))
+
+    def use_energy_grids(self, spacing: float, like: Optional["GpuSystem"] = None):
+        """Builds one energy grid per pseudo-atom type of the molecule over the
+        (orthorhombic) unit cell, int(size / spacing) intervals per axis as
+        the reference's SpacingVDWGrid (src/grids.c:337-367), in device memory
+        this object keeps, and switches the engine's host VDW energies to
+        them. With `like` (a system of the same framework and molecule whose
+        grids are built at this spacing) its grids are shared instead of
+        built. Returns the grid geometry (npts, size, shift, cell)."""
+        import torch
+        uc = np.asarray(self.sysm.unit_cell, float)
+        npts = (uc / spacing).astype(np.int32)
+        shift = np.zeros(3)
+        n = int(np.prod(npts.astype(np.int64) + 1)) * 8
+        types = [int(t) for t in self.sysm.molecule_types()]
+        if like is not None:
+            o = like.sysm
+            if not (np.array_equal(o.unit_cell, self.sysm.unit_cell) and np.array_equal(o.frac, self.sysm.frac)
+                    and list(o.uc_types) == list(self.sysm.uc_types) and like._grid_geom[0].tolist() == npts.tolist()
+                    and o.molecule.atom_types == self.sysm.molecule.atom_types):
+                raise ValueError("grids can be shared only between systems of one framework, molecule and spacing")
+            self.share_grids_of(like)
+            return self._grid_geom
+        else:
+            bufs = {}
+            for t in sorted(set(types)):
+                buf = torch.empty(n, dtype=torch.float32, device="cuda")
+                torch.cuda.synchronize()
+                self.grid_build(t, npts, uc, shift, buf.data_ptr())
+                bufs[t] = buf
+        self._grids = bufs
+        self._grid_geom = (npts, uc, shift, uc)
+        self.set_grids([bufs[t].data_ptr() for t in types], npts, uc, shift, uc)
+        return self._grid_geom
+
+    def share_grids_of(self, other: "GpuSystem"):
+        """Uses the grids `other` uses (a system of the same framework and
+        molecule)."""
+        self._grids = other._grids
+        self._grid_geom = other._grid_geom
+        types = [int(t) for t in self.sysm.molecule_types()]
+        self.set_grids([self._grids[t].data_ptr() for t in types], *self._grid_geom)
+
     def intra_energy(self) -> float:
         """Intramolecular energy of flexible chains (rgpu_intra_energy)."""
         out = C.c_double()
@@ -274,6 +331,20 @@ class GpuSystem:
         widom = sm[6] / sm[7] if sm[7] > 0 else float("nan")
         return {"samples": int(sm[0]), "loading": N, "energy": U, "enthalpy": dh, "widom_weight": widom,
                 "sums": sm}
+
+    def checkpoint(self) -> bytes:
+        """The system's whole mutable state (rgpu_system_checkpoint)."""
+        L = load()
+        n = C.c_size_t()
+        _check(L.rgpu_system_checkpoint_size(self.h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(L.rgpu_system_checkpoint(self.h, buf, n))
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Continues from a checkpoint of a system of the same model."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(load().rgpu_system_restore(self.h, buf, C.c_size_t(len(data))))
 
     def reset_averages(self):
         _check(load().rgpu_system_reset_averages(self.h))
