@@ -451,8 +451,12 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
             evs[k][1].record(stream)
     torch.cuda.synchronize()
     t = sum(a.elapsed_time(b) for a, b in evs) / 1e3
-    d = (np.array([g.state()["counters"] for g in gs]) - c0).sum(axis=0)
+    dc = np.array([g.state()["counters"] for g in gs]) - c0
+    d = dc.sum(axis=0)
     moves = float(d[8])
+    cyc = dc[:, 15].astype(float)
+    phases = {"us_per_move_mean": float(np.mean(cyc / np.maximum(dc[:, 8], 1)) / 1965.0),
+              "share_eval": float(dc[:, 16].sum() / max(cyc.sum(), 1.0))}
     # bead positions looked up per move type: translation/rotation 6 new + 6
     # old, insertion/deletion 8 first-bead + 5 x 16 trials, reinsertion both
     lookups = 12.0 * (d[0] + d[1]) + 88.0 * (d[2] + d[3]) + 176.0 * d[18]
@@ -485,7 +489,7 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
                                        "median_rel": float(np.median(rel)), "max_rel": float(max(rel))},
            "acceptance": {k: (float(d[4 + i]) / max(float(d[i]), 1.0)) for i, k in
                           enumerate(["translation", "rotation", "insertion", "deletion"])},
-           "reinsertion_acceptance": float(d[19]) / max(float(d[18]), 1.0)}
+           "reinsertion_acceptance": float(d[19]) / max(float(d[18]), 1.0), "phases": phases}
     del flush
     return out
 

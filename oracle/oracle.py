@@ -153,10 +153,10 @@ class Oracle:
             s = o.s
             s.flexible = 1
             s.bond = mol.bond
-            s.bend_k = mol.bend_k * units.K_B
+            s.bend_k = mol.bend_k * units.KELVIN_TO_ENERGY
             s.bend_theta0 = np.deg2rad(mol.bend_theta0)
             s.bend_sigma = 1.0 / np.sqrt(s.beta * s.bend_k)
-            s.torsion[:] = [x * units.K_B for x in mol.torsion]
+            s.torsion[:] = [x * units.KELVIN_TO_ENERGY for x in mol.torsion]
             phi = np.linspace(-np.pi, np.pi, 20001)
             c = np.cos(phi)
             e = (s.torsion[0] + s.torsion[1] * (1 + c) + s.torsion[2] * (1 - (2 * c * c - 1))

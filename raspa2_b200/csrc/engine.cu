@@ -865,6 +865,56 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
 }
 
 /* ------------------------------------------------------------------------ */
+/* chain_trial for bead i >= 2 of trial t, computed by one warp: lane l draws
+ * proposals l, l + 32, ... of the bend angle (and of the dihedral) at once,
+ * and the lowest accepted proposal wins, so the result is chain_trial's (its
+ * proposals are tried in order and the first accepted one is taken). Every
+ * lane returns the trial position p and its bonded energy. */
+__device__ __forceinline__ double chain_trial_warp(const RgpuSys &S, const double (*x)[3], int i, int stage, int t,
+                                                   uint64_t step, int lane, double *p)
+{
+  auto U = [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); };
+  double theta = S.bend_theta0;
+  for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
+    const int a = base + lane;
+    double th = 0.0;
+    bool ok = false;
+    if (a < RGPU_CHAIN_TRIES) {
+      const double u1 = U(3 * a), u2 = U(3 * a + 1), u3 = U(3 * a + 2);
+      th = S.bend_theta0 + S.bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
+      ok = th > 0.0 && th < M_PI && u3 < sin(th);
+    }
+    const unsigned b = __ballot_sync(RGPU_FULL, ok);
+    if (b) {
+      theta = __shfl_sync(RGPU_FULL, th, __ffs(b) - 1);
+      break;
+    }
+  }
+  const int k = 3 * RGPU_CHAIN_TRIES;
+  double phi;
+  if (i == 2) {
+    phi = 2.0 * M_PI * U(k) - M_PI;
+  } else {
+    phi = M_PI;
+    for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
+      const int a = base + lane;
+      double f = 0.0;
+      bool ok = false;
+      if (a < RGPU_CHAIN_TRIES) {
+        f = 2.0 * M_PI * U(k + 2 * a) - M_PI;
+        ok = U(k + 2 * a + 1) < exp(-S.beta * (chain_torsion_energy(S, cos(f)) - S.torsion_min));
+      }
+      const unsigned b = __ballot_sync(RGPU_FULL, ok);
+      if (b) {
+        phi = __shfl_sync(RGPU_FULL, f, __ffs(b) - 1);
+        break;
+      }
+    }
+  }
+  chain_place(i >= 3 ? x[i - 3] : nullptr, x[i - 2], x[i - 1], S.bond, theta, phi, p);
+  return chain_bonded_energy(S, x, i, p);
+}
+
 /* CBMC growth (retrace = false) or retrace (retrace = true) of a flexible
  * chain, bead by bead from atom 0 (GrowMolecule / RetraceMolecule,
  * src/cbmc.c:2928-3181, for a linear chain): the first bead from nf trials
@@ -891,7 +941,23 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED> &E, bool retrace, int stag
   }
   for (int i = 0; i < na; i++) {
     const int k = i == 0 ? nf : nt;
-    if (threadIdx.x < k) {
+    if (i >= 2) {
+      /* bend and dihedral draws: one warp per trial */
+      const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      for (int t = threadIdx.x >> 5; t < k; t += nw) {
+        double p[3], ub = 0.0;
+        if (retrace && t == 0) {
+          atom_xyz(E, m, i, p);
+          ub = chain_bonded_energy(S, C.cp, i, p);
+        } else {
+          ub = chain_trial_warp(S, C.cp, i, stage, t, E.step, lane, p);
+        }
+        if (lane == 0) {
+          bead_set(E.pos[t], S, p[0], p[1], p[2], i, exclude);
+          C.ub[t] = ub;
+        }
+      }
+    } else if (threadIdx.x < k) {
       const int t = threadIdx.x;
       double p[3], ub = 0.0;
       if (retrace && t == 0) {

@@ -161,9 +161,9 @@ class GpuSystem:
         if not mol.rigid:
             d.flexible = 1
             d.bond = mol.bond
-            d.bend_k = mol.bend_k * units.K_B
+            d.bend_k = mol.bend_k * units.KELVIN_TO_ENERGY
             d.bend_theta0 = np.deg2rad(mol.bend_theta0)
-            d.torsion[:] = [t * units.K_B for t in mol.torsion]
+            d.torsion[:] = [t * units.KELVIN_TO_ENERGY for t in mol.torsion]
         self.natom = d.natom
         self.maxmol = maxmol
         h = C.c_void_p()

@@ -137,14 +137,14 @@ def _flexible_chain_terms(m, lines) -> None:
 def simulation_input(sys: System, cycles: int = 0, init_cycles: int = 0,
                      print_every: int = 1000, seed: Optional[int] = None,
                      simulation_type: str = "MonteCarlo",
-                     grid: Optional[dict] = None, extra: str = "") -> str:
+                     grid: Optional[dict] = None, extra: str = "", restart: bool = False) -> str:
     mv = sys.moves
     lines = [
         f"SimulationType                {simulation_type}",
         f"NumberOfCycles                {cycles}",
         f"NumberOfInitializationCycles  {init_cycles}",
         f"PrintEvery                    {print_every}",
-        "RestartFile                   no",
+        f"RestartFile                   {'yes' if restart else 'no'}",
         "Forcefield                    Local",
         f"CutOff                        {sys.cutoff}",
         f"ChargeMethod                  {'Ewald' if sys.ewald else 'None'}",

@@ -53,6 +53,11 @@ class Job:
     seed: int = 1
     arrival: float = 0.0        # seconds after the stream starts
     maxmol: int = 512
+    # resumable jobs: start from a checkpoint of the same system and stream
+    # (GpuSystem.checkpoint; `steps` and `equil` count from step 0 of the
+    # original job), and/or return the final checkpoint with the result
+    resume: Optional[bytes] = None
+    keep_checkpoint: bool = False
     # filled in by the server
     admitted: Optional[float] = None
     finished: Optional[float] = None
@@ -98,7 +103,10 @@ class Server:
 
     def _admit(self, job: Job, now: float) -> "native.GpuSystem":
         g = native.GpuSystem(job.system, maxmol=job.maxmol, seed=job.seed, stream_id=job.id)
-        g.set_adsorbates(np.zeros((0, job.system.molecule.n_atoms, 3)))
+        if job.resume is not None:
+            g.restore(job.resume)
+        else:
+            g.set_adsorbates(np.zeros((0, job.system.molecule.n_atoms, 3)))
         g.set_limits(job.steps, job.equil)
         job.admitted = now
         return g
@@ -108,11 +116,14 @@ class Server:
         st = g.state()
         av = g.averages()
         kT = units.K_B * job.system.temperature
-        return {"loading": av["loading"], "energy_K": av["energy"] / units.K_B,
-                "enthalpy_K": av["enthalpy"] / units.K_B if np.isfinite(av["enthalpy"]) else None,
-                "samples": av["samples"], "final_nmol": st["nmol"], "steps": int(st["step"]),
-                "status": st["status"], "energy_terms": st["energy"][:6].tolist(),
-                "counters": st["counters"][:10].tolist(), "kT": kT}
+        out = {"loading": av["loading"], "energy_K": av["energy"] / units.K_B,
+               "enthalpy_K": av["enthalpy"] / units.K_B if np.isfinite(av["enthalpy"]) else None,
+               "samples": av["samples"], "final_nmol": st["nmol"], "steps": int(st["step"]),
+               "status": st["status"], "energy_terms": st["energy"][:6].tolist(),
+               "counters": st["counters"][:10].tolist(), "kT": kT}
+        if job.keep_checkpoint:
+            out["checkpoint"] = g.checkpoint()
+        return out
 
     def run(self, jobs: Sequence[Job], realtime: bool = True) -> dict:
         """Serves `jobs` (arrival times relative to the call) to completion.
@@ -142,7 +153,8 @@ class Server:
                 if mem_used + fp > self.mem_budget and active:
                     break
                 job = waiting.popleft()
-                active.append([job, self._admit(job, now()), 0, fp])
+                g = self._admit(job, now())
+                active.append([job, g, int(g.state()["step"]) if job.resume is not None else 0, fp])
                 mem_used += fp
                 dirty = True
 
