@@ -117,6 +117,7 @@ struct Ctl {
   double sums[RGPU_NSUM];     /* ensemble sums of this launch */
   int next;                   /* unit counter of eval_units */
   double ewt[2][2];           /* this CTA's Ewald sums {e_ads, e_host}, by buffer */
+  double gv[RGPU_MAX_POS];    /* grid host VDW of the positions of the current evaluation */
 };
 static_assert(sizeof(Ctl) <= RGPU_CTL_BYTES, "control block exceeds its shared-memory slot");
 
@@ -219,19 +220,23 @@ __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 
 /* Pair evaluation of P positions on this CTA's share, then one cluster
  * barrier; the totals are read with gather(). All threads call. */
-/* Host VDW of one bead from its type's energy grid, out of line so that the
- * lookup's registers stay out of the evaluation loop's allocation. */
-__device__ __noinline__ double engine_grid_value(const RgpuSys *S, int atom, double x, double y, double z)
-{
-  const double p[3] = {x, y, z};
-  return rgpu_grid_value(S->grid[atom], S->grid_geom, p);
-}
-
 template <bool MIXED>
 __device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
+  if (E.S->use_grid && E.rank == 0) {
+    /* host VDW from the bead types' energy grids (one CTA of the cluster):
+     * 8 lanes per position, 4 positions per warp, before the pair units */
+    const int lane = threadIdx.x & 31;
+    for (int base = (threadIdx.x >> 5) * 4; base < P; base += (blockDim.x >> 5) * 4) {
+      const int p = base + (lane >> 3);
+      const bool live = p < P;
+      const double x[3] = {live ? E.pos[p].x : 0.0, live ? E.pos[p].y : 0.0, live ? E.pos[p].z : 0.0};
+      const double g = rgpu_grid_value8(E.S->grid[live ? E.pos[p].atom : 0], E.S->grid_geom, x, lane & 7, live);
+      if (live && (lane & 7) == 0) C.gv[p] = g;
+    }
+  }
   const EvalPlan pl = eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.sc, RGPU_MAX_UNITS);
   const int per = pl.cf + pl.ca;
   __syncthreads();
@@ -248,8 +253,7 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check
       ov |= E.uo[u];
     }
     if (E.S->use_grid && E.rank == 0) {
-      /* host VDW from the bead type's energy grid (one CTA of the cluster) */
-      const double g = engine_grid_value(E.S, E.pos[p].atom, E.pos[p].x, E.pos[p].y, E.pos[p].z);
+      const double g = C.gv[p];
       hv += g;
       ov |= g >= E.S->overlap;
     }

@@ -71,4 +71,54 @@ __device__ __forceinline__ double rgpu_grid_value(const float *grid, const RgpuG
   return val;
 }
 
+/* The same lookup by a group of 8 lanes (lane8 = lane % 8; every lane of
+ * the warp calls, converged): lane c reads corner c's 8 values and forms its
+ * share of the Hermite sum, and three xor-shuffles add the shares, so a
+ * lookup costs one memory round trip instead of eight. Every lane of the
+ * group returns the value (the same polynomial as rgpu_grid_value, summed in
+ * another order). A group with live = false only takes part in the
+ * shuffles. */
+__device__ __forceinline__ double rgpu_grid_value8(const float *grid, const RgpuGridGeom &ip, const double *xyz,
+                                                   int lane8, bool live)
+{
+  double val = 0.0;
+  int big = 0;
+  if (live) {
+    const int ny = ip.npts[1] + 1, nz = ip.npts[2] + 1;
+    double r[3];
+    int i0[3];
+    for (int c = 0; c < 3; c++) {
+      double p = xyz[c];
+      p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
+      if (p < 0.0) p += ip.cell[c];
+      const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
+      i0[c] = min(max((int)s, 0), ip.npts[c] - 1);
+      r[c] = s - i0[c];
+    }
+    const int dx = lane8 & 1, dy = (lane8 >> 1) & 1, dz = lane8 >> 2;
+    const float4 *src = (const float4 *)(grid + (((size_t)(i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz)) * 8);
+    const float4 a = __ldg(src), b = __ldg(src + 1);
+    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    big = v[0] > 1e10f;
+    double hx[4], hy[4], hz[4];
+    rgpu_hermite(r[0], hx);
+    rgpu_hermite(r[1], hy);
+    rgpu_hermite(r[2], hz);
+    const int idx[2][2][2] = {{{0, 3}, {2, 6}}, {{1, 5}, {4, 7}}};
+#pragma unroll
+    for (int ox = 0; ox < 2; ox++)
+#pragma unroll
+      for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+        for (int oz = 0; oz < 2; oz++)
+          val += (double)v[idx[ox][oy][oz]] * hx[2 * ox + dx] * hy[2 * oy + dy] * hz[2 * oz + dz];
+  }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    val += __shfl_xor_sync(0xffffffffu, val, o);
+    big |= __shfl_xor_sync(0xffffffffu, big, o);
+  }
+  return big ? 1e8 : val;
+}
+
 #endif

@@ -13,6 +13,12 @@ run's output:
 The JSON keeps every seed's values and their mean and standard error across
 seeds. tests/test_gpu_stats.py compares the engine's averages against it.
 
+Henry cases (HENRY_CASES) run Widom test insertions only: into the framework
+(average Rosenbluth weight <W>) and into an empty box (the ideal-gas weight
+W_IG), each with `seeds` seeds, and store the Henry ratio <W> / W_IG, the
+quantity that is independent of how a code draws the bonded part of its CBMC
+trials.
+
     python tests/golden/make_stat_golden.py [--workdir DIR] [case ...]
 """
 from __future__ import annotations
@@ -50,6 +56,11 @@ WIDOM_CYCLES = 20000
 SEEDS = 8
 IDEAL = {}
 
+# name -> (builder, temperature, Widom cycles in the framework, in the empty box)
+HENRY_CASES = {
+    "hexane_small_henry": (lambda: systems.hexane_system(seed=4, n_atoms=1200, cell=26.0), 433.0, 4000, 4000),
+}
+
 
 def parse(path):
     txt = open(path).read()
@@ -74,6 +85,41 @@ def reference_ideal_gas_rosenbluth(molecule, temperature, workdir):
     txt = open(os.path.join(out, os.listdir(out)[0])).read()
     m = re.search(r"Average Widom Rosenbluth-weight:\s+([-\d.eE+]+) \+/-\s+([-\d.eE+]+)", txt)
     return float(m.group(1)), float(m.group(2))
+
+
+def _widom_run(s, d, cycles, seed):
+    raspa_io.write_inputs(s, d, cycles=cycles, init_cycles=0, print_every=10 ** 9, seed=seed)
+    r = subprocess.run([SIMULATE, "-i", "simulation.input"], cwd=d, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"simulate failed in {d}: {r.stderr[-500:]}")
+    out = os.path.join(d, "Output", "System_0")
+    txt = open(os.path.join(out, os.listdir(out)[0])).read()
+    m = re.search(r"Average Widom Rosenbluth-weight:\s+([-\d.eE+]+) \+/-\s+([-\d.eE+]+)", txt)
+    return float(m.group(1))
+
+
+def run_henry_case(name, workdir):
+    build, T, cyc_fw, cyc_ig = HENRY_CASES[name]
+    widom = systems.MoveMix(translation=0.0, rotation=0.0, swap_insert=0.0, swap_delete=0.0, widom=1.0)
+    fw = dataclasses.replace(build(), temperature=T, moves=widom)
+    ig = systems.empty_box_system(fw.molecule, T)
+    jobs = [(fw, os.path.join(workdir, f"{name}_fw_{k}"), cyc_fw, 7001 + 13 * k) for k in range(SEEDS)]
+    jobs += [(ig, os.path.join(workdir, f"{name}_ig_{k}"), cyc_ig, 8001 + 13 * k) for k in range(SEEDS)]
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        w = list(ex.map(lambda j: _widom_run(*j), jobs))
+    wf, wi = np.array(w[:SEEDS]), np.array(w[SEEDS:])
+    mf, sf = wf.mean(), wf.std(ddof=1) / np.sqrt(SEEDS)
+    mi, si = wi.mean(), wi.std(ddof=1) / np.sqrt(SEEDS)
+    doc = {"case": name, "system": fw.name, "temperature_K": T, "seeds": SEEDS,
+           "widom_cycles_framework": cyc_fw, "widom_cycles_empty_box": cyc_ig,
+           "widom_weight_runs": wf.tolist(), "ideal_gas_runs": wi.tolist(),
+           "widom_weight_mean": float(mf), "widom_weight_se": float(sf),
+           "ideal_gas_rosenbluth_mean": float(mi), "ideal_gas_rosenbluth_se": float(si),
+           "henry_ratio": float(mf / mi), "henry_ratio_se": float(mf / mi * np.hypot(sf / mf, si / mi)),
+           "source": "reference simulate (oracle/_ref) built from the reference sources; Widom moves only"}
+    with open(os.path.join(OUT, f"stat_{name}.json"), "w") as fh:
+        json.dump(doc, fh, indent=1)
+    print(name, doc["henry_ratio"], "+-", doc["henry_ratio_se"])
 
 
 def run_case(name, workdir):
@@ -104,8 +150,11 @@ def main(argv):
     if argv[:1] == ["--workdir"]:
         work, argv = argv[1], argv[2:]
         os.makedirs(work, exist_ok=True)
-    names = argv or list(CASES)
+    names = argv or list(CASES) + list(HENRY_CASES)
     work = work or tempfile.mkdtemp(prefix="raspa_stat_")
+    for name in [n for n in names if n in HENRY_CASES]:
+        run_henry_case(name, work)
+    names = [n for n in names if n not in HENRY_CASES]
     jobs = []
     meta = {}
     for name in names:
