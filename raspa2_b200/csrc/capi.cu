@@ -97,6 +97,7 @@ struct rgpu_engine {
   RgpuSys *d_systems;
   int mixed, threads, kw, max_ads, cluster, fw_items, tile_items, k_items;
   bool wide;                  /* 64-register build of the mixed kernel */
+  bool flex;                  /* build with flexible-chain moves and energy grids */
   size_t smem;
   cudaStream_t st;
   /* CUDA graph of one launch, replayed by rgpu_engine_run when enabled */
@@ -1114,6 +1115,7 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->mixed = precision == RGPU_MIXED;
   e->threads = threads;
   e->wide = wide;
+  e->flex = false;
   e->cluster = cluster ? cluster : auto_cluster(n);
   e->kw = 1;
   e->max_ads = 0;
@@ -1124,6 +1126,7 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
     if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
     e->sys.push_back(s);
     all_grids = all_grids && s->h.use_grid;
+    e->flex = e->flex || s->h.use_grid || s->h.flexible;
     e->kw = std::max(e->kw, s->kw);
     e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
     maxfw = std::max(maxfw, (s->d.nfw + e->cluster - 1) / e->cluster);
@@ -1207,10 +1210,10 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   const int n = (int)e->sys.size();
-  CK(rgpu_engine_prepare(e->mixed, e->wide, e->smem));
+  CK(rgpu_engine_prepare(e->mixed, e->wide, e->flex, e->smem));
   if (!e->use_graph) {
     CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
-                          e->k_items, e->cluster, e->threads, e->wide, st));
+                          e->k_items, e->cluster, e->threads, e->wide, e->flex, st));
   } else {
     if (!e->gexec || e->g_nsteps != nsteps) {
       if (e->gexec) {
@@ -1220,7 +1223,7 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       cudaError_t le = rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items,
-                                          e->tile_items, e->k_items, e->cluster, e->threads, e->wide, st);
+                                          e->tile_items, e->k_items, e->cluster, e->threads, e->wide, e->flex, st);
       cudaError_t ce = cudaStreamEndCapture(st, &g);
       if (le != cudaSuccess || ce != cudaSuccess) {
         if (g) cudaGraphDestroy(g);

@@ -121,7 +121,7 @@ struct Ctl {
 };
 static_assert(sizeof(Ctl) <= RGPU_CTL_BYTES, "control block exceeds its shared-memory slot");
 
-template <bool MIXED>
+template <bool MIXED, bool FLEX>
 struct Eng {
   RgpuSys *S;
   EvalSlice sl;
@@ -146,8 +146,8 @@ struct Eng {
 /* Position of atom a of molecule m. FP64 records carry the position; on the
  * mixed path the FP64 positions stay in global memory (ads_xyz), which every
  * CTA of the cluster writes with the same values on each accepted move. */
-template <bool MIXED>
-__device__ __forceinline__ void atom_xyz(const Eng<MIXED> &E, int m, int a, double *p)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void atom_xyz(const Eng<MIXED, FLEX> &E, int m, int a, double *p)
 {
   const int idx = m * E.S->natom + a;
   if (MIXED) {
@@ -159,8 +159,8 @@ __device__ __forceinline__ void atom_xyz(const Eng<MIXED> &E, int m, int a, doub
   }
 }
 
-template <bool MIXED>
-__device__ __forceinline__ void atom_store(const Eng<MIXED> &E, int m, int a, const double *p)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void atom_store(const Eng<MIXED, FLEX> &E, int m, int a, const double *p)
 {
   const RgpuSys &S = *E.S;
   const int idx = m * S.natom + a;
@@ -220,12 +220,12 @@ __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 
 /* Pair evaluation of P positions on this CTA's share, then one cluster
  * barrier; the totals are read with gather(). All threads call. */
-template <bool MIXED>
-__device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair_check)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
-  if (E.S->use_grid && E.rank == 0) {
+  if (FLEX && E.S->use_grid && E.rank == 0) {
     /* host VDW from the bead types' energy grids (one CTA of the cluster):
      * 8 lanes per position, 4 positions per warp, before the pair units */
     const int lane = threadIdx.x & 31;
@@ -252,7 +252,7 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check
       else { av += E.uv[u]; ac += E.uc[u]; }
       ov |= E.uo[u];
     }
-    if (E.S->use_grid && E.rank == 0) {
+    if (FLEX && E.S->use_grid && E.rank == 0) {
       const double g = C.gv[p];
       hv += g;
       ov |= g >= E.S->overlap;
@@ -266,8 +266,8 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED> &E, int P, int pair_check
 
 /* Totals of position p of the last evaluation (buffer b): the CTAs' sums
  * added in rank order. */
-template <bool MIXED>
-__device__ __forceinline__ void gather(const Eng<MIXED> &E, int b, int p, double *r, int &ov)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void gather(const Eng<MIXED, FLEX> &E, int b, int p, double *r, int &ov)
 {
   cg::cluster_group cl = cg::this_cluster();
   const PosSum *own = E.part + b * RGPU_MAX_POS + p;
@@ -283,8 +283,8 @@ __device__ __forceinline__ void gather(const Eng<MIXED> &E, int b, int p, double
 
 /* Ewald sum over this CTA's wave vectors for the sites in E.sites[0..ns),
  * warp partials left in E.red[b]; one cluster barrier. All threads call. */
-template <bool MIXED>
-__device__ __forceinline__ void engine_ewald(Eng<MIXED> &E, int ns)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void engine_ewald(Eng<MIXED, FLEX> &E, int ns)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
@@ -317,8 +317,8 @@ __device__ __forceinline__ void engine_ewald(Eng<MIXED> &E, int ns)
 }
 
 /* cluster total of the last Ewald sum (buffer b) */
-template <bool MIXED>
-__device__ __forceinline__ void gather_ewald(const Eng<MIXED> &E, int b, double &ea, double &eh)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void gather_ewald(const Eng<MIXED, FLEX> &E, int b, double &ea, double &eh)
 {
   cg::cluster_group cl = cg::this_cluster();
   ea = eh = 0.0;
@@ -337,8 +337,8 @@ __device__ __forceinline__ void gather_ewald(const Eng<MIXED> &E, int b, double 
  * LJ biasing (src/cbmc.c:734-735, :1432-1436). Selection as
  * SelectTrialPosition (src/cbmc.c:563-599). Lane 0 leaves the weight sum
  * (w_sum = sum exp(bf)), the selected trial and its energies in Ctl. */
-template <bool MIXED>
-__device__ __forceinline__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, int nb, bool first, bool select, double usel,
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void cbmc_trials(const Eng<MIXED, FLEX> &E, int b, int n, int nb, bool first, bool select, double usel,
                             double &w_sum, int &sel, double *usum, int &any, int off = 0, double *w_sel = nullptr)
 {
   const int lane = threadIdx.x & 31;
@@ -390,8 +390,8 @@ __device__ __forceinline__ void cbmc_trials(const Eng<MIXED> &E, int b, int n, i
 /* ------------------------------------------------------------------------ */
 /* translation (mv=0) and rotation (mv=1):
  * TranslationMoveAdsorbate src/mc_moves.c:1529-1762, RotationMoveAdsorbate :2636 */
-template <bool MIXED>
-__device__ __forceinline__ void step_displace(Eng<MIXED> &E, int mv)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void step_displace(Eng<MIXED, FLEX> &E, int mv)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -424,7 +424,7 @@ __device__ __forceinline__ void step_displace(Eng<MIXED> &E, int mv)
     E.sites[na + a].q = -S.mol_q[a];
   }
   __syncthreads();
-  engine_eval<MIXED>(E, 2 * na, na);
+  engine_eval(E, 2 * na, na);
   const int be = E.xb;
   E.xb ^= 1;
   if (threadIdx.x < 32) {
@@ -452,7 +452,7 @@ __device__ __forceinline__ void step_displace(Eng<MIXED> &E, int mv)
   const bool ew = S.ewald && S.mol_charged;
   int bw = 0;
   if (ew) {
-    engine_ewald<MIXED>(E, 2 * na);
+    engine_ewald(E, 2 * na);
     bw = E.xb;
     E.xb ^= 1;
   }
@@ -500,8 +500,8 @@ __device__ __forceinline__ void step_displace(Eng<MIXED> &E, int mv)
  * of GenerateTrialOrientationsSimpleSphere :1480-1578 and
  * ComputeExternalEnergies :1154-1478, LJ biasing; acceptance of
  * SwapAddAdsorbateMove src/mc_moves.c:7016 and SwapRemoveAdsorbateMove :7228. */
-template <bool MIXED>
-__device__ __forceinline__ void step_swap(Eng<MIXED> &E, bool insert, bool widom = false)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool widom = false)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -528,7 +528,7 @@ __device__ __forceinline__ void step_swap(Eng<MIXED> &E, bool insert, bool widom
     bead_set(E.pos[i], S, p[0], p[1], p[2], sb, exclude);
   }
   __syncthreads();
-  engine_eval<MIXED>(E, nf, 0);
+  engine_eval(E, nf, 0);
   int b1 = E.xb;
   E.xb ^= 1;
   if (threadIdx.x < 32) {
@@ -579,7 +579,7 @@ __device__ __forceinline__ void step_swap(Eng<MIXED> &E, bool insert, bool widom
       }
     }
     __syncthreads();
-    engine_eval<MIXED>(E, nt * nb, 0);
+    engine_eval(E, nt * nb, 0);
     const int b2 = E.xb;
     E.xb ^= 1;
     if (threadIdx.x < 32) {
@@ -616,7 +616,7 @@ __device__ __forceinline__ void step_swap(Eng<MIXED> &E, bool insert, bool widom
   const bool ew = S.ewald && S.mol_charged;
   int bw = 0;
   if (ew) {
-    engine_ewald<MIXED>(E, na);
+    engine_ewald(E, na);
     bw = E.xb;
     E.xb ^= 1;
   }
@@ -687,8 +687,8 @@ __device__ __forceinline__ void step_swap(Eng<MIXED> &E, bool insert, bool widom
  * Evaluation 1 holds the nf new first-bead trials, the old first bead and
  * the retrace orientations (all known up front); evaluation 2 the new
  * orientations around the chosen first bead. */
-template <bool MIXED>
-__device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void step_reinsert(Eng<MIXED, FLEX> &E)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -731,7 +731,7 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
     }
   }
   __syncthreads();
-  engine_eval<MIXED>(E, nf + 1 + (na > 1 ? nt * nb : 0), 0);
+  engine_eval(E, nf + 1 + (na > 1 ? nt * nb : 0), 0);
   const int b1 = E.xb;
   E.xb ^= 1;
   if (threadIdx.x < 32) {
@@ -792,7 +792,7 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
       }
     }
     __syncthreads();
-    engine_eval<MIXED>(E, nt * nb, 0);
+    engine_eval(E, nt * nb, 0);
     const int b2 = E.xb;
     E.xb ^= 1;
     if (threadIdx.x < 32) {
@@ -830,7 +830,7 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED> &E)
   const bool ew = S.ewald && S.mol_charged;
   int bw = 0;
   if (ew) {
-    engine_ewald<MIXED>(E, 2 * na);
+    engine_ewald(E, 2 * na);
     bw = E.xb;
     E.xb ^= 1;
   }
@@ -931,8 +931,8 @@ __device__ __forceinline__ double chain_trial_warp(const RgpuSys &S, const doubl
  * host and adsorbate VDW (u[0], u[2]) and the intramolecular energy
  * (uintra: bonded + LJ), or fail. Molecule m is the one retraced; `exclude`
  * leaves a molecule out of the adsorbate sums. All threads call. */
-template <bool MIXED>
-__device__ __forceinline__ void grow_chain(Eng<MIXED> &E, bool retrace, int stage, int m, int exclude)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, int stage, int m, int exclude)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -979,7 +979,7 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED> &E, bool retrace, int stag
       C.ub[t] = ub;
     }
     __syncthreads();
-    engine_eval<MIXED>(E, k, 0);
+    engine_eval(E, k, 0);
     const int b = E.xb;
     E.xb ^= 1;
     if (threadIdx.x < 32) {
@@ -1030,8 +1030,8 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED> &E, bool retrace, int stag
 /* CBMC insertion, deletion and Widom test insertion of a flexible chain
  * (SwapAddAdsorbateMove src/mc_moves.c:7016, SwapRemoveAdsorbateMove :7228,
  * WidomAdsorbateMove :7844; uncharged chains, no Fourier part). */
-template <bool MIXED>
-__device__ __forceinline__ void step_swap_chain(Eng<MIXED> &E, bool insert, bool widom)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void step_swap_chain(Eng<MIXED, FLEX> &E, bool insert, bool widom)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -1042,7 +1042,7 @@ __device__ __forceinline__ void step_swap_chain(Eng<MIXED> &E, bool insert, bool
     m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
     if (m >= nmol) m = nmol - 1;
   }
-  grow_chain<MIXED>(E, !insert, insert ? 0 : 1, m, insert ? -1 : m);
+  grow_chain(E, !insert, insert ? 0 : 1, m, insert ? -1 : m);
   if (C.fail) return;
   if (threadIdx.x == 0) {
     double pacc;
@@ -1082,15 +1082,15 @@ __device__ __forceinline__ void step_swap_chain(Eng<MIXED> &E, bool insert, bool
 /* CBMC reinsertion of a flexible chain (ReinsertionAdsorbateMove,
  * src/mc_moves.c:4415): a new configuration grown with molecule m left out,
  * the old one retraced; accepted with W(new) / W(old). */
-template <bool MIXED>
-__device__ __forceinline__ void step_reinsert_chain(Eng<MIXED> &E)
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void step_reinsert_chain(Eng<MIXED, FLEX> &E)
 {
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
   const int na = S.natom, nmol = C.nmol;
   int m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
   if (m >= nmol) m = nmol - 1;
-  grow_chain<MIXED>(E, false, 0, m, m);
+  grow_chain(E, false, 0, m, m);
   if (C.fail) return;
   if (threadIdx.x == 0) {
     C.rosen_old = C.rosen;     /* the new configuration's weight, kept while the old one is retraced */
@@ -1101,7 +1101,7 @@ __device__ __forceinline__ void step_reinsert_chain(Eng<MIXED> &E)
       for (int d = 0; d < 3; d++) C.cpn[a][d] = C.cp[a][d];
   }
   __syncthreads();
-  grow_chain<MIXED>(E, true, 1, m, m);
+  grow_chain(E, true, 1, m, m);
   if (C.fail) return;
   if (threadIdx.x == 0) {
     const double w_new = C.rosen_old, w_old = C.rosen;
@@ -1134,8 +1134,11 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
 
 /* WIDE: compiled for CTAs of up to 1024 threads (64 registers per thread);
  * otherwise up to 512 threads with 128 registers. The engine picks WIDE for
- * CTAs above 512 threads and when several CTAs must share an SM. */
-template <bool MIXED, bool WIDE>
+ * CTAs above 512 threads and when several CTAs must share an SM. FLEX:
+ * compiled with flexible-chain moves and energy grids; batches of rigid
+ * molecules without grids run the build without them, whose register
+ * allocation the chain and grid code does not touch. */
+template <bool MIXED, bool WIDE, bool FLEX>
 __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps,
                                                                        int kw, int max_ads_atoms, int fw_items,
                                                                        int tile_items, int k_items)
@@ -1148,7 +1151,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
   const int nwarps = blockDim.x >> 5;
   const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw, k_items, nwarps);
   if (sysi < nsys) {
-    Eng<MIXED> E;
+    Eng<MIXED, FLEX> E;
     E.rank = rank;
     E.csize = csize;
     E.xb = 0;
@@ -1219,7 +1222,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
       }
     }
     E.sl.ads = E.ads;
-    if (S.use_grid) E.sl.fw_hi = E.sl.fw_lo;   /* host VDW from the grids: no framework pairs */
+    if (FLEX && S.use_grid) E.sl.fw_hi = E.sl.fw_lo;   /* host VDW from the grids: no framework pairs */
     /* this CTA's wave vectors with their prefactors and S(k) */
     if (S.ewald) share(S.nk, rank, csize, E.k0, E.k1);
     else { E.k0 = 0; E.k1 = 0; }
@@ -1274,34 +1277,34 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
       if (mv <= 1) {
         if (!(nmol == 0 || (mv == 1 && S.natom == 1))) {
           if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + mv]++; }
-          step_displace<MIXED>(E, mv);
+          step_displace(E, mv);
         }
       } else if (mv == 2) {
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 2]++; }
         if (nmol >= S.maxmol) {
           if (threadIdx.x == 0) C.status |= RGPU_ERR_MAXMOL;
-        } else if (S.flexible) {
-          step_swap_chain<MIXED>(E, true, false);
+        } else if (FLEX && S.flexible) {
+          step_swap_chain(E, true, false);
         } else {
-          step_swap<MIXED>(E, true);
+          step_swap(E, true);
         }
       } else if (mv == 3) {
         if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_ATTEMPT + 3]++; }
         if (nmol != 0) {
-          if (S.flexible) step_swap_chain<MIXED>(E, false, false);
-          else step_swap<MIXED>(E, false);
+          if (FLEX && S.flexible) step_swap_chain(E, false, false);
+          else step_swap(E, false);
         }
       } else if (mv == 4) {
         /* the reference returns before counting when there is no molecule */
         if (nmol != 0) {
           if (threadIdx.x == 0) { C.cnt[RGPU_CNT_MOVES]++; C.cnt[RGPU_CNT_REINS_ATTEMPT]++; }
-          if (S.flexible) step_reinsert_chain<MIXED>(E);
-          else step_reinsert<MIXED>(E);
+          if (FLEX && S.flexible) step_reinsert_chain(E);
+          else step_reinsert(E);
         }
       } else {
         if (threadIdx.x == 0) C.cnt[RGPU_CNT_MOVES]++;
-        if (S.flexible) step_swap_chain<MIXED>(E, true, true);
-        else step_swap<MIXED>(E, true, true);
+        if (FLEX && S.flexible) step_swap_chain(E, true, true);
+        else step_swap(E, true, true);
       }
       /* ensemble sums after the step (thread 0 owns the running values) */
       if (threadIdx.x == 0 && step >= avg0) {
@@ -1352,17 +1355,23 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
   cl.sync();
 }
 
-cudaError_t rgpu_engine_prepare(int mixed, bool wide, size_t smem)
+/* the kernel build for (mixed, wide, flex) */
+using EngineKernel = void (*)(RgpuSys *, int, long long, int, int, int, int, int);
+static EngineKernel engine_kernel(int mixed, bool wide, bool flex)
 {
-  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (mixed && wide) return cudaFuncSetAttribute(rgpu_engine_kernel<true, true>, a, (int)smem);
-  if (mixed) return cudaFuncSetAttribute(rgpu_engine_kernel<true, false>, a, (int)smem);
-  return cudaFuncSetAttribute(rgpu_engine_kernel<false, false>, a, (int)smem);
+  if (mixed && wide) return flex ? rgpu_engine_kernel<true, true, true> : rgpu_engine_kernel<true, true, false>;
+  if (mixed) return flex ? rgpu_engine_kernel<true, false, true> : rgpu_engine_kernel<true, false, false>;
+  return flex ? rgpu_engine_kernel<false, false, true> : rgpu_engine_kernel<false, false, false>;
+}
+
+cudaError_t rgpu_engine_prepare(int mixed, bool wide, bool flex, size_t smem)
+{
+  return cudaFuncSetAttribute(engine_kernel(mixed, wide, flex), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
-                               int threads, bool wide, cudaStream_t st)
+                               int threads, bool wide, bool flex, cudaStream_t st)
 {
   size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items, threads);
   cudaLaunchConfig_t cfg = {};
@@ -1377,19 +1386,10 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e;
   /* the dynamic shared-memory limit is raised by rgpu_engine_prepare, outside
    * any stream capture */
-  if (mixed && wide)
-    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true, true>, d_systems, nsys, nsteps, kw, max_ads_atoms,
-                           fw_items, tile_items, k_items);
-  else if (mixed)
-    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<true, false>, d_systems, nsys, nsteps, kw, max_ads_atoms,
-                           fw_items, tile_items, k_items);
-  else
-    e = cudaLaunchKernelEx(&cfg, rgpu_engine_kernel<false, false>, d_systems, nsys, nsteps, kw, max_ads_atoms,
-                           fw_items, tile_items, k_items);
-  return e;
+  return cudaLaunchKernelEx(&cfg, engine_kernel(mixed, wide, flex), d_systems, nsys, nsteps, kw, max_ads_atoms,
+                            fw_items, tile_items, k_items);
 }
 
 struct CallSmem {

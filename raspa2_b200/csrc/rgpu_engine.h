@@ -13,11 +13,12 @@
 size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tile_items, int max_ads_atoms, int kw, int k_items,
                               int threads);
 /* raises the kernel's dynamic shared-memory limit to `smem` (call before a
- * launch or a capture of one) */
-cudaError_t rgpu_engine_prepare(int mixed, bool wide, size_t smem);
+ * launch or a capture of one); flex selects the build with flexible-chain
+ * moves and energy grids */
+cudaError_t rgpu_engine_prepare(int mixed, bool wide, bool flex, size_t smem);
 cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long long nsteps, int kw,
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
-                               int threads, bool wide, cudaStream_t st);
+                               int threads, bool wide, bool flex, cudaStream_t st);
 cudaError_t rgpu_point_energies_launch(int mixed, const RgpuSys *d_sys, const void *d_ads, int nads,
                                        const double *d_xyz, const int *d_atom, const int *d_excl, int P,
                                        int pair_check, double *d_out, int *d_ov, cudaStream_t st);
