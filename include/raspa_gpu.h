@@ -166,8 +166,20 @@ int rgpu_intra_energy(rgpu_system *sys, double *out);
  * (nx+1)(ny+1)(nz+1)*8 floats. */
 int rgpu_grid_build(rgpu_system *sys, int type, const int npts[3], const double size[3],
                     const double shift[3], float *d_grid);
+/* The Coulomb grid (MakeGrid's electrostatic part, src/grids.c:586-690,
+ * with CalculateDerivativesAtPositionReal, src/framework_hessian.c:111-180):
+ * the real-space Ewald energy K q_fw erfc(alpha r)/r of a unit probe charge
+ * with the framework, with the same 8 values per point and the same layout
+ * as rgpu_grid_build; a point within 1 A of a framework atom, or above the
+ * overlap criterion, is capped as the reference caps it. Needs Ewald. The
+ * reference makes the point counts odd (int(size/spacing), +1 if even). */
+int rgpu_grid_build_coulomb(rgpu_system *sys, const int npts[3], const double size[3], const double shift[3],
+                            float *d_grid);
 /* InterpolateVDWGrid (src/grids.c:979-1077) at n points (host arrays),
- * reading the device grid; cell = the unit-cell lengths the grid spans. */
+ * reading the device grid; cell = the unit-cell lengths the grid spans.
+ * The same lookup serves a Coulomb grid (InterpolateCoulombGrid,
+ * src/grids.c:1200-1295, before the multiplication by the bead charge): its
+ * capped points hold 2e7, below the VDW lookup's 1e10 corner test. */
 int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3], const double shift[3],
                           const double cell[3], int n, const double *xyz, double *out);
 
@@ -192,12 +204,21 @@ int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const 
  * that atom's pseudo-atom type; atoms of one type can share a grid) instead
  * of the pair sum over the framework, as the reference does with
  * UseTabularGrid (src/grids.c:979, called from src/framework_energy.c).
- * npts/size/shift/cell as rgpu_grid_interpolate; the molecule must be
- * uncharged. d_grids = NULL switches the grids off. Takes effect for
+ * npts/size/shift/cell as rgpu_grid_interpolate; a charged molecule needs a
+ * Coulomb grid (rgpu_system_set_coulomb_grid) set first. d_grids = NULL switches the grids off. Takes effect for
  * engines created afterwards; rgpu_bead_energies and rgpu_total_energy
  * keep the direct pair sums. */
 int rgpu_system_set_grids(rgpu_system *sys, const float *const *d_grids, const int npts[3], const double size[3],
                           const double shift[3], const double cell[3]);
+/* The Coulomb grid of the engine (a grid of rgpu_grid_build_coulomb): the
+ * host real-space charge energy of a bead becomes its charge times the
+ * lookup, as the reference's grid framework model does
+ * (src/framework_energy.c:195-198, :5437-5438); the Fourier part stays
+ * ΔS(k). Set it before rgpu_system_set_grids when the molecule is charged.
+ * d_grid = NULL removes it (refused while VDW grids of a charged molecule
+ * are on). */
+int rgpu_system_set_coulomb_grid(rgpu_system *sys, const float *d_grid, const int npts[3], const double size[3],
+                                 const double shift[3], const double cell[3]);
 
 /* ---- persistent batched engine ------------------------------------------ */
 /* Groups systems for one persistent launch; each system is advanced by one

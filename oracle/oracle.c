@@ -54,18 +54,29 @@ static int grid_vdw(const or_sys *s, int type, const double *p, double *e)
   return 1;
 }
 
+/* the framework real-space charge energy of charge q at p from the Coulomb
+ * grid (InterpolateCoulombGrid, src/grids.c:1200-1295); 0 when none */
+static int grid_coul(const or_sys *s, double q, const double *p, double *e)
+{
+  if (!s->coul_grid || !s->ewald) return 0;
+  *e = q == 0.0 ? 0.0 : q * or_grid_interpolate(s->coul_grid, s->coul_npts, s->coul_size, s->coul_shift,
+                                                s->coul_cell, p);
+  return 1;
+}
+
 /* ---------------------------------------------------------------------- */
 void or_point_energy(const or_sys *s, int type, double q, const double *p, int exclude,
                      double *out)
 {
   double d[3];
   double uv = 0.0, uc = 0.0, av = 0.0, ac = 0.0;
-  /* framework VDW: src/framework_energy.c:151-170 (grid: :60-75); charge: :258-279 */
+  /* framework VDW: src/framework_energy.c:151-170 (grid: :60-75); charge: :258-279 (grid: :195-198) */
   const int gv = grid_vdw(s, type, p, &uv);
+  const int gc = grid_coul(s, q, p, &uc);
   for (int i = 0; i < s->nfw; i++) {
     double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
     if (!gv && r2 < s->rc2_vdw) uv += or_lj(s, type, s->fw_type[i], r2);
-    if (s->ewald && q != 0.0 && r2 < s->rc2_cc) uc += or_real_ewald(s, q, s->fw_q[i], sqrt(r2));
+    if (!gc && s->ewald && q != 0.0 && r2 < s->rc2_cc) uc += or_real_ewald(s, q, s->fw_q[i], sqrt(r2));
   }
   /* other adsorbates: src/inter_energy.c:365-388, :455-480 */
   for (int m = 0; m < s->nmol; m++) {
@@ -186,8 +197,15 @@ int or_move_delta(const or_sys *s, int m, const double *new_xyz, double *out)
       if (r2 < s->rc2_vdw) dhv -= or_lj(s, ta, s->fw_type[i], r2);
     }
   }
-  /* framework charge-charge */
-  if (s->ewald) {
+  /* framework charge-charge (grid: src/framework_energy.c:5437-5438, :5506) */
+  if (s->ewald && s->coul_grid) {
+    for (int a = 0; a < s->natom; a++) {
+      double en = 0.0, eo = 0.0;
+      grid_coul(s, s->mol_q[a], new_xyz + 3 * a, &en);
+      grid_coul(s, s->mol_q[a], old_xyz + 3 * a, &eo);
+      dhc += en - eo;
+    }
+  } else if (s->ewald) {
     for (int a = 0; a < s->natom; a++) {
       double qa = s->mol_q[a];
       if (qa == 0.0) continue;
@@ -402,13 +420,15 @@ void or_total_energy(const or_sys *s, double *out)
       const double *p = s->ads_xyz + 3 * (m * s->natom + a);
       int ta = s->mol_type[a];
       double qa = s->mol_q[a];
-      double g;
+      double g, gq;
       const int gv = grid_vdw(s, ta, p, &g);
       if (gv) hv += g;
+      const int gc = grid_coul(s, qa, p, &gq);
+      if (gc) hc += gq;
       for (int i = 0; i < s->nfw; i++) {
         double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
         if (!gv && r2 < s->rc2_vdw) hv += or_lj(s, ta, s->fw_type[i], r2);
-        if (s->ewald && qa != 0.0 && r2 < s->rc2_cc) hc += or_real_ewald(s, qa, s->fw_q[i], sqrt(r2));
+        if (!gc && s->ewald && qa != 0.0 && r2 < s->rc2_cc) hc += or_real_ewald(s, qa, s->fw_q[i], sqrt(r2));
       }
       for (int j = m + 1; j < s->nmol; j++)
         for (int b = 0; b < s->natom; b++) {
@@ -1021,6 +1041,75 @@ static inline void hermite(double t, double *h)
   h[1] = 3.0 * t2 - 2.0 * t3;         /* p1 */
   h[2] = t - 2.0 * t2 + t3;           /* d0 */
   h[3] = -t2 + t3;                    /* d1 */
+}
+
+/* The real-space Ewald term f(r) = K q erfc(alpha r) / r of a unit probe
+ * charge and its radial derivative factors: d f/dx_i = x_i DF,
+ * d2 f/dx_i dx_j = x_i x_j DDF (+ DF for i = j), d3 f/dx dy dz = x y z DDDF
+ * (src/framework_hessian.c:142-160). */
+void or_grid_derivatives_real(const or_sys *s, const double *p, double *o)
+{
+  double d[3];
+  double rmin = 1e300;
+  for (int k = 0; k < 8; k++) o[k] = 0.0;
+  const double a2 = s->alpha * s->alpha, c = 2.0 * s->alpha / sqrt(M_PI);
+  for (int i = 0; i < s->nfw; i++) {
+    double r2 = dist2(s, p, s->fw_xyz + 3 * i, d);
+    if (r2 >= s->rc2_cc) continue;
+    double r = sqrt(r2);
+    if (r < rmin) rmin = r;
+    double kq = s->coulomb * s->fw_q[i];
+    double e = erfc(s->alpha * r), g = c * r * exp(-a2 * r2), x = a2 * r2;
+    double F = kq * e / r;
+    double DF = -kq * (g + e) / (r * r2);
+    double DDF = kq * (g * (3.0 + 2.0 * x) + 3.0 * e) / (r2 * r2 * r);
+    double DDDF = -kq * (g * (15.0 + 10.0 * x + 4.0 * x * x) + 15.0 * e) / (r2 * r2 * r2 * r);
+    o[0] += F;
+    o[1] += d[0] * DF;
+    o[2] += d[1] * DF;
+    o[3] += d[2] * DF;
+    o[4] += DDF * d[0] * d[1];
+    o[5] += DDF * d[0] * d[2];
+    o[6] += DDF * d[1] * d[2];
+    o[7] += DDDF * d[0] * d[1] * d[2];
+  }
+  o[8] = rmin;
+}
+
+/* src/grids.c:586-690: as or_grid_build, capped where the value exceeds the
+ * overlap criterion or a framework atom is within 1 A (:656-668) */
+void or_grid_build_coulomb(const or_sys *s, const int npts[3], const double size[3], const double shift[3],
+                           float *grid)
+{
+  const int nx = npts[0] + 1, ny = npts[1] + 1, nz = npts[2] + 1;
+  const size_t plane = (size_t)nx * ny * nz;
+  double delta[3];
+  for (int c = 0; c < 3; c++) delta[c] = size[c] / (double)npts[c];
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        double p[3] = {i * size[0] / npts[0] + shift[0], j * size[1] / npts[1] + shift[1],
+                       k * size[2] / npts[2] + shift[2]};
+        double o[9];
+        or_grid_derivatives_real(s, p, o);
+        if (o[0] > s->overlap || o[8] < 1.0) {
+          o[0] = 2.0 * s->overlap;
+          for (int c = 1; c <= 3; c++) {
+            if (o[c] > s->overlap) o[c] = s->overlap;
+            if (o[c] < -s->overlap) o[c] = -s->overlap;
+          }
+          o[4] = o[5] = o[6] = o[7] = 0.0;
+        }
+        size_t idx = ((size_t)i * ny + j) * nz + k;
+        grid[0 * plane + idx] = (float)o[0];
+        grid[1 * plane + idx] = (float)o[1] * delta[0];
+        grid[2 * plane + idx] = (float)o[2] * delta[1];
+        grid[3 * plane + idx] = (float)o[3] * delta[2];
+        grid[4 * plane + idx] = (float)o[4] * (delta[0] * delta[1]);
+        grid[5 * plane + idx] = (float)o[5] * (delta[0] * delta[2]);
+        grid[6 * plane + idx] = (float)o[6] * (delta[1] * delta[2]);
+        grid[7 * plane + idx] = (float)o[7] * (delta[0] * delta[1] * delta[2]);
+      }
 }
 
 /* InterpolateVDWGrid (src/grids.c:979-1077). The reference solves for the 64

@@ -59,6 +59,12 @@ typedef struct {
   const float *const *grid;             /* [ntypes] or NULL */
   int grid_npts[3];
   double grid_size[3], grid_shift[3], grid_cell[3];
+  /* Coulomb grid of a unit probe charge (or_grid_build_coulomb): when set,
+   * a bead's framework real-space charge energy is its charge times the
+   * lookup (src/framework_energy.c:195-198), with no overlap test */
+  const float *coul_grid;
+  int coul_npts[3];
+  double coul_size[3], coul_shift[3], coul_cell[3];
 } or_sys;
 
 /* pair terms */
@@ -120,6 +126,13 @@ void or_cbmc_retrace(const or_sys *s, int m, int ntrial_first, int ntrial, or_rn
 void or_grid_derivatives(const or_sys *s, int type, const double *p, double *out8);
 void or_grid_build(const or_sys *s, int type, const int npts[3], const double size[3],
                    const double shift[3], float *grid /* [8][nx+1][ny+1][nz+1] */);
+/* CalculateDerivativesAtPositionReal (src/framework_hessian.c:111-180) for a
+ * unit probe charge: out = the 8 values of or_grid_derivatives, then the
+ * smallest distance to a framework atom within the cut-off */
+void or_grid_derivatives_real(const or_sys *s, const double *p, double *out9);
+/* the Coulomb grid (src/grids.c:586-690), layout as or_grid_build */
+void or_grid_build_coulomb(const or_sys *s, const int npts[3], const double size[3], const double shift[3],
+                           float *grid);
 double or_grid_interpolate(const float *grid, const int npts[3], const double size[3],
                            const double shift[3], const double cell[3], const double *p);
 

@@ -33,6 +33,8 @@ class OrSys(C.Structure):
         ("bend_sigma", C.c_double), ("torsion", C.c_double * 4), ("torsion_min", C.c_double),
         ("grid", C.POINTER(C.POINTER(C.c_float))), ("grid_npts", C.c_int * 3), ("grid_size", C.c_double * 3),
         ("grid_shift", C.c_double * 3), ("grid_cell", C.c_double * 3),
+        ("coul_grid", C.POINTER(C.c_float)), ("coul_npts", C.c_int * 3), ("coul_size", C.c_double * 3),
+        ("coul_shift", C.c_double * 3), ("coul_cell", C.c_double * 3),
     ]
 
 
@@ -166,6 +168,31 @@ class Oracle:
 
     def intra_energy(self):
         return lib().or_intra_energy(C.byref(self.s))
+
+    def set_coulomb_grid(self, grid, npts=None, size=None, shift=None, cell=None):
+        """grid: plane-major Coulomb grid of a unit probe charge; None removes it."""
+        if grid is None:
+            self.s.coul_grid = None
+            self._coul = None
+            return
+        self._coul = np.ascontiguousarray(grid, np.float32)
+        self.s.coul_grid = self._coul.ctypes.data_as(C.POINTER(C.c_float))
+        self.s.coul_npts[:] = [int(x) for x in npts]
+        self.s.coul_size[:] = [float(x) for x in size]
+        self.s.coul_shift[:] = [float(x) for x in shift]
+        self.s.coul_cell[:] = [float(x) for x in cell]
+
+    def grid_derivatives_real(self, p):
+        out = np.zeros(9)
+        lib().or_grid_derivatives_real(C.byref(self.s), _ptr(np.ascontiguousarray(p, float)), _ptr(out))
+        return out
+
+    def grid_build_coulomb(self, npts, size, shift):
+        npts = np.asarray(npts, np.int32)
+        g = np.zeros((8, npts[0] + 1, npts[1] + 1, npts[2] + 1), np.float32)
+        lib().or_grid_build_coulomb(C.byref(self.s), _ptr(npts, _ip), _ptr(np.asarray(size, float)),
+                                    _ptr(np.asarray(shift, float)), g.ctypes.data_as(C.POINTER(C.c_float)))
+        return g
 
     def set_grids(self, grids, npts, size, shift, cell):
         """grids: {pseudo-atom type: plane-major grid (8, nx+1, ny+1, nz+1)}

@@ -31,6 +31,11 @@
  *                          (src/framework_hessian.c:63)
  *   interp T x y z         InterpolateVDWGrid (src/grids.c:979); needs
  *                          UseTabularGrid and a grid file in the run directory
+ *   derivreal x y z        CalculateDerivativesAtPositionReal
+ *                          (src/framework_hessian.c:111), unit probe charge;
+ *                          prints the smallest distance last
+ *   interpc T x y z        InterpolateCoulombGrid (src/grids.c:1200) for
+ *                          pseudo-atom T (its charge times the grid value)
  *   makegrid               MakeGrid (src/grids.c:431); writes the grid files
  *                          and (as the reference does) ends the process
  *
@@ -362,6 +367,21 @@ int main(int argc, char **argv)
       CalculateDerivativesAtPositionVDW(p, (int)v[0], &val, &d1, &d2, &d3);
       double r[8] = {val, d1.x, d1.y, d1.z, d2.ay, d2.az, d2.bz, d3};
       p1("deriv", 8, r);
+    } else if (!strcmp(cmd, "derivreal")) {
+      int n = parse_doubles(rest, v, 8);
+      if (n != 3) return 3;
+      VECTOR p = {v[0], v[1], v[2]}, d1;
+      REAL val, d3;
+      REAL_MATRIX3x3 d2;
+      REAL rmin = CalculateDerivativesAtPositionReal(p, 0, &val, &d1, &d2, &d3);
+      double r[9] = {val, d1.x, d1.y, d1.z, d2.ay, d2.az, d2.bz, d3, rmin};
+      p1("derivreal", 9, r);
+    } else if (!strcmp(cmd, "interpc")) {
+      int n = parse_doubles(rest, v, 8);
+      if (n != 4) return 3;
+      VECTOR p = {v[1], v[2], v[3]};
+      double r = InterpolateCoulombGrid((int)v[0], p);
+      p1("interpc", 1, &r);
     } else if (!strcmp(cmd, "interp")) {
       int n = parse_doubles(rest, v, 8);
       if (n != 4) return 3;

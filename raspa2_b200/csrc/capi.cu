@@ -857,6 +857,35 @@ extern "C" int rgpu_ewald_accept(rgpu_system *s)
 
 static bool grid_covers_cell(const int npts[3], const double size[3], const double shift[3], const double cell[3]);
 
+extern "C" int rgpu_system_set_coulomb_grid(rgpu_system *s, const float *d_grid, const int npts[3],
+                                            const double size[3], const double shift[3], const double cell[3])
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  RgpuSys &h = s->h;
+  if (!d_grid) {
+    if (h.use_grid && h.mol_charged)
+      return fail(RGPU_E_INVALID, "the VDW grids of a charged molecule stay on: switch them off first");
+    h.use_coul_grid = 0;
+    h.coul_grid = nullptr;
+  } else {
+    if (!npts || !size || !shift || !cell) return fail(RGPU_E_INVALID, "bad argument");
+    if (!h.ewald) return fail(RGPU_E_INVALID, "a Coulomb grid needs Ewald summation");
+    if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "grids must be 16-byte aligned");
+    if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
+    for (int c = 0; c < 3; c++) {
+      h.coul_geom.npts[c] = npts[c];
+      h.coul_geom.size[c] = size[c];
+      h.coul_geom.shift[c] = shift[c];
+      h.coul_geom.cell[c] = cell[c];
+    }
+    h.coul_grid = d_grid;
+    h.use_coul_grid = 1;
+  }
+  CK(cudaMemcpyAsync(s->d_sys, &h, sizeof(RgpuSys), cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
 extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids, const int npts[3],
                                      const double size[3], const double shift[3], const double cell[3])
 {
@@ -867,8 +896,8 @@ extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids
     for (int a = 0; a < RGPU_MAX_ATOMS; a++) h.grid[a] = nullptr;
   } else {
     if (!npts || !size || !shift || !cell) return fail(RGPU_E_INVALID, "bad argument");
-    if (h.mol_charged)
-      return fail(RGPU_E_INVALID, "grids replace the host VDW pair sums only: the molecule must be uncharged");
+    if (h.mol_charged && !h.use_coul_grid)
+      return fail(RGPU_E_INVALID, "a charged molecule needs a Coulomb grid (rgpu_system_set_coulomb_grid) first");
     if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
     for (int a = 0; a < h.natom; a++) {
       if (!d_grids[a]) return fail(RGPU_E_INVALID, "no grid for molecule atom %d", a);
@@ -976,6 +1005,19 @@ extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], cons
     lj[sg].shift = s->lj_shift[ij];
   }
   CK(rgpu_grid_build_launch_lj(s->d_sys, lj, npts, size, shift, d_grid, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_grid_build_coulomb(rgpu_system *s, const int npts[3], const double size[3],
+                                       const double shift[3], float *d_grid)
+{
+  if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
+  if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
+  if (!s->h.ewald) return fail(RGPU_E_INVALID, "a Coulomb grid needs Ewald summation");
+  for (int c = 0; c < 3; c++)
+    if (npts[c] < 1) return fail(RGPU_E_INVALID, "npts");
+  CK(rgpu_grid_build_launch_coulomb(s->d_sys, npts, size, shift, d_grid, s->st));
   CK(cudaStreamSynchronize(s->st));
   return RGPU_SUCCESS;
 }
@@ -1125,6 +1167,10 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
     rgpu_system *s = systems[i];
     if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
     e->sys.push_back(s);
+    if (s->h.use_grid && s->h.mol_charged && !s->h.use_coul_grid) {
+      delete e;
+      return fail(RGPU_E_INVALID, "system with VDW grids and a charged molecule but no Coulomb grid");
+    }
     all_grids = all_grids && s->h.use_grid;
     e->flex = e->flex || s->h.use_grid || s->h.flexible;
     e->kw = std::max(e->kw, s->kw);

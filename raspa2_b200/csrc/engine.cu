@@ -118,6 +118,7 @@ struct Ctl {
   int next;                   /* unit counter of eval_units */
   double ewt[2][2];           /* this CTA's Ewald sums {e_ads, e_host}, by buffer */
   double gv[RGPU_MAX_POS];    /* grid host VDW of the positions of the current evaluation */
+  double gq[RGPU_MAX_POS];    /* grid host real-space charge energy of the positions */
 };
 static_assert(sizeof(Ctl) <= RGPU_CTL_BYTES, "control block exceeds its shared-memory slot");
 
@@ -235,6 +236,13 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair
       const double x[3] = {live ? E.pos[p].x : 0.0, live ? E.pos[p].y : 0.0, live ? E.pos[p].z : 0.0};
       const double g = rgpu_grid_value8(E.S->grid[live ? E.pos[p].atom : 0], E.S->grid_geom, x, lane & 7, live);
       if (live && (lane & 7) == 0) C.gv[p] = g;
+      if (E.S->use_coul_grid) {
+        /* real-space charge energy: the bead charge times the unit-charge
+         * Coulomb grid (InterpolateCoulombGrid, src/grids.c:1200) */
+        const double q = live ? E.S->mol_q[E.pos[p].atom] : 0.0;
+        const double gq = rgpu_grid_value8(E.S->coul_grid, E.S->coul_geom, x, lane & 7, live && q != 0.0, false);
+        if (live && (lane & 7) == 0) C.gq[p] = q * gq;
+      }
     }
   }
   const EvalPlan pl = eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.sc, RGPU_MAX_UNITS);
@@ -256,6 +264,7 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair
       const double g = C.gv[p];
       hv += g;
       ov |= g >= E.S->overlap;
+      if (E.S->use_coul_grid) hc += C.gq[p];
     }
     ps[p].v[0] = hv; ps[p].v[1] = hc; ps[p].v[2] = av; ps[p].v[3] = ac;
     ps[p].ov = ov;

@@ -36,6 +36,12 @@ struct GridParams {
   RgpuLJ lj[RGPU_MAX_FWTYPES];
 };
 
+/* COUL = false: the LJ grid of one probe pseudo-atom (gp.lj by framework
+ * segment). COUL = true: the real-space Ewald (Coulomb) grid of a unit probe
+ * charge, CalculateDerivativesAtPositionReal (src/framework_hessian.c:111-180)
+ * with the framework charges, capped where the value exceeds the overlap
+ * criterion or a framework atom is closer than 1 A (src/grids.c:656-668). */
+template <bool COUL>
 __global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp, GridParams gp, float *grid)
 {
   __shared__ double4 fwc[GRID_THREADS];
@@ -66,6 +72,8 @@ __global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp
   const double Lx = S.box[0], Ly = S.box[1], Lz = S.box[2];
   const double ix = S.inv_box[0], iy = S.inv_box[1], iz = S.inv_box[2];
   double o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double rmin2 = 1e300;
+  const double a2 = S.alpha * S.alpha, two_a_sqrtpi = 2.0 * S.alpha / sqrt(M_PI);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int base = 0; base < S.nfw; base += GRID_THREADS) {
     const int a = base + threadIdx.x;
@@ -105,14 +113,28 @@ __global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp
         dz -= Lz * rgpu_nint(dz * iz);
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < S.rc2) {
-          const RgpuLJ P = gp.lj[segc[q]];
-          const double eps = 0.25 * P.eps4;
-          double r3 = P.sig2 / r2;
-          r3 = r3 * r3 * r3;
-          const double U = 4.0 * eps * (r3 * (r3 - 1.0)) - P.shift;
-          const double DF = 24.0 * eps * (r3 * (1.0 - 2.0 * r3)) / r2;
-          const double DDF = 96.0 * eps * (r3 * (7.0 * r3 - 2.0)) / (r2 * r2);
-          const double DDDF = 384.0 * eps * (r3 * (5.0 - 28.0 * r3)) / (r2 * r2 * r2 * r2);
+          double U, DF, DDF, DDDF;
+          if (COUL) {
+            /* f(r) = K q erfc(a r) / r; DF = f'/r, DDF = (f'' - f'/r)/r^2,
+             * DDDF = the r-part of the mixed third derivative */
+            rmin2 = fmin(rmin2, r2);
+            const double r = sqrt(r2), kq = S.coulomb * g.w;
+            const double e = erfc(S.alpha * r), gr = two_a_sqrtpi * r * exp(-a2 * r2);
+            const double ar2 = a2 * r2;
+            U = kq * e / r;
+            DF = -kq * (gr + e) / (r * r2);
+            DDF = kq * (gr * (3.0 + 2.0 * ar2) + 3.0 * e) / (r2 * r2 * r);
+            DDDF = -kq * (gr * (15.0 + 10.0 * ar2 + 4.0 * ar2 * ar2) + 15.0 * e) / (r2 * r2 * r2 * r);
+          } else {
+            const RgpuLJ P = gp.lj[segc[q]];
+            const double eps = 0.25 * P.eps4;
+            double r3 = P.sig2 / r2;
+            r3 = r3 * r3 * r3;
+            U = 4.0 * eps * (r3 * (r3 - 1.0)) - P.shift;
+            DF = 24.0 * eps * (r3 * (1.0 - 2.0 * r3)) / r2;
+            DDF = 96.0 * eps * (r3 * (7.0 * r3 - 2.0)) / (r2 * r2);
+            DDDF = 384.0 * eps * (r3 * (5.0 - 28.0 * r3)) / (r2 * r2 * r2 * r2);
+          }
           o[0] += U;
           o[1] += dx * DF;
           o[2] += dy * DF;
@@ -127,8 +149,8 @@ __global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp
     __syncthreads();
   }
   if (!valid) return;
-  /* cap, src/grids.c:546-563 */
-  if (o[0] > S.overlap) {
+  /* cap, src/grids.c:546-563 (Coulomb: also within 1 A of an atom, :656-668) */
+  if (o[0] > S.overlap || (COUL && rmin2 < 1.0)) {
     o[0] = 2.0 * S.overlap;
     for (int c = 1; c <= 3; c++) {
       if (o[c] > S.overlap) o[c] = S.overlap;
@@ -161,7 +183,26 @@ cudaError_t rgpu_grid_build_launch_lj(const RgpuSys *d_sys, const RgpuLJ *lj, co
   const long long blocks = (long long)((nx + GRID_TX - 1) / GRID_TX) * ((ny + GRID_TY - 1) / GRID_TY) *
                            ((nz + GRID_TZ - 1) / GRID_TZ);
   if (blocks > 2147483647LL) return cudaErrorInvalidValue;
-  k_grid_build<<<(unsigned)blocks, GRID_THREADS, 0, st>>>(d_sys, gp, d_grid);
+  k_grid_build<false><<<(unsigned)blocks, GRID_THREADS, 0, st>>>(d_sys, gp, d_grid);
+  return cudaGetLastError();
+}
+
+/* the Coulomb grid of a unit probe charge */
+cudaError_t rgpu_grid_build_launch_coulomb(const RgpuSys *d_sys, const int npts[3], const double size[3],
+                                           const double shift[3], float *d_grid, cudaStream_t st)
+{
+  GridParams gp = {};
+  for (int c = 0; c < 3; c++) {
+    gp.npts[c] = npts[c];
+    gp.size[c] = size[c];
+    gp.shift[c] = shift[c];
+    gp.delta[c] = size[c] / (double)npts[c];
+  }
+  const int nx = npts[0] + 1, ny = npts[1] + 1, nz = npts[2] + 1;
+  const long long blocks = (long long)((nx + GRID_TX - 1) / GRID_TX) * ((ny + GRID_TY - 1) / GRID_TY) *
+                           ((nz + GRID_TZ - 1) / GRID_TZ);
+  if (blocks > 2147483647LL) return cudaErrorInvalidValue;
+  k_grid_build<true><<<(unsigned)blocks, GRID_THREADS, 0, st>>>(d_sys, gp, d_grid);
   return cudaGetLastError();
 }
 

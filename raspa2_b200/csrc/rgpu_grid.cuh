@@ -77,9 +77,10 @@ __device__ __forceinline__ double rgpu_grid_value(const float *grid, const RgpuG
  * lookup costs one memory round trip instead of eight. Every lane of the
  * group returns the value (the same polynomial as rgpu_grid_value, summed in
  * another order). A group with live = false only takes part in the
- * shuffles. */
+ * shuffles. cap: the VDW lookup's 1e8 for a corner above 1e10; the Coulomb
+ * lookup (InterpolateCoulombGrid, src/grids.c:1200-1295) has none. */
 __device__ __forceinline__ double rgpu_grid_value8(const float *grid, const RgpuGridGeom &ip, const double *xyz,
-                                                   int lane8, bool live)
+                                                   int lane8, bool live, bool cap = true)
 {
   double val = 0.0;
   int big = 0;
@@ -118,7 +119,7 @@ __device__ __forceinline__ double rgpu_grid_value8(const float *grid, const Rgpu
     val += __shfl_xor_sync(0xffffffffu, val, o);
     big |= __shfl_xor_sync(0xffffffffu, big, o);
   }
-  return big ? 1e8 : val;
+  return (cap && big) ? 1e8 : val;
 }
 
 #endif

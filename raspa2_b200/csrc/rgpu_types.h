@@ -158,9 +158,11 @@ typedef struct RgpuSys {
   /* energy grids (rgpu_system_set_grids): the engine takes the host VDW
    * energy of molecule atom a from grid[a] instead of the pair sums */
   int use_grid;
-  int pad_grid;
+  int use_coul_grid;          /* host real-space charge energy from coul_grid (x the bead charge) */
   RgpuGridGeom grid_geom;
   const float *grid[RGPU_MAX_ATOMS];
+  RgpuGridGeom coul_geom;
+  const float *coul_grid;     /* Coulomb grid of a unit probe charge (rgpu_system_set_coulomb_grid) */
   /* device pointers */
   const double4 *fw64;        /* [nfw] x, y, z, q (sorted by type) */
   const int4 *fw32;           /* [ntile*RGPU_TILE] tiled: fixed-point x, y, z (low 2 bits of z = segment), float bits of q */

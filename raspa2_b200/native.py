@@ -32,6 +32,7 @@ EXPORTS = [
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
     "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_intra_energy",
     "rgpu_system_set_grids", "rgpu_system_checkpoint_size", "rgpu_system_checkpoint", "rgpu_system_restore",
+    "rgpu_grid_build_coulomb", "rgpu_system_set_coulomb_grid",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -283,18 +284,32 @@ class GpuSystem:
                 torch.cuda.synchronize()
                 self.grid_build(t, npts, uc, shift, buf.data_ptr())
                 bufs[t] = buf
+            if np.any(self.sysm.molecule.charges() != 0.0):
+                # the Coulomb grid: odd point counts (src/grids.c:588-594)
+                nc = npts + (npts % 2 == 0)
+                buf = torch.empty(int(np.prod(nc.astype(np.int64) + 1)) * 8, dtype=torch.float32, device="cuda")
+                torch.cuda.synchronize()
+                self.grid_build_coulomb(nc, uc, shift, buf.data_ptr())
+                bufs["coulomb"] = (buf, nc)
         self._grids = bufs
         self._grid_geom = (npts, uc, shift, uc)
-        self.set_grids([bufs[t].data_ptr() for t in types], npts, uc, shift, uc)
+        self._apply_grids()
         return self._grid_geom
+
+    def _apply_grids(self):
+        types = [int(t) for t in self.sysm.molecule_types()]
+        npts, uc, shift, cell = self._grid_geom
+        if "coulomb" in self._grids:
+            buf, nc = self._grids["coulomb"]
+            self.set_coulomb_grid(buf.data_ptr(), nc, uc, shift, cell)
+        self.set_grids([self._grids[t].data_ptr() for t in types], npts, uc, shift, cell)
 
     def share_grids_of(self, other: "GpuSystem"):
         """Uses the grids `other` uses (a system of the same framework and
         molecule)."""
         self._grids = other._grids
         self._grid_geom = other._grid_geom
-        types = [int(t) for t in self.sysm.molecule_types()]
-        self.set_grids([self._grids[t].data_ptr() for t in types], *self._grid_geom)
+        self._apply_grids()
 
     def intra_energy(self) -> float:
         """Intramolecular energy of flexible chains (rgpu_intra_energy)."""
@@ -354,6 +369,21 @@ class GpuSystem:
         _check(load().rgpu_system_set_energy(self.h, e.ctypes.data_as(_dp)))
 
     # ---- grids --------------------------------------------------------------
+    def grid_build_coulomb(self, npts, size, shift, d_grid_ptr: int):
+        n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64)
+        _check(load().rgpu_grid_build_coulomb(self.h, n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),
+                                              sh.ctypes.data_as(_dp), C.c_void_p(d_grid_ptr)))
+
+    def set_coulomb_grid(self, d_grid_ptr, npts=None, size=None, shift=None, cell=None):
+        """rgpu_system_set_coulomb_grid; None removes it."""
+        L = load()
+        if d_grid_ptr is None:
+            _check(L.rgpu_system_set_coulomb_grid(self.h, None, None, None, None, None))
+            return
+        n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64); ce = _arr(cell, np.float64)
+        _check(L.rgpu_system_set_coulomb_grid(self.h, C.c_void_p(d_grid_ptr), n.ctypes.data_as(_ip),
+                                              s.ctypes.data_as(_dp), sh.ctypes.data_as(_dp), ce.ctypes.data_as(_dp)))
+
     def grid_build(self, type_: int, npts, size, shift, d_grid_ptr: int):
         n = _arr(npts, np.int32); s = _arr(size, np.float64); sh = _arr(shift, np.float64)
         _check(load().rgpu_grid_build(self.h, C.c_int(type_), n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),

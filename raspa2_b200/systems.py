@@ -40,6 +40,8 @@ PSEUDO_ATOMS = {
     "CH2_sp3":  (46.0,   3.95,   0.0,    14.02658),
     # no interaction: the single atom of an otherwise empty box
     "Dummy":    (0.0,    1.00,   0.0,    1.0),
+    # unit probe charge of the Coulomb grid (the reference's "UNIT", src/grids.c:637)
+    "UNIT":     (0.0,    1.00,   1.0,    1.0),
 }
 TYPE_ORDER = list(PSEUDO_ATOMS.keys())
 

@@ -7,7 +7,8 @@ own energy, Ewald, CBMC and grid routines) and stores inputs and outputs as
 small JSON files. The committed JSON is what the tests read; nothing at test
 time needs the reference.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py coulomb    # only grid_co2_coulomb.json
 """
 from __future__ import annotations
 
@@ -225,9 +226,75 @@ def grid_case(seed=0, spacing=1.0):
     }
 
 
+def read_coulomb_grid_file(path):
+    """The Coulomb grid file (src/grids.c:856-869): the VDW header, then the
+    Ewald precision, then the 8 planes."""
+    with open(path, "rb") as fh:
+        b = fh.read()
+    spacing = struct.unpack_from("d", b, 0)[0]
+    n = struct.unpack_from("3i", b, 8)
+    off = 8 + 12
+    size = struct.unpack_from("3d", b, off); off += 24
+    shift = struct.unpack_from("3d", b, off); off += 24
+    delta = struct.unpack_from("3d", b, off); off += 24
+    cell = struct.unpack_from("3d", b, off); off += 24
+    ncell = struct.unpack_from("3i", b, off); off += 12
+    prec = struct.unpack_from("d", b, off)[0]; off += 8
+    npts = (n[0] + 1) * (n[1] + 1) * (n[2] + 1)
+    g = np.frombuffer(b, dtype=np.float32, count=8 * npts, offset=off).reshape(8, n[0] + 1, n[1] + 1, n[2] + 1)
+    return {"spacing": spacing, "n": list(n), "size": list(size), "shift": list(shift), "delta": list(delta),
+            "cell": list(cell), "ncell": list(ncell), "ewald_precision": prec}, g
+
+
+def coulomb_grid_case(seed=1, spacing=1.0):
+    """The reference's Coulomb grid of the CO2 framework: derivatives at
+    points, the grid file, and InterpolateCoulombGrid for the CO2 sites."""
+    sysm = systems.co2_system(seed=seed)
+    rng = np.random.default_rng(seed + 199)
+    types = ["C_co2", "O_co2"]
+    with tempfile.TemporaryDirectory() as d:
+        grid = {"types": types, "spacing": spacing}
+        raspa_io.write_inputs(sysm, d, simulation_type="MakeGrid", grid=grid)
+        os.makedirs(os.path.join(d, "share", "raspa", "grids"), exist_ok=True)
+        pts = rng.random((12, 3)) * sysm.unit_cell
+        rows = run_harness(d, [f"derivreal {fmt(p)}" for p in pts] + ["makegrid"])
+        deriv = [list(map(float, r[1:])) for r in rows if r[0] == "derivreal"]
+        a, b, c = (int(x) for x in sysm.unit_cells)
+        gpath = os.path.join(d, "share", "raspa", "grids", "Local", sysm.name, f"{spacing:.6f}", f"{a}x{b}x{c}",
+                             f"{sysm.name}_Electrostatics_Ewald.grid")
+        meta, g = read_coulomb_grid_file(gpath)
+        grid["use"] = True
+        raspa_io.write_inputs(sysm, d, simulation_type="MonteCarlo", grid=grid)
+        q = rng.random((40, 3)) * sysm.box - 0.5 * sysm.box
+        cmds = []
+        for name in types:
+            t = systems.TYPE_ORDER.index(name)
+            cmds += [f"interpc {t + 1} {fmt(p)}" for p in q]
+        rows = run_harness(d, cmds)
+        interp = [float(r[1]) for r in rows if r[0] == "interpc"]
+    sel = rng.integers(0, g[0].size, 64)
+    flat = g.reshape(8, -1)
+    return {
+        "name": "grid_co2_coulomb",
+        "system": {"builder": "co2_config1", "seed": seed},
+        "meta": meta, "types": types,
+        "deriv_points": pts.tolist(), "deriv_ref": deriv,
+        "sample_index": sel.tolist(), "sample_values": flat[:, sel].T.astype(float).tolist(),
+        "plane_sums": [float(np.sum(flat[m].astype(np.float64))) for m in range(8)],
+        "plane_abs_sums": [float(np.sum(np.abs(flat[m].astype(np.float64)))) for m in range(8)],
+        "interp_points": q.tolist(), "interp_ref": interp,
+    }
+
+
 def main():
     if not os.path.exists(HARNESS):
         raise SystemExit("build the harness first: make -C oracle ref")
+    if sys.argv[1:] == ["coulomb"]:
+        g = coulomb_grid_case()
+        with open(os.path.join(OUT, "grid_co2_coulomb.json"), "w") as fh:
+            json.dump(g, fh)
+        print("coulomb grid", g["meta"]["n"], len(g["interp_ref"]))
+        return
     cases = {
         "co2_tiny": (systems.tiny_co2_system(), 6, 11),
         "co2_config1": (systems.co2_system(seed=1), 10, 12),
@@ -242,6 +309,10 @@ def main():
     with open(os.path.join(OUT, "grid_methane.json"), "w") as fh:
         json.dump(g, fh)
     print("grid", g["meta"]["n"], len(g["interp_ref"]))
+    g = coulomb_grid_case()
+    with open(os.path.join(OUT, "grid_co2_coulomb.json"), "w") as fh:
+        json.dump(g, fh)
+    print("coulomb grid", g["meta"]["n"], len(g["interp_ref"]))
 
 
 if __name__ == "__main__":
