@@ -274,6 +274,30 @@ int rgpu_system_set_limits(rgpu_system *sys, unsigned long long end_step, unsign
 int rgpu_system_averages(rgpu_system *sys, double *sums8);
 int rgpu_system_reset_averages(rgpu_system *sys);
 
+/* ---- batched state transfer of an engine's systems ------------------------ */
+/* No counterpart in the reference (its state is host memory). The
+ * per-system calls below cost a synchronisation each; these move all
+ * systems of an engine through one pinned staging buffer, with one copy and
+ * one synchronisation per call.
+ *
+ * rgpu_engine_get_state: for system i of the engine (creation order),
+ * energy8[8i..], counters20[20i..], nmol[i], status[i], step[i] as
+ * rgpu_system_state, and its positions into xyz[i] (room for maxmol * natom
+ * * 3 doubles; xyz or xyz[i] may be NULL) as rgpu_get_adsorbates. Any output
+ * pointer may be NULL.
+ *
+ * rgpu_engine_set_adsorbates: as rgpu_set_adsorbates(sys_i, nmol[i],
+ * xyz[i]) for every system: positions, molecule count, the per-call
+ * records and S_ads(k) from the new positions; running energies untouched.
+ *
+ * Both wait for the device first (no engine launch may be in flight). */
+int rgpu_engine_get_state(rgpu_engine *eng, double *energy8, long long *counters20, int *nmol, int *status,
+                          unsigned long long *step, double *const *xyz);
+int rgpu_engine_set_adsorbates(rgpu_engine *eng, const int *nmol, const double *const *xyz);
+/* Bytes each of those calls copies between host and device (the whole
+ * staging buffer: every system's state block and room for maxmol molecules). */
+int rgpu_engine_staging_bytes(rgpu_engine *eng, size_t *bytes);
+
 /* ---- checkpoints (binary crash files) ------------------------------------ */
 /* The counterpart of the binary crash file that ContinueAfterCrash writes
  * and reads (WriteBinaryRestartFiles, src/output.c:7903;

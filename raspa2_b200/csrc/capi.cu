@@ -87,6 +87,7 @@ struct rgpu_system {
   double net_ads, pending_dq;
   int grid_type_seg;
   uint64_t fingerprint;       /* of the model a checkpoint must match (checkpoint_fingerprint) */
+  double *io_q_all;           /* charge of every adsorbate slot (batched uploads), filled at creation */
   std::vector<int> fw_seg_type; /* framework pseudo-atom type of each segment */
   std::vector<double> lj_eps, lj_sig2, lj_shift;
   int ntypes;
@@ -104,6 +105,13 @@ struct rgpu_engine {
   int use_graph;
   cudaGraphExec_t gexec;
   long long g_nsteps;
+  /* staging of the batched state transfer (allocated at first use):
+   * system i's region at off[i], sized for its maxmol */
+  std::vector<unsigned long long> off;
+  size_t stage_bytes;
+  unsigned long long *d_off;
+  unsigned char *d_stage;
+  unsigned char *h_stage;     /* pinned */
 };
 
 static void sys_free(rgpu_system *s)
@@ -111,7 +119,7 @@ static void sys_free(rgpu_system *s)
   if (!s) return;
   void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->tiles_d, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
                   s->state, s->rec32, s->rec64, s->io_xyz,
-                  s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov};
+                  s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov, s->io_q_all};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->st) cudaStreamDestroy(s->st);
@@ -542,6 +550,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   const size_t io_n = std::max((size_t)RGPU_MAX_POS, std::max((size_t)d->nfw, nads));
   ALLOC(s->io_xyz, sizeof(double) * 3 * io_n);
   ALLOC(s->io_q, sizeof(double) * io_n);
+  ALLOC(s->io_q_all, sizeof(double) * std::max((size_t)1, nads));
   ALLOC(s->io_out, sizeof(double) * 4 * RGPU_MAX_POS);
   ALLOC(s->io_atom, sizeof(int) * RGPU_MAX_POS);
   ALLOC(s->io_excl, sizeof(int) * RGPU_MAX_POS);
@@ -578,6 +587,13 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       if (cudaMemcpyAsync(s->kvec, kv.data(), sizeof(char4) * h.nk, cudaMemcpyHostToDevice, st) ||
           cudaMemcpyAsync(s->kfactor, kf.data(), sizeof(double) * h.nk, cudaMemcpyHostToDevice, st)) {
         rc = fail(RGPU_E_CUDA, "upload k");
+        break;
+      }
+      /* charge of every adsorbate slot, for S_ads(k) of batched uploads */
+      std::vector<double> qs(std::max((size_t)1, nads));
+      for (size_t a = 0; a < nads; a++) qs[a] = h.mol_q[a % d->natom];
+      if (cudaMemcpy(s->io_q_all, qs.data(), sizeof(double) * qs.size(), cudaMemcpyHostToDevice)) {
+        rc = fail(RGPU_E_CUDA, "upload slot charges");
         break;
       }
       /* S_fw(k) (PrecomputeFixedEwaldContributions, src/ewald.c:744) from the
@@ -1221,6 +1237,10 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->use_graph = 0;
   e->gexec = nullptr;
   e->g_nsteps = -1;
+  e->stage_bytes = 0;
+  e->d_off = nullptr;
+  e->d_stage = nullptr;
+  e->h_stage = nullptr;
   std::vector<RgpuSys> hs(n);
   for (int i = 0; i < n; i++) {
     hs[i] = e->sys[i]->h;
@@ -1244,6 +1264,9 @@ extern "C" int rgpu_engine_destroy(rgpu_engine *e)
 {
   if (!e) return RGPU_SUCCESS;
   if (e->gexec) cudaGraphExecDestroy(e->gexec);
+  if (e->d_off) cudaFree(e->d_off);
+  if (e->d_stage) cudaFree(e->d_stage);
+  if (e->h_stage) cudaFreeHost(e->h_stage);
   cudaFree(e->d_systems);
   delete e;
   return RGPU_SUCCESS;
@@ -1296,6 +1319,109 @@ extern "C" int rgpu_engine_use_graph(rgpu_engine *e, int on)
 extern "C" int rgpu_engine_cluster(rgpu_engine *e)
 {
   return e ? e->cluster : 0;
+}
+
+/* ---- batched state transfer ---------------------------------------------- */
+static int engine_staging(rgpu_engine *e)
+{
+  if (e->d_stage) return RGPU_SUCCESS;
+  const int n = (int)e->sys.size();
+  e->off.resize(n);
+  size_t o = 0;
+  for (int i = 0; i < n; i++) {
+    e->off[i] = o;
+    const rgpu_system *s = e->sys[i];
+    o += sizeof(RgpuState) + sizeof(double) * 3 * (size_t)s->d.maxmol * s->d.natom;
+    o = (o + 255) & ~(size_t)255;
+  }
+  e->stage_bytes = o;
+  if (cudaMalloc((void **)&e->d_off, sizeof(unsigned long long) * n) != cudaSuccess ||
+      cudaMalloc((void **)&e->d_stage, o) != cudaSuccess || cudaMallocHost((void **)&e->h_stage, o) != cudaSuccess) {
+    if (e->d_off) cudaFree(e->d_off);
+    if (e->d_stage) cudaFree(e->d_stage);
+    e->d_off = nullptr;
+    e->d_stage = nullptr;
+    e->h_stage = nullptr;
+    return fail(RGPU_E_CUDA, "engine staging allocation");
+  }
+  CK(cudaMemcpy(e->d_off, e->off.data(), sizeof(unsigned long long) * n, cudaMemcpyHostToDevice));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_staging_bytes(rgpu_engine *e, size_t *bytes)
+{
+  if (!e || !bytes) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = engine_staging(e);
+  if (rc) return rc;
+  *bytes = e->stage_bytes;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_get_state(rgpu_engine *e, double *energy8, long long *counters20, int *nmol, int *status,
+                                     unsigned long long *step, double *const *xyz)
+{
+  if (!e) return fail(RGPU_E_INVALID, "bad argument");
+  int rc = engine_staging(e);
+  if (rc) return rc;
+  const int n = (int)e->sys.size();
+  CK(cudaDeviceSynchronize());
+  CK(rgpu_gather_states_launch(e->d_systems, n, e->d_off, e->d_stage, e->st));
+  CK(cudaMemcpyAsync(e->h_stage, e->d_stage, e->stage_bytes, cudaMemcpyDeviceToHost, e->st));
+  CK(cudaStreamSynchronize(e->st));
+  for (int i = 0; i < n; i++) {
+    rgpu_system *s = e->sys[i];
+    const unsigned char *r = e->h_stage + e->off[i];
+    memcpy(&s->h_state, r, sizeof(RgpuState));
+    const RgpuState &st = s->h_state;
+    if (energy8) memcpy(energy8 + (size_t)RGPU_NE * i, st.energy, sizeof(double) * RGPU_NE);
+    if (counters20) memcpy(counters20 + (size_t)RGPU_NCNT * i, st.counters, sizeof(long long) * RGPU_NCNT);
+    if (nmol) nmol[i] = st.nmol;
+    if (status) status[i] = st.status;
+    if (step) step[i] = st.step[0];
+    if (xyz && xyz[i]) memcpy(xyz[i], r + sizeof(RgpuState), sizeof(double) * 3 * (size_t)st.nmol * s->d.natom);
+  }
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_set_adsorbates(rgpu_engine *e, const int *nmol, const double *const *xyz)
+{
+  if (!e || !nmol || !xyz) return fail(RGPU_E_INVALID, "bad argument");
+  const int n = (int)e->sys.size();
+  for (int i = 0; i < n; i++) {
+    if (nmol[i] < 0 || (nmol[i] > 0 && !xyz[i])) return fail(RGPU_E_INVALID, "system %d: bad configuration", i);
+    if (nmol[i] > e->sys[i]->d.maxmol)
+      return fail(RGPU_E_CAPACITY, "system %d: nmol %d > maxmol %d", i, nmol[i], e->sys[i]->d.maxmol);
+  }
+  int rc = engine_staging(e);
+  if (rc) return rc;
+  CK(cudaDeviceSynchronize());
+  for (int i = 0; i < n; i++) {
+    rgpu_system *s = e->sys[i];
+    unsigned char *r = e->h_stage + e->off[i];
+    ((RgpuState *)r)->nmol = nmol[i];
+    const size_t nx = (size_t)nmol[i] * s->d.natom * 3;
+    if (nx) memcpy(r + sizeof(RgpuState), xyz[i], sizeof(double) * nx);
+    s->h_xyz.assign(xyz[i], xyz[i] + nx);
+    s->h_nmol = nmol[i];
+    s->net_ads = nmol[i] * s->h.mol_charge;
+    s->pending_dq = 0.0;
+  }
+  CK(cudaMemcpyAsync(e->d_stage, e->h_stage, e->stage_bytes, cudaMemcpyHostToDevice, e->st));
+  CK(rgpu_scatter_positions_launch(e->d_systems, n, e->d_off, e->d_stage, e->st));
+  for (int i = 0; i < n; i++) {
+    rgpu_system *s = e->sys[i];
+    const int nads = nmol[i] * s->d.natom;
+    CK(rgpu_records_launch(s->d_sys, nads, s->rec32, s->rec64, e->st));
+    s->records_stale = 0;
+    if (!s->h.nk) continue;
+    if (nads == 0) {
+      CK(cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * s->h.nk, e->st));
+      continue;
+    }
+    CK(rgpu_structure_factor_launch(s->d_sys, s->ads_xyz, s->io_q_all, nads, s->h.nk, s->sk_ads, e->st));
+  }
+  CK(cudaStreamSynchronize(e->st));
+  return RGPU_SUCCESS;
 }
 
 extern "C" int rgpu_engine_sync(rgpu_engine *e)

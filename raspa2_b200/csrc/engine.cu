@@ -1543,6 +1543,49 @@ cudaError_t rgpu_structure_factor_launch(const RgpuSys *d_sys, const double *d_x
   return cudaGetLastError();
 }
 
+/* Batched state transfer of an engine's systems through one staging buffer:
+ * system i's region starts at off[i] (8-byte aligned) and holds its state
+ * block (RgpuState; for an upload only its nmol field is read), then
+ * nmol * natom positions (FP64 xyz). One block per system. */
+__global__ void k_gather_states(const RgpuSys *systems, const unsigned long long *off, unsigned char *buf)
+{
+  const RgpuSys &S = systems[blockIdx.x];
+  unsigned char *dst = buf + off[blockIdx.x];
+  const RgpuState *st = (const RgpuState *)S.energy;   /* energy is the first field of the block */
+  const unsigned long long *src8 = (const unsigned long long *)st;
+  unsigned long long *dst8 = (unsigned long long *)dst;
+  for (int i = threadIdx.x; i < (int)(sizeof(RgpuState) / 8); i += blockDim.x) dst8[i] = src8[i];
+  const int n = st->nmol * S.natom * 3;
+  double *xd = (double *)(dst + sizeof(RgpuState));
+  for (int i = threadIdx.x; i < n; i += blockDim.x) xd[i] = S.ads_xyz[i];
+}
+
+__global__ void k_scatter_positions(const RgpuSys *systems, const unsigned long long *off, const unsigned char *buf)
+{
+  const RgpuSys &S = systems[blockIdx.x];
+  const unsigned char *src = buf + off[blockIdx.x];
+  const int nmol = ((const RgpuState *)src)->nmol;
+  const double *xs = (const double *)(src + sizeof(RgpuState));
+  for (int i = threadIdx.x; i < nmol * S.natom * 3; i += blockDim.x) S.ads_xyz[i] = xs[i];
+  if (threadIdx.x == 0) *S.nmol = nmol;
+}
+
+cudaError_t rgpu_gather_states_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
+                                      unsigned char *d_buf, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  k_gather_states<<<n, 256, 0, st>>>(d_systems, d_off, d_buf);
+  return cudaGetLastError();
+}
+
+cudaError_t rgpu_scatter_positions_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
+                                          const unsigned char *d_buf, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  k_scatter_positions<<<n, 256, 0, st>>>(d_systems, d_off, d_buf);
+  return cudaGetLastError();
+}
+
 /* adsorbate records (fixed-point and FP64) from the authoritative positions */
 __global__ void k_build_records(const RgpuSys *sysp, int nads, int4 *rec32, AdsRec64 *rec64)
 {

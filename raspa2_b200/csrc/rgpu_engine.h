@@ -32,6 +32,11 @@ cudaError_t rgpu_records_launch(const RgpuSys *d_sys, int nads, int4 *d_rec32, v
 /* grids (grid.cu) */
 cudaError_t rgpu_grid_build_launch_lj(const RgpuSys *d_sys, const RgpuLJ *lj, const int npts[3],
                                       const double size[3], const double shift[3], float *d_grid, cudaStream_t st);
+/* batched state transfer of an engine's systems (see k_gather_states) */
+cudaError_t rgpu_gather_states_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
+                                      unsigned char *d_buf, cudaStream_t st);
+cudaError_t rgpu_scatter_positions_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
+                                          const unsigned char *d_buf, cudaStream_t st);
 cudaError_t rgpu_grid_build_launch_coulomb(const RgpuSys *d_sys, const int npts[3], const double size[3],
                                            const double shift[3], float *d_grid, cudaStream_t st);
 cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], const double size[3],

@@ -32,7 +32,8 @@ EXPORTS = [
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
     "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_intra_energy",
     "rgpu_system_set_grids", "rgpu_system_checkpoint_size", "rgpu_system_checkpoint", "rgpu_system_restore",
-    "rgpu_grid_build_coulomb", "rgpu_system_set_coulomb_grid",
+    "rgpu_grid_build_coulomb", "rgpu_system_set_coulomb_grid", "rgpu_engine_get_state", "rgpu_engine_set_adsorbates",
+    "rgpu_engine_staging_bytes",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -437,6 +438,46 @@ class Engine:
 
     def sync(self):
         _check(load().rgpu_engine_sync(self.h))
+
+    def get_states(self, positions: bool = True):
+        """Every system's state (and positions) with one transfer
+        (rgpu_engine_get_state): a list of dicts as GpuSystem.state(), with
+        "xyz" [nmol, natom, 3] when positions is true (a view of a buffer
+        that the next call overwrites: copy it to keep it)."""
+        n = len(self.systems)
+        e = np.zeros((n, 8)); c = np.zeros((n, 20), np.int64)
+        nm = np.zeros(n, np.int32); stt = np.zeros(n, np.int32); stp = np.zeros(n, np.uint64)
+        bufs, ptrs = None, None
+        if positions:
+            if getattr(self, "_xyz_bufs", None) is None:
+                self._xyz_bufs = [np.zeros((g.init_args["maxmol"], g.natom, 3)) for g in self.systems]
+                self._xyz_ptrs = (C.POINTER(C.c_double) * n)(*[b.ctypes.data_as(_dp) for b in self._xyz_bufs])
+            bufs, ptrs = self._xyz_bufs, self._xyz_ptrs
+        _check(load().rgpu_engine_get_state(self.h, e.ctypes.data_as(_dp), c.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                            nm.ctypes.data_as(_ip), stt.ctypes.data_as(_ip),
+                                            stp.ctypes.data_as(C.POINTER(C.c_ulonglong)), ptrs))
+        out = []
+        for i in range(n):
+            d = {"energy": e[i], "counters": c[i], "nmol": int(nm[i]), "status": int(stt[i]), "step": int(stp[i])}
+            if positions:
+                d["xyz"] = bufs[i][: nm[i]]
+            out.append(d)
+        return out
+
+    def set_adsorbates(self, xyz_list):
+        """Every system's configuration with one transfer
+        (rgpu_engine_set_adsorbates); xyz_list[i]: [nmol, natom, 3]."""
+        n = len(self.systems)
+        keep = [np.ascontiguousarray(np.asarray(x, float).reshape(-1, g.natom, 3))
+                for x, g in zip(xyz_list, self.systems)]
+        nm = np.array([len(x) for x in keep], np.int32)
+        ptrs = (C.POINTER(C.c_double) * n)(*[x.ctypes.data_as(_dp) for x in keep])
+        _check(load().rgpu_engine_set_adsorbates(self.h, nm.ctypes.data_as(_ip), ptrs))
+
+    def staging_bytes(self) -> int:
+        n = C.c_size_t()
+        _check(load().rgpu_engine_staging_bytes(self.h, C.byref(n)))
+        return n.value
 
     def use_graph(self, on: bool = True):
         """Replay a CUDA graph of the launch in run() (rgpu_engine_use_graph)."""
