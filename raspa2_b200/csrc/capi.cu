@@ -87,7 +87,6 @@ struct rgpu_system {
   double net_ads, pending_dq;
   int grid_type_seg;
   uint64_t fingerprint;       /* of the model a checkpoint must match (checkpoint_fingerprint) */
-  double *io_q_all;           /* charge of every adsorbate slot (batched uploads), filled at creation */
   std::vector<int> fw_seg_type; /* framework pseudo-atom type of each segment */
   std::vector<double> lj_eps, lj_sig2, lj_shift;
   int ntypes;
@@ -119,7 +118,7 @@ static void sys_free(rgpu_system *s)
   if (!s) return;
   void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->tiles_d, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
                   s->state, s->rec32, s->rec64, s->io_xyz,
-                  s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov, s->io_q_all};
+                  s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->st) cudaStreamDestroy(s->st);
@@ -550,7 +549,6 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
   const size_t io_n = std::max((size_t)RGPU_MAX_POS, std::max((size_t)d->nfw, nads));
   ALLOC(s->io_xyz, sizeof(double) * 3 * io_n);
   ALLOC(s->io_q, sizeof(double) * io_n);
-  ALLOC(s->io_q_all, sizeof(double) * std::max((size_t)1, nads));
   ALLOC(s->io_out, sizeof(double) * 4 * RGPU_MAX_POS);
   ALLOC(s->io_atom, sizeof(int) * RGPU_MAX_POS);
   ALLOC(s->io_excl, sizeof(int) * RGPU_MAX_POS);
@@ -587,13 +585,6 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       if (cudaMemcpyAsync(s->kvec, kv.data(), sizeof(char4) * h.nk, cudaMemcpyHostToDevice, st) ||
           cudaMemcpyAsync(s->kfactor, kf.data(), sizeof(double) * h.nk, cudaMemcpyHostToDevice, st)) {
         rc = fail(RGPU_E_CUDA, "upload k");
-        break;
-      }
-      /* charge of every adsorbate slot, for S_ads(k) of batched uploads */
-      std::vector<double> qs(std::max((size_t)1, nads));
-      for (size_t a = 0; a < nads; a++) qs[a] = h.mol_q[a % d->natom];
-      if (cudaMemcpy(s->io_q_all, qs.data(), sizeof(double) * qs.size(), cudaMemcpyHostToDevice)) {
-        rc = fail(RGPU_E_CUDA, "upload slot charges");
         break;
       }
       /* S_fw(k) (PrecomputeFixedEwaldContributions, src/ewald.c:744) from the
@@ -1408,18 +1399,14 @@ extern "C" int rgpu_engine_set_adsorbates(rgpu_engine *e, const int *nmol, const
   }
   CK(cudaMemcpyAsync(e->d_stage, e->h_stage, e->stage_bytes, cudaMemcpyHostToDevice, e->st));
   CK(rgpu_scatter_positions_launch(e->d_systems, n, e->d_off, e->d_stage, e->st));
+  int max_nk = 0;
   for (int i = 0; i < n; i++) {
     rgpu_system *s = e->sys[i];
-    const int nads = nmol[i] * s->d.natom;
-    CK(rgpu_records_launch(s->d_sys, nads, s->rec32, s->rec64, e->st));
+    CK(rgpu_records_launch(s->d_sys, nmol[i] * s->d.natom, s->rec32, s->rec64, e->st));
     s->records_stale = 0;
-    if (!s->h.nk) continue;
-    if (nads == 0) {
-      CK(cudaMemsetAsync(s->sk_ads, 0, sizeof(double2) * s->h.nk, e->st));
-      continue;
-    }
-    CK(rgpu_structure_factor_launch(s->d_sys, s->ads_xyz, s->io_q_all, nads, s->h.nk, s->sk_ads, e->st));
+    max_nk = std::max(max_nk, s->h.nk);
   }
+  CK(rgpu_upload_sk_launch(e->d_systems, n, max_nk, e->st));
   CK(cudaStreamSynchronize(e->st));
   return RGPU_SUCCESS;
 }

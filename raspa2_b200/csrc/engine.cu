@@ -1570,6 +1570,36 @@ __global__ void k_scatter_positions(const RgpuSys *systems, const unsigned long 
   if (threadIdx.x == 0) *S.nmol = nmol;
 }
 
+/* S_ads(k) of every system of an engine from its positions (the batched
+ * upload): block (x, y) = wave vectors x*128.. of system y; the same sum, in
+ * the same order, as k_structure_factor with the molecule's charges. */
+__global__ void k_upload_sk(const RgpuSys *systems)
+{
+  const RgpuSys &S = systems[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= S.nk) return;
+  const int n = *S.nmol * S.natom;
+  const char4 kv = S.kvec[k];
+  double re = 0.0, im = 0.0;
+  for (int i = 0; i < n; i++) {
+    const double *x = S.ads_xyz + 3 * i;
+    const double q = S.mol_q[i % S.natom];
+    double a = 2.0 * (kv.x * x[0] * S.inv_box[0] + kv.y * x[1] * S.inv_box[1] + kv.z * x[2] * S.inv_box[2]);
+    double sn, cs;
+    sincospi(a, &sn, &cs);
+    re += q * cs;
+    im += q * sn;
+  }
+  S.sk_ads[k] = make_double2(re, im);
+}
+
+cudaError_t rgpu_upload_sk_launch(const RgpuSys *d_systems, int n, int max_nk, cudaStream_t st)
+{
+  if (n <= 0 || max_nk <= 0) return cudaSuccess;
+  k_upload_sk<<<dim3((unsigned)((max_nk + 127) / 128), (unsigned)n), 128, 0, st>>>(d_systems);
+  return cudaGetLastError();
+}
+
 cudaError_t rgpu_gather_states_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
                                       unsigned char *d_buf, cudaStream_t st)
 {

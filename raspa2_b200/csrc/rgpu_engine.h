@@ -35,6 +35,7 @@ cudaError_t rgpu_grid_build_launch_lj(const RgpuSys *d_sys, const RgpuLJ *lj, co
 /* batched state transfer of an engine's systems (see k_gather_states) */
 cudaError_t rgpu_gather_states_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
                                       unsigned char *d_buf, cudaStream_t st);
+cudaError_t rgpu_upload_sk_launch(const RgpuSys *d_systems, int n, int max_nk, cudaStream_t st);
 cudaError_t rgpu_scatter_positions_launch(const RgpuSys *d_systems, int n, const unsigned long long *d_off,
                                           const unsigned char *d_buf, cudaStream_t st);
 cudaError_t rgpu_grid_build_launch_coulomb(const RgpuSys *d_sys, const int npts[3], const double size[3],
