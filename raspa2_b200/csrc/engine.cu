@@ -222,10 +222,22 @@ __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 /* Pair evaluation of P positions on this CTA's share, then one cluster
  * barrier; the totals are read with gather(). All threads call. */
 template <bool MIXED, bool FLEX>
-__device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair_check)
+__device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair_check, int ew_ns = 0)
 {
   Ctl &C = *E.ctl;
   const long long t0 = clock64();
+  if (ew_ns) {
+    /* the Ewald sum of sites E.sites[0..ew_ns) rides along (a displacement,
+     * whose sites are known up front): phase tables now, each warp's share
+     * of the wave vectors right after its pair units, so it fills the
+     * units' tail; the CTA total goes to C.ewt[E.xb] as engine_ewald does */
+    ewald_phases<MIXED>(*E.S, E.sites, ew_ns, E.tab, E.kw);
+    if (threadIdx.x == 0) {
+      C.work[3] += (unsigned long long)(E.k1 - E.k0) * ew_ns;
+      C.work[4] += (unsigned long long)(E.k1 - E.k0);
+    }
+    __syncthreads();
+  }
   if (FLEX && E.S->use_grid && E.rank == 0) {
     /* host VDW from the bead types' energy grids (one CTA of the cluster):
      * 8 lanes per position, 4 positions per warp, before the pair units */
@@ -247,8 +259,25 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair
   }
   const EvalPlan pl = eval_units<MIXED>(*E.S, E.sl, E.pos, P, pair_check, E.sc, RGPU_MAX_UNITS);
   const int per = pl.cf + pl.ca;
+  double *ewred = E.red + E.xb * 2 * RGPU_MAX_WARPS;
+  if (ew_ns) ewald_energy_warps<MIXED>(*E.S, E.tab, E.kw, E.sites, ew_ns, E.k0, E.k1, ewred);
   __syncthreads();
   if (threadIdx.x == 0) C.next = 0;      /* unit counter of the next evaluation */
+  if (ew_ns && threadIdx.x < 32) {
+    /* this CTA's Ewald total (warp 0, fixed reduction order) */
+    const int nw = blockDim.x >> 5;
+    double a = 0.0, h = 0.0;
+    if (threadIdx.x < nw) {
+      a = ewred[2 * threadIdx.x];
+      h = ewred[2 * threadIdx.x + 1];
+    }
+    a = warp_sum(a);
+    h = warp_sum(h);
+    if (threadIdx.x == 0) {
+      C.ewt[E.xb][0] = a;
+      C.ewt[E.xb][1] = h;
+    }
+  }
   /* this CTA's sum per position, units in order */
   PosSum *ps = E.part + E.xb * RGPU_MAX_POS;
   for (int p = threadIdx.x; p < P; p += blockDim.x) {
@@ -433,7 +462,8 @@ __device__ __forceinline__ void step_displace(Eng<MIXED, FLEX> &E, int mv)
     E.sites[na + a].q = -S.mol_q[a];
   }
   __syncthreads();
-  engine_eval(E, 2 * na, na);
+  const bool ew = S.ewald && S.mol_charged;
+  engine_eval(E, 2 * na, na, ew ? 2 * na : 0);
   const int be = E.xb;
   E.xb ^= 1;
   if (threadIdx.x < 32) {
@@ -458,18 +488,11 @@ __device__ __forceinline__ void step_displace(Eng<MIXED, FLEX> &E, int mv)
   }
   __syncthreads();
   if (C.fail) return;
-  const bool ew = S.ewald && S.mol_charged;
-  int bw = 0;
-  if (ew) {
-    engine_ewald(E, 2 * na);
-    bw = E.xb;
-    E.xb ^= 1;
-  }
   if (threadIdx.x == 0) {
     double d_ads = 0.0, d_host = 0.0;
     if (ew) {
       double ea, eh;
-      gather_ewald(E, bw, ea, eh);
+      gather_ewald(E, be, ea, eh);
       /* the exclusion energy of a rigid molecule is the same before and
        * after the displacement (the reference's difference of the two is
        * zero up to rounding) */
