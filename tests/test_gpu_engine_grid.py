@@ -83,3 +83,35 @@ def test_mixed_engine_with_grids_matches_lookups_and_direct_sums(cuda):
     # the direct total of the engine's configuration, switched back to pair sums
     g.set_grids(None, None, None, None, None)
     assert abs(g.total_energy()[0] - direct.sum()) <= 1e-9 * np.abs(direct).sum() + 1e-6 * kT
+
+
+def test_grid_loading_matches_direct_sums(cuda):
+    """GCMC of n-hexane at 3e4 Pa: the average loading with 0.1 A grids equals
+    the loading with direct pair sums within the combined statistical error
+    (64 independent replicas each)."""
+    import dataclasses
+    from test_gpu_stats import engine_ideal_gas_rosenbluth
+    s = small_hexane(pressure=3e4)
+    w, _ = engine_ideal_gas_rosenbluth(s.molecule, s.temperature)
+    s = dataclasses.replace(s, ideal_gas_rosenbluth=w)
+    equil, prod, nrep = 50000, 100000, 64
+    loads = {}
+    for grids in (False, True):
+        gs = []
+        for i in range(nrep):
+            g = native.GpuSystem(s, maxmol=32, seed=(9000 if grids else 7000) + i, stream_id=i)
+            g.set_adsorbates(np.zeros((0, 6, 3)))
+            if grids:
+                if gs:
+                    g.use_energy_grids(0.1, like=gs[0])
+                else:
+                    g.use_energy_grids(0.1)
+            g.set_limits(equil + prod, equil)
+            gs.append(g)
+        e = native.Engine(gs, precision=native.RGPU_MIXED)
+        e.run(equil + prod)
+        e.sync()
+        loads[grids] = np.array([g.averages()["loading"] for g in gs])
+    a, b = loads[False], loads[True]
+    se = np.hypot(a.std(ddof=1), b.std(ddof=1)) / np.sqrt(nrep)
+    assert abs(a.mean() - b.mean()) <= 4.0 * se, (a.mean(), b.mean(), se)
