@@ -1214,7 +1214,7 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   const int k_try[4] = {maxk, 0, maxk, 0};
   int pick = -1;
   for (int t = 0; t < 4 && pick < 0; t++)
-    if (rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t], threads) <=
+    if (rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t], threads, e->flex) <=
         (size_t)smem_max)
       pick = t;
   if (pick < 0) {
@@ -1224,7 +1224,8 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->fw_items = fw_try[pick];
   e->tile_items = tile_try[pick];
   e->k_items = k_try[pick];
-  e->smem = rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw, e->k_items, threads);
+  e->smem = rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw, e->k_items, threads,
+                                   e->flex);
   e->use_graph = 0;
   e->gexec = nullptr;
   e->g_nsteps = -1;

@@ -40,7 +40,7 @@ namespace cg = cooperative_groups;
  * mixed path), tiles: tile records of the share (mixed only), k_items: wave
  * vectors of the share staged with their S(k) (0: read from global memory). */
 struct EngineLayout {
-  size_t sys, fw, tiles, ads, pos, uv, uc, uo, part, q, sites, tab, red, kvec, kf, skfw, skads, ctl, total;
+  size_t sys, fw, tiles, ads, pos, uv, uc, uo, part, q, sites, tab, red, kvec, kf, skfw, skads, ctl, ang, total;
 };
 
 /* this CTA's sums for one position of an evaluation: host VDW, host real,
@@ -54,8 +54,13 @@ static_assert(sizeof(PosSum) % 16 == 0, "PosSum must keep 16-byte alignment in a
 
 __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
+/* bend and dihedral trigonometry of every trial of a chain growth stage
+ * (flexible-chain builds only): {cos theta, sin theta, cos phi, sin phi} for
+ * beads 2.. natom-1 and each trial */
+#define RGPU_ANG_DOUBLES (4 * (RGPU_MAX_ATOMS - 2) * RGPU_MAX_TRIALS)
+
 __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw,
-                                                      int k_items, int nwarps)
+                                                      int k_items, int nwarps, int flex)
 {
   EngineLayout L;
   size_t o = 0;
@@ -77,14 +82,15 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.skfw = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
   L.skads = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
   L.ctl = o; o = rgpu_align(o + RGPU_CTL_BYTES);
+  L.ang = o; o = rgpu_align(o + (flex ? RGPU_ANG_DOUBLES * sizeof(double) : 0));
   L.total = o;
   return L;
 }
 
 size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw, int k_items,
-                              int threads)
+                              int threads, int flex)
 {
-  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw, k_items, threads / 32).total;
+  return engine_layout(mixed, fw_items, tiles, max_ads_atoms, kw, k_items, threads / 32, flex).total;
 }
 
 /* broadcast/control block in shared memory */
@@ -98,11 +104,10 @@ struct Ctl {
   double rosen;
   double rosen_old;
   /* flexible chains: chosen bead positions of the configuration being grown
-   * or retraced (cp) and of a reinsertion's new one (cpn), bonded energies
-   * of the current trials, intramolecular energies of the configurations */
+   * or retraced (cp) and of a reinsertion's new one (cpn), intramolecular
+   * energies of the configurations */
   double cp[RGPU_MAX_ATOMS][3];
   double cpn[RGPU_MAX_ATOMS][3];
-  double ub[RGPU_MAX_TRIALS];
   double uintra, uintra_old;
   double dl[4];
   int nmol;
@@ -137,6 +142,7 @@ struct Eng {
   int kw;
   int k0, k1;                /* this CTA's wave vectors */
   double *red;               /* [2][2*RGPU_MAX_WARPS] */
+  double *ang;               /* [RGPU_ANG_DOUBLES] chain trial trigonometry (flexible-chain builds) */
   Ctl *ctl;
   const double *rnd;         /* this step's uniforms */
   uint64_t step;             /* index of the current MC step */
@@ -901,54 +907,50 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED, FLEX> &E)
 }
 
 /* ------------------------------------------------------------------------ */
-/* chain_trial for bead i >= 2 of trial t, computed by one warp: lane l draws
- * proposals l, l + 32, ... of the bend angle (and of the dihedral) at once,
- * and the lowest accepted proposal wins, so the result is chain_trial's (its
- * proposals are tried in order and the first accepted one is taken). Every
- * lane returns the trial position p and its bonded energy. */
-__device__ __forceinline__ double chain_trial_warp(const RgpuSys &S, const double (*x)[3], int i, int stage, int t,
-                                                   uint64_t step, int lane, double *p)
+/* The bend angle and dihedral of trial t of bead i >= 2, as chain_trial
+ * draws them, by a group of 8 lanes (lane8 = lane % 8; every lane of the
+ * warp calls): lane8 l forms proposals l, l + 8, ... of the bend angle and
+ * of the dihedral, and the lowest accepted proposal of each wins, so the
+ * result is chain_trial's (its proposals are tried in order and the first
+ * accepted one is taken). The draws need no bead position, so a whole
+ * growth stage's angles are drawn at once, before its first bead. A group
+ * with live = false only takes part in the warp's votes. */
+__device__ __forceinline__ void chain_angles_group(const RgpuSys &S, int i, int stage, int t, bool live,
+                                                   uint64_t step, int lane, double &theta, double &phi)
 {
   auto U = [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); };
-  double theta = S.bend_theta0;
-  for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
-    const int a = base + lane;
-    double th = 0.0;
-    bool ok = false;
-    if (a < RGPU_CHAIN_TRIES) {
+  const int k = 3 * RGPU_CHAIN_TRIES, l8 = lane & 7;
+  const unsigned gmask = 0xffu << (lane & ~7);
+  theta = S.bend_theta0;
+  phi = M_PI;
+  bool th_done = !live, ph_done = !live || i < 3;
+  if (live && i == 2) phi = 2.0 * M_PI * U(k) - M_PI;
+  for (int base = 0; base < RGPU_CHAIN_TRIES; base += 8) {
+    if (!__any_sync(RGPU_FULL, !(th_done && ph_done))) break;
+    const int a = base + l8;
+    double th = 0.0, f = 0.0;
+    bool okt = false, okp = false;
+    if (!th_done) {
       const double u1 = U(3 * a), u2 = U(3 * a + 1), u3 = U(3 * a + 2);
       th = S.bend_theta0 + S.bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
-      ok = th > 0.0 && th < M_PI && u3 < sin(th);
+      okt = th > 0.0 && th < M_PI && u3 < sin(th);
     }
-    const unsigned b = __ballot_sync(RGPU_FULL, ok);
-    if (b) {
-      theta = __shfl_sync(RGPU_FULL, th, __ffs(b) - 1);
-      break;
+    if (!ph_done) {
+      f = 2.0 * M_PI * U(k + 2 * a) - M_PI;
+      okp = U(k + 2 * a + 1) < exp(-S.beta * (chain_torsion_energy(S, cos(f)) - S.torsion_min));
     }
-  }
-  const int k = 3 * RGPU_CHAIN_TRIES;
-  double phi;
-  if (i == 2) {
-    phi = 2.0 * M_PI * U(k) - M_PI;
-  } else {
-    phi = M_PI;
-    for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
-      const int a = base + lane;
-      double f = 0.0;
-      bool ok = false;
-      if (a < RGPU_CHAIN_TRIES) {
-        f = 2.0 * M_PI * U(k + 2 * a) - M_PI;
-        ok = U(k + 2 * a + 1) < exp(-S.beta * (chain_torsion_energy(S, cos(f)) - S.torsion_min));
-      }
-      const unsigned b = __ballot_sync(RGPU_FULL, ok);
-      if (b) {
-        phi = __shfl_sync(RGPU_FULL, f, __ffs(b) - 1);
-        break;
-      }
+    const unsigned bt = __ballot_sync(RGPU_FULL, okt) & gmask, bp = __ballot_sync(RGPU_FULL, okp) & gmask;
+    const double ts = __shfl_sync(RGPU_FULL, th, bt ? __ffs(bt) - 1 : lane);
+    const double fs = __shfl_sync(RGPU_FULL, f, bp ? __ffs(bp) - 1 : lane);
+    if (!th_done && bt) {
+      theta = ts;
+      th_done = true;
+    }
+    if (!ph_done && bp) {
+      phi = fs;
+      ph_done = true;
     }
   }
-  chain_place(i >= 3 ? x[i - 3] : nullptr, x[i - 2], x[i - 1], S.bond, theta, phi, p);
-  return chain_bonded_energy(S, x, i, p);
 }
 
 /* CBMC growth (retrace = false) or retrace (retrace = true) of a flexible
@@ -975,40 +977,46 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
     C.uintra = 0.0;
     C.fail = 0;
   }
+  /* the bend angles and dihedrals of beads 2.. of every trial: 8 lanes per
+   * (bead, trial), four per warp, ahead of the first bead (the first barrier
+   * below publishes them) */
+  {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int ntask = na > 2 ? (na - 2) * nt : 0;
+    for (int t0 = (threadIdx.x >> 5) * 4; t0 < ntask; t0 += nw * 4) {
+      const int task = t0 + (lane >> 3);
+      const bool live = task < ntask;
+      const int i = live ? 2 + task / nt : 2, t = live ? task % nt : 0;
+      double th, ph;
+      chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
+      if (live && (lane & 7) == 0) {
+        double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+        a[0] = cos(th);
+        a[1] = sin(th);
+        a[2] = cos(ph);
+        a[3] = sin(ph);
+      }
+    }
+  }
   for (int i = 0; i < na; i++) {
     const int k = i == 0 ? nf : nt;
-    if (i >= 2) {
-      /* bend and dihedral draws: one warp per trial */
-      const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-      for (int t = threadIdx.x >> 5; t < k; t += nw) {
-        double p[3], ub = 0.0;
-        if (retrace && t == 0) {
-          atom_xyz(E, m, i, p);
-          ub = chain_bonded_energy(S, C.cp, i, p);
-        } else {
-          ub = chain_trial_warp(S, C.cp, i, stage, t, E.step, lane, p);
-        }
-        if (lane == 0) {
-          bead_set(E.pos[t], S, p[0], p[1], p[2], i, exclude);
-          C.ub[t] = ub;
-        }
-      }
-    } else if (threadIdx.x < k) {
+    if (threadIdx.x < k) {
       const int t = threadIdx.x;
-      double p[3], ub = 0.0;
+      double p[3];
       if (retrace && t == 0) {
         atom_xyz(E, m, i, p);
-        ub = chain_bonded_energy(S, C.cp, i, p);
       } else if (i == 0) {
         for (int d = 0; d < 3; d++)
           p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
-      } else {
+      } else if (i == 1) {
         const uint64_t step = E.step;
-        ub = chain_trial(S, C.cp, i,
-                         [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); }, p);
+        chain_trial(S, C.cp, i,
+                    [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); }, p);
+      } else {
+        const double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+        chain_place_trig(i >= 3 ? C.cp[i - 3] : nullptr, C.cp[i - 2], C.cp[i - 1], S.bond, a[0], a[1], a[2], a[3], p);
       }
       bead_set(E.pos[t], S, p[0], p[1], p[2], i, exclude);
-      C.ub[t] = ub;
     }
     __syncthreads();
     engine_eval(E, k, 0);
@@ -1047,7 +1055,9 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
         if (!any || (!retrace && C.rosen < 1e-150)) C.fail = 1;
         C.u[0] += hv;
         C.u[2] += av;
-        C.uintra += ljs + C.ub[sel];
+        /* the bonded energy of the chosen trial */
+        const double ps[3] = {E.pos[sel].x, E.pos[sel].y, E.pos[sel].z};
+        C.uintra += ljs + chain_bonded_energy(S, C.cp, i, ps);
         C.cp[i][0] = E.pos[sel].x;
         C.cp[i][1] = E.pos[sel].y;
         C.cp[i][2] = E.pos[sel].z;
@@ -1181,7 +1191,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
   const int rank = (int)cl.block_rank();
   const int sysi = blockIdx.x / csize;
   const int nwarps = blockDim.x >> 5;
-  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw, k_items, nwarps);
+  const EngineLayout L = engine_layout(MIXED, fw_items, tile_items, max_ads_atoms, kw, k_items, nwarps, FLEX);
   if (sysi < nsys) {
     Eng<MIXED, FLEX> E;
     E.rank = rank;
@@ -1204,6 +1214,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
     E.tab = (typename PhaseT<MIXED>::T *)(smem + L.tab);
     E.kw = kw;
     E.red = (double *)(smem + L.red);
+    E.ang = (double *)(smem + L.ang);
     E.ctl = (Ctl *)(smem + L.ctl);
     Ctl &C = *E.ctl;
     E.sc.cnt = C.work;
@@ -1405,7 +1416,7 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
                                int max_ads_atoms, int fw_items, int tile_items, int k_items, int cluster,
                                int threads, bool wide, bool flex, cudaStream_t st)
 {
-  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items, threads);
+  size_t smem = rgpu_engine_smem_bytes(mixed, fw_items, tile_items, max_ads_atoms, kw, k_items, threads, flex);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nsys * cluster), 1, 1);
   cfg.blockDim = dim3((unsigned)threads, 1, 1);

@@ -84,8 +84,18 @@ __host__ __device__ inline double chain_cos_dihedral(const double *a, const doub
 /* Places a bead at distance L from c, with angle theta at c (b-c-new) and
  * dihedral phi (a-b-c-new). Without a (the third bead of the chain) phi is
  * the azimuth about b-c from a fixed perpendicular reference. */
+__host__ __device__ inline void chain_place_trig(const double *a, const double *b, const double *c, double L,
+                                                 double ct, double st, double cp, double sp, double *out);
+
 __host__ __device__ inline void chain_place(const double *a, const double *b, const double *c, double L, double theta,
                                             double phi, double *out)
+{
+  chain_place_trig(a, b, c, L, cos(theta), sin(theta), cos(phi), sin(phi), out);
+}
+
+/* chain_place with cos/sin of theta (ct, st) and of phi (cp, sp) given */
+__host__ __device__ inline void chain_place_trig(const double *a, const double *b, const double *c, double L,
+                                                 double ct, double st, double cp, double sp, double *out)
 {
   double bc[3] = {c[0] - b[0], c[1] - b[1], c[2] - b[2]};
   double nb = sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]);
@@ -105,7 +115,7 @@ __host__ __device__ inline void chain_place(const double *a, const double *b, co
   const double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
   n[0] /= nn; n[1] /= nn; n[2] /= nn;
   const double m[3] = {n[1] * bc[2] - n[2] * bc[1], n[2] * bc[0] - n[0] * bc[2], n[0] * bc[1] - n[1] * bc[0]};
-  const double dx = -L * cos(theta), dy = L * sin(theta) * cos(phi), dz = L * sin(theta) * sin(phi);
+  const double dx = -L * ct, dy = L * st * cp, dz = L * st * sp;
   for (int k = 0; k < 3; k++) out[k] = c[k] + dx * bc[k] + dy * m[k] + dz * n[k];
 }
 

@@ -11,7 +11,7 @@
  * framework is read from global memory); k_items: wave vectors one CTA
  * stages with their S(k) (0: read from global memory) */
 size_t rgpu_engine_smem_bytes(int mixed, int fw_items, int tile_items, int max_ads_atoms, int kw, int k_items,
-                              int threads);
+                              int threads, int flex);
 /* raises the kernel's dynamic shared-memory limit to `smem` (call before a
  * launch or a capture of one); flex selects the build with flexible-chain
  * moves and energy grids */
