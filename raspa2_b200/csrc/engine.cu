@@ -108,6 +108,7 @@ struct Ctl {
    * energies of the configurations */
   double cp[RGPU_MAX_ATOMS][3];
   double cpn[RGPU_MAX_ATOMS][3];
+  double ub[RGPU_MAX_TRIALS];  /* bonded energies of the current bead's trials */
   double uintra, uintra_old;
   double dl[4];
   int nmol;
@@ -1055,16 +1056,24 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
         if (!any || (!retrace && C.rosen < 1e-150)) C.fail = 1;
         C.u[0] += hv;
         C.u[2] += av;
-        /* the bonded energy of the chosen trial */
-        const double ps[3] = {E.pos[sel].x, E.pos[sel].y, E.pos[sel].z};
-        C.uintra += ljs + chain_bonded_energy(S, C.cp, i, ps);
+        C.uintra += ljs;
+        C.sel = sel;
         C.cp[i][0] = E.pos[sel].x;
         C.cp[i][1] = E.pos[sel].y;
         C.cp[i][2] = E.pos[sel].z;
         if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
       }
+    } else if (i >= 2 && threadIdx.x < 32 + k) {
+      /* meanwhile warp 1: the trials' bonded energies (beads i-1.. of C.cp
+       * are fixed; warp 0 writes only C.cp[i]) */
+      const int t = threadIdx.x - 32;
+      const double p[3] = {E.pos[t].x, E.pos[t].y, E.pos[t].z};
+      C.ub[t] = chain_bonded_energy(S, C.cp, i, p);
     }
     __syncthreads();
+    /* the chosen trial's bonded energy; C.ub and C.sel stay untouched until
+     * the next bead's selection, several barriers on */
+    if (threadIdx.x == 0 && i >= 2) C.uintra += C.ub[C.sel];
     if (C.fail) return;
   }
 }
