@@ -37,7 +37,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-from . import native, systems, units
+from . import native, output, systems, units
 
 # a reference cycle is max(MinimumInnerCycles = 20, N) MC steps
 # (src/monte_carlo.c:367, src/input.c:346)
@@ -58,6 +58,11 @@ class Job:
     # original job), and/or return the final checkpoint with the result
     resume: Optional[bytes] = None
     keep_checkpoint: bool = False
+    # RASPA-style results: the production in NR_BLOCKS equal blocks, each
+    # block's ensemble sums, and the `.data` results text built from them
+    # (raspa2_b200.output); the job pauses at each block boundary until the
+    # next launch
+    raspa_output: bool = False
     # filled in by the server
     admitted: Optional[float] = None
     finished: Optional[float] = None
@@ -107,9 +112,35 @@ class Server:
             g.restore(job.resume)
         else:
             g.set_adsorbates(np.zeros((0, job.system.molecule.n_atoms, 3)))
-        g.set_limits(job.steps, job.equil)
+        if job.raspa_output:
+            if job.resume is not None and int(g.state()["step"]) > job.equil:
+                raise ValueError("raspa_output: the job's production must start within one admission")
+            prod = job.steps - job.equil
+            job._bounds = [job.equil + prod * (b + 1) // output.NR_BLOCKS for b in range(output.NR_BLOCKS)]
+            job._blocks = []
+            job._prev = output.Block.from_sums(g.averages()["sums"])
+            g.set_limits(self._next_bound(job, int(g.state()["step"])), job.equil)
+        else:
+            g.set_limits(job.steps, job.equil)
         job.admitted = now
         return g
+
+    @staticmethod
+    def _next_bound(job: Job, step: int) -> int:
+        for b in job._bounds:
+            if b > step:
+                return b
+        return job.steps
+
+    @staticmethod
+    def _close_blocks(job: Job, g: "native.GpuSystem", step: int):
+        """Records the blocks that end at or before `step`, then lets the job
+        run to its next block boundary."""
+        while len(job._blocks) < len(job._bounds) and job._bounds[len(job._blocks)] <= step:
+            cur = output.Block.from_sums(g.averages()["sums"])
+            job._blocks.append(cur.minus(job._prev))
+            job._prev = cur
+        g.set_limits(Server._next_bound(job, step), job.equil)
 
     @staticmethod
     def _result(job: Job, g: "native.GpuSystem") -> dict:
@@ -123,6 +154,9 @@ class Server:
                "counters": st["counters"][:10].tolist(), "kT": kT}
         if job.keep_checkpoint:
             out["checkpoint"] = g.checkpoint()
+        if job.raspa_output:
+            out["blocks"] = list(job._blocks)
+            out["raspa_summary"] = output.summary_text(job.system, job._blocks)
         return out
 
     def run(self, jobs: Sequence[Job], realtime: bool = True) -> dict:
@@ -181,7 +215,13 @@ class Server:
             retired = set()
             for a in running:
                 job, g, done, fp = a
-                adv = min(self.chunk, job.steps - done)       # the engine stops each job at its limit
+                if job.raspa_output:
+                    # the engine stopped the job at its block boundary or ran the chunk
+                    step = int(g.state()["step"])
+                    adv = step - done
+                    self._close_blocks(job, g, step)
+                else:
+                    adv = min(self.chunk, job.steps - done)   # the engine stops each job at its limit
                 total_steps += adv
                 a[2] = done + adv
                 if a[2] >= job.steps:

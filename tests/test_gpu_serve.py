@@ -66,3 +66,29 @@ def test_memory_budget_limits_admission(cuda):
     assert st["max_active"] == 1
     assert all(j.result is not None and j.result["steps"] == j.steps for j in jobs)
     assert st["p99_job_ms"] >= st["p50_job_ms"] > 0
+
+
+def test_served_job_returns_raspa_output(cuda):
+    """A job with raspa_output returns its production as five equal blocks
+    (the job pauses at each boundary) and the `.data` results text; the
+    blocks add up to the job's own averages, and the reference's parser
+    layout is produced (tests/test_restart_output.py checks the parser)."""
+    from raspa2_b200 import output
+    s = dataclasses.replace(systems.tiny_co2_system(seed=7), pressure=1e6, temperature=298.0)
+    job = serve.Job(id=5, system=s, steps=2400, equil=400, seed=31, maxmol=64, raspa_output=True)
+    plain = serve.Job(id=5, system=s, steps=2400, equil=400, seed=31, maxmol=64)
+    serve.Server(chunk=300, threads=256).run([job], realtime=False)
+    serve.Server(chunk=300, threads=256).run([plain], realtime=False)
+    r = job.result
+    assert r["steps"] == 2400 and len(r["blocks"]) == output.NR_BLOCKS
+    assert [b.samples for b in r["blocks"]] == [400.0] * output.NR_BLOCKS
+    # pausing at the block boundaries leaves the trajectory unchanged; the
+    # energy sum is added up over other launches, so it may differ in the
+    # last bits
+    for key in ("loading", "samples", "final_nmol", "energy_terms", "counters"):
+        assert r[key] == plain.result[key], key
+    assert abs(r["energy_K"] - plain.result["energy_K"]) <= 1e-12 * abs(plain.result["energy_K"])
+    n = sum(b.n for b in r["blocks"]) / sum(b.samples for b in r["blocks"])
+    assert abs(n - r["loading"]) <= 1e-12 * max(1.0, n)
+    assert "Average loading absolute [molecules/unit cell]" in r["raspa_summary"]
+    assert "Enthalpy of adsorption:" in r["raspa_summary"]
