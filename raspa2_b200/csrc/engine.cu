@@ -109,6 +109,9 @@ struct Ctl {
   double cp[RGPU_MAX_ATOMS][3];
   double cpn[RGPU_MAX_ATOMS][3];
   double ub[RGPU_MAX_TRIALS];  /* bonded energies of the current bead's trials */
+  /* a retrace's beads: trial weight sum, the old bead's host VDW, adsorbate
+   * VDW, intramolecular LJ and bonded energy, any valid trial */
+  double rb[RGPU_MAX_ATOMS][6];
   double uintra, uintra_old;
   double dl[4];
   int nmol;
@@ -966,9 +969,150 @@ __device__ __forceinline__ void chain_angles_group(const RgpuSys &S, int i, int 
  * host and adsorbate VDW (u[0], u[2]) and the intramolecular energy
  * (uintra: bonded + LJ), or fail. Molecule m is the one retraced; `exclude`
  * leaves a molecule out of the adsorbate sums. All threads call. */
+/* The bend angles and dihedrals of beads 2.. of every trial of a growth
+ * stage into E.ang: 8 lanes per (bead, trial), four per warp. All threads
+ * call; the caller's next barrier publishes the table. */
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage)
+{
+  const RgpuSys &S = *E.S;
+  const int na = S.natom, nt = S.ntrial;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int ntask = na > 2 ? (na - 2) * nt : 0;
+  for (int t0 = (threadIdx.x >> 5) * 4; t0 < ntask; t0 += nw * 4) {
+    const int task = t0 + (lane >> 3);
+    const bool live = task < ntask;
+    const int i = live ? 2 + task / nt : 2, t = live ? task % nt : 0;
+    double th, ph;
+    chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
+    if (live && (lane & 7) == 0) {
+      double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+      a[0] = cos(th);
+      a[1] = sin(th);
+      a[2] = cos(ph);
+      a[3] = sin(ph);
+    }
+  }
+}
+
+/* Retrace of a flexible chain's configuration (RetraceMolecule,
+ * src/cbmc.c:3056-3181, for a linear chain). The beads a retrace "chooses"
+ * are the old ones, known before anything is evaluated, so the trial sets of
+ * several beads are placed together and evaluated at once: beads are taken
+ * in growth order in groups whose trials fit one evaluation (RGPU_MAX_POS
+ * positions; for 6 beads of 16 trials and 8 first-bead trials, two
+ * evaluations instead of six). Each bead's weights are summed by one warp in
+ * trial order, and the Rosenbluth weight and the energies are combined bead
+ * by bead in growth order, stopping at the first bead without a valid
+ * trial, as the bead-by-bead retrace does. The trials draw the same random
+ * numbers as that retrace (counter-based, by stage, bead and trial). All
+ * threads call. */
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, int m, int exclude)
+{
+  RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int na = S.natom, nf = S.ntrial_first, nt = S.ntrial;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) {
+    C.rosen = 1.0;
+    C.u[0] = C.u[1] = C.u[2] = C.u[3] = 0.0;
+    C.uintra = 0.0;
+    C.fail = 0;
+  }
+  if (threadIdx.x < na) atom_xyz(E, m, threadIdx.x, C.cp[threadIdx.x]);
+  chain_angles_table(E, stage);
+  __syncthreads();
+  for (int i0 = 0; i0 < na;) {
+    int i1 = i0, P = 0;
+    while (i1 < na && P + (i1 == 0 ? nf : nt) <= RGPU_MAX_POS) {
+      P += i1 == 0 ? nf : nt;
+      i1++;
+    }
+    for (int j = threadIdx.x; j < P; j += blockDim.x) {
+      int i = i0, t = j;
+      while (t >= (i == 0 ? nf : nt)) {
+        t -= i == 0 ? nf : nt;
+        i++;
+      }
+      double p[3];
+      if (t == 0) {
+        p[0] = C.cp[i][0];
+        p[1] = C.cp[i][1];
+        p[2] = C.cp[i][2];
+      } else if (i == 0) {
+        for (int d = 0; d < 3; d++)
+          p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
+      } else if (i == 1) {
+        const uint64_t step = E.step;
+        chain_trial(S, C.cp, i,
+                    [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); }, p);
+      } else {
+        const double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+        chain_place_trig(i >= 3 ? C.cp[i - 3] : nullptr, C.cp[i - 2], C.cp[i - 1], S.bond, a[0], a[1], a[2], a[3], p);
+      }
+      bead_set(E.pos[j], S, p[0], p[1], p[2], i, exclude);
+    }
+    __syncthreads();
+    engine_eval(E, P, 0);
+    const int b = E.xb;
+    E.xb ^= 1;
+    /* warp g: bead i0 + g, its trials at positions off .. off + k */
+    for (int g = warp; g < i1 - i0; g += nw) {
+      const int i = i0 + g, k = i == 0 ? nf : nt;
+      const int off = i0 == 0 ? (i == 0 ? 0 : nf + (i - 1) * nt) : g * nt;
+      double r[4] = {0.0, 0.0, 0.0, 0.0}, lj = 0.0, bf = 0.0;
+      int o = 0, ov = 0;
+      if (lane < k) {
+        gather(E, b, off + lane, r, o);
+        const double p[3] = {E.pos[off + lane].x, E.pos[off + lane].y, E.pos[off + lane].z};
+        lj = chain_intra_lj(S, C.cp, i, p);
+        ov = r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap || lj >= S.overlap;
+        bf = -S.beta * (r[0] + r[2] + lj);
+      }
+      const bool valid = lane < k && !ov;
+      const double w = valid ? exp(bf) : 0.0;
+      const bool any = __ballot_sync(RGPU_FULL, valid) != 0u;
+      double wsum = 0.0;
+      for (int t = 0; t < k; t++) wsum += __shfl_sync(RGPU_FULL, w, t);
+      if (lane == 0) {
+        double *rb = C.rb[i];
+        rb[0] = wsum;
+        rb[1] = r[0];
+        rb[2] = r[2];
+        rb[3] = lj;
+        rb[4] = i >= 2 ? chain_bonded_energy(S, C.cp, i, C.cp[i]) : 0.0;
+        rb[5] = any ? 1.0 : 0.0;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int i = i0; i < i1 && !C.fail; i++) {
+        const double *rb = C.rb[i];
+        C.rosen *= rb[0] / (double)(i == 0 ? nf : nt);
+        C.u[0] += rb[1];
+        C.u[2] += rb[2];
+        C.uintra += rb[3];
+        if (i >= 2) C.uintra += rb[4];
+        if (rb[5] == 0.0) {
+          C.fail = 1;
+          C.cnt[RGPU_CNT_OVERLAP]++;
+        }
+      }
+    }
+    __syncthreads();
+    if (C.fail) return;
+    i0 = i1;
+  }
+}
+
 template <bool MIXED, bool FLEX>
 __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, int stage, int m, int exclude)
 {
+  if (retrace) {
+    retrace_chain(E, stage, m, exclude);
+    return;
+  }
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
   const int na = S.natom, nf = S.ntrial_first, nt = S.ntrial;
@@ -978,27 +1122,9 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
     C.uintra = 0.0;
     C.fail = 0;
   }
-  /* the bend angles and dihedrals of beads 2.. of every trial: 8 lanes per
-   * (bead, trial), four per warp, ahead of the first bead (the first barrier
-   * below publishes them) */
-  {
-    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int ntask = na > 2 ? (na - 2) * nt : 0;
-    for (int t0 = (threadIdx.x >> 5) * 4; t0 < ntask; t0 += nw * 4) {
-      const int task = t0 + (lane >> 3);
-      const bool live = task < ntask;
-      const int i = live ? 2 + task / nt : 2, t = live ? task % nt : 0;
-      double th, ph;
-      chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
-      if (live && (lane & 7) == 0) {
-        double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
-        a[0] = cos(th);
-        a[1] = sin(th);
-        a[2] = cos(ph);
-        a[3] = sin(ph);
-      }
-    }
-  }
+  /* the bend angles and dihedrals of beads 2.. of every trial, ahead of the
+   * first bead (the first barrier below publishes them) */
+  chain_angles_table(E, stage);
   for (int i = 0; i < na; i++) {
     const int k = i == 0 ? nf : nt;
     if (threadIdx.x < k) {
