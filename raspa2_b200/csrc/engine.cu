@@ -556,6 +556,13 @@ __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool
     if (m >= nmol) m = nmol - 1;
   }
   const int exclude = insert ? -1 : m;
+  const int nb = na - 1;   /* beads grown per orientation trial */
+  const bool ew = S.ewald && S.mol_charged;
+  /* a deletion retraces the old molecule: its first bead and orientation
+   * are trial 0 of each stage, known up front, so both stages' trials and
+   * the Ewald sum of the removed molecule go into one evaluation (first-bead
+   * trials at positions 0..nf, orientation t's beads at nf + t*nb + j) */
+  const bool one = !insert && nf + (na > 1 ? nt * nb : 0) <= RGPU_MAX_POS;
   /* first-bead trials */
   if (threadIdx.x < nf) {
     const int i = threadIdx.x;
@@ -569,8 +576,45 @@ __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool
     }
     bead_set(E.pos[i], S, p[0], p[1], p[2], sb, exclude);
   }
+  if (one) {
+    /* the retrace orientations about the old first bead (trial 0: the old
+     * one) and the removed molecule's Ewald sites (nf, nt <= 16, na <= 8;
+     * blocks have at least 64 threads) */
+    if (na > 1 && threadIdx.x >= 32 && threadIdx.x < 32 + nt) {
+      const int t = threadIdx.x - 32;
+      double o[3];
+      atom_xyz(E, m, sb, o);
+      double R[3][3];
+      if (t > 0)
+        random_rotation(E.rnd[SLOT_ORIENT + 4 * t + 0], E.rnd[SLOT_ORIENT + 4 * t + 1],
+                        E.rnd[SLOT_ORIENT + 4 * t + 2], R);
+      int j = 0;
+      for (int a = 0; a < na; a++) {
+        if (a == sb) continue;
+        double p[3];
+        if (t == 0) {
+          atom_xyz(E, m, a, p);
+        } else {
+          const double c[3] = {S.mol_ref[a][0] - S.mol_ref[sb][0], S.mol_ref[a][1] - S.mol_ref[sb][1],
+                               S.mol_ref[a][2] - S.mol_ref[sb][2]};
+          p[0] = o[0] + c[0] * R[0][0] + c[1] * R[0][1] + c[2] * R[0][2];
+          p[1] = o[1] + c[0] * R[1][0] + c[1] * R[1][1] + c[2] * R[1][2];
+          p[2] = o[2] + c[0] * R[2][0] + c[1] * R[2][1] + c[2] * R[2][2];
+        }
+        bead_set(E.pos[nf + t * nb + j], S, p[0], p[1], p[2], a, exclude);
+        j++;
+      }
+    }
+    if (threadIdx.x >= 48 && threadIdx.x < 48 + na) {
+      const int a = threadIdx.x - 48;
+      double p[3];
+      atom_xyz(E, m, a, p);
+      bead_set(E.sites[a].b, S, p[0], p[1], p[2], a, exclude);
+      E.sites[a].q = -S.mol_q[a];
+    }
+  }
   __syncthreads();
-  engine_eval(E, nf, 0);
+  engine_eval(E, one ? nf + (na > 1 ? nt * nb : 0) : nf, 0, one && ew ? na : 0);
   int b1 = E.xb;
   E.xb ^= 1;
   if (threadIdx.x < 32) {
@@ -585,11 +629,23 @@ __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool
       C.first = E.pos[sel];
       if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
     }
+    if (one && na > 1 && any) {
+      /* the retrace orientations (trial 0 is the old one, not selected) */
+      cbmc_trials(E, b1, nt, nb, false, false, E.rnd[SLOT_ORIENT_SELECT], wsum, sel, u, any, nf);
+      if (threadIdx.x == 0) {
+        if (!any) C.fail = 1;
+        else {
+          C.rosen *= wsum / (double)nt;
+          for (int k = 0; k < 4; k++) C.u[k] += u[k];
+        }
+        C.sel = sel;
+        if (C.fail) C.cnt[RGPU_CNT_OVERLAP]++;
+      }
+    }
   }
   __syncthreads();
   if (C.fail) return;
-  const int nb = na - 1;   /* beads grown per orientation trial */
-  if (na > 1) {
+  if (na > 1 && !one) {
     const BeadPos first = C.first;
     if (threadIdx.x < nt) {
       const int t = threadIdx.x;
@@ -642,25 +698,26 @@ __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool
     __syncthreads();
     if (C.fail) return;
   }
-  /* sites of the chosen configuration: first bead + beads of trial C.sel */
-  if (threadIdx.x < na) {
-    const int a = threadIdx.x;
-    BeadPos bp;
-    if (a == sb) bp = C.first;
-    else {
-      int j = a < sb ? a : a - 1;
-      bp = E.pos[C.sel * nb + j];
+  int bw = b1;
+  if (!one) {
+    /* sites of the chosen configuration: first bead + beads of trial C.sel */
+    if (threadIdx.x < na) {
+      const int a = threadIdx.x;
+      BeadPos bp;
+      if (a == sb) bp = C.first;
+      else {
+        int j = a < sb ? a : a - 1;
+        bp = E.pos[C.sel * nb + j];
+      }
+      E.sites[a].b = bp;
+      E.sites[a].q = insert ? S.mol_q[a] : -S.mol_q[a];
     }
-    E.sites[a].b = bp;
-    E.sites[a].q = insert ? S.mol_q[a] : -S.mol_q[a];
-  }
-  __syncthreads();
-  const bool ew = S.ewald && S.mol_charged;
-  int bw = 0;
-  if (ew) {
-    engine_ewald(E, na);
-    bw = E.xb;
-    E.xb ^= 1;
+    __syncthreads();
+    if (ew) {
+      engine_ewald(E, na);
+      bw = E.xb;
+      E.xb ^= 1;
+    }
   }
   if (threadIdx.x == 0) {
     /* LJ-biasing correction, src/cbmc.c:3171-3178 / :3044-3051 */
