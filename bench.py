@@ -266,9 +266,11 @@ def run_ours(args):
     if not (args.threads and args.cluster):
         from raspa2_b200 import autotune
         tuned = autotune.tune(gs, precision=prec)
-        shape = {"cluster": tuned.cluster, "threads": tuned.threads, "tuned": True, "table": tuned.table}
+        shape = {"cluster": tuned.cluster, "threads": tuned.threads, "tuned": True,
+                 "split": {"systems": len(tuned.split), "cluster": tuned.cluster_b}, "table": tuned.table}
         eng.close()
         eng = native.Engine(gs, precision=prec, threads=tuned.threads, cluster=tuned.cluster)
+        tuned.apply(eng)
         eng.run(args.moves_per_step, stream.cuda_stream)
         torch.cuda.synchronize()
     c0 = counters()
@@ -350,7 +352,7 @@ def run_ours(args):
                    "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
                    "framework_atoms": [int(s.n_framework()) for s in sys_list[:8]] + ["..."],
                    "mean_loading": float(np.mean(loads))},
-        "wall_s": t_wall, "gpu_launches": args.steps,
+        "wall_s": t_wall, "gpu_launches": args.steps * (2 if eng.split[0] else 1),
         "status_nonzero_systems": int(sum(1 for s in status if s)),
         "load_balance": imbalance, "cluster": eng.cluster,
         "acceptance": {k: (float(d[4 + i]) / max(float(d[i]), 1.0)) for i, k in
@@ -436,6 +438,7 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
     tuned = autotune.tune(gs, precision=native.RGPU_MIXED)
     e.close()
     e = native.Engine(gs, precision=native.RGPU_MIXED, threads=tuned.threads, cluster=tuned.cluster)
+    tuned.apply(e)
     e.run(args.hexane_moves, stream.cuda_stream)
     e.sync()
     c0 = np.array([g.state()["counters"] for g in gs])
@@ -476,7 +479,8 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
     out = {"workload": "hexane_grid_cbmc_64 (4096-atom 40 A framework, 64 pressures 1e2-1e6 Pa, 433 K)",
            "systems": len(gs), "moves_per_step_per_system": args.hexane_moves, "steps": steps,
            "moves_per_s": moves / t, "ms_per_step": 1000.0 * t / steps,
-           "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads},
+           "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads,
+                            "split": {"systems": len(tuned.split), "cluster": tuned.cluster_b}},
            "grid": {"spacing_A": args.hexane_spacing, "points_per_axis": [int(x) + 1 for x in geom[0]],
                     "bytes_per_grid": int(np.prod(geom[0].astype(np.int64) + 1) * 32), "types": 2,
                     "build_s": t_build},

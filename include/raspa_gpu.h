@@ -237,6 +237,14 @@ int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *systems, int n,
                           int cluster, int ctas_per_sm);
 /* CTAs per system of an engine. */
 int rgpu_engine_cluster(rgpu_engine *eng);
+/* Runs the systems second[0..nsecond) (indices into the engine's systems)
+ * in a second launch with clusters of `cluster_b` CTAs (1, 2, 4 or 8), side
+ * by side with the launch of the others on a stream of the engine's own;
+ * rgpu_engine_run's stream waits for both. One cluster size per launch, so
+ * this is how the costliest systems get more CTAs, on SMs a single launch
+ * would leave idle. nsecond = 0 returns to one launch. Synchronises the
+ * device. No counterpart in the reference. */
+int rgpu_engine_set_split(rgpu_engine *eng, const int *second, int nsecond, int cluster_b);
 int rgpu_engine_destroy(rgpu_engine *eng);
 /* Advances every system by `nsteps` MC moves (asynchronous on `stream`, a
  * cudaStream_t or NULL for the library stream). */

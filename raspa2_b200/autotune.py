@@ -12,6 +12,11 @@ The best pair depends on the number of boxes against the SM count, on the
 framework sizes and on the loadings. Measured on a B200 for 64 CO2 boxes of
 512-4096 atoms, cluster x threads gave 0.22-1.48 M moves/s.
 
+When the best shape leaves SMs idle (64 boxes at 2 CTAs each fill 128 of
+148), the costliest boxes, by the clock cycles they spent in the best run,
+can run in a second launch at twice the cluster size beside the first
+(`Engine.set_split`); the tuner times such splits too.
+
 `tune()` times every admissible shape on copies of the caller's boxes (same
 force fields, configurations and random seeds), so the caller's state does
 not move, and returns the fastest. Results are cached per batch signature
@@ -35,14 +40,24 @@ class Shape:
     threads: int
     moves_per_s: float
     table: List[dict]
+    split: Tuple[int, ...] = ()     # boxes run in a second launch
+    cluster_b: int = 0              # its cluster size
+
+    def apply(self, eng: "native.Engine") -> None:
+        """Sets the split of this shape on an engine built with its cluster
+        and threads."""
+        if self.split:
+            eng.set_split(self.split, self.cluster_b)
 
 
-def _signature(systems: Sequence["native.GpuSystem"], precision: int) -> tuple:
+def _signature(systems: Sequence["native.GpuSystem"], precision: int, ordered: bool = False) -> tuple:
+    """Key of a batch: its boxes' sizes, sorted (in order when `ordered`,
+    for shapes that name boxes by index)."""
     sig = []
     for g in systems:
         fw = g.sysm.framework()[0]
         sig.append((len(fw), g.natom, tuple(g.sysm.kmax), g.maxmol, bool(getattr(g, "grids_active", False))))
-    return (precision, tuple(sorted(sig)))
+    return (precision, tuple(sig) if ordered else tuple(sorted(sig)))
 
 
 def candidates(nsys: int, precision: int, sms: int) -> List[Tuple[int, int]]:
@@ -68,49 +83,81 @@ def _clone(g: "native.GpuSystem", xyz: np.ndarray) -> "native.GpuSystem":
 
 
 def tune(systems: Sequence["native.GpuSystem"], precision: int = native.RGPU_MIXED, moves: int = 400,
-         warm: int = 100, shapes: Optional[Sequence[Tuple[int, int]]] = None, use_cache: bool = True) -> Shape:
+         warm: int = 100, shapes: Optional[Sequence[Tuple[int, int]]] = None, use_cache: bool = True,
+         split: bool = True) -> Shape:
     """Times each candidate shape on copies of `systems` and returns the
-    fastest as a Shape (with the full table of measurements)."""
+    fastest as a Shape (with the full table of measurements). With `split`,
+    and when the candidates are the default ones, splits of the best shape
+    that fill the idle SMs are timed as well."""
     import torch
 
-    key = _signature(systems, precision)
+    key = (_signature(systems, precision, ordered=split), split)
     if use_cache and shapes is None and key in _CACHE:
         return _CACHE[key]
     props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    auto_split = split and shapes is None
     shapes = list(shapes) if shapes is not None else candidates(len(systems), precision, props.multi_processor_count)
     start = [g.adsorbates() for g in systems]
     clones = [_clone(g, x) for g, x in zip(systems, start)]
     stream = torch.cuda.Stream()
     table = []
     best = None
-    for c, t in shapes:
+
+    def time_shape(c, t, split=()):
+        """moves/s of one shape and each box's clock cycles in the timed run"""
         for g, x in zip(clones, start):
             g.set_adsorbates(x)
+        eng = native.Engine(clones, precision=precision, threads=t, cluster=c)
         try:
-            eng = native.Engine(clones, precision=precision, threads=t, cluster=c)
+            if split:
+                eng.set_split(split, 2 * c)
+            eng.run(warm, stream.cuda_stream)
+            torch.cuda.synchronize()
+            c0 = [g.state()["counters"] for g in clones]
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            eng.run(moves, stream.cuda_stream)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            c1 = [g.state()["counters"] for g in clones]
+        finally:
+            eng.close()
+        rate = sum(int(b[8]) - int(a[8]) for a, b in zip(c0, c1)) / (ms / 1e3)
+        return rate, [int(b[15]) - int(a[15]) for a, b in zip(c0, c1)]
+
+    cycles = None
+    for c, t in shapes:
+        try:
+            rate, cyc = time_shape(c, t)
         except native.NativeError as e:
             table.append({"cluster": c, "threads": t, "error": str(e)})
             continue
-        eng.run(warm, stream.cuda_stream)
-        torch.cuda.synchronize()
-        m0 = sum(int(g.state()["counters"][8]) for g in clones)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        eng.run(moves, stream.cuda_stream)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
-        m1 = sum(int(g.state()["counters"][8]) for g in clones)
-        rate = (m1 - m0) / (ms / 1e3)
-        eng.close()
         table.append({"cluster": c, "threads": t, "moves_per_s": rate})
         if best is None or rate > best[2]:
-            best = (c, t, rate)
+            best = (c, t, rate, ())
+            cycles = cyc
+    if best is not None and auto_split:
+        c, t = best[0], best[1]
+        spare = props.multi_processor_count - len(systems) * c
+        kmax = min(spare // c, len(systems) - 1) if 2 * c <= 8 else 0
+        by_cost = list(np.argsort(cycles)[::-1])
+        for k in sorted({kmax, kmax // 2} - {0}, reverse=True):
+            split = tuple(int(i) for i in by_cost[:k])
+            try:
+                rate, _ = time_shape(c, t, split)
+            except native.NativeError as e:
+                table.append({"cluster": c, "threads": t, "split": k, "cluster_b": 2 * c, "error": str(e)})
+                continue
+            table.append({"cluster": c, "threads": t, "split": k, "cluster_b": 2 * c, "moves_per_s": rate})
+            if rate > best[2]:
+                best = (c, t, rate, split)
     for g in clones:
         g.close()
     if best is None:
         raise native.NativeError("no launch shape could be created for this batch")
-    shape = Shape(cluster=best[0], threads=best[1], moves_per_s=best[2], table=table)
+    shape = Shape(cluster=best[0], threads=best[1], moves_per_s=best[2], table=table, split=best[3],
+                  cluster_b=2 * best[0] if best[3] else 0)
     if use_cache:
         _CACHE[key] = shape
     return shape

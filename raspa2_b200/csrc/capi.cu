@@ -111,7 +111,59 @@ struct rgpu_engine {
   unsigned long long *d_off;
   unsigned char *d_stage;
   unsigned char *h_stage;     /* pinned */
+  /* device slot j of d_systems (and of d_off) holds system order[j]. Slots
+   * [0, n - nsplit) run in one launch at `cluster`; the last nsplit slots in
+   * a second launch at cluster_b on st_b, side by side with the first
+   * (rgpu_engine_set_split). */
+  std::vector<int> order;
+  int smem_max;
+  int nsplit, cluster_b, fw_items_b, tile_items_b, k_items_b;
+  size_t smem_b;
+  cudaStream_t st_b;
+  cudaEvent_t ev_fork, ev_join;
 };
+
+/* Launch parameters of the systems in device slots [lo, hi) at a cluster
+ * size: each CTA's share of the framework (tiles) and of the wave vectors,
+ * staged in shared memory as far as it fits, in order of preference:
+ * framework share and wave vectors, framework only, wave vectors only,
+ * neither. Returns false when not even the adsorbates fit. */
+struct EngineGroup {
+  int fw_items, tile_items, k_items;
+  size_t smem;
+};
+
+static bool plan_group(const rgpu_engine *e, int lo, int hi, int cluster, EngineGroup &g)
+{
+  int maxfw = 0, maxtile = 0, maxk = 0;
+  bool all_grids = true;
+  for (int j = lo; j < hi; j++) {
+    const rgpu_system *s = e->sys[e->order[j]];
+    all_grids = all_grids && s->h.use_grid;
+    maxfw = std::max(maxfw, (s->d.nfw + cluster - 1) / cluster);
+    maxtile = std::max(maxtile, (s->h.ntile + cluster - 1) / cluster);
+    if (s->h.ewald) maxk = std::max(maxk, (s->h.nk + cluster - 1) / cluster);
+  }
+  int fw = e->mixed ? maxtile * RGPU_TILE : maxfw, tiles = e->mixed ? maxtile : 0;
+  if (all_grids) {
+    /* no framework pairs are evaluated: nothing of the framework to stage */
+    fw = 0;
+    tiles = 0;
+  }
+  const int fw_try[4] = {fw, fw, 0, 0}, tile_try[4] = {tiles, tiles, 0, 0}, k_try[4] = {maxk, 0, maxk, 0};
+  for (int t = 0; t < 4; t++) {
+    const size_t b = rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t],
+                                            e->threads, e->flex);
+    if (b <= (size_t)e->smem_max) {
+      g.fw_items = fw_try[t];
+      g.tile_items = tile_try[t];
+      g.k_items = k_try[t];
+      g.smem = b;
+      return true;
+    }
+  }
+  return false;
+}
 
 static void sys_free(rgpu_system *s)
 {
@@ -1120,6 +1172,24 @@ extern "C" int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts
   return RGPU_SUCCESS;
 }
 
+/* The device slots: d_systems[j] = system order[j], its framework staged in
+ * shared memory when its launch group stages it; d_off (once the staging
+ * buffer exists) in the same slot order. */
+static cudaError_t upload_slots(rgpu_engine *e)
+{
+  const int n = (int)e->sys.size();
+  std::vector<RgpuSys> hs(n);
+  for (int j = 0; j < n; j++) {
+    hs[j] = e->sys[e->order[j]]->h;
+    hs[j].smem_fw = (j < n - e->nsplit ? e->fw_items : e->fw_items_b) > 0;
+  }
+  cudaError_t err = cudaMemcpy(e->d_systems, hs.data(), sizeof(RgpuSys) * n, cudaMemcpyHostToDevice);
+  if (err != cudaSuccess || !e->d_off) return err;
+  std::vector<unsigned long long> off(n);
+  for (int j = 0; j < n; j++) off[j] = e->off[e->order[j]];
+  return cudaMemcpy(e->d_off, off.data(), sizeof(unsigned long long) * n, cudaMemcpyHostToDevice);
+}
+
 /* ---------------------------------------------------------------------- */
 /* Cluster size of an engine launch: the CTAs of one system. More CTAs per
  * system when there are few systems (up to 8, the portable cluster size),
@@ -1168,23 +1238,18 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->cluster = cluster ? cluster : auto_cluster(n);
   e->kw = 1;
   e->max_ads = 0;
-  int maxfw = 0, maxtile = 0, maxk = 0;
-  bool all_grids = true;
   for (int i = 0; i < n; i++) {
     rgpu_system *s = systems[i];
     if (!s) { delete e; return fail(RGPU_E_INVALID, "null system"); }
     e->sys.push_back(s);
+    e->order.push_back(i);
     if (s->h.use_grid && s->h.mol_charged && !s->h.use_coul_grid) {
       delete e;
       return fail(RGPU_E_INVALID, "system with VDW grids and a charged molecule but no Coulomb grid");
     }
-    all_grids = all_grids && s->h.use_grid;
     e->flex = e->flex || s->h.use_grid || s->h.flexible;
     e->kw = std::max(e->kw, s->kw);
     e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
-    maxfw = std::max(maxfw, (s->d.nfw + e->cluster - 1) / e->cluster);
-    maxtile = std::max(maxtile, (s->h.ntile + e->cluster - 1) / e->cluster);
-    if (s->h.ewald) maxk = std::max(maxk, (s->h.nk + e->cluster - 1) / e->cluster);
   }
   int dev = 0, smem_max = 0;
   cudaGetDevice(&dev);
@@ -1196,36 +1261,22 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
     cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     smem_max = std::min(smem_max, per_sm / ctas_per_sm - 1024);
   }
-  if (e->mixed) {
-    e->tile_items = maxtile;
-    e->fw_items = maxtile * RGPU_TILE;
-  } else {
-    e->tile_items = 0;
-    e->fw_items = maxfw;
-  }
-  if (all_grids) {
-    /* no framework pairs are evaluated: nothing of the framework to stage */
-    e->tile_items = 0;
-    e->fw_items = 0;
-  }
-  /* shared-memory staging, in order of preference: framework share and wave
-   * vectors, framework only, wave vectors only, neither */
-  const int fw_try[4] = {e->fw_items, e->fw_items, 0, 0}, tile_try[4] = {e->tile_items, e->tile_items, 0, 0};
-  const int k_try[4] = {maxk, 0, maxk, 0};
-  int pick = -1;
-  for (int t = 0; t < 4 && pick < 0; t++)
-    if (rgpu_engine_smem_bytes(e->mixed, fw_try[t], tile_try[t], e->max_ads, e->kw, k_try[t], threads, e->flex) <=
-        (size_t)smem_max)
-      pick = t;
-  if (pick < 0) {
+  e->smem_max = smem_max;
+  EngineGroup g;
+  if (!plan_group(e, 0, n, e->cluster, g)) {
     delete e;
     return fail(RGPU_E_INVALID, "adsorbate capacity does not fit in shared memory");
   }
-  e->fw_items = fw_try[pick];
-  e->tile_items = tile_try[pick];
-  e->k_items = k_try[pick];
-  e->smem = rgpu_engine_smem_bytes(e->mixed, e->fw_items, e->tile_items, e->max_ads, e->kw, e->k_items, threads,
-                                   e->flex);
+  e->fw_items = g.fw_items;
+  e->tile_items = g.tile_items;
+  e->k_items = g.k_items;
+  e->smem = g.smem;
+  e->nsplit = 0;
+  e->cluster_b = 0;
+  e->fw_items_b = e->tile_items_b = e->k_items_b = 0;
+  e->smem_b = 0;
+  e->st_b = nullptr;
+  e->ev_fork = e->ev_join = nullptr;
   e->use_graph = 0;
   e->gexec = nullptr;
   e->g_nsteps = -1;
@@ -1233,17 +1284,12 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->d_off = nullptr;
   e->d_stage = nullptr;
   e->h_stage = nullptr;
-  std::vector<RgpuSys> hs(n);
-  for (int i = 0; i < n; i++) {
-    hs[i] = e->sys[i]->h;
-    hs[i].smem_fw = e->fw_items > 0;
-  }
   if (cudaMalloc((void **)&e->d_systems, sizeof(RgpuSys) * n) != cudaSuccess) {
     delete e;
     return fail(RGPU_E_CUDA, "cudaMalloc engine");
   }
   e->st = e->sys[0]->st;
-  if (cudaMemcpy(e->d_systems, hs.data(), sizeof(RgpuSys) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (upload_slots(e) != cudaSuccess) {
     cudaFree(e->d_systems);
     delete e;
     return fail(RGPU_E_CUDA, "upload engine");
@@ -1259,9 +1305,90 @@ extern "C" int rgpu_engine_destroy(rgpu_engine *e)
   if (e->d_off) cudaFree(e->d_off);
   if (e->d_stage) cudaFree(e->d_stage);
   if (e->h_stage) cudaFreeHost(e->h_stage);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
+  if (e->st_b) cudaStreamDestroy(e->st_b);
   cudaFree(e->d_systems);
   delete e;
   return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_engine_set_split(rgpu_engine *e, const int *second, int nsecond, int cluster_b)
+{
+  if (!e || nsecond < 0 || (nsecond > 0 && !second)) return fail(RGPU_E_INVALID, "bad argument");
+  const int n = (int)e->sys.size();
+  if (nsecond >= n) return fail(RGPU_E_INVALID, "the first launch needs at least one system");
+  if (nsecond > 0 && (cluster_b < 1 || cluster_b > 8 || (cluster_b & (cluster_b - 1))))
+    return fail(RGPU_E_INVALID, "cluster %d", cluster_b);
+  std::vector<char> in_b(n, 0);
+  for (int k = 0; k < nsecond; k++) {
+    if (second[k] < 0 || second[k] >= n || in_b[second[k]])
+      return fail(RGPU_E_INVALID, "system index %d out of range or repeated", second[k]);
+    in_b[second[k]] = 1;
+  }
+  std::vector<int> order;
+  for (int i = 0; i < n; i++)
+    if (!in_b[i]) order.push_back(i);
+  for (int k = 0; k < nsecond; k++) order.push_back(second[k]);
+  const std::vector<int> old_order = e->order;
+  e->order = order;
+  EngineGroup ga, gb = {0, 0, 0, 0};
+  if (!plan_group(e, 0, n - nsecond, e->cluster, ga) || (nsecond > 0 && !plan_group(e, n - nsecond, n, cluster_b, gb))) {
+    e->order = old_order;
+    return fail(RGPU_E_INVALID, "adsorbate capacity does not fit in shared memory");
+  }
+  if (nsecond > 0 && !e->st_b) {
+    if (cudaStreamCreateWithFlags(&e->st_b, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      e->order = old_order;
+      return fail(RGPU_E_CUDA, "split streams");
+    }
+  }
+  /* launches and staging kernels in flight (on any stream) read the old slots */
+  CK(cudaDeviceSynchronize());
+  e->fw_items = ga.fw_items;
+  e->tile_items = ga.tile_items;
+  e->k_items = ga.k_items;
+  e->smem = ga.smem;
+  e->nsplit = nsecond;
+  e->cluster_b = nsecond > 0 ? cluster_b : 0;
+  e->fw_items_b = gb.fw_items;
+  e->tile_items_b = gb.tile_items;
+  e->k_items_b = gb.k_items;
+  e->smem_b = gb.smem;
+  if (e->gexec) {
+    cudaGraphExecDestroy(e->gexec);
+    e->gexec = nullptr;
+  }
+  CK(upload_slots(e));
+  return RGPU_SUCCESS;
+}
+
+/* The engine launch(es) of nsteps steps on stream st: the first group of
+ * slots there, the second (if any) on st_b, forked from st and joined back,
+ * so that both run side by side and st waits for both (also under stream
+ * capture, where the fork and join become graph edges). */
+static cudaError_t engine_launch_all(rgpu_engine *e, long long nsteps, cudaStream_t st)
+{
+  const int n = (int)e->sys.size(), na = n - e->nsplit;
+  cudaError_t err;
+  if (e->nsplit > 0) {
+    if ((err = cudaEventRecord(e->ev_fork, st)) != cudaSuccess) return err;
+    if ((err = cudaStreamWaitEvent(e->st_b, e->ev_fork, 0)) != cudaSuccess) return err;
+  }
+  err = rgpu_engine_launch(e->mixed, e->d_systems, na, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
+                           e->k_items, e->cluster, e->threads, e->wide, e->flex, st);
+  if (e->nsplit > 0) {
+    cudaError_t eb = rgpu_engine_launch(e->mixed, e->d_systems + na, e->nsplit, nsteps, e->kw, e->max_ads,
+                                        e->fw_items_b, e->tile_items_b, e->k_items_b, e->cluster_b, e->threads,
+                                        e->wide, e->flex, e->st_b);
+    if (err == cudaSuccess) err = eb;
+    cudaError_t ej = cudaEventRecord(e->ev_join, e->st_b);
+    if (ej == cudaSuccess) ej = cudaStreamWaitEvent(st, e->ev_join, 0);
+    if (err == cudaSuccess) err = ej;
+  }
+  return err;
 }
 
 extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
@@ -1270,11 +1397,9 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
   cudaStream_t st = stream ? (cudaStream_t)stream : e->st;
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
-  const int n = (int)e->sys.size();
-  CK(rgpu_engine_prepare(e->mixed, e->wide, e->flex, e->smem));
+  CK(rgpu_engine_prepare(e->mixed, e->wide, e->flex, std::max(e->smem, e->smem_b)));
   if (!e->use_graph) {
-    CK(rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items, e->tile_items,
-                          e->k_items, e->cluster, e->threads, e->wide, e->flex, st));
+    CK(engine_launch_all(e, nsteps, st));
   } else {
     if (!e->gexec || e->g_nsteps != nsteps) {
       if (e->gexec) {
@@ -1283,8 +1408,7 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
       }
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      cudaError_t le = rgpu_engine_launch(e->mixed, e->d_systems, n, nsteps, e->kw, e->max_ads, e->fw_items,
-                                          e->tile_items, e->k_items, e->cluster, e->threads, e->wide, e->flex, st);
+      cudaError_t le = engine_launch_all(e, nsteps, st);
       cudaError_t ce = cudaStreamEndCapture(st, &g);
       if (le != cudaSuccess || ce != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
@@ -1336,7 +1460,7 @@ static int engine_staging(rgpu_engine *e)
     e->h_stage = nullptr;
     return fail(RGPU_E_CUDA, "engine staging allocation");
   }
-  CK(cudaMemcpy(e->d_off, e->off.data(), sizeof(unsigned long long) * n, cudaMemcpyHostToDevice));
+  CK(upload_slots(e));
   return RGPU_SUCCESS;
 }
 

@@ -30,7 +30,7 @@ EXPORTS = [
     "rgpu_grid_interpolate", "rgpu_engine_create", "rgpu_engine_destroy", "rgpu_engine_run",
     "rgpu_engine_sync", "rgpu_system_state", "rgpu_system_set_energy", "rgpu_fp32_peak_probe",
     "rgpu_engine_cluster", "rgpu_grid_interpolate_noalloc", "rgpu_system_set_limits", "rgpu_system_averages",
-    "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_intra_energy",
+    "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_engine_set_split", "rgpu_intra_energy",
     "rgpu_system_set_grids", "rgpu_system_checkpoint_size", "rgpu_system_checkpoint", "rgpu_system_restore",
     "rgpu_grid_build_coulomb", "rgpu_system_set_coulomb_grid", "rgpu_engine_get_state", "rgpu_engine_set_adsorbates",
     "rgpu_engine_staging_bytes",
@@ -432,6 +432,7 @@ class Engine:
         self.precision = precision
         self.h = h
         self.systems = list(systems)
+        self.split = ([], 0)
 
     def run(self, nsteps: int, stream: Optional[int] = None):
         _check(load().rgpu_engine_run(self.h, C.c_longlong(nsteps), C.c_void_p(stream or 0)))
@@ -478,6 +479,15 @@ class Engine:
         n = C.c_size_t()
         _check(load().rgpu_engine_staging_bytes(self.h, C.byref(n)))
         return n.value
+
+    def set_split(self, second: Sequence[int], cluster_b: int):
+        """Run the systems at indices `second` in a second launch with
+        clusters of `cluster_b` CTAs, beside the first (rgpu_engine_set_split);
+        an empty `second` returns to one launch."""
+        idx = [int(i) for i in second]
+        arr = (C.c_int * max(len(idx), 1))(*idx)
+        _check(load().rgpu_engine_set_split(self.h, arr, C.c_int(len(idx)), C.c_int(cluster_b)))
+        self.split = (idx, int(cluster_b) if idx else 0)
 
     def use_graph(self, on: bool = True):
         """Replay a CUDA graph of the launch in run() (rgpu_engine_use_graph)."""

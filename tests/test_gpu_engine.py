@@ -194,3 +194,52 @@ def test_graph_replay_matches_direct_launches(cuda):
     np.testing.assert_array_equal(a["counters"][:15], b["counters"][:15])
     np.testing.assert_array_equal(a["energy"], b["energy"])
     np.testing.assert_array_equal(xa, xb)
+
+
+def test_split_launch_matches_single_runs(cuda):
+    """rgpu_engine_set_split: the systems moved to a second launch at cluster
+    2 run bitwise as they do alone at cluster 2, the others as alone at
+    cluster 1, also when the two launches are replayed from one CUDA graph;
+    the batched state read (device slots reordered) returns each system's
+    own state, and a batched upload reaches the right systems."""
+    specs = [systems.tiny_co2_system(seed=7), systems.co2_system(seed=21, n_atoms=512, cell=20.0, kmax=5),
+             systems.methane_system(seed=3)]
+    second = [2, 0]
+    n = 200
+    alone = []
+    for i, s in enumerate(specs):
+        g, st = engine_run(s, np.zeros((0, s.molecule.n_atoms, 3)), n, native.RGPU_MIXED, seed=5, stream_id=i,
+                           cluster=2 if i in second else 1)
+        alone.append((st, g.adsorbates()))
+    gs = []
+    for i, s in enumerate(specs):
+        g = native.GpuSystem(s, maxmol=64, seed=5, stream_id=i)
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+        gs.append(g)
+    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=256, cluster=1)
+    e.set_split(second, 2)
+    e.use_graph(True)
+    e.run(n)
+    e.sync()
+    batched = e.get_states()
+    for g, b, (st, xyz) in zip(gs, batched, alone):
+        st2 = g.state()
+        np.testing.assert_array_equal(st2["counters"][:15], st["counters"][:15])
+        assert st2["nmol"] == st["nmol"] and b["nmol"] == st["nmol"]
+        np.testing.assert_array_equal(st2["energy"], st["energy"])
+        np.testing.assert_array_equal(b["energy"], st["energy"])
+        np.testing.assert_array_equal(b["counters"][:15], st["counters"][:15])
+        np.testing.assert_array_equal(g.adsorbates(), xyz)
+        np.testing.assert_array_equal(b["xyz"], xyz)
+    # a batched upload lands in each system's own slot
+    e.set_adsorbates([xyz[: max(len(xyz) - 1, 0)] for _, xyz in alone])
+    for g, (_, xyz) in zip(gs, alone):
+        np.testing.assert_array_equal(g.adsorbates(), xyz[: max(len(xyz) - 1, 0)])
+    with pytest.raises(native.NativeError):
+        e.set_split([0, 1, 2], 2)
+    with pytest.raises(native.NativeError):
+        e.set_split([1, 1], 2)
+    e.set_split([], 0)
+    e.run(10)
+    e.sync()
+    assert all(g.state()["status"] == 0 for g in gs)
