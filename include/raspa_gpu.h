@@ -222,7 +222,7 @@ int rgpu_system_set_coulomb_grid(rgpu_system *sys, const float *d_grid, const in
 
 /* ---- persistent batched engine ------------------------------------------ */
 /* Groups systems for one persistent launch; each system is advanced by one
- * thread-block cluster of `cluster` CTAs (1, 2, 4 or 8; 0 chooses from the
+ * thread-block cluster of `cluster` CTAs (1 to 8; 0 chooses from the
  * number of systems and SMs) that split its framework between them.
  * `threads` = CTA size, a multiple of 32 in 64..1024 (RGPU_MIXED) or
  * 64..512 (RGPU_FP64). */
@@ -238,7 +238,7 @@ int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *systems, int n,
 /* CTAs per system of an engine. */
 int rgpu_engine_cluster(rgpu_engine *eng);
 /* Runs the systems second[0..nsecond) (indices into the engine's systems)
- * in a second launch with clusters of `cluster_b` CTAs (1, 2, 4 or 8), side
+ * in a second launch with clusters of `cluster_b` CTAs (1 to 8), side
  * by side with the launch of the others on a stream of the engine's own;
  * rgpu_engine_run's stream waits for both. One cluster size per launch, so
  * this is how the costliest systems get more CTAs, on SMs a single launch

@@ -14,8 +14,9 @@ framework sizes and on the loadings. Measured on a B200 for 64 CO2 boxes of
 
 When the best shape leaves SMs idle (64 boxes at 2 CTAs each fill 128 of
 148), the costliest boxes, by the clock cycles they spent in the best run,
-can run in a second launch at twice the cluster size beside the first
-(`Engine.set_split`); the tuner times such splits too.
+can run in a second launch at a larger cluster size (one or two times
+more CTAs) beside the first (`Engine.set_split`); the tuner times such
+splits too.
 
 `tune()` times every admissible shape on copies of the caller's boxes (same
 force fields, configurations and random seeds), so the caller's state does
@@ -103,14 +104,14 @@ def tune(systems: Sequence["native.GpuSystem"], precision: int = native.RGPU_MIX
     table = []
     best = None
 
-    def time_shape(c, t, split=()):
+    def time_shape(c, t, split=(), cb=0):
         """moves/s of one shape and each box's clock cycles in the timed run"""
         for g, x in zip(clones, start):
             g.set_adsorbates(x)
         eng = native.Engine(clones, precision=precision, threads=t, cluster=c)
         try:
             if split:
-                eng.set_split(split, 2 * c)
+                eng.set_split(split, cb)
             eng.run(warm, stream.cuda_stream)
             torch.cuda.synchronize()
             c0 = [g.state()["counters"] for g in clones]
@@ -135,29 +136,32 @@ def tune(systems: Sequence["native.GpuSystem"], precision: int = native.RGPU_MIX
             continue
         table.append({"cluster": c, "threads": t, "moves_per_s": rate})
         if best is None or rate > best[2]:
-            best = (c, t, rate, ())
+            best = (c, t, rate, (), 0)
             cycles = cyc
     if best is not None and auto_split:
         c, t = best[0], best[1]
         spare = props.multi_processor_count - len(systems) * c
-        kmax = min(spare // c, len(systems) - 1) if 2 * c <= 8 else 0
         by_cost = list(np.argsort(cycles)[::-1])
-        for k in sorted({kmax, kmax // 2} - {0}, reverse=True):
-            split = tuple(int(i) for i in by_cost[:k])
-            try:
-                rate, _ = time_shape(c, t, split)
-            except native.NativeError as e:
-                table.append({"cluster": c, "threads": t, "split": k, "cluster_b": 2 * c, "error": str(e)})
+        for cb in sorted({c + 1, 2 * c}):
+            if cb > 8:
                 continue
-            table.append({"cluster": c, "threads": t, "split": k, "cluster_b": 2 * c, "moves_per_s": rate})
-            if rate > best[2]:
-                best = (c, t, rate, split)
+            kmax = min(spare // (cb - c), len(systems) - 1)
+            for k in sorted({kmax, kmax // 2} - {0}, reverse=True):
+                split = tuple(int(i) for i in by_cost[:k])
+                try:
+                    rate, _ = time_shape(c, t, split, cb)
+                except native.NativeError as e:
+                    table.append({"cluster": c, "threads": t, "split": k, "cluster_b": cb, "error": str(e)})
+                    continue
+                table.append({"cluster": c, "threads": t, "split": k, "cluster_b": cb, "moves_per_s": rate})
+                if rate > best[2]:
+                    best = (c, t, rate, split, cb)
     for g in clones:
         g.close()
     if best is None:
         raise native.NativeError("no launch shape could be created for this batch")
     shape = Shape(cluster=best[0], threads=best[1], moves_per_s=best[2], table=table, split=best[3],
-                  cluster_b=2 * best[0] if best[3] else 0)
+                  cluster_b=best[4])
     if use_cache:
         _CACHE[key] = shape
     return shape

@@ -1221,7 +1221,7 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   const int max_threads = precision == RGPU_MIXED ? 1024 : 512;
   if (threads < 64 || threads > max_threads || threads % 32)
     return fail(RGPU_E_INVALID, "threads %d outside [64,%d] or not a multiple of 32", threads, max_threads);
-  if (cluster < 0 || cluster > 8 || (cluster & (cluster - 1))) return fail(RGPU_E_INVALID, "cluster %d", cluster);
+  if (cluster < 0 || cluster > 8) return fail(RGPU_E_INVALID, "cluster %d", cluster);
   /* registers: 128 per thread (the narrow build) unless the CTAs of an SM
    * need more than 65536 together; then the mixed kernel's 64-register build */
   const bool wide = threads > 512 || (long long)threads * 128 * ctas_per_sm > 65536;
@@ -1318,7 +1318,7 @@ extern "C" int rgpu_engine_set_split(rgpu_engine *e, const int *second, int nsec
   if (!e || nsecond < 0 || (nsecond > 0 && !second)) return fail(RGPU_E_INVALID, "bad argument");
   const int n = (int)e->sys.size();
   if (nsecond >= n) return fail(RGPU_E_INVALID, "the first launch needs at least one system");
-  if (nsecond > 0 && (cluster_b < 1 || cluster_b > 8 || (cluster_b & (cluster_b - 1))))
+  if (nsecond > 0 && (cluster_b < 1 || cluster_b > 8))
     return fail(RGPU_E_INVALID, "cluster %d", cluster_b);
   std::vector<char> in_b(n, 0);
   for (int k = 0; k < nsecond; k++) {

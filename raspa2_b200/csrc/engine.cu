@@ -220,13 +220,12 @@ __device__ __forceinline__ void random_rotation(double x0, double y1, double y2,
   R[1][0] = 2.0 * u2 * u1 + ce * u3;
 }
 
-/* share [lo, hi) of n items for rank r of c (c a power of two <= 8; n far
- * below 2^28, so n * c fits in 32 bits) */
+/* share [lo, hi) of n items for rank r of c (1 <= c <= 8; n far below
+ * 2^28, so n * c fits in 32 bits) */
 __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 {
-  const int sh = __ffs(c) - 1;
-  lo = (n * r) >> sh;
-  hi = (n * (r + 1)) >> sh;
+  lo = n * r / c;
+  hi = n * (r + 1) / c;
 }
 
 /* Pair evaluation of P positions on this CTA's share, then one cluster

@@ -31,7 +31,8 @@ def oracle_run(sysm, mols, nsteps, seed=777, stream_id=3, maxmol=64):
 
 
 @pytest.mark.parametrize("name,cluster,occ", [("co2_tiny", 1, 1), ("co2_tiny", 2, 1), ("co2_config1", 8, 1),
-                                              ("methane_config0", 2, 1), ("co2_config1", 2, 2)])
+                                              ("co2_config1", 3, 1), ("methane_config0", 2, 1),
+                                              ("co2_config1", 2, 2)])
 def test_fp64_engine_reproduces_oracle_trajectory(cuda, name, cluster, occ):
     """Same counter-based stream, same decisions: the FP64 engine (framework
     split over `cluster` CTAs; with occ = 2 sized for two CTAs per SM, so
@@ -198,7 +199,7 @@ def test_graph_replay_matches_direct_launches(cuda):
 
 def test_split_launch_matches_single_runs(cuda):
     """rgpu_engine_set_split: the systems moved to a second launch at cluster
-    2 run bitwise as they do alone at cluster 2, the others as alone at
+    3 run bitwise as they do alone at cluster 3, the others as alone at
     cluster 1, also when the two launches are replayed from one CUDA graph;
     the batched state read (device slots reordered) returns each system's
     own state, and a batched upload reaches the right systems."""
@@ -209,7 +210,7 @@ def test_split_launch_matches_single_runs(cuda):
     alone = []
     for i, s in enumerate(specs):
         g, st = engine_run(s, np.zeros((0, s.molecule.n_atoms, 3)), n, native.RGPU_MIXED, seed=5, stream_id=i,
-                           cluster=2 if i in second else 1)
+                           cluster=3 if i in second else 1)
         alone.append((st, g.adsorbates()))
     gs = []
     for i, s in enumerate(specs):
@@ -217,7 +218,7 @@ def test_split_launch_matches_single_runs(cuda):
         g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
         gs.append(g)
     e = native.Engine(gs, precision=native.RGPU_MIXED, threads=256, cluster=1)
-    e.set_split(second, 2)
+    e.set_split(second, 3)
     e.use_graph(True)
     e.run(n)
     e.sync()
