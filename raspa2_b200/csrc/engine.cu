@@ -82,7 +82,7 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.skfw = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
   L.skads = o; o = rgpu_align(o + (size_t)k_items * sizeof(double2));
   L.ctl = o; o = rgpu_align(o + RGPU_CTL_BYTES);
-  L.ang = o; o = rgpu_align(o + (flex ? RGPU_ANG_DOUBLES * sizeof(double) : 0));
+  L.ang = o; o = rgpu_align(o + (flex ? 2 * RGPU_ANG_DOUBLES * sizeof(double) : 0));   /* growth, retrace */
   L.total = o;
   return L;
 }
@@ -112,6 +112,7 @@ struct Ctl {
   /* a retrace's beads: trial weight sum, the old bead's host VDW, adsorbate
    * VDW, intramolecular LJ and bonded energy, any valid trial */
   double rb[RGPU_MAX_ATOMS][6];
+  double co[RGPU_MAX_ATOMS][3];  /* the old beads of a reinsertion's retrace */
   double uintra, uintra_old;
   double dl[4];
   int nmol;
@@ -146,7 +147,8 @@ struct Eng {
   int kw;
   int k0, k1;                /* this CTA's wave vectors */
   double *red;               /* [2][2*RGPU_MAX_WARPS] */
-  double *ang;               /* [RGPU_ANG_DOUBLES] chain trial trigonometry (flexible-chain builds) */
+  double *ang;               /* [2][RGPU_ANG_DOUBLES] chain trial trigonometry of a growth and of a retrace
+                              * stage (flexible-chain builds) */
   Ctl *ctl;
   const double *rnd;         /* this step's uniforms */
   uint64_t step;             /* index of the current MC step */
@@ -1029,7 +1031,7 @@ __device__ __forceinline__ void chain_angles_group(const RgpuSys &S, int i, int 
  * stage into E.ang: 8 lanes per (bead, trial), four per warp. All threads
  * call; the caller's next barrier publishes the table. */
 template <bool MIXED, bool FLEX>
-__device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage)
+__device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage, double *tab)
 {
   const RgpuSys &S = *E.S;
   const int na = S.natom, nt = S.ntrial;
@@ -1042,11 +1044,135 @@ __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stag
     double th, ph;
     chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
     if (live && (lane & 7) == 0) {
-      double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+      double *a = tab + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
       a[0] = cos(th);
       a[1] = sin(th);
       a[2] = cos(ph);
       a[3] = sin(ph);
+    }
+  }
+}
+
+/* Retrace of a flexible chain's configuration (RetraceMolecule,
+ * src/cbmc.c:3056-3181, for a linear chain). The beads a retrace "chooses"
+ * are the old ones, known before anything is evaluated, so the trial sets of
+ * several beads are placed together and evaluated at once: beads are taken
+ * in growth order in groups whose trials fit one evaluation (RGPU_MAX_POS
+ * positions; for 6 beads of 16 trials and 8 first-bead trials, two
+ * evaluations instead of six). Each bead's weights are summed by one warp in
+ * trial order, and the Rosenbluth weight and the energies are combined bead
+ * by bead in growth order, stopping at the first bead without a valid
+ * trial, as the bead-by-bead retrace does. The trials draw the same random
+ * numbers as that retrace (counter-based, by stage, bead and trial). All
+ * threads call. */
+/* Beads of a retrace taken in one evaluation: from bead i0 on, as many as
+ * fit `room` positions (at least one; room >= RGPU_MAX_TRIALS). */
+__device__ __forceinline__ int retrace_group_end(int i0, int na, int nf, int nt, int room, int &P)
+{
+  int i1 = i0;
+  P = 0;
+  while (i1 < na && P + (i1 == 0 ? nf : nt) <= room) {
+    P += i1 == 0 ? nf : nt;
+    i1++;
+  }
+  return i1;
+}
+
+/* Places the trials of retrace beads [i0, i0 + ...) at positions off ..
+ * off + P, position j of the group being bead i, trial t in growth order;
+ * trial 0 of each bead is the old bead old[i]. Threads t0, t0 + step, ...
+ * of the block place. */
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void retrace_place(Eng<MIXED, FLEX> &E, int stage, int i0, int P, int off,
+                                              const double (*old)[3], const double *ang, int exclude, int t0,
+                                              int step)
+{
+  const RgpuSys &S = *E.S;
+  const int nf = S.ntrial_first, nt = S.ntrial;
+  for (int j = t0; j < P; j += step) {
+    int i = i0, t = j;
+    while (t >= (i == 0 ? nf : nt)) {
+      t -= i == 0 ? nf : nt;
+      i++;
+    }
+    double p[3];
+    if (t == 0) {
+      p[0] = old[i][0];
+      p[1] = old[i][1];
+      p[2] = old[i][2];
+    } else if (i == 0) {
+      for (int d = 0; d < 3; d++)
+        p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
+    } else if (i == 1) {
+      const uint64_t stp = E.step;
+      chain_trial(S, old, i, [&](int d) { return rgpu_uniform(S.seed, S.sys_id, stp, chain_slot(stage, i, t, d)); },
+                  p);
+    } else {
+      const double *a = ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+      chain_place_trig(i >= 3 ? old[i - 3] : nullptr, old[i - 2], old[i - 1], S.bond, a[0], a[1], a[2], a[3], p);
+    }
+    bead_set(E.pos[off + j], S, p[0], p[1], p[2], i, exclude);
+  }
+}
+
+/* Bookkeeping of retrace beads [i0, i1) evaluated at positions off.. of
+ * buffer b: warp w0 + g takes bead i0 + g (warps w0, w0 + 1, ... of the
+ * block), sums its weights in trial order and leaves in C.rb[i] the sum,
+ * the old bead's host and adsorbate VDW, intramolecular LJ and bonded
+ * energy, and whether any trial was valid. */
+template <bool MIXED, bool FLEX>
+__device__ __forceinline__ void retrace_book(const Eng<MIXED, FLEX> &E, int b, int i0, int i1, int off,
+                                             const double (*old)[3], int w0)
+{
+  const RgpuSys &S = *E.S;
+  Ctl &C = *E.ctl;
+  const int nf = S.ntrial_first, nt = S.ntrial;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (warp < w0) return;
+  for (int g = warp - w0; g < i1 - i0; g += nw - w0) {
+    const int i = i0 + g, k = i == 0 ? nf : nt;
+    const int o0 = off + (i0 == 0 ? (i == 0 ? 0 : nf + (i - 1) * nt) : g * nt);
+    double r[4] = {0.0, 0.0, 0.0, 0.0}, lj = 0.0, bf = 0.0;
+    int o = 0, ov = 0;
+    if (lane < k) {
+      gather(E, b, o0 + lane, r, o);
+      const double p[3] = {E.pos[o0 + lane].x, E.pos[o0 + lane].y, E.pos[o0 + lane].z};
+      lj = chain_intra_lj(S, old, i, p);
+      ov = r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap || lj >= S.overlap;
+      bf = -S.beta * (r[0] + r[2] + lj);
+    }
+    const bool valid = lane < k && !ov;
+    const double w = valid ? exp(bf) : 0.0;
+    const bool any = __ballot_sync(RGPU_FULL, valid) != 0u;
+    double wsum = 0.0;
+    for (int t = 0; t < k; t++) wsum += __shfl_sync(RGPU_FULL, w, t);
+    if (lane == 0) {
+      double *rb = C.rb[i];
+      rb[0] = wsum;
+      rb[1] = r[0];
+      rb[2] = r[2];
+      rb[3] = lj;
+      rb[4] = i >= 2 ? chain_bonded_energy(S, old, i, old[i]) : 0.0;
+      rb[5] = any ? 1.0 : 0.0;
+    }
+  }
+}
+
+/* Thread 0: the retrace beads [i0, i1) into the Rosenbluth weight and the
+ * energies, in growth order, stopping at the first bead without a valid
+ * trial. */
+__device__ __forceinline__ void retrace_combine(Ctl &C, int i0, int i1, int nf, int nt)
+{
+  for (int i = i0; i < i1 && !C.fail; i++) {
+    const double *rb = C.rb[i];
+    C.rosen *= rb[0] / (double)(i == 0 ? nf : nt);
+    C.u[0] += rb[1];
+    C.u[2] += rb[2];
+    C.uintra += rb[3];
+    if (i >= 2) C.uintra += rb[4];
+    if (rb[5] == 0.0) {
+      C.fail = 1;
+      C.cnt[RGPU_CNT_OVERLAP]++;
     }
   }
 }
@@ -1069,7 +1195,6 @@ __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, in
   RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
   const int na = S.natom, nf = S.ntrial_first, nt = S.ntrial;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (threadIdx.x == 0) {
     C.rosen = 1.0;
     C.u[0] = C.u[1] = C.u[2] = C.u[3] = 0.0;
@@ -1077,85 +1202,19 @@ __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, in
     C.fail = 0;
   }
   if (threadIdx.x < na) atom_xyz(E, m, threadIdx.x, C.cp[threadIdx.x]);
-  chain_angles_table(E, stage);
+  chain_angles_table(E, stage, E.ang);
   __syncthreads();
   for (int i0 = 0; i0 < na;) {
-    int i1 = i0, P = 0;
-    while (i1 < na && P + (i1 == 0 ? nf : nt) <= RGPU_MAX_POS) {
-      P += i1 == 0 ? nf : nt;
-      i1++;
-    }
-    for (int j = threadIdx.x; j < P; j += blockDim.x) {
-      int i = i0, t = j;
-      while (t >= (i == 0 ? nf : nt)) {
-        t -= i == 0 ? nf : nt;
-        i++;
-      }
-      double p[3];
-      if (t == 0) {
-        p[0] = C.cp[i][0];
-        p[1] = C.cp[i][1];
-        p[2] = C.cp[i][2];
-      } else if (i == 0) {
-        for (int d = 0; d < 3; d++)
-          p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
-      } else if (i == 1) {
-        const uint64_t step = E.step;
-        chain_trial(S, C.cp, i,
-                    [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); }, p);
-      } else {
-        const double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
-        chain_place_trig(i >= 3 ? C.cp[i - 3] : nullptr, C.cp[i - 2], C.cp[i - 1], S.bond, a[0], a[1], a[2], a[3], p);
-      }
-      bead_set(E.pos[j], S, p[0], p[1], p[2], i, exclude);
-    }
+    int P;
+    const int i1 = retrace_group_end(i0, na, nf, nt, RGPU_MAX_POS, P);
+    retrace_place(E, stage, i0, P, 0, C.cp, E.ang, exclude, threadIdx.x, blockDim.x);
     __syncthreads();
     engine_eval(E, P, 0);
     const int b = E.xb;
     E.xb ^= 1;
-    /* warp g: bead i0 + g, its trials at positions off .. off + k */
-    for (int g = warp; g < i1 - i0; g += nw) {
-      const int i = i0 + g, k = i == 0 ? nf : nt;
-      const int off = i0 == 0 ? (i == 0 ? 0 : nf + (i - 1) * nt) : g * nt;
-      double r[4] = {0.0, 0.0, 0.0, 0.0}, lj = 0.0, bf = 0.0;
-      int o = 0, ov = 0;
-      if (lane < k) {
-        gather(E, b, off + lane, r, o);
-        const double p[3] = {E.pos[off + lane].x, E.pos[off + lane].y, E.pos[off + lane].z};
-        lj = chain_intra_lj(S, C.cp, i, p);
-        ov = r[0] >= S.overlap || r[1] >= S.overlap || r[2] >= S.overlap || r[3] >= S.overlap || lj >= S.overlap;
-        bf = -S.beta * (r[0] + r[2] + lj);
-      }
-      const bool valid = lane < k && !ov;
-      const double w = valid ? exp(bf) : 0.0;
-      const bool any = __ballot_sync(RGPU_FULL, valid) != 0u;
-      double wsum = 0.0;
-      for (int t = 0; t < k; t++) wsum += __shfl_sync(RGPU_FULL, w, t);
-      if (lane == 0) {
-        double *rb = C.rb[i];
-        rb[0] = wsum;
-        rb[1] = r[0];
-        rb[2] = r[2];
-        rb[3] = lj;
-        rb[4] = i >= 2 ? chain_bonded_energy(S, C.cp, i, C.cp[i]) : 0.0;
-        rb[5] = any ? 1.0 : 0.0;
-      }
-    }
+    retrace_book(E, b, i0, i1, 0, C.cp, 0);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int i = i0; i < i1 && !C.fail; i++) {
-        const double *rb = C.rb[i];
-        C.rosen *= rb[0] / (double)(i == 0 ? nf : nt);
-        C.u[0] += rb[1];
-        C.u[2] += rb[2];
-        C.uintra += rb[3];
-        if (i >= 2) C.uintra += rb[4];
-        if (rb[5] == 0.0) {
-          C.fail = 1;
-          C.cnt[RGPU_CNT_OVERLAP]++;
-        }
-      }
-    }
+    if (threadIdx.x == 0) retrace_combine(C, i0, i1, nf, nt);
     __syncthreads();
     if (C.fail) return;
     i0 = i1;
@@ -1163,7 +1222,8 @@ __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, in
 }
 
 template <bool MIXED, bool FLEX>
-__device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, int stage, int m, int exclude)
+__device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, int stage, int m, int exclude,
+                                           bool ride = false)
 {
   if (retrace) {
     retrace_chain(E, stage, m, exclude);
@@ -1180,9 +1240,24 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
   }
   /* the bend angles and dihedrals of beads 2.. of every trial, ahead of the
    * first bead (the first barrier below publishes them) */
-  chain_angles_table(E, stage);
+  chain_angles_table(E, stage, E.ang);
+  /* ride: a reinsertion's retrace (stage 1) of molecule m rides along with
+   * the first beads' evaluations, one group of retrace beads each, in the
+   * positions after the growth's trials; its beads' sums are left in C.rb */
+  double *ang_r = E.ang + RGPU_ANG_DOUBLES;
+  if (ride) {
+    if (threadIdx.x < na) atom_xyz(E, m, threadIdx.x, C.co[threadIdx.x]);
+    chain_angles_table(E, 1, ang_r);
+  }
+  int r0 = ride ? 0 : na;   /* next retrace bead */
   for (int i = 0; i < na; i++) {
     const int k = i == 0 ? nf : nt;
+    int r1 = r0, rP = 0;
+    if (r0 < na) {
+      r1 = retrace_group_end(r0, na, nf, nt, RGPU_MAX_POS - k, rP);
+      if (i == 0) __syncthreads();   /* C.co and the retrace angles */
+      if (threadIdx.x >= 32) retrace_place(E, 1, r0, rP, k, C.co, ang_r, m, threadIdx.x - 32, blockDim.x - 32);
+    }
     if (threadIdx.x < k) {
       const int t = threadIdx.x;
       double p[3];
@@ -1202,9 +1277,15 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
       bead_set(E.pos[t], S, p[0], p[1], p[2], i, exclude);
     }
     __syncthreads();
-    engine_eval(E, k, 0);
+    engine_eval(E, k + rP, 0);
     const int b = E.xb;
     E.xb ^= 1;
+    if (r1 > r0) {
+      /* warps 1..: the retrace group's bookkeeping (warp 1 then goes on to
+       * this bead's bonded energies) */
+      retrace_book(E, b, r0, r1, k, C.co, 1);
+      r0 = r1;
+    }
     if (threadIdx.x < 32) {
       const int lane = threadIdx.x;
       double r[4] = {0.0, 0.0, 0.0, 0.0}, lj = 0.0, bf = 0.0;
@@ -1323,18 +1404,24 @@ __device__ __forceinline__ void step_reinsert_chain(Eng<MIXED, FLEX> &E)
   const int na = S.natom, nmol = C.nmol;
   int m = (int)(E.rnd[SLOT_MOLECULE] * nmol);
   if (m >= nmol) m = nmol - 1;
-  grow_chain(E, false, 0, m, m);
+  /* the retrace of the old configuration rides along with the growth's
+   * first evaluations (it does not depend on the new chain); its beads are
+   * combined after a successful growth, as a retrace run after it would */
+  grow_chain(E, false, 0, m, m, true);
   if (C.fail) return;
   if (threadIdx.x == 0) {
-    C.rosen_old = C.rosen;     /* the new configuration's weight, kept while the old one is retraced */
+    C.rosen_old = C.rosen;     /* the new configuration's weight */
     C.dl[0] = C.u[0];
     C.dl[2] = C.u[2];
     C.uintra_old = C.uintra;
     for (int a = 0; a < na; a++)
       for (int d = 0; d < 3; d++) C.cpn[a][d] = C.cp[a][d];
+    C.rosen = 1.0;
+    C.u[0] = C.u[1] = C.u[2] = C.u[3] = 0.0;
+    C.uintra = 0.0;
+    retrace_combine(C, 0, na, S.ntrial_first, S.ntrial);
   }
   __syncthreads();
-  grow_chain(E, true, 1, m, m);
   if (C.fail) return;
   if (threadIdx.x == 0) {
     const double w_new = C.rosen_old, w_old = C.rosen;
