@@ -5,7 +5,7 @@
  * (src/mc_moves.c, src/cbmc.c) calls them once per trial position or move.
  * This library exports the same operations over an explicit system handle,
  * with plain pointers and sizes, so that a patched copy of those routines can
- * forward to the GPU (see INTEGRATION.md), plus batched entry points that
+ * forward to the GPU, plus batched entry points that
  * evaluate a whole CBMC trial set per call and a persistent engine that runs
  * many independent systems entirely on the device.
  *

@@ -20,6 +20,7 @@ import sys
 import numpy as np
 import pytest
 
+from oracle import REFROOT
 from oracle import oracle as O
 from raspa2_b200 import output, raspa_io, restart, systems, units
 
@@ -27,7 +28,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 ROOT = os.path.dirname(HERE)
 SIMULATE = os.path.join(ROOT, "oracle", "_ref", "simulate")
-REF_PYTHON = "/root/reference/python"
+REF_PYTHON = os.path.join(REFROOT, "python")
 
 CASES = {
     "co2_config1": lambda: systems.co2_system(seed=1),
