@@ -190,10 +190,12 @@ int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double s
  * 256 KB (one per device) instead of buffers allocated per call. The first
  * call on each device looks up that array's address (cudaGetSymbolAddress)
  * with the device current and keeps it, so make the first call before any
- * stream capture. n above RGPU_NOALLOC_MAX_POINTS returns RGPU_E_INVALID.
+ * stream capture. The kept address belongs to the device's current context:
+ * it does not survive cudaDeviceReset, so do not call this after a reset in
+ * the same process. n above RGPU_NOALLOC_MAX_POINTS returns RGPU_E_INVALID.
  * Calls that overlap on one device (several host threads) share the array
- * and race: serialise them. Runs on the legacy default stream and returns
- * when the results are in `out`. */
+ * and race: serialise them. Runs on the legacy default stream, synchronises
+ * that stream and returns when the results are in `out`. */
 #define RGPU_NOALLOC_MAX_POINTS 8192
 int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const double size[3],
                                   const double shift[3], const double cell[3], int n, const double *xyz,

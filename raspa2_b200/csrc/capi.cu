@@ -1121,7 +1121,9 @@ extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], con
 /* Grid lookup without device allocation. The positions and results of one
  * call live in a file-scope device array (one per device, 256 KB); the
  * first call on a device looks up its address with cudaGetSymbolAddress
- * and keeps it. Calls that overlap on one device share the array and race. */
+ * and keeps it (an address of the device's current context: it does not
+ * survive cudaDeviceReset). Calls that overlap on one device share the array
+ * and race. */
 struct NoAllocInterp {
   double xyz[RGPU_NOALLOC_MAX_POINTS * 3];
   double out[RGPU_NOALLOC_MAX_POINTS];

@@ -60,3 +60,21 @@ def test_noalloc_rejects_more_points_than_scratch(grid):
     pts = _points(m, native.RGPU_NOALLOC_MAX_POINTS + 1, 14)
     with pytest.raises(native.NativeError, match="RGPU_NOALLOC_MAX_POINTS"):
         native.grid_interpolate_noalloc(buf.data_ptr(), m["n"], m["size"], m["shift"], m["cell"], pts)
+
+
+def test_noalloc_allocates_no_device_memory(grid):
+    """The property the entry point exists for: after the first call (which
+    may load the module's code), further calls leave the device's free
+    memory unchanged."""
+    import torch
+    m, g, buf = grid
+    args = (buf.data_ptr(), m["n"], m["size"], m["shift"], m["cell"])
+    pts = _points(m, native.RGPU_NOALLOC_MAX_POINTS, 15)
+    first = native.grid_interpolate_noalloc(*args, pts)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        np.testing.assert_array_equal(native.grid_interpolate_noalloc(*args, pts), first)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
