@@ -66,7 +66,10 @@ def parse_args():
     p.add_argument("--maxmol", type=int, default=768)
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--e2e-steps", type=int, default=3)
-    p.add_argument("--ref-cycles", type=int, default=10)
+    p.add_argument("--ref-cycles", type=int, default=2,
+                   help="reference production cycles per system and step (a cycle is max(20, N) moves)")
+    p.add_argument("--single-ref-cycles", type=int, default=20,
+                   help="reference production cycles of each single-system configuration")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--hexane-systems", type=int, default=64,
@@ -136,35 +139,81 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
+def equilibrated_configs(args, sys_list):
+    """The GPU arm's starting state, reproduced: every system from empty
+    through the GPU arm's warm-up (warmup + 1 steps of moves_per_step MC
+    moves, the same seeds and random streams; a system's trajectory does not
+    depend on the launch shape or the batch) on the engine. Returns the
+    configurations, or None when no GPU or library is there."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        from raspa2_b200 import native
+        native.load()
+    except Exception:
+        return None
+    gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240, stream_id=i) for i, s in enumerate(sys_list)]
+    for g, s in zip(gs, sys_list):
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+    prec = native.RGPU_MIXED if args.precision == "mixed" else native.RGPU_FP64
+    eng = native.Engine(gs, precision=prec, threads=512, cluster=0)
+    for _ in range(args.warmup + 1):
+        eng.run(args.moves_per_step)
+    eng.sync()
+    xs = [g.adsorbates() for g in gs]
+    eng.close()
+    return xs
+
+
 def run_reference_arm(args, sys_list):
     if not os.path.exists(REF_SIMULATE):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/simulate was not built "
                                                               "(needs the reference sources: make -C oracle ref)"}))
         return
     cores = min(cpu_cores(), len(sys_list))
+    xs = equilibrated_configs(args, sys_list)
+    start = "the GPU arm's equilibrated configuration of each system (restart file)" if xs is not None else \
+        "empty framework (no GPU to equilibrate on)"
+    if xs is None:
+        xs = [np.zeros((0, s.molecule.n_atoms, 3)) for s in sys_list]
     tmp = tempfile.mkdtemp(prefix="raspa_ref_")
+    n = len(sys_list)
     try:
+        def sample(k, cycles, tag):
+            idx = [(k * cores + j) % n for j in range(cores)]
+            return idx, reference_from([(sys_list[i], xs[i]) for i in idx], cycles, 1000 + 97 * k,
+                                       os.path.join(tmp, f"{tag}{k}"), cores)
         for w in range(args.warmup):
-            reference_sample(sys_list, 1, 100 + w, os.path.join(tmp, f"w{w}"), cores)
-        total_moves, total_cpu, total_wall = 0.0, 0.0, 0.0
+            sample(w, 1, "w")
+        total_moves, total_cpu, total_wall, loads, seen = 0.0, 0.0, 0.0, {}, []
         for k in range(args.steps):
-            mv, cpu, wall, _ = reference_sample(sys_list, args.ref_cycles, 1000 + 97 * k, os.path.join(tmp, f"k{k}"),
-                                                cores)
-            total_moves += mv
-            total_cpu += cpu
-            total_wall += wall
+            t0 = time.perf_counter()
+            idx, res = sample(k, args.ref_cycles, "k")
+            total_wall += time.perf_counter() - t0
+            for i, (mv, cpu, wall, ld) in zip(idx, res):
+                total_moves += mv
+                total_cpu += cpu
+                loads[i] = ld
+                seen.append(i)
         per_core = total_moves / total_cpu
         value = per_core * cores
+        sampled = sorted(loads)
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": "MC moves/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * total_wall / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"co2_gcmc_batched_{len(sys_list)}", "systems": len(sys_list),
-                       "cycles_per_step": args.ref_cycles},
+            "config": {"workload": f"co2_gcmc_batched_{n}", "systems_per_gpu": n,
+                       "moves_per_step_per_system": f"{args.ref_cycles} cycles of max(20, N) moves",
+                       "precision": "fp64", "start": start,
+                       "mean_loading": float(np.mean([loads[i] for i in sampled])),
+                       "start_mean_loading": float(np.mean([len(xs[i]) for i in sampled])),
+                       "systems_sampled": len(sampled)},
             "cpu_baseline": {"value": value, "unit": "MC moves/s", "cores": cores, "kind": "reference",
-                             "sample": f"{len(sys_list)} systems x {args.ref_cycles} cycles per step, "
-                                       f"one process per system, {cores} at a time",
+                             "sample": f"per step {cores} of the {n} systems (in turn), {args.ref_cycles} "
+                                       "production cycles each from the equilibrated configuration, one "
+                                       "process per system; moves / production MC-move CPU time x cores",
                              "single_core": per_core, "wall_clock_aggregate": total_moves / total_wall},
             "e2e": {"value": value, "unit": "MC moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
@@ -230,6 +279,84 @@ class ClockSampler:
 
 def make_systems(n, rank):
     return systems.batched_co2_systems(n, seed=ranks.batch_seed(2, rank))
+
+
+def energy_error(gs, sys_list):
+    """The engine's running energies (accumulated move by move) of every
+    system against an FP64 recomputation of its configuration from scratch
+    (rgpu_total_energy; rgpu_intra_energy for chains): the largest plain
+    relative error of the total potential energy and of each term larger
+    than k_B T, and the largest absolute differences in k_B T."""
+    rel_tot, abs_tot, rel_term, abs_term, per_mol, n = 0.0, 0.0, 0.0, 0.0, 0.0, 0
+    for g, s in zip(gs, sys_list):
+        st = g.state()
+        if st["nmol"] == 0:
+            continue
+        n += 1
+        run = np.array(st["energy"][:6])
+        ref = np.array(g.total_energy())
+        if not s.molecule.rigid:
+            run = np.append(run, st["energy"][6])
+            ref = np.append(ref, g.intra_energy())
+        kT = units.K_B * s.temperature
+        d = abs(run.sum() - ref.sum())
+        rel_tot = max(rel_tot, d / abs(ref.sum()))
+        abs_tot = max(abs_tot, d / kT)
+        per_mol = max(per_mol, d / kT / st["nmol"])
+        for a, b in zip(run, ref):
+            if abs(b) > kT:
+                rel_term = max(rel_term, abs(a - b) / abs(b))
+                abs_term = max(abs_term, abs(a - b) / kT)
+    return {"systems": n, "max_rel_total": rel_tot, "max_abs_total_kT": abs_tot,
+            "max_abs_total_kT_per_molecule": per_mol, "max_rel_term": rel_term, "max_abs_term_kT": abs_term,
+            "reference": "FP64 recomputation from scratch of each system's final configuration"}
+
+
+def roofline_of(d, seconds, peak):
+    """FP32 roofline of an engine run from its counter deltas d (summed over
+    systems) and its device time."""
+    n_charged = float(d[12])
+    n_lj = float(d[11]) - n_charged
+    flop = FLOP_PAIR_LJ * n_lj + FLOP_PAIR_LJ_EWALD * n_charged + FLOP_KSITE * float(d[13]) + FLOP_KVEC * float(d[14])
+    achieved = flop / seconds / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak}
+
+
+def write_restart_inputs(s, d, xyz, cycles, seed):
+    """Input files of system s in directory d for a production run of the
+    reference that starts from the configuration xyz ([n][natom][3]) through
+    its restart file (RestartFile yes)."""
+    from raspa2_b200 import restart
+    raspa_io.write_inputs(s, d, cycles=cycles, init_cycles=0, print_every=10 ** 9, seed=seed, restart=True)
+    restart.write_restart(restart.restart_path(s, d), s, np.asarray(xyz, float).reshape(-1, s.molecule.n_atoms, 3))
+    return d
+
+
+def reference_from(sys_xyz, cycles, seed0, workdir, cores):
+    """The reference `simulate` on each (system, configuration), one process
+    per system, `cores` at a time, each for `cycles` production cycles from
+    its configuration; returns per run (moves, MC-move CPU s, wall s, mean
+    loading in molecules per box)."""
+    dirs = []
+    for i, (s, x) in enumerate(sys_xyz):
+        dirs.append((s, write_restart_inputs(s, os.path.join(workdir, f"s{i}"), x, cycles, seed0 + i)))
+
+    def run(sd):
+        s, d = sd
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_SIMULATE, "-i", "simulation.input"], cwd=d, capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"reference simulate failed in {d}: {r.stderr[-500:]}")
+        out = os.path.join(d, "Output", "System_0")
+        f = os.path.join(out, os.listdir(out)[0])
+        mv, cpu = parse_reference_output(f)
+        m = re.search(r"Average loading absolute \[molecules/unit cell\]\s+([-\d.eE+]+)", open(f).read())
+        per_cell = float(m.group(1)) if m else float("nan")
+        return mv, cpu, wall, per_cell * float(np.prod(s.unit_cells))
+
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        return list(ex.map(run, dirs))
 
 
 def run_ours(args):
@@ -367,25 +494,39 @@ def run_ours(args):
     }
     if e2e:
         line["e2e"] = e2e
+    line["precision"] = {"co2_batched": energy_error(gs, sys_list)}
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_gpu"] = plain_gpu_rate(native, stream)
+        # the two single-system configurations, each on its own
+        line["config0_methane"] = single_config_run(native, stream, peak, systems.methane_system(seed=0), 256,
+                                                    60000, 20000, args.single_ref_cycles)
+        line["config1_co2"] = single_config_run(native, stream, peak, systems.co2_system(seed=1), 384, 200000,
+                                                20000, args.single_ref_cycles)
+        line["precision"]["config0_methane"] = line["config0_methane"]["mixed"]["energy_error"]
+        line["precision"]["config1_co2"] = line["config1_co2"]["mixed"]["energy_error"]
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         line["serving"] = serving_run(args)
     if rank == 0 and world == 1 and args.hexane_systems > 0:
         line["hexane_grid"] = hexane_grid_run(args, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_SIMULATE):
+        # the reference on the GPU arm's final configurations: the first
+        # `cores` systems, one process each, 2 production cycles
         cores = min(cpu_cores(), len(sys_list))
         tmp = tempfile.mkdtemp(prefix="raspa_ref_")
         try:
-            mv, cpu, wall, _ = reference_sample(sys_list, args.ref_cycles, 4242, tmp, cores)
+            res = reference_from([(sys_list[i], gs[i].adsorbates()) for i in range(cores)], args.ref_cycles, 4242,
+                                 tmp, cores)
         finally:
             shutil.rmtree(tmp, ignore_errors=True)
-        per_core = mv / cpu
+        per_core = sum(r[0] for r in res) / sum(r[1] for r in res)
         line["cpu_baseline"] = {"value": per_core * cores, "unit": "MC moves/s", "cores": cores,
                                 "kind": "reference",
-                                "sample": f"{len(sys_list)} systems x {args.ref_cycles} cycles from empty, "
-                                          "reference simulate (oracle/_ref), one process per system",
-                                "single_core": per_core}
+                                "sample": f"{cores} of the {len(sys_list)} systems x {args.ref_cycles} production "
+                                          "cycles from this run's final configurations, reference simulate "
+                                          "(oracle/_ref), one process per system",
+                                "single_core": per_core,
+                                "mean_loading": float(np.mean([r[3] for r in res])),
+                                "gpu_mean_loading_same_systems": float(np.mean(loads[:cores]))}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -493,6 +634,58 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
                           enumerate(["translation", "rotation", "insertion", "deletion"])},
            "reinsertion_acceptance": float(d[19]) / max(float(d[18]), 1.0), "phases": phases}
     del flush
+    return out
+
+
+def single_config_run(native, stream, peak, sysm, maxmol, equil, timed, ref_cycles):
+    """One system of a single-system configuration (the plain path): the
+    system is equilibrated once by the FP64 engine; from that configuration
+    the FP64 and the mixed-precision engine each run `timed` MC moves at
+    their own autotuned launch shape (device-timed), with the FP32 roofline
+    of the run and the error of the running energies against an FP64
+    recomputation; and the reference program runs `ref_cycles` production
+    cycles from the same configuration on one host core."""
+    import torch
+    from raspa2_b200 import autotune
+    natom = sysm.molecule.n_atoms
+    g = native.GpuSystem(sysm, maxmol=maxmol, seed=5, stream_id=0)
+    g.set_adsorbates(np.zeros((0, natom, 3)))
+    e = native.Engine([g], precision=native.RGPU_FP64, threads=256, cluster=4)
+    e.run(equil, stream.cuda_stream)
+    e.sync()
+    e.close()
+    x_eq = g.adsorbates()
+    out = {"system": sysm.name, "framework_atoms": int(sysm.n_framework()), "loading": int(len(x_eq)),
+           "equilibration_moves": equil, "timed_moves": timed}
+    for prec, key in ((native.RGPU_FP64, "fp64"), (native.RGPU_MIXED, "mixed")):
+        g = native.GpuSystem(sysm, maxmol=maxmol, seed=6, stream_id=0)
+        g.set_adsorbates(x_eq)
+        tuned = autotune.tune([g], precision=prec, moves=200, warm=50, split=False)
+        g.set_adsorbates(x_eq)
+        g.set_energy(list(g.total_energy()) + [g.intra_energy() if not sysm.molecule.rigid else 0.0, 0.0])
+        e = native.Engine([g], precision=prec, threads=tuned.threads, cluster=tuned.cluster)
+        c0 = g.state()["counters"].copy()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.run(timed, stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t = ev0.elapsed_time(ev1) / 1e3
+        d = g.state()["counters"] - c0
+        e.close()
+        out[key] = {"moves_per_s": float(d[8]) / t, "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads},
+                    "roofline": roofline_of(d, t, peak), "energy_error": energy_error([g], [sysm])}
+    out["mixed_vs_fp64"] = out["mixed"]["moves_per_s"] / out["fp64"]["moves_per_s"]
+    if os.path.exists(REF_SIMULATE):
+        tmp = tempfile.mkdtemp(prefix="raspa_ref1_")
+        try:
+            mv, cpu, wall, ld = reference_from([(sysm, x_eq)], ref_cycles, 31, tmp, 1)[0]
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        out["reference_single_core"] = {"moves_per_s": mv / cpu, "moves": mv, "cycles": ref_cycles, "wall_s": wall,
+                                        "mean_loading": ld,
+                                        "start": "the same equilibrated configuration (restart file)"}
+        out["mixed_vs_reference_single_core"] = out["mixed"]["moves_per_s"] / out["reference_single_core"]["moves_per_s"]
     return out
 
 

@@ -88,6 +88,19 @@ typedef struct {
   double bond;
   double bend_k, bend_theta0;
   double torsion[4];
+  /* Bonded part of a chain's CBMC trials. chain_scheme 0 (the reference's
+   * GenerateTrialOrientationsMCScheme, src/cbmc.c:1580-2480): one bend angle
+   * per growth step, drawn from sin(theta) exp(-beta U_bend) and shared by
+   * the step's trials (a retrace keeps the old angle); per trial `ntors`
+   * uniform rotations about the previous bond, one chosen by its torsion
+   * Boltzmann factor; the weight carries the chosen trial's torsion
+   * Rosenbluth factor, averaged, as the reference averages it, over the
+   * first ntrial candidates (src/cbmc.c:548, :2401, :2793). ntors = 0 means
+   * the reference's default NumberOfTrialPositionsTorsion, 100 (at most
+   * 248). chain_scheme 1: each trial draws its own bend angle and dihedral
+   * from their Boltzmann distributions (no torsion factor in the weight). */
+  int chain_scheme;
+  int ntors;
 } rgpu_system_desc;
 
 const char *rgpu_error_string(int code);

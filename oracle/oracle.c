@@ -749,17 +749,25 @@ void or_cbmc_retrace(const or_sys *s, int m, int nf, int nt, or_rng_fn rng, void
 /* ---------------------------------------------------------------------- */
 /* Flexible linear chains. CBMC growth bead by bead from atom 0
  * (GrowMolecule / RetraceMolecule, src/cbmc.c:2928-3181, for a linear
- * chain; bonded terms sampled as in GenerateTrialOrientationsMCScheme,
- * src/cbmc.c:1580-2480): bead i >= 1 at the fixed bond length from bead i-1,
- * its bend angle drawn from sin(theta) exp(-beta U_bend) (Gaussian proposal
- * accepted with probability sin(theta)), its dihedral from exp(-beta
- * U_torsion) (uniform proposal accepted with exp(-beta (U - min U))). The
- * draws are keyed (stage, bead, trial, draw) in the counter-based stream;
- * the GPU engine uses the same keys. Bend HARMONIC_BEND and torsion
- * TRAPPE_DIHEDRAL as src/internal_energy.c:205, :2324. */
+ * chain): bead i >= 1 at the fixed bond length from bead i-1; the bonded
+ * part of the trials as the reference draws it (chain_scheme 0, see
+ * ref_scheme_angles) or, with chain_scheme 1, each trial's bend angle drawn
+ * from sin(theta) exp(-beta U_bend) (Gaussian proposal accepted with
+ * probability sin(theta)) and its dihedral from exp(-beta U_torsion)
+ * (uniform proposal accepted with exp(-beta (U - min U))). The draws are
+ * keyed (stage, bead, trial, draw) in the counter-based stream; the GPU
+ * engine uses the same keys. Bend HARMONIC_BEND and torsion TRAPPE_DIHEDRAL
+ * as src/internal_energy.c:205, :2324. */
 #define CHAIN_SLOT_SEL (1u << 15)
 #define CHAIN_SLOT (1u << 16)
 #define CHAIN_TRIES 64
+/* chain_scheme 0: the shared bend angle's draws sit in the slots of trial
+ * REF_THETA_TRIAL from REF_THETA_SLOT on; the torsion choice of trial t in
+ * slot REF_TORS_SEL_SLOT; candidate dihedral k of trial t in slot k */
+#define MAX_TORS 248
+#define REF_TORS_SEL_SLOT 255
+#define REF_THETA_TRIAL 15
+#define REF_THETA_SLOT 256
 
 static uint32_t chain_slot(int stage, int bead, int trial, int k)
 {
@@ -911,6 +919,78 @@ static double chain_trial(const or_sys *s, const double (*x)[3], int i, const ph
   return bonded_energy(s, x, i, p);
 }
 
+/* The reference's bonded trials (chain_scheme 0), GenerateTrialOrientationsMCScheme
+ * src/cbmc.c:1580-2480 for a linear chain, bead i >= 2 grown from bead i-1:
+ * - one bend angle for all trials of the step (the internal Metropolis
+ *   chain of src/cbmc.c:1822-2106 samples sin(theta) exp(-beta U_bend);
+ *   here the same distribution is drawn directly); a retrace keeps the old
+ *   bead's angle (src/cbmc.c:1661, the chain runs only when growing);
+ * - per trial, `ntors` rotations about the bond (i-2)-(i-1) by uniform
+ *   angles (src/cbmc.c:2361-2399), i.e. uniform dihedrals, one of them
+ *   chosen by its torsion Boltzmann factor (SelectTrialPosition,
+ *   src/cbmc.c:2403-2410); a retrace's trial 0 keeps the old dihedral as
+ *   its first candidate (src/cbmc.c:2376-2377). Without a torsion (i = 2)
+ *   the choice is uniform (src/cbmc.c:2410);
+ * - the trial's torsion Rosenbluth factor (src/cbmc.c:2401). The reference
+ *   computes it with ComputeNormalizedRosenbluthWeight, whose loop runs over
+ *   the global NumberOfTrialPositions, not over its argument (src/cbmc.c:548):
+ *   it is the mean over the first `nt` candidates only, nt = the CBMC trials
+ *   per bead. This is kept, because it sets the reference's GCMC loadings.
+ * Fills theta_sh, and per trial t the dihedral phi[t] (unused for the old
+ * trial 0 of a retrace) and the torsion factor wt[t]. */
+static void ref_scheme_angles(const or_sys *s, const double (*x)[3], int i, int retrace, const double *old, int nt,
+                              const philox_ctx *c, int stage, double *theta_sh, double *phi, double *wt)
+{
+  if (retrace) {
+    *theta_sh = angle3(x[i - 2], x[i - 1], old);
+  } else {
+    double th = s->bend_theta0;
+    for (int a = 0; a < CHAIN_TRIES; a++) {
+      int k = REF_THETA_SLOT + 3 * a;
+      double u1 = chain_u(c, stage, i, REF_THETA_TRIAL, k), u2 = chain_u(c, stage, i, REF_THETA_TRIAL, k + 1);
+      double u3 = chain_u(c, stage, i, REF_THETA_TRIAL, k + 2);
+      double t = s->bend_theta0 + s->bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
+      if (t > 0.0 && t < M_PI && u3 < sin(t)) {
+        th = t;
+        break;
+      }
+    }
+    *theta_sh = th;
+  }
+  for (int t = 0; t < nt; t++) {
+    wt[t] = 1.0;
+    if (i == 2) {
+      phi[t] = 2.0 * M_PI * chain_u(c, stage, i, t, 0) - M_PI;
+      continue;
+    }
+    double bf[MAX_TORS], f[MAX_TORS];
+    for (int k = 0; k < s->ntors; k++) {
+      double cs;
+      if (retrace && t == 0 && k == 0) {
+        cs = cos_dihedral(x[i - 3], x[i - 2], x[i - 1], old);
+        f[k] = 0.0;
+      } else {
+        f[k] = 2.0 * M_PI * chain_u(c, stage, i, t, k) - M_PI;
+        cs = cos(f[k]);
+      }
+      bf[k] = -s->beta * torsion_energy(s, cs);
+    }
+    double sum = 0.0;
+    for (int k = 0; k < nt && k < s->ntors; k++) sum += exp(bf[k]);
+    wt[t] = sum / (double)nt;
+    int sel = 0;
+    if (!(retrace && t == 0)) {
+      double largest = -DBL_MAX, tot = 0.0;
+      for (int k = 0; k < s->ntors; k++)
+        if (bf[k] > largest) largest = bf[k];
+      for (int k = 0; k < s->ntors; k++) tot += exp(bf[k] - largest);
+      double ws = chain_u(c, stage, i, t, REF_TORS_SEL_SLOT) * tot, cum = exp(bf[0] - largest);
+      while (cum < ws && sel < s->ntors - 1) cum += exp(bf[++sel] - largest);
+    }
+    phi[t] = f[sel];
+  }
+}
+
 /* CBMC growth (retrace = 0) or retrace of a chain; exclude = molecule left
  * out of the adsorbate sums, m = molecule retraced. out = {fail, W, host VDW,
  * adsorbate VDW, intramolecular}; x receives the chosen beads. */
@@ -923,14 +1003,23 @@ static void chain_grow(const or_sys *s, int retrace, int stage, int m, int exclu
   for (int i = 0; i < na; i++) {
     const int k = i == 0 ? nf : nt;
     double w[MAX_TRIALS], pe[MAX_TRIALS][4], lj[MAX_TRIALS], ub[MAX_TRIALS], pos[MAX_TRIALS][3];
+    double wt[MAX_TRIALS], phi[MAX_TRIALS], theta_sh = 0.0;
+    const int ref = s->chain_scheme == 0 && i >= 2;
+    if (ref)
+      ref_scheme_angles(s, (const double(*)[3])x, i, retrace, s->ads_xyz + 3 * (m * na + i), k, c, stage, &theta_sh,
+                        phi, wt);
     int any = 0;
     for (int t = 0; t < k; t++) {
       ub[t] = 0.0;
+      if (!ref) wt[t] = 1.0;
       if (retrace && t == 0) {
         for (int d = 0; d < 3; d++) pos[0][d] = s->ads_xyz[3 * (m * na + i) + d];
         ub[0] = bonded_energy(s, (const double(*)[3])x, i, pos[0]);
       } else if (i == 0) {
         for (int d = 0; d < 3; d++) pos[t][d] = s->box[d] * chain_u(c, stage, 0, t, d);
+      } else if (ref) {
+        place(i >= 3 ? x[i - 3] : NULL, x[i - 2], x[i - 1], s->bond, theta_sh, phi[t], pos[t]);
+        ub[t] = bonded_energy(s, (const double(*)[3])x, i, pos[t]);
       } else {
         ub[t] = chain_trial(s, (const double(*)[3])x, i, c, stage, t, pos[t]);
       }
@@ -949,7 +1038,7 @@ static void chain_grow(const or_sys *s, int retrace, int stage, int m, int exclu
       double cum = w[0];
       while (cum < target && sel < k - 1) cum += w[++sel];
     }
-    rosen *= wsum / (double)k;
+    rosen *= wsum / (double)k * wt[sel];
     if (!any || (!retrace && rosen < 1e-150)) return;
     hv += pe[sel][0];
     av += pe[sel][2];

@@ -65,6 +65,15 @@ typedef struct {
   const float *coul_grid;
   int coul_npts[3];
   double coul_size[3], coul_shift[3], coul_cell[3];
+  /* bonded trial scheme of a flexible chain: 0 = the reference's
+   * GenerateTrialOrientationsMCScheme (src/cbmc.c:1580-2480): one bend angle
+   * per growth step shared by all trials, and per trial `ntors` random
+   * rotations about the previous bond from which one is chosen by its
+   * torsion Boltzmann factor, the chosen trial's torsion Rosenbluth factor
+   * multiplying the weight (src/cbmc.c:2787-2793); 1 = bend angle and
+   * dihedral drawn per trial from their Boltzmann distributions */
+  int chain_scheme;
+  int ntors;
 } or_sys;
 
 /* pair terms */

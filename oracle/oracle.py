@@ -35,6 +35,7 @@ class OrSys(C.Structure):
         ("grid_shift", C.c_double * 3), ("grid_cell", C.c_double * 3),
         ("coul_grid", C.POINTER(C.c_float)), ("coul_npts", C.c_int * 3), ("coul_size", C.c_double * 3),
         ("coul_shift", C.c_double * 3), ("coul_cell", C.c_double * 3),
+        ("chain_scheme", C.c_int), ("ntors", C.c_int),
     ]
 
 
@@ -164,6 +165,8 @@ class Oracle:
             e = (s.torsion[0] + s.torsion[1] * (1 + c) + s.torsion[2] * (1 - (2 * c * c - 1))
                  + s.torsion[3] * (1 + c * (4 * c * c - 3)))
             s.torsion_min = e.min() - 1e-6 * (e.max() - e.min()) - 1e-12
+            s.chain_scheme = sysm.chain_scheme
+            s.ntors = sysm.torsion_trials
         return o
 
     def intra_energy(self):

@@ -291,6 +291,9 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     if (d->natom > 1 && !(d->bend_k > 0.0)) return fail(RGPU_E_INVALID, "flexible chain: bend_k must be positive");
     for (int a = 0; a < d->natom; a++)
       if (d->mol_q[a] != 0.0) return fail(RGPU_E_INVALID, "flexible chains must be uncharged");
+    if (d->chain_scheme != 0 && d->chain_scheme != 1) return fail(RGPU_E_INVALID, "chain_scheme must be 0 or 1");
+    if (d->ntors < 0 || d->ntors > RGPU_MAX_TORS)
+      return fail(RGPU_E_INVALID, "ntors must be in [0,%d] (0: 100)", RGPU_MAX_TORS);
   }
   if (d->maxmol < 1 || (long long)d->maxmol * d->natom > (1 << 20)) return fail(RGPU_E_INVALID, "maxmol");
   if (d->ntrial_first < 1 || d->ntrial_first > RGPU_MAX_TRIALS || d->ntrial < 1 || d->ntrial > RGPU_MAX_TRIALS)
@@ -541,6 +544,9 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       tmax = std::max(tmax, e);
     }
     h.torsion_min = tmin - 1e-6 * (tmax - tmin) - 1e-12;
+    h.chain_scheme = d->chain_scheme;
+    /* NumberOfTrialPositionsTorsion defaults to 100 (src/input.c:349) */
+    h.ntors = d->ntors > 0 ? d->ntors : 100;
   }
   /* the exclusion sum K qa qb erf(alpha r)/r over the molecule's charged
    * pairs (src/ewald.c:7312-7330) is a constant of a rigid molecule */

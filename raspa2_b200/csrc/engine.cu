@@ -55,9 +55,10 @@ static_assert(sizeof(PosSum) % 16 == 0, "PosSum must keep 16-byte alignment in a
 __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
 /* bend and dihedral trigonometry of every trial of a chain growth stage
- * (flexible-chain builds only): {cos theta, sin theta, cos phi, sin phi} for
- * beads 2.. natom-1 and each trial */
-#define RGPU_ANG_DOUBLES (4 * (RGPU_MAX_ATOMS - 2) * RGPU_MAX_TRIALS)
+ * (flexible-chain builds only): {cos theta, sin theta, cos phi, sin phi,
+ * torsion Rosenbluth factor} for beads 2.. natom-1 and each trial */
+#define RGPU_ANG_STRIDE 5
+#define RGPU_ANG_DOUBLES (RGPU_ANG_STRIDE * (RGPU_MAX_ATOMS - 2) * RGPU_MAX_TRIALS)
 
 __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw,
                                                       int k_items, int nwarps, int flex)
@@ -1027,16 +1028,138 @@ __device__ __forceinline__ void chain_angles_group(const RgpuSys &S, int i, int 
  * host and adsorbate VDW (u[0], u[2]) and the intramolecular energy
  * (uintra: bonded + LJ), or fail. Molecule m is the one retraced; `exclude`
  * leaves a molecule out of the adsorbate sums. All threads call. */
+/* The reference's bonded trials (chain_scheme 0; GenerateTrialOrientationsMCScheme,
+ * src/cbmc.c:1580-2480, for a linear chain) of trial t of bead i >= 2, by
+ * one warp (every lane calls), into a[0..4] (lane 0 writes):
+ * - the bend angle, one per bead and stage: a growth draws it from
+ *   sin(theta) exp(-beta U_bend) (proposals in the slots of trial
+ *   RGPU_REF_THETA_TRIAL from RGPU_REF_THETA_SLOT on, tried in order: the
+ *   lanes try 32 at once and the lowest accepted wins), which is the
+ *   distribution the reference's internal Metropolis chain
+ *   (src/cbmc.c:1822-2106) samples; a retrace (old != nullptr) keeps the
+ *   old bead's angle;
+ * - the dihedral: ntors uniform candidates (slot k of the trial), one chosen
+ *   by its torsion Boltzmann factor with SelectTrialPosition's rule
+ *   (src/cbmc.c:563-599, 2403-2408; one uniform in slot
+ *   RGPU_REF_TORS_SEL_SLOT); candidate k is lane k % 32 of row k / 32,
+ *   and the cumulative sum runs row by row as warp scans. A retrace's
+ *   trial 0 keeps the old dihedral as its candidate 0 and chooses it.
+ *   Without a torsion (bead 2) the dihedral is uniform (src/cbmc.c:2410);
+ * - the torsion Rosenbluth factor: the mean of exp(-beta U_torsion) over
+ *   candidates 0 .. ntrial-1, the reference's ComputeNormalizedRosenbluthWeight
+ *   (src/cbmc.c:542-552 sums up to the global NumberOfTrialPositions; called
+ *   at :2401); 1 for bead 2. */
+__device__ __forceinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage, int t, uint64_t step, int lane,
+                                                const double (*old)[3], double *a)
+{
+  auto U = [&](int tr, int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, tr, d)); };
+  double theta = S.bend_theta0;
+  if (old) {
+    theta = chain_angle(old[i - 2], old[i - 1], old[i]);
+  } else {
+    for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
+      const int k = RGPU_REF_THETA_SLOT + 3 * (base + lane);
+      const double u1 = U(RGPU_REF_THETA_TRIAL, k), u2 = U(RGPU_REF_THETA_TRIAL, k + 1);
+      const double u3 = U(RGPU_REF_THETA_TRIAL, k + 2);
+      const double th = S.bend_theta0 + S.bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
+      const unsigned ok = __ballot_sync(RGPU_FULL, th > 0.0 && th < M_PI && u3 < sin(th));
+      if (ok) {
+        theta = __shfl_sync(RGPU_FULL, th, __ffs(ok) - 1);
+        break;
+      }
+    }
+  }
+  const bool keep_old = old && t == 0;
+  double phi = 0.0, wt = 1.0;
+  if (i == 2) {
+    if (!keep_old) phi = 2.0 * M_PI * U(t, 0) - M_PI;
+  } else {
+    /* candidate k = lane + 32 j sits in row j of the warp */
+    const int n = S.ntors, nt = S.ntrial, rows = (n + 31) >> 5;
+    double bf[RGPU_TORS_PER_LANE];
+    double big = -1e300, wsum = 0.0;
+#pragma unroll
+    for (int j = 0; j < RGPU_TORS_PER_LANE; j++) {
+      const int k = lane + 32 * j;
+      bf[j] = -1e300;
+      if (j < rows && k < n) {
+        const double cs = (keep_old && k == 0) ? chain_cos_dihedral(old[i - 3], old[i - 2], old[i - 1], old[i])
+                                               : cos(2.0 * M_PI * U(t, k) - M_PI);
+        bf[j] = -S.beta * chain_torsion_energy(S, cs);
+        big = fmax(big, bf[j]);
+        if (k < nt) wsum += exp(bf[j]);
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      big = fmax(big, __shfl_xor_sync(RGPU_FULL, big, o));
+      wsum += __shfl_xor_sync(RGPU_FULL, wsum, o);
+    }
+    wt = wsum / (double)nt;
+    if (!keep_old) {
+      double tot = 0.0;
+#pragma unroll
+      for (int j = 0; j < RGPU_TORS_PER_LANE; j++)
+        if (j < rows && lane + 32 * j < n) tot += exp(bf[j] - big);
+      for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(RGPU_FULL, tot, o);
+      const double target = U(t, RGPU_REF_TORS_SEL_SLOT) * tot;
+      /* the first candidate whose cumulative sum reaches the target, row
+       * by row; none (rounding only): the last, where the serial search
+       * stops */
+      int kc = n - 1;
+      double before = 0.0;
+      bool done = false;
+#pragma unroll
+      for (int j = 0; j < RGPU_TORS_PER_LANE; j++) {
+        if (!done && j < rows) {
+          const bool in = lane + 32 * j < n;
+          const double e = in ? exp(bf[j] - big) : 0.0;
+          double incl = e;
+          for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(RGPU_FULL, incl, o);
+            if (lane >= o) incl += y;
+          }
+          const unsigned hit = __ballot_sync(RGPU_FULL, in && before + incl >= target);
+          if (hit) {
+            kc = 32 * j + __ffs(hit) - 1;
+            done = true;
+          }
+          before += __shfl_sync(RGPU_FULL, incl, 31);
+        }
+      }
+      if (lane == 0) phi = 2.0 * M_PI * U(t, kc) - M_PI;
+    }
+  }
+  if (lane == 0) {
+    a[0] = cos(theta);
+    a[1] = sin(theta);
+    a[2] = cos(phi);
+    a[3] = sin(phi);
+    a[4] = wt;
+  }
+}
+
 /* The bend angles and dihedrals of beads 2.. of every trial of a growth
- * stage into E.ang: 8 lanes per (bead, trial), four per warp. All threads
- * call; the caller's next barrier publishes the table. */
+ * stage into `tab`, with each trial's torsion Rosenbluth factor. The
+ * reference's scheme (S.chain_scheme 0): one warp per (bead, trial); a
+ * retrace passes the old configuration `old` (published by a barrier
+ * before the call). Independent draws (S.chain_scheme 1): 8 lanes per
+ * (bead, trial), four per warp, and factor 1. All threads call; the
+ * caller's next barrier publishes the table. */
 template <bool MIXED, bool FLEX>
-__device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage, double *tab)
+__device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage, double *tab,
+                                                   const double (*old)[3])
 {
   const RgpuSys &S = *E.S;
   const int na = S.natom, nt = S.ntrial;
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int ntask = na > 2 ? (na - 2) * nt : 0;
+  if (S.chain_scheme == 0) {
+    for (int task = threadIdx.x >> 5; task < ntask; task += nw) {
+      const int i = 2 + task / nt, t = task % nt;
+      chain_ref_trial(S, i, stage, t, E.step, lane, old, tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t));
+    }
+    return;
+  }
   for (int t0 = (threadIdx.x >> 5) * 4; t0 < ntask; t0 += nw * 4) {
     const int task = t0 + (lane >> 3);
     const bool live = task < ntask;
@@ -1044,11 +1167,12 @@ __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stag
     double th, ph;
     chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
     if (live && (lane & 7) == 0) {
-      double *a = tab + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+      double *a = tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t);
       a[0] = cos(th);
       a[1] = sin(th);
       a[2] = cos(ph);
       a[3] = sin(ph);
+      a[4] = 1.0;
     }
   }
 }
@@ -1108,7 +1232,7 @@ __device__ __forceinline__ void retrace_place(Eng<MIXED, FLEX> &E, int stage, in
       chain_trial(S, old, i, [&](int d) { return rgpu_uniform(S.seed, S.sys_id, stp, chain_slot(stage, i, t, d)); },
                   p);
     } else {
-      const double *a = ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+      const double *a = ang + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t);
       chain_place_trig(i >= 3 ? old[i - 3] : nullptr, old[i - 2], old[i - 1], S.bond, a[0], a[1], a[2], a[3], p);
     }
     bead_set(E.pos[off + j], S, p[0], p[1], p[2], i, exclude);
@@ -1122,7 +1246,7 @@ __device__ __forceinline__ void retrace_place(Eng<MIXED, FLEX> &E, int stage, in
  * energy, and whether any trial was valid. */
 template <bool MIXED, bool FLEX>
 __device__ __forceinline__ void retrace_book(const Eng<MIXED, FLEX> &E, int b, int i0, int i1, int off,
-                                             const double (*old)[3], int w0)
+                                             const double (*old)[3], const double *ang, int w0)
 {
   const RgpuSys &S = *E.S;
   Ctl &C = *E.ctl;
@@ -1148,7 +1272,8 @@ __device__ __forceinline__ void retrace_book(const Eng<MIXED, FLEX> &E, int b, i
     for (int t = 0; t < k; t++) wsum += __shfl_sync(RGPU_FULL, w, t);
     if (lane == 0) {
       double *rb = C.rb[i];
-      rb[0] = wsum;
+      /* with the old trial's torsion Rosenbluth factor (1 for independent draws) */
+      rb[0] = i >= 2 ? wsum * ang[RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS) + 4] : wsum;
       rb[1] = r[0];
       rb[2] = r[2];
       rb[3] = lj;
@@ -1202,7 +1327,8 @@ __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, in
     C.fail = 0;
   }
   if (threadIdx.x < na) atom_xyz(E, m, threadIdx.x, C.cp[threadIdx.x]);
-  chain_angles_table(E, stage, E.ang);
+  if (S.chain_scheme == 0) __syncthreads();   /* the old configuration, read by the table */
+  chain_angles_table(E, stage, E.ang, (const double(*)[3])C.cp);
   __syncthreads();
   for (int i0 = 0; i0 < na;) {
     int P;
@@ -1212,7 +1338,7 @@ __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, in
     engine_eval(E, P, 0);
     const int b = E.xb;
     E.xb ^= 1;
-    retrace_book(E, b, i0, i1, 0, C.cp, 0);
+    retrace_book(E, b, i0, i1, 0, C.cp, E.ang, 0);
     __syncthreads();
     if (threadIdx.x == 0) retrace_combine(C, i0, i1, nf, nt);
     __syncthreads();
@@ -1240,14 +1366,15 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
   }
   /* the bend angles and dihedrals of beads 2.. of every trial, ahead of the
    * first bead (the first barrier below publishes them) */
-  chain_angles_table(E, stage, E.ang);
+  chain_angles_table(E, stage, E.ang, nullptr);
   /* ride: a reinsertion's retrace (stage 1) of molecule m rides along with
    * the first beads' evaluations, one group of retrace beads each, in the
    * positions after the growth's trials; its beads' sums are left in C.rb */
   double *ang_r = E.ang + RGPU_ANG_DOUBLES;
   if (ride) {
     if (threadIdx.x < na) atom_xyz(E, m, threadIdx.x, C.co[threadIdx.x]);
-    chain_angles_table(E, 1, ang_r);
+    if (S.chain_scheme == 0) __syncthreads();   /* the old configuration, read by the table */
+    chain_angles_table(E, 1, ang_r, (const double(*)[3])C.co);
   }
   int r0 = ride ? 0 : na;   /* next retrace bead */
   for (int i = 0; i < na; i++) {
@@ -1271,7 +1398,7 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
         chain_trial(S, C.cp, i,
                     [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, d)); }, p);
       } else {
-        const double *a = E.ang + 4 * ((i - 2) * RGPU_MAX_TRIALS + t);
+        const double *a = E.ang + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t);
         chain_place_trig(i >= 3 ? C.cp[i - 3] : nullptr, C.cp[i - 2], C.cp[i - 1], S.bond, a[0], a[1], a[2], a[3], p);
       }
       bead_set(E.pos[t], S, p[0], p[1], p[2], i, exclude);
@@ -1283,7 +1410,7 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
     if (r1 > r0) {
       /* warps 1..: the retrace group's bookkeeping (warp 1 then goes on to
        * this bead's bonded energies) */
-      retrace_book(E, b, r0, r1, k, C.co, 1);
+      retrace_book(E, b, r0, r1, k, C.co, ang_r, 1);
       r0 = r1;
     }
     if (threadIdx.x < 32) {
@@ -1315,7 +1442,9 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
       const double hv = __shfl_sync(RGPU_FULL, r[0], sel), av = __shfl_sync(RGPU_FULL, r[2], sel);
       const double ljs = __shfl_sync(RGPU_FULL, lj, sel);
       if (lane == 0) {
-        C.rosen *= wsum / (double)k;
+        /* with the chosen trial's torsion Rosenbluth factor (src/cbmc.c:2793;
+         * 1 for independent draws) */
+        C.rosen *= wsum / (double)k * (i >= 2 ? E.ang[RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + sel) + 4] : 1.0);
         if (!any || (!retrace && C.rosen < 1e-150)) C.fail = 1;
         C.u[0] += hv;
         C.u[2] += av;

@@ -3,17 +3,20 @@
  * bend angle and dihedral, and the draw of a CBMC trial direction.
  *
  * CBMC growth of a chain (the configurational-bias scheme of GrowMolecule,
- * src/cbmc.c:3056-3181, with the bonded part handled as in
- * GenerateTrialOrientationsMCScheme, src/cbmc.c:1580-2480): bead i >= 1 is
- * placed at the fixed bond length from bead i-1, its bend angle theta drawn
- * from p(theta) ~ sin(theta) exp(-beta U_bend(theta)) and its dihedral phi
- * from p(phi) ~ exp(-beta U_torsion(phi)). The trials therefore carry the
- * bonded Boltzmann factor, and the Rosenbluth weights hold only the external
- * energy and the intramolecular LJ. The draws here are our own (a Gaussian
- * proposal for theta accepted with probability sin(theta); a uniform
- * proposal for phi accepted with exp(-beta (U_torsion - min U_torsion))),
- * each keyed by (stage, bead, trial, draw) in the system's counter-based
- * stream, so the oracle reproduces every trial.
+ * src/cbmc.c:3056-3181): bead i >= 1 is placed at the fixed bond length from
+ * bead i-1. The bonded part of its trials follows
+ * GenerateTrialOrientationsMCScheme (src/cbmc.c:1580-2480) in the engine's
+ * chain_ref_trial (chain_scheme 0: a shared bend angle, torsion candidates
+ * and the torsion Rosenbluth factor). chain_trial below is the other
+ * scheme (chain_scheme 1): each trial's bend angle theta drawn from
+ * p(theta) ~ sin(theta) exp(-beta U_bend(theta)) and its dihedral phi from
+ * p(phi) ~ exp(-beta U_torsion(phi)), so the trials carry the bonded
+ * Boltzmann factor and the Rosenbluth weights hold only the external energy
+ * and the intramolecular LJ. The draws are our own (a Gaussian proposal for
+ * theta accepted with probability sin(theta); a uniform proposal for phi
+ * accepted with exp(-beta (U_torsion - min U_torsion))), each keyed by
+ * (stage, bead, trial, draw) in the system's counter-based stream, so the
+ * oracle reproduces every trial.
  *
  * Shared by host and device code; positions are FP64 Cartesian, the chain
  * unwrapped (no periodic image between bonded beads).
@@ -34,6 +37,15 @@
 #define RGPU_SLOT_CHAIN_SEL (1u << 15)   /* + stage * 8 + bead: selection among the trials */
 #define RGPU_SLOT_CHAIN (1u << 16)       /* + draws of one trial, see chain_slot */
 #define RGPU_CHAIN_TRIES 64              /* proposals per angle before the fallback */
+/* the reference's bonded trials (chain_scheme 0): candidate dihedral k of
+ * trial t in slot k of the trial (k < RGPU_MAX_TORS), its choice in slot
+ * RGPU_REF_TORS_SEL_SLOT, and the draws of the bend angle shared by a
+ * growth step in the slots of trial RGPU_REF_THETA_TRIAL from
+ * RGPU_REF_THETA_SLOT on (3 per proposal, RGPU_CHAIN_TRIES proposals) */
+#define RGPU_REF_TORS_SEL_SLOT 255
+#define RGPU_REF_THETA_TRIAL 15
+#define RGPU_REF_THETA_SLOT 256
+#define RGPU_TORS_PER_LANE ((RGPU_MAX_TORS + 31) / 32)
 
 /* slot of draw k (< 512) of trial t of bead i in growth stage `stage`
  * (0: growth of a new configuration, 1: retrace of an old one) */

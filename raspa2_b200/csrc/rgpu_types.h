@@ -23,6 +23,7 @@
 #define RGPU_MAX_FWTYPES 4     /* framework pseudo-atom types */
 #define RGPU_MAX_TRIALS 16     /* CBMC trial positions per step */
 #define RGPU_MAX_POS 64        /* bead positions evaluated in one batch */
+#define RGPU_MAX_TORS 248      /* torsion candidates per chain trial (chain_scheme 0); slots 0..247 */
 #define RGPU_TILE 16           /* framework atoms per tile (mixed-precision layout) */
 
 /* per-system counters */
@@ -155,6 +156,8 @@ typedef struct RgpuSys {
   int pad_flex;
   double bond, bend_k, bend_theta0, bend_sigma;   /* bend_sigma = 1 / sqrt(beta bend_k) */
   double torsion[4], torsion_min;                 /* torsion_min: minimum of the torsion energy over phi */
+  int chain_scheme;           /* rgpu_system_desc.chain_scheme: 0 the reference's bonded trials, 1 independent draws */
+  int ntors;                  /* torsion candidates per trial (chain_scheme 0) */
   /* energy grids (rgpu_system_set_grids): the engine takes the host VDW
    * energy of molecule atom a from grid[a] instead of the pair sums */
   int use_grid;

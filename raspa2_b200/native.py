@@ -53,7 +53,7 @@ class SystemDesc(C.Structure):
         ("ntrial_first", C.c_int), ("ntrial", C.c_int),
         ("seed", C.c_uint64), ("stream_id", C.c_uint32),
         ("flexible", C.c_int), ("bond", C.c_double), ("bend_k", C.c_double), ("bend_theta0", C.c_double),
-        ("torsion", C.c_double * 4),
+        ("torsion", C.c_double * 4), ("chain_scheme", C.c_int), ("ntors", C.c_int),
     ]
 
 
@@ -166,6 +166,8 @@ class GpuSystem:
             d.bend_k = mol.bend_k * units.KELVIN_TO_ENERGY
             d.bend_theta0 = np.deg2rad(mol.bend_theta0)
             d.torsion[:] = [t * units.KELVIN_TO_ENERGY for t in mol.torsion]
+            d.chain_scheme = sysm.chain_scheme
+            d.ntors = sysm.torsion_trials
         self.natom = d.natom
         self.maxmol = maxmol
         h = C.c_void_p()

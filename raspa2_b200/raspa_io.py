@@ -152,8 +152,16 @@ def simulation_input(sys: System, cycles: int = 0, init_cycles: int = 0,
     if sys.ewald:
         kx, ky, kz = sys.kmax
         lines.append(f"EwaldParameters               {sys.alpha} {kx} {ky} {kz}")
+    # The reference's swap, Widom and reinsertion moves grow with their own
+    # trial counts (src/mc_moves.c:6965, :4454; defaults 10, src/input.c:352-364),
+    # not with NumberOfTrialPositions: all are set to the system's counts.
     lines.append(f"NumberOfTrialPositions        {sys.trials}")
     lines.append(f"NumberOfTrialPositionsForTheFirstBead {sys.trials_first_bead}")
+    for move in ("Swap", "Widom", "Reinsertion"):
+        lines.append(f"NumberOfTrialPositions{move} {sys.trials}")
+        lines.append(f"NumberOfTrialPositionsForTheFirstBead{move} {sys.trials_first_bead}")
+    if not sys.molecule.rigid:
+        lines.append(f"NumberOfTrialPositionsTorsion {sys.torsion_trials}")
     if seed is not None:
         lines.append(f"RandomSeed                    {seed}")
     if grid:

@@ -142,6 +142,12 @@ class System:
     # reference's IdealGasRosenbluthWeight); insertion and deletion
     # acceptance use W / ideal_gas_rosenbluth. 1 for rigid molecules.
     ideal_gas_rosenbluth: float = 1.0
+    # bonded part of a flexible chain's CBMC trials: 0 = the reference's
+    # scheme (src/cbmc.c:1580-2480: a shared bend angle per growth step,
+    # `torsion_trials` torsion candidates per trial, the torsion Rosenbluth
+    # factor in the weight), 1 = bend angle and dihedral drawn per trial
+    chain_scheme: int = 0
+    torsion_trials: int = 100          # NumberOfTrialPositionsTorsion
 
     # ----- derived quantities --------------------------------------------
     @property
@@ -352,12 +358,33 @@ def methane_like_system(seed: int = 0, n_atoms: int = 288, temperature: float = 
         seed=seed)
 
 
+def torsion_rosenbluth(molecule: Molecule, temperature: float) -> float:
+    """<exp(-U_torsion / k_B T)> over a uniform dihedral: the mean torsion
+    Rosenbluth factor of one growth step of the reference's chain scheme."""
+    phi = np.linspace(-np.pi, np.pi, 100001)[:-1]
+    c = np.cos(phi)
+    t = molecule.torsion
+    u = t[0] + t[1] * (1 + c) + t[2] * (1 - np.cos(2 * phi)) + t[3] * (1 + np.cos(3 * phi))
+    return float(np.mean(np.exp(-u / temperature)))
+
+
+def chain_ideal_gas_estimate(molecule: Molecule, temperature: float) -> float:
+    """Ideal-gas Rosenbluth weight of a linear chain under the reference's
+    bonded scheme, without the intramolecular LJ (which raises n-hexane's by
+    about 10 %): one torsion factor per bead from the fourth on. Runs whose
+    averages depend on it measure it instead, by Widom insertions into an
+    empty box (empty_box_system)."""
+    return torsion_rosenbluth(molecule, temperature) ** max(molecule.n_atoms - 3, 0)
+
+
 def hexane_system(seed: int = 4, n_atoms: int = 4096, cell: float = 40.0, temperature: float = 433.0,
                   pressure: float = 1e5, name: Optional[str] = None) -> System:
     """United-atom n-hexane (flexible chain, TraPPE bends and torsions, 1.54 A
     bonds) in a neutral Si/O framework of `n_atoms` atoms in a cubic cell,
-    grown by CBMC with 8 first-bead trials and 16 trials per further bead;
-    translation, rotation, reinsertion and swap moves."""
+    grown by CBMC with 8 first-bead trials and 16 trials per further bead, the
+    bonded part as the reference draws it (100 torsion candidates per trial);
+    translation, rotation, reinsertion and swap moves. The ideal-gas
+    Rosenbluth weight is chain_ideal_gas_estimate's."""
     rng = np.random.default_rng(seed)
     c = np.array([cell, cell, cell], float)
     pore = pore_radius(c, VOID_FRACTION, rng)
@@ -370,7 +397,7 @@ def hexane_system(seed: int = 4, n_atoms: int = 4096, cell: float = 40.0, temper
         uc_charges=np.zeros(n_atoms), molecule=HEXANE, temperature=temperature, pressure=pressure,
         cutoff=12.0, ewald=False, trials=16, trials_first_bead=8,
         moves=MoveMix(translation=1.0, rotation=1.0, swap_insert=1.0, swap_delete=1.0, reinsertion=1.0),
-        seed=seed)
+        seed=seed, ideal_gas_rosenbluth=chain_ideal_gas_estimate(HEXANE, temperature))
 
 
 def empty_box_system(molecule: Molecule, temperature: float, cell: float = 30.0, trials: int = 16,

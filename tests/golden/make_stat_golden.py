@@ -51,7 +51,12 @@ CASES = {
     # weight, measured first by Widom insertions into an empty box
     "hexane_small_3e4": (lambda: systems.hexane_system(seed=4, n_atoms=1200, cell=26.0),
                          dict(pressure=3e4, temperature=433.0), 2000, 6000),
+    "hexane_small_3e3": (lambda: systems.hexane_system(seed=4, n_atoms=1200, cell=26.0),
+                         dict(pressure=3e3, temperature=433.0), 2000, 6000),
 }
+# cases that take the ideal-gas Rosenbluth weight recorded in another case's
+# fixture (same molecule and temperature) instead of measuring it again
+REUSE_IDEAL = {"hexane_small_3e3": "hexane_small_3e4"}
 WIDOM_CYCLES = 20000
 SEEDS = 8
 IDEAL = {}
@@ -126,7 +131,12 @@ def run_case(name, workdir):
     build, state, init, prod = CASES[name]
     s = dataclasses.replace(build(), **state)
     if not s.molecule.rigid:
-        w, w_err = reference_ideal_gas_rosenbluth(s.molecule, s.temperature, workdir)
+        src = os.path.join(OUT, f"stat_{REUSE_IDEAL.get(name, '')}.json")
+        if name in REUSE_IDEAL and os.path.exists(src):
+            doc = json.load(open(src))
+            w, w_err = doc["ideal_gas_rosenbluth_reference"], doc["ideal_gas_rosenbluth_reference_err"]
+        else:
+            w, w_err = reference_ideal_gas_rosenbluth(s.molecule, s.temperature, workdir)
         s = dataclasses.replace(s, ideal_gas_rosenbluth=w)
         IDEAL[name] = (w, w_err)
     dirs = []

@@ -1,8 +1,12 @@
 """Flexible chains (united-atom n-hexane): the FP64 engine follows the
 oracle's GCMC trajectory move for move (CBMC growth bead by bead with
-sampled bends and torsions, translation, rotation, reinsertion, swaps), and
-the mixed engine's running energies, the intramolecular part included, agree
-with a full recomputation."""
+sampled bends and torsions, translation, rotation, reinsertion, swaps), with
+the reference's bonded-trial scheme (chain_scheme 0) and with independent
+draws (chain_scheme 1), for CTA sizes of 64 and 256 threads and clusters of
+1 to 8 CTAs; and the mixed engine's running energies, the intramolecular
+part included, agree with a full recomputation."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -16,13 +20,16 @@ def small_hexane(pressure=1e6):
     return systems.hexane_system(seed=4, n_atoms=1200, cell=26.0, pressure=pressure)
 
 
-@pytest.mark.parametrize("cluster", [1, 2])
-def test_fp64_engine_follows_oracle_with_chains(cuda, cluster):
+@pytest.mark.parametrize("threads,cluster,scheme", [(256, 1, 0), (256, 2, 0), (64, 1, 0), (64, 3, 0), (256, 8, 0),
+                                                     (256, 2, 1), (64, 3, 1)])
+def test_fp64_engine_follows_oracle_with_chains(cuda, threads, cluster, scheme):
     s = small_hexane()
+    # independent draws carry no torsion factor: their ideal-gas weight is ~1.1
+    s = dataclasses.replace(s, chain_scheme=scheme, ideal_gas_rosenbluth=s.ideal_gas_rosenbluth if scheme == 0 else 1.1)
     n = 1500
     g = native.GpuSystem(s, maxmol=64, seed=777, stream_id=3)
     g.set_adsorbates(np.zeros((0, 6, 3)))
-    e = native.Engine([g], precision=native.RGPU_FP64, threads=256, cluster=cluster)
+    e = native.Engine([g], precision=native.RGPU_FP64, threads=threads, cluster=cluster)
     e.run(n)
     e.sync()
     st = g.state()
