@@ -157,7 +157,7 @@ def equilibrated_configs(args, sys_list):
     for g, s in zip(gs, sys_list):
         g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
     prec = native.RGPU_MIXED if args.precision == "mixed" else native.RGPU_FP64
-    eng = native.Engine(gs, precision=prec, threads=512, cluster=0)
+    eng = native.Engine(gs, precision=prec, threads=512, cluster=0)   # one GPU: stream ids = batch order
     for _ in range(args.warmup + 1):
         eng.run(args.moves_per_step)
     eng.sync()
@@ -281,6 +281,20 @@ def make_systems(n, rank):
     return systems.batched_co2_systems(n, seed=ranks.batch_seed(2, rank))
 
 
+def placed_systems(args, world, rank):
+    """This rank's systems: the job set of `world` GPUs is the union of
+    `world` seeded batches of `nsys` systems, placed on the GPUs by
+    device-memory footprint (ranks.place, the same on every rank), at most
+    nsys per GPU. Returns (systems, their indices in the job set); with one
+    GPU, the one batch in order."""
+    from raspa2_b200 import serve
+    allsys = [s for r in range(world) for s in make_systems(args.nsys, r)]
+    fp = [serve.system_footprint_bytes(s, args.maxmol) for s in allsys]
+    work = [float(s.n_framework() + (len(systems.kvector_indices(s.kmax)) if s.ewald else 0)) for s in allsys]
+    mine = ranks.place(fp, work, world, max_items=args.nsys)[rank]
+    return [allsys[i] for i in mine], mine
+
+
 def energy_error(gs, sys_list):
     """The engine's running energies (accumulated move by move) of every
     system against an FP64 recomputation of its configuration from scratch
@@ -372,8 +386,8 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     prec = native.RGPU_MIXED if args.precision == "mixed" else native.RGPU_FP64
 
-    sys_list = make_systems(args.nsys, rank)
-    gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240 + rank, stream_id=i) for i, s in enumerate(sys_list)]
+    sys_list, sys_ids = placed_systems(args, world, rank)
+    gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240, stream_id=i) for i, s in zip(sys_ids, sys_list)]
     for g, s in zip(gs, sys_list):
         g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
     eng = native.Engine(gs, precision=prec, threads=args.threads or 512, cluster=args.cluster)
@@ -475,6 +489,8 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == native.RGPU_MIXED else "f64",
         "data": "synthetic (seeded frameworks, random-init adsorbate state)",
         "config": {"workload": f"co2_gcmc_batched_{args.nsys}", "systems_per_gpu": args.nsys,
+                   "placement": "job set of n_gpus seeded batches, placed by device-memory footprint "
+                                "(ranks.place), no collective on the data path",
                    "moves_per_step_per_system": args.moves_per_step, "launch_shape": shape,
                    "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
                    "framework_atoms": [int(s.n_framework()) for s in sys_list[:8]] + ["..."],

@@ -37,7 +37,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-from . import native, output, systems, units
+from . import native, output, ranks, systems, units
 
 # a reference cycle is max(MinimumInnerCycles = 20, N) MC steps
 # (src/monte_carlo.c:367, src/input.c:346)
@@ -74,19 +74,54 @@ class Job:
 
 
 def footprint_bytes(job: Job) -> int:
-    """Device memory of one job as rgpu_system_create allocates it, plus the
-    engine's per-system descriptor."""
-    s = job.system
+    """Device memory of one job (system_footprint_bytes)."""
+    return system_footprint_bytes(job.system, job.maxmol)
+
+
+def system_footprint_bytes(s: systems.System, maxmol: int) -> int:
+    """Device memory of one system as rgpu_system_create allocates it, plus
+    the engine's per-system descriptor."""
     nfw = s.n_framework()
     ntile = (nfw + 31) // 32 + 8
     nk = len(systems.kvector_indices(s.kmax)) if s.ewald else 1
-    nads = job.maxmol * s.molecule.n_atoms
+    nads = maxmol * s.molecule.n_atoms
     io_n = max(64, nfw, nads)
     b = nfw * 32 + ntile * (32 * 16 + 32)          # fw64, fw32, tiles
     b += nk * (4 + 8 + 16 * 3)                     # kvec, kfactor, S_fw, S_ads, dS
     b += nads * (24 + 16 + 32)                     # positions, records
     b += io_n * 32 + 64 * (32 + 12) + 4096         # per-call scratch, descriptor, state
     return int(b)
+
+
+def work_estimate(job: Job) -> float:
+    """Relative device work of a job: MC steps times the pairs a step
+    visits (framework atoms plus, with charges, the wave vectors)."""
+    s = job.system
+    nk = len(systems.kvector_indices(s.kmax)) if s.ewald else 0
+    return float(job.steps) * (s.n_framework() + nk) * s.molecule.n_atoms
+
+
+def serve_placed(jobs: Sequence[Job], rank: int, world: int, make_server=None, mem_budget: float = 150e9,
+                 realtime: bool = True):
+    """Serves one job list over `world` GPUs, one server per rank: the jobs
+    are placed by device-memory footprint (ranks.place, the same placement
+    on every rank, no communication), rank `rank` serves its share with its
+    own server, and the per-job results are gathered on rank 0. Returns
+    (this rank's job indices, this rank's server statistics, on rank 0 the
+    results of all jobs by job id, else None). A job's result does not
+    depend on where it runs: each job has its own random stream."""
+    parts = ranks.place([footprint_bytes(j) for j in jobs], [work_estimate(j) for j in jobs], world,
+                        budget=mem_budget)
+    mine = [jobs[i] for i in parts[rank]]
+    srv = make_server() if make_server else Server(mem_budget=mem_budget)
+    stats = srv.run(mine, realtime=realtime) if mine else {"jobs": 0}
+    gathered = ranks.gather_results({j.id: j.result for j in mine})
+    allres = None
+    if gathered is not None:
+        allres = {}
+        for d in gathered:
+            allres.update(d)
+    return parts[rank], stats, allres
 
 
 class Server:

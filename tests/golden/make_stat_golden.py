@@ -54,9 +54,10 @@ CASES = {
     "hexane_small_3e3": (lambda: systems.hexane_system(seed=4, n_atoms=1200, cell=26.0),
                          dict(pressure=3e3, temperature=433.0), 2000, 6000),
 }
-# cases that take the ideal-gas Rosenbluth weight recorded in another case's
-# fixture (same molecule and temperature) instead of measuring it again
-REUSE_IDEAL = {"hexane_small_3e3": "hexane_small_3e4"}
+# cases that take the ideal-gas Rosenbluth weight from the Henry fixture of
+# the same molecule and temperature (the mean of its empty-box Widom runs)
+# instead of measuring it again; run the Henry case first
+REUSE_IDEAL = {"hexane_small_3e4": "hexane_small_henry", "hexane_small_3e3": "hexane_small_henry"}
 WIDOM_CYCLES = 20000
 SEEDS = 8
 IDEAL = {}
@@ -134,7 +135,7 @@ def run_case(name, workdir):
         src = os.path.join(OUT, f"stat_{REUSE_IDEAL.get(name, '')}.json")
         if name in REUSE_IDEAL and os.path.exists(src):
             doc = json.load(open(src))
-            w, w_err = doc["ideal_gas_rosenbluth_reference"], doc["ideal_gas_rosenbluth_reference_err"]
+            w, w_err = doc["ideal_gas_rosenbluth_mean"], doc["ideal_gas_rosenbluth_se"]
         else:
             w, w_err = reference_ideal_gas_rosenbluth(s.molecule, s.temperature, workdir)
         s = dataclasses.replace(s, ideal_gas_rosenbluth=w)
