@@ -407,11 +407,9 @@ def run_ours(args):
     if not (args.threads and args.cluster):
         from raspa2_b200 import autotune
         tuned = autotune.tune(gs, precision=prec)
-        shape = {"cluster": tuned.cluster, "threads": tuned.threads, "tuned": True,
-                 "split": {"systems": len(tuned.split), "cluster": tuned.cluster_b}, "table": tuned.table}
+        shape = dict(tuned.describe(), tuned=True, table=tuned.table)
         eng.close()
-        eng = native.Engine(gs, precision=prec, threads=tuned.threads, cluster=tuned.cluster)
-        tuned.apply(eng)
+        eng = tuned.engine(gs, prec)
         eng.run(args.moves_per_step, stream.cuda_stream)
         torch.cuda.synchronize()
     c0 = counters()
@@ -594,8 +592,7 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
     e.sync()
     tuned = autotune.tune(gs, precision=native.RGPU_MIXED)
     e.close()
-    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=tuned.threads, cluster=tuned.cluster)
-    tuned.apply(e)
+    e = tuned.engine(gs, native.RGPU_MIXED)
     e.run(args.hexane_moves, stream.cuda_stream)
     e.sync()
     c0 = np.array([g.state()["counters"] for g in gs])
@@ -636,8 +633,7 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
     out = {"workload": "hexane_grid_cbmc_64 (4096-atom 40 A framework, 64 pressures 1e2-1e6 Pa, 433 K)",
            "systems": len(gs), "moves_per_step_per_system": args.hexane_moves, "steps": steps,
            "moves_per_s": moves / t, "ms_per_step": 1000.0 * t / steps,
-           "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads,
-                            "split": {"systems": len(tuned.split), "cluster": tuned.cluster_b}},
+           "launch_shape": tuned.describe(),
            "grid": {"spacing_A": args.hexane_spacing, "points_per_axis": [int(x) + 1 for x in geom[0]],
                     "bytes_per_grid": int(np.prod(geom[0].astype(np.int64) + 1) * 32), "types": 2,
                     "build_s": t_build},
@@ -679,7 +675,7 @@ def single_config_run(native, stream, peak, sysm, maxmol, equil, timed, ref_cycl
         tuned = autotune.tune([g], precision=prec, moves=200, warm=50, split=False)
         g.set_adsorbates(x_eq)
         g.set_energy(list(g.total_energy()) + [g.intra_energy() if not sysm.molecule.rigid else 0.0, 0.0])
-        e = native.Engine([g], precision=prec, threads=tuned.threads, cluster=tuned.cluster)
+        e = tuned.engine([g], prec)
         c0 = g.state()["counters"].copy()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
@@ -689,7 +685,7 @@ def single_config_run(native, stream, peak, sysm, maxmol, equil, timed, ref_cycl
         t = ev0.elapsed_time(ev1) / 1e3
         d = g.state()["counters"] - c0
         e.close()
-        out[key] = {"moves_per_s": float(d[8]) / t, "launch_shape": {"cluster": tuned.cluster, "threads": tuned.threads},
+        out[key] = {"moves_per_s": float(d[8]) / t, "launch_shape": tuned.describe(),
                     "roofline": roofline_of(d, t, peak), "energy_error": energy_error([g], [sysm])}
     out["mixed_vs_fp64"] = out["mixed"]["moves_per_s"] / out["fp64"]["moves_per_s"]
     if os.path.exists(REF_SIMULATE):

@@ -8,7 +8,10 @@ parameters decide how a batch maps onto the GPU:
 - the CTA size: warps per CTA, which split the trial positions and
   framework chunks of one energy evaluation.
 
-The best pair depends on the number of boxes against the SM count, on the
+- the CTAs per SM (1, 2 or 4): CTAs of different boxes sharing an SM fill
+  each other's barrier waits, with smaller CTAs and less shared memory each.
+
+The best shape depends on the number of boxes against the SM count, on the
 framework sizes and on the loadings. Measured on a B200 for 64 CO2 boxes of
 512-4096 atoms, cluster x threads gave 0.22-1.48 M moves/s.
 
@@ -43,12 +46,24 @@ class Shape:
     table: List[dict]
     split: Tuple[int, ...] = ()     # boxes run in a second launch
     cluster_b: int = 0              # its cluster size
+    ctas_per_sm: int = 1
 
     def apply(self, eng: "native.Engine") -> None:
         """Sets the split of this shape on an engine built with its cluster
         and threads."""
         if self.split:
             eng.set_split(self.split, self.cluster_b)
+
+    def engine(self, systems: Sequence["native.GpuSystem"], precision: int) -> "native.Engine":
+        """An engine of `systems` with this shape."""
+        eng = native.Engine(systems, precision=precision, threads=self.threads, cluster=self.cluster,
+                            ctas_per_sm=self.ctas_per_sm)
+        self.apply(eng)
+        return eng
+
+    def describe(self) -> dict:
+        return {"cluster": self.cluster, "threads": self.threads, "ctas_per_sm": self.ctas_per_sm,
+                "split": {"systems": len(self.split), "cluster": self.cluster_b}}
 
 
 def _signature(systems: Sequence["native.GpuSystem"], precision: int, ordered: bool = False) -> tuple:
@@ -61,17 +76,26 @@ def _signature(systems: Sequence["native.GpuSystem"], precision: int, ordered: b
     return (precision, tuple(sig) if ordered else tuple(sorted(sig)))
 
 
-def candidates(nsys: int, precision: int, sms: int) -> List[Tuple[int, int]]:
-    """Shapes worth timing. A cluster size that needs more CTAs than there
-    are SMs runs in waves (the engine's CTAs hold most of an SM's shared
-    memory) and is skipped."""
+def candidates(nsys: int, precision: int, sms: int) -> List[Tuple[int, int, int]]:
+    """Shapes (cluster, threads, CTAs per SM) worth timing. A shape whose
+    CTAs do not all fit the SMs at once runs in waves and is skipped; several
+    CTAs per SM need the 64-register build (mixed precision) and at most
+    1024 threads per SM between them."""
     threads = (256, 512, 1024) if precision == native.RGPU_MIXED else (128, 256, 512)
     out = []
     for c in (1, 2, 4, 8):
         if nsys * c > sms and c > 1:
             continue
         for t in threads:
-            out.append((c, t))
+            out.append((c, t, 1))
+    if precision == native.RGPU_MIXED:
+        for occ in (2, 4):
+            for c in (2, 4, 8):
+                if nsys * c > sms * occ or nsys * c <= sms:
+                    continue
+                for t in (256, 512):
+                    if t * occ <= 1024:
+                        out.append((c, t, occ))
     return out
 
 
@@ -104,11 +128,11 @@ def tune(systems: Sequence["native.GpuSystem"], precision: int = native.RGPU_MIX
     table = []
     best = None
 
-    def time_shape(c, t, split=(), cb=0):
+    def time_shape(c, t, split=(), cb=0, occ=1):
         """moves/s of one shape and each box's clock cycles in the timed run"""
         for g, x in zip(clones, start):
             g.set_adsorbates(x)
-        eng = native.Engine(clones, precision=precision, threads=t, cluster=c)
+        eng = native.Engine(clones, precision=precision, threads=t, cluster=c, ctas_per_sm=occ)
         try:
             if split:
                 eng.set_split(split, cb)
@@ -128,17 +152,19 @@ def tune(systems: Sequence["native.GpuSystem"], precision: int = native.RGPU_MIX
         return rate, [int(b[15]) - int(a[15]) for a, b in zip(c0, c1)]
 
     cycles = None
-    for c, t in shapes:
+    for shp in shapes:
+        c, t = shp[0], shp[1]
+        occ = shp[2] if len(shp) > 2 else 1
         try:
-            rate, cyc = time_shape(c, t)
+            rate, cyc = time_shape(c, t, occ=occ)
         except native.NativeError as e:
-            table.append({"cluster": c, "threads": t, "error": str(e)})
+            table.append({"cluster": c, "threads": t, "ctas_per_sm": occ, "error": str(e)})
             continue
-        table.append({"cluster": c, "threads": t, "moves_per_s": rate})
+        table.append({"cluster": c, "threads": t, "ctas_per_sm": occ, "moves_per_s": rate})
         if best is None or rate > best[2]:
-            best = (c, t, rate, (), 0)
+            best = (c, t, rate, (), 0, occ)
             cycles = cyc
-    if best is not None and auto_split:
+    if best is not None and auto_split and best[5] == 1:
         c, t = best[0], best[1]
         spare = props.multi_processor_count - len(systems) * c
         by_cost = list(np.argsort(cycles)[::-1])
@@ -155,13 +181,13 @@ def tune(systems: Sequence["native.GpuSystem"], precision: int = native.RGPU_MIX
                     continue
                 table.append({"cluster": c, "threads": t, "split": k, "cluster_b": cb, "moves_per_s": rate})
                 if rate > best[2]:
-                    best = (c, t, rate, split, cb)
+                    best = (c, t, rate, split, cb, 1)
     for g in clones:
         g.close()
     if best is None:
         raise native.NativeError("no launch shape could be created for this batch")
     shape = Shape(cluster=best[0], threads=best[1], moves_per_s=best[2], table=table, split=best[3],
-                  cluster_b=best[4])
+                  cluster_b=best[4], ctas_per_sm=best[5])
     if use_cache:
         _CACHE[key] = shape
     return shape
