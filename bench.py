@@ -78,6 +78,9 @@ def parse_args():
     p.add_argument("--hexane-spacing", type=float, default=0.1, help="energy-grid spacing of the hexane workload [A]")
     p.add_argument("--serve-jobs", type=int, default=300, help="jobs of the served Poisson stream (0 = skip)")
     p.add_argument("--serve-rate", type=float, default=200.0, help="mean arrivals per second")
+    p.add_argument("--serve-steady-rate", type=float, default=25.0,
+                   help="arrival rate of the second, below-capacity served stream (0 = skip)")
+    p.add_argument("--serve-steady-jobs", type=int, default=100)
     return p.parse_args()
 
 
@@ -560,6 +563,14 @@ def serving_run(args):
                "launch_shape": {"cluster": srv.cluster, "threads": srv.threads}, "chunk_steps": srv.chunk,
                "slots": srv.max_slots, "mem_budget_gb": srv.mem_budget / 1e9,
                "status_nonzero_jobs": int(sum(1 for j in jobs if j.result["status"]))})
+    # the same stream at an offered load below what the server serves: the
+    # latencies of a steady state rather than of a queue behind a burst
+    if args.serve_steady_rate > 0:
+        jobs2 = serve.served_jobs(args.serve_steady_jobs, rate=args.serve_steady_rate, seed=5)
+        st2 = serve.Server().run(jobs2, realtime=True)
+        st2.update({"arrival_rate_jobs_per_s": args.serve_steady_rate,
+                    "status_nonzero_jobs": int(sum(1 for j in jobs2 if j.result["status"]))})
+        st["steady_state"] = st2
     return st
 
 

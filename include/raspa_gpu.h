@@ -269,6 +269,19 @@ int rgpu_engine_sync(rgpu_engine *eng);
  * (captured on the first run, and again whenever nsteps changes) instead
  * of launching the kernel directly. */
 int rgpu_engine_use_graph(rgpu_engine *eng, int on);
+/* Replaces system i (creation order) of the engine by `sys` in place, for a
+ * request loop that admits jobs into the slots of finished ones: one
+ * asynchronous copy on `stream` (a cudaStream_t, NULL for the library
+ * stream), ordered after the launches already queued there, with no
+ * allocation, no device synchronisation and a captured graph left valid.
+ * The new system must fit the engine's launch layout (molecule capacity,
+ * Ewald phase tables, kernel build) and the engine must have no batched
+ * staging buffer; otherwise RGPU_E_INVALID and the caller builds a new
+ * engine. A system at its step limit takes no step in a launch, so a
+ * finished job can stay in its slot until it is replaced; the replaced
+ * system may be destroyed once `stream` has passed the copy. No
+ * counterpart in the reference. */
+int rgpu_engine_replace_system(rgpu_engine *eng, int i, rgpu_system *sys, void *stream);
 /* Running energies (8 doubles, first six as rgpu_total_energy), counters
  * (20: attempts[4] and accepted[4] of translation, rotation, insertion,
  * deletion; counted moves, overlaps, pairs visited, pairs in cut-off,
@@ -283,7 +296,9 @@ int rgpu_system_set_energy(rgpu_system *sys, const double *energy8);
  * at step `end_step` (exclusive; 0 = no limit), and steps from `avg_start`
  * on enter the ensemble sums. The reference samples its averages once per
  * cycle (src/monte_carlo.c:580, src/statistics.c:1112); the engine samples
- * once per MC step. */
+ * once per MC step. The limits take effect from the next engine launch;
+ * call this between launches of an engine that holds the system (it does
+ * not wait for other work on the device). */
 int rgpu_system_set_limits(rgpu_system *sys, unsigned long long end_step, unsigned long long avg_start);
 /* Ensemble sums: {steps sampled, sum N, sum N^2, sum U, sum U*N, sum U^2,
  * sum of Widom Rosenbluth weights, Widom samples}, U = the six running

@@ -116,6 +116,10 @@ struct rgpu_engine {
    * a second launch at cluster_b on st_b, side by side with the first
    * (rgpu_engine_set_split). */
   std::vector<int> order;
+  /* rgpu_engine_replace_system: pinned copies of the slot descriptors and
+   * the event of each slot's last copy */
+  RgpuSys *h_slots;
+  std::vector<cudaEvent_t> slot_ev;
   int smem_max;
   int nsplit, cluster_b, fw_items_b, tile_items_b, k_items_b;
   size_t smem_b;
@@ -1183,13 +1187,25 @@ extern "C" int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts
 /* The device slots: d_systems[j] = system order[j], its framework staged in
  * shared memory when its launch group stages it; d_off (once the staging
  * buffer exists) in the same slot order. */
+/* whether system s, in the first launch (second = false) or the second,
+ * has its framework share staged in shared memory: the engine stages when
+ * its plan holds a framework share and the system's share fits it */
+static bool slot_smem_fw(const rgpu_engine *e, const rgpu_system *s, bool second)
+{
+  const int c = second ? e->cluster_b : e->cluster;
+  const int fw_items = second ? e->fw_items_b : e->fw_items, tile_items = second ? e->tile_items_b : e->tile_items;
+  const int share_tiles = (s->h.ntile + c - 1) / c, share_fw = (s->d.nfw + c - 1) / c;
+  return fw_items > 0 && (e->mixed ? share_tiles * RGPU_TILE <= fw_items && share_tiles <= tile_items
+                                   : share_fw <= fw_items);
+}
+
 static cudaError_t upload_slots(rgpu_engine *e)
 {
   const int n = (int)e->sys.size();
   std::vector<RgpuSys> hs(n);
   for (int j = 0; j < n; j++) {
     hs[j] = e->sys[e->order[j]]->h;
-    hs[j].smem_fw = (j < n - e->nsplit ? e->fw_items : e->fw_items_b) > 0;
+    hs[j].smem_fw = slot_smem_fw(e, e->sys[e->order[j]], j >= n - e->nsplit);
   }
   cudaError_t err = cudaMemcpy(e->d_systems, hs.data(), sizeof(RgpuSys) * n, cudaMemcpyHostToDevice);
   if (err != cudaSuccess || !e->d_off) return err;
@@ -1292,6 +1308,7 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
   e->d_off = nullptr;
   e->d_stage = nullptr;
   e->h_stage = nullptr;
+  e->h_slots = nullptr;
   if (cudaMalloc((void **)&e->d_systems, sizeof(RgpuSys) * n) != cudaSuccess) {
     delete e;
     return fail(RGPU_E_CUDA, "cudaMalloc engine");
@@ -1316,6 +1333,9 @@ extern "C" int rgpu_engine_destroy(rgpu_engine *e)
   if (e->ev_fork) cudaEventDestroy(e->ev_fork);
   if (e->ev_join) cudaEventDestroy(e->ev_join);
   if (e->st_b) cudaStreamDestroy(e->st_b);
+  for (cudaEvent_t ev : e->slot_ev)
+    if (ev) cudaEventDestroy(ev);
+  if (e->h_slots) cudaFreeHost(e->h_slots);
   cudaFree(e->d_systems);
   delete e;
   return RGPU_SUCCESS;
@@ -1430,6 +1450,47 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
     CK(cudaGraphLaunch(e->gexec, st));
   }
   for (rgpu_system *s : e->sys) s->records_stale = 1;
+  return RGPU_SUCCESS;
+}
+
+/* Replaces system i of an engine (creation order) by `s`, ordered on
+ * `stream` after the work already queued there: the device slot's
+ * descriptor is rewritten with one asynchronous copy from a pinned host
+ * copy, with no allocation and no device synchronisation, and a captured
+ * graph of the engine stays valid. The new system must fit the engine's
+ * launch layout: the molecule capacity, the Ewald phase tables and the
+ * kernel build; its framework share is staged in shared memory when it
+ * fits the engine's staging, else read from global memory (L2). */
+extern "C" int rgpu_engine_replace_system(rgpu_engine *e, int i, rgpu_system *s, void *stream)
+{
+  if (!e || !s || i < 0 || i >= (int)e->sys.size()) return fail(RGPU_E_INVALID, "bad argument");
+  if (s->h.use_grid && s->h.mol_charged && !s->h.use_coul_grid)
+    return fail(RGPU_E_INVALID, "system with VDW grids and a charged molecule but no Coulomb grid");
+  if ((s->h.use_grid || s->h.flexible) && !e->flex)
+    return fail(RGPU_E_INVALID, "the system needs the flexible-chain/grid build of the engine");
+  if (s->kw > e->kw) return fail(RGPU_E_INVALID, "the system's wave vectors exceed the engine's phase tables");
+  if (s->d.maxmol * s->d.natom > e->max_ads) return fail(RGPU_E_INVALID, "molecule capacity exceeds the engine's");
+  if (e->d_stage) return fail(RGPU_E_INVALID, "engine with a batched-transfer staging buffer");
+  const int n = (int)e->sys.size();
+  int j = 0;
+  while (e->order[j] != i) j++;
+  const bool second = j >= n - e->nsplit;
+  if (!e->h_slots) {
+    if (cudaMallocHost((void **)&e->h_slots, sizeof(RgpuSys) * n) != cudaSuccess)
+      return fail(RGPU_E_CUDA, "cudaMallocHost");
+    e->slot_ev.assign(n, nullptr);
+  }
+  /* the pinned copy of this slot may still be in flight from an earlier
+   * replacement */
+  if (e->slot_ev[j]) CK(cudaEventSynchronize(e->slot_ev[j]));
+  else CK(cudaEventCreateWithFlags(&e->slot_ev[j], cudaEventDisableTiming));
+  RgpuSys h = s->h;
+  h.smem_fw = slot_smem_fw(e, s, second);
+  e->h_slots[j] = h;
+  cudaStream_t st = stream ? (cudaStream_t)stream : e->st;
+  CK(cudaMemcpyAsync(e->d_systems + j, e->h_slots + j, sizeof(RgpuSys), cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(e->slot_ev[j], st));
+  e->sys[i] = s;
   return RGPU_SUCCESS;
 }
 
@@ -1662,8 +1723,11 @@ extern "C" int rgpu_system_set_limits(rgpu_system *s, unsigned long long end_ste
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
   unsigned long long v[2] = {end_step ? end_step : ~0ULL, avg_start};
-  CK(cudaDeviceSynchronize());
-  CK(cudaMemcpy(s->step + 1, v, sizeof v, cudaMemcpyHostToDevice));
+  /* ordered on the system's own stream, which every engine launch waits
+   * for; no device-wide synchronisation, so a request loop can set up new
+   * systems while a launch of other systems runs */
+  CK(cudaMemcpyAsync(s->step + 1, v, sizeof v, cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
   return RGPU_SUCCESS;
 }
 

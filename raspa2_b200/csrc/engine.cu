@@ -1628,6 +1628,11 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
     E.sc.next = &C.next;
     load_sys(E.S, &systems[sysi]);
     RgpuSys &S = *E.S;
+    /* a system at its step limit (a finished job left in its slot) takes
+     * no step in this launch: its CTAs leave before staging anything and
+     * write nothing back. All CTAs of the cluster read the same limits, so
+     * the whole cluster leaves and none waits at the cluster barrier below. */
+    if (S.step[0] >= S.step[1]) return;
     double2 *sk_global = S.sk_ads;
     if (threadIdx.x < 5) C.work[threadIdx.x] = 0ULL;
     if (threadIdx.x < RGPU_NCNT) C.cnt[threadIdx.x] = 0;

@@ -21,6 +21,7 @@ _ip = C.POINTER(C.c_int)
 
 RGPU_FP64 = 0
 RGPU_MIXED = 1
+RGPU_E_INVALID = -1   # include/raspa_gpu.h
 
 EXPORTS = [
     "rgpu_error_string", "rgpu_device_count", "rgpu_system_create", "rgpu_system_destroy",
@@ -33,7 +34,7 @@ EXPORTS = [
     "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_engine_set_split", "rgpu_intra_energy",
     "rgpu_system_set_grids", "rgpu_system_checkpoint_size", "rgpu_system_checkpoint", "rgpu_system_restore",
     "rgpu_grid_build_coulomb", "rgpu_system_set_coulomb_grid", "rgpu_engine_get_state", "rgpu_engine_set_adsorbates",
-    "rgpu_engine_staging_bytes",
+    "rgpu_engine_staging_bytes", "rgpu_engine_replace_system",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -494,6 +495,17 @@ class Engine:
     def use_graph(self, on: bool = True):
         """Replay a CUDA graph of the launch in run() (rgpu_engine_use_graph)."""
         _check(load().rgpu_engine_use_graph(self.h, C.c_int(1 if on else 0)))
+
+    def replace(self, i: int, system: GpuSystem, stream: Optional[int] = None) -> bool:
+        """Puts `system` in place of system i, ordered on `stream` after the
+        queued launches (rgpu_engine_replace_system). Returns False when the
+        system does not fit this engine's layout (build a new engine)."""
+        rc = load().rgpu_engine_replace_system(self.h, C.c_int(i), system.h, C.c_void_p(stream or 0))
+        if rc == RGPU_E_INVALID:
+            return False
+        _check(rc)
+        self.systems[i] = system
+        return True
 
     def close(self):
         if getattr(self, "h", None):

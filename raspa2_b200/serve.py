@@ -197,58 +197,103 @@ class Server:
     def run(self, jobs: Sequence[Job], realtime: bool = True) -> dict:
         """Serves `jobs` (arrival times relative to the call) to completion.
         With realtime=False every job is available at once. Returns the
-        latency and throughput figures; per-job results are on the jobs."""
+        latency and throughput figures; per-job results are on the jobs.
+
+        The engine's slots are reused in place: a finished job's system
+        stays in its slot (at its step limit it takes no step) until a new
+        job's system replaces it (Engine.replace, no allocation, no device
+        synchronisation, the captured graph stays valid). A new engine is
+        built only when more jobs are active than the engine has slots, or
+        when a new system does not fit its layout. Replaced systems are freed
+        in batches, when the device is idle anyway."""
         import torch
 
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
         waiting: collections.deque = collections.deque()
-        active: List[list] = []          # [job, GpuSystem, steps done, footprint]
+        slots: List[Optional[list]] = []     # engine slot -> [job, GpuSystem, steps done, footprint] or None
+        occupants: List["native.GpuSystem"] = []   # the system in each slot (a finished job's until replaced)
+        unplaced: List[list] = []            # admitted, not yet in the engine
+        to_free: List["native.GpuSystem"] = []
         mem_used = 0
         eng = None
-        dirty = True
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
         total_steps = 0
         busy = 0.0
         max_active = 0
+        rebuilds = 0
+        replacements = 0
+
+        def n_active():
+            return sum(1 for a in slots if a is not None) + len(unplaced)
 
         def admit_ready():
-            nonlocal mem_used, dirty
+            nonlocal mem_used
             t = now()
             while pending and (pending[0].arrival <= t or not realtime):
                 waiting.append(pending.popleft())
-            while waiting and len(active) < self.max_slots:
+            while waiting and n_active() < self.max_slots:
                 fp = footprint_bytes(waiting[0])
-                if mem_used + fp > self.mem_budget and active:
+                if mem_used + fp > self.mem_budget and n_active():
                     break
                 job = waiting.popleft()
                 g = self._admit(job, now())
-                active.append([job, g, int(g.state()["step"]) if job.resume is not None else 0, fp])
+                unplaced.append([job, g, int(g.state()["step"]) if job.resume is not None else 0, fp])
                 mem_used += fp
-                dirty = True
 
-        while pending or waiting or active:
+        def place():
+            """the admitted jobs into free slots, or a new engine"""
+            nonlocal eng, slots, occupants, rebuilds, replacements
+            rest = []
+            for entry in unplaced:
+                i = next((k for k, a in enumerate(slots) if a is None), None)
+                if eng is not None and i is not None and eng.replace(i, entry[1], self.stream.cuda_stream):
+                    to_free.append(occupants[i])
+                    slots[i], occupants[i] = entry, entry[1]
+                    replacements += 1
+                else:
+                    rest.append(entry)
+            unplaced.clear()
+            if not rest:
+                return
+            # a new engine: the active jobs, the new ones, and the finished
+            # jobs' systems still held (their slots stay free for later jobs)
+            keep = [(a, g) for a, g in zip(slots, occupants)]
+            keep = [(a, g) for a, g in keep if a is not None] + [(e, e[1]) for e in rest] + \
+                   [(a, g) for a, g in keep if a is None]
+            keep = keep[:max(self.max_slots, sum(1 for a, _ in keep if a is not None))]
+            held = {id(g) for _, g in keep}
+            to_free.extend(g for g in occupants if id(g) not in held)
+            slots = [a for a, _ in keep]
+            occupants = [g for _, g in keep]
+            if eng is not None:
+                eng.close()
+            eng = native.Engine(occupants, precision=self.precision, threads=self.threads, cluster=self.cluster)
+            eng.use_graph(True)
+            rebuilds += 1
+
+        while pending or waiting or unplaced or any(a is not None for a in slots):
             admit_ready()
-            if not active:
+            if unplaced:
+                place()
+            running = [a for a in slots if a is not None]
+            if not running:
                 if pending:
                     time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
                 continue
-            if dirty:
-                if eng is not None:
-                    eng.close()
-                eng = native.Engine([a[1] for a in active], precision=self.precision, threads=self.threads,
-                                    cluster=self.cluster)
-                dirty = False
-            running = list(active)                            # the jobs in this launch
             max_active = max(max_active, len(running))
-            tl = now()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(self.stream)
             eng.run(self.chunk, self.stream.cuda_stream)      # asynchronous
+            ev1.record(self.stream)
             self.launches += 1
             admit_ready()                                     # overlaps the launch
             eng.sync()
-            busy += now() - tl
-            retired = set()
-            for a in running:
+            ev1.synchronize()
+            busy += ev0.elapsed_time(ev1) / 1e3               # device time of the launch
+            for k, a in enumerate(slots):
+                if a is None:
+                    continue
                 job, g, done, fp = a
                 if job.raspa_output:
                     # the engine stopped the job at its block boundary or ran the chunk
@@ -262,23 +307,30 @@ class Server:
                 if a[2] >= job.steps:
                     job.result = self._result(job, g)
                     job.finished = now()
-                    g.close()
                     mem_used -= fp
-                    retired.add(job.id)
-                    dirty = True
-            active = [a for a in active if a[0].id not in retired]
+                    slots[k] = None                           # the system stays in the slot, idle
+            if len(to_free) >= 32:
+                for g in to_free:
+                    g.close()
+                to_free.clear()
         if eng is not None:
             eng.close()
+        for g in to_free + occupants:
+            g.close()
         torch.cuda.synchronize()
         makespan = now()
         lat = np.array([j.latency for j in jobs]) * 1e3
         wait = np.array([j.admitted - j.arrival for j in jobs]) * 1e3
+        span = max(j.arrival for j in jobs) - min(j.arrival for j in jobs) if realtime and len(jobs) > 1 else 0.0
+        req = float(sum(j.steps for j in jobs))
         return {"jobs": len(jobs), "makespan_s": makespan, "launches": self.launches,
                 "p50_job_ms": float(np.percentile(lat, 50)), "p99_job_ms": float(np.percentile(lat, 99)),
                 "p50_wait_ms": float(np.percentile(wait, 50)), "p99_wait_ms": float(np.percentile(wait, 99)),
                 "mc_steps": int(total_steps), "mc_steps_per_s": total_steps / makespan, "max_active": max_active,
                 "p50_service_ms": float(np.percentile([(j.finished - j.admitted) * 1e3 for j in jobs], 50)),
-                "gpu_busy_frac": busy / makespan}
+                "gpu_busy_frac": busy / makespan,
+                "offered_steps_per_s": req / span if span > 0 else None,
+                "engine_builds": rebuilds, "slot_replacements": replacements}
 
 
 # --------------------------------------------------------------------------
