@@ -92,3 +92,20 @@ def test_served_job_returns_raspa_output(cuda):
     assert abs(n - r["loading"]) <= 1e-12 * max(1.0, n)
     assert "Average loading absolute [molecules/unit cell]" in r["raspa_summary"]
     assert "Enthalpy of adsorption:" in r["raspa_summary"]
+
+
+def test_jobs_reuse_the_slots_of_finished_ones(cuda):
+    """With two slots, later jobs go into the slots of finished ones
+    (rgpu_engine_replace_system, a system of another framework and size in
+    place of the old one) and their results are bitwise those of the jobs run
+    alone."""
+    base = _jobs()
+    alone = []
+    for j in _fresh(base):
+        serve.Server(chunk=200, threads=256).run([j], realtime=False)
+        alone.append(j.result)
+    jobs = _fresh(base)
+    st = serve.Server(chunk=200, threads=256, max_slots=2).run(jobs, realtime=False)
+    assert st["max_active"] == 2 and st["slot_replacements"] >= 1
+    for a, j in zip(alone, jobs):
+        _same(a, j.result)
