@@ -344,7 +344,7 @@ def write_restart_inputs(s, d, xyz, cycles, seed):
     reference that starts from the configuration xyz ([n][natom][3]) through
     its restart file (RestartFile yes)."""
     from raspa2_b200 import restart
-    raspa_io.write_inputs(s, d, cycles=cycles, init_cycles=0, print_every=10 ** 9, seed=seed, restart=True)
+    raspa_io.write_inputs(s, d, cycles=cycles, init_cycles=0, print_every=1, seed=seed, restart=True)
     restart.write_restart(restart.restart_path(s, d), s, np.asarray(xyz, float).reshape(-1, s.molecule.n_atoms, 3))
     return d
 
@@ -368,9 +368,11 @@ def reference_from(sys_xyz, cycles, seed0, workdir, cores):
         out = os.path.join(d, "Output", "System_0")
         f = os.path.join(out, os.listdir(out)[0])
         mv, cpu = parse_reference_output(f)
-        m = re.search(r"Average loading absolute \[molecules/unit cell\]\s+([-\d.eE+]+)", open(f).read())
-        per_cell = float(m.group(1)) if m else float("nan")
-        return mv, cpu, wall, per_cell * float(np.prod(s.unit_cells))
+        # the running average of the molecule count the reference prints
+        # every cycle (its block averages need five blocks of cycles)
+        m = re.findall(r"current number of integer/fractional/reaction molecules: \d+/\d+/\d+ \(avg\.\s+([-\d.eE+]+)\)",
+                       open(f).read())
+        return mv, cpu, wall, float(m[-1]) if m else float("nan")
 
     with ThreadPoolExecutor(max_workers=cores) as ex:
         return list(ex.map(run, dirs))

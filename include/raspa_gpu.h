@@ -97,7 +97,7 @@ typedef struct {
    * Rosenbluth factor, averaged, as the reference averages it, over the
    * first ntrial candidates (src/cbmc.c:548, :2401, :2793). ntors = 0 means
    * the reference's default NumberOfTrialPositionsTorsion, 100 (at most
-   * 248). chain_scheme 1: each trial draws its own bend angle and dihedral
+   * 128). chain_scheme 1: each trial draws its own bend angle and dihedral
    * from their Boltzmann distributions (no torsion factor in the weight). */
   int chain_scheme;
   int ntors;

@@ -58,7 +58,8 @@ __host__ __device__ inline size_t rgpu_align(size_t x) { return (x + 255) & ~(si
  * (flexible-chain builds only): {cos theta, sin theta, cos phi, sin phi,
  * torsion Rosenbluth factor} for beads 2.. natom-1 and each trial */
 #define RGPU_ANG_STRIDE 5
-#define RGPU_ANG_DOUBLES (RGPU_ANG_STRIDE * (RGPU_MAX_ATOMS - 2) * RGPU_MAX_TRIALS)
+#define RGPU_ANG_TABLE (RGPU_ANG_STRIDE * (RGPU_MAX_ATOMS - 2) * RGPU_MAX_TRIALS)
+#define RGPU_ANG_DOUBLES (RGPU_ANG_TABLE + RGPU_MAX_ATOMS)   /* + the bend angle of each bead (chain_scheme 0) */
 
 __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, int tiles, int max_ads_atoms, int kw,
                                                       int k_items, int nwarps, int flex)
@@ -1028,66 +1029,74 @@ __device__ __forceinline__ void chain_angles_group(const RgpuSys &S, int i, int 
  * host and adsorbate VDW (u[0], u[2]) and the intramolecular energy
  * (uintra: bonded + LJ), or fail. Molecule m is the one retraced; `exclude`
  * leaves a molecule out of the adsorbate sums. All threads call. */
+/* The bend angle shared by the trials of bead i >= 2 in the reference's
+ * scheme (chain_scheme 0): a growth draws it from sin(theta) exp(-beta
+ * U_bend) (proposals in the slots of trial RGPU_REF_THETA_TRIAL from
+ * RGPU_REF_THETA_SLOT on, tried in order: the lanes try 32 at once and the
+ * lowest accepted wins), the distribution the reference's internal
+ * Metropolis chain (src/cbmc.c:1822-2106) samples; a retrace (old !=
+ * nullptr) keeps the old bead's angle. Every lane of the warp calls and
+ * gets the angle. */
+__device__ __noinline__ double chain_ref_theta(const RgpuSys &S, int i, int stage, uint64_t step, int lane,
+                                                  const double (*old)[3])
+{
+  if (old) return chain_angle(old[i - 2], old[i - 1], old[i]);
+  for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
+    const int k = RGPU_REF_THETA_SLOT + 3 * (base + lane);
+    auto U = [&](int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, RGPU_REF_THETA_TRIAL, d)); };
+    const double u1 = U(k), u2 = U(k + 1), u3 = U(k + 2);
+    const double th = S.bend_theta0 + S.bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
+    const unsigned ok = __ballot_sync(RGPU_FULL, th > 0.0 && th < M_PI && u3 < sin(th));
+    if (ok) return __shfl_sync(RGPU_FULL, th, __ffs(ok) - 1);
+  }
+  return S.bend_theta0;
+}
+
 /* The reference's bonded trials (chain_scheme 0; GenerateTrialOrientationsMCScheme,
- * src/cbmc.c:1580-2480, for a linear chain) of trial t of bead i >= 2, by
- * one warp (every lane calls), into a[0..4] (lane 0 writes):
- * - the bend angle, one per bead and stage: a growth draws it from
- *   sin(theta) exp(-beta U_bend) (proposals in the slots of trial
- *   RGPU_REF_THETA_TRIAL from RGPU_REF_THETA_SLOT on, tried in order: the
- *   lanes try 32 at once and the lowest accepted wins), which is the
- *   distribution the reference's internal Metropolis chain
- *   (src/cbmc.c:1822-2106) samples; a retrace (old != nullptr) keeps the
- *   old bead's angle;
+ * src/cbmc.c:1580-2480, for a linear chain) of trial t of bead i >= 2 with
+ * the bead's bend angle theta, by one warp (every lane calls), into
+ * a[0..4] (lane 0 writes):
  * - the dihedral: ntors uniform candidates (slot k of the trial), one chosen
  *   by its torsion Boltzmann factor with SelectTrialPosition's rule
  *   (src/cbmc.c:563-599, 2403-2408; one uniform in slot
- *   RGPU_REF_TORS_SEL_SLOT); candidate k is lane k % 32 of row k / 32,
- *   and the cumulative sum runs row by row as warp scans. A retrace's
- *   trial 0 keeps the old dihedral as its candidate 0 and chooses it.
- *   Without a torsion (bead 2) the dihedral is uniform (src/cbmc.c:2410);
+ *   RGPU_REF_TORS_SEL_SLOT). Candidates 2p and 2p+1 come from one Philox
+ *   block and belong to lane p % 32 of row p / 32; the cumulative sum runs
+ *   row by row as warp scans. A retrace's trial 0 keeps the old dihedral as
+ *   its candidate 0 and chooses it. Without a torsion (bead 2) the dihedral
+ *   is uniform (src/cbmc.c:2410);
  * - the torsion Rosenbluth factor: the mean of exp(-beta U_torsion) over
  *   candidates 0 .. ntrial-1, the reference's ComputeNormalizedRosenbluthWeight
  *   (src/cbmc.c:542-552 sums up to the global NumberOfTrialPositions; called
  *   at :2401); 1 for bead 2. */
-__device__ __forceinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage, int t, uint64_t step, int lane,
-                                                const double (*old)[3], double *a)
+__device__ __noinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage, int t, uint64_t step, int lane,
+                                                const double (*old)[3], double theta, double *a)
 {
-  auto U = [&](int tr, int d) { return rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, tr, d)); };
-  double theta = S.bend_theta0;
-  if (old) {
-    theta = chain_angle(old[i - 2], old[i - 1], old[i]);
-  } else {
-    for (int base = 0; base < RGPU_CHAIN_TRIES; base += 32) {
-      const int k = RGPU_REF_THETA_SLOT + 3 * (base + lane);
-      const double u1 = U(RGPU_REF_THETA_TRIAL, k), u2 = U(RGPU_REF_THETA_TRIAL, k + 1);
-      const double u3 = U(RGPU_REF_THETA_TRIAL, k + 2);
-      const double th = S.bend_theta0 + S.bend_sigma * sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
-      const unsigned ok = __ballot_sync(RGPU_FULL, th > 0.0 && th < M_PI && u3 < sin(th));
-      if (ok) {
-        theta = __shfl_sync(RGPU_FULL, th, __ffs(ok) - 1);
-        break;
-      }
-    }
-  }
   const bool keep_old = old && t == 0;
   double phi = 0.0, wt = 1.0;
   if (i == 2) {
-    if (!keep_old) phi = 2.0 * M_PI * U(t, 0) - M_PI;
+    if (!keep_old) phi = 2.0 * M_PI * rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, 0)) - M_PI;
   } else {
-    /* candidate k = lane + 32 j sits in row j of the warp */
-    const int n = S.ntors, nt = S.ntrial, rows = (n + 31) >> 5;
-    double bf[RGPU_TORS_PER_LANE];
+    const int n = S.ntors, nt = S.ntrial, rows = (n + 63) >> 6;
+    double bf[RGPU_TORS_ROWS][2];
     double big = -1e300, wsum = 0.0;
 #pragma unroll
-    for (int j = 0; j < RGPU_TORS_PER_LANE; j++) {
-      const int k = lane + 32 * j;
-      bf[j] = -1e300;
-      if (j < rows && k < n) {
-        const double cs = (keep_old && k == 0) ? chain_cos_dihedral(old[i - 3], old[i - 2], old[i - 1], old[i])
-                                               : cos(2.0 * M_PI * U(t, k) - M_PI);
-        bf[j] = -S.beta * chain_torsion_energy(S, cs);
-        big = fmax(big, bf[j]);
-        if (k < nt) wsum += exp(bf[j]);
+    for (int j = 0; j < RGPU_TORS_ROWS; j++) {
+      const int k0 = 2 * (lane + 32 * j);
+      bf[j][0] = bf[j][1] = -1e300;
+      if (j < rows && k0 < n) {
+        double u[2];
+        rgpu_uniform_pair(S.seed, S.sys_id, step, chain_slot(stage, i, t, k0) >> 1, u);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int k = k0 + h;
+          if (k < n) {
+            const double cs = (keep_old && k == 0) ? chain_cos_dihedral(old[i - 3], old[i - 2], old[i - 1], old[i])
+                                                   : cos(2.0 * M_PI * u[h] - M_PI);
+            bf[j][h] = -S.beta * chain_torsion_energy(S, cs);
+            big = fmax(big, bf[j][h]);
+            if (k < nt) wsum += exp(bf[j][h]);
+          }
+        }
       }
     }
     for (int o = 16; o; o >>= 1) {
@@ -1098,10 +1107,14 @@ __device__ __forceinline__ void chain_ref_trial(const RgpuSys &S, int i, int sta
     if (!keep_old) {
       double tot = 0.0;
 #pragma unroll
-      for (int j = 0; j < RGPU_TORS_PER_LANE; j++)
-        if (j < rows && lane + 32 * j < n) tot += exp(bf[j] - big);
+      for (int j = 0; j < RGPU_TORS_ROWS; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+          if (j < rows && 2 * (lane + 32 * j) + h < n) tot += exp(bf[j][h] - big);
       for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(RGPU_FULL, tot, o);
-      const double target = U(t, RGPU_REF_TORS_SEL_SLOT) * tot;
+      const double target =
+          rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, RGPU_REF_TORS_SEL_SLOT)) *
+          tot;
       /* the first candidate whose cumulative sum reaches the target, row
        * by row; none (rounding only): the last, where the serial search
        * stops */
@@ -1109,24 +1122,27 @@ __device__ __forceinline__ void chain_ref_trial(const RgpuSys &S, int i, int sta
       double before = 0.0;
       bool done = false;
 #pragma unroll
-      for (int j = 0; j < RGPU_TORS_PER_LANE; j++) {
+      for (int j = 0; j < RGPU_TORS_ROWS; j++) {
         if (!done && j < rows) {
-          const bool in = lane + 32 * j < n;
-          const double e = in ? exp(bf[j] - big) : 0.0;
-          double incl = e;
+          const int k0 = 2 * (lane + 32 * j);
+          const double e0 = k0 < n ? exp(bf[j][0] - big) : 0.0, e1 = k0 + 1 < n ? exp(bf[j][1] - big) : 0.0;
+          const double part = e0 + e1;
+          double incl = part;
           for (int o = 1; o < 32; o <<= 1) {
             const double y = __shfl_up_sync(RGPU_FULL, incl, o);
             if (lane >= o) incl += y;
           }
-          const unsigned hit = __ballot_sync(RGPU_FULL, in && before + incl >= target);
+          const double c0 = before + (incl - part) + e0;
+          const int mine = (k0 < n && c0 >= target) ? k0 : ((k0 + 1 < n && c0 + e1 >= target) ? k0 + 1 : -1);
+          const unsigned hit = __ballot_sync(RGPU_FULL, mine >= 0);
           if (hit) {
-            kc = 32 * j + __ffs(hit) - 1;
+            kc = __shfl_sync(RGPU_FULL, mine, __ffs(hit) - 1);
             done = true;
           }
           before += __shfl_sync(RGPU_FULL, incl, 31);
         }
       }
-      if (lane == 0) phi = 2.0 * M_PI * U(t, kc) - M_PI;
+      if (lane == 0) phi = 2.0 * M_PI * rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, kc)) - M_PI;
     }
   }
   if (lane == 0) {
@@ -1154,9 +1170,18 @@ __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stag
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int ntask = na > 2 ? (na - 2) * nt : 0;
   if (S.chain_scheme == 0) {
+    /* each bead's bend angle once (one warp per bead), then one warp per
+     * (bead, trial); the angles sit after the table */
+    double *theta = tab + RGPU_ANG_TABLE;
+    for (int i = 2 + (threadIdx.x >> 5); i < na; i += nw) {
+      const double th = chain_ref_theta(S, i, stage, E.step, lane, old);
+      if (lane == 0) theta[i] = th;
+    }
+    __syncthreads();
     for (int task = threadIdx.x >> 5; task < ntask; task += nw) {
       const int i = 2 + task / nt, t = task % nt;
-      chain_ref_trial(S, i, stage, t, E.step, lane, old, tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t));
+      chain_ref_trial(S, i, stage, t, E.step, lane, old, theta[i],
+                      tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t));
     }
     return;
   }

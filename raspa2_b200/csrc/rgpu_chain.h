@@ -45,7 +45,7 @@
 #define RGPU_REF_TORS_SEL_SLOT 255
 #define RGPU_REF_THETA_TRIAL 15
 #define RGPU_REF_THETA_SLOT 256
-#define RGPU_TORS_PER_LANE ((RGPU_MAX_TORS + 31) / 32)
+#define RGPU_TORS_ROWS ((RGPU_MAX_TORS + 63) / 64)   /* rows of candidate pairs per warp */
 
 /* slot of draw k (< 512) of trial t of bead i in growth stage `stage`
  * (0: growth of a new configuration, 1: retrace of an old one) */

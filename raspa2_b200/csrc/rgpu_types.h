@@ -23,7 +23,7 @@
 #define RGPU_MAX_FWTYPES 4     /* framework pseudo-atom types */
 #define RGPU_MAX_TRIALS 16     /* CBMC trial positions per step */
 #define RGPU_MAX_POS 64        /* bead positions evaluated in one batch */
-#define RGPU_MAX_TORS 248      /* torsion candidates per chain trial (chain_scheme 0); slots 0..247 */
+#define RGPU_MAX_TORS 128      /* torsion candidates per chain trial (chain_scheme 0; the reference default is 100) */
 #define RGPU_TILE 16           /* framework atoms per tile (mixed-precision layout) */
 
 /* per-system counters */
