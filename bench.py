@@ -514,6 +514,8 @@ def run_ours(args):
     if e2e:
         line["e2e"] = e2e
     line["precision"] = {"co2_batched": energy_error(gs, sys_list)}
+    if rank == 0 and world == 1 and not args.no_plain and prec == native.RGPU_MIXED:
+        line["batched_fp64"] = batched_fp64_run(native, stream, gs, sys_list, args, peak)
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_gpu"] = plain_gpu_rate(native, stream)
         # the two single-system configurations, each on its own
@@ -659,6 +661,37 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
                           enumerate(["translation", "rotation", "insertion", "deletion"])},
            "reinsertion_acceptance": float(d[19]) / max(float(d[18]), 1.0), "phases": phases}
     del flush
+    return out
+
+
+def batched_fp64_run(native, stream, gs, sys_list, args, peak, steps=3):
+    """The same batch of systems on the FP64 engine (the plain path's
+    arithmetic: FP64 pair terms, erfc and S(k)), from the mixed run's final
+    configurations, at its own autotuned launch shape: device-timed moves/s
+    and the error of its running energies against the FP64 recomputation."""
+    import torch
+    from raspa2_b200 import autotune
+    g64 = [native.GpuSystem(s, maxmol=args.maxmol, seed=777, stream_id=i) for i, s in enumerate(sys_list)]
+    for g, src in zip(g64, gs):
+        g.set_adsorbates(src.adsorbates())
+        g.set_energy(list(g.total_energy()) + [0.0, 0.0])
+    tuned = autotune.tune(g64, precision=native.RGPU_FP64, moves=300, warm=50)
+    e = tuned.engine(g64, native.RGPU_FP64)
+    c0 = np.array([g.state()["counters"] for g in g64])
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        evs[k][0].record(stream)
+        e.run(args.moves_per_step, stream.cuda_stream)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in evs) / 1e3
+    d = (np.array([g.state()["counters"] for g in g64]) - c0).sum(axis=0)
+    out = {"moves_per_s": float(d[8]) / t, "launch_shape": tuned.describe(), "steps": steps,
+           "moves_per_step_per_system": args.moves_per_step, "roofline_fp32_equivalent": roofline_of(d, t, peak),
+           "energy_error": energy_error(g64, sys_list)}
+    e.close()
+    for g in g64:
+        g.close()
     return out
 
 
