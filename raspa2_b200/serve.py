@@ -141,6 +141,31 @@ class Server:
         self.stream = torch.cuda.Stream()
         self.launches = 0
 
+    def _placeholder(self, jobs: Sequence[Job]) -> Optional["native.GpuSystem"]:
+        """A system that takes no step (one step run, limit 1) and holds the
+        engine's free slots. It is the job list's largest framework with the
+        largest wave-vector set and molecule capacity of the list, so that an
+        engine sized with it takes every job of the list in place."""
+        if not jobs:
+            return None
+        big = max(jobs, key=lambda j: j.system.n_framework())
+        ew = [j for j in jobs if j.system.ewald]
+        s = big.system
+        if ew:
+            kmax = max((tuple(j.system.kmax) for j in ew), key=lambda k: max(k))
+            src = max(ew, key=lambda j: j.system.n_framework()).system
+            s = dataclasses.replace(src, kmax=kmax, name="placeholder")
+        natom = s.molecule.n_atoms
+        maxmol = max((j.maxmol * j.system.molecule.n_atoms + natom - 1) // natom for j in jobs)
+        g = native.GpuSystem(s, maxmol=maxmol, seed=1, stream_id=1 << 30)
+        g.set_adsorbates(np.zeros((0, natom, 3)))
+        g.set_limits(1, 1)
+        e = native.Engine([g], precision=self.precision, threads=self.threads, cluster=self.cluster)
+        e.run(1, self.stream.cuda_stream)
+        e.sync()
+        e.close()
+        return g
+
     def _admit(self, job: Job, now: float) -> "native.GpuSystem":
         g = native.GpuSystem(job.system, maxmol=job.maxmol, seed=job.seed, stream_id=job.id)
         if job.resume is not None:
@@ -199,13 +224,14 @@ class Server:
         With realtime=False every job is available at once. Returns the
         latency and throughput figures; per-job results are on the jobs.
 
-        The engine's slots are reused in place: a finished job's system
-        stays in its slot (at its step limit it takes no step) until a new
-        job's system replaces it (Engine.replace, no allocation, no device
+        The engine has max_slots slots from its first build; the free ones
+        hold an idle placeholder system sized for the job list
+        (`_placeholder`), and a finished job's system stays in its slot (at
+        its step limit it takes no step). A new job's system replaces one of
+        them in place (Engine.replace: no allocation, no device
         synchronisation, the captured graph stays valid). A new engine is
-        built only when more jobs are active than the engine has slots, or
-        when a new system does not fit its layout. Replaced systems are freed
-        in batches, when the device is idle anyway."""
+        built only when a system does not fit the engine's layout. Replaced
+        systems are freed in batches, when the device is idle anyway."""
         import torch
 
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
@@ -223,6 +249,7 @@ class Server:
         max_active = 0
         rebuilds = 0
         replacements = 0
+        holder = self._placeholder(jobs)
 
         def n_active():
             return sum(1 for a in slots if a is not None) + len(unplaced)
@@ -248,7 +275,8 @@ class Server:
             for entry in unplaced:
                 i = next((k for k, a in enumerate(slots) if a is None), None)
                 if eng is not None and i is not None and eng.replace(i, entry[1], self.stream.cuda_stream):
-                    to_free.append(occupants[i])
+                    if occupants[i] is not holder:
+                        to_free.append(occupants[i])
                     slots[i], occupants[i] = entry, entry[1]
                     replacements += 1
                 else:
@@ -263,7 +291,9 @@ class Server:
                    [(a, g) for a, g in keep if a is None]
             keep = keep[:max(self.max_slots, sum(1 for a, _ in keep if a is not None))]
             held = {id(g) for _, g in keep}
-            to_free.extend(g for g in occupants if id(g) not in held)
+            to_free.extend(g for g in occupants if id(g) not in held and g is not holder)
+            if holder is not None:
+                keep += [(None, holder)] * (self.max_slots - len(keep))
             slots = [a for a, _ in keep]
             occupants = [g for _, g in keep]
             if eng is not None:
@@ -315,7 +345,7 @@ class Server:
                 to_free.clear()
         if eng is not None:
             eng.close()
-        for g in to_free + occupants:
+        for g in set(to_free + occupants + ([holder] if holder is not None else [])):
             g.close()
         torch.cuda.synchronize()
         makespan = now()
