@@ -552,22 +552,6 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     /* NumberOfTrialPositionsTorsion defaults to 100 (src/input.c:349) */
     h.ntors = d->ntors > 0 ? d->ntors : 100;
   }
-  /* reach of a molecule from its atom 0: the rigid geometry's largest
-   * distance, or a chain's bonds laid end to end */
-  {
-    double reach = 0.0;
-    if (d->flexible) {
-      reach = (d->natom - 1) * d->bond;
-    } else {
-      for (int a = 1; a < d->natom; a++) {
-        double r2 = 0.0;
-        for (int c = 0; c < 3; c++) r2 += (d->mol_ref[3 * a + c] - d->mol_ref[c]) * (d->mol_ref[3 * a + c] - d->mol_ref[c]);
-        reach = std::max(reach, sqrt(r2));
-      }
-    }
-    const double cull = d->cutoff + reach + 1e-3;
-    h.ads_cull2f = (float)(cull * cull);
-  }
   /* the exclusion sum K qa qb erf(alpha r)/r over the molecule's charged
    * pairs (src/ewald.c:7312-7330) is a constant of a rigid molecule */
   h.excl_mol = 0.0;

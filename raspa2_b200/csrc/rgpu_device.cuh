@@ -200,15 +200,6 @@ __device__ inline void block_sum2(double &a, double &b, double *red)
  * per-warp queue and evaluated 32 at a time, so the LJ + erfc arithmetic runs
  * with all lanes busy instead of under a divergent branch.
  */
-/* Accumulator of a lane's FP32 pair terms on the mixed path: each term is
- * added to a double (the sums of a unit mix positive and negative
- * real-space terms of magnitude 1e4, so an FP32 running sum would add
- * rounding of the partial sums to the terms' own) */
-#ifndef RGPU_ACC_T
-#define RGPU_ACC_T double
-#endif
-typedef RGPU_ACC_T rgpu_acc;
-
 struct EvalScratch {
   double *uv;     /* [max units] */
   double *uc;
@@ -253,7 +244,7 @@ __device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwar
 /* The LJ + real-space term of one queued pair; lane `lane` takes entry
  * `lane` of the warp queue. */
 __device__ __forceinline__ void pair_mixed_queued(const RgpuLJf *P, float r2, float qj, bool charged, float qa,
-                                                  float alpha, bool check, float thr, rgpu_acc &av, rgpu_acc &ac, int &ov,
+                                                  float alpha, bool check, float thr, float &av, float &ac, int &ov,
                                                   int &nch, int type)
 {
   const RgpuLJf L = P[type];
@@ -287,7 +278,7 @@ struct PairQueue {
   float qa, alpha, thr;
 };
 
-__device__ __forceinline__ void queue_add(PairQueue &Q, bool in, float r2, float q, int t, rgpu_acc &av, rgpu_acc &ac,
+__device__ __forceinline__ void queue_add(PairQueue &Q, bool in, float r2, float q, int t, float &av, float &ac,
                                           int &ov, int &nin, int &nch)
 {
   const int lane = threadIdx.x & 31;
@@ -316,7 +307,7 @@ __device__ __forceinline__ void queue_add(PairQueue &Q, bool in, float r2, float
 }
 
 /* evaluates what is left in the queue */
-__device__ __forceinline__ void queue_drain(PairQueue &Q, rgpu_acc &av, rgpu_acc &ac, int &ov, int &nin, int &nch)
+__device__ __forceinline__ void queue_drain(PairQueue &Q, float &av, float &ac, int &ov, int &nin, int &nch)
 {
   const int lane = threadIdx.x & 31;
   __syncwarp();
@@ -329,11 +320,11 @@ __device__ __forceinline__ void queue_drain(PairQueue &Q, rgpu_acc &av, rgpu_acc
   __syncwarp();
 }
 
-static_assert(RGPU_TILE == 8 || RGPU_TILE == 16 || RGPU_TILE == 32, "unit_tiles_mixed splits a warp into whole tiles");
+static_assert(RGPU_TILE == 16, "unit_tiles_mixed visits two tiles per warp pass, one per half warp");
 
 /* framework tiles [t0, t1) for bead b, FP32 path (warp-wide) */
 __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *fw, const TileRec *tiles, int t0, int t1,
-                                                 const BeadPos &b, bool check, rgpu_acc &av, rgpu_acc &ac, int &ov,
+                                                 const BeadPos &b, bool check, float &av, float &ac, int &ov,
                                                  int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
 {
   const int lane = threadIdx.x & 31;
@@ -360,19 +351,19 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
       vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
     }
     unsigned m = __ballot_sync(RGPU_FULL, vis);
-    /* 32 / RGPU_TILE visible tiles per pass of the warp: lane group g
-     * (lanes g*RGPU_TILE ..) takes the atoms of the g-th remaining visible
-     * tile */
-    const int g = lane / RGPU_TILE, hl = lane % RGPU_TILE;
+    /* two visible tiles per pass of the warp: lanes 0-15 take the atoms of
+     * the first, lanes 16-31 those of the second */
+    const int half = lane >> 4, hl = lane & 15;
     while (m) {
-      const unsigned pos = __fns(m, 0, g + 1);
-      const bool have = pos != 0xffffffffu;
-      const int mine = have ? (int)pos : 0;
-      const int ns = __shfl_sync(RGPU_FULL, tn, mine);
-      const int nmine = have ? ns : 0;
-#pragma unroll
-      for (int r = 0; r < 32 / RGPU_TILE; r++) m &= m - 1;
-      if (hl == 0) nvis += nmine;
+      const int i1 = __ffs(m) - 1;
+      m &= m - 1;
+      const int i2 = m ? __ffs(m) - 1 : -1;
+      m &= m - 1;
+      const int n1 = __shfl_sync(RGPU_FULL, tn, i1);
+      const int n2s = __shfl_sync(RGPU_FULL, tn, i2 >= 0 ? i2 : 0);
+      const int n2 = i2 >= 0 ? n2s : 0;
+      nvis += n1 + n2;
+      const int mine = half ? i2 : i1, nmine = half ? n2 : n1;
       int4 f = make_int4(0, 0, 0, 0);
       if (hl < nmine) f = fw[(tb + mine) * RGPU_TILE + hl];
       const float dx = __int2float_rn(f.x - b.xi) * sx;
@@ -397,7 +388,7 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
   const double qa = S.mol_q[b.atom] * S.coulomb;
   const bool charged = S.fw_charged && qa != 0.0;
   const double alpha = S.alpha;
-  if (lane == 0) nvis += hi - lo;   /* reduced over the warp's lanes */
+  nvis += hi - lo;
   for (int s = 0; s < S.nseg; s++) {
     int a0 = max(lo, S.seg_start[s]), a1 = min(hi, S.seg_start[s + 1]);
     if (a0 >= a1) continue;
@@ -428,21 +419,13 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
   }
 }
 
-/* adsorbate molecules whose atom 0 lies in atoms [lo, hi) of the records,
- * for bead b, FP32 path (warp-wide). Each molecule is tested once, by its
- * atom 0 against the cut-off widened by the molecule's reach (min-image
- * distances obey the triangle inequality with the unwrapped intramolecular
- * distance, so a molecule that fails has no atom inside the cut-off); the
- * atoms of the molecules that pass are then spread over the lanes and
- * queued. Every molecule belongs to the one chunk holding its atom 0. */
 __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo,
-                                               int hi, int exclude, bool check, rgpu_acc &av, rgpu_acc &ac, int &ov,
+                                               int hi, int exclude, bool check, float &av, float &ac, int &ov,
                                                int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
 {
   const int lane = threadIdx.x & 31;
   const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
-  const float rc2 = S.rc2f, cull2 = S.ads_cull2f;
-  const int na = S.natom;
+  const float rc2 = S.rc2f;
   PairQueue Q;
   Q.r2 = qr2; Q.q = qq; Q.t = qt; Q.n = 0;
   Q.P = S.ljf_bb[b.atom];
@@ -451,38 +434,25 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
   Q.check = check;
   Q.alpha = S.alphaf;
   Q.thr = (float)S.overlap;
-  const int m0 = (lo + na - 1) / na, m1 = (hi + na - 1) / na;
-  for (int mb = m0; mb < m1; mb += 32) {
-    const int mj = mb + lane;
-    bool pass = false;
-    if (mj < m1 && mj != exclude) {
-      const int4 f = ads[mj * na];
-      const float dx = __int2float_rn(f.x - b.xi) * sx;
-      const float dy = __int2float_rn(f.y - b.yi) * sy;
-      const float dz = __int2float_rn(f.z - b.zi) * sz;
-      pass = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < cull2;
-    }
-    const unsigned mask = __ballot_sync(RGPU_FULL, pass);
-    const int cnt = __popc(mask) * na;
-    if (lane == 0) nvis += cnt;
-    for (int base = 0; base < cnt; base += 32) {
-      const int fl = base + lane;
-      bool in = false;
-      float r2 = 0.0f, q = 0.0f;
-      int at = 0;
-      if (fl < cnt) {
-        const int k = fl / na, a = fl - k * na;
-        const int4 g = ads[(mb + (int)__fns(mask, 0, k + 1)) * na + a];
-        at = g.w & 15;
-        const float dx = __int2float_rn(g.x - b.xi) * sx;
-        const float dy = __int2float_rn(g.y - b.yi) * sy;
-        const float dz = __int2float_rn(g.z - b.zi) * sz;
+  nvis += hi - lo;
+  for (int jb = lo; jb < hi; jb += 32) {
+    const int j = jb + lane;
+    bool in = false;
+    float r2 = 0.0f, q = 0.0f;
+    int at = 0;
+    if (j < hi) {
+      const int4 f = ads[j];
+      if ((f.w >> 4) != exclude) {
+        at = f.w & 15;
+        const float dx = __int2float_rn(f.x - b.xi) * sx;
+        const float dy = __int2float_rn(f.y - b.yi) * sy;
+        const float dz = __int2float_rn(f.z - b.zi) * sz;
         r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         in = r2 < rc2;
         q = S.mol_qf[at];
       }
-      queue_add(Q, in, r2, q, at, av, ac, ov, nin, nch);
     }
+    queue_add(Q, in, r2, q, at, av, ac, ov, nin, nch);
   }
   queue_drain(Q, av, ac, ov, nin, nch);
 }
@@ -498,7 +468,7 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
   const double qa = S.mol_q[b.atom] * S.coulomb;
   const bool charged = S.mol_charged && qa != 0.0;
   const double alpha = S.alpha;
-  if (lane == 0) nvis += hi - lo;   /* reduced over the warp's lanes */
+  nvis += hi - lo;
   for (int j = lo + lane; j < hi; j += 32) {
     AdsRec64 f = ads[j];
     int tag = (int)f.tag;
@@ -589,7 +559,7 @@ __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice
       hi = sl.ads_lo + (int)((unsigned)(nads * (cc + 1)) / (unsigned)pl.ca);
     }
     if (MIXED) {
-      rgpu_acc av = 0.0f, ac = 0.0f;
+      float av = 0.0f, ac = 0.0f;
       if (c < pl.cf)
         unit_tiles_mixed(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
                          sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
@@ -618,7 +588,6 @@ __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice
   if (sc.cnt) {
     nin = __reduce_add_sync(RGPU_FULL, (unsigned)nin);
     nch = __reduce_add_sync(RGPU_FULL, (unsigned)nch);
-    nvis = __reduce_add_sync(RGPU_FULL, (unsigned)nvis);
     if (lane == 0) {
       atomicAdd(&sc.cnt[0], (unsigned long long)nvis);
       atomicAdd(&sc.cnt[1], (unsigned long long)nin);

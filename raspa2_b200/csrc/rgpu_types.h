@@ -24,9 +24,7 @@
 #define RGPU_MAX_TRIALS 16     /* CBMC trial positions per step */
 #define RGPU_MAX_POS 64        /* bead positions evaluated in one batch */
 #define RGPU_MAX_TORS 128      /* torsion candidates per chain trial (chain_scheme 0; the reference default is 100) */
-#ifndef RGPU_TILE
 #define RGPU_TILE 16           /* framework atoms per tile (mixed-precision layout) */
-#endif
 
 /* per-system counters */
 enum {
@@ -134,9 +132,6 @@ typedef struct RgpuSys {
   int mol_charged;
   double mol_q[RGPU_MAX_ATOMS];
   float mol_qf[RGPU_MAX_ATOMS];
-  float ads_cull2f;           /* (cut-off + largest distance of an atom from atom 0 of its molecule)^2:
-                               * a molecule whose atom 0 is farther has no atom inside the cut-off */
-  int pad_cull;
   double mol_ref[RGPU_MAX_ATOMS][3];
   RgpuLJ lj_bf[RGPU_MAX_ATOMS][RGPU_MAX_FWTYPES];   /* bead atom x framework segment */
   RgpuLJ lj_bb[RGPU_MAX_ATOMS][RGPU_MAX_ATOMS];     /* bead atom x bead atom */
