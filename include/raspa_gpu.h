@@ -31,6 +31,7 @@ extern "C" {
 #define RGPU_E_CUDA -2         /* a CUDA runtime call failed (see rgpu_error_string) */
 #define RGPU_E_NODEVICE -3     /* no CUDA device */
 #define RGPU_E_CAPACITY -4     /* molecule capacity of the system exceeded */
+#define RGPU_E_IO -5           /* a file could not be opened, read or written, or is not a grid file */
 
 /* precision of a call */
 #define RGPU_FP64 0            /* FP64 throughout (the reference's REAL) */
@@ -196,6 +197,50 @@ int rgpu_grid_build_coulomb(rgpu_system *sys, const int npts[3], const double si
 int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3], const double shift[3],
                           const double cell[3], int n, const double *xyz, double *out);
 
+/* ---- grid files --------------------------------------------------------- */
+/* The reference's grid files: WriteVDWGrid / ReadVDWGrid (src/grids.c:692-813)
+ * and WriteCoulombGrid / ReadCoulombGrid (:815-977). A file is the header
+ * below, in the fields' native binary form and this order (REAL = double,
+ * INT_VECTOR3 = 3 ints, VECTOR = 3 doubles; 128 bytes, 136 with the Coulomb
+ * file's Ewald precision), then the 8 values of every grid point as 8 planes
+ * of (npts[0]+1)(npts[1]+1)(npts[2]+1) floats, [m][i][j][k]. On the device a
+ * grid is point-major ([i][j][k][m], the layout of rgpu_grid_build); the
+ * calls below transpose between the two on the GPU. */
+typedef struct rgpu_grid_file_header {
+  double spacing;       /* SpacingVDWGrid / SpacingCoulombGrid */
+  int npts[3];          /* NumberOfVDWGridPoints / NumberOfCoulombGridPoints */
+  double size[3];       /* SizeGrid */
+  double shift[3];      /* ShiftGrid */
+  double delta[3];      /* DeltaVDWGrid / DeltaCoulombGrid */
+  double unit_cell[3];  /* UnitCellSize */
+  int unit_cells[3];    /* NumberOfUnitCells */
+  double ewald_precision; /* EwaldPrecision: Coulomb files only */
+} rgpu_grid_file_header;
+/* Reads the header of the grid file at `path` (coulomb = 1 for a Coulomb
+ * grid file) and checks that the file holds exactly the grid it announces;
+ * RGPU_E_IO otherwise. */
+int rgpu_grid_read_file_header(const char *path, int coulomb, rgpu_grid_file_header *hdr);
+/* Reads the grid file into d_grid (device, 16-byte aligned, capacity in
+ * floats >= 8 (npts+1)^3) in the device layout, and its header into hdr.
+ * The caller checks hdr->unit_cell (and, for a Coulomb grid,
+ * hdr->unit_cells) against the system, as ReadVDWGrid and ReadCoulombGrid
+ * do (src/grids.c:787-792, :936-949). Uses a temporary device buffer of the
+ * grid's size; returns when the grid is in place. */
+int rgpu_grid_read_file(const char *path, int coulomb, rgpu_grid_file_header *hdr, float *d_grid, size_t capacity);
+/* Writes the device grid d_grid (npts from hdr) with header hdr to `path`
+ * in the reference's format, creating missing parent directories (mode
+ * 0700, as WriteVDWGrid's mkdir calls). */
+int rgpu_grid_write_file(const char *path, int coulomb, const rgpu_grid_file_header *hdr, const float *d_grid);
+/* The path the reference gives a grid file, written into buf (size n):
+ * <raspa_dir>/share/raspa/grids/<forcefield>/<framework>/<spacing %lf>/ then
+ * <framework>_<pseudo_atom>_<shifted|truncated>.grid for a VDW grid
+ * (src/grids.c:716-723), or, when pseudo_atom is NULL, the Coulomb grid's
+ * <ncx>x<ncy>x<ncz>/<framework>_Electrostatics_<method>.grid with method
+ * "Ewald" (:841-853; unit_cells required then). RGPU_E_INVALID when buf is
+ * too small. */
+int rgpu_grid_file_path(char *buf, size_t n, const char *raspa_dir, const char *forcefield, const char *framework,
+                        double spacing, const char *pseudo_atom, int shifted, const int unit_cells[3]);
+
 /* ---- grid lookup without device allocation ------------------------------ */
 /* No counterpart in the reference. Same result as rgpu_grid_interpolate for
  * n <= RGPU_NOALLOC_MAX_POINTS points, but the call makes no device
@@ -220,9 +265,11 @@ int rgpu_grid_interpolate_noalloc(const float *d_grid, const int npts[3], const 
  * of the pair sum over the framework, as the reference does with
  * UseTabularGrid (src/grids.c:979, called from src/framework_energy.c).
  * npts/size/shift/cell as rgpu_grid_interpolate; a charged molecule needs a
- * Coulomb grid (rgpu_system_set_coulomb_grid) set first. d_grids = NULL switches the grids off. Takes effect for
- * engines created afterwards; rgpu_bead_energies and rgpu_total_energy
- * keep the direct pair sums. */
+ * Coulomb grid (rgpu_system_set_coulomb_grid) set first. d_grids = NULL switches the grids off (and sets the
+ * FULL framework model below). Takes effect for engines created afterwards;
+ * the per-call energies (rgpu_bead_energies, rgpu_move_energy_difference,
+ * rgpu_total_energy) keep the direct pair sums unless the framework model is
+ * RGPU_FRAMEWORK_GRID. */
 int rgpu_system_set_grids(rgpu_system *sys, const float *const *d_grids, const int npts[3], const double size[3],
                           const double shift[3], const double cell[3]);
 /* The Coulomb grid of the engine (a grid of rgpu_grid_build_coulomb): the
@@ -234,6 +281,27 @@ int rgpu_system_set_grids(rgpu_system *sys, const float *const *d_grids, const i
  * are on). */
 int rgpu_system_set_coulomb_grid(rgpu_system *sys, const float *d_grid, const int npts[3], const double size[3],
                                  const double shift[3], const double cell[3]);
+
+/* ---- framework model of the per-call energies --------------------------- */
+/* Framework[].FrameworkModel (src/framework.h) for the per-call routines:
+ * RGPU_FRAMEWORK_FULL (the default) sums the framework pairs;
+ * RGPU_FRAMEWORK_GRID takes the framework terms from the grids set with
+ * rgpu_system_set_grids / rgpu_system_set_coulomb_grid, as the reference
+ * does when the model is GRID: the framework VDW energy of a bead of
+ * molecule atom a is the lookup in atom a's grid
+ * (CalculateFrameworkVDWEnergyAtPosition, src/framework_energy.c:73-77), its
+ * real-space charge energy the bead charge times the Coulomb-grid lookup
+ * (CalculateFrameworkChargeEnergyAtPosition, :195-198), and the same in the
+ * move differences (:4893-4894, :5437-5438) and the totals (:2707, :2920).
+ * rgpu_bead_energies, rgpu_move_energy_difference and rgpu_total_energy
+ * follow the model; the engine uses the grids whenever they are set. A grid
+ * value raises no overlap flag in rgpu_move_energy_difference (the
+ * reference's grid branch sets none; a capped lookup returns 1e8, which the
+ * acceptance rule rejects). GRID without grids set, or an unknown model,
+ * returns RGPU_E_INVALID. */
+#define RGPU_FRAMEWORK_FULL 0
+#define RGPU_FRAMEWORK_GRID 1
+int rgpu_system_set_framework_model(rgpu_system *sys, int model);
 
 /* ---- persistent batched engine ------------------------------------------ */
 /* Groups systems for one persistent launch; each system is advanced by one

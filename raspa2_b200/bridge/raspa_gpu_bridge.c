@@ -35,9 +35,14 @@
  * flexible chain's external energies as well), one rigid framework, an
  * orthorhombic box without replicas or cell lists, Lennard-Jones (or zero)
  * potentials, charges by the Ewald method with one cut-off, no CFCMC
- * scaling, no energy grids. Anything else stops the program with a message,
- * as the reference's own fatal paths do (fprintf, exit); no routine falls
- * back to the CPU.
+ * scaling. With the GRID framework model (UseTabularGrid) the grid files
+ * the reference read at start-up (the VDW grid of every adsorbate
+ * pseudo-atom, and the Coulomb grid for a charged adsorbate) are read once
+ * more, by the library's reader, into device memory, and the per-call
+ * routines take the framework terms from them
+ * (rgpu_system_set_framework_model). Anything else stops the
+ * program with a message, as the reference's own fatal paths do (fprintf,
+ * exit); no routine falls back to the CPU.
  *
  * Environment: RASPA_GPU_PRECISION=mixed selects the mixed-precision path
  * (default FP64); RASPA_GPU_BRIDGE_STATS=1 prints the number of device
@@ -56,6 +61,10 @@
 #include "ewald.h"
 #include "cbmc.h"
 #include "mc_moves.h"
+
+#include "grids.h"
+
+#include <cuda_runtime_api.h>
 
 #include "raspa_gpu.h"
 
@@ -84,6 +93,64 @@ static void print_stats(void)
           g_calls[0], g_calls[1], g_calls[2], g_calls[3]);
 }
 
+/* a grid file of the reference (the one ReadVDWGrid / ReadCoulombGrid read
+ * before the first call) into a new device buffer, through the library's
+ * reader; the header must match the grid the reference holds */
+static float *bridge_read_grid(const char *pseudo_atom, int coulomb, int s, rgpu_grid_file_header *h)
+{
+  char path[4096];
+  const int nc[3] = {NumberOfUnitCells[s].x, NumberOfUnitCells[s].y, NumberOfUnitCells[s].z};
+  int rc = rgpu_grid_file_path(path, sizeof path, RASPA_DIRECTORY, ForceField, Framework[s].Name[0],
+                               coulomb ? SpacingCoulombGrid : SpacingVDWGrid, coulomb ? NULL : pseudo_atom,
+                               ShiftPotentials, nc);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_file_path", rc);
+  rc = rgpu_grid_read_file_header(path, coulomb, h);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_read_file_header", rc);
+  if (fabs(h->unit_cell[0] - UnitCellSize[s].x) > 1e-8 || fabs(h->unit_cell[1] - UnitCellSize[s].y) > 1e-8 ||
+      fabs(h->unit_cell[2] - UnitCellSize[s].z) > 1e-8)
+    bridge_fail("grid file: unit-cell size does not match", 0);
+  if (!coulomb && (h->npts[0] != NumberOfVDWGridPoints.x || h->npts[1] != NumberOfVDWGridPoints.y ||
+                   h->npts[2] != NumberOfVDWGridPoints.z))
+    bridge_fail("grid file: number of grid points does not match the reference's grid", 0);
+  const size_t n = (size_t)8 * (h->npts[0] + 1) * (h->npts[1] + 1) * (h->npts[2] + 1);
+  float *d = NULL;
+  if (cudaMalloc((void **)&d, sizeof(float) * n) != cudaSuccess) bridge_fail("cudaMalloc of a grid", 0);
+  rc = rgpu_grid_read_file(path, coulomb, h, d, n);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_read_file", rc);
+  return d;
+}
+
+/* the GRID framework model (src/framework_energy.c:73-77, :195-198): every
+ * adsorbate pseudo-atom needs its VDW grid, a charged adsorbate the Coulomb
+ * grid; the device grids live until the program exits */
+static void bridge_grids(const COMPONENT *C, int s)
+{
+  const float *ptr[64];
+  float *by_type[BRIDGE_MAXTYPES];
+  memset(by_type, 0, sizeof by_type);
+  rgpu_grid_file_header h;
+  int charged = 0;
+  for (int a = 0; a < C->NumberOfAtoms; a++) {
+    const int t = C->Type[a];
+    if (!VDWGrid || !VDWGrid[t]) bridge_fail("the GRID framework model needs a VDW grid of every adsorbate atom", 0);
+    if (!by_type[t]) by_type[t] = bridge_read_grid(PseudoAtoms[t].Name, 0, s, &h);
+    ptr[a] = by_type[t];
+    charged |= C->Charge[a] != 0.0;
+  }
+  int rc;
+  if (charged && ChargeMethod == EWALD) {
+    if (!CoulombGrid) bridge_fail("the GRID framework model of a charged adsorbate needs the Coulomb grid", 0);
+    rgpu_grid_file_header hc;
+    float *dc = bridge_read_grid(NULL, 1, s, &hc);
+    rc = rgpu_system_set_coulomb_grid(g_sys, dc, hc.npts, hc.size, hc.shift, hc.unit_cell);
+    if (rc != RGPU_SUCCESS) bridge_fail("rgpu_system_set_coulomb_grid", rc);
+  }
+  rc = rgpu_system_set_grids(g_sys, ptr, h.npts, h.size, h.shift, h.unit_cell);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_system_set_grids", rc);
+  rc = rgpu_system_set_framework_model(g_sys, RGPU_FRAMEWORK_GRID);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_system_set_framework_model", rc);
+}
+
 /* the GPU system from the reference's globals (src/input.c, src/ewald.c:200-261) */
 static void bridge_init(void)
 {
@@ -95,9 +162,8 @@ static void bridge_init(void)
   if (NumberOfSystems != 1) bridge_fail("only one system is supported", 0);
   if (NumberOfComponents != 1 || Components[0].ExtraFrameworkMolecule)
     bridge_fail("only one adsorbate component is supported", 0);
-  if (Framework[s].FrameworkModel == NONE || Framework[s].FrameworkModel == GRID ||
-      Framework[s].NumberOfFrameworks != 1)
-    bridge_fail("only one rigid framework of atoms is supported (no grids)", 0);
+  if (Framework[s].FrameworkModel == NONE || Framework[s].NumberOfFrameworks != 1)
+    bridge_fail("only one rigid framework is supported", 0);
   if (UseReplicas[s] || UseCellLists[s]) bridge_fail("replica cells and cell lists are not supported", 0);
   const REAL_MATRIX3x3 B = Box[s];
   if (fabs(B.bx) + fabs(B.cx) + fabs(B.ay) + fabs(B.cy) + fabs(B.az) + fabs(B.bz) > 1e-8 * (B.ax + B.by + B.cz))
@@ -181,6 +247,7 @@ static void bridge_init(void)
   d.ntrial_first = d.ntrial = 1;
   const int rc = rgpu_system_create(&g_sys, &d);
   if (rc != RGPU_SUCCESS) bridge_fail("rgpu_system_create", rc);
+  if (Framework[s].FrameworkModel == GRID) bridge_grids(C, s);
   free(eps);
   free(sig2);
   free(shift);

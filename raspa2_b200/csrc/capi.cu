@@ -7,13 +7,16 @@
  * function exits the process; errors are returned as codes.
  */
 #include <cuda_runtime.h>
+#include <errno.h>
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
 
 #include <algorithm>
+#include <string>
 #include <mutex>
 #include <vector>
 
@@ -86,6 +89,7 @@ struct rgpu_system {
   int records_stale;          /* device records must be rebuilt from ads_xyz */
   double net_ads, pending_dq;
   int grid_type_seg;
+  int fw_model;               /* RGPU_FRAMEWORK_FULL or _GRID: the per-call energies' framework terms */
   uint64_t fingerprint;       /* of the model a checkpoint must match (checkpoint_fingerprint) */
   std::vector<int> fw_seg_type; /* framework pseudo-atom type of each segment */
   std::vector<double> lj_eps, lj_sig2, lj_shift;
@@ -786,7 +790,7 @@ static int bead_batch(rgpu_system *s, int precision, int n, const double *xyz, c
   const int mixed = precision == RGPU_MIXED;
   const void *ads = mixed ? (const void *)s->rec32 : (const void *)s->rec64;
   CK(rgpu_point_energies_launch(mixed, s->d_sys, ads, s->h_nmol * s->d.natom, s->io_xyz, s->io_atom, s->io_excl, n,
-                                pair_check, s->io_out, s->io_ov, s->st));
+                                pair_check, s->fw_model == RGPU_FRAMEWORK_GRID, s->io_out, s->io_ov, s->st));
   CK(cudaMemcpyAsync(out, s->io_out, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s->st));
   if (ov) CK(cudaMemcpyAsync(ov, s->io_ov, sizeof(int) * n, cudaMemcpyDeviceToHost, s->st));
   CK(cudaStreamSynchronize(s->st));
@@ -962,6 +966,7 @@ extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids
   RgpuSys &h = s->h;
   if (!d_grids) {
     h.use_grid = 0;
+    s->fw_model = RGPU_FRAMEWORK_FULL;
     for (int a = 0; a < RGPU_MAX_ATOMS; a++) h.grid[a] = nullptr;
   } else {
     if (!npts || !size || !shift || !cell) return fail(RGPU_E_INVALID, "bad argument");
@@ -983,6 +988,17 @@ extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids
   }
   CK(cudaMemcpyAsync(s->d_sys, &h, sizeof(RgpuSys), cudaMemcpyHostToDevice, s->st));
   CK(cudaStreamSynchronize(s->st));
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_system_set_framework_model(rgpu_system *s, int model)
+{
+  if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  if (model != RGPU_FRAMEWORK_FULL && model != RGPU_FRAMEWORK_GRID)
+    return fail(RGPU_E_INVALID, "framework model %d", model);
+  if (model == RGPU_FRAMEWORK_GRID && !s->h.use_grid)
+    return fail(RGPU_E_INVALID, "the GRID framework model needs the system's grids (rgpu_system_set_grids)");
+  s->fw_model = model;
   return RGPU_SUCCESS;
 }
 
@@ -1100,6 +1116,172 @@ static bool grid_covers_cell(const int npts[3], const double size[3], const doub
     if (shift[c] > 1e-9 * cell[c] || shift[c] + size[c] < cell[c] * (1.0 - 1e-9)) return false;
   }
   return true;
+}
+
+/* ---------------------------------------------------------------------- */
+/* grid files (src/grids.c:692-977) */
+
+static const size_t GRID_HDR_BYTES = 8 + 12 + 4 * 24 + 12;   /* the Coulomb file adds 8 */
+
+static long long grid_points(const int npts[3])
+{
+  return (long long)(npts[0] + 1) * (npts[1] + 1) * (npts[2] + 1);
+}
+
+static void hdr_pack(const rgpu_grid_file_header *h, int coulomb, unsigned char *b)
+{
+  size_t o = 0;
+  auto put = [&](const void *p, size_t n) { memcpy(b + o, p, n); o += n; };
+  put(&h->spacing, 8);
+  put(h->npts, 12);
+  put(h->size, 24);
+  put(h->shift, 24);
+  put(h->delta, 24);
+  put(h->unit_cell, 24);
+  put(h->unit_cells, 12);
+  if (coulomb) put(&h->ewald_precision, 8);
+}
+
+static void hdr_unpack(const unsigned char *b, int coulomb, rgpu_grid_file_header *h)
+{
+  size_t o = 0;
+  auto get = [&](void *p, size_t n) { memcpy(p, b + o, n); o += n; };
+  memset(h, 0, sizeof *h);
+  get(&h->spacing, 8);
+  get(h->npts, 12);
+  get(h->size, 24);
+  get(h->shift, 24);
+  get(h->delta, 24);
+  get(h->unit_cell, 24);
+  get(h->unit_cells, 12);
+  if (coulomb) get(&h->ewald_precision, 8);
+}
+
+/* opens `path`, reads and checks its header; on success the file is left
+ * positioned at the first plane */
+static int grid_file_open(const char *path, int coulomb, rgpu_grid_file_header *h, FILE **out)
+{
+  if (!path || !h) return fail(RGPU_E_INVALID, "bad argument");
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(RGPU_E_IO, "cannot open grid file %s", path);
+  const size_t hb = GRID_HDR_BYTES + (coulomb ? 8 : 0);
+  unsigned char b[GRID_HDR_BYTES + 8];
+  if (fread(b, 1, hb, f) != hb) {
+    fclose(f);
+    return fail(RGPU_E_IO, "%s: short header", path);
+  }
+  hdr_unpack(b, coulomb, h);
+  for (int c = 0; c < 3; c++)
+    if (h->npts[c] < 1 || h->npts[c] > (1 << 16)) {
+      fclose(f);
+      return fail(RGPU_E_IO, "%s: not a grid file (grid points %d)", path, h->npts[c]);
+    }
+  struct stat st;
+  const long long want = (long long)hb + 32LL * grid_points(h->npts);
+  if (fstat(fileno(f), &st) || (long long)st.st_size != want) {
+    fclose(f);
+    return fail(RGPU_E_IO, "%s: %lld bytes, the header announces %lld", path, (long long)st.st_size, want);
+  }
+  *out = f;
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_grid_read_file_header(const char *path, int coulomb, rgpu_grid_file_header *hdr)
+{
+  FILE *f = nullptr;
+  int rc = grid_file_open(path, coulomb, hdr, &f);
+  if (rc) return rc;
+  fclose(f);
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_grid_read_file(const char *path, int coulomb, rgpu_grid_file_header *hdr, float *d_grid,
+                                   size_t capacity)
+{
+  if (!d_grid || (uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be a 16-byte aligned device pointer");
+  FILE *f = nullptr;
+  int rc = grid_file_open(path, coulomb, hdr, &f);
+  if (rc) return rc;
+  const long long npt = grid_points(hdr->npts);
+  if ((unsigned long long)capacity < 8ULL * npt) {
+    fclose(f);
+    return fail(RGPU_E_INVALID, "d_grid holds %zu floats, the grid %lld", capacity, 8LL * npt);
+  }
+  const size_t bytes = sizeof(float) * 8 * (size_t)npt;
+  std::vector<float> host((size_t)8 * npt);
+  const size_t got = fread(host.data(), 1, bytes, f);
+  fclose(f);
+  if (got != bytes) return fail(RGPU_E_IO, "%s: short read", path);
+  float *planes = nullptr;
+  CK(cudaMalloc((void **)&planes, bytes));
+  cudaStream_t st = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (!e) e = cudaMemcpyAsync(planes, host.data(), bytes, cudaMemcpyHostToDevice, st);
+  if (!e) e = rgpu_grid_planes_to_points_launch(planes, npt, d_grid, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (st) cudaStreamDestroy(st);
+  cudaFree(planes);
+  if (e) return fail(RGPU_E_CUDA, "grid file upload: %s", cudaGetErrorString(e));
+  return RGPU_SUCCESS;
+}
+
+/* mkdir -p of the directory part of path (mode 0700) */
+static int make_parents(const char *path)
+{
+  std::string p(path);
+  for (size_t i = 1; i < p.size(); i++) {
+    if (p[i] != '/') continue;
+    const std::string d = p.substr(0, i);
+    if (mkdir(d.c_str(), S_IRWXU) && errno != EEXIST) return -1;
+  }
+  return 0;
+}
+
+extern "C" int rgpu_grid_write_file(const char *path, int coulomb, const rgpu_grid_file_header *hdr,
+                                    const float *d_grid)
+{
+  if (!path || !hdr || !d_grid || (uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "bad argument");
+  for (int c = 0; c < 3; c++)
+    if (hdr->npts[c] < 1) return fail(RGPU_E_INVALID, "grid points %d", hdr->npts[c]);
+  const long long npt = grid_points(hdr->npts);
+  const size_t bytes = sizeof(float) * 8 * (size_t)npt;
+  std::vector<float> host((size_t)8 * npt);
+  float *planes = nullptr;
+  CK(cudaMalloc((void **)&planes, bytes));
+  cudaStream_t st = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (!e) e = rgpu_grid_points_to_planes_launch(d_grid, npt, planes, st);
+  if (!e) e = cudaMemcpyAsync(host.data(), planes, bytes, cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (st) cudaStreamDestroy(st);
+  cudaFree(planes);
+  if (e) return fail(RGPU_E_CUDA, "grid file download: %s", cudaGetErrorString(e));
+  if (make_parents(path)) return fail(RGPU_E_IO, "cannot create the directories of %s", path);
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(RGPU_E_IO, "cannot create grid file %s", path);
+  unsigned char b[GRID_HDR_BYTES + 8];
+  hdr_pack(hdr, coulomb, b);
+  const size_t hb = GRID_HDR_BYTES + (coulomb ? 8 : 0);
+  const bool ok = fwrite(b, 1, hb, f) == hb && fwrite(host.data(), 1, bytes, f) == bytes;
+  if (fclose(f) || !ok) return fail(RGPU_E_IO, "%s: write failed", path);
+  return RGPU_SUCCESS;
+}
+
+extern "C" int rgpu_grid_file_path(char *buf, size_t n, const char *raspa_dir, const char *forcefield,
+                                   const char *framework, double spacing, const char *pseudo_atom, int shifted,
+                                   const int unit_cells[3])
+{
+  if (!buf || !raspa_dir || !forcefield || !framework || (!pseudo_atom && !unit_cells))
+    return fail(RGPU_E_INVALID, "bad argument");
+  int w;
+  if (pseudo_atom)
+    w = snprintf(buf, n, "%s/share/raspa/grids/%s/%s/%lf/%s_%s_%s.grid", raspa_dir, forcefield, framework, spacing,
+                 framework, pseudo_atom, shifted ? "shifted" : "truncated");
+  else
+    w = snprintf(buf, n, "%s/share/raspa/grids/%s/%s/%lf/%dx%dx%d/%s_Electrostatics_Ewald.grid", raspa_dir,
+                 forcefield, framework, spacing, unit_cells[0], unit_cells[1], unit_cells[2], framework);
+  if (w < 0 || (size_t)w >= n) return fail(RGPU_E_INVALID, "path buffer of %zu bytes is too small", n);
+  return RGPU_SUCCESS;
 }
 
 extern "C" int rgpu_grid_interpolate(const float *d_grid, const int npts[3], const double size[3],
@@ -1313,8 +1495,15 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
     delete e;
     return fail(RGPU_E_CUDA, "cudaMalloc engine");
   }
-  e->st = e->sys[0]->st;
+  /* the engine's own stream: a system may be replaced and destroyed while
+   * the engine lives (rgpu_engine_replace_system) */
+  if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(e->d_systems);
+    delete e;
+    return fail(RGPU_E_CUDA, "cudaStreamCreate engine");
+  }
   if (upload_slots(e) != cudaSuccess) {
+    cudaStreamDestroy(e->st);
     cudaFree(e->d_systems);
     delete e;
     return fail(RGPU_E_CUDA, "upload engine");
@@ -1337,6 +1526,10 @@ extern "C" int rgpu_engine_destroy(rgpu_engine *e)
     if (ev) cudaEventDestroy(ev);
   if (e->h_slots) cudaFreeHost(e->h_slots);
   cudaFree(e->d_systems);
+  if (e->st) {
+    cudaStreamSynchronize(e->st);
+    cudaStreamDestroy(e->st);
+  }
   delete e;
   return RGPU_SUCCESS;
 }

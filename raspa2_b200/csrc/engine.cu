@@ -1886,11 +1886,21 @@ struct CallSmem {
 
 
 /* Energies of P bead positions (P <= RGPU_MAX_POS), given as FP64 xyz with
- * the molecule-atom index of each bead. out[p*4 + k], ov[p]. */
+ * the molecule-atom index of each bead. out[p*4 + k], ov[p].
+ *
+ * fw_grid (the GRID framework model, with the system's grids set): the
+ * framework VDW energy of a bead is its atom's energy-grid value and the
+ * framework real-space charge energy its charge times the Coulomb-grid value
+ * (zero without a Coulomb grid: an uncharged molecule), with no framework
+ * pairs, as CalculateFrameworkVDWEnergyAtPosition and
+ * CalculateFrameworkChargeEnergyAtPosition do when the model is GRID
+ * (src/framework_energy.c:73-77, :195-198) and the move differences
+ * (:4893-4894, :5437-5438). A grid value sets no overlap flag: the
+ * reference's grid branches set none. */
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, const void *ads, int nads,
                                                         const double *xyz, const int *atom, const int *excl, int P,
-                                                        int pair_check, double *out, int *ov)
+                                                        int pair_check, int fw_grid, double *out, int *ov)
 {
   __shared__ RgpuSys S;
   __shared__ CallSmem sm;
@@ -1903,11 +1913,32 @@ __global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, con
   sl.fw = MIXED ? (const void *)S.fw32 : (const void *)S.fw64;
   sl.tiles = S.tiles;
   sl.fw_lo = 0;
-  sl.fw_hi = MIXED ? S.ntile : S.nfw;
+  sl.fw_hi = (fw_grid && S.use_grid) ? 0 : (MIXED ? S.ntile : S.nfw);
   sl.ads = ads;
   sl.ads_lo = 0;
   sl.ads_hi = nads;
   eval_positions<MIXED>(S, sl, sm.pos, P, pair_check, sm.res, sm.ovf, sc, RGPU_MAX_UNITS);
+  if (fw_grid && S.use_grid) {
+    /* 8 lanes per lookup, 4 positions per warp pass (every lane takes part) */
+    const int lane = threadIdx.x & 31;
+    for (int base = (threadIdx.x >> 5) * 4; base < P; base += (blockDim.x >> 5) * 4) {
+      const int p = base + (lane >> 3);
+      const bool live = p < P;
+      const int a = live ? atom[p] : 0;
+      const double x[3] = {live ? xyz[3 * p] : 0.0, live ? xyz[3 * p + 1] : 0.0, live ? xyz[3 * p + 2] : 0.0};
+      const double g = rgpu_grid_value8(S.grid[a], S.grid_geom, x, lane & 7, live);
+      double gq = 0.0;
+      if (S.use_coul_grid) {
+        const double q = S.mol_q[a];
+        gq = q * rgpu_grid_value8(S.coul_grid, S.coul_geom, x, lane & 7, live && q != 0.0, false);
+      }
+      if (live && (lane & 7) == 0) {
+        sm.res[p][0] = g;
+        sm.res[p][1] = gq;
+      }
+    }
+    __syncthreads();
+  }
   for (int p = threadIdx.x; p < P; p += blockDim.x) {
     for (int k = 0; k < 4; k++) out[4 * p + k] = sm.res[p][k];
     if (ov) ov[p] = sm.ovf[p];
@@ -1916,13 +1947,15 @@ __global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, con
 
 cudaError_t rgpu_point_energies_launch(int mixed, const RgpuSys *d_sys, const void *d_ads, int nads,
                                        const double *d_xyz, const int *d_atom, const int *d_excl, int P,
-                                       int pair_check, double *d_out, int *d_ov, cudaStream_t st)
+                                       int pair_check, int fw_grid, double *d_out, int *d_ov, cudaStream_t st)
 {
   if (P > RGPU_MAX_POS) return cudaErrorInvalidValue;
   if (mixed)
-    k_point_energies<true><<<1, 256, 0, st>>>(d_sys, d_ads, nads, d_xyz, d_atom, d_excl, P, pair_check, d_out, d_ov);
+    k_point_energies<true><<<1, 256, 0, st>>>(d_sys, d_ads, nads, d_xyz, d_atom, d_excl, P, pair_check, fw_grid,
+                                              d_out, d_ov);
   else
-    k_point_energies<false><<<1, 256, 0, st>>>(d_sys, d_ads, nads, d_xyz, d_atom, d_excl, P, pair_check, d_out, d_ov);
+    k_point_energies<false><<<1, 256, 0, st>>>(d_sys, d_ads, nads, d_xyz, d_atom, d_excl, P, pair_check, fw_grid,
+                                               d_out, d_ov);
   return cudaGetLastError();
 }
 

@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <algorithm>
+
 #include "rgpu_device.cuh"
 #include "rgpu_engine.h"
 #include "rgpu_grid.cuh"
@@ -227,5 +229,53 @@ cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], cons
   }
   if (n <= 0) return cudaSuccess;
   k_grid_interp<<<(n + 255) / 256, 256, 0, st>>>(d_grid, ip, n, d_xyz, d_out);
+  return cudaGetLastError();
+}
+
+/* Grid files store the 8 values as planes ([m][i][j][k], src/grids.c:734-738);
+ * the device layout is point-major (8 floats per point). One thread per
+ * point: the plane reads (or writes) of neighbouring threads are contiguous,
+ * and the point's 8 floats move as two 16-byte words. */
+__global__ void k_grid_planes_to_points(const float *__restrict__ planes, long long npt, float *__restrict__ points)
+{
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npt; p += (long long)gridDim.x * blockDim.x) {
+    float v[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) v[m] = planes[m * npt + p];
+    float4 *dst = (float4 *)(points + 8 * p);
+    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+}
+
+__global__ void k_grid_points_to_planes(const float *__restrict__ points, long long npt, float *__restrict__ planes)
+{
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npt; p += (long long)gridDim.x * blockDim.x) {
+    const float4 *src = (const float4 *)(points + 8 * p);
+    const float4 a = src[0], b = src[1];
+    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int m = 0; m < 8; m++) planes[m * npt + p] = v[m];
+  }
+}
+
+static unsigned transpose_blocks(long long npt)
+{
+  /* at most 8 CTAs of 256 per SM-count multiple: 148 SMs x 8 */
+  const long long want = (npt + 255) / 256;
+  return (unsigned)std::min<long long>(want, 148LL * 8);
+}
+
+cudaError_t rgpu_grid_planes_to_points_launch(const float *d_planes, long long npt, float *d_points, cudaStream_t st)
+{
+  if (npt <= 0) return cudaSuccess;
+  k_grid_planes_to_points<<<transpose_blocks(npt), 256, 0, st>>>(d_planes, npt, d_points);
+  return cudaGetLastError();
+}
+
+cudaError_t rgpu_grid_points_to_planes_launch(const float *d_points, long long npt, float *d_planes, cudaStream_t st)
+{
+  if (npt <= 0) return cudaSuccess;
+  k_grid_points_to_planes<<<transpose_blocks(npt), 256, 0, st>>>(d_points, npt, d_planes);
   return cudaGetLastError();
 }

@@ -21,7 +21,7 @@ cudaError_t rgpu_engine_launch(int mixed, RgpuSys *d_systems, int nsys, long lon
                                int threads, bool wide, bool flex, cudaStream_t st);
 cudaError_t rgpu_point_energies_launch(int mixed, const RgpuSys *d_sys, const void *d_ads, int nads,
                                        const double *d_xyz, const int *d_atom, const int *d_excl, int P,
-                                       int pair_check, double *d_out, int *d_ov, cudaStream_t st);
+                                       int pair_check, int fw_grid, double *d_out, int *d_ov, cudaStream_t st);
 cudaError_t rgpu_ewald_delta_launch(int mixed, const RgpuSys *d_sys, const double *d_xyz, const double *d_q, int ns,
                                     double2 *d_ds, double *d_out, int kw, cudaStream_t st);
 cudaError_t rgpu_ewald_accept_launch(const RgpuSys *d_sys, const double2 *d_ds, int nk, cudaStream_t st);
@@ -43,5 +43,8 @@ cudaError_t rgpu_grid_build_launch_coulomb(const RgpuSys *d_sys, const int npts[
 cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], const double size[3],
                                     const double shift[3], const double cell[3], int n, const double *d_xyz,
                                     double *d_out, cudaStream_t st);
+/* plane-major (grid file) <-> point-major (device) layout of npt grid points */
+cudaError_t rgpu_grid_planes_to_points_launch(const float *d_planes, long long npt, float *d_points, cudaStream_t st);
+cudaError_t rgpu_grid_points_to_planes_launch(const float *d_points, long long npt, float *d_planes, cudaStream_t st);
 
 #endif

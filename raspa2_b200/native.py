@@ -22,6 +22,8 @@ _ip = C.POINTER(C.c_int)
 RGPU_FP64 = 0
 RGPU_MIXED = 1
 RGPU_E_INVALID = -1   # include/raspa_gpu.h
+RGPU_FRAMEWORK_FULL = 0
+RGPU_FRAMEWORK_GRID = 1
 
 EXPORTS = [
     "rgpu_error_string", "rgpu_device_count", "rgpu_system_create", "rgpu_system_destroy",
@@ -34,7 +36,8 @@ EXPORTS = [
     "rgpu_system_reset_averages", "rgpu_engine_use_graph", "rgpu_engine_create_ex", "rgpu_engine_set_split", "rgpu_intra_energy",
     "rgpu_system_set_grids", "rgpu_system_checkpoint_size", "rgpu_system_checkpoint", "rgpu_system_restore",
     "rgpu_grid_build_coulomb", "rgpu_system_set_coulomb_grid", "rgpu_engine_get_state", "rgpu_engine_set_adsorbates",
-    "rgpu_engine_staging_bytes", "rgpu_engine_replace_system",
+    "rgpu_engine_staging_bytes", "rgpu_engine_replace_system", "rgpu_system_set_framework_model",
+    "rgpu_grid_read_file_header", "rgpu_grid_read_file", "rgpu_grid_write_file", "rgpu_grid_file_path",
 ]
 
 RGPU_NOALLOC_MAX_POINTS = 8192   # include/raspa_gpu.h
@@ -259,10 +262,18 @@ class GpuSystem:
         _check(L.rgpu_system_set_grids(self.h, arr, n.ctypes.data_as(_ip), s.ctypes.data_as(_dp),
                                        sh.ctypes.data_as(_dp), ce.ctypes.data_as(_dp)))
 
+    def set_framework_model(self, model: int):
+        """RGPU_FRAMEWORK_GRID: the per-call energies (bead_energies,
+        move_difference, total_energy) take the framework terms from the grids,
+        as the reference's GRID framework model; RGPU_FRAMEWORK_FULL (the
+        default) sums the framework pairs."""
+        _check(load().rgpu_system_set_framework_model(self.h, C.c_int(model)))
+
     def use_energy_grids(self, spacing: float, like: Optional["GpuSystem"] = None):
         """Builds one energy grid per pseudo-atom type of the molecule over the
-        (orthorhombic) unit cell, int(size / spacing) intervals per axis as
-        the reference's SpacingVDWGrid (src/grids.c:337-367), in device memory
+        (orthorhombic) unit cell, int(size / spacing) intervals per axis,
+        made odd, as MakeGrid counts them from SpacingVDWGrid
+        (src/grids.c:486-492), in device memory
         this object keeps, and switches the engine's host VDW energies to
         them. With `like` (a system of the same framework and molecule whose
         grids are built at this spacing) its grids are shared instead of
@@ -270,6 +281,7 @@ class GpuSystem:
         import torch
         uc = np.asarray(self.sysm.unit_cell, float)
         npts = (uc / spacing).astype(np.int32)
+        npts += npts % 2 == 0
         shift = np.zeros(3)
         n = int(np.prod(npts.astype(np.int64) + 1)) * 8
         types = [int(t) for t in self.sysm.molecule_types()]
@@ -289,8 +301,8 @@ class GpuSystem:
                 self.grid_build(t, npts, uc, shift, buf.data_ptr())
                 bufs[t] = buf
             if np.any(self.sysm.molecule.charges() != 0.0):
-                # the Coulomb grid: odd point counts (src/grids.c:588-594)
-                nc = npts + (npts % 2 == 0)
+                # the Coulomb grid: odd point counts as well (src/grids.c:588-594)
+                nc = npts.copy()
                 buf = torch.empty(int(np.prod(nc.astype(np.int64) + 1)) * 8, dtype=torch.float32, device="cuda")
                 torch.cuda.synchronize()
                 self.grid_build_coulomb(nc, uc, shift, buf.data_ptr())
@@ -418,6 +430,67 @@ def grid_interpolate_noalloc(d_grid_ptr: int, npts, size, shift, cell, xyz) -> n
                                                 ce.ctypes.data_as(_dp), C.c_int(len(x)), x.ctypes.data_as(_dp),
                                                 out.ctypes.data_as(_dp)))
     return out
+
+
+class GridFileHeader(C.Structure):
+    """rgpu_grid_file_header: the header of the reference's grid files
+    (src/grids.c:726-732; the Coulomb file adds the Ewald precision)."""
+    _fields_ = [("spacing", C.c_double), ("npts", C.c_int * 3), ("size", C.c_double * 3),
+                ("shift", C.c_double * 3), ("delta", C.c_double * 3), ("unit_cell", C.c_double * 3),
+                ("unit_cells", C.c_int * 3), ("ewald_precision", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"spacing": self.spacing, "n": list(self.npts), "size": list(self.size), "shift": list(self.shift),
+                "delta": list(self.delta), "cell": list(self.unit_cell), "ncell": list(self.unit_cells),
+                "ewald_precision": self.ewald_precision}
+
+    @classmethod
+    def of(cls, meta: dict) -> "GridFileHeader":
+        h = cls()
+        h.spacing = meta["spacing"]
+        h.npts[:] = [int(x) for x in meta["n"]]
+        h.size[:] = [float(x) for x in meta["size"]]
+        h.shift[:] = [float(x) for x in meta["shift"]]
+        h.delta[:] = [float(x) for x in meta["delta"]]
+        h.unit_cell[:] = [float(x) for x in meta["cell"]]
+        h.unit_cells[:] = [int(x) for x in meta["ncell"]]
+        h.ewald_precision = float(meta.get("ewald_precision", 0.0))
+        return h
+
+
+def grid_file_header(path: str, coulomb: bool = False) -> GridFileHeader:
+    """The header of a reference grid file (checked against the file size)."""
+    h = GridFileHeader()
+    _check(load().rgpu_grid_read_file_header(os.fsencode(path), C.c_int(int(coulomb)), C.byref(h)))
+    return h
+
+
+def grid_read_file(path: str, d_grid_ptr: int, capacity: int, coulomb: bool = False) -> GridFileHeader:
+    """Reads a reference grid file into device memory (point-major layout);
+    capacity in floats."""
+    h = GridFileHeader()
+    _check(load().rgpu_grid_read_file(os.fsencode(path), C.c_int(int(coulomb)), C.byref(h), C.c_void_p(d_grid_ptr),
+                                      C.c_size_t(capacity)))
+    return h
+
+
+def grid_write_file(path: str, header: GridFileHeader, d_grid_ptr: int, coulomb: bool = False):
+    """Writes a device grid to `path` in the reference's file format."""
+    _check(load().rgpu_grid_write_file(os.fsencode(path), C.c_int(int(coulomb)), C.byref(header),
+                                       C.c_void_p(d_grid_ptr)))
+
+
+def grid_file_path(raspa_dir: str, forcefield: str, framework: str, spacing: float,
+                   pseudo_atom: Optional[str] = None, shifted: bool = True, unit_cells=None) -> str:
+    """The reference's path of a VDW grid file (pseudo_atom given) or of the
+    Ewald Coulomb grid file (pseudo_atom None, unit_cells given)."""
+    buf = C.create_string_buffer(4096)
+    uc = None if unit_cells is None else (C.c_int * 3)(*[int(x) for x in unit_cells])
+    _check(load().rgpu_grid_file_path(buf, C.c_size_t(len(buf)), os.fsencode(raspa_dir), os.fsencode(forcefield),
+                                      os.fsencode(framework), C.c_double(spacing),
+                                      None if pseudo_atom is None else os.fsencode(pseudo_atom),
+                                      C.c_int(int(shifted)), uc))
+    return buf.value.decode()
 
 
 class Engine:

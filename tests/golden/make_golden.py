@@ -9,6 +9,7 @@ time needs the reference.
 
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py coulomb    # only grid_co2_coulomb.json
+    python tests/golden/make_golden.py gridfiles  # only grid_co2_files.json + grid_files/
 """
 from __future__ import annotations
 
@@ -286,9 +287,62 @@ def coulomb_grid_case(seed=1, spacing=1.0):
     }
 
 
+def grid_files_case(seed=1, spacing=2.0):
+    """The reference's own grid files of the CO2 framework at a coarse
+    spacing (VDW grids of C_co2 and O_co2, the Ewald Coulomb grid), copied
+    to tests/golden/grid_files/, with InterpolateVDWGrid and
+    InterpolateCoulombGrid of the reference on those files at points."""
+    import shutil
+    sysm = systems.co2_system(seed=seed)
+    rng = np.random.default_rng(seed + 299)
+    types = ["C_co2", "O_co2"]
+    dst = os.path.join(OUT, "grid_files")
+    os.makedirs(dst, exist_ok=True)
+    with tempfile.TemporaryDirectory() as d:
+        grid = {"types": types, "spacing": spacing}
+        raspa_io.write_inputs(sysm, d, simulation_type="MakeGrid", grid=grid)
+        os.makedirs(os.path.join(d, "share", "raspa", "grids"), exist_ok=True)
+        run_harness(d, ["makegrid"])
+        base = os.path.join(d, "share", "raspa", "grids", "Local", sysm.name, f"{spacing:.6f}")
+        a, b, c = (int(x) for x in sysm.unit_cells)
+        files = {t: os.path.join(base, f"{sysm.name}_{t}_shifted.grid") for t in types}
+        files["coulomb"] = os.path.join(base, f"{a}x{b}x{c}", f"{sysm.name}_Electrostatics_Ewald.grid")
+        rel, meta = {}, {}
+        for k, f in files.items():
+            rel[k] = os.path.relpath(f, d)
+            meta[k] = (read_coulomb_grid_file(f) if k == "coulomb" else read_grid_file(f))[0]
+            shutil.copyfile(f, os.path.join(dst, os.path.basename(f)))
+        grid["use"] = True
+        raspa_io.write_inputs(sysm, d, simulation_type="MonteCarlo", grid=grid)
+        q = rng.random((24, 3)) * sysm.box - 0.5 * sysm.box
+        cmds = []
+        for name in types:
+            t = systems.TYPE_ORDER.index(name)
+            cmds += [f"interp {t + 1} {fmt(p)}" for p in q] + [f"interpc {t + 1} {fmt(p)}" for p in q]
+        rows = run_harness(d, cmds)
+    vals = [float(r[1]) for r in rows if r[0] in ("interp", "interpc")]
+    n = len(q)
+    interp = {name: {"vdw": vals[2 * i * n: (2 * i + 1) * n], "coulomb": vals[(2 * i + 1) * n: (2 * i + 2) * n]}
+              for i, name in enumerate(types)}
+    return {
+        "name": "grid_co2_files",
+        "system": {"builder": "co2_config1", "seed": seed},
+        "spacing": spacing, "types": types,
+        "files": {k: os.path.basename(v) for k, v in files.items()},
+        "reference_paths": rel, "meta": meta,
+        "points": q.tolist(), "interp_ref": interp,
+    }
+
+
 def main():
     if not os.path.exists(HARNESS):
         raise SystemExit("build the harness first: make -C oracle ref")
+    if sys.argv[1:] == ["gridfiles"]:
+        g = grid_files_case()
+        with open(os.path.join(OUT, "grid_co2_files.json"), "w") as fh:
+            json.dump(g, fh)
+        print("grid files", g["files"], g["meta"]["coulomb"]["n"])
+        return
     if sys.argv[1:] == ["coulomb"]:
         g = coulomb_grid_case()
         with open(os.path.join(OUT, "grid_co2_coulomb.json"), "w") as fh:
@@ -313,6 +367,10 @@ def main():
     with open(os.path.join(OUT, "grid_co2_coulomb.json"), "w") as fh:
         json.dump(g, fh)
     print("coulomb grid", g["meta"]["n"], len(g["interp_ref"]))
+    g = grid_files_case()
+    with open(os.path.join(OUT, "grid_co2_files.json"), "w") as fh:
+        json.dump(g, fh)
+    print("grid files", g["files"], g["meta"]["coulomb"]["n"])
 
 
 if __name__ == "__main__":

@@ -10,6 +10,13 @@ programs take the same decisions: the counter blocks of every move type are
 equal, and the energies they print agree to 1e-9 relative (the GPU sums in
 another order than the CPU, so the last digits differ).
 
+The *_grid cases run with the GRID framework model (UseTabularGrid): the
+stock program first makes the grids (SimulationType MakeGrid), then both
+programs read them; the bridge reads the same files into device memory
+with the library's grid-file reader. The hexane cases grow flexible chains
+by the reference's CBMC with the external energies of every bead on the
+GPU.
+
 Both binaries are built where the reference's sources are (build()); the
 test is skipped when they are absent.
 """
@@ -30,11 +37,33 @@ SIMULATE = os.path.join(REF, "simulate")
 SIMULATE_GPU = os.path.join(REF, "simulate_gpu")
 RTOL = 1e-9
 
+def hexane_small():
+    return systems.hexane_system(seed=4, n_atoms=1200, cell=26.0)
+
+
+# case: (system builder, cycles, grid spacing or None)
 CASES = {
-    "co2_tiny": (lambda: systems.tiny_co2_system(), 60),
-    "co2_config1": (lambda: systems.co2_system(seed=1), 12),
-    "methane_config0": (lambda: systems.methane_system(seed=0), 12),
+    "co2_tiny": (lambda: systems.tiny_co2_system(), 60, None),
+    "co2_config1": (lambda: systems.co2_system(seed=1), 12, None),
+    "methane_config0": (lambda: systems.methane_system(seed=0), 12, None),
+    "hexane_small": (hexane_small, 12, None),
+    "co2_config1_grid": (lambda: systems.co2_system(seed=1), 12, 0.5),
+    "methane_config0_grid": (lambda: systems.methane_system(seed=0), 12, 0.5),
+    "hexane_small_grid": (hexane_small, 12, 0.5),
 }
+
+
+def make_grids(s, d, spacing):
+    """The reference's MakeGrid run of the stock program: grid files under
+    d/share/raspa/grids (RASPA_DIR=d) for every pseudo-atom of the molecule."""
+    types = sorted({systems.TYPE_ORDER[int(t)] for t in s.molecule_types()})
+    grid = {"types": types, "spacing": spacing}
+    raspa_io.write_inputs(s, d, simulation_type="MakeGrid", grid=grid)
+    os.makedirs(os.path.join(d, "share", "raspa", "grids"), exist_ok=True)
+    r = subprocess.run([SIMULATE, "-i", "simulation.input"], cwd=d, capture_output=True, text=True, timeout=1200,
+                       env=dict(os.environ, RASPA_DIR=d))
+    assert r.returncode == 0, r.stderr[-2000:]
+    return dict(grid, use=True)
 
 
 def run(binary, d, env=None):
@@ -59,13 +88,18 @@ def summary(txt):
 def test_reference_program_on_gpu_matches_stock_reference(cuda, case, tmp_path):
     if not (os.path.exists(SIMULATE) and os.path.exists(SIMULATE_GPU)):
         pytest.skip("reference programs not built (make -C oracle ref dropin)")
-    build, cycles = CASES[case]
+    build, cycles, spacing = CASES[case]
     s = build()
     kw = dict(cycles=cycles, init_cycles=0, print_every=max(1, cycles // 4), seed=4242)
+    env = dict(os.environ)
+    if spacing:
+        d_grid = str(tmp_path / "grids")
+        kw["grid"] = make_grids(s, d_grid, spacing)
+        env["RASPA_DIR"] = d_grid
     d_cpu = raspa_io.write_inputs(s, str(tmp_path / "cpu"), **kw)
     d_gpu = raspa_io.write_inputs(s, str(tmp_path / "gpu"), **kw)
-    txt_cpu, _ = run(SIMULATE, d_cpu)
-    txt_gpu, err = run(SIMULATE_GPU, d_gpu, env=dict(os.environ, RASPA_GPU_BRIDGE_STATS="1"))
+    txt_cpu, _ = run(SIMULATE, d_cpu, env=env)
+    txt_gpu, err = run(SIMULATE_GPU, d_gpu, env=dict(env, RASPA_GPU_BRIDGE_STATS="1"))
     # the GPU did the work: the bridge reports its device calls
     m = re.search(r"point energies (\d+), move differences (\d+), Ewald (\d+)", err)
     assert m and int(m.group(1)) > 0 and int(m.group(2)) > 0, err[-500:]

@@ -109,3 +109,23 @@ def test_jobs_reuse_the_slots_of_finished_ones(cuda):
     assert st["max_active"] == 2 and st["slot_replacements"] >= 1
     for a, j in zip(alone, jobs):
         _same(a, j.result)
+
+
+def test_engine_outlives_a_replaced_and_destroyed_system(cuda):
+    """The engine keeps no resource of a system it no longer holds: slot 0's
+    system replaced, then destroyed, and the engine runs on."""
+    a = native.GpuSystem(systems.tiny_co2_system(seed=7), maxmol=16, seed=1, stream_id=0)
+    b = native.GpuSystem(systems.tiny_co2_system(seed=8), maxmol=16, seed=2, stream_id=1)
+    c = native.GpuSystem(systems.tiny_co2_system(seed=9), maxmol=16, seed=3, stream_id=2)
+    eng = native.Engine([a, b], precision=native.RGPU_MIXED, threads=256, cluster=1)
+    eng.run(50)
+    eng.sync()
+    assert eng.replace(0, c)
+    a.close()
+    eng.run(50)
+    eng.sync()
+    st = c.state()
+    assert st["status"] == 0 and int(st["step"]) == 50
+    assert int(b.state()["step"]) == 100
+    eng.close()
+    np.testing.assert_array_equal(c.state()["counters"], st["counters"])
