@@ -18,6 +18,8 @@
  */
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 #include <float.h>
 #include <math.h>
 #include <stdint.h>
@@ -1068,71 +1070,100 @@ __device__ __noinline__ double chain_ref_theta(const RgpuSys &S, int i, int stag
  *   candidates 0 .. ntrial-1, the reference's ComputeNormalizedRosenbluthWeight
  *   (src/cbmc.c:542-552 sums up to the global NumberOfTrialPositions; called
  *   at :2401); 1 for bead 2. */
+template <bool F32>
 __device__ __noinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage, int t, uint64_t step, int lane,
                                                 const double (*old)[3], double theta, double *a)
 {
+  /* F32 (the mixed engine): the candidates' Boltzmann factors in FP32, the
+   * chosen dihedral itself from its FP64 uniform as in FP64 */
+  typedef typename std::conditional<F32, float, double>::type T;
   const bool keep_old = old && t == 0;
   double phi = 0.0, wt = 1.0;
   if (i == 2) {
     if (!keep_old) phi = 2.0 * M_PI * rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, 0)) - M_PI;
   } else {
     const int n = S.ntors, nt = S.ntrial, rows = (n + 63) >> 6;
-    double bf[RGPU_TORS_ROWS][2];
-    double big = -1e300, wsum = 0.0;
+    const T beta = (T)S.beta;
+    const T p0 = (T)S.torsion[0], p1 = (T)S.torsion[1], p2 = (T)S.torsion[2], p3 = (T)S.torsion[3];
+    T bf[RGPU_TORS_ROWS][2];
+    T big = (T)-1e30, wsum = 0;
 #pragma unroll
     for (int j = 0; j < RGPU_TORS_ROWS; j++) {
       const int k0 = 2 * (lane + 32 * j);
-      bf[j][0] = bf[j][1] = -1e300;
+      bf[j][0] = bf[j][1] = (T)-1e30;
       if (j < rows && k0 < n) {
         double u[2];
-        rgpu_uniform_pair(S.seed, S.sys_id, step, chain_slot(stage, i, t, k0) >> 1, u);
+        float uf[2];
+        if (F32) {
+          /* the leading 24 bits of the two FP64 uniforms of the block
+           * (rgpu_uniform_pair: o[0] and o[2] head their 53 bits) */
+          uint32_t o[4];
+          rgpu_philox((uint32_t)step, (uint32_t)(step >> 32), chain_slot(stage, i, t, k0) >> 1, S.sys_id,
+                      (uint32_t)S.seed, (uint32_t)(S.seed >> 32), o);
+          uf[0] = (float)(o[0] >> 8) * 5.9604644775390625e-8f;   /* 2^-24 */
+          uf[1] = (float)(o[2] >> 8) * 5.9604644775390625e-8f;
+        } else {
+          rgpu_uniform_pair(S.seed, S.sys_id, step, chain_slot(stage, i, t, k0) >> 1, u);
+        }
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int k = k0 + h;
           if (k < n) {
-            const double cs = (keep_old && k == 0) ? chain_cos_dihedral(old[i - 3], old[i - 2], old[i - 1], old[i])
-                                                   : cos(2.0 * M_PI * u[h] - M_PI);
-            bf[j][h] = -S.beta * chain_torsion_energy(S, cs);
-            big = fmax(big, bf[j][h]);
-            if (k < nt) wsum += exp(bf[j][h]);
+            T c;
+            if (keep_old && k == 0) c = (T)chain_cos_dihedral(old[i - 3], old[i - 2], old[i - 1], old[i]);
+            else if (F32) c = (T)-cospif(2.0f * uf[h]);
+            else c = (T)cos(2.0 * M_PI * u[h] - M_PI);
+            if (F32) {
+              /* chain_torsion_energy in FP32 */
+              const T c2 = (T)2 * c * c - (T)1, c3 = c * ((T)4 * c * c - (T)3);
+              bf[j][h] = -beta * (p0 + p1 * ((T)1 + c) + p2 * ((T)1 - c2) + p3 * ((T)1 + c3));
+            } else {
+              bf[j][h] = -beta * (T)chain_torsion_energy(S, (double)c);
+            }
+            big = big > bf[j][h] ? big : bf[j][h];
+            if (k < nt) wsum += F32 ? (T)__expf((float)bf[j][h]) : (T)exp((double)bf[j][h]);
           }
         }
       }
     }
     for (int o = 16; o; o >>= 1) {
-      big = fmax(big, __shfl_xor_sync(RGPU_FULL, big, o));
+      const T ob = __shfl_xor_sync(RGPU_FULL, big, o);
+      big = big > ob ? big : ob;
       wsum += __shfl_xor_sync(RGPU_FULL, wsum, o);
     }
-    wt = wsum / (double)nt;
+    wt = (double)wsum / (double)nt;
     if (!keep_old) {
-      double tot = 0.0;
+      /* the shifted factors, once: summed here, scanned below */
+      T tot = 0;
 #pragma unroll
       for (int j = 0; j < RGPU_TORS_ROWS; j++)
 #pragma unroll
-        for (int h = 0; h < 2; h++)
-          if (j < rows && 2 * (lane + 32 * j) + h < n) tot += exp(bf[j][h] - big);
+        for (int h = 0; h < 2; h++) {
+          const bool v = j < rows && 2 * (lane + 32 * j) + h < n;
+          bf[j][h] = v ? (F32 ? (T)__expf((float)(bf[j][h] - big)) : (T)exp((double)(bf[j][h] - big))) : (T)0;
+          tot += bf[j][h];
+        }
       for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(RGPU_FULL, tot, o);
-      const double target =
-          rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, RGPU_REF_TORS_SEL_SLOT)) *
-          tot;
+      const T target =
+          (T)rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, RGPU_REF_TORS_SEL_SLOT)) * tot;
       /* the first candidate whose cumulative sum reaches the target, row
        * by row; none (rounding only): the last, where the serial search
        * stops */
       int kc = n - 1;
-      double before = 0.0;
+      T before = 0;
       bool done = false;
 #pragma unroll
       for (int j = 0; j < RGPU_TORS_ROWS; j++) {
         if (!done && j < rows) {
           const int k0 = 2 * (lane + 32 * j);
-          const double e0 = k0 < n ? exp(bf[j][0] - big) : 0.0, e1 = k0 + 1 < n ? exp(bf[j][1] - big) : 0.0;
-          const double part = e0 + e1;
-          double incl = part;
+          const T e0 = bf[j][0], e1 = bf[j][1];
+          const T part = e0 + e1;
+          T incl = part;
           for (int o = 1; o < 32; o <<= 1) {
-            const double y = __shfl_up_sync(RGPU_FULL, incl, o);
+            const T y = __shfl_up_sync(RGPU_FULL, incl, o);
             if (lane >= o) incl += y;
           }
-          const double c0 = before + (incl - part) + e0;
+          const T c0 = before + (incl - part) + e0;
           const int mine = (k0 < n && c0 >= target) ? k0 : ((k0 + 1 < n && c0 + e1 >= target) ? k0 + 1 : -1);
           const unsigned hit = __ballot_sync(RGPU_FULL, mine >= 0);
           if (hit) {
@@ -1142,7 +1173,21 @@ __device__ __noinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage,
           before += __shfl_sync(RGPU_FULL, incl, 31);
         }
       }
-      if (lane == 0) phi = 2.0 * M_PI * rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, kc)) - M_PI;
+      if (lane == 0) {
+        const double uk = rgpu_uniform(S.seed, S.sys_id, step, chain_slot(stage, i, t, kc));
+        if (F32) {
+          /* phi = 2 pi u - pi: cos phi = -cospi(2u), sin phi = -sinpi(2u) */
+          double sn, cs;
+          sincospi(2.0 * uk, &sn, &cs);
+          a[2] = -cs;
+          a[3] = -sn;
+          a[0] = cos(theta);
+          a[1] = sin(theta);
+          a[4] = wt;
+          return;
+        }
+        phi = 2.0 * M_PI * uk - M_PI;
+      }
     }
   }
   if (lane == 0) {
@@ -1159,8 +1204,11 @@ __device__ __noinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage,
  * reference's scheme (S.chain_scheme 0): one warp per (bead, trial); a
  * retrace passes the old configuration `old` (published by a barrier
  * before the call). Independent draws (S.chain_scheme 1): 8 lanes per
- * (bead, trial), four per warp, and factor 1. All threads call; the
- * caller's next barrier publishes the table. */
+ * (bead, trial), four per warp, and factor 1. The (bead, trial) tasks are
+ * shared out over the warps of all CTAs of the cluster; after a cluster
+ * barrier each CTA copies the other CTAs' rows from their shared memory.
+ * All threads of the cluster call; the caller's next barrier publishes the
+ * table. */
 template <bool MIXED, bool FLEX>
 __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage, double *tab,
                                                    const double (*old)[3])
@@ -1169,36 +1217,52 @@ __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stag
   const int na = S.natom, nt = S.ntrial;
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int ntask = na > 2 ? (na - 2) * nt : 0;
+  const int gw = E.rank * nw + (threadIdx.x >> 5), ngw = nw * E.csize;   /* warp of the cluster */
+  const int per = S.chain_scheme == 0 ? 1 : 4;                           /* tasks a warp takes at once */
   if (S.chain_scheme == 0) {
-    /* each bead's bend angle once (one warp per bead), then one warp per
-     * (bead, trial); the angles sit after the table */
+    /* each bead's bend angle once (one warp per bead, in every CTA), then
+     * one warp per (bead, trial); the angles sit after the table */
     double *theta = tab + RGPU_ANG_TABLE;
     for (int i = 2 + (threadIdx.x >> 5); i < na; i += nw) {
       const double th = chain_ref_theta(S, i, stage, E.step, lane, old);
       if (lane == 0) theta[i] = th;
     }
     __syncthreads();
-    for (int task = threadIdx.x >> 5; task < ntask; task += nw) {
+    for (int task = gw; task < ntask; task += ngw) {
       const int i = 2 + task / nt, t = task % nt;
-      chain_ref_trial(S, i, stage, t, E.step, lane, old, theta[i],
-                      tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t));
+      chain_ref_trial<MIXED>(S, i, stage, t, E.step, lane, old, theta[i],
+                             tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t));
     }
-    return;
+  } else {
+    for (int t0 = gw * 4; t0 < ntask; t0 += ngw * 4) {
+      const int task = t0 + (lane >> 3);
+      const bool live = task < ntask;
+      const int i = live ? 2 + task / nt : 2, t = live ? task % nt : 0;
+      double th, ph;
+      chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
+      if (live && (lane & 7) == 0) {
+        double *a = tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t);
+        a[0] = cos(th);
+        a[1] = sin(th);
+        a[2] = cos(ph);
+        a[3] = sin(ph);
+        a[4] = 1.0;
+      }
+    }
   }
-  for (int t0 = (threadIdx.x >> 5) * 4; t0 < ntask; t0 += nw * 4) {
-    const int task = t0 + (lane >> 3);
-    const bool live = task < ntask;
-    const int i = live ? 2 + task / nt : 2, t = live ? task % nt : 0;
-    double th, ph;
-    chain_angles_group(S, i, stage, t, live, E.step, lane, th, ph);
-    if (live && (lane & 7) == 0) {
-      double *a = tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t);
-      a[0] = cos(th);
-      a[1] = sin(th);
-      a[2] = cos(ph);
-      a[3] = sin(ph);
-      a[4] = 1.0;
+  if (E.csize > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+      const int owner = ((task / per) % ngw) / nw;
+      if (owner == E.rank) continue;
+      const int off = RGPU_ANG_STRIDE * ((task / nt) * RGPU_MAX_TRIALS + task % nt);
+      const double *src = cl.map_shared_rank(tab, owner) + off;
+      for (int d = 0; d < RGPU_ANG_STRIDE; d++) tab[off + d] = src[d];
     }
+    /* no CTA writes this table again before the next cluster barrier (the
+     * evaluation that follows ends with one), so the peers' reads are done
+     * by then */
   }
 }
 

@@ -14,12 +14,15 @@ launches:
   back;
 - jobs that have arrived are admitted, as long as both hold:
   - an engine slot is free (one cluster per job; slots = SMs / cluster
-    size);
+    size), or will be: up to `lookahead` jobs beyond the slots are admitted
+    ahead and wait, set up, for the next free slot;
   - the job's estimated device-memory footprint fits the budget.
 
 A newly admitted job's device set-up (framework upload, structure factors)
-is issued on its own stream while the current launch runs, so admission
-overlaps the other jobs' work on the GPU.
+runs on a host thread of its own and on the job system's own stream, while
+the serving loop launches and retires, so admission overlaps the other jobs'
+work on the GPU; a job admitted ahead goes into the slot of a finished one
+at the next launch without set-up work in between.
 
 The engine stops each job exactly at its step count (rgpu_system_set_limits).
 Each job has its own random stream, and the launch shape is fixed for the
@@ -65,6 +68,7 @@ class Job:
     raspa_output: bool = False
     # filled in by the server
     admitted: Optional[float] = None
+    started: Optional[float] = None     # placed in an engine slot
     finished: Optional[float] = None
     result: Optional[dict] = None
 
@@ -128,7 +132,8 @@ class Server:
     """Admits, advances and retires jobs; see the module docstring."""
 
     def __init__(self, precision: int = native.RGPU_MIXED, threads: int = 1024, cluster: int = 1,
-                 chunk: int = 400, max_slots: Optional[int] = None, mem_budget: float = 150e9):
+                 chunk: int = 400, max_slots: Optional[int] = None, mem_budget: float = 150e9,
+                 lookahead: int = 16):
         import torch
 
         self.precision = precision
@@ -137,6 +142,7 @@ class Server:
         self.chunk = chunk
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         self.max_slots = max_slots or max(1, sms // cluster)
+        self.lookahead = lookahead
         self.mem_budget = mem_budget
         self.stream = torch.cuda.Stream()
         self.launches = 0
@@ -224,23 +230,27 @@ class Server:
         With realtime=False every job is available at once. Returns the
         latency and throughput figures; per-job results are on the jobs.
 
-        The engine has max_slots slots from its first build; the free ones
-        hold an idle placeholder system sized for the job list
-        (`_placeholder`), and a finished job's system stays in its slot (at
-        its step limit it takes no step). A new job's system replaces one of
-        them in place (Engine.replace: no allocation, no device
-        synchronisation, the captured graph stays valid). A new engine is
-        built only when a system does not fit the engine's layout. Replaced
-        systems are freed in batches, when the device is idle anyway."""
+        Admission runs on a host thread of its own: it sets up each arrived
+        job's system (device allocation, upload, structure factors, on the
+        system's own stream) while this thread launches and retires, for
+        the free slots plus `lookahead` more. The engine has max_slots slots
+        from its first build; the free ones hold an idle placeholder system
+        sized for the job list (`_placeholder`), and a finished job's system
+        stays in its slot (at its step limit it takes no step). A new job's
+        system replaces one of them in place (Engine.replace: no allocation,
+        no device synchronisation, the captured graph stays valid). A new
+        engine is built only when a system does not fit the engine's layout.
+        Replaced systems are freed in batches, when the device is idle
+        anyway."""
+        import threading
+
         import torch
 
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
-        waiting: collections.deque = collections.deque()
         slots: List[Optional[list]] = []     # engine slot -> [job, GpuSystem, steps done, footprint] or None
         occupants: List["native.GpuSystem"] = []   # the system in each slot (a finished job's until replaced)
         unplaced: List[list] = []            # admitted, not yet in the engine
         to_free: List["native.GpuSystem"] = []
-        mem_used = 0
         eng = None
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
@@ -249,118 +259,186 @@ class Server:
         max_active = 0
         rebuilds = 0
         replacements = 0
+        host = collections.defaultdict(float)   # host seconds by phase
         holder = self._placeholder(jobs)
 
-        def n_active():
-            return sum(1 for a in slots if a is not None) + len(unplaced)
+        # shared with the admission thread, under `cond`
+        cond = threading.Condition()
+        adm = {"mem": 0, "busy": 0, "held": 0, "left": len(jobs), "error": None}
+        ready: collections.deque = collections.deque()   # set up, handed to this thread
+        stop = threading.Event()
+        fps = {id(j): footprint_bytes(j) for j in jobs}
 
-        def admit_ready():
-            nonlocal mem_used
-            t = now()
-            while pending and (pending[0].arrival <= t or not realtime):
-                waiting.append(pending.popleft())
-            while waiting and n_active() < self.max_slots:
-                fp = footprint_bytes(waiting[0])
-                if mem_used + fp > self.mem_budget and n_active():
-                    break
-                job = waiting.popleft()
-                g = self._admit(job, now())
-                unplaced.append([job, g, int(g.state()["step"]) if job.resume is not None else 0, fp])
-                mem_used += fp
+        def admission():
+            """sets up arrived jobs while slots (plus lookahead) and the
+            memory budget allow; busy = jobs in slots, held = admitted
+            jobs not yet in a slot (set up or being set up). Waits on `cond`
+            for the next arrival or for jobs to finish."""
+            try:
+                while not stop.is_set() and pending:
+                    job = None
+                    with cond:
+                        fp = fps[id(pending[0])]
+                        n = adm["busy"] + adm["held"]
+                        arrived = pending[0].arrival <= now() or not realtime
+                        if arrived and n < self.max_slots + self.lookahead and \
+                                (adm["mem"] + fp <= self.mem_budget or n == 0):
+                            job = pending.popleft()
+                            adm["mem"] += fp
+                            adm["held"] += 1
+                        else:
+                            wait = pending[0].arrival - now() if not arrived else 0.05
+                            cond.wait(timeout=max(wait, 1e-4))
+                    if job is None:
+                        continue
+                    h0 = time.perf_counter()
+                    g = self._admit(job, now())
+                    entry = [job, g, int(g.state()["step"]) if job.resume is not None else 0, fp]
+                    with cond:
+                        ready.append(entry)
+                        host["admit"] += time.perf_counter() - h0
+                        cond.notify_all()
+            except BaseException as e:  # surfaced by the serving loop
+                with cond:
+                    adm["error"] = e
 
         def place():
-            """the admitted jobs into free slots, or a new engine"""
+            """the admitted jobs into free slots, or a new engine; jobs
+            admitted ahead wait while every slot is busy"""
             nonlocal eng, slots, occupants, rebuilds, replacements
-            rest = []
+            rest, wait_slot = [], []
             for entry in unplaced:
                 i = next((k for k, a in enumerate(slots) if a is None), None)
-                if eng is not None and i is not None and eng.replace(i, entry[1], self.stream.cuda_stream):
+                if eng is not None and i is None:
+                    wait_slot.append(entry)
+                elif eng is not None and eng.replace(i, entry[1], self.stream.cuda_stream):
                     if occupants[i] is not holder:
                         to_free.append(occupants[i])
                     slots[i], occupants[i] = entry, entry[1]
+                    entry[0].started = now()
                     replacements += 1
                 else:
                     rest.append(entry)
-            unplaced.clear()
-            if not rest:
-                return
-            # a new engine: the active jobs, the new ones, and the finished
-            # jobs' systems still held (their slots stay free for later jobs)
-            keep = [(a, g) for a, g in zip(slots, occupants)]
-            keep = [(a, g) for a, g in keep if a is not None] + [(e, e[1]) for e in rest] + \
-                   [(a, g) for a, g in keep if a is None]
-            keep = keep[:max(self.max_slots, sum(1 for a, _ in keep if a is not None))]
-            held = {id(g) for _, g in keep}
-            to_free.extend(g for g in occupants if id(g) not in held and g is not holder)
-            if holder is not None:
-                keep += [(None, holder)] * (self.max_slots - len(keep))
-            slots = [a for a, _ in keep]
-            occupants = [g for _, g in keep]
-            if eng is not None:
-                eng.close()
-            eng = native.Engine(occupants, precision=self.precision, threads=self.threads, cluster=self.cluster)
-            eng.use_graph(True)
-            rebuilds += 1
+            free = self.max_slots - sum(1 for a in slots if a is not None)
+            unplaced[:] = wait_slot + rest[max(free, 0):]
+            rest = rest[:max(free, 0)]
+            if rest:
+                # a new engine: the active jobs, the new ones, and the finished
+                # jobs' systems still held (their slots stay free for later jobs)
+                keep = [(a, g) for a, g in zip(slots, occupants)]
+                keep = [(a, g) for a, g in keep if a is not None] + [(e, e[1]) for e in rest] + \
+                       [(a, g) for a, g in keep if a is None]
+                keep = keep[:max(self.max_slots, sum(1 for a, _ in keep if a is not None))]
+                held = {id(g) for _, g in keep}
+                to_free.extend(g for g in occupants if id(g) not in held and g is not holder)
+                if holder is not None:
+                    keep += [(None, holder)] * (self.max_slots - len(keep))
+                slots = [a for a, _ in keep]
+                occupants = [g for _, g in keep]
+                for e in rest:
+                    e[0].started = now()
+                if eng is not None:
+                    eng.close()
+                eng = native.Engine(occupants, precision=self.precision, threads=self.threads, cluster=self.cluster)
+                eng.use_graph(True)
+                rebuilds += 1
+            n_busy = sum(1 for a in slots if a is not None)
+            with cond:
+                adm["held"] -= n_busy - adm["busy"]
+                adm["busy"] = n_busy
+                cond.notify_all()
 
-        while pending or waiting or unplaced or any(a is not None for a in slots):
-            admit_ready()
-            if unplaced:
-                place()
-            running = [a for a in slots if a is not None]
-            if not running:
-                if pending:
-                    time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
-                continue
-            max_active = max(max_active, len(running))
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(self.stream)
-            eng.run(self.chunk, self.stream.cuda_stream)      # asynchronous
-            ev1.record(self.stream)
-            self.launches += 1
-            admit_ready()                                     # overlaps the launch
-            eng.sync()
-            ev1.synchronize()
-            busy += ev0.elapsed_time(ev1) / 1e3               # device time of the launch
-            for k, a in enumerate(slots):
-                if a is None:
+        worker = threading.Thread(target=admission, name="raspa2-admission", daemon=True)
+        worker.start()
+        try:
+            while True:
+                with cond:
+                    if adm["error"] is not None:
+                        raise adm["error"]
+                    while ready:
+                        unplaced.append(ready.popleft())
+                    left = adm["left"]
+                h1 = time.perf_counter()
+                if unplaced:
+                    place()
+                host["place"] += time.perf_counter() - h1
+                running = [a for a in slots if a is not None]
+                if not running:
+                    if left == 0:
+                        break
+                    with cond:                                # the admission thread is setting jobs up
+                        if not ready and adm["error"] is None:
+                            cond.wait(timeout=5e-3)
                     continue
-                job, g, done, fp = a
-                if job.raspa_output:
-                    # the engine stopped the job at its block boundary or ran the chunk
-                    step = int(g.state()["step"])
-                    adv = step - done
-                    self._close_blocks(job, g, step)
-                else:
-                    adv = min(self.chunk, job.steps - done)   # the engine stops each job at its limit
-                total_steps += adv
-                a[2] = done + adv
-                if a[2] >= job.steps:
-                    job.result = self._result(job, g)
-                    job.finished = now()
-                    mem_used -= fp
-                    slots[k] = None                           # the system stays in the slot, idle
-            if len(to_free) >= 32:
-                for g in to_free:
-                    g.close()
-                to_free.clear()
+                max_active = max(max_active, len(running))
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(self.stream)
+                eng.run(self.chunk, self.stream.cuda_stream)      # asynchronous
+                ev1.record(self.stream)
+                self.launches += 1
+                h1 = time.perf_counter()
+                eng.sync()
+                ev1.synchronize()
+                h2 = time.perf_counter()
+                host["wait"] += h2 - h1
+                busy += ev0.elapsed_time(ev1) / 1e3               # device time of the launch
+                freed_mem, finished = 0, 0
+                for k, a in enumerate(slots):
+                    if a is None:
+                        continue
+                    job, g, done, fp = a
+                    if job.raspa_output:
+                        # the engine stopped the job at its block boundary or ran the chunk
+                        step = int(g.state()["step"])
+                        adv = step - done
+                        self._close_blocks(job, g, step)
+                    else:
+                        adv = min(self.chunk, job.steps - done)   # the engine stops each job at its limit
+                    total_steps += adv
+                    a[2] = done + adv
+                    if a[2] >= job.steps:
+                        job.result = self._result(job, g)
+                        job.finished = now()
+                        freed_mem += fp
+                        finished += 1
+                        slots[k] = None                           # the system stays in the slot, idle
+                if finished:
+                    with cond:
+                        adm["mem"] -= freed_mem
+                        adm["busy"] -= finished
+                        adm["left"] -= finished
+                        cond.notify_all()
+                h3 = time.perf_counter()
+                host["results"] += h3 - h2
+                if len(to_free) >= 32:
+                    for g in to_free:
+                        g.close()
+                    to_free.clear()
+                host["free"] += time.perf_counter() - h3
+        finally:
+            stop.set()
+            with cond:
+                cond.notify_all()
+            worker.join()
         if eng is not None:
             eng.close()
-        for g in set(to_free + occupants + ([holder] if holder is not None else [])):
+        for g in set(to_free + occupants + list(e[1] for e in unplaced) + ([holder] if holder is not None else [])):
             g.close()
         torch.cuda.synchronize()
         makespan = now()
         lat = np.array([j.latency for j in jobs]) * 1e3
-        wait = np.array([j.admitted - j.arrival for j in jobs]) * 1e3
+        wait = np.array([j.started - j.arrival for j in jobs]) * 1e3
         span = max(j.arrival for j in jobs) - min(j.arrival for j in jobs) if realtime and len(jobs) > 1 else 0.0
         req = float(sum(j.steps for j in jobs))
         return {"jobs": len(jobs), "makespan_s": makespan, "launches": self.launches,
                 "p50_job_ms": float(np.percentile(lat, 50)), "p99_job_ms": float(np.percentile(lat, 99)),
                 "p50_wait_ms": float(np.percentile(wait, 50)), "p99_wait_ms": float(np.percentile(wait, 99)),
                 "mc_steps": int(total_steps), "mc_steps_per_s": total_steps / makespan, "max_active": max_active,
-                "p50_service_ms": float(np.percentile([(j.finished - j.admitted) * 1e3 for j in jobs], 50)),
+                "p50_service_ms": float(np.percentile([(j.finished - j.started) * 1e3 for j in jobs], 50)),
                 "gpu_busy_frac": busy / makespan,
                 "offered_steps_per_s": req / span if span > 0 else None,
-                "engine_builds": rebuilds, "slot_replacements": replacements}
+                "engine_builds": rebuilds, "slot_replacements": replacements,
+                "host_s": {k: round(v, 4) for k, v in host.items()}}
 
 
 # --------------------------------------------------------------------------
