@@ -617,6 +617,7 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
     c0 = np.array([g.state()["counters"] for g in gs])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=stream.device)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.nvtx.range_push("hexane_timed")
     with torch.cuda.stream(stream):
         for k in range(steps):
             flush.zero_()
@@ -624,6 +625,7 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
             e.run(args.hexane_moves, stream.cuda_stream)
             evs[k][1].record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     t = sum(a.elapsed_time(b) for a, b in evs) / 1e3
     dc = np.array([g.state()["counters"] for g in gs]) - c0
     d = dc.sum(axis=0)
