@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import collections
 import dataclasses
+import gc
 import time
 from typing import Dict, List, Optional, Sequence
 
@@ -348,6 +349,12 @@ class Server:
                 adm["busy"] = n_busy
                 cond.notify_all()
 
+        # no cyclic garbage collection while serving: a full collection of a
+        # large process holds the interpreter lock for tens of milliseconds,
+        # and the serving loop would miss its next launch meanwhile
+        gc_on = gc.isenabled()
+        gc.collect()
+        gc.disable()
         worker = threading.Thread(target=admission, name="raspa2-admission", daemon=True)
         worker.start()
         try:
@@ -420,6 +427,8 @@ class Server:
             with cond:
                 cond.notify_all()
             worker.join()
+            if gc_on:
+                gc.enable()
         if eng is not None:
             eng.close()
         for g in set(to_free + occupants + list(e[1] for e in unplaced) + ([holder] if holder is not None else [])):
