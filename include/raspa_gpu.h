@@ -45,7 +45,7 @@ typedef struct rgpu_engine rgpu_engine;
  * Components[], PseudoAtoms and the Ewald globals (src/input.c ReadInputFile,
  * src/ewald.c:200-261 InitializeEwald, :532-599 SetupKVectors). */
 typedef struct {
-  double box[3];              /* orthorhombic box lengths; each >= 2 * cutoff */
+  double box[3];              /* orthorhombic box lengths; each >= 2 * cutoff (see cell_matrix) */
   double cutoff;              /* VDW and real-space charge cut-off */
   double beta;                /* 1 / (k_B T), inverse internal energy units */
   double coulomb;             /* COULOMBIC_CONVERSION_FACTOR (src/constants.c:162) */
@@ -102,6 +102,16 @@ typedef struct {
    * from their Boltzmann distributions (no torsion factor in the weight). */
   int chain_scheme;
   int ntors;
+  /* Triclinic box (BoundaryCondition TRICLINIC): the box matrix, row-major,
+   * whose columns are the cell vectors a, b, c, upper triangular as the
+   * reference builds Box (a along x, b in the xy plane; src/framework.c:
+   * 2025-2040). All zero: the orthorhombic box of box[3]. Every
+   * perpendicular width must be >= 2 * cutoff. Distances use the
+   * reference's triclinic minimum image (fractional coordinates wrapped to
+   * the nearest integer, src/potentials.h:246-262), wave vectors 2 pi H^-T n
+   * (src/ewald.c:560-595). Energy grids are not available in a triclinic
+   * box. */
+  double cell_matrix[9];
 } rgpu_system_desc;
 
 const char *rgpu_error_string(int code);

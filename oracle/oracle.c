@@ -15,10 +15,32 @@
 /* NINT of src/utils.h:60 */
 static inline double nint(double x) { return (double)(int)(x >= 0.0 ? x + 0.5 : x - 0.5); }
 
-/* rectangular branch of ApplyBoundaryCondition, src/potentials.h:241-245 */
+/* ApplyBoundaryCondition, src/potentials.h:232-268: the rectangular branch
+ * (:241-245), or the triclinic one (:246-262: to fractional coordinates,
+ * each wrapped to its nearest integer, back to Cartesian) */
 static inline void min_image(const or_sys *s, double *d)
 {
-  for (int c = 0; c < 3; c++) d[c] -= s->box[c] * nint(d[c] * (1.0 / s->box[c]));
+  if (!s->triclinic) {
+    for (int c = 0; c < 3; c++) d[c] -= s->box[c] * nint(d[c] * (1.0 / s->box[c]));
+    return;
+  }
+  double t[3];
+  for (int r = 0; r < 3; r++) {
+    const double f = s->hinv[3 * r] * d[0] + s->hinv[3 * r + 1] * d[1] + s->hinv[3 * r + 2] * d[2];
+    t[r] = f - nint(f);
+  }
+  for (int r = 0; r < 3; r++) d[r] = s->hm[3 * r] * t[0] + s->hm[3 * r + 1] * t[1] + s->hm[3 * r + 2] * t[2];
+}
+
+/* the point of fractional coordinates u in the box (ConvertFromABCtoXYZ,
+ * src/potentials.c:5548) */
+static inline void box_point(const or_sys *s, const double *u, double *p)
+{
+  if (!s->triclinic) {
+    for (int c = 0; c < 3; c++) p[c] = s->box[c] * u[c];
+    return;
+  }
+  for (int r = 0; r < 3; r++) p[r] = s->hm[3 * r] * u[0] + s->hm[3 * r + 1] * u[1] + s->hm[3 * r + 2] * u[2];
 }
 
 static inline double dist2(const or_sys *s, const double *a, const double *b, double *d)
@@ -236,12 +258,22 @@ int or_move_delta(const or_sys *s, int m, const double *new_xyz, double *out)
 
 static double recip_factor(const or_sys *s, const int *k)
 {
-  /* SetupKVectors, src/ewald.c:560-595 (orthorhombic: k = 2 pi n / L) */
-  double kx = 2.0 * M_PI * k[0] / s->box[0];
-  double ky = 2.0 * M_PI * k[1] / s->box[1];
-  double kz = 2.0 * M_PI * k[2] / s->box[2];
+  /* SetupKVectors, src/ewald.c:560-595: k = 2 pi n / L (orthorhombic), or
+   * k = 2 pi H^-T n (triclinic, the inverse box's columns, :562-575) */
+  double kx, ky, kz, vol;
+  if (!s->triclinic) {
+    kx = 2.0 * M_PI * k[0] / s->box[0];
+    ky = 2.0 * M_PI * k[1] / s->box[1];
+    kz = 2.0 * M_PI * k[2] / s->box[2];
+    vol = s->box[0] * s->box[1] * s->box[2];
+  } else {
+    const double *v = s->hinv;
+    kx = 2.0 * M_PI * (k[0] * v[0] + k[1] * v[3] + k[2] * v[6]);
+    ky = 2.0 * M_PI * (k[0] * v[1] + k[1] * v[4] + k[2] * v[7]);
+    kz = 2.0 * M_PI * (k[0] * v[2] + k[1] * v[5] + k[2] * v[8]);
+    vol = s->hm[0] * s->hm[4] * s->hm[8];
+  }
   double k2 = kx * kx + ky * ky + kz * kz;
-  double vol = s->box[0] * s->box[1] * s->box[2];
   double pre = (k[0] == 0 ? 2.0 : 4.0) * M_PI / vol;
   return s->coulomb * pre * exp((-0.25 / SQR(s->alpha)) * k2) / k2;
 }
@@ -250,8 +282,14 @@ static double recip_factor(const or_sys *s, const int *k)
  * fractional coordinate times 2 pi (src/ewald.c:6941-7100) */
 static void site_phase(const or_sys *s, const double *p, const int *k, double *re, double *im)
 {
-  double a = 2.0 * M_PI * (k[0] * p[0] / s->box[0] + k[1] * p[1] / s->box[1] +
-                           k[2] * p[2] / s->box[2]);
+  double a;
+  if (!s->triclinic) {
+    a = 2.0 * M_PI * (k[0] * p[0] / s->box[0] + k[1] * p[1] / s->box[1] + k[2] * p[2] / s->box[2]);
+  } else {
+    double f[3];
+    for (int r = 0; r < 3; r++) f[r] = s->hinv[3 * r] * p[0] + s->hinv[3 * r + 1] * p[1] + s->hinv[3 * r + 2] * p[2];
+    a = 2.0 * M_PI * (k[0] * f[0] + k[1] * f[1] + k[2] * f[2]);
+  }
   *re = cos(a);
   *im = sin(a);
 }
@@ -648,12 +686,11 @@ static void cbmc_common(const or_sys *s, int retrace, int reins, int m, int nf, 
     if (retrace && i == 0) {
       pos1[0][0] = old[3 * sb]; pos1[0][1] = old[3 * sb + 1]; pos1[0][2] = old[3 * sb + 2];
     } else {
-      double sz = rng(ctx, SLOT_FIRST + 3 * i + 0);
-      double sy = rng(ctx, SLOT_FIRST + 3 * i + 1);
-      double sx = rng(ctx, SLOT_FIRST + 3 * i + 2);
-      pos1[i][0] = s->box[0] * sx;
-      pos1[i][1] = s->box[1] * sy;
-      pos1[i][2] = s->box[2] * sz;
+      double u[3];
+      u[2] = rng(ctx, SLOT_FIRST + 3 * i + 0);
+      u[1] = rng(ctx, SLOT_FIRST + 3 * i + 1);
+      u[0] = rng(ctx, SLOT_FIRST + 3 * i + 2);
+      box_point(s, u, pos1[i]);      /* src/cbmc.c:655-662 */
     }
     or_point_energy(s, type0, q0, pos1[i], exclude, e1[i]);
     if (e1[i][0] >= s->overlap || e1[i][1] >= s->overlap || e1[i][2] >= s->overlap ||
@@ -1016,7 +1053,9 @@ static void chain_grow(const or_sys *s, int retrace, int stage, int m, int exclu
         for (int d = 0; d < 3; d++) pos[0][d] = s->ads_xyz[3 * (m * na + i) + d];
         ub[0] = bonded_energy(s, (const double(*)[3])x, i, pos[0]);
       } else if (i == 0) {
-        for (int d = 0; d < 3; d++) pos[t][d] = s->box[d] * chain_u(c, stage, 0, t, d);
+        double u[3];
+        for (int d = 0; d < 3; d++) u[d] = chain_u(c, stage, 0, t, d);
+        box_point(s, u, pos[t]);
       } else if (ref) {
         place(i >= 3 ? x[i - 3] : NULL, x[i - 2], x[i - 1], s->bond, theta_sh, phi[t], pos[t]);
         ub[t] = bonded_energy(s, (const double(*)[3])x, i, pos[t]);

@@ -17,9 +17,10 @@
 extern "C" {
 #endif
 
-/* One simulation box. Orthorhombic cells only (the synthetic workloads are
- * orthorhombic/cubic); the minimum image is the rectangular branch of
- * ApplyBoundaryCondition (src/potentials.h:232-268). */
+/* One simulation box. Orthorhombic (box[3]), or triclinic (triclinic = 1,
+ * hm = the box matrix whose columns are the cell vectors, hinv its
+ * inverse, both row-major): the minimum image is the rectangular or the
+ * triclinic branch of ApplyBoundaryCondition (src/potentials.h:232-268). */
 typedef struct {
   double box[3];
   double rc2_vdw, rc2_cc;   /* squared cut-offs */
@@ -74,6 +75,9 @@ typedef struct {
    * dihedral drawn per trial from their Boltzmann distributions */
   int chain_scheme;
   int ntors;
+  /* triclinic box */
+  int triclinic;
+  double hm[9], hinv[9];
 } or_sys;
 
 /* pair terms */

@@ -36,6 +36,7 @@ class OrSys(C.Structure):
         ("coul_grid", C.POINTER(C.c_float)), ("coul_npts", C.c_int * 3), ("coul_size", C.c_double * 3),
         ("coul_shift", C.c_double * 3), ("coul_cell", C.c_double * 3),
         ("chain_scheme", C.c_int), ("ntors", C.c_int),
+        ("triclinic", C.c_int), ("hm", C.c_double * 9), ("hinv", C.c_double * 9),
     ]
 
 
@@ -95,7 +96,7 @@ class Oracle:
 
     def __init__(self, box, rc, beta, eps, sig2, shift, fw_xyz, fw_type, fw_q,
                  mol_type, mol_q, mol_ref, start_bead, ewald=False, alpha=0.0,
-                 kidx=None, coulomb=None, overlap=1e7, maxmol=4096, rc_cc=None):
+                 kidx=None, coulomb=None, overlap=1e7, maxmol=4096, rc_cc=None, cell_matrix=None):
         from raspa2_b200 import units
         self._keep = []
 
@@ -106,6 +107,12 @@ class Oracle:
 
         s = OrSys()
         s.box[:] = [float(x) for x in box]
+        if cell_matrix is not None:
+            # triclinic box: the cell vectors as the matrix's columns
+            h = np.asarray(cell_matrix, float)
+            s.triclinic = 1
+            s.hm[:] = [float(x) for x in h.reshape(-1)]
+            s.hinv[:] = [float(x) for x in np.linalg.inv(h).reshape(-1)]
         s.rc2_vdw = rc * rc
         s.rc2_cc = (rc_cc if rc_cc is not None else rc) ** 2
         s.overlap = overlap
@@ -150,7 +157,8 @@ class Oracle:
         o = cls(sysm.box, sysm.cutoff, units.beta(sysm.temperature), eps, sig2, shift,
                 pos, t, q, sysm.molecule_types(), sysm.molecule.charges(),
                 sysm.molecule.positions, sysm.molecule.starting_bead,
-                ewald=sysm.ewald, alpha=sysm.alpha, kidx=kidx, maxmol=maxmol)
+                ewald=sysm.ewald, alpha=sysm.alpha, kidx=kidx, maxmol=maxmol,
+                cell_matrix=sysm.box_matrix if sysm.triclinic else None)
         mol = sysm.molecule
         if not mol.rigid:
             s = o.s

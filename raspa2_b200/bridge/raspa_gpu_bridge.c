@@ -33,7 +33,7 @@
  *
  * Supported: one system, one adsorbate component (rigid or single-bead; a
  * flexible chain's external energies as well), one rigid framework, an
- * orthorhombic box without replicas or cell lists, Lennard-Jones (or zero)
+ * orthorhombic or triclinic box without replicas or cell lists, Lennard-Jones (or zero)
  * potentials, charges by the Ewald method with one cut-off, no CFCMC
  * scaling. With the GRID framework model (UseTabularGrid) the grid files
  * the reference read at start-up (the VDW grid of every adsorbate
@@ -166,8 +166,15 @@ static void bridge_init(void)
     bridge_fail("only one rigid framework is supported", 0);
   if (UseReplicas[s] || UseCellLists[s]) bridge_fail("replica cells and cell lists are not supported", 0);
   const REAL_MATRIX3x3 B = Box[s];
-  if (fabs(B.bx) + fabs(B.cx) + fabs(B.ay) + fabs(B.cy) + fabs(B.az) + fabs(B.bz) > 1e-8 * (B.ax + B.by + B.cz))
-    bridge_fail("only orthorhombic boxes are supported", 0);
+  if (BoundaryCondition[s] != TRICLINIC && BoundaryCondition[s] != RECTANGULAR && BoundaryCondition[s] != CUBIC)
+    bridge_fail("only rectangular, cubic and triclinic boundary conditions are supported", 0);
+  /* the reference also takes a cubic cell as TRICLINIC (src/framework.c:
+   * 1987-1991), with off-diagonal elements of rounding size (cos 90 deg):
+   * such a box goes to the orthorhombic path */
+  const int tri = BoundaryCondition[s] == TRICLINIC &&
+                  fabs(B.bx) + fabs(B.cx) + fabs(B.cy) > 1e-12 * (B.ax + B.by + B.cz);
+  if (tri && (B.ay != 0.0 || B.az != 0.0 || B.bz != 0.0))
+    bridge_fail("the triclinic box must have a along x and b in the xy plane", 0);
   if (ChargeMethod != NONE && ChargeMethod != EWALD) bridge_fail("charges need the Ewald method", 0);
   if (ChargeMethod == EWALD && (OmitEwaldFourier || fabs(CutOffChargeChargeSquared[s] - CutOffVDWSquared) > 1e-12))
     bridge_fail("Ewald needs its Fourier part and one cut-off for VDW and charges", 0);
@@ -215,6 +222,14 @@ static void bridge_init(void)
   d.box[0] = B.ax;
   d.box[1] = B.by;
   d.box[2] = B.cz;
+  if (tri) {
+    /* the box matrix, row-major, columns a, b, c (Box[], src/framework.c:2025-2040) */
+    const double m[9] = {B.ax, B.bx, B.cx, B.ay, B.by, B.cy, B.az, B.bz, B.cz};
+    for (int i = 0; i < 9; i++) d.cell_matrix[i] = m[i];
+    d.box[0] = sqrt(B.ax * B.ax);
+    d.box[1] = sqrt(B.bx * B.bx + B.by * B.by);
+    d.box[2] = sqrt(B.cx * B.cx + B.cy * B.cy + B.cz * B.cz);
+  }
   d.cutoff = sqrt(CutOffVDWSquared);
   d.beta = Beta[s];
   d.coulomb = COULOMBIC_CONVERSION_FACTOR;

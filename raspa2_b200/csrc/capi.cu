@@ -23,6 +23,7 @@
 #include "../../include/raspa_gpu.h"
 #include "rgpu_engine.h"
 #include "rgpu_chain.h"
+#include "rgpu_device.cuh"
 #include "rgpu_types.h"
 
 static thread_local char g_err[512];
@@ -191,20 +192,66 @@ extern "C" int rgpu_system_destroy(rgpu_system *sys)
   return RGPU_SUCCESS;
 }
 
-/* k-vector list of src/ewald.c:224-259 and the prefactor of :584-591 */
+/* a triclinic description: any element of cell_matrix set */
+static bool desc_triclinic(const rgpu_system_desc *d)
+{
+  for (int i = 0; i < 9; i++)
+    if (d->cell_matrix[i] != 0.0) return true;
+  return false;
+}
+
+/* inverse of the upper-triangular box matrix m (row-major) */
+static void inverse_upper(const double *m, double *v)
+{
+  const double ax = m[0], bx = m[1], cx = m[2], by = m[4], cy = m[5], cz = m[8];
+  for (int i = 0; i < 9; i++) v[i] = 0.0;
+  v[0] = 1.0 / ax;
+  v[1] = -bx / (ax * by);
+  v[2] = (bx * cy - by * cx) / (ax * by * cz);
+  v[4] = 1.0 / by;
+  v[5] = -cy / (by * cz);
+  v[8] = 1.0 / cz;
+}
+
+/* perpendicular widths of the box: volume over the area of each pair of cell vectors */
+static void perpendicular_widths(const double *m, double *w)
+{
+  const double a[3] = {m[0], m[3], m[6]}, b[3] = {m[1], m[4], m[7]}, c[3] = {m[2], m[5], m[8]};
+  auto cross_norm = [](const double *u, const double *v) {
+    const double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2], z = u[0] * v[1] - u[1] * v[0];
+    return sqrt(x * x + y * y + z * z);
+  };
+  const double vol = m[0] * m[4] * m[8];
+  w[0] = vol / cross_norm(b, c);
+  w[1] = vol / cross_norm(c, a);
+  w[2] = vol / cross_norm(a, b);
+}
+
+/* k-vector list of src/ewald.c:224-259 and the prefactor of :584-591
+ * (triclinic: k = 2 pi H^-T n, :560-575) */
 static void kvectors(const rgpu_system_desc *d, std::vector<char4> &kv, std::vector<double> &kf)
 {
   const int kx = d->kmax[0], ky = d->kmax[1], kz = d->kmax[2];
   const int km = std::max(kx, std::max(ky, kz));
   const double rc = (1.05 * km) * (1.05 * km);
-  const double vol = d->box[0] * d->box[1] * d->box[2];
+  const bool tri = desc_triclinic(d);
+  double hinv[9];
+  if (tri) inverse_upper(d->cell_matrix, hinv);
+  const double vol = tri ? d->cell_matrix[0] * d->cell_matrix[4] * d->cell_matrix[8] : d->box[0] * d->box[1] * d->box[2];
   for (int i = 0; i <= kx; i++)
     for (int j = -ky; j <= ky; j++)
       for (int k = -kz; k <= kz; k++) {
         int s = i * i + j * j + k * k;
         if (s == 0 || !(s < rc)) continue;
         kv.push_back(make_char4((signed char)i, (signed char)j, (signed char)k, 0));
-        double rx = 2.0 * M_PI * i / d->box[0], ry = 2.0 * M_PI * j / d->box[1], rz = 2.0 * M_PI * k / d->box[2];
+        double rx, ry, rz;
+        if (!tri) {
+          rx = 2.0 * M_PI * i / d->box[0], ry = 2.0 * M_PI * j / d->box[1], rz = 2.0 * M_PI * k / d->box[2];
+        } else {
+          rx = 2.0 * M_PI * (i * hinv[0] + j * hinv[3] + k * hinv[6]);
+          ry = 2.0 * M_PI * (i * hinv[1] + j * hinv[4] + k * hinv[7]);
+          rz = 2.0 * M_PI * (i * hinv[2] + j * hinv[5] + k * hinv[8]);
+        }
         double k2 = rx * rx + ry * ry + rz * rz;
         double pre = (i == 0 ? 2.0 : 4.0) * M_PI / vol;
         kf.push_back(d->coulomb * pre * exp((-0.25 / (d->alpha * d->alpha)) * k2) / k2);
@@ -271,6 +318,7 @@ static uint64_t checkpoint_fingerprint(const rgpu_system_desc *d)
     h = fnv1a(h, &d->alpha, sizeof d->alpha);
     h = fnv1a(h, d->kmax, sizeof d->kmax);
   }
+  if (desc_triclinic(d)) h = fnv1a(h, d->cell_matrix, sizeof d->cell_matrix);
   h = fnv1a(h, &d->flexible, sizeof d->flexible);
   if (d->flexible) {
     h = fnv1a(h, &d->bond, sizeof d->bond);
@@ -308,8 +356,18 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     return fail(RGPU_E_INVALID, "trial counts must be in [1,%d]", RGPU_MAX_TRIALS);
   if (!d->flexible && d->ntrial * (d->natom - 1) > RGPU_MAX_POS)
     return fail(RGPU_E_INVALID, "ntrial*(natom-1) > %d", RGPU_MAX_POS);
-  for (int c = 0; c < 3; c++)
-    if (!(d->box[c] >= 2.0 * d->cutoff)) return fail(RGPU_E_INVALID, "box length %g < 2*cutoff", d->box[c]);
+  if (desc_triclinic(d)) {
+    const double *m = d->cell_matrix;
+    if (m[3] != 0.0 || m[6] != 0.0 || m[7] != 0.0 || !(m[0] > 0.0) || !(m[4] > 0.0) || !(m[8] > 0.0))
+      return fail(RGPU_E_INVALID, "cell_matrix must be upper triangular with a positive diagonal");
+    double w[3];
+    perpendicular_widths(m, w);
+    for (int c = 0; c < 3; c++)
+      if (!(w[c] >= 2.0 * d->cutoff)) return fail(RGPU_E_INVALID, "perpendicular width %g < 2*cutoff", w[c]);
+  } else {
+    for (int c = 0; c < 3; c++)
+      if (!(d->box[c] >= 2.0 * d->cutoff)) return fail(RGPU_E_INVALID, "box length %g < 2*cutoff", d->box[c]);
+  }
   if (d->ewald && (d->kmax[0] < 1 || d->kmax[1] < 1 || d->kmax[2] < 1 ||
                    std::max(d->kmax[0], std::max(d->kmax[1], d->kmax[2])) > 20))
     return fail(RGPU_E_INVALID, "kmax must be in [1,20]");
@@ -376,6 +434,18 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     h.fix_scale[c] = (float)(d->box[c] / 4294967296.0);
     h.kmax[c] = d->ewald ? d->kmax[c] : 0;
   }
+  const bool tri = desc_triclinic(d);
+  double wperp[3] = {d->box[0], d->box[1], d->box[2]};
+  if (tri) {
+    h.triclinic = 1;
+    for (int i = 0; i < 9; i++) {
+      h.hm[i] = d->cell_matrix[i];
+      h.hmf[i] = (float)(d->cell_matrix[i] / 4294967296.0);
+    }
+    inverse_upper(h.hm, h.hinv);
+    perpendicular_widths(h.hm, wperp);
+    for (int c = 0; c < 3; c++) h.wperp[c] = (float)(wperp[c] * (1.0 - 1e-6));
+  }
   /* Mixed-precision layout: fixed-point coordinates (see rgpu_types.h), the
    * framework cut into tiles of RGPU_TILE spatially close atoms with a bounding box
    * each, by recursive bisection: the atoms of a group are split at the
@@ -394,8 +464,14 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
       seg_of[idx] = sgi;
       const double p[3] = {fw64[idx].x, fw64[idx].y, fw64[idx].z};
       for (int c = 0; c < 3; c++) {
-        double f = p[c] * h.inv_box[c];
-        fr[3 * (size_t)idx + c] = (f - floor(f)) * d->box[c];
+        if (!tri) {
+          double f = p[c] * h.inv_box[c];
+          fr[3 * (size_t)idx + c] = (f - floor(f)) * d->box[c];
+        } else {
+          /* fractional coordinate in lengths of the perpendicular width */
+          double f = rgpu_frac(h, c, p[0], p[1], p[2]);
+          fr[3 * (size_t)idx + c] = (f - floor(f)) * wperp[c];
+        }
       }
     }
     std::vector<int> sp(d->nfw);
@@ -442,7 +518,61 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
     }
     fw32.assign((size_t)ntile * RGPU_TILE, make_int4(0, 0, 0, 0));
     tiles.resize(ntile);
-    for (int o = 0; o < ntile; o++) {
+    for (int o = 0; o < ntile && tri; o++) {
+      /* triclinic tile: fractional extents about the first atom (each
+       * offset wrapped to the nearest integer), the centre in fixed point,
+       * h = fractional half extents, h.w = the Cartesian radius about the
+       * centre */
+      const int t = order[o];
+      const int n = std::min(RGPU_TILE, d->nfw - RGPU_TILE * t);
+      const double4 r0 = fw64[sp[RGPU_TILE * t]];
+      double f0[3], lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+      for (int c = 0; c < 3; c++) f0[c] = rgpu_frac(h, c, r0.x, r0.y, r0.z);
+      double off[RGPU_TILE][3];
+      for (int j = 0; j < n; j++) {
+        const int idx = sp[RGPU_TILE * t + j];
+        int v[3];
+        rgpu_fix3(h, fw64[idx].x, fw64[idx].y, fw64[idx].z, v[0], v[1], v[2]);
+        for (int c = 0; c < 3; c++) {
+          double dd = rgpu_frac(h, c, fw64[idx].x, fw64[idx].y, fw64[idx].z) - f0[c];
+          dd -= floor(dd + 0.5);
+          off[j][c] = dd;
+          lo[c] = std::min(lo[c], dd);
+          hi[c] = std::max(hi[c], dd);
+        }
+        v[2] = (v[2] & ~3) | seg_of[idx];
+        float qf = (float)fw64[idx].w;
+        int qb;
+        memcpy(&qb, &qf, 4);
+        fw32[(size_t)RGPU_TILE * o + j] = make_int4(v[0], v[1], v[2], qb);
+      }
+      double cen[3], half[3], rad = 0.0;
+      for (int c = 0; c < 3; c++) {
+        cen[c] = 0.5 * (lo[c] + hi[c]);
+        half[c] = 0.5 * (hi[c] - lo[c]);
+      }
+      for (int j = 0; j < n; j++) {
+        const double u[3] = {off[j][0] - cen[0], off[j][1] - cen[1], off[j][2] - cen[2]};
+        double r2 = 0.0;
+        for (int r = 0; r < 3; r++) {
+          const double x = h.hm[3 * r] * u[0] + h.hm[3 * r + 1] * u[1] + h.hm[3 * r + 2] * u[2];
+          r2 += x * x;
+        }
+        rad = std::max(rad, sqrt(r2));
+      }
+      float hh[3];
+      int cv[3];
+      for (int c = 0; c < 3; c++) {
+        /* margins for the fixed-point and FP32 rounding */
+        hh[c] = half[c] >= 0.25 ? 0.5f : (float)(half[c] * (1.0 + 1e-6) + 1e-8);
+        cv[c] = rgpu_fix_frac(f0[c] + cen[c]);
+      }
+      TileRec tr;
+      tr.c = make_int4(cv[0], cv[1], cv[2], n);
+      tr.h = make_float4(hh[0], hh[1], hh[2], (float)(rad * (1.0 + 1e-5) + 1e-3));
+      tiles[o] = tr;
+    }
+    for (int o = 0; o < ntile && !tri; o++) {
       const int t = order[o];
       const int n = std::min(RGPU_TILE, d->nfw - RGPU_TILE * t);
       const double4 r0 = fw64[sp[RGPU_TILE * t]];
@@ -934,6 +1064,7 @@ extern "C" int rgpu_system_set_coulomb_grid(rgpu_system *s, const float *d_grid,
                                             const double size[3], const double shift[3], const double cell[3])
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  if (s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   RgpuSys &h = s->h;
   if (!d_grid) {
     if (h.use_grid && h.mol_charged)
@@ -963,6 +1094,7 @@ extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids
                                      const double size[3], const double shift[3], const double cell[3])
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
+  if (s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   RgpuSys &h = s->h;
   if (!d_grids) {
     h.use_grid = 0;
@@ -1076,6 +1208,7 @@ extern "C" int rgpu_total_energy(rgpu_system *s, double *out)
 extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], const double size[3], const double shift[3],
                                float *d_grid)
 {
+  if (s && s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
   if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
   if (type < 0 || type >= s->ntypes) return fail(RGPU_E_INVALID, "type %d", type);
@@ -1097,6 +1230,7 @@ extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], cons
 extern "C" int rgpu_grid_build_coulomb(rgpu_system *s, const int npts[3], const double size[3],
                                        const double shift[3], float *d_grid)
 {
+  if (s && s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
   if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
   if (!s->h.ewald) return fail(RGPU_E_INVALID, "a Coulomb grid needs Ewald summation");

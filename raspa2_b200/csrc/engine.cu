@@ -184,8 +184,9 @@ __device__ __forceinline__ void atom_store(const Eng<MIXED, FLEX> &E, int m, int
   if (MIXED) {
     double *x = E.S->ads_xyz + 3 * idx;
     x[0] = p[0]; x[1] = p[1]; x[2] = p[2];
-    ((int4 *)E.ads)[idx] = make_int4(rgpu_to_fix(p[0], S.inv_box[0]), rgpu_to_fix(p[1], S.inv_box[1]),
-                                     rgpu_to_fix(p[2], S.inv_box[2]), m * 16 + a);
+    int xi, yi, zi;
+    rgpu_fix3(S, p[0], p[1], p[2], xi, yi, zi);
+    ((int4 *)E.ads)[idx] = make_int4(xi, yi, zi, m * 16 + a);
   } else {
     AdsRec64 r;
     r.x = p[0]; r.y = p[1]; r.z = p[2]; r.tag = m * 16 + a;
@@ -575,9 +576,8 @@ __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool
     if (!insert && i == 0) {
       atom_xyz(E, m, sb, p);
     } else {
-      p[0] = S.box[0] * E.rnd[SLOT_FIRST + 3 * i + 2];
-      p[1] = S.box[1] * E.rnd[SLOT_FIRST + 3 * i + 1];
-      p[2] = S.box[2] * E.rnd[SLOT_FIRST + 3 * i + 0];
+      rgpu_box_point(S, E.rnd[SLOT_FIRST + 3 * i + 2], E.rnd[SLOT_FIRST + 3 * i + 1], E.rnd[SLOT_FIRST + 3 * i + 0],
+                     p);
     }
     bead_set(E.pos[i], S, p[0], p[1], p[2], sb, exclude);
   }
@@ -804,8 +804,9 @@ __device__ __forceinline__ void step_reinsert(Eng<MIXED, FLEX> &E)
   const int old_orient = nf + 1;         /* first position of the retrace orientations */
   if (threadIdx.x < nf) {
     const int i = threadIdx.x;
-    bead_set(E.pos[i], S, S.box[0] * E.rnd[SLOT_FIRST + 3 * i + 2], S.box[1] * E.rnd[SLOT_FIRST + 3 * i + 1],
-             S.box[2] * E.rnd[SLOT_FIRST + 3 * i + 0], sb, m);
+    double p[3];
+    rgpu_box_point(S, E.rnd[SLOT_FIRST + 3 * i + 2], E.rnd[SLOT_FIRST + 3 * i + 1], E.rnd[SLOT_FIRST + 3 * i + 0], p);
+    bead_set(E.pos[i], S, p[0], p[1], p[2], sb, m);
   } else if (threadIdx.x == nf) {
     double p[3];
     atom_xyz(E, m, sb, p);
@@ -1314,8 +1315,9 @@ __device__ __forceinline__ void retrace_place(Eng<MIXED, FLEX> &E, int stage, in
       p[1] = old[i][1];
       p[2] = old[i][2];
     } else if (i == 0) {
-      for (int d = 0; d < 3; d++)
-        p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
+      rgpu_box_point(S, rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, 0)),
+                     rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, 1)),
+                     rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, 2)), p);
     } else if (i == 1) {
       const uint64_t stp = E.step;
       chain_trial(S, old, i, [&](int d) { return rgpu_uniform(S.seed, S.sys_id, stp, chain_slot(stage, i, t, d)); },
@@ -1480,8 +1482,9 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
       if (retrace && t == 0) {
         atom_xyz(E, m, i, p);
       } else if (i == 0) {
-        for (int d = 0; d < 3; d++)
-          p[d] = S.box[d] * rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, d));
+        rgpu_box_point(S, rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, 0)),
+                       rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, 1)),
+                       rgpu_uniform(S.seed, S.sys_id, E.step, chain_slot(stage, 0, t, 2)), p);
       } else if (i == 1) {
         const uint64_t step = E.step;
         chain_trial(S, C.cp, i,
@@ -1795,10 +1798,11 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
     for (int i = threadIdx.x; i < C.nads; i += blockDim.x) {
       const int mm = i / S.natom, a = i - mm * S.natom;
       const double *x = S.ads_xyz + 3 * i;
-      if (MIXED)
-        ((int4 *)E.ads)[i] = make_int4(rgpu_to_fix(x[0], S.inv_box[0]), rgpu_to_fix(x[1], S.inv_box[1]),
-                                       rgpu_to_fix(x[2], S.inv_box[2]), mm * 16 + a);
-      else
+      if (MIXED) {
+        int xi, yi, zi;
+        rgpu_fix3(S, x[0], x[1], x[2], xi, yi, zi);
+        ((int4 *)E.ads)[i] = make_int4(xi, yi, zi, mm * 16 + a);
+      } else
         atom_store(E, mm, a, x);
     }
     __syncthreads();
@@ -2092,8 +2096,13 @@ __global__ void k_structure_factor(const RgpuSys *sysp, const double *xyz, const
   char4 kv = S->kvec[k];
   double re = 0.0, im = 0.0;
   for (int i = 0; i < n; i++) {
-    double a = 2.0 * (kv.x * xyz[3 * i] * S->inv_box[0] + kv.y * xyz[3 * i + 1] * S->inv_box[1] +
-                      kv.z * xyz[3 * i + 2] * S->inv_box[2]);
+    const double *x = xyz + 3 * i;
+    double a;
+    if (!S->triclinic)
+      a = 2.0 * (kv.x * x[0] * S->inv_box[0] + kv.y * x[1] * S->inv_box[1] + kv.z * x[2] * S->inv_box[2]);
+    else
+      a = 2.0 * (kv.x * rgpu_frac(*S, 0, x[0], x[1], x[2]) + kv.y * rgpu_frac(*S, 1, x[0], x[1], x[2]) +
+                 kv.z * rgpu_frac(*S, 2, x[0], x[1], x[2]));
     double sn, cs;
     sincospi(a, &sn, &cs);
     re += q[i] * cs;
@@ -2152,7 +2161,12 @@ __global__ void k_upload_sk(const RgpuSys *systems)
   for (int i = 0; i < n; i++) {
     const double *x = S.ads_xyz + 3 * i;
     const double q = S.mol_q[i % S.natom];
-    double a = 2.0 * (kv.x * x[0] * S.inv_box[0] + kv.y * x[1] * S.inv_box[1] + kv.z * x[2] * S.inv_box[2]);
+    double a;
+    if (!S.triclinic)
+      a = 2.0 * (kv.x * x[0] * S.inv_box[0] + kv.y * x[1] * S.inv_box[1] + kv.z * x[2] * S.inv_box[2]);
+    else
+      a = 2.0 * (kv.x * rgpu_frac(S, 0, x[0], x[1], x[2]) + kv.y * rgpu_frac(S, 1, x[0], x[1], x[2]) +
+                 kv.z * rgpu_frac(S, 2, x[0], x[1], x[2]));
     double sn, cs;
     sincospi(a, &sn, &cs);
     re += q * cs;
@@ -2192,8 +2206,9 @@ __global__ void k_build_records(const RgpuSys *sysp, int nads, int4 *rec32, AdsR
   if (i >= nads) return;
   const int m = i / S->natom, a = i - m * S->natom;
   const double x = S->ads_xyz[3 * i], y = S->ads_xyz[3 * i + 1], z = S->ads_xyz[3 * i + 2];
-  rec32[i] = make_int4(rgpu_to_fix(x, S->inv_box[0]), rgpu_to_fix(y, S->inv_box[1]), rgpu_to_fix(z, S->inv_box[2]),
-                       m * 16 + a);
+  int xi, yi, zi;
+  rgpu_fix3(*S, x, y, z, xi, yi, zi);
+  rec32[i] = make_int4(xi, yi, zi, m * 16 + a);
   AdsRec64 r;
   r.x = x; r.y = y; r.z = z; r.tag = m * 16 + a;
   rec64[i] = r;

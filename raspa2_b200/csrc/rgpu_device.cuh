@@ -76,12 +76,76 @@ enum {
 /* NINT of src/utils.h:60 */
 __device__ __forceinline__ double rgpu_nint(double x) { return (double)(int)(x >= 0.0 ? x + 0.5 : x - 0.5); }
 
-__host__ __device__ inline int rgpu_to_fix(double x, double inv_l)
+/* fixed-point form of a fractional coordinate f: f mod 1 in units of 2^-32 */
+__host__ __device__ inline int rgpu_fix_frac(double f)
 {
-  double f = x * inv_l;
   f -= floor(f);
   long long v = (long long)llrint(f * 4294967296.0);
   return (int)(uint32_t)(v & 0xffffffffLL);
+}
+
+__host__ __device__ inline int rgpu_to_fix(double x, double inv_l)
+{
+  return rgpu_fix_frac(x * inv_l);
+}
+
+/* fractional coordinate r (0..2) of the Cartesian point (x, y, z): x_r / L_r
+ * in an orthorhombic box, row r of H^-1 times the point in a triclinic one */
+__host__ __device__ inline double rgpu_frac(const RgpuSys &S, int r, double x, double y, double z)
+{
+  if (!S.triclinic) return (r == 0 ? x : (r == 1 ? y : z)) * S.inv_box[r];
+  return S.hinv[3 * r] * x + S.hinv[3 * r + 1] * y + S.hinv[3 * r + 2] * z;
+}
+
+/* fixed-point fractional coordinates of a Cartesian point */
+__host__ __device__ inline void rgpu_fix3(const RgpuSys &S, double x, double y, double z, int &xi, int &yi, int &zi)
+{
+  if (!S.triclinic) {
+    xi = rgpu_to_fix(x, S.inv_box[0]);
+    yi = rgpu_to_fix(y, S.inv_box[1]);
+    zi = rgpu_to_fix(z, S.inv_box[2]);
+    return;
+  }
+  xi = rgpu_fix_frac(rgpu_frac(S, 0, x, y, z));
+  yi = rgpu_fix_frac(rgpu_frac(S, 1, x, y, z));
+  zi = rgpu_fix_frac(rgpu_frac(S, 2, x, y, z));
+}
+
+/* the point of fractional coordinates (u0, u1, u2) in the box
+ * (ConvertFromABCtoXYZ, src/potentials.c:5548) */
+__host__ __device__ inline void rgpu_box_point(const RgpuSys &S, double u0, double u1, double u2, double *p)
+{
+  if (!S.triclinic) {
+    p[0] = S.box[0] * u0;
+    p[1] = S.box[1] * u1;
+    p[2] = S.box[2] * u2;
+    return;
+  }
+  for (int r = 0; r < 3; r++) p[r] = S.hm[3 * r] * u0 + S.hm[3 * r + 1] * u1 + S.hm[3 * r + 2] * u2;
+}
+
+/* triclinic minimum image of a Cartesian difference (src/potentials.h:246-262) */
+__device__ __forceinline__ void rgpu_min_image_tri(const RgpuSys &S, double &dx, double &dy, double &dz)
+{
+  double t[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const double f = S.hinv[3 * r] * dx + S.hinv[3 * r + 1] * dy + S.hinv[3 * r + 2] * dz;
+    t[r] = f - rgpu_nint(f);
+  }
+  dx = S.hm[0] * t[0] + S.hm[1] * t[1] + S.hm[2] * t[2];
+  dy = S.hm[3] * t[0] + S.hm[4] * t[1] + S.hm[5] * t[2];
+  dz = S.hm[6] * t[0] + S.hm[7] * t[1] + S.hm[8] * t[2];
+}
+
+/* Cartesian difference from fixed-point fractional differences (FP32) */
+__device__ __forceinline__ void rgpu_fix_to_cart_tri(const RgpuSys &S, int ix, int iy, int iz, float &dx, float &dy,
+                                                     float &dz)
+{
+  const float fx = __int2float_rn(ix), fy = __int2float_rn(iy), fz = __int2float_rn(iz);
+  dx = fmaf(S.hmf[0], fx, fmaf(S.hmf[1], fy, S.hmf[2] * fz));
+  dy = fmaf(S.hmf[4], fy, S.hmf[5] * fz);
+  dz = S.hmf[8] * fz;
 }
 
 /* A bead position under evaluation. `atom` is the index of the bead in the
@@ -98,9 +162,7 @@ __device__ __forceinline__ void bead_set(BeadPos &b, const RgpuSys &S, double x,
                                          int excl)
 {
   b.x = x; b.y = y; b.z = z;
-  b.xi = rgpu_to_fix(x, S.inv_box[0]);
-  b.yi = rgpu_to_fix(y, S.inv_box[1]);
-  b.zi = rgpu_to_fix(z, S.inv_box[2]);
+  rgpu_fix3(S, x, y, z, b.xi, b.yi, b.zi);
   b.atom = atom;
   b.excl = excl;
 }
@@ -322,7 +384,9 @@ __device__ __forceinline__ void queue_drain(PairQueue &Q, float &av, float &ac, 
 
 static_assert(RGPU_TILE == 16, "unit_tiles_mixed visits two tiles per warp pass, one per half warp");
 
-/* framework tiles [t0, t1) for bead b, FP32 path (warp-wide) */
+/* framework tiles [t0, t1) for bead b, FP32 path (warp-wide); TRI: the
+ * box is triclinic (S.triclinic) */
+template <bool TRI>
 __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *fw, const TileRec *tiles, int t0, int t1,
                                                  const BeadPos &b, bool check, float &av, float &ac, int &ov,
                                                  int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
@@ -338,6 +402,7 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
   Q.check = check;
   Q.alpha = S.alphaf;
   Q.thr = (float)S.overlap;
+  const bool tri = TRI;
   for (int tb = t0; tb < t1; tb += 32) {
     const int t = tb + lane;
     bool vis = false;
@@ -345,10 +410,32 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
     if (t < t1) {
       const TileRec tr = tiles[t];
       tn = tr.c.w;
-      float dx = fmaxf(fabsf(__int2float_rn(tr.c.x - b.xi) * sx) - tr.h.x, 0.0f);
-      float dy = fmaxf(fabsf(__int2float_rn(tr.c.y - b.yi) * sy) - tr.h.y, 0.0f);
-      float dz = fmaxf(fabsf(__int2float_rn(tr.c.z - b.zi) * sz) - tr.h.z, 0.0f);
-      vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
+      if (!tri) {
+        float dx = fmaxf(fabsf(__int2float_rn(tr.c.x - b.xi) * sx) - tr.h.x, 0.0f);
+        float dy = fmaxf(fabsf(__int2float_rn(tr.c.y - b.yi) * sy) - tr.h.y, 0.0f);
+        float dz = fmaxf(fabsf(__int2float_rn(tr.c.z - b.zi) * sz) - tr.h.z, 0.0f);
+        vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
+      } else {
+        /* triclinic tile: h = fractional half extents, h.w = Cartesian
+         * radius. Every atom's wrapped fractional offset along axis r is at
+         * least |t_r| - h_r, so it lies at least that many perpendicular
+         * widths away; when no atom can wrap differently from the centre
+         * (|t_r| + h_r < 1/2 on every axis), it also lies at least the
+         * centre's distance minus the radius away. */
+        const int ix = tr.c.x - b.xi, iy = tr.c.y - b.yi, iz = tr.c.z - b.zi;
+        const float tx = fabsf(__int2float_rn(ix) * 2.3283064365386963e-10f);
+        const float ty = fabsf(__int2float_rn(iy) * 2.3283064365386963e-10f);
+        const float tz = fabsf(__int2float_rn(iz) * 2.3283064365386963e-10f);
+        const float m = fmaxf(fmaxf((tx - tr.h.x) * S.wperp[0], (ty - tr.h.y) * S.wperp[1]),
+                              (tz - tr.h.z) * S.wperp[2]);
+        vis = !(m > 0.0f && m * m >= rc2);
+        if (vis && tx + tr.h.x < 0.5f && ty + tr.h.y < 0.5f && tz + tr.h.z < 0.5f) {
+          float dx, dy, dz;
+          rgpu_fix_to_cart_tri(S, ix, iy, iz, dx, dy, dz);
+          const float e = fmaxf(sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - tr.h.w, 0.0f);
+          vis = e * e < rc2;
+        }
+      }
     }
     unsigned m = __ballot_sync(RGPU_FULL, vis);
     /* two visible tiles per pass of the warp: lanes 0-15 take the atoms of
@@ -366,9 +453,14 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
       const int mine = half ? i2 : i1, nmine = half ? n2 : n1;
       int4 f = make_int4(0, 0, 0, 0);
       if (hl < nmine) f = fw[(tb + mine) * RGPU_TILE + hl];
-      const float dx = __int2float_rn(f.x - b.xi) * sx;
-      const float dy = __int2float_rn(f.y - b.yi) * sy;
-      const float dz = __int2float_rn(f.z - b.zi) * sz;
+      float dx, dy, dz;
+      if (!tri) {
+        dx = __int2float_rn(f.x - b.xi) * sx;
+        dy = __int2float_rn(f.y - b.yi) * sy;
+        dz = __int2float_rn(f.z - b.zi) * sz;
+      } else {
+        rgpu_fix_to_cart_tri(S, f.x - b.xi, f.y - b.yi, f.z - b.zi, dx, dy, dz);
+      }
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       queue_add(Q, hl < nmine && r2 < rc2, r2, __int_as_float(f.w), f.z & 3, av, ac, ov, nin, nch);
     }
@@ -396,9 +488,13 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
     for (int j = a0 + lane; j < a1; j += 32) {
       double4 f = fw[j];
       double dx = b.x - f.x, dy = b.y - f.y, dz = b.z - f.z;
-      dx -= Lx * rgpu_nint(dx * ix);
-      dy -= Ly * rgpu_nint(dy * iy);
-      dz -= Lz * rgpu_nint(dz * iz);
+      if (!S.triclinic) {
+        dx -= Lx * rgpu_nint(dx * ix);
+        dy -= Ly * rgpu_nint(dy * iy);
+        dz -= Lz * rgpu_nint(dz * iz);
+      } else {
+        rgpu_min_image_tri(S, dx, dy, dz);
+      }
       double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 < rc2) {
         nin++;
@@ -419,6 +515,7 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
   }
 }
 
+template <bool TRI>
 __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo,
                                                int hi, int exclude, bool check, float &av, float &ac, int &ov,
                                                int &nin, int &nch, int &nvis, float *qr2, float *qq, int *qt)
@@ -444,9 +541,14 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
       const int4 f = ads[j];
       if ((f.w >> 4) != exclude) {
         at = f.w & 15;
-        const float dx = __int2float_rn(f.x - b.xi) * sx;
-        const float dy = __int2float_rn(f.y - b.yi) * sy;
-        const float dz = __int2float_rn(f.z - b.zi) * sz;
+        float dx, dy, dz;
+        if (!TRI) {
+          dx = __int2float_rn(f.x - b.xi) * sx;
+          dy = __int2float_rn(f.y - b.yi) * sy;
+          dz = __int2float_rn(f.z - b.zi) * sz;
+        } else {
+          rgpu_fix_to_cart_tri(S, f.x - b.xi, f.y - b.yi, f.z - b.zi, dx, dy, dz);
+        }
         r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         in = r2 < rc2;
         q = S.mol_qf[at];
@@ -475,9 +577,13 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
     if ((tag >> 4) == exclude) continue;
     int at = tag & 15;
     double dx = b.x - f.x, dy = b.y - f.y, dz = b.z - f.z;
-    dx -= Lx * rgpu_nint(dx * ix);
-    dy -= Ly * rgpu_nint(dy * iy);
-    dz -= Lz * rgpu_nint(dz * iz);
+    if (!S.triclinic) {
+      dx -= Lx * rgpu_nint(dx * ix);
+      dy -= Ly * rgpu_nint(dy * iy);
+      dz -= Lz * rgpu_nint(dz * iz);
+    } else {
+      rgpu_min_image_tri(S, dx, dy, dz);
+    }
     double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 < rc2) {
       nin++;
@@ -560,12 +666,20 @@ __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice
     }
     if (MIXED) {
       float av = 0.0f, ac = 0.0f;
-      if (c < pl.cf)
-        unit_tiles_mixed(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
-                         sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
-      else
-        unit_ads_mixed(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
-                       sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
+      if (c < pl.cf) {
+        if (S.triclinic)
+          unit_tiles_mixed<true>(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
+                                 sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
+        else
+          unit_tiles_mixed<false>(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
+                                  sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
+      } else if (S.triclinic) {
+        unit_ads_mixed<true>(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
+                             sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
+      } else {
+        unit_ads_mixed<false>(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
+                              sc.qr2 + 64 * w, sc.qq + 64 * w, sc.qt + 64 * w);
+      }
       e_v = (double)warp_sum(av);
       e_q = (double)warp_sum(ac);
     } else {
@@ -656,8 +770,13 @@ __device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sit
       sincospif(2.0f * turns, &sn, &cs);
       ((float2 *)tab)[i] = make_float2(cs, sn);
     } else {
-      double x = axis == 0 ? b.x : (axis == 1 ? b.y : b.z);
-      double f = x * S.inv_box[axis];
+      double f;
+      if (!S.triclinic) {
+        double x = axis == 0 ? b.x : (axis == 1 ? b.y : b.z);
+        f = x * S.inv_box[axis];
+      } else {
+        f = rgpu_frac(S, axis, b.x, b.y, b.z);
+      }
       double sn, cs;
       sincospi(2.0 * (double)kk * f, &sn, &cs);
       ((double2 *)tab)[i] = make_double2(cs, sn);

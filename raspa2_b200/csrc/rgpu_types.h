@@ -116,6 +116,14 @@ typedef struct RgpuSys {
   /* geometry */
   double box[3], inv_box[3];
   float fix_scale[3];         /* L / 2^32 per axis */
+  /* triclinic box (triclinic = 1): hm = box matrix (columns a, b, c),
+   * hinv its inverse, row-major; hmf = hm / 2^32 in FP32 (Cartesian
+   * difference from fixed-point fractional differences); wperp = the
+   * perpendicular widths (distance between opposite faces) */
+  int triclinic;
+  float wperp[3];
+  double hm[9], hinv[9];
+  float hmf[9];
   float rc2f;
   double rc2;                 /* VDW and real-space cut-off squared (equal) */
   double overlap;             /* EnergyOverlapCriteria */

@@ -58,6 +58,7 @@ class SystemDesc(C.Structure):
         ("seed", C.c_uint64), ("stream_id", C.c_uint32),
         ("flexible", C.c_int), ("bond", C.c_double), ("bend_k", C.c_double), ("bend_theta0", C.c_double),
         ("torsion", C.c_double * 4), ("chain_scheme", C.c_int), ("ntors", C.c_int),
+        ("cell_matrix", C.c_double * 9),
     ]
 
 
@@ -135,6 +136,8 @@ class GpuSystem:
 
         d = SystemDesc()
         d.box[:] = [float(x) for x in sysm.box]
+        if sysm.triclinic:
+            d.cell_matrix[:] = [float(x) for x in sysm.box_matrix.reshape(-1)]
         d.cutoff = sysm.cutoff
         d.beta = units.beta(sysm.temperature)
         d.coulomb = units.COULOMBIC_CONVERSION_FACTOR

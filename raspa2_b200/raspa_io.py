@@ -20,14 +20,16 @@ from .systems import PSEUDO_ATOMS, TYPE_ORDER, System
 
 def write_cif(sys: System, path: str) -> None:
     a, b, c = (float(x) for x in sys.unit_cell)
+    al, be, ga = (float(x) for x in sys.cell_angles)
+    vol = float(np.prod(np.diag(sys.unit_cell_matrix)))
     lines = [
         f"data_{sys.name}", "",
         f"_cell_length_a    {a:.10f}",
         f"_cell_length_b    {b:.10f}",
         f"_cell_length_c    {c:.10f}",
-        "_cell_angle_alpha 90", "_cell_angle_beta  90", "_cell_angle_gamma 90",
-        f"_cell_volume      {a * b * c:.10f}", "",
-        "_symmetry_cell_setting          orthorhombic",
+        f"_cell_angle_alpha {al:.10g}", f"_cell_angle_beta  {be:.10g}", f"_cell_angle_gamma {ga:.10g}",
+        f"_cell_volume      {vol:.10f}", "",
+        f"_symmetry_cell_setting          {'triclinic' if sys.triclinic else 'orthorhombic'}",
         "_symmetry_space_group_name_Hall 'P 1'",
         "_symmetry_space_group_name_H-M  'P 1'",
         "_symmetry_Int_Tables_number     1", "",

@@ -120,7 +120,7 @@ class MoveMix:
 @dataclasses.dataclass
 class System:
     name: str
-    unit_cell: np.ndarray            # (3,) orthorhombic cell lengths, Angstrom
+    unit_cell: np.ndarray            # (3,) cell lengths a, b, c, Angstrom
     unit_cells: np.ndarray           # (3,) replication
     frac: np.ndarray                 # (n_uc, 3) fractional positions in one unit cell
     uc_types: List[str]              # per unit-cell atom
@@ -148,15 +148,67 @@ class System:
     # factor in the weight), 1 = bend angle and dihedral drawn per trial
     chain_scheme: int = 0
     torsion_trials: int = 100          # NumberOfTrialPositionsTorsion
+    # cell angles alpha, beta, gamma in degrees (the CIF's _cell_angle_*);
+    # any angle other than 90 makes the box triclinic
+    cell_angles: tuple = (90.0, 90.0, 90.0)
 
     # ----- derived quantities --------------------------------------------
     @property
     def box(self) -> np.ndarray:
+        """box lengths along the cell vectors (a, b, c times the unit cells)"""
         return self.unit_cell * self.unit_cells
 
     @property
+    def triclinic(self) -> bool:
+        return any(float(x) != 90.0 for x in self.cell_angles)
+
+    def _cell_matrix(self, lengths) -> np.ndarray:
+        """Upper-triangular matrix whose columns are the cell vectors a, b, c
+        for cell lengths `lengths` and the cell angles (src/framework.c:2003-2040)."""
+        al, be, ga = (np.deg2rad(float(x)) for x in self.cell_angles)
+        a, b, c = (float(x) for x in lengths)
+        t = (np.cos(al) - np.cos(ga) * np.cos(be)) / np.sin(ga)
+        return np.array([[a, b * np.cos(ga), c * np.cos(be)],
+                         [0.0, b * np.sin(ga), c * t],
+                         [0.0, 0.0, c * np.sqrt(1.0 - np.cos(be) ** 2 - t * t)]])
+
+    @property
+    def unit_cell_matrix(self) -> np.ndarray:
+        if not self.triclinic:
+            return np.diag(np.asarray(self.unit_cell, float))
+        return self._cell_matrix(self.unit_cell)
+
+    @property
+    def box_matrix(self) -> np.ndarray:
+        """cell vectors of the simulation box as columns"""
+        if not self.triclinic:
+            return np.diag(np.asarray(self.box, float))
+        return self._cell_matrix(self.box)
+
+    @property
     def volume(self) -> float:
-        return float(np.prod(self.box))
+        if not self.triclinic:
+            return float(np.prod(self.box))
+        return float(np.prod(np.diag(self.box_matrix)))
+
+    def box_point(self, u) -> np.ndarray:
+        """the point of fractional coordinates u (..., 3) in the box"""
+        u = np.asarray(u, float)
+        if not self.triclinic:
+            return u * self.box
+        return u @ self.box_matrix.T
+
+    def min_image(self, d) -> np.ndarray:
+        """minimum image of difference vectors d (..., 3): each fractional
+        coordinate wrapped to the nearest integer (ApplyBoundaryCondition,
+        src/potentials.h:232-268)"""
+        d = np.asarray(d, float)
+        if not self.triclinic:
+            return d - self.box * np.rint(d / self.box)
+        h = self.box_matrix
+        s = d @ np.linalg.inv(h).T
+        s -= np.rint(s)
+        return s @ h.T
 
     def framework(self):
         """Cartesian framework atoms of the full simulation box.
@@ -172,11 +224,16 @@ class System:
                 for k in range(int(self.unit_cells[2])):
                     cells.append((i, j, k))
         pos = []
+        hu = self.unit_cell_matrix
         for (i, j, k) in cells:
-            p = np.empty_like(self.frac)
-            p[:, 0] = uc[0] * self.frac[:, 0] + uc[0] * i
-            p[:, 1] = uc[1] * self.frac[:, 1] + uc[1] * j
-            p[:, 2] = uc[2] * self.frac[:, 2] + uc[2] * k
+            if self.triclinic:
+                # the unit cell's atoms, shifted by whole cell vectors
+                p = (self.frac + np.array([i, j, k], float)) @ hu.T
+            else:
+                p = np.empty_like(self.frac)
+                p[:, 0] = uc[0] * self.frac[:, 0] + uc[0] * i
+                p[:, 1] = uc[1] * self.frac[:, 1] + uc[1] * j
+                p[:, 2] = uc[2] * self.frac[:, 2] + uc[2] * k
             pos.append(p)
         pos = np.concatenate(pos, axis=0) if pos else np.zeros((0, 3))
         ncell = len(cells)
@@ -436,6 +493,19 @@ def co2_system(seed: int = 1, n_atoms: int = 1536, cell: float = 25.8,
         kmax=(kmax, kmax, kmax), trials=10, trials_first_bead=10,
         moves=MoveMix(translation=1.0, rotation=1.0, swap_insert=1.0, swap_delete=1.0),
         seed=seed)
+
+
+def co2_triclinic_system(seed: int = 11, n_atoms: int = 2000, cell=(29.0, 28.0, 30.0),
+                         angles=(80.0, 95.0, 110.0)) -> System:
+    """The CO2 model of co2_system in a triclinic cell: lengths `cell`,
+    angles alpha, beta, gamma = `angles` (perpendicular widths 27.2, 26.0 and
+    29.5 A, so one cell holds the 12 A cut-off sphere). The framework's
+    fractional positions are a Poisson-disk set drawn in a cube of the same
+    density, then taken as fractions of the triclinic cell."""
+    base = co2_system(seed=seed, n_atoms=n_atoms, cell=float((n_atoms / 0.0894) ** (1.0 / 3.0)),
+                      name=f"co2tri_s{seed}")
+    return dataclasses.replace(base, unit_cell=np.array(cell, float), unit_cells=np.array([1, 1, 1]),
+                               cell_angles=tuple(float(x) for x in angles))
 
 
 def batched_co2_systems(n: int = 64, seed: int = 2) -> List[System]:

@@ -10,6 +10,7 @@ time needs the reference.
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py coulomb    # only grid_co2_coulomb.json
     python tests/golden/make_golden.py gridfiles  # only grid_co2_files.json + grid_files/
+    python tests/golden/make_golden.py triclinic  # only co2_triclinic.json
 """
 from __future__ import annotations
 
@@ -55,7 +56,7 @@ def random_molecule(rng, sysm, fw, min_d=2.2):
     ref = sysm.molecule.positions
     sb = sysm.molecule.starting_bead
     for _ in range(10000):
-        c = rng.random(3) * sysm.box
+        c = sysm.box_point(rng.random(3))
         q = rng.normal(size=4)
         q /= np.linalg.norm(q)
         a, b, cc, d = q
@@ -63,8 +64,7 @@ def random_molecule(rng, sysm, fw, min_d=2.2):
                       [2*(b*cc+a*d), a*a-b*b+cc*cc-d*d, 2*(cc*d-a*b)],
                       [2*(b*d-a*cc), 2*(cc*d+a*b), a*a-b*b-cc*cc+d*d]])
         x = c + (ref - ref[sb]) @ R.T
-        dd = x[:, None, :] - fw[None, :, :]
-        dd -= sysm.box * np.rint(dd / sysm.box)
+        dd = sysm.min_image(x[:, None, :] - fw[None, :, :])
         if np.min(np.linalg.norm(dd, axis=2)) > min_d:
             return x
     raise RuntimeError("could not place a molecule")
@@ -85,7 +85,7 @@ def energy_case(name, sysm, n_mol, seed, n_points=12, n_moves=8, n_cbmc=4):
         # bead energies at points, for every bead type of the molecule
         pts = []
         for i in range(n_points):
-            p = rng.random(3) * sysm.box
+            p = sysm.box_point(rng.random(3))
             a = int(rng.integers(0, na))
             excl = int(rng.integers(-1, n_mol)) if n_mol else -1
             pts.append((a, p, excl))
@@ -337,6 +337,13 @@ def grid_files_case(seed=1, spacing=2.0):
 def main():
     if not os.path.exists(HARNESS):
         raise SystemExit("build the harness first: make -C oracle ref")
+    if sys.argv[1:] == ["triclinic"]:
+        case = energy_case("co2_triclinic", systems.co2_triclinic_system(), 10, 14)
+        with open(os.path.join(OUT, "co2_triclinic.json"), "w") as fh:
+            json.dump(case, fh)
+        print("co2_triclinic points", len(case["points"]), "moves", len(case["moves"]),
+              "fw diff", case["framework_max_abs_diff_vs_generator"])
+        return
     if sys.argv[1:] == ["gridfiles"]:
         g = grid_files_case()
         with open(os.path.join(OUT, "grid_co2_files.json"), "w") as fh:
@@ -353,6 +360,7 @@ def main():
         "co2_tiny": (systems.tiny_co2_system(), 6, 11),
         "co2_config1": (systems.co2_system(seed=1), 10, 12),
         "methane_config0": (systems.methane_system(seed=0), 8, 13),
+        "co2_triclinic": (systems.co2_triclinic_system(), 10, 14),
     }
     for name, (sysm, nmol, seed) in cases.items():
         case = energy_case(name, sysm, nmol, seed)

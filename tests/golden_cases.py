@@ -12,6 +12,7 @@ BUILDERS = {
     "co2_tiny": lambda seed: systems.tiny_co2_system(),
     "co2_config1": lambda seed: systems.co2_system(seed=seed),
     "methane_config0": lambda seed: systems.methane_system(seed=seed),
+    "co2_triclinic": lambda seed: systems.co2_triclinic_system(seed=seed),
 }
 ENERGY_CASES = list(BUILDERS)
 

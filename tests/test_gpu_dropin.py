@@ -10,7 +10,8 @@ programs take the same decisions: the counter blocks of every move type are
 equal, and the energies they print agree to 1e-9 relative (the GPU sums in
 another order than the CPU, so the last digits differ).
 
-The *_grid cases run with the GRID framework model (UseTabularGrid): the
+co2_triclinic runs in a triclinic cell (angles 80, 95, 110 degrees). The
+*_grid cases run with the GRID framework model (UseTabularGrid): the
 stock program first makes the grids (SimulationType MakeGrid), then both
 programs read them; the bridge reads the same files into device memory
 with the library's grid-file reader. The hexane cases grow flexible chains
@@ -47,6 +48,7 @@ CASES = {
     "co2_config1": (lambda: systems.co2_system(seed=1), 12, None),
     "methane_config0": (lambda: systems.methane_system(seed=0), 12, None),
     "hexane_small": (hexane_small, 12, None),
+    "co2_triclinic": (lambda: systems.co2_triclinic_system(), 12, None),
     "co2_config1_grid": (lambda: systems.co2_system(seed=1), 12, 0.5),
     "methane_config0_grid": (lambda: systems.methane_system(seed=0), 12, 0.5),
     "hexane_small_grid": (hexane_small, 12, 0.5),
