@@ -18,6 +18,7 @@
  *   CalculateInterChargeChargeEnergyDifferenceAdsorbate      src/inter_energy.c:3652
  *   CalculateEwaldFourierAdsorbate                  src/ewald.c:6859
  *   AcceptEwaldAdsorbateMove                        src/ewald.c:11732
+ *   MakeGrid                                        src/grids.c:431
  *
  * The GPU system is built from the reference's globals on the first call
  * (the input has been read and Ewald set up by then). The adsorbate
@@ -63,6 +64,7 @@
 #include "mc_moves.h"
 
 #include "grids.h"
+#include "output.h"
 
 #include <cuda_runtime_api.h>
 
@@ -479,4 +481,102 @@ void __wrap_AcceptEwaldAdsorbateMove(int A)
   const int rc = rgpu_ewald_accept(g_sys);
   if (rc != RGPU_SUCCESS) bridge_fail("rgpu_ewald_accept", rc);
   g_pending_store = -1;
+}
+
+/* MakeGrid (src/grids.c:431-690), the MAKE_GRID simulation type: the VDW
+ * grid of every pseudo-atom of GridTypeList and, with Ewald charges, the
+ * Coulomb grid of a unit charge are built on the GPU (rgpu_grid_build,
+ * rgpu_grid_build_coulomb) over the unit cell, with the reference's point
+ * counts (odd, from the spacings), and written where and as WriteVDWGrid and
+ * WriteCoulombGrid write them (rgpu_grid_write_file). The grids agree with
+ * the reference's to FP32 rounding (the framework sums run in another
+ * order). Orthorhombic cells only (a cubic cell, which the reference marks
+ * triclinic with rounding-size off-diagonal elements, counts as one). */
+static float *bridge_grid_buffer(const int n[3])
+{
+  float *d = NULL;
+  const size_t bytes = sizeof(float) * 8 * (size_t)(n[0] + 1) * (n[1] + 1) * (n[2] + 1);
+  if (cudaMalloc((void **)&d, bytes) != cudaSuccess) bridge_fail("cudaMalloc of a grid", 0);
+  return d;
+}
+
+void __wrap_MakeGrid(void)
+{
+  bridge_init();
+  const int s = CurrentSystem;
+  const REAL_MATRIX3x3 U = UnitCellBox[s];
+  if (fabs(U.bx) + fabs(U.cx) + fabs(U.cy) + fabs(U.ay) + fabs(U.az) + fabs(U.bz) > 1e-12 * (U.ax + U.by + U.cz))
+    bridge_fail("MakeGrid on the GPU: orthorhombic cells only", 0);
+  /* the enclosing box of the unit cell (src/grids.c:336-360) */
+  double size[3] = {0.0, 0.0, 0.0}, shift[3] = {0.0, 0.0, 0.0};
+  const double vec[3][3] = {{U.ax, U.ay, U.az}, {U.bx, U.by, U.bz}, {U.cx, U.cy, U.cz}};
+  for (int v = 0; v < 3; v++)
+    for (int c = 0; c < 3; c++) {
+      size[c] += fabs(vec[v][c]);
+      if (vec[v][c] < 0.0) shift[c] += vec[v][c];
+    }
+  rgpu_grid_file_header h;
+  memset(&h, 0, sizeof h);
+  for (int c = 0; c < 3; c++) {
+    h.size[c] = size[c];
+    h.shift[c] = shift[c];
+  }
+  h.unit_cell[0] = UnitCellSize[s].x;
+  h.unit_cell[1] = UnitCellSize[s].y;
+  h.unit_cell[2] = UnitCellSize[s].z;
+  h.unit_cells[0] = NumberOfUnitCells[s].x;
+  h.unit_cells[1] = NumberOfUnitCells[s].y;
+  h.unit_cells[2] = NumberOfUnitCells[s].z;
+  /* point counts: size / spacing, made odd (:486-492, :588-594) */
+  int n[3];
+  for (int c = 0; c < 3; c++) {
+    n[c] = (int)(size[c] / SpacingVDWGrid);
+    if (n[c] % 2 == 0) n[c]++;
+    h.npts[c] = n[c];
+    h.delta[c] = size[c] / (double)n[c];
+  }
+  NumberOfVDWGridPoints.x = n[0];
+  NumberOfVDWGridPoints.y = n[1];
+  NumberOfVDWGridPoints.z = n[2];
+  h.spacing = SpacingVDWGrid;
+  char path[4096];
+  float *d = bridge_grid_buffer(n);
+  for (int l = 0; l < NumberOfGrids; l++) {
+    const int type = GridTypeList[l];
+    fprintf(OutputFilePtr[s], "Creating grid %d [%s] on the GPU\n", l, PseudoAtoms[type].Name);
+    fflush(OutputFilePtr[s]);
+    int rc = rgpu_grid_build(g_sys, type, n, size, shift, d);
+    if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_build", rc);
+    rc = rgpu_grid_file_path(path, sizeof path, RASPA_DIRECTORY, ForceField, Framework[s].Name[0], SpacingVDWGrid,
+                             PseudoAtoms[type].Name, ShiftPotentials, NULL);
+    if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_file_path", rc);
+    rc = rgpu_grid_write_file(path, 0, &h, d);
+    if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_write_file", rc);
+  }
+  cudaFree(d);
+  if (ChargeMethod != EWALD) {
+    /* the reference's MakeGrid ends the program here without charges (:611-614) */
+    fprintf(stderr, "Skipping the Coulombic grid\n");
+    exit(0);
+  }
+  for (int c = 0; c < 3; c++) {
+    n[c] = (int)(size[c] / SpacingCoulombGrid);
+    if (n[c] % 2 == 0) n[c]++;
+    h.npts[c] = n[c];
+    h.delta[c] = size[c] / (double)n[c];
+  }
+  h.spacing = SpacingCoulombGrid;
+  h.ewald_precision = EwaldPrecision;
+  fprintf(OutputFilePtr[s], "Creating the Ewald-Coulomb grid on the GPU (%d x %d x %d)\n", n[0], n[1], n[2]);
+  fflush(OutputFilePtr[s]);
+  d = bridge_grid_buffer(n);
+  int rc = rgpu_grid_build_coulomb(g_sys, n, size, shift, d);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_build_coulomb", rc);
+  const int nc[3] = {NumberOfUnitCells[s].x, NumberOfUnitCells[s].y, NumberOfUnitCells[s].z};
+  rc = rgpu_grid_file_path(path, sizeof path, RASPA_DIRECTORY, ForceField, Framework[s].Name[0], SpacingCoulombGrid,
+                           NULL, ShiftPotentials, nc);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_file_path", rc);
+  rc = rgpu_grid_write_file(path, 1, &h, d);
+  if (rc != RGPU_SUCCESS) bridge_fail("rgpu_grid_write_file", rc);
+  cudaFree(d);
 }

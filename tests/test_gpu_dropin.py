@@ -120,3 +120,38 @@ def test_reference_program_on_gpu_matches_stock_reference(cuda, case, tmp_path):
     # and the GPU run's running energy agrees with the reference's own
     # recomputation from scratch (its energy-drift check)
     np.testing.assert_allclose(tot_g[-2], tot_g[-1], rtol=RTOL, atol=RTOL * scale)
+
+
+@pytest.mark.parametrize("case,spacing", [("methane_config0", 0.5), ("co2_config1", 1.0)])
+def test_make_grid_on_gpu_writes_the_reference_grid_files(cuda, case, spacing, tmp_path):
+    """SimulationType MakeGrid: simulate_gpu builds the grids on the GPU and
+    writes the same files as the stock program (same paths, headers equal
+    byte for byte, values equal to FP32 rounding of differently ordered
+    framework sums)."""
+    if not (os.path.exists(SIMULATE) and os.path.exists(SIMULATE_GPU)):
+        pytest.skip("reference programs not built (make -C oracle ref dropin)")
+    build, _, _ = CASES[case]
+    s = build()
+    types = sorted({systems.TYPE_ORDER[int(t)] for t in s.molecule_types()})
+    out = {}
+    for name, binary in (("cpu", SIMULATE), ("gpu", SIMULATE_GPU)):
+        d = str(tmp_path / name)
+        raspa_io.write_inputs(s, d, simulation_type="MakeGrid", grid={"types": types, "spacing": spacing})
+        os.makedirs(os.path.join(d, "share", "raspa", "grids"), exist_ok=True)
+        r = subprocess.run([binary, "-i", "simulation.input"], cwd=d, capture_output=True, text=True, timeout=1200,
+                           env=dict(os.environ, RASPA_DIR=d))
+        assert r.returncode == 0, (binary, r.stderr[-2000:])
+        root = os.path.join(d, "share", "raspa", "grids")
+        out[name] = {os.path.relpath(os.path.join(p, f), root): os.path.join(p, f)
+                     for p, _, fs in os.walk(root) for f in fs if f.endswith(".grid")}
+    assert sorted(out["cpu"]) == sorted(out["gpu"]) and len(out["cpu"]) == len(types) + (1 if s.ewald else 0)
+    for rel, fc in out["cpu"].items():
+        coulomb = "Electrostatics" in rel
+        hb = 136 if coulomb else 128
+        with open(fc, "rb") as a, open(out["gpu"][rel], "rb") as b:
+            ba, bb = a.read(), b.read()
+        assert len(ba) == len(bb) and ba[:hb] == bb[:hb], rel
+        va = np.frombuffer(ba, np.float32, offset=hb).astype(np.float64)
+        vb = np.frombuffer(bb, np.float32, offset=hb).astype(np.float64)
+        err = np.abs(va - vb) / (np.abs(va) + 1.0)
+        assert err.max() <= 1e-5, (rel, float(err.max()), int(err.argmax()))
