@@ -284,7 +284,7 @@ __device__ __forceinline__ EvalPlan eval_plan(int P, int nfw, int nads, int nwar
 {
   EvalPlan pl;
   int target = nwarps;
-  int cf = (target + P - 1) / P;
+  int cf = target / P;                /* at most one framework unit per warp */
   int maxcf = (nfw + minitems - 1) / minitems;
   if (cf > maxcf) cf = maxcf;
   if (cf < 1) cf = 1;
