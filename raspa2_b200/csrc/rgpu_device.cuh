@@ -468,7 +468,9 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
   queue_drain(Q, av, ac, ov, nin, nch);
 }
 
-/* framework atoms [lo, hi) of the type-sorted FP64 layout */
+/* framework atoms [lo, hi) of the type-sorted FP64 layout; TRI: the box is
+ * triclinic (S.triclinic) */
+template <bool TRI>
 __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw, const BeadPos &b, int lo,
                                              int hi, bool check, double &av, double &ac, int &ov, int &nin, int &nch,
                                              int &nvis)
@@ -488,7 +490,7 @@ __device__ __forceinline__ void unit_fw_fp64(const RgpuSys &S, const double4 *fw
     for (int j = a0 + lane; j < a1; j += 32) {
       double4 f = fw[j];
       double dx = b.x - f.x, dy = b.y - f.y, dz = b.z - f.z;
-      if (!S.triclinic) {
+      if (!TRI) {
         dx -= Lx * rgpu_nint(dx * ix);
         dy -= Ly * rgpu_nint(dy * iy);
         dz -= Lz * rgpu_nint(dz * iz);
@@ -559,6 +561,7 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
   queue_drain(Q, av, ac, ov, nin, nch);
 }
 
+template <bool TRI>
 __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *ads, const BeadPos &b, int lo,
                                               int hi, int exclude, bool check, double &av, double &ac, int &ov,
                                               int &nin, int &nch, int &nvis)
@@ -577,7 +580,7 @@ __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *
     if ((tag >> 4) == exclude) continue;
     int at = tag & 15;
     double dx = b.x - f.x, dy = b.y - f.y, dz = b.z - f.z;
-    if (!S.triclinic) {
+    if (!TRI) {
       dx -= Lx * rgpu_nint(dx * ix);
       dy -= Ly * rgpu_nint(dy * iy);
       dz -= Lz * rgpu_nint(dz * iz);
@@ -684,10 +687,16 @@ __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice
       e_q = (double)warp_sum(ac);
     } else {
       double av = 0.0, ac = 0.0;
-      if (c < pl.cf)
-        unit_fw_fp64(S, (const double4 *)sl.fw, b, lo, hi, check, av, ac, ov, nin, nch, nvis);
-      else
-        unit_ads_fp64(S, (const AdsRec64 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
+      if (c < pl.cf) {
+        if (S.triclinic)
+          unit_fw_fp64<true>(S, (const double4 *)sl.fw, b, lo, hi, check, av, ac, ov, nin, nch, nvis);
+        else
+          unit_fw_fp64<false>(S, (const double4 *)sl.fw, b, lo, hi, check, av, ac, ov, nin, nch, nvis);
+      } else if (S.triclinic) {
+        unit_ads_fp64<true>(S, (const AdsRec64 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
+      } else {
+        unit_ads_fp64<false>(S, (const AdsRec64 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis);
+      }
       e_v = warp_sum(av);
       e_q = warp_sum(ac);
     }
