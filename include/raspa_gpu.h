@@ -109,8 +109,10 @@ typedef struct {
    * perpendicular width must be >= 2 * cutoff. Distances use the
    * reference's triclinic minimum image (fractional coordinates wrapped to
    * the nearest integer, src/potentials.h:246-262), wave vectors 2 pi H^-T n
-   * (src/ewald.c:560-595). Energy grids are not available in a triclinic
-   * box. */
+   * (src/ewald.c:560-595). Energy grids span the enclosing box of the unit
+   * cell and their lookups wrap a point into the unit cell through its
+   * fractional coordinates (src/grids.c:336-360, :1004-1021); the unit cell
+   * is the box's with the cell lengths passed to the grid calls. */
   double cell_matrix[9];
 } rgpu_system_desc;
 

@@ -72,7 +72,8 @@ double or_real_ewald(const or_sys *s, double qa, double qb, double r)
 static int grid_vdw(const or_sys *s, int type, const double *p, double *e)
 {
   if (!s->grid || !s->grid[type]) return 0;
-  *e = or_grid_interpolate(s->grid[type], s->grid_npts, s->grid_size, s->grid_shift, s->grid_cell, p);
+  *e = or_grid_interpolate_cell(s->grid[type], s->grid_npts, s->grid_size, s->grid_shift, s->grid_cell,
+                                s->grid_tri ? s->grid_ucm : NULL, s->grid_ucinv, p);
   return 1;
 }
 
@@ -81,8 +82,9 @@ static int grid_vdw(const or_sys *s, int type, const double *p, double *e)
 static int grid_coul(const or_sys *s, double q, const double *p, double *e)
 {
   if (!s->coul_grid || !s->ewald) return 0;
-  *e = q == 0.0 ? 0.0 : q * or_grid_interpolate(s->coul_grid, s->coul_npts, s->coul_size, s->coul_shift,
-                                                s->coul_cell, p);
+  *e = q == 0.0 ? 0.0 : q * or_grid_interpolate_cell(s->coul_grid, s->coul_npts, s->coul_size, s->coul_shift,
+                                                     s->coul_cell, s->grid_tri ? s->grid_ucm : NULL,
+                                                     s->grid_ucinv, p);
   return 1;
 }
 
@@ -1248,10 +1250,28 @@ void or_grid_build_coulomb(const or_sys *s, const int npts[3], const double size
 double or_grid_interpolate(const float *grid, const int npts[3], const double size[3],
                            const double shift[3], const double cell[3], const double *pin)
 {
+  return or_grid_interpolate_cell(grid, npts, size, shift, cell, NULL, NULL, pin);
+}
+
+double or_grid_interpolate_cell(const float *grid, const int npts[3], const double size[3], const double shift[3],
+                                const double cell[3], const double *ucm, const double *ucinv, const double *pin)
+{
   double p[3];
-  for (int c = 0; c < 3; c++) {
-    p[c] = pin[c] - cell[c] * nint(pin[c] / cell[c]);
-    if (p[c] < 0.0) p[c] += cell[c];
+  if (!ucm) {
+    /* the RECTANGULAR branch, src/grids.c:995-1002 */
+    for (int c = 0; c < 3; c++) {
+      p[c] = pin[c] - cell[c] * nint(pin[c] / cell[c]);
+      if (p[c] < 0.0) p[c] += cell[c];
+    }
+  } else {
+    /* the TRICLINIC branch, src/grids.c:1004-1021 */
+    double f[3];
+    for (int r = 0; r < 3; r++) {
+      f[r] = ucinv[3 * r] * pin[0] + ucinv[3 * r + 1] * pin[1] + ucinv[3 * r + 2] * pin[2];
+      f[r] -= nint(f[r]);
+      if (f[r] < 0.0) f[r] += 1.0;
+    }
+    for (int r = 0; r < 3; r++) p[r] = ucm[3 * r] * f[0] + ucm[3 * r + 1] * f[1] + ucm[3 * r + 2] * f[2];
   }
   const int nx = npts[0] + 1, ny = npts[1] + 1, nz = npts[2] + 1;
   const size_t plane = (size_t)nx * ny * nz;

@@ -78,6 +78,12 @@ typedef struct {
   /* triclinic box */
   int triclinic;
   double hm[9], hinv[9];
+  /* energy grids of a triclinic unit cell (grid_tri = 1): lookups wrap a
+   * point into the unit cell through its fractional coordinates, with the
+   * unit-cell matrix grid_ucm (columns a, b, c; row-major) and its inverse
+   * (InterpolateVDWGrid, src/grids.c:1004-1021) */
+  int grid_tri;
+  double grid_ucm[9], grid_ucinv[9];
 } or_sys;
 
 /* pair terms */
@@ -146,6 +152,10 @@ void or_grid_derivatives_real(const or_sys *s, const double *p, double *out9);
 /* the Coulomb grid (src/grids.c:586-690), layout as or_grid_build */
 void or_grid_build_coulomb(const or_sys *s, const int npts[3], const double size[3], const double shift[3],
                            float *grid);
+/* as or_grid_interpolate, the point wrapped into a triclinic unit cell
+ * (ucm, ucinv: its matrix and inverse, row-major) when ucm is not NULL */
+double or_grid_interpolate_cell(const float *grid, const int npts[3], const double size[3], const double shift[3],
+                                const double cell[3], const double *ucm, const double *ucinv, const double *p);
 double or_grid_interpolate(const float *grid, const int npts[3], const double size[3],
                            const double shift[3], const double cell[3], const double *p);
 

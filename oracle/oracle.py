@@ -37,6 +37,7 @@ class OrSys(C.Structure):
         ("coul_shift", C.c_double * 3), ("coul_cell", C.c_double * 3),
         ("chain_scheme", C.c_int), ("ntors", C.c_int),
         ("triclinic", C.c_int), ("hm", C.c_double * 9), ("hinv", C.c_double * 9),
+        ("grid_tri", C.c_int), ("grid_ucm", C.c_double * 9), ("grid_ucinv", C.c_double * 9),
     ]
 
 
@@ -77,6 +78,7 @@ def lib():
         L.or_philox_uniform.restype = C.c_double
         L.or_philox_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32]
         L.or_grid_interpolate.restype = C.c_double
+        L.or_grid_interpolate_cell.restype = C.c_double
         L.or_rng_mt.restype = C.c_double
         L.or_intra_energy.restype = C.c_double
         _lib = L
@@ -159,6 +161,12 @@ class Oracle:
                 sysm.molecule.positions, sysm.molecule.starting_bead,
                 ewald=sysm.ewald, alpha=sysm.alpha, kidx=kidx, maxmol=maxmol,
                 cell_matrix=sysm.box_matrix if sysm.triclinic else None)
+        if sysm.triclinic:
+            # grid lookups wrap into the triclinic unit cell
+            u = sysm.unit_cell_matrix
+            o.s.grid_tri = 1
+            o.s.grid_ucm[:] = [float(x) for x in u.reshape(-1)]
+            o.s.grid_ucinv[:] = [float(x) for x in np.linalg.inv(u).reshape(-1)]
         mol = sysm.molecule
         if not mol.rigid:
             s = o.s
@@ -327,15 +335,21 @@ class Oracle:
         return state
 
 
-def grid_interpolate(grid, npts, size, shift, cell, p):
+def grid_interpolate(grid, npts, size, shift, cell, p, cell_matrix=None):
+    """cell_matrix: the unit-cell matrix of a triclinic cell (columns a, b, c)"""
     g = np.ascontiguousarray(grid, np.float32)
     npts = np.ascontiguousarray(npts, np.int32)
     size = np.ascontiguousarray(size, float)
     shift = np.ascontiguousarray(shift, float)
     cell = np.ascontiguousarray(cell, float)
     p = np.ascontiguousarray(p, float)
-    return lib().or_grid_interpolate(g.ctypes.data_as(C.POINTER(C.c_float)), _ptr(npts, _ip),
-                                     _ptr(size), _ptr(shift), _ptr(cell), _ptr(p))
+    if cell_matrix is None:
+        return lib().or_grid_interpolate(g.ctypes.data_as(C.POINTER(C.c_float)), _ptr(npts, _ip),
+                                         _ptr(size), _ptr(shift), _ptr(cell), _ptr(p))
+    m = np.ascontiguousarray(cell_matrix, float)
+    mi = np.ascontiguousarray(np.linalg.inv(m), float)
+    return lib().or_grid_interpolate_cell(g.ctypes.data_as(C.POINTER(C.c_float)), _ptr(npts, _ip), _ptr(size),
+                                          _ptr(shift), _ptr(cell), _ptr(m), _ptr(mi), _ptr(p))
 
 
 def philox_uniform(seed, system, step, slot):

@@ -490,8 +490,7 @@ void __wrap_AcceptEwaldAdsorbateMove(int A)
  * counts (odd, from the spacings), and written where and as WriteVDWGrid and
  * WriteCoulombGrid write them (rgpu_grid_write_file). The grids agree with
  * the reference's to FP32 rounding (the framework sums run in another
- * order). Orthorhombic cells only (a cubic cell, which the reference marks
- * triclinic with rounding-size off-diagonal elements, counts as one). */
+ * order). */
 static float *bridge_grid_buffer(const int n[3])
 {
   float *d = NULL;
@@ -505,8 +504,6 @@ void __wrap_MakeGrid(void)
   bridge_init();
   const int s = CurrentSystem;
   const REAL_MATRIX3x3 U = UnitCellBox[s];
-  if (fabs(U.bx) + fabs(U.cx) + fabs(U.cy) + fabs(U.ay) + fabs(U.az) + fabs(U.bz) > 1e-12 * (U.ax + U.by + U.cz))
-    bridge_fail("MakeGrid on the GPU: orthorhombic cells only", 0);
   /* the enclosing box of the unit cell (src/grids.c:336-360) */
   double size[3] = {0.0, 0.0, 0.0}, shift[3] = {0.0, 0.0, 0.0};
   const double vec[3][3] = {{U.ax, U.ay, U.az}, {U.bx, U.by, U.bz}, {U.cx, U.cy, U.cz}};

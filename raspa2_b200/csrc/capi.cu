@@ -91,6 +91,7 @@ struct rgpu_system {
   double net_ads, pending_dq;
   int grid_type_seg;
   int fw_model;               /* RGPU_FRAMEWORK_FULL or _GRID: the per-call energies' framework terms */
+  double *d_uc;               /* triclinic box: unit-cell matrices of the VDW and Coulomb grids, 2 x 18 doubles */
   uint64_t fingerprint;       /* of the model a checkpoint must match (checkpoint_fingerprint) */
   std::vector<int> fw_seg_type; /* framework pseudo-atom type of each segment */
   std::vector<double> lj_eps, lj_sig2, lj_shift;
@@ -177,7 +178,7 @@ static bool plan_group(const rgpu_engine *e, int lo, int hi, int cluster, Engine
 static void sys_free(rgpu_system *s)
 {
   if (!s) return;
-  void *ptrs[] = {s->d_sys, s->fw64, s->fw32, s->tiles_d, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
+  void *ptrs[] = {s->d_uc, s->d_sys, s->fw64, s->fw32, s->tiles_d, s->kvec, s->kfactor, s->sk_fw, s->sk_ads, s->ds, s->ads_xyz,
                   s->state, s->rec32, s->rec64, s->io_xyz,
                   s->io_out, s->io_q, s->io_atom, s->io_excl, s->io_ov};
   for (void *p : ptrs)
@@ -724,6 +725,7 @@ extern "C" int rgpu_system_create(rgpu_system **out, const rgpu_system_desc *d)
 #define ALLOC(p, n) \
   if (cudaMalloc((void **)&(p), (n)) != cudaSuccess) { sys_free(s); return fail(RGPU_E_CUDA, "cudaMalloc " #p); }
   ALLOC(s->d_sys, sizeof(RgpuSys));
+  if (tri) ALLOC(s->d_uc, sizeof(double) * 36);
   ALLOC(s->fw64, sizeof(double4) * d->nfw);
   ALLOC(s->fw32, sizeof(int4) * RGPU_TILE * (size_t)h.ntile);
   ALLOC(s->tiles_d, sizeof(TileRec) * (size_t)h.ntile);
@@ -1060,11 +1062,47 @@ extern "C" int rgpu_ewald_accept(rgpu_system *s)
 
 static bool grid_covers_cell(const int npts[3], const double size[3], const double shift[3], const double cell[3]);
 
+/* The geometry of a grid of system s: npts, size, shift and the unit-cell
+ * lengths `cell`; in a triclinic box also the unit-cell matrix (the box
+ * matrix's columns scaled to the cell lengths) and its inverse. False when
+ * the grid does not span the unit cell (its enclosing box in a triclinic
+ * one, src/grids.c:336-360). */
+static bool grid_geom_set(rgpu_system *s, int which, RgpuGridGeom &g, const int npts[3], const double size[3],
+                          const double shift[3], const double cell[3])
+{
+  memset(&g, 0, sizeof g);
+  for (int c = 0; c < 3; c++) {
+    g.npts[c] = npts[c];
+    g.size[c] = size[c];
+    g.shift[c] = shift[c];
+    g.cell[c] = cell[c];
+  }
+  if (!s->h.triclinic) return grid_covers_cell(npts, size, shift, cell);
+  g.tri = 1;
+  double uc[18];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) uc[3 * r + c] = s->h.hm[3 * r + c] * (cell[c] / s->d.box[c]);
+  inverse_upper(uc, uc + 9);
+  for (int r = 0; r < 3; r++) {
+    if (npts[r] < 1 || !(size[r] > 0.0) || !(cell[r] > 0.0)) return false;
+    double lo = 0.0, hi = 0.0;
+    for (int c = 0; c < 3; c++) {
+      lo += std::min(0.0, uc[3 * r + c]);
+      hi += std::max(0.0, uc[3 * r + c]);
+    }
+    const double tol = 1e-9 * (hi - lo);
+    if (shift[r] > lo + tol || shift[r] + size[r] < hi - tol) return false;
+  }
+  double *d = s->d_uc + 18 * which;
+  if (cudaMemcpyAsync(d, uc, sizeof uc, cudaMemcpyHostToDevice, s->st) != cudaSuccess) return false;
+  g.uc = d;
+  return true;
+}
+
 extern "C" int rgpu_system_set_coulomb_grid(rgpu_system *s, const float *d_grid, const int npts[3],
                                             const double size[3], const double shift[3], const double cell[3])
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
-  if (s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   RgpuSys &h = s->h;
   if (!d_grid) {
     if (h.use_grid && h.mol_charged)
@@ -1075,13 +1113,9 @@ extern "C" int rgpu_system_set_coulomb_grid(rgpu_system *s, const float *d_grid,
     if (!npts || !size || !shift || !cell) return fail(RGPU_E_INVALID, "bad argument");
     if (!h.ewald) return fail(RGPU_E_INVALID, "a Coulomb grid needs Ewald summation");
     if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "grids must be 16-byte aligned");
-    if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
-    for (int c = 0; c < 3; c++) {
-      h.coul_geom.npts[c] = npts[c];
-      h.coul_geom.size[c] = size[c];
-      h.coul_geom.shift[c] = shift[c];
-      h.coul_geom.cell[c] = cell[c];
-    }
+    RgpuGridGeom g;
+    if (!grid_geom_set(s, 1, g, npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
+    h.coul_geom = g;
     h.coul_grid = d_grid;
     h.use_coul_grid = 1;
   }
@@ -1094,7 +1128,6 @@ extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids
                                      const double size[3], const double shift[3], const double cell[3])
 {
   if (!s) return fail(RGPU_E_INVALID, "bad argument");
-  if (s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   RgpuSys &h = s->h;
   if (!d_grids) {
     h.use_grid = 0;
@@ -1104,18 +1137,14 @@ extern "C" int rgpu_system_set_grids(rgpu_system *s, const float *const *d_grids
     if (!npts || !size || !shift || !cell) return fail(RGPU_E_INVALID, "bad argument");
     if (h.mol_charged && !h.use_coul_grid)
       return fail(RGPU_E_INVALID, "a charged molecule needs a Coulomb grid (rgpu_system_set_coulomb_grid) first");
-    if (!grid_covers_cell(npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
+    RgpuGridGeom g;
+    if (!grid_geom_set(s, 0, g, npts, size, shift, cell)) return fail(RGPU_E_INVALID, "grid does not cover the cell");
     for (int a = 0; a < h.natom; a++) {
       if (!d_grids[a]) return fail(RGPU_E_INVALID, "no grid for molecule atom %d", a);
       if ((uintptr_t)d_grids[a] % 16) return fail(RGPU_E_INVALID, "grids must be 16-byte aligned");
       h.grid[a] = d_grids[a];
     }
-    for (int c = 0; c < 3; c++) {
-      h.grid_geom.npts[c] = npts[c];
-      h.grid_geom.size[c] = size[c];
-      h.grid_geom.shift[c] = shift[c];
-      h.grid_geom.cell[c] = cell[c];
-    }
+    h.grid_geom = g;
     h.use_grid = 1;
   }
   CK(cudaMemcpyAsync(s->d_sys, &h, sizeof(RgpuSys), cudaMemcpyHostToDevice, s->st));
@@ -1208,7 +1237,6 @@ extern "C" int rgpu_total_energy(rgpu_system *s, double *out)
 extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], const double size[3], const double shift[3],
                                float *d_grid)
 {
-  if (s && s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
   if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
   if (type < 0 || type >= s->ntypes) return fail(RGPU_E_INVALID, "type %d", type);
@@ -1230,7 +1258,6 @@ extern "C" int rgpu_grid_build(rgpu_system *s, int type, const int npts[3], cons
 extern "C" int rgpu_grid_build_coulomb(rgpu_system *s, const int npts[3], const double size[3],
                                        const double shift[3], float *d_grid)
 {
-  if (s && s->h.triclinic) return fail(RGPU_E_INVALID, "energy grids are not available in a triclinic box");
   if (!s || !npts || !size || !shift || !d_grid) return fail(RGPU_E_INVALID, "bad argument");
   if ((uintptr_t)d_grid % 16) return fail(RGPU_E_INVALID, "d_grid must be 16-byte aligned");
   if (!s->h.ewald) return fail(RGPU_E_INVALID, "a Coulomb grid needs Ewald summation");

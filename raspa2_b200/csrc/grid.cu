@@ -20,6 +20,7 @@
  */
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 
 #include <algorithm>
 
@@ -84,11 +85,17 @@ __global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp
     int seg = 0;
     if (a < S.nfw) {
       f = S.fw64[a];
-      double dx = cx - f.x, dy = cy - f.y, dz = cz - f.z;
-      dx -= Lx * rgpu_nint(dx * ix);
-      dy -= Ly * rgpu_nint(dy * iy);
-      dz -= Lz * rgpu_nint(dz * iz);
-      keep = dx * dx + dy * dy + dz * dz < rcut2;
+      if (S.triclinic) {
+        /* a triclinic box: every atom is staged (its minimum image may
+         * differ across the tile's points near half a cell vector) */
+        keep = 1;
+      } else {
+        double dx = cx - f.x, dy = cy - f.y, dz = cz - f.z;
+        dx -= Lx * rgpu_nint(dx * ix);
+        dy -= Ly * rgpu_nint(dy * iy);
+        dz -= Lz * rgpu_nint(dz * iz);
+        keep = dx * dx + dy * dy + dz * dz < rcut2;
+      }
       while (seg + 1 < S.nseg && a >= S.seg_start[seg + 1]) seg++;
     }
     unsigned m = __ballot_sync(RGPU_FULL, keep);
@@ -110,9 +117,13 @@ __global__ void __launch_bounds__(GRID_THREADS) k_grid_build(const RgpuSys *sysp
       for (int q = 0; q < nsel; q++) {
         const double4 g = fwc[q];
         double dx = px - g.x, dy = py - g.y, dz = pz - g.z;
-        dx -= Lx * rgpu_nint(dx * ix);
-        dy -= Ly * rgpu_nint(dy * iy);
-        dz -= Lz * rgpu_nint(dz * iz);
+        if (S.triclinic) {
+          rgpu_min_image_tri(S, dx, dy, dz);
+        } else {
+          dx -= Lx * rgpu_nint(dx * ix);
+          dy -= Ly * rgpu_nint(dy * iy);
+          dz -= Lz * rgpu_nint(dz * iz);
+        }
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < S.rc2) {
           double U, DF, DDF, DDDF;
@@ -221,6 +232,7 @@ cudaError_t rgpu_grid_interp_launch(const float *d_grid, const int npts[3], cons
                                     double *d_out, cudaStream_t st)
 {
   RgpuGridGeom ip;
+  memset(&ip, 0, sizeof ip);   /* a rectangular cell (tri = 0) */
   for (int c = 0; c < 3; c++) {
     ip.npts[c] = npts[c];
     ip.size[c] = size[c];

@@ -5,12 +5,40 @@
  * and the third mixed derivative, scaled to the grid cell). The interpolant
  * is the Hermite tensor product of those values at the 8 corners of the
  * cell holding the point, the same polynomial as the reference's 64 x 64
- * coefficient product. Points are wrapped into the unit cell the grid spans.
+ * coefficient product. Points are wrapped into the unit cell the grid spans
+ * (rgpu_grid_wrap).
  */
 #ifndef RGPU_GRID_CUH
 #define RGPU_GRID_CUH
 
 #include "rgpu_types.h"
+
+/* the point wrapped into the unit cell the grid spans: per axis in a
+ * rectangular cell (src/grids.c:995-1002), through the fractional
+ * coordinates in a triclinic one (:1004-1021) */
+__device__ __forceinline__ void rgpu_grid_wrap(const RgpuGridGeom &ip, const double *xyz, double *pw)
+{
+  if (!ip.tri) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double p = xyz[c];
+      p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
+      if (p < 0.0) p += ip.cell[c];
+      pw[c] = p;
+    }
+    return;
+  }
+  const double *m = ip.uc, *v = ip.uc + 9;
+  double f[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    f[r] = __ldg(v + 3 * r) * xyz[0] + __ldg(v + 3 * r + 1) * xyz[1] + __ldg(v + 3 * r + 2) * xyz[2];
+    f[r] -= rgpu_nint(f[r]);
+    if (f[r] < 0.0) f[r] += 1.0;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; r++) pw[r] = __ldg(m + 3 * r) * f[0] + __ldg(m + 3 * r + 1) * f[1] + __ldg(m + 3 * r + 2) * f[2];
+}
 
 /* Cubic Hermite basis on [0,1]: {p0, p1, slope0, slope1} */
 __device__ __forceinline__ void rgpu_hermite(double t, double *h)
@@ -29,10 +57,10 @@ __device__ __forceinline__ double rgpu_grid_value(const float *grid, const RgpuG
   const int ny = ip.npts[1] + 1, nz = ip.npts[2] + 1;
   double r[3];
   int i0[3];
+  double pw[3];
+  rgpu_grid_wrap(ip, xyz, pw);
   for (int c = 0; c < 3; c++) {
-    double p = xyz[c];
-    p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
-    if (p < 0.0) p += ip.cell[c];
+    const double p = pw[c];
     const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
     /* a point on the upper cell face (p == cell after wrapping) uses the last
      * grid cell at r = 1, so the 2x2x2 corner block stays inside the grid */
@@ -88,10 +116,10 @@ __device__ __forceinline__ double rgpu_grid_value8(const float *grid, const Rgpu
     const int ny = ip.npts[1] + 1, nz = ip.npts[2] + 1;
     double r[3];
     int i0[3];
+    double pw[3];
+    rgpu_grid_wrap(ip, xyz, pw);
     for (int c = 0; c < 3; c++) {
-      double p = xyz[c];
-      p -= ip.cell[c] * rgpu_nint(p / ip.cell[c]);
-      if (p < 0.0) p += ip.cell[c];
+      const double p = pw[c];
       const double s = ((p - ip.shift[c]) / ip.size[c]) * (double)ip.npts[c];
       i0[c] = min(max((int)s, 0), ip.npts[c] - 1);
       r[c] = s - i0[c];

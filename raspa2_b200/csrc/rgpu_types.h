@@ -105,11 +105,14 @@ typedef struct {
 } TileRec;
 
 /* geometry of an energy grid: npts cells per axis over `size` from `shift`,
- * spanning a unit cell of lengths `cell` */
+ * spanning a unit cell of lengths `cell`; a triclinic unit cell (tri = 1)
+ * has its matrix (columns a, b, c; row-major) and then its inverse in
+ * device memory at uc[0..17] */
 typedef struct {
   int npts[3];
-  int pad;
+  int tri;
   double size[3], shift[3], cell[3];
+  const double *uc;
 } RgpuGridGeom;
 
 typedef struct RgpuSys {

@@ -274,7 +274,7 @@ class GpuSystem:
 
     def use_energy_grids(self, spacing: float, like: Optional["GpuSystem"] = None):
         """Builds one energy grid per pseudo-atom type of the molecule over the
-        (orthorhombic) unit cell, int(size / spacing) intervals per axis,
+        unit cell (a triclinic cell: over its enclosing box), int(size / spacing) intervals per axis,
         made odd, as MakeGrid counts them from SpacingVDWGrid
         (src/grids.c:486-492), in device memory
         this object keeps, and switches the engine's host VDW energies to
@@ -283,9 +283,16 @@ class GpuSystem:
         built. Returns the grid geometry (npts, size, shift, cell)."""
         import torch
         uc = np.asarray(self.sysm.unit_cell, float)
-        npts = (uc / spacing).astype(np.int32)
+        if self.sysm.triclinic:
+            # the enclosing box of the unit cell (src/grids.c:336-360)
+            m = self.sysm.unit_cell_matrix
+            size = np.abs(m).sum(axis=1)
+            shift = np.minimum(m, 0.0).sum(axis=1)
+        else:
+            size = uc
+            shift = np.zeros(3)
+        npts = (size / spacing).astype(np.int32)
         npts += npts % 2 == 0
-        shift = np.zeros(3)
         n = int(np.prod(npts.astype(np.int64) + 1)) * 8
         types = [int(t) for t in self.sysm.molecule_types()]
         if like is not None:
@@ -301,27 +308,27 @@ class GpuSystem:
             for t in sorted(set(types)):
                 buf = torch.empty(n, dtype=torch.float32, device="cuda")
                 torch.cuda.synchronize()
-                self.grid_build(t, npts, uc, shift, buf.data_ptr())
+                self.grid_build(t, npts, size, shift, buf.data_ptr())
                 bufs[t] = buf
             if np.any(self.sysm.molecule.charges() != 0.0):
                 # the Coulomb grid: odd point counts as well (src/grids.c:588-594)
                 nc = npts.copy()
                 buf = torch.empty(int(np.prod(nc.astype(np.int64) + 1)) * 8, dtype=torch.float32, device="cuda")
                 torch.cuda.synchronize()
-                self.grid_build_coulomb(nc, uc, shift, buf.data_ptr())
+                self.grid_build_coulomb(nc, size, shift, buf.data_ptr())
                 bufs["coulomb"] = (buf, nc)
         self._grids = bufs
-        self._grid_geom = (npts, uc, shift, uc)
+        self._grid_geom = (npts, size, shift, uc)
         self._apply_grids()
         return self._grid_geom
 
     def _apply_grids(self):
         types = [int(t) for t in self.sysm.molecule_types()]
-        npts, uc, shift, cell = self._grid_geom
+        npts, size, shift, cell = self._grid_geom
         if "coulomb" in self._grids:
             buf, nc = self._grids["coulomb"]
-            self.set_coulomb_grid(buf.data_ptr(), nc, uc, shift, cell)
-        self.set_grids([self._grids[t].data_ptr() for t in types], npts, uc, shift, cell)
+            self.set_coulomb_grid(buf.data_ptr(), nc, size, shift, cell)
+        self.set_grids([self._grids[t].data_ptr() for t in types], npts, size, shift, cell)
 
     def share_grids_of(self, other: "GpuSystem"):
         """Uses the grids `other` uses (a system of the same framework and

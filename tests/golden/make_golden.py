@@ -11,6 +11,7 @@ time needs the reference.
     python tests/golden/make_golden.py coulomb    # only grid_co2_coulomb.json
     python tests/golden/make_golden.py gridfiles  # only grid_co2_files.json + grid_files/
     python tests/golden/make_golden.py triclinic  # only co2_triclinic.json
+    python tests/golden/make_golden.py gridtri    # only grid_co2_triclinic.json
 """
 from __future__ import annotations
 
@@ -334,9 +335,58 @@ def grid_files_case(seed=1, spacing=2.0):
     }
 
 
+def grid_triclinic_case(seed=11, spacing=1.0):
+    """MakeGrid in the triclinic CO2 cell (co2_triclinic_system): the VDW
+    grids of C_co2 and O_co2 and the Ewald Coulomb grid as the reference
+    writes them (samples and plane sums), and the reference's
+    InterpolateVDWGrid / InterpolateCoulombGrid (their TRICLINIC branches)
+    at points anywhere in and around the box."""
+    sysm = systems.co2_triclinic_system(seed=seed)
+    rng = np.random.default_rng(seed + 399)
+    types = ["C_co2", "O_co2"]
+    with tempfile.TemporaryDirectory() as d:
+        grid = {"types": types, "spacing": spacing}
+        raspa_io.write_inputs(sysm, d, simulation_type="MakeGrid", grid=grid)
+        os.makedirs(os.path.join(d, "share", "raspa", "grids"), exist_ok=True)
+        run_harness(d, ["makegrid"])
+        base = os.path.join(d, "share", "raspa", "grids", "Local", sysm.name, f"{spacing:.6f}")
+        files = {t: os.path.join(base, f"{sysm.name}_{t}_shifted.grid") for t in types}
+        files["coulomb"] = os.path.join(base, "1x1x1", f"{sysm.name}_Electrostatics_Ewald.grid")
+        meta, samples, sums = {}, {}, {}
+        for k, f in files.items():
+            m, g = read_coulomb_grid_file(f) if k == "coulomb" else read_grid_file(f)
+            flat = g.reshape(8, -1)
+            sel = rng.integers(0, flat.shape[1], 64)
+            meta[k] = m
+            samples[k] = {"index": sel.tolist(), "values": flat[:, sel].T.astype(float).tolist()}
+            sums[k] = {"sum": [float(np.sum(flat[q].astype(np.float64))) for q in range(8)],
+                       "abs": [float(np.sum(np.abs(flat[q].astype(np.float64)))) for q in range(8)]}
+        grid["use"] = True
+        raspa_io.write_inputs(sysm, d, simulation_type="MonteCarlo", grid=grid)
+        q = sysm.box_point(rng.random((24, 3)) * 1.4 - 0.2)
+        cmds = []
+        for name in types:
+            t = systems.TYPE_ORDER.index(name)
+            cmds += [f"interp {t + 1} {fmt(p)}" for p in q] + [f"interpc {t + 1} {fmt(p)}" for p in q]
+        rows = run_harness(d, cmds)
+    vals = [float(r[1]) for r in rows if r[0] in ("interp", "interpc")]
+    n = len(q)
+    interp = {name: {"vdw": vals[2 * i * n: (2 * i + 1) * n], "coulomb": vals[(2 * i + 1) * n: (2 * i + 2) * n]}
+              for i, name in enumerate(types)}
+    return {"name": "grid_co2_triclinic", "system": {"builder": "co2_triclinic", "seed": seed},
+            "spacing": spacing, "types": types, "meta": meta, "samples": samples, "plane_sums": sums,
+            "points": q.tolist(), "interp_ref": interp}
+
+
 def main():
     if not os.path.exists(HARNESS):
         raise SystemExit("build the harness first: make -C oracle ref")
+    if sys.argv[1:] == ["gridtri"]:
+        g = grid_triclinic_case()
+        with open(os.path.join(OUT, "grid_co2_triclinic.json"), "w") as fh:
+            json.dump(g, fh)
+        print("triclinic grids", {k: v["n"] for k, v in g["meta"].items()})
+        return
     if sys.argv[1:] == ["triclinic"]:
         case = energy_case("co2_triclinic", systems.co2_triclinic_system(), 10, 14)
         with open(os.path.join(OUT, "co2_triclinic.json"), "w") as fh:

@@ -49,6 +49,7 @@ CASES = {
     "methane_config0": (lambda: systems.methane_system(seed=0), 12, None),
     "hexane_small": (hexane_small, 12, None),
     "co2_triclinic": (lambda: systems.co2_triclinic_system(), 12, None),
+    "co2_triclinic_grid": (lambda: systems.co2_triclinic_system(), 12, 1.0),
     "co2_config1_grid": (lambda: systems.co2_system(seed=1), 12, 0.5),
     "methane_config0_grid": (lambda: systems.methane_system(seed=0), 12, 0.5),
     "hexane_small_grid": (hexane_small, 12, 0.5),
@@ -122,7 +123,7 @@ def test_reference_program_on_gpu_matches_stock_reference(cuda, case, tmp_path):
     np.testing.assert_allclose(tot_g[-2], tot_g[-1], rtol=RTOL, atol=RTOL * scale)
 
 
-@pytest.mark.parametrize("case,spacing", [("methane_config0", 0.5), ("co2_config1", 1.0)])
+@pytest.mark.parametrize("case,spacing", [("methane_config0", 0.5), ("co2_config1", 1.0), ("co2_triclinic", 1.0)])
 def test_make_grid_on_gpu_writes_the_reference_grid_files(cuda, case, spacing, tmp_path):
     """SimulationType MakeGrid: simulate_gpu builds the grids on the GPU and
     writes the same files as the stock program (same paths, headers equal
