@@ -1094,7 +1094,9 @@ static bool grid_geom_set(rgpu_system *s, int which, RgpuGridGeom &g, const int 
     if (shift[r] > lo + tol || shift[r] + size[r] < hi - tol) return false;
   }
   double *d = s->d_uc + 18 * which;
-  if (cudaMemcpyAsync(d, uc, sizeof uc, cudaMemcpyHostToDevice, s->st) != cudaSuccess) return false;
+  if (cudaMemcpyAsync(d, uc, sizeof uc, cudaMemcpyHostToDevice, s->st) != cudaSuccess ||
+      cudaStreamSynchronize(s->st) != cudaSuccess)
+    return false;
   g.uc = d;
   return true;
 }
