@@ -520,6 +520,13 @@ def run_ours(args):
     line["precision"] = {"co2_batched": energy_error(gs, sys_list)}
     if rank == 0 and world == 1 and not args.no_plain and prec == native.RGPU_MIXED:
         line["batched_fp64"] = batched_fp64_run(native, stream, gs, sys_list, args, peak)
+        # the mixed engine and its variant with FP64 real-space charge-charge
+        # terms over the same number of moves from the same anchored start:
+        # their moves/s and the error their running energies accumulate
+        for key, p in (("batched_mixed_cc64", native.RGPU_MIXED_CC64), ("batched_mixed_anchored", native.RGPU_MIXED)):
+            line[key] = batched_fp64_run(native, stream, gs, sys_list, args, peak, steps=args.steps, precision=p)
+        line["precision"]["co2_batched_cc64"] = line["batched_mixed_cc64"]["energy_error"]
+        line["precision"]["co2_batched_mixed_anchored"] = line["batched_mixed_anchored"]["energy_error"]
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_gpu"] = plain_gpu_rate(native, stream)
         # the two single-system configurations, each on its own
@@ -670,19 +677,22 @@ def hexane_grid_run(args, stream, steps=3, warmup=3):
     return out
 
 
-def batched_fp64_run(native, stream, gs, sys_list, args, peak, steps=3):
+def batched_fp64_run(native, stream, gs, sys_list, args, peak, steps=3, precision=None):
     """The same batch of systems on the FP64 engine (the plain path's
-    arithmetic: FP64 pair terms, erfc and S(k)), from the mixed run's final
-    configurations, at its own autotuned launch shape: device-timed moves/s
-    and the error of its running energies against the FP64 recomputation."""
+    arithmetic: FP64 pair terms, erfc and S(k)), or on the engine of
+    `precision`, from the mixed run's final configurations with every
+    running energy set to an FP64 recomputation, at its own autotuned launch
+    shape: device-timed moves/s and the error of its running energies
+    against the FP64 recomputation after the `steps` timed steps."""
     import torch
     from raspa2_b200 import autotune
+    precision = native.RGPU_FP64 if precision is None else precision
     g64 = [native.GpuSystem(s, maxmol=args.maxmol, seed=777, stream_id=i) for i, s in enumerate(sys_list)]
     for g, src in zip(g64, gs):
         g.set_adsorbates(src.adsorbates())
         g.set_energy(list(g.total_energy()) + [0.0, 0.0])
-    tuned = autotune.tune(g64, precision=native.RGPU_FP64, moves=300, warm=50)
-    e = tuned.engine(g64, native.RGPU_FP64)
+    tuned = autotune.tune(g64, precision=precision, moves=300, warm=50)
+    e = tuned.engine(g64, precision)
     c0 = np.array([g.state()["counters"] for g in g64])
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for k in range(steps):

@@ -36,6 +36,9 @@ extern "C" {
 /* precision of a call */
 #define RGPU_FP64 0            /* FP64 throughout (the reference's REAL) */
 #define RGPU_MIXED 1           /* FP32 pair terms / FP64 sums and S(k) */
+#define RGPU_MIXED_CC64 2      /* as RGPU_MIXED, with each pair's distance, cut-off test and
+                                * real-space charge-charge term in FP64 (rgpu_engine_create
+                                * only; rigid molecules without energy grids) */
 
 typedef struct rgpu_system rgpu_system;
 typedef struct rgpu_engine rgpu_engine;
@@ -319,8 +322,8 @@ int rgpu_system_set_framework_model(rgpu_system *sys, int model);
 /* Groups systems for one persistent launch; each system is advanced by one
  * thread-block cluster of `cluster` CTAs (1 to 8; 0 chooses from the
  * number of systems and SMs) that split its framework between them.
- * `threads` = CTA size, a multiple of 32 in 64..1024 (RGPU_MIXED) or
- * 64..512 (RGPU_FP64). */
+ * `threads` = CTA size, a multiple of 32 in 64..1024 (RGPU_MIXED,
+ * RGPU_MIXED_CC64) or 64..512 (RGPU_FP64). */
 int rgpu_engine_create(rgpu_engine **out, rgpu_system *const *systems, int n, int precision, int threads,
                        int cluster);
 /* As rgpu_engine_create, with the shared memory and registers of each CTA

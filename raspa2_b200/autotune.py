@@ -81,14 +81,15 @@ def candidates(nsys: int, precision: int, sms: int) -> List[Tuple[int, int, int]
     CTAs do not all fit the SMs at once runs in waves and is skipped; several
     CTAs per SM need the 64-register build (mixed precision) and at most
     1024 threads per SM between them."""
-    threads = (256, 512, 1024) if precision == native.RGPU_MIXED else (128, 256, 512)
+    mixed = precision != native.RGPU_FP64
+    threads = (256, 512, 1024) if mixed else (128, 256, 512)
     out = []
     for c in (1, 2, 4, 8):
         if nsys * c > sms and c > 1:
             continue
         for t in threads:
             out.append((c, t, 1))
-    if precision == native.RGPU_MIXED:
+    if mixed:
         for occ in (2, 4):
             for c in (2, 4, 8):
                 if nsys * c > sms * occ or nsys * c <= sms:

@@ -1584,23 +1584,24 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
 {
   if (!out || !systems || n < 1) return fail(RGPU_E_INVALID, "bad argument");
   if (ctas_per_sm < 1 || ctas_per_sm > 4) return fail(RGPU_E_INVALID, "ctas_per_sm %d outside [1,4]", ctas_per_sm);
-  if (precision != RGPU_FP64 && precision != RGPU_MIXED) return fail(RGPU_E_INVALID, "precision");
-  /* the mixed kernel is compiled for up to 1024 threads (64 registers), the
+  if (precision != RGPU_FP64 && precision != RGPU_MIXED && precision != RGPU_MIXED_CC64)
+    return fail(RGPU_E_INVALID, "precision");
+  /* the mixed kernels are compiled for up to 1024 threads (64 registers), the
    * FP64 one for up to 512 */
-  const int max_threads = precision == RGPU_MIXED ? 1024 : 512;
+  const int max_threads = precision != RGPU_FP64 ? 1024 : 512;
   if (threads < 64 || threads > max_threads || threads % 32)
     return fail(RGPU_E_INVALID, "threads %d outside [64,%d] or not a multiple of 32", threads, max_threads);
   if (cluster < 0 || cluster > 8) return fail(RGPU_E_INVALID, "cluster %d", cluster);
   /* registers: 128 per thread (the narrow build) unless the CTAs of an SM
    * need more than 65536 together; then the mixed kernel's 64-register build */
   const bool wide = threads > 512 || (long long)threads * 128 * ctas_per_sm > 65536;
-  if (wide && precision != RGPU_MIXED)
+  if (wide && precision == RGPU_FP64)
     return fail(RGPU_E_INVALID, "FP64 engine: %d CTAs of %d threads do not fit one SM", ctas_per_sm, threads);
   if ((long long)threads * 64 * ctas_per_sm > 65536)
     return fail(RGPU_E_INVALID, "%d CTAs of %d threads do not fit one SM", ctas_per_sm, threads);
   *out = nullptr;
   rgpu_engine *e = new rgpu_engine();
-  e->mixed = precision == RGPU_MIXED;
+  e->mixed = precision;     /* 0 FP64, 1 mixed, 2 mixed with FP64 charge-charge terms */
   e->threads = threads;
   e->wide = wide;
   e->flex = false;
@@ -1617,6 +1618,10 @@ extern "C" int rgpu_engine_create_ex(rgpu_engine **out, rgpu_system *const *syst
       return fail(RGPU_E_INVALID, "system with VDW grids and a charged molecule but no Coulomb grid");
     }
     e->flex = e->flex || s->h.use_grid || s->h.flexible;
+    if (e->flex && precision == RGPU_MIXED_CC64) {
+      delete e;
+      return fail(RGPU_E_INVALID, "RGPU_MIXED_CC64 covers rigid molecules without energy grids");
+    }
     e->kw = std::max(e->kw, s->kw);
     e->max_ads = std::max(e->max_ads, s->d.maxmol * s->d.natom);
   }

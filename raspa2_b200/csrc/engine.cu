@@ -77,7 +77,8 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   L.uc = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(double));
   L.uo = o; o = rgpu_align(o + RGPU_MAX_UNITS * sizeof(int));
   L.part = o; o = rgpu_align(o + 2 * RGPU_MAX_POS * sizeof(PosSum));   /* double-buffered */
-  L.q = o; o = rgpu_align(o + (mixed ? (size_t)nwarps * 64 * 12 : 0));     /* per-warp pair queues */
+  /* per-warp pair queues: r2 (FP32, or FP64 for mixed = 2), charge, type */
+  L.q = o; o = rgpu_align(o + (mixed ? (size_t)nwarps * 64 * (mixed == 2 ? 16 : 12) : 0));
   L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
   L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed ? sizeof(float2) : sizeof(double2)));
   L.red = o; o = rgpu_align(o + 2 * 2 * RGPU_MAX_WARPS * sizeof(double));
@@ -136,7 +137,7 @@ struct Ctl {
 };
 static_assert(sizeof(Ctl) <= RGPU_CTL_BYTES, "control block exceeds its shared-memory slot");
 
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 struct Eng {
   RgpuSys *S;
   EvalSlice sl;
@@ -163,7 +164,7 @@ struct Eng {
 /* Position of atom a of molecule m. FP64 records carry the position; on the
  * mixed path the FP64 positions stay in global memory (ads_xyz), which every
  * CTA of the cluster writes with the same values on each accepted move. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void atom_xyz(const Eng<MIXED, FLEX> &E, int m, int a, double *p)
 {
   const int idx = m * E.S->natom + a;
@@ -176,7 +177,7 @@ __device__ __forceinline__ void atom_xyz(const Eng<MIXED, FLEX> &E, int m, int a
   }
 }
 
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void atom_store(const Eng<MIXED, FLEX> &E, int m, int a, const double *p)
 {
   const RgpuSys &S = *E.S;
@@ -237,7 +238,7 @@ __device__ __forceinline__ void share(int n, int r, int c, int &lo, int &hi)
 
 /* Pair evaluation of P positions on this CTA's share, then one cluster
  * barrier; the totals are read with gather(). All threads call. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair_check, int ew_ns = 0)
 {
   Ctl &C = *E.ctl;
@@ -320,7 +321,7 @@ __device__ __forceinline__ void engine_eval(Eng<MIXED, FLEX> &E, int P, int pair
 
 /* Totals of position p of the last evaluation (buffer b): the CTAs' sums
  * added in rank order. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void gather(const Eng<MIXED, FLEX> &E, int b, int p, double *r, int &ov)
 {
   cg::cluster_group cl = cg::this_cluster();
@@ -337,7 +338,7 @@ __device__ __forceinline__ void gather(const Eng<MIXED, FLEX> &E, int b, int p, 
 
 /* Ewald sum over this CTA's wave vectors for the sites in E.sites[0..ns),
  * warp partials left in E.red[b]; one cluster barrier. All threads call. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void engine_ewald(Eng<MIXED, FLEX> &E, int ns)
 {
   Ctl &C = *E.ctl;
@@ -371,7 +372,7 @@ __device__ __forceinline__ void engine_ewald(Eng<MIXED, FLEX> &E, int ns)
 }
 
 /* cluster total of the last Ewald sum (buffer b) */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void gather_ewald(const Eng<MIXED, FLEX> &E, int b, double &ea, double &eh)
 {
   cg::cluster_group cl = cg::this_cluster();
@@ -391,7 +392,7 @@ __device__ __forceinline__ void gather_ewald(const Eng<MIXED, FLEX> &E, int b, d
  * LJ biasing (src/cbmc.c:734-735, :1432-1436). Selection as
  * SelectTrialPosition (src/cbmc.c:563-599). Lane 0 leaves the weight sum
  * (w_sum = sum exp(bf)), the selected trial and its energies in Ctl. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void cbmc_trials(const Eng<MIXED, FLEX> &E, int b, int n, int nb, bool first, bool select, double usel,
                             double &w_sum, int &sel, double *usum, int &any, int off = 0, double *w_sel = nullptr)
 {
@@ -444,7 +445,7 @@ __device__ __forceinline__ void cbmc_trials(const Eng<MIXED, FLEX> &E, int b, in
 /* ------------------------------------------------------------------------ */
 /* translation (mv=0) and rotation (mv=1):
  * TranslationMoveAdsorbate src/mc_moves.c:1529-1762, RotationMoveAdsorbate :2636 */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void step_displace(Eng<MIXED, FLEX> &E, int mv)
 {
   RgpuSys &S = *E.S;
@@ -548,7 +549,7 @@ __device__ __forceinline__ void step_displace(Eng<MIXED, FLEX> &E, int mv)
  * of GenerateTrialOrientationsSimpleSphere :1480-1578 and
  * ComputeExternalEnergies :1154-1478, LJ biasing; acceptance of
  * SwapAddAdsorbateMove src/mc_moves.c:7016 and SwapRemoveAdsorbateMove :7228. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool widom = false)
 {
   RgpuSys &S = *E.S;
@@ -791,7 +792,7 @@ __device__ __forceinline__ void step_swap(Eng<MIXED, FLEX> &E, bool insert, bool
  * Evaluation 1 holds the nf new first-bead trials, the old first bead and
  * the retrace orientations (all known up front); evaluation 2 the new
  * orientations around the chosen first bead. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void step_reinsert(Eng<MIXED, FLEX> &E)
 {
   RgpuSys &S = *E.S;
@@ -1210,7 +1211,7 @@ __device__ __noinline__ void chain_ref_trial(const RgpuSys &S, int i, int stage,
  * barrier each CTA copies the other CTAs' rows from their shared memory.
  * All threads of the cluster call; the caller's next barrier publishes the
  * table. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stage, double *tab,
                                                    const double (*old)[3])
 {
@@ -1231,7 +1232,7 @@ __device__ __forceinline__ void chain_angles_table(Eng<MIXED, FLEX> &E, int stag
     __syncthreads();
     for (int task = gw; task < ntask; task += ngw) {
       const int i = 2 + task / nt, t = task % nt;
-      chain_ref_trial<MIXED>(S, i, stage, t, E.step, lane, old, theta[i],
+      chain_ref_trial<(MIXED != 0)>(S, i, stage, t, E.step, lane, old, theta[i],
                              tab + RGPU_ANG_STRIDE * ((i - 2) * RGPU_MAX_TRIALS + t));
     }
   } else {
@@ -1296,7 +1297,7 @@ __device__ __forceinline__ int retrace_group_end(int i0, int na, int nf, int nt,
  * off + P, position j of the group being bead i, trial t in growth order;
  * trial 0 of each bead is the old bead old[i]. Threads t0, t0 + step, ...
  * of the block place. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void retrace_place(Eng<MIXED, FLEX> &E, int stage, int i0, int P, int off,
                                               const double (*old)[3], const double *ang, int exclude, int t0,
                                               int step)
@@ -1335,7 +1336,7 @@ __device__ __forceinline__ void retrace_place(Eng<MIXED, FLEX> &E, int stage, in
  * block), sums its weights in trial order and leaves in C.rb[i] the sum,
  * the old bead's host and adsorbate VDW, intramolecular LJ and bonded
  * energy, and whether any trial was valid. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void retrace_book(const Eng<MIXED, FLEX> &E, int b, int i0, int i1, int off,
                                              const double (*old)[3], const double *ang, int w0)
 {
@@ -1405,7 +1406,7 @@ __device__ __forceinline__ void retrace_combine(Ctl &C, int i0, int i1, int nf, 
  * trial, as the bead-by-bead retrace does. The trials draw the same random
  * numbers as that retrace (counter-based, by stage, bead and trial). All
  * threads call. */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, int m, int exclude)
 {
   RgpuSys &S = *E.S;
@@ -1438,7 +1439,7 @@ __device__ __forceinline__ void retrace_chain(Eng<MIXED, FLEX> &E, int stage, in
   }
 }
 
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, int stage, int m, int exclude,
                                            bool ride = false)
 {
@@ -1565,7 +1566,7 @@ __device__ __forceinline__ void grow_chain(Eng<MIXED, FLEX> &E, bool retrace, in
 /* CBMC insertion, deletion and Widom test insertion of a flexible chain
  * (SwapAddAdsorbateMove src/mc_moves.c:7016, SwapRemoveAdsorbateMove :7228,
  * WidomAdsorbateMove :7844; uncharged chains, no Fourier part). */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void step_swap_chain(Eng<MIXED, FLEX> &E, bool insert, bool widom)
 {
   RgpuSys &S = *E.S;
@@ -1617,7 +1618,7 @@ __device__ __forceinline__ void step_swap_chain(Eng<MIXED, FLEX> &E, bool insert
 /* CBMC reinsertion of a flexible chain (ReinsertionAdsorbateMove,
  * src/mc_moves.c:4415): a new configuration grown with molecule m left out,
  * the old one retraced; accepted with W(new) / W(old). */
-template <bool MIXED, bool FLEX>
+template <int MIXED, bool FLEX>
 __device__ __forceinline__ void step_reinsert_chain(Eng<MIXED, FLEX> &E)
 {
   RgpuSys &S = *E.S;
@@ -1679,7 +1680,7 @@ __device__ inline void load_sys(RgpuSys *dst, const RgpuSys *src)
  * compiled with flexible-chain moves and energy grids; batches of rigid
  * molecules without grids run the build without them, whose register
  * allocation the chain and grid code does not touch. */
-template <bool MIXED, bool WIDE, bool FLEX>
+template <int MIXED, bool WIDE, bool FLEX>
 __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys *systems, int nsys, long long nsteps,
                                                                        int kw, int max_ads_atoms, int fw_items,
                                                                        int tile_items, int k_items)
@@ -1707,7 +1708,7 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
     E.sc.uc = E.uc;
     E.sc.uo = E.uo;
     E.sc.qr2 = (float *)(smem + L.q);
-    E.sc.qq = E.sc.qr2 + nwarps * 64;
+    E.sc.qq = E.sc.qr2 + nwarps * (MIXED == 2 ? 128 : 64);
     E.sc.qt = (int *)(E.sc.qq + nwarps * 64);
     E.sites = (EwSite *)(smem + L.sites);
     E.tab = (typename PhaseT<MIXED>::T *)(smem + L.tab);
@@ -1907,9 +1908,10 @@ __global__ void __launch_bounds__(WIDE ? 1024 : 512) rgpu_engine_kernel(RgpuSys 
 using EngineKernel = void (*)(RgpuSys *, int, long long, int, int, int, int, int);
 static EngineKernel engine_kernel(int mixed, bool wide, bool flex)
 {
-  if (mixed && wide) return flex ? rgpu_engine_kernel<true, true, true> : rgpu_engine_kernel<true, true, false>;
-  if (mixed) return flex ? rgpu_engine_kernel<true, false, true> : rgpu_engine_kernel<true, false, false>;
-  return flex ? rgpu_engine_kernel<false, false, true> : rgpu_engine_kernel<false, false, false>;
+  if (mixed == 2) return wide ? rgpu_engine_kernel<2, true, false> : rgpu_engine_kernel<2, false, false>;
+  if (mixed && wide) return flex ? rgpu_engine_kernel<1, true, true> : rgpu_engine_kernel<1, true, false>;
+  if (mixed) return flex ? rgpu_engine_kernel<1, false, true> : rgpu_engine_kernel<1, false, false>;
+  return flex ? rgpu_engine_kernel<0, false, true> : rgpu_engine_kernel<0, false, false>;
 }
 
 cudaError_t rgpu_engine_prepare(int mixed, bool wide, bool flex, size_t smem)
@@ -1965,7 +1967,7 @@ struct CallSmem {
  * (src/framework_energy.c:73-77, :195-198) and the move differences
  * (:4893-4894, :5437-5438). A grid value sets no overlap flag: the
  * reference's grid branches set none. */
-template <bool MIXED>
+template <int MIXED>
 __global__ void __launch_bounds__(256) k_point_energies(const RgpuSys *sysp, const void *ads, int nads,
                                                         const double *xyz, const int *atom, const int *excl, int P,
                                                         int pair_check, int fw_grid, double *out, int *ov)
@@ -2029,7 +2031,7 @@ cudaError_t rgpu_point_energies_launch(int mixed, const RgpuSys *d_sys, const vo
 
 /* Ewald Fourier difference of ns signed sites (FP64 xyz + charges), writing
  * dS(k) of the candidate into d_ds (for a later accept) and {e_ads, e_host}. */
-template <bool MIXED>
+template <int MIXED>
 __global__ void __launch_bounds__(256) k_ewald_delta(const RgpuSys *sysp, const double *xyz, const double *q, int ns,
                                                      double2 *d_ds, double *out, int kw)
 {

@@ -1,11 +1,15 @@
 /* Device building blocks of the B200 GCMC energy path.
  *
  * Shared by the per-call entry points (capi.cu) and the persistent batched
- * engine (engine.cu). Two precisions are instantiated from one template:
- *   MIXED = false : FP64 everywhere (the plain path; parity 1e-9 relative);
- *   MIXED = true  : FP32 pair terms and exp(ik.r) products on 32-bit
- *                   fixed-point coordinates, FP32 per-warp sums, FP64 per-move
- *                   sums, FP64 structure factors, totals and acceptance.
+ * engine (engine.cu). Three precisions are instantiated from one template:
+ *   MIXED = 0 : FP64 everywhere (the plain path; parity 1e-9 relative);
+ *   MIXED = 1 : FP32 pair terms and exp(ik.r) products on 32-bit fixed-point
+ *               coordinates, FP32 per-warp sums, FP64 per-move sums, FP64
+ *               structure factors, totals and acceptance;
+ *   MIXED = 2 : as 1, but the real-space charge-charge term of every pair, its
+ *               distance and the cut-off test in FP64, with FP64 warp sums
+ *               (the framework and adsorbate charges stay FP32); the batched
+ *               engine only.
  */
 #ifndef RGPU_DEVICE_CUH
 #define RGPU_DEVICE_CUH
@@ -268,7 +272,8 @@ struct EvalScratch {
   int *uo;
   int *next;      /* unit counter of the dynamic schedule; 0 when an evaluation starts */
   unsigned long long *cnt;   /* optional {pairs visited, in cut-off, charged in cut-off} */
-  float *qr2;     /* per-warp queue of in-cut-off pairs (mixed path): [nwarps][64] */
+  float *qr2;     /* per-warp queue of in-cut-off pairs (mixed path): [nwarps][64], or
+                   * [nwarps][64] doubles for MIXED = 2 */
   float *qq;
   int *qt;
 };
@@ -382,6 +387,99 @@ __device__ __forceinline__ void queue_drain(PairQueue &Q, float &av, float &ac, 
   __syncwarp();
 }
 
+/* The same queue for MIXED = 2: the squared distance is queued in FP64; the
+ * LJ term is formed in FP32 from it as above, the real-space charge-charge
+ * term in FP64 (erfc of the CUDA math library) and summed per lane in FP64. */
+struct PairQueueQ {
+  double *r2;
+  float *q;
+  int *t;
+  int n;
+  const RgpuLJf *P;
+  bool charged, check;
+  double qa, alpha;
+  float thr;
+};
+
+__device__ __forceinline__ void pair_qq_queued(const PairQueueQ &Q, double r2d, float qj, int type, float &av,
+                                               double &ac, int &ov, int &nch)
+{
+  const RgpuLJf L = Q.P[type];
+  const float r2 = (float)r2d;
+  float ri = rsqrtf(r2);
+  ri = ri * fmaf(-0.5f * r2, ri * ri, 1.5f);
+  float s6 = L.sig2 * (ri * ri);
+  s6 = s6 * s6 * s6;
+  const float u = fmaf(L.eps4 * s6, s6 - 1.0f, -L.shift);
+  av += u;
+  if (Q.check && u >= Q.thr) ov = 1;
+  if (Q.charged && qj != 0.0f) {
+    nch++;
+    const double r = sqrt(r2d);
+    const double uc = Q.qa * (double)qj * (erfc(Q.alpha * r) / r);
+    ac += uc;
+    if (Q.check && uc >= (double)Q.thr) ov = 1;
+  }
+}
+
+__device__ __forceinline__ void queue_add(PairQueueQ &Q, bool in, double r2, float q, int t, float &av, double &ac,
+                                          int &ov, int &nin, int &nch)
+{
+  const int lane = threadIdx.x & 31;
+  const unsigned bal = __ballot_sync(RGPU_FULL, in);
+  if (in) {
+    const int p = Q.n + __popc(bal & ((1u << lane) - 1u));
+    Q.r2[p] = r2;
+    Q.q[p] = q;
+    Q.t[p] = t;
+  }
+  Q.n += __popc(bal);
+  if (Q.n >= 32) {
+    __syncwarp();
+    const double e_r2 = Q.r2[lane];
+    const float e_q = Q.q[lane];
+    const int e_t = Q.t[lane];
+    double t_r2 = 0.0;
+    float t_q = 0.0f;
+    int t_t = 0;
+    if (lane < Q.n - 32) { t_r2 = Q.r2[32 + lane]; t_q = Q.q[32 + lane]; t_t = Q.t[32 + lane]; }
+    __syncwarp();
+    if (lane < Q.n - 32) { Q.r2[lane] = t_r2; Q.q[lane] = t_q; Q.t[lane] = t_t; }
+    nin++;
+    pair_qq_queued(Q, e_r2, e_q, e_t, av, ac, ov, nch);
+    Q.n -= 32;
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void queue_drain(PairQueueQ &Q, float &av, double &ac, int &ov, int &nin, int &nch)
+{
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  if (lane < Q.n) {
+    nin++;
+    pair_qq_queued(Q, Q.r2[lane], Q.q[lane], Q.t[lane], av, ac, ov, nch);
+  }
+  Q.n = 0;
+  __syncwarp();
+}
+
+/* FP64 Cartesian difference of two fixed-point positions (MIXED = 2) */
+template <bool TRI>
+__device__ __forceinline__ double rgpu_fix_r2_d(const RgpuSys &S, int ix, int iy, int iz)
+{
+  const double k = 2.3283064365386963e-10;     /* 2^-32 */
+  const double fx = (double)ix * k, fy = (double)iy * k, fz = (double)iz * k;
+  if (!TRI) {
+    const double dx = fx * S.box[0], dy = fy * S.box[1], dz = fz * S.box[2];
+    return dx * dx + dy * dy + dz * dz;
+  }
+  const double dx = S.hm[0] * fx + S.hm[1] * fy + S.hm[2] * fz;
+  const double dy = S.hm[4] * fy + S.hm[5] * fz;
+  const double dz = S.hm[8] * fz;
+  return dx * dx + dy * dy + dz * dz;
+}
+
 static_assert(RGPU_TILE == 16, "unit_tiles_mixed visits two tiles per warp pass, one per half warp");
 
 /* framework tiles [t0, t1) for bead b, FP32 path (warp-wide); TRI: the
@@ -463,6 +561,85 @@ __device__ __forceinline__ void unit_tiles_mixed(const RgpuSys &S, const int4 *f
       }
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       queue_add(Q, hl < nmine && r2 < rc2, r2, __int_as_float(f.w), f.z & 3, av, ac, ov, nin, nch);
+    }
+  }
+  queue_drain(Q, av, ac, ov, nin, nch);
+}
+
+/* unit_tiles_mixed for MIXED = 2: the same tile culling in FP32, then each
+ * visited pair's distance and cut-off test in FP64 (queued as FP64), its LJ
+ * term in FP32 and its real-space charge-charge term in FP64; qr2 holds 64
+ * doubles */
+template <bool TRI>
+__device__ __forceinline__ void unit_tiles_cc64(const RgpuSys &S, const int4 *fw, const TileRec *tiles, int t0, int t1,
+                                                const BeadPos &b, bool check, float &av,
+                                                double &ac, int &ov, int &nin, int &nch, int &nvis, float *qr2,
+                                                float *qq, int *qt)
+{
+  const int lane = threadIdx.x & 31;
+  const float sx = S.fix_scale[0], sy = S.fix_scale[1], sz = S.fix_scale[2];
+  const float rc2 = S.rc2f;
+  PairQueueQ Q;
+  Q.r2 = reinterpret_cast<double *>(qr2); Q.q = qq; Q.t = qt; Q.n = 0;
+  Q.P = S.ljf_bf[b.atom];
+  Q.qa = S.mol_q[b.atom] * S.coulomb;
+  Q.alpha = S.alpha;
+  Q.charged = S.fw_charged && Q.qa != 0.0;
+  Q.check = check;
+  Q.thr = (float)S.overlap;
+  const bool tri = TRI;
+  for (int tb = t0; tb < t1; tb += 32) {
+    const int t = tb + lane;
+    bool vis = false;
+    int tn = 0;                  /* atoms of this lane's tile */
+    if (t < t1) {
+      const TileRec tr = tiles[t];
+      tn = tr.c.w;
+      if (!tri) {
+        float dx = fmaxf(fabsf(__int2float_rn(tr.c.x - b.xi) * sx) - tr.h.x, 0.0f);
+        float dy = fmaxf(fabsf(__int2float_rn(tr.c.y - b.yi) * sy) - tr.h.y, 0.0f);
+        float dz = fmaxf(fabsf(__int2float_rn(tr.c.z - b.zi) * sz) - tr.h.z, 0.0f);
+        vis = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rc2;
+      } else {
+        /* triclinic tile: h = fractional half extents, h.w = Cartesian
+         * radius. Every atom's wrapped fractional offset along axis r is at
+         * least |t_r| - h_r, so it lies at least that many perpendicular
+         * widths away; when no atom can wrap differently from the centre
+         * (|t_r| + h_r < 1/2 on every axis), it also lies at least the
+         * centre's distance minus the radius away. */
+        const int ix = tr.c.x - b.xi, iy = tr.c.y - b.yi, iz = tr.c.z - b.zi;
+        const float tx = fabsf(__int2float_rn(ix) * 2.3283064365386963e-10f);
+        const float ty = fabsf(__int2float_rn(iy) * 2.3283064365386963e-10f);
+        const float tz = fabsf(__int2float_rn(iz) * 2.3283064365386963e-10f);
+        const float m = fmaxf(fmaxf((tx - tr.h.x) * S.wperp[0], (ty - tr.h.y) * S.wperp[1]),
+                              (tz - tr.h.z) * S.wperp[2]);
+        vis = !(m > 0.0f && m * m >= rc2);
+        if (vis && tx + tr.h.x < 0.5f && ty + tr.h.y < 0.5f && tz + tr.h.z < 0.5f) {
+          float dx, dy, dz;
+          rgpu_fix_to_cart_tri(S, ix, iy, iz, dx, dy, dz);
+          const float e = fmaxf(sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - tr.h.w, 0.0f);
+          vis = e * e < rc2;
+        }
+      }
+    }
+    unsigned m = __ballot_sync(RGPU_FULL, vis);
+    /* two visible tiles per pass of the warp: lanes 0-15 take the atoms of
+     * the first, lanes 16-31 those of the second */
+    const int half = lane >> 4, hl = lane & 15;
+    while (m) {
+      const int i1 = __ffs(m) - 1;
+      m &= m - 1;
+      const int i2 = m ? __ffs(m) - 1 : -1;
+      m &= m - 1;
+      const int n1 = __shfl_sync(RGPU_FULL, tn, i1);
+      const int n2s = __shfl_sync(RGPU_FULL, tn, i2 >= 0 ? i2 : 0);
+      const int n2 = i2 >= 0 ? n2s : 0;
+      nvis += n1 + n2;
+      const int mine = half ? i2 : i1, nmine = half ? n2 : n1;
+      int4 f = make_int4(0, 0, 0, 0);
+      if (hl < nmine) f = fw[(tb + mine) * RGPU_TILE + hl];
+      const double r2 = rgpu_fix_r2_d<TRI>(S, f.x - b.xi, f.y - b.yi, f.z - b.zi);
+      queue_add(Q, hl < nmine && r2 < S.rc2, r2, __int_as_float(f.w), f.z & 3, av, ac, ov, nin, nch);
     }
   }
   queue_drain(Q, av, ac, ov, nin, nch);
@@ -561,6 +738,42 @@ __device__ __forceinline__ void unit_ads_mixed(const RgpuSys &S, const int4 *ads
   queue_drain(Q, av, ac, ov, nin, nch);
 }
 
+/* unit_ads_mixed for MIXED = 2 (see unit_tiles_cc64) */
+template <bool TRI>
+__device__ __forceinline__ void unit_ads_cc64(const RgpuSys &S, const int4 *ads, const BeadPos &b, int lo, int hi,
+                                              int exclude, bool check, float &av, double &ac, int &ov, int &nin,
+                                              int &nch, int &nvis, float *qr2, float *qq, int *qt)
+{
+  const int lane = threadIdx.x & 31;
+  PairQueueQ Q;
+  Q.r2 = reinterpret_cast<double *>(qr2); Q.q = qq; Q.t = qt; Q.n = 0;
+  Q.P = S.ljf_bb[b.atom];
+  Q.qa = S.mol_q[b.atom] * S.coulomb;
+  Q.alpha = S.alpha;
+  Q.charged = S.mol_charged && Q.qa != 0.0;
+  Q.check = check;
+  Q.thr = (float)S.overlap;
+  nvis += hi - lo;
+  for (int jb = lo; jb < hi; jb += 32) {
+    const int j = jb + lane;
+    bool in = false;
+    double r2 = 0.0;
+    float q = 0.0f;
+    int at = 0;
+    if (j < hi) {
+      const int4 f = ads[j];
+      if ((f.w >> 4) != exclude) {
+        at = f.w & 15;
+        r2 = rgpu_fix_r2_d<TRI>(S, f.x - b.xi, f.y - b.yi, f.z - b.zi);
+        in = r2 < S.rc2;
+        q = S.mol_qf[at];
+      }
+    }
+    queue_add(Q, in, r2, q, at, av, ac, ov, nin, nch);
+  }
+  queue_drain(Q, av, ac, ov, nin, nch);
+}
+
 template <bool TRI>
 __device__ __forceinline__ void unit_ads_fp64(const RgpuSys &S, const AdsRec64 *ads, const BeadPos &b, int lo,
                                               int hi, int exclude, bool check, double &av, double &ac, int &ov,
@@ -625,7 +838,7 @@ struct EvalSlice {
  * the warps of the block finish together. The stored sums do not depend on
  * which warp evaluated a unit. No block barrier; *sc.next is left past the
  * last unit (the caller resets it after its barrier). Returns the plan. */
-template <bool MIXED>
+template <int MIXED>
 __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
                                EvalScratch sc, int max_units)
 {
@@ -667,7 +880,27 @@ __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice
       lo = sl.ads_lo + (int)((unsigned)(nads * cc) / (unsigned)pl.ca);
       hi = sl.ads_lo + (int)((unsigned)(nads * (cc + 1)) / (unsigned)pl.ca);
     }
-    if (MIXED) {
+    if constexpr (MIXED == 2) {
+      float av = 0.0f;
+      double ac = 0.0;
+      float *qr2 = sc.qr2 + 128 * w;   /* 64 FP64 squared distances per warp */
+      if (c < pl.cf) {
+        if (S.triclinic)
+          unit_tiles_cc64<true>(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
+                                qr2, sc.qq + 64 * w, sc.qt + 64 * w);
+        else
+          unit_tiles_cc64<false>(S, (const int4 *)sl.fw, sl.tiles, lo, hi, b, check, av, ac, ov, nin, nch, nvis,
+                                 qr2, sc.qq + 64 * w, sc.qt + 64 * w);
+      } else if (S.triclinic) {
+        unit_ads_cc64<true>(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
+                            qr2, sc.qq + 64 * w, sc.qt + 64 * w);
+      } else {
+        unit_ads_cc64<false>(S, (const int4 *)sl.ads, b, lo, hi, b.excl, check, av, ac, ov, nin, nch, nvis,
+                             qr2, sc.qq + 64 * w, sc.qt + 64 * w);
+      }
+      e_v = warp_sum((double)av);
+      e_q = warp_sum(ac);
+    } else if (MIXED) {
       float av = 0.0f, ac = 0.0f;
       if (c < pl.cf) {
         if (S.triclinic)
@@ -722,7 +955,7 @@ __device__ __forceinline__ EvalPlan eval_units(const RgpuSys &S, const EvalSlice
 
 /* Evaluates P bead positions over the slice; all threads of the block must
  * call it. Writes this slice's partial results to res/ovf. */
-template <bool MIXED>
+template <int MIXED>
 __device__ void eval_positions(const RgpuSys &S, const EvalSlice &sl, const BeadPos *pos, int P, int pair_check,
                                double (*res)[4], int *ovf, EvalScratch sc, int max_units)
 {
@@ -755,13 +988,13 @@ __device__ void eval_positions(const RgpuSys &S, const EvalSlice &sl, const Bead
  * fixed-point coordinate, so each phase has FP32 accuracy at every k. */
 struct EwSite { BeadPos b; double q; };
 
-template <bool MIXED>
-struct PhaseT { typedef double2 T; };
+template <int MIXED>
+struct PhaseT { typedef float2 T; };
 template <>
-struct PhaseT<true> { typedef float2 T; };
+struct PhaseT<0> { typedef double2 T; };
 
 /* table layout: tab[(site*3 + axis)*KW + (k + kmax)], KW = 2*kmaxall+1 */
-template <bool MIXED>
+template <int MIXED>
 __device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sites, int ns, typename PhaseT<MIXED>::T *tab, int kw)
 {
   const int km = (kw - 1) / 2;
@@ -794,7 +1027,7 @@ __device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sit
 }
 
 /* delta S(k) for wave vector k from the tables */
-template <bool MIXED>
+template <int MIXED>
 __device__ __forceinline__ double2 ewald_dS(const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
                                             int ns, char4 kv)
 {
@@ -832,7 +1065,7 @@ __device__ __forceinline__ double2 ewald_dS(const typename PhaseT<MIXED>::T *tab
 /* Sum over wave vectors [k0, k1) of the energy change; every thread returns
  * {e_ads, e_host}:
  * e_ads = sum kf (|S+dS|^2 - |S|^2), e_host = sum kf Re(S_fw^* dS). */
-template <bool MIXED>
+template <int MIXED>
 __device__ void ewald_energy_sum(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
                                  const EwSite *sites, int ns, int k0, int k1, double &e_ads, double &e_host,
                                  double *red)
@@ -853,7 +1086,7 @@ __device__ void ewald_energy_sum(const RgpuSys &S, const typename PhaseT<MIXED>:
 
 /* As ewald_energy_sum, without block reduction: warp w leaves its partial
  * {e_ads, e_host} in red[2w], red[2w+1]. No block barrier. */
-template <bool MIXED>
+template <int MIXED>
 __device__ __forceinline__ void ewald_energy_warps(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw,
                                    const EwSite *sites, int ns, int k0, int k1, double *red)
 {
@@ -877,7 +1110,7 @@ __device__ __forceinline__ void ewald_energy_warps(const RgpuSys &S, const typen
 /* S_ads(k) += dS(k) (AcceptEwaldAdsorbateMove, src/ewald.c:11732). The same
  * ewald_dS call as in the energy sum, so the stored sums are those the
  * accepted energy was computed with. */
-template <bool MIXED>
+template <int MIXED>
 __device__ __forceinline__ void ewald_apply(const RgpuSys &S, const typename PhaseT<MIXED>::T *tab, int kw, const EwSite *sites,
                             int ns, int k0, int k1)
 {
