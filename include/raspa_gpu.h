@@ -37,7 +37,8 @@ extern "C" {
 #define RGPU_FP64 0            /* FP64 throughout (the reference's REAL) */
 #define RGPU_MIXED 1           /* FP32 pair terms / FP64 sums and S(k) */
 #define RGPU_MIXED_CC64 2      /* as RGPU_MIXED, with each pair's distance, cut-off test and
-                                * real-space charge-charge term in FP64 (rgpu_engine_create
+                                * real-space charge-charge term, and the Fourier phases and
+                                * dS(k), in FP64; LJ terms stay FP32 (rgpu_engine_create
                                 * only; rigid molecules without energy grids) */
 
 typedef struct rgpu_system rgpu_system;

@@ -8,8 +8,9 @@
  *               structure factors, totals and acceptance;
  *   MIXED = 2 : as 1, but the real-space charge-charge term of every pair, its
  *               distance and the cut-off test in FP64, with FP64 warp sums
- *               (the framework and adsorbate charges stay FP32); the batched
- *               engine only.
+ *               (the framework and adsorbate charges stay FP32), and the
+ *               exp(ik.r) phases (of the same exact fixed-point angles) and
+ *               their products in FP64; the batched engine only.
  */
 #ifndef RGPU_DEVICE_CUH
 #define RGPU_DEVICE_CUH
@@ -992,6 +993,8 @@ template <int MIXED>
 struct PhaseT { typedef float2 T; };
 template <>
 struct PhaseT<0> { typedef double2 T; };
+template <>
+struct PhaseT<2> { typedef double2 T; };
 
 /* table layout: tab[(site*3 + axis)*KW + (k + kmax)], KW = 2*kmaxall+1 */
 template <int MIXED>
@@ -1004,13 +1007,20 @@ __device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sit
     int sa = i / kw;
     int axis = sa % 3, s = sa / 3;
     const BeadPos &b = sites[s].b;
-    if (MIXED) {
+    if (MIXED == 1) {
       int xi = axis == 0 ? b.xi : (axis == 1 ? b.yi : b.zi);
       int ang = (int)((unsigned)kk * (unsigned)xi);          /* k*s mod 1 turn, exact */
       float turns = __int2float_rn(ang) * 2.3283064365386963e-10f;   /* 2^-32 */
       float sn, cs;
       sincospif(2.0f * turns, &sn, &cs);
       ((float2 *)tab)[i] = make_float2(cs, sn);
+    } else if (MIXED == 2) {
+      /* the same exact angle, its phase in FP64 */
+      int xi = axis == 0 ? b.xi : (axis == 1 ? b.yi : b.zi);
+      int ang = (int)((unsigned)kk * (unsigned)xi);
+      double sn, cs;
+      sincospi(2.0 * ((double)ang * 2.3283064365386963e-10), &sn, &cs);
+      ((double2 *)tab)[i] = make_double2(cs, sn);
     } else {
       double f;
       if (!S.triclinic) {
@@ -1032,7 +1042,7 @@ __device__ __forceinline__ double2 ewald_dS(const typename PhaseT<MIXED>::T *tab
                                             int ns, char4 kv)
 {
   const int km = (kw - 1) / 2;
-  if (MIXED) {
+  if (MIXED == 1) {
     float re = 0.0f, im = 0.0f;
     const float2 *t = (const float2 *)tab;
     for (int s = 0; s < ns; s++) {

@@ -21,7 +21,7 @@ _ip = C.POINTER(C.c_int)
 
 RGPU_FP64 = 0
 RGPU_MIXED = 1
-RGPU_MIXED_CC64 = 2   # mixed, with FP64 distances and real-space charge-charge terms (engine only)
+RGPU_MIXED_CC64 = 2   # mixed, with FP64 distances, real-space charge-charge terms and dS(k) (engine only)
 RGPU_E_INVALID = -1   # include/raspa_gpu.h
 RGPU_FRAMEWORK_FULL = 0
 RGPU_FRAMEWORK_GRID = 1
