@@ -527,6 +527,14 @@ def run_ours(args):
             line[key] = batched_fp64_run(native, stream, gs, sys_list, args, peak, steps=args.steps, precision=p)
         line["precision"]["co2_batched_cc64"] = line["batched_mixed_cc64"]["energy_error"]
         line["precision"]["co2_batched_mixed_anchored"] = line["batched_mixed_anchored"]["energy_error"]
+        # the metric's error bound, engine by engine: moves/s and the largest
+        # relative error of a box's running total energy
+        line["at_1e-6_rel_err"] = {
+            k: {"moves_per_s": v, "max_rel_total": e, "within": e <= 1e-6} for k, v, e in (
+                ("mixed", value, line["precision"]["co2_batched"]["max_rel_total"]),
+                ("mixed_cc64", line["batched_mixed_cc64"]["moves_per_s"],
+                 line["precision"]["co2_batched_cc64"]["max_rel_total"]),
+                ("fp64", line["batched_fp64"]["moves_per_s"], line["batched_fp64"]["energy_error"]["max_rel_total"]))}
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_gpu"] = plain_gpu_rate(native, stream)
         # the two single-system configurations, each on its own
