@@ -36,3 +36,14 @@ def test_errors_are_codes_not_exits():
     rc = L.rgpu_system_create(C.byref(h), None)
     assert rc == -1
     assert b"null" in L.rgpu_error_string(rc)
+
+
+def test_constants_match_header():
+    """Precision, framework-model and error constants of native.py equal the
+    header's #defines."""
+    with open(os.path.join(ROOT, "include", "raspa_gpu.h")) as fh:
+        defs = dict(re.findall(r"#define\s+(RGPU_[A-Z0-9_]+)\s+(-?\d+)\b", fh.read()))
+    names = ["RGPU_FP64", "RGPU_MIXED", "RGPU_MIXED_CC64", "RGPU_E_INVALID", "RGPU_FRAMEWORK_FULL",
+             "RGPU_FRAMEWORK_GRID"]
+    for n in names:
+        assert int(defs[n]) == getattr(native, n), n
