@@ -22,12 +22,16 @@ from test_gpu_engine import engine_run
 pytestmark = pytest.mark.gpu
 
 
-def test_tracks_fp64_engine(cuda):
-    c = load("co2_tiny")
+@pytest.mark.parametrize("name,n", [("co2_tiny", 150), ("co2_triclinic", 300)])
+def test_tracks_fp64_engine(cuda, name, n):
+    """Same decisions as the FP64 engine, in an orthorhombic and a triclinic
+    box (the FP64 pair distance then goes through the box matrix)."""
+    c = load(name)
     s = system_of(c)
     mols = np.array(c["molecules"])
-    _, a = engine_run(s, mols, 150, native.RGPU_FP64, cluster=2)
-    _, b = engine_run(s, mols, 150, native.RGPU_MIXED_CC64, cluster=2)
+    _, a = engine_run(s, mols, n, native.RGPU_FP64, cluster=2)
+    _, b = engine_run(s, mols, n, native.RGPU_MIXED_CC64, cluster=2)
+    assert a["counters"][4:8].sum() > 10
     np.testing.assert_array_equal(a["counters"][:9], b["counters"][:9])
     kT = units.K_B * s.temperature
     np.testing.assert_allclose(b["energy"][:6], a["energy"][:6], rtol=1e-5, atol=1e-3 * kT)
