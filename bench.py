@@ -64,7 +64,7 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0, help="CTA size; 0 = autotuned")
     p.add_argument("--cluster", type=int, default=0, help="CTAs per system; 0 = autotuned")
     p.add_argument("--maxmol", type=int, default=768)
-    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "mixed_cc64"])
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--ref-cycles", type=int, default=2,
                    help="reference production cycles per system and step (a cycle is max(20, N) moves)")
@@ -159,7 +159,7 @@ def equilibrated_configs(args, sys_list):
     gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240, stream_id=i) for i, s in enumerate(sys_list)]
     for g, s in zip(gs, sys_list):
         g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
-    prec = native.RGPU_MIXED if args.precision == "mixed" else native.RGPU_FP64
+    prec = {"mixed": native.RGPU_MIXED, "fp64": native.RGPU_FP64, "mixed_cc64": native.RGPU_MIXED_CC64}[args.precision]
     eng = native.Engine(gs, precision=prec, threads=512, cluster=0)   # one GPU: stream ids = batch order
     for _ in range(args.warmup + 1):
         eng.run(args.moves_per_step)
@@ -389,7 +389,7 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://",
                                 timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
-    prec = native.RGPU_MIXED if args.precision == "mixed" else native.RGPU_FP64
+    prec = {"mixed": native.RGPU_MIXED, "fp64": native.RGPU_FP64, "mixed_cc64": native.RGPU_MIXED_CC64}[args.precision]
 
     sys_list, sys_ids = placed_systems(args, world, rank)
     gs = [native.GpuSystem(s, maxmol=args.maxmol, seed=20240, stream_id=i) for i, s in zip(sys_ids, sys_list)]
@@ -493,7 +493,8 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "MC moves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == native.RGPU_MIXED else "f64",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {native.RGPU_MIXED: "f32", native.RGPU_FP64: "f64"}.get(prec, "f32+f64"),
         "data": "synthetic (seeded frameworks, random-init adsorbate state)",
         "config": {"workload": f"co2_gcmc_batched_{args.nsys}", "systems_per_gpu": args.nsys,
                    "placement": "job set of n_gpus seeded batches, placed by device-memory footprint "
