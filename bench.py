@@ -531,7 +531,7 @@ def run_ours(args):
         # the metric's error bound, engine by engine: moves/s and the largest
         # relative error of a box's running total energy
         line["at_1e-6_rel_err"] = {
-            k: {"moves_per_s": v, "max_rel_total": e, "within": e <= 1e-6} for k, v, e in (
+            k: {"moves_per_s": float(v), "max_rel_total": float(e), "within": bool(e <= 1e-6)} for k, v, e in (
                 ("mixed", value, line["precision"]["co2_batched"]["max_rel_total"]),
                 ("mixed_cc64", line["batched_mixed_cc64"]["moves_per_s"],
                  line["precision"]["co2_batched_cc64"]["max_rel_total"]),
