@@ -80,7 +80,8 @@ __host__ __device__ inline EngineLayout engine_layout(int mixed, int fw_items, i
   /* per-warp pair queues: r2 (FP32, or FP64 for mixed = 2), charge, type */
   L.q = o; o = rgpu_align(o + (mixed ? (size_t)nwarps * 64 * (mixed == 2 ? 16 : 12) : 0));
   L.sites = o; o = rgpu_align(o + 2 * RGPU_MAX_ATOMS * sizeof(EwSite));
-  L.tab = o; o = rgpu_align(o + (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * (mixed == 1 ? sizeof(float2) : sizeof(double2)));
+  /* per-site phase tables (none on the mixed path) */
+  L.tab = o; o = rgpu_align(o + (mixed == 1 ? 0 : (size_t)2 * RGPU_MAX_ATOMS * 3 * kw * sizeof(double2)));
   L.red = o; o = rgpu_align(o + 2 * 2 * RGPU_MAX_WARPS * sizeof(double));
   L.kvec = o; o = rgpu_align(o + (size_t)k_items * sizeof(char4));
   L.kf = o; o = rgpu_align(o + (size_t)k_items * sizeof(double));

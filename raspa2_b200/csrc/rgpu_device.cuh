@@ -983,10 +983,13 @@ __device__ void eval_positions(const RgpuSys &S, const EvalSlice &sl, const Bead
 /* Ewald Fourier difference (CalculateEwaldFourierAdsorbate,
  * src/ewald.c:6859-7567, charge sites only).
  *
- * Sites carry a signed charge (+q for new, -q for old positions). Per site
- * and axis, exp(i 2 pi k s) is tabulated for k in [-kmax, kmax]; on the mixed
- * path the angle k*s is reduced exactly in 32-bit integer arithmetic on the
- * fixed-point coordinate, so each phase has FP32 accuracy at every k. */
+ * Sites carry a signed charge (+q for new, -q for old positions). On the
+ * FP64 path (and MIXED = 2) exp(i 2 pi k s) is tabulated per site and axis
+ * for k in [-kmax, kmax] and multiplied out per wave vector. On the mixed
+ * path (MIXED = 1) each wave vector's angle n.s is reduced exactly in 32-bit
+ * integer arithmetic on the fixed-point coordinates and its phase formed
+ * directly (ewald_dS), so each phase has FP32 accuracy at every k; MIXED = 2
+ * tabulates the per-axis phases of the same exact angles in FP64. */
 struct EwSite { BeadPos b; double q; };
 
 template <int MIXED>
@@ -996,10 +999,12 @@ struct PhaseT<0> { typedef double2 T; };
 template <>
 struct PhaseT<2> { typedef double2 T; };
 
-/* table layout: tab[(site*3 + axis)*KW + (k + kmax)], KW = 2*kmaxall+1 */
+/* table layout: tab[(site*3 + axis)*KW + (k + kmax)], KW = 2*kmaxall+1;
+ * the mixed path (MIXED = 1) keeps no table */
 template <int MIXED>
 __device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sites, int ns, typename PhaseT<MIXED>::T *tab, int kw)
 {
+  if (MIXED == 1) return;
   const int km = (kw - 1) / 2;
   const int n = ns * 3 * kw;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -1007,15 +1012,8 @@ __device__ __forceinline__ void ewald_phases(const RgpuSys &S, const EwSite *sit
     int sa = i / kw;
     int axis = sa % 3, s = sa / 3;
     const BeadPos &b = sites[s].b;
-    if (MIXED == 1) {
-      int xi = axis == 0 ? b.xi : (axis == 1 ? b.yi : b.zi);
-      int ang = (int)((unsigned)kk * (unsigned)xi);          /* k*s mod 1 turn, exact */
-      float turns = __int2float_rn(ang) * 2.3283064365386963e-10f;   /* 2^-32 */
-      float sn, cs;
-      sincospif(2.0f * turns, &sn, &cs);
-      ((float2 *)tab)[i] = make_float2(cs, sn);
-    } else if (MIXED == 2) {
-      /* the same exact angle, its phase in FP64 */
+    if (MIXED == 2) {
+      /* the exact fixed-point angle, its phase in FP64 */
       int xi = axis == 0 ? b.xi : (axis == 1 ? b.yi : b.zi);
       int ang = (int)((unsigned)kk * (unsigned)xi);
       double sn, cs;
@@ -1043,19 +1041,24 @@ __device__ __forceinline__ double2 ewald_dS(const typename PhaseT<MIXED>::T *tab
 {
   const int km = (kw - 1) / 2;
   if (MIXED == 1) {
-    float re = 0.0f, im = 0.0f;
-    const float2 *t = (const float2 *)tab;
+    /* exp(ik.r) of each site in FP32 from its exact angle n.s (the wave
+     * vector's integer indices times the fixed-point fractional
+     * coordinates, in turns modulo 1): sincospif of the angle's leading 24
+     * bits, rotated to first order by its last 8 (at most 3.7e-7 rad);
+     * q exp(ik.r) summed in FP64. No phase table. */
+    double re = 0.0, im = 0.0;
     for (int s = 0; s < ns; s++) {
-      float2 a = t[(s * 3 + 0) * kw + kv.x + km];
-      float2 b = t[(s * 3 + 1) * kw + kv.y + km];
-      float2 c = t[(s * 3 + 2) * kw + kv.z + km];
-      float xr = a.x * b.x - a.y * b.y, xi = a.x * b.y + a.y * b.x;
-      float er = xr * c.x - xi * c.y, ei = xr * c.y + xi * c.x;
-      float q = (float)sites[s].q;
-      re = fmaf(q, er, re);
-      im = fmaf(q, ei, im);
+      const BeadPos &b = sites[s].b;
+      const int ang = (int)((unsigned)kv.x * (unsigned)b.xi + (unsigned)kv.y * (unsigned)b.yi +
+                            (unsigned)kv.z * (unsigned)b.zi);
+      float sn, cs;
+      sincospif(__int2float_rn(ang & ~0xff) * 4.656612873077393e-10f, &sn, &cs);   /* 2^-31: x in [-1, 1) */
+      const float d = __int2float_rn(ang & 0xff) * 1.4629180792671596e-09f;       /* 2 pi 2^-32 */
+      const float er = fmaf(-sn, d, cs), ei = fmaf(cs, d, sn);
+      re = fma(sites[s].q, (double)er, re);
+      im = fma(sites[s].q, (double)ei, im);
     }
-    return make_double2((double)re, (double)im);
+    return make_double2(re, im);
   } else {
     double re = 0.0, im = 0.0;
     const double2 *t = (const double2 *)tab;
