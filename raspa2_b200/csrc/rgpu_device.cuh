@@ -3,9 +3,9 @@
  * Shared by the per-call entry points (capi.cu) and the persistent batched
  * engine (engine.cu). Three precisions are instantiated from one template:
  *   MIXED = 0 : FP64 everywhere (the plain path; parity 1e-9 relative);
- *   MIXED = 1 : FP32 pair terms and exp(ik.r) products on 32-bit fixed-point
- *               coordinates, FP32 per-warp sums, FP64 per-move sums, FP64
- *               structure factors, totals and acceptance;
+ *   MIXED = 1 : FP32 pair terms and exp(ik.r) phases on 32-bit fixed-point
+ *               coordinates, FP32 per-warp pair sums, FP64 dS(k) and per-move
+ *               sums, FP64 structure factors, totals and acceptance;
  *   MIXED = 2 : as 1, but the real-space charge-charge term of every pair, its
  *               distance and the cut-off test in FP64, with FP64 warp sums
  *               (the framework and adsorbate charges stay FP32), and the
