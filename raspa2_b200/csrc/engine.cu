@@ -2038,7 +2038,8 @@ __global__ void __launch_bounds__(256) k_ewald_delta(const RgpuSys *sysp, const 
 {
   __shared__ RgpuSys S;
   __shared__ EwSite sites[2 * RGPU_MAX_ATOMS];
-  __shared__ typename PhaseT<MIXED>::T tab[2 * RGPU_MAX_ATOMS * 3 * 41];
+  /* phase tables of the FP64 path; the mixed path forms its phases directly */
+  __shared__ typename PhaseT<MIXED>::T tab[MIXED == 1 ? 1 : 2 * RGPU_MAX_ATOMS * 3 * 41];
   __shared__ double red[72];
   load_sys(&S, sysp);
   for (int s = threadIdx.x; s < ns; s += blockDim.x) {
