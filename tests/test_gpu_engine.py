@@ -244,3 +244,30 @@ def test_split_launch_matches_single_runs(cuda):
     e.run(10)
     e.sync()
     assert all(g.state()["status"] == 0 for g in gs)
+
+
+def test_mixed_running_totals_within_1e6_on_batched_boxes(cuda):
+    """The metric's bound on its own workload: the first 8 boxes of the
+    batched CO2 set (512-4096 framework atoms per cell, charges up to
+    +-1.2 e), grown from empty over 2000 moves each in one mixed engine;
+    every box's running total energy is within 1e-6 relative of an FP64
+    recomputation of its final configuration."""
+    specs = systems.batched_co2_systems(64, seed=2)[:8]
+    gs = []
+    for i, s in enumerate(specs):
+        g = native.GpuSystem(s, maxmol=768, seed=20240, stream_id=i)
+        g.set_adsorbates(np.zeros((0, s.molecule.n_atoms, 3)))
+        gs.append(g)
+    e = native.Engine(gs, precision=native.RGPU_MIXED, threads=512, cluster=2)
+    for _ in range(4):
+        e.run(500)
+    e.sync()
+    worst = 0.0
+    for g in gs:
+        st = g.state()
+        assert st["status"] == 0
+        if st["nmol"] == 0:
+            continue
+        ref = np.asarray(g.total_energy())
+        worst = max(worst, abs(np.sum(st["energy"][:6]) - ref.sum()) / abs(ref.sum()))
+    assert worst <= 1e-6, worst
