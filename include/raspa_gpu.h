@@ -346,7 +346,9 @@ int rgpu_engine_cluster(rgpu_engine *eng);
 int rgpu_engine_set_split(rgpu_engine *eng, const int *second, int nsecond, int cluster_b);
 int rgpu_engine_destroy(rgpu_engine *eng);
 /* Advances every system by `nsteps` MC moves (asynchronous on `stream`, a
- * cudaStream_t or NULL for the library stream). */
+ * cudaStream_t or NULL for the library stream). RGPU_E_INVALID if a system
+ * was given energy grids after an engine without the flexible-chain/grid
+ * build was created over it. */
 int rgpu_engine_run(rgpu_engine *eng, long long nsteps, void *stream);
 int rgpu_engine_sync(rgpu_engine *eng);
 /* With `on` != 0, rgpu_engine_run replays a CUDA graph of the launch

@@ -1784,6 +1784,11 @@ extern "C" int rgpu_engine_run(rgpu_engine *e, long long nsteps, void *stream)
 {
   if (!e || nsteps < 0) return fail(RGPU_E_INVALID, "bad argument");
   cudaStream_t st = stream ? (cudaStream_t)stream : e->st;
+  /* a system given grids after the engine was built needs the engine's
+   * flexible-chain/grid build */
+  for (rgpu_system *s : e->sys)
+    if ((s->h.use_grid || s->h.flexible) && !e->flex)
+      return fail(RGPU_E_INVALID, "a system needs the flexible-chain/grid build of the engine");
   /* every system's own stream work (uploads) must be visible to the launch */
   for (rgpu_system *s : e->sys) CK(cudaStreamSynchronize(s->st));
   CK(rgpu_engine_prepare(e->mixed, e->wide, e->flex, std::max(e->smem, e->smem_b)));
